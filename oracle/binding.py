@@ -1,0 +1,176 @@
+"""ctypes binding of the CPU FP64 oracle (oracle/liboracle.so).
+
+Test infrastructure only: imported by tests/, __graft_entry__.smoke() and bench.py's
+CPU-baseline legs, never by the product package. Parity status: unpinned against the
+reference binary (it cannot be built here); see oracle/oracle.h.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+_d = C.POINTER(C.c_double)
+_i32 = C.POINTER(C.c_int32)
+_i64 = C.POINTER(C.c_int64)
+_u8 = C.POINTER(C.c_uint8)
+
+
+class NewtonOpts(C.Structure):
+    _fields_ = [
+        ("dt", C.c_double), ("t_final", C.c_double), ("max_steps", C.c_int),
+        ("max_newton", C.c_int), ("tol_rel", C.c_double), ("tol_abs", C.c_double),
+        ("cg_rtol", C.c_double), ("cg_maxit", C.c_int), ("nthreads", C.c_int),
+    ]
+
+
+def build(force: bool = False) -> str:
+    """Compile liboracle.so with the committed Makefile (system g++)."""
+    if force or not os.path.exists(_LIB_PATH) or (
+        os.path.getmtime(_LIB_PATH) < max(os.path.getmtime(os.path.join(_HERE, f))
+                                          for f in ("oracle.cpp", "oracle.h", "Makefile"))):
+        subprocess.run(["make", "-s", "-C", _HERE, "-B" if force else "liboracle.so"], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = C.CDLL(_LIB_PATH)
+        L.orc_nh_stress_tangent.argtypes = [_d, C.c_double, C.c_double, C.c_int, _d, _d]
+        L.orc_set_consistent_tangent.argtypes = [C.c_int]
+        L.orc_set_pattern_mode.argtypes = [C.c_int]
+        L.orc_vol_dU.argtypes = [C.c_int, C.c_double, C.c_double]
+        L.orc_vol_dU.restype = C.c_double
+        L.orc_vol_d2U.argtypes = [C.c_int, C.c_double, C.c_double]
+        L.orc_vol_d2U.restype = C.c_double
+        L.orc_elem_stiffness_residual.argtypes = [C.c_int, _d, _d, C.c_double, C.c_double, C.c_int, _d, _d]
+        L.orc_gauss_rule.argtypes = [C.c_int, _d, _d, _d, _d]
+        L.orc_problem_create.argtypes = [C.c_int, _d, C.c_int, C.c_int, _i32, _i32, C.c_int, _d, _u8]
+        L.orc_problem_create.restype = C.c_void_p
+        L.orc_problem_destroy.argtypes = [C.c_void_p]
+        L.orc_problem_nfree.argtypes = [C.c_void_p]
+        L.orc_problem_nnz.argtypes = [C.c_void_p]
+        L.orc_problem_nnz.restype = C.c_int64
+        L.orc_problem_export_pattern.argtypes = [C.c_void_p, _i32, _i32, _i64, _i32]
+        L.orc_problem_elements.argtypes = [C.c_void_p, _d, _d, _d, C.c_int]
+        L.orc_problem_elements.restype = C.c_int64
+        L.orc_problem_assemble.argtypes = [C.c_void_p, _d, _d, _d, _d, C.c_int]
+        L.orc_problem_assemble.restype = C.c_int64
+        L.orc_cg_jacobi.argtypes = [C.c_void_p, _d, _d, _d, C.c_double, C.c_double, C.c_int, C.c_int,
+                                    C.POINTER(C.c_int), _d]
+        L.orc_newton_run.argtypes = [C.c_void_p, _d, C.POINTER(NewtonOpts), _d, _d, C.c_int]
+        _lib = L
+    return _lib
+
+
+def set_consistent_tangent(on: bool) -> None:
+    lib().orc_set_consistent_tangent(1 if on else 0)
+
+
+def set_pattern_mode(mode: int) -> None:
+    lib().orc_set_pattern_mode(int(mode))
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t) if a is not None else None
+
+
+def nh_stress_tangent(F, mu, Kinv, utype=3):
+    F = np.ascontiguousarray(F, dtype=np.float64).reshape(9)
+    s, Cm = np.zeros(9), np.zeros(81)
+    lib().orc_nh_stress_tangent(_p(F, _d), mu, Kinv, utype, _p(s, _d), _p(Cm, _d))
+    return s, Cm.reshape(9, 9)
+
+
+def elem_stiffness_residual(X, u, mu, Kinv, utype=3):
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    npe = X.shape[0]
+    K, R = np.zeros((3 * npe, 3 * npe)), np.zeros(3 * npe)
+    bad = lib().orc_elem_stiffness_residual(npe, _p(X, _d), _p(u, _d), mu, Kinv, utype, _p(K, _d), _p(R, _d))
+    return K, R, bad
+
+
+def gauss_rule(npe):
+    xi, w = np.zeros((8, 3)), np.zeros(8)
+    N, dN = np.zeros((8, npe)), np.zeros((8, 3, npe))
+    ngp = lib().orc_gauss_rule(npe, _p(xi, _d), _p(w, _d), _p(N, _d), _p(dN, _d))
+    return xi[:ngp], w[:ngp], N[:ngp], dN[:ngp]
+
+
+class OracleProblem:
+    """A mesh with its DOF map and CSR pattern, restating prepareMatrixPattern."""
+
+    def __init__(self, prob):
+        self.prob = prob
+        self._keep = [np.ascontiguousarray(prob.coords, np.float64), np.ascontiguousarray(prob.conn, np.int32),
+                      np.ascontiguousarray(prob.mat_id, np.int32), np.ascontiguousarray(prob.mats, np.float64),
+                      np.ascontiguousarray(prob.fixed, np.uint8)]
+        c, cn, m, mt, fx = self._keep
+        self.h = lib().orc_problem_create(prob.n_node, _p(c, _d), prob.n_elem, prob.npe, _p(cn, _i32),
+                                          _p(m, _i32), mt.shape[0], _p(mt, _d), _p(fx, _u8))
+        if not self.h:
+            raise ValueError("oracle: unsupported element type")
+        self.n_free = lib().orc_problem_nfree(self.h)
+        self.nnz = lib().orc_problem_nnz(self.h)
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.orc_problem_destroy(self.h)
+            self.h = None
+
+    def pattern(self):
+        ns = 3 * self.prob.npe
+        afs = np.zeros(self.n_free, np.int32)
+        fav = np.zeros((self.prob.n_elem, ns), np.int32)
+        rp = np.zeros(self.n_free + 1, np.int64)
+        col = np.zeros(self.nnz, np.int32)
+        lib().orc_problem_export_pattern(self.h, _p(afs, _i32), _p(fav, _i32), _p(rp, _i64), _p(col, _i32))
+        return afs, fav, rp, col
+
+    def elements(self, disp, nthreads=1):
+        ns = 3 * self.prob.npe
+        disp = np.ascontiguousarray(disp, np.float64)
+        Ke = np.zeros((self.prob.n_elem, ns, ns))
+        Re = np.zeros((self.prob.n_elem, ns))
+        bad = lib().orc_problem_elements(self.h, _p(disp, _d), _p(Ke, _d), _p(Re, _d), nthreads)
+        return Ke, Re, int(bad)
+
+    def assemble(self, disp, nthreads=1, want_val=True, want_reac=True):
+        disp = np.ascontiguousarray(disp, np.float64)
+        val = np.zeros(self.nnz) if want_val else None
+        rhs = np.zeros(self.n_free)
+        reac = np.zeros(self.prob.n_dof) if want_reac else None
+        bad = lib().orc_problem_assemble(self.h, _p(disp, _d), _p(val, _d), _p(rhs, _d), _p(reac, _d), nthreads)
+        return val, rhs, reac, int(bad)
+
+    def cg(self, val, b, rtol=1e-12, abstol=1e-50, maxit=10000, nthreads=1):
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.zeros(self.n_free)
+        its, fn = C.c_int(0), C.c_double(0.0)
+        st = lib().orc_cg_jacobi(self.h, _p(val, _d), _p(b, _d), _p(x, _d), rtol, abstol, maxit, nthreads,
+                                 C.byref(its), C.byref(fn))
+        return x, its.value, fn.value, st
+
+    def newton(self, tol_rel=None, tol_abs=0.0, cg_rtol=None, cg_maxit=10000, max_newton=10,
+               nthreads=1, disp=None, max_hist=4096):
+        p = self.prob
+        o = NewtonOpts(p.dt, p.t_final, p.max_steps, max_newton,
+                       p.newton_rtol if tol_rel is None else tol_rel, tol_abs,
+                       p.cg_rtol if cg_rtol is None else cg_rtol, cg_maxit, nthreads)
+        u = np.zeros(p.n_dof) if disp is None else np.array(disp, np.float64)
+        f = np.ascontiguousarray(p.fnodal, np.float64)
+        hist = np.zeros((max_hist, 4))
+        rows = lib().orc_newton_run(self.h, _p(f, _d), C.byref(o), _p(u, _d), _p(hist, _d), max_hist)
+        if rows < 0:
+            raise RuntimeError("oracle Newton: time step size fell below 1% of the initial value")
+        return u, hist[:rows]

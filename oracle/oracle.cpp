@@ -1,0 +1,689 @@
+// oracle.cpp -- CPU FP64 restatement of chennachaos/mphyfem's femSolidmechanics Newton step.
+//
+// TEST INFRASTRUCTURE ONLY: the checker for the CUDA product path and the timed CPU baseline.
+// Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline / --impl reference legs
+// load it. Parity status: unpinned against the reference binary (unbuildable here: PETSc,
+// Eigen, Boost, MPI and VTK are absent); pinned by the analytic and finite-difference checks
+// in tests/test_oracle_*.py. Every function names the reference lines it restates.
+
+#include "oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+constexpr int kMaxNpe = 10;
+constexpr int kMaxGp = 8;
+
+struct GaussRule {
+    int ngp = 0;
+    double xi[kMaxGp][3];
+    double w[kMaxGp];
+};
+
+// 2-point Gauss-Legendre abscissa exactly as written in src/utilities/QuadratureUtil.cpp:24-25.
+constexpr double kGauss2 = 0.577350269189626;
+
+// Hex 2x2x2 rule, point ordering of QuadratureUtil.cpp:481-492 (xi1 fastest, then xi2, xi3,
+// with the (+,+) point of each layer third, matching the hex8 node order).
+void rule_hex8(GaussRule& r) {
+    const double g[2] = {-kGauss2, kGauss2};
+    const int pattern[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0},
+                               {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+    r.ngp = 8;
+    for (int q = 0; q < 8; ++q) {
+        for (int d = 0; d < 3; ++d) r.xi[q][d] = g[pattern[q][d]];
+        r.w[q] = 1.0;
+    }
+}
+
+// Tetrahedron 4-point rule of QuadratureUtil.cpp:690-712 (weights 1/4 of the volume 1/6).
+void rule_tet4(GaussRule& r) {
+    const double a = 0.1381966011250105, b = 0.5854101966249685;
+    const double pts[4][3] = {{a, a, a}, {b, a, a}, {a, b, a}, {a, a, b}};
+    r.ngp = 4;
+    for (int q = 0; q < 4; ++q) {
+        for (int d = 0; d < 3; ++d) r.xi[q][d] = pts[q][d];
+        r.w[q] = 0.25 * (1.0 / 6.0);
+    }
+}
+
+// Trilinear hex: tensor product of the linear 1D Lagrange pair (BasisFunctionsLagrange.cpp:146-152)
+// with the node order of :1243-1250: (-,-,-),(+,-,-),(+,+,-),(-,+,-),(-,-,+),(+,-,+),(+,+,+),(-,+,+).
+void shape_hex8(const double* xi, double* N, double dN[3][kMaxNpe]) {
+    double n1[3][2], d1[3][2];
+    for (int d = 0; d < 3; ++d) {
+        n1[d][0] = 0.5 * (1.0 - xi[d]);
+        n1[d][1] = 0.5 * (1.0 + xi[d]);
+        d1[d][0] = -0.5;
+        d1[d][1] = 0.5;
+    }
+    const int corner[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0},
+                              {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+    for (int a = 0; a < 8; ++a) {
+        const int i = corner[a][0], j = corner[a][1], k = corner[a][2];
+        N[a] = n1[0][i] * n1[1][j] * n1[2][k];
+        dN[0][a] = d1[0][i] * n1[1][j] * n1[2][k];
+        dN[1][a] = n1[0][i] * d1[1][j] * n1[2][k];
+        dN[2][a] = n1[0][i] * n1[1][j] * d1[2][k];
+    }
+}
+
+// Quadratic tetrahedron (BasisFunctionsLagrange.cpp:870-956). Barycentric L0 = 1-x1-x2-x3,
+// vertices 0..3 at L0, x1, x2, x3; mid-side nodes 4:(0,1) 5:(1,2) 6:(0,2) 7:(0,3) 8:(2,3) 9:(1,3).
+void shape_tet10(const double* xi, double* N, double dN[3][kMaxNpe]) {
+    const double L[4] = {1.0 - xi[0] - xi[1] - xi[2], xi[0], xi[1], xi[2]};
+    // dL_v / dxi_d: L0 -> -1 in every direction, L_{d+1} -> 1 in direction d.
+    auto dL = [](int v, int d) { return v == 0 ? -1.0 : (v == d + 1 ? 1.0 : 0.0); };
+    for (int v = 0; v < 4; ++v) {
+        N[v] = L[v] * (2.0 * L[v] - 1.0);
+        for (int d = 0; d < 3; ++d) dN[d][v] = (4.0 * L[v] - 1.0) * dL(v, d);
+    }
+    const int edge[6][2] = {{0, 1}, {1, 2}, {0, 2}, {0, 3}, {2, 3}, {1, 3}};
+    for (int e = 0; e < 6; ++e) {
+        const int p = edge[e][0], q = edge[e][1];
+        N[4 + e] = 4.0 * L[p] * L[q];
+        for (int d = 0; d < 3; ++d) dN[d][4 + e] = 4.0 * (dL(p, d) * L[q] + L[p] * dL(q, d));
+    }
+}
+
+bool element_rule(int npe, GaussRule& r) {
+    if (npe == 8) { rule_hex8(r); return true; }
+    if (npe == 10) { rule_tet4(r); return true; }
+    return false;
+}
+
+void shape(int npe, const double* xi, double* N, double dN[3][kMaxNpe]) {
+    if (npe == 8) shape_hex8(xi, N, dN);
+    else shape_tet10(xi, N, dN);
+}
+
+double det3(const double A[3][3]) {
+    return A[0][0] * (A[1][1] * A[2][2] - A[1][2] * A[2][1]) -
+           A[0][1] * (A[1][0] * A[2][2] - A[1][2] * A[2][0]) +
+           A[0][2] * (A[1][0] * A[2][1] - A[1][1] * A[2][0]);
+}
+
+// Inverse by cofactors (stands in for Eigen's MatrixXd::inverse(); last-ulp differences only).
+void inv3(const double A[3][3], double det, double Ai[3][3]) {
+    const double r = 1.0 / det;
+    Ai[0][0] = (A[1][1] * A[2][2] - A[1][2] * A[2][1]) * r;
+    Ai[0][1] = (A[0][2] * A[2][1] - A[0][1] * A[2][2]) * r;
+    Ai[0][2] = (A[0][1] * A[1][2] - A[0][2] * A[1][1]) * r;
+    Ai[1][0] = (A[1][2] * A[2][0] - A[1][0] * A[2][2]) * r;
+    Ai[1][1] = (A[0][0] * A[2][2] - A[0][2] * A[2][0]) * r;
+    Ai[1][2] = (A[0][2] * A[1][0] - A[0][0] * A[1][2]) * r;
+    Ai[2][0] = (A[1][0] * A[2][1] - A[1][1] * A[2][0]) * r;
+    Ai[2][1] = (A[0][1] * A[2][0] - A[0][0] * A[2][1]) * r;
+    Ai[2][2] = (A[0][0] * A[1][1] - A[0][1] * A[1][0]) * r;
+}
+
+// computeBasisFunctions3D (GeomDataLagrange.cpp:349-458): the mapping gradient
+// G(r, c) = sum_I x_I[c] dN_I/dxi_r, its determinant, and spatial gradients
+// dN/dx_c = sum_r dN/dxi_r * Ginv(c, r).
+double spatial_gradients(int npe, const double* x, const double dN[3][kMaxNpe],
+                         double grad[3][kMaxNpe]) {
+    double G[3][3] = {{0}};
+    for (int I = 0; I < npe; ++I)
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) G[r][c] += x[3 * I + c] * dN[r][I];
+    const double jac = det3(G);
+    double Gi[3][3];
+    inv3(G, jac, Gi);
+    for (int I = 0; I < npe; ++I)
+        for (int c = 0; c < 3; ++c)
+            grad[c][I] = dN[0][I] * Gi[c][0] + dN[1][I] * Gi[c][1] + dN[2][I] * Gi[c][2];
+    return jac;
+}
+
+// 9-index <-> (i, j) of src/material/utilitiesmaterialHyperelastic.cpp:192 (column-major 3x3).
+constexpr int kPairI[9] = {0, 1, 2, 0, 1, 2, 0, 1, 2};
+constexpr int kPairJ[9] = {0, 0, 0, 1, 1, 1, 2, 2, 2};
+
+inline double kd(int a, int b) { return a == b ? 1.0 : 0.0; }
+
+// 0: the reference's tangent (volumetric part without the geometric stress term,
+// utilitiesmaterialHyperelastic.cpp:283-288); 1: the consistent tangent, which adds
+// U'(J) d_ik d_jl back. Test-only switch for the consistency checks.
+int g_consistent_tangent = 0;
+// 0: pick the pattern construction by size; 1: always the literal per-element push_back
+// restatement; 2: always the per-node construction. Test-only switch (both give one pattern).
+int g_pattern_mode = 0;
+
+struct CsrPattern {
+    int n_free = 0;
+    std::vector<int32_t> node_dof;       // [n_node*3] free id or -1 (NodeDofArray)
+    std::vector<int32_t> assy_for_soln;  // [n_free]
+    std::vector<int32_t> for_assy;       // [n_elem][3npe] (forAssyVec)
+    std::vector<int64_t> rowptr;         // [n_free+1]
+    std::vector<int32_t> col;            // [nnz]
+};
+
+}  // namespace
+
+struct orc_problem {
+    int n_node, n_elem, npe;
+    std::vector<double> coords;
+    std::vector<int32_t> conn, mat_id;
+    std::vector<double> mats;  // [n_mat][3]
+    std::vector<uint8_t> fixed;
+    CsrPattern pat;
+    // position of each (element row i, element col j) entry in the CSR value array, -1 if
+    // either DOF is prescribed (what MatSetValue's row search resolves, SolverPetsc.cpp:370-374)
+    std::vector<int64_t> slot;  // [n_elem][nsize*nsize]
+};
+
+extern "C" {
+
+double orc_vol_dU(int type, double K, double J) {
+    switch (type) {
+        case -1: return 0.0;
+        case 1: return 0.1 * K * (std::pow(J, 4) - 1.0 / std::pow(J, 6));
+        case 2: return 0.125 * K * (J * J - 1.0 / (J * J)) * (J + 1.0 / (J * J * J));
+        case 3: return K * (J - 1.0);
+        case 4: return 0.5 * K * (J - 1.0 / J);
+        case 5: return 0.5 * K * (J - 1.0 + std::log(J) / J);
+        case 6: return K * std::log(J);
+        case 7: return K * (1.0 - 1.0 / J);
+        case 8: return K * std::log(J) / J;
+        default: return 0.0;
+    }
+}
+
+double orc_vol_d2U(int type, double K, double J) {
+    switch (type) {
+        case -1: return 0.0;
+        case 1: return 0.2 * K * (2.0 * J * J * J + 3.0 / std::pow(J, 7));
+        case 2: return 0.125 * K * (3.0 * J * J + 5.0 / std::pow(J, 6));
+        case 3: return K;
+        case 4: return 0.5 * K * (1.0 + 1.0 / (J * J));
+        case 5: return 0.5 * K * (J * J + 1.0 - std::log(J)) / (J * J);
+        case 6: return K / std::log(J);
+        case 7: return K / (J * J);
+        case 8: return K * (1.0 - std::log(J)) / (J * J);
+        default: return 0.0;
+    }
+}
+
+// Compressible Neo-Hookean, utilitiesmaterialHyperelastic.cpp:186-295 with MIXED_ELEMENT false:
+//   sigma = mu J^{-5/3} (b - Ib/3 I) + U'(J) I
+//   C_{ijkl} = (mu J^{-5/3} Ib/3) d_il d_jk - (2/3) mu J^{-5/3} (b_ij d_kl + d_ij b_kl)
+//            + (2/9) mu J^{-5/3} Ib d_ij d_kl + mu J^{-5/3} b_jl d_ik
+//            + (J U'' + U') d_ij d_kl - U' d_il d_jk - U' d_jl d_ik
+int orc_nh_stress_tangent(const double* Fm, double mu, double Kinv, int Utype, double* stre,
+                          double* C) {
+    const double K = 1.0 / Kinv;
+    double F[3][3], b[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) F[i][j] = Fm[3 * i + j];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) b[i][j] = F[i][0] * F[j][0] + F[i][1] * F[j][1] + F[i][2] * F[j][2];
+    const double J = det3(F);
+    const double Jm2d3 = std::pow(J, -2.0 / 3.0);
+    const double Jm5d3 = Jm2d3 / J;
+    const double Ib = b[0][0] + b[1][1] + b[2][2];
+    const double dU = orc_vol_dU(Utype, K, J);
+    const double d2U = orc_vol_d2U(Utype, K, J);
+
+    const double s1 = mu * Jm5d3;
+    const double s2 = -s1 * (1.0 / 3.0) * Ib + dU;
+    for (int q = 0; q < 9; ++q) {
+        const int i = kPairI[q], j = kPairJ[q];
+        stre[q] = s1 * b[i][j] + (i == j ? s2 : 0.0);
+    }
+
+    const double c_iljk = (1.0 / 3.0) * mu * Jm5d3 * Ib;  // with d_il d_jk
+    const double c_bdd = -(2.0 / 3.0) * mu * Jm5d3;        // with b_ij d_kl + d_ij b_kl
+    const double c_dd = (2.0 / 3.0) * (1.0 / 3.0) * mu * Jm5d3 * Ib;
+    const double c_bjl = mu * Jm5d3;                       // with b_jl d_ik
+    const double c_vol = J * d2U + dU;                     // with d_ij d_kl
+    for (int p = 0; p < 9; ++p) {
+        const int i = kPairI[p], j = kPairJ[p];
+        for (int q = 0; q < 9; ++q) {
+            const int k = kPairI[q], l = kPairJ[q];
+            double v = 0.0;
+            v += c_iljk * (kd(i, l) * kd(j, k));
+            v += c_bdd * (b[i][j] * kd(k, l) + kd(i, j) * b[k][l]);
+            v += c_dd * (kd(i, j) * kd(k, l));
+            v += c_bjl * (b[j][l] * kd(i, k));
+            v += c_vol * (kd(i, j) * kd(k, l)) - dU * (kd(i, l) * kd(j, k)) - dU * (kd(j, l) * kd(i, k));
+            if (g_consistent_tangent) v += dU * (kd(j, l) * kd(i, k));
+            C[9 * p + q] = v;
+        }
+    }
+    return 0;
+}
+
+void orc_set_consistent_tangent(int on) { g_consistent_tangent = on ? 1 : 0; }
+void orc_set_pattern_mode(int mode) { g_pattern_mode = mode; }
+
+int orc_gauss_rule(int npe, double* xi, double* w, double* N, double* dNdxi) {
+    GaussRule r;
+    if (!element_rule(npe, r)) return 0;
+    for (int q = 0; q < r.ngp; ++q) {
+        double n[kMaxNpe], dn[3][kMaxNpe];
+        shape(npe, r.xi[q], n, dn);
+        for (int d = 0; d < 3; ++d) xi[3 * q + d] = r.xi[q][d];
+        w[q] = r.w[q];
+        for (int a = 0; a < npe; ++a) {
+            N[q * npe + a] = n[a];
+            for (int d = 0; d < 3; ++d) dNdxi[(q * 3 + d) * npe + a] = dn[d][a];
+        }
+    }
+    return r.ngp;
+}
+
+// Elem_Solid_3D_Disp::calcStiffnessAndResidual (Elem_Solid_3D_Disp.cpp:196-373), STATIC
+// scheme: af = td[2] = 1, no inertia or body force. The two configurations are built as in
+// the reference: F from the reference-configuration gradients (ElementBase.cpp:334-361),
+// then gradients and volume in the current configuration x = X + u.
+int orc_elem_stiffness_residual(int npe, const double* X, const double* u, double mu, double Kinv,
+                                int Utype, double* K, double* R) {
+    GaussRule rule;
+    if (!element_rule(npe, rule)) return 2;
+    const int ns = 3 * npe;
+    std::fill(K, K + ns * ns, 0.0);
+    std::fill(R, R + ns, 0.0);
+    double x[3 * kMaxNpe];
+    for (int a = 0; a < 3 * npe; ++a) x[a] = X[a] + u[a];
+    int bad = 0;
+    for (int q = 0; q < rule.ngp; ++q) {
+        double N[kMaxNpe], dN[3][kMaxNpe], g0[3][kMaxNpe], g[3][kMaxNpe];
+        shape(npe, rule.xi[q], N, dN);
+        spatial_gradients(npe, X, dN, g0);
+        double F[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+        for (int I = 0; I < npe; ++I)
+            for (int a = 0; a < 3; ++a)
+                for (int m = 0; m < 3; ++m) F[3 * a + m] += u[3 * I + a] * g0[m][I];
+        double Fa[3][3];
+        for (int i = 0; i < 9; ++i) Fa[i / 3][i % 3] = F[i];
+        if (det3(Fa) < 0.0) bad = 1;
+        const double dvol = rule.w[q] * spatial_gradients(npe, x, dN, g);
+        double stre[9], C[81];
+        orc_nh_stress_tangent(F, mu, Kinv, Utype, stre, C);
+        for (int I = 0; I < npe; ++I) {
+            const double bb[3] = {dvol * g[0][I], dvol * g[1][I], dvol * g[2][I]};
+            double Gc[3][9];
+            for (int kk = 0; kk < 9; ++kk)
+                for (int a = 0; a < 3; ++a)
+                    Gc[a][kk] = bb[0] * C[9 * a + kk] + bb[1] * C[9 * (3 + a) + kk] + bb[2] * C[9 * (6 + a) + kk];
+            for (int a = 0; a < 3; ++a)
+                R[3 * I + a] -= bb[0] * stre[a] + bb[1] * stre[3 + a] + bb[2] * stre[6 + a];
+            for (int J = 0; J < npe; ++J) {
+                const double c[3] = {g[0][J], g[1][J], g[2][J]};
+                for (int a = 0; a < 3; ++a)
+                    for (int b = 0; b < 3; ++b)
+                        K[(3 * I + a) * ns + 3 * J + b] +=
+                            Gc[a][b] * c[0] + Gc[a][3 + b] * c[1] + Gc[a][6 + b] * c[2];
+            }
+        }
+    }
+    return bad;
+}
+
+}  // extern "C"
+
+namespace {
+
+// prepareMatrixPattern (femSolidmechanics2.cpp:121-478), single-rank branch: free DOFs
+// numbered node-major skipping prescribed ones (:142-152), assyForSoln (:155-165),
+// forAssyVec (:248-280), and per row the sorted unique union of the free columns of every
+// element that touches it (:294-324, :390, findUnique = sort + unique).
+void build_pattern(orc_problem* p) {
+    CsrPattern& P = p->pat;
+    const int nd = 3 * p->n_node, ns = 3 * p->npe;
+    P.node_dof.assign(nd, -1);
+    P.n_free = 0;
+    for (int n = 0; n < p->n_node; ++n)
+        for (int d = 0; d < 3; ++d)
+            if (!p->fixed[3 * n + d]) P.node_dof[3 * n + d] = P.n_free++;
+    P.assy_for_soln.clear();
+    for (int i = 0; i < nd; ++i)
+        if (P.node_dof[i] != -1) P.assy_for_soln.push_back(i);
+    P.for_assy.resize((size_t)p->n_elem * ns);
+    for (int e = 0; e < p->n_elem; ++e)
+        for (int I = 0; I < p->npe; ++I)
+            for (int d = 0; d < 3; ++d)
+                P.for_assy[(size_t)e * ns + 3 * I + d] = P.node_dof[3 * p->conn[(size_t)e * p->npe + I] + d];
+
+    const double literal_entries = (double)p->n_elem * ns * ns;
+    std::vector<std::vector<int32_t>> rows(P.n_free);
+    const bool literal = g_pattern_mode == 1 || (g_pattern_mode == 0 && literal_entries < 6.0e7);
+    if (literal) {
+        // literal restatement: every element pushes every free column into every free row
+        for (int e = 0; e < p->n_elem; ++e) {
+            const int32_t* fa = &P.for_assy[(size_t)e * ns];
+            for (int i = 0; i < ns; ++i) {
+                if (fa[i] == -1) continue;
+                for (int j = 0; j < ns; ++j)
+                    if (fa[j] != -1) rows[fa[i]].push_back(fa[j]);
+            }
+        }
+        for (auto& r : rows) {
+            std::sort(r.begin(), r.end());
+            r.erase(std::unique(r.begin(), r.end()), r.end());
+        }
+    } else {
+        // same set, built per node to bound memory on large meshes: the free columns of row
+        // (n, d) are the free DOFs of every node sharing an element with n, ascending
+        std::vector<std::vector<int32_t>> adj(p->n_node);
+        for (int e = 0; e < p->n_elem; ++e) {
+            const int32_t* cn = &p->conn[(size_t)e * p->npe];
+            for (int I = 0; I < p->npe; ++I)
+                for (int J = 0; J < p->npe; ++J) adj[cn[I]].push_back(cn[J]);
+        }
+        for (int n = 0; n < p->n_node; ++n) {
+            auto& a = adj[n];
+            std::sort(a.begin(), a.end());
+            a.erase(std::unique(a.begin(), a.end()), a.end());
+            for (int d = 0; d < 3; ++d) {
+                const int r = P.node_dof[3 * n + d];
+                if (r == -1) continue;
+                for (int m : a)
+                    for (int c = 0; c < 3; ++c)
+                        if (P.node_dof[3 * m + c] != -1) rows[r].push_back(P.node_dof[3 * m + c]);
+            }
+            std::vector<int32_t>().swap(a);
+        }
+    }
+    P.rowptr.assign(P.n_free + 1, 0);
+    for (int r = 0; r < P.n_free; ++r) P.rowptr[r + 1] = P.rowptr[r] + (int64_t)rows[r].size();
+    P.col.resize(P.rowptr[P.n_free]);
+    for (int r = 0; r < P.n_free; ++r) {
+        std::copy(rows[r].begin(), rows[r].end(), P.col.begin() + P.rowptr[r]);
+        std::vector<int32_t>().swap(rows[r]);
+    }
+
+    // value slot of every element entry (the AIJ row search MatSetValue performs)
+    p->slot.assign((size_t)p->n_elem * ns * ns, -1);
+    for (int e = 0; e < p->n_elem; ++e) {
+        const int32_t* fa = &P.for_assy[(size_t)e * ns];
+        for (int i = 0; i < ns; ++i) {
+            if (fa[i] == -1) continue;
+            const int32_t* b = &P.col[P.rowptr[fa[i]]];
+            const int32_t* en = &P.col[P.rowptr[fa[i] + 1]];
+            for (int j = 0; j < ns; ++j) {
+                if (fa[j] == -1) continue;
+                const int32_t* it = std::lower_bound(b, en, fa[j]);
+                p->slot[((size_t)e * ns + i) * ns + j] = P.rowptr[fa[i]] + (it - b);
+            }
+        }
+    }
+}
+
+inline void set_threads(int nthreads) {
+#ifdef _OPENMP
+    omp_set_num_threads(nthreads > 0 ? nthreads : 1);
+#else
+    (void)nthreads;
+#endif
+}
+
+void gather_element(const orc_problem* p, int64_t e, const double* disp, double* X, double* u) {
+    for (int I = 0; I < p->npe; ++I) {
+        const int n = p->conn[e * p->npe + I];
+        for (int d = 0; d < 3; ++d) {
+            X[3 * I + d] = p->coords[3 * (size_t)n + d];
+            u[3 * I + d] = disp[3 * (size_t)n + d];
+        }
+    }
+}
+
+void elem_eval(const orc_problem* p, int64_t e, const double* disp, double* K, double* R, int* bad) {
+    double X[3 * kMaxNpe], u[3 * kMaxNpe];
+    gather_element(p, e, disp, X, u);
+    const double* m = &p->mats[3 * (size_t)p->mat_id[e]];
+    *bad = orc_elem_stiffness_residual(p->npe, X, u, m[0], m[1], (int)m[2], K, R);
+}
+
+}  // namespace
+
+extern "C" {
+
+orc_problem* orc_problem_create(int n_node, const double* coords, int n_elem, int npe,
+                                const int32_t* conn, const int32_t* mat_id, int n_mat,
+                                const double* mats, const uint8_t* fixed) {
+    if (npe != 8 && npe != 10) return nullptr;
+    orc_problem* p = new orc_problem;
+    p->n_node = n_node;
+    p->n_elem = n_elem;
+    p->npe = npe;
+    p->coords.assign(coords, coords + 3 * (size_t)n_node);
+    p->conn.assign(conn, conn + (size_t)n_elem * npe);
+    p->mat_id.assign(mat_id, mat_id + n_elem);
+    p->mats.assign(mats, mats + 3 * (size_t)n_mat);
+    p->fixed.assign(fixed, fixed + 3 * (size_t)n_node);
+    build_pattern(p);
+    return p;
+}
+
+void orc_problem_destroy(orc_problem* p) { delete p; }
+int orc_problem_nfree(const orc_problem* p) { return p->pat.n_free; }
+int64_t orc_problem_nnz(const orc_problem* p) { return p->pat.rowptr.back(); }
+
+void orc_problem_export_pattern(const orc_problem* p, int32_t* assy_for_soln, int32_t* for_assy_vec,
+                                int64_t* rowptr, int32_t* col) {
+    const CsrPattern& P = p->pat;
+    if (assy_for_soln) std::copy(P.assy_for_soln.begin(), P.assy_for_soln.end(), assy_for_soln);
+    if (for_assy_vec) std::copy(P.for_assy.begin(), P.for_assy.end(), for_assy_vec);
+    if (rowptr) std::copy(P.rowptr.begin(), P.rowptr.end(), rowptr);
+    if (col) std::copy(P.col.begin(), P.col.end(), col);
+}
+
+int64_t orc_problem_elements(const orc_problem* p, const double* disp, double* Ke, double* Re,
+                             int nthreads) {
+    const int ns = 3 * p->npe;
+    // the first bad element in ascending order, as the reference's serial loop meets it
+    int64_t first_bad = p->n_elem;
+    set_threads(nthreads);
+#pragma omp parallel for schedule(static) reduction(min : first_bad) if (nthreads > 1)
+    for (int64_t e = 0; e < p->n_elem; ++e) {
+        int bad = 0;
+        elem_eval(p, e, disp, Ke + e * ns * ns, Re + e * ns, &bad);
+        if (bad && e < first_bad) first_bad = e;
+    }
+    return first_bad == p->n_elem ? -1 : first_bad;
+}
+
+int64_t orc_problem_assemble(const orc_problem* p, const double* disp, double* val, double* rhs,
+                             double* reac, int nthreads) {
+    const CsrPattern& P = p->pat;
+    const int ns = 3 * p->npe;
+    if (val) std::fill(val, val + P.rowptr.back(), 0.0);
+    if (rhs) std::fill(rhs, rhs + P.n_free, 0.0);
+    if (reac) std::fill(reac, reac + 3 * (size_t)p->n_node, 0.0);
+    int64_t first_bad = p->n_elem;
+    set_threads(nthreads);
+    const bool par = nthreads > 1;
+#pragma omp parallel if (par)
+    {
+        std::vector<double> K(ns * ns), R(ns);
+#pragma omp for schedule(static) reduction(min : first_bad)
+        for (int64_t e = 0; e < p->n_elem; ++e) {
+            int bad = 0;
+            elem_eval(p, e, disp, K.data(), R.data(), &bad);
+            if (bad && e < first_bad) first_bad = e;
+            const int32_t* fa = &P.for_assy[e * ns];
+            const int64_t* sl = &p->slot[e * ns * ns];
+            for (int i = 0; i < ns; ++i) {
+                if (fa[i] == -1) continue;
+                if (rhs) {
+                    if (par) {
+#pragma omp atomic
+                        rhs[fa[i]] += R[i];
+                    } else {
+                        rhs[fa[i]] += R[i];
+                    }
+                }
+                if (val) {
+                    for (int j = 0; j < ns; ++j) {
+                        const int64_t s = sl[i * ns + j];
+                        if (s < 0) continue;
+                        if (par) {
+#pragma omp atomic
+                            val[s] += K[i * ns + j];
+                        } else {
+                            val[s] += K[i * ns + j];
+                        }
+                    }
+                }
+            }
+            if (reac) {
+                for (int I = 0; I < p->npe; ++I)
+                    for (int d = 0; d < 3; ++d) {
+                        const size_t g = 3 * (size_t)p->conn[e * p->npe + I] + d;
+                        if (par) {
+#pragma omp atomic
+                            reac[g] += R[3 * I + d];
+                        } else {
+                            reac[g] += R[3 * I + d];
+                        }
+                    }
+            }
+        }
+    }
+    return first_bad == p->n_elem ? -1 : first_bad;
+}
+
+// KSPCG (Hestenes-Stiefel) with PCJACOBI, restated from PETSc's documented algorithm as the
+// reference's solver runs it (SolverPetsc.cpp:250-314: zero initial guess, KSPSolve).
+// Norm type KSP_NORM_PRECONDITIONED; KSPConvergedDefault tests ||z_k|| against
+// max(rtol * ||z_0||, abstol).
+int orc_cg_jacobi(const orc_problem* p, const double* val, const double* b, double* x, double rtol,
+                  double abstol, int maxit, int nthreads, int* its_out, double* final_norm) {
+    const CsrPattern& P = p->pat;
+    const int n = P.n_free;
+    set_threads(nthreads);
+    const bool par = nthreads > 1;
+    std::vector<double> dinv(n), r(b, b + n), z(n), pv(n), q(n);
+#pragma omp parallel for if (par)
+    for (int i = 0; i < n; ++i) {
+        double d = 0.0;
+        for (int64_t k = P.rowptr[i]; k < P.rowptr[i + 1]; ++k)
+            if (P.col[k] == i) d = val[k];
+        dinv[i] = d != 0.0 ? 1.0 / d : 1.0;  // PCJACOBI replaces a zero diagonal by 1
+        x[i] = 0.0;
+    }
+    auto dot = [&](const std::vector<double>& a, const std::vector<double>& c) {
+        double s = 0.0;
+#pragma omp parallel for reduction(+ : s) if (par)
+        for (int i = 0; i < n; ++i) s += a[i] * c[i];
+        return s;
+    };
+#pragma omp parallel for if (par)
+    for (int i = 0; i < n; ++i) z[i] = dinv[i] * r[i];
+    double dp = std::sqrt(dot(z, z));
+    const double ttol = std::max(rtol * dp, abstol);
+    int its = 0, status = 1;
+    if (final_norm) *final_norm = dp;
+    if (dp <= ttol) {
+        if (its_out) *its_out = 0;
+        return 0;
+    }
+    double beta = dot(z, r), betaold = 0.0;
+    for (int i = 0; i < maxit; ++i) {
+        its = i + 1;
+        if (beta == 0.0) { status = 0; break; }
+        if (i == 0) {
+            pv = z;
+        } else {
+            const double bk = beta / betaold;
+#pragma omp parallel for if (par)
+            for (int k = 0; k < n; ++k) pv[k] = z[k] + bk * pv[k];
+        }
+#pragma omp parallel for schedule(static) if (par)
+        for (int row = 0; row < n; ++row) {
+            double s = 0.0;
+            for (int64_t k = P.rowptr[row]; k < P.rowptr[row + 1]; ++k) s += val[k] * pv[P.col[k]];
+            q[row] = s;
+        }
+        const double dpi = dot(q, pv);
+        betaold = beta;
+        if (!(dpi > 0.0)) { status = std::isnan(dpi) ? 3 : 2; break; }
+        const double a = beta / dpi;
+#pragma omp parallel for if (par)
+        for (int k = 0; k < n; ++k) {
+            x[k] += a * pv[k];
+            r[k] -= a * q[k];
+            z[k] = dinv[k] * r[k];
+        }
+        dp = std::sqrt(dot(z, z));
+        if (final_norm) *final_norm = dp;
+        if (std::isnan(dp)) { status = 3; break; }
+        if (dp <= ttol) { status = 0; break; }
+        beta = dot(z, r);
+    }
+    if (its_out) *its_out = its;
+    return status;
+}
+
+// solveWithNewtonRaphson (femSolidmechanics2.cpp:730-851) for the STATIC scheme with nodal
+// forces (addExternalForces, femSolidmechanics1.cpp:1094-1113), the load factor of the time
+// function "1 0 1000 0 1 0 0 0 0 0 0" (lambda(t) = t, TimeFunction.cpp:47-68), converged()
+// and diverging(1e7) of femSolidmechanics1.cpp:616-636, and MyTime::cut/reset on failure
+// (MyTime.cpp:41-58, SolutionDataSolid.cpp:157-167).
+int orc_newton_run(const orc_problem* p, const double* fnodal, const orc_newton_opts* o,
+                   double* disp, double* hist, int max_hist) {
+    const CsrPattern& P = p->pat;
+    const int n = P.n_free;
+    const size_t nd = 3 * (size_t)p->n_node;
+    std::vector<double> val(P.rowptr.back()), rhs(n), dx(n), disp_prev(nd);
+    double t = 0.0, dt = o->dt;
+    const double dt0 = o->dt;
+    int steps_done = 1, rows = 0;
+    while (t <= o->t_final - 1.0e-10 && steps_done <= o->max_steps) {
+        t += dt;
+        const double lambda = t;
+        std::copy(disp, disp + nd, disp_prev.begin());
+        bool converged = false;
+        double norm = -1.0, norm_prev = -1.0, tol = o->tol_abs;
+        for (int iter = 1; iter <= o->max_newton; ++iter) {
+            const int64_t bad = orc_problem_assemble(p, disp, val.data(), rhs.data(), nullptr, o->nthreads);
+            if (bad >= 0) break;  // "Negative Jacobian encountered": the iteration loop ends
+            for (int i = 0; i < n; ++i) rhs[i] += lambda * fnodal[P.assy_for_soln[i]];
+            norm_prev = norm;
+            double s = 0.0;
+            for (int i = 0; i < n; ++i) s += rhs[i] * rhs[i];
+            norm = std::sqrt(s);
+            if (iter == 1) tol = std::max(o->tol_abs, o->tol_rel * norm);
+            int its = 0;
+            bool stop = false;
+            if (norm < tol) {
+                converged = true;
+                stop = true;
+            } else if (iter > 3 && (std::isnan(norm) || (norm_prev > -0.1 && norm / norm_prev > 1.0e7))) {
+                stop = true;
+            } else {
+                double fn = 0.0;
+                orc_cg_jacobi(p, val.data(), rhs.data(), dx.data(), o->cg_rtol, 1.0e-50, o->cg_maxit,
+                              o->nthreads, &its, &fn);
+                for (int i = 0; i < n; ++i) disp[P.assy_for_soln[i]] += dx[i];
+            }
+            if (rows < max_hist && hist) {
+                hist[4 * rows + 0] = steps_done;
+                hist[4 * rows + 1] = iter;
+                hist[4 * rows + 2] = norm;
+                hist[4 * rows + 3] = its;
+                ++rows;
+            }
+            if (stop) break;
+        }
+        if (converged) {
+            ++steps_done;
+        } else {
+            t -= dt;
+            dt *= 0.5;
+            if (dt < dt0 * 0.01) return -1;
+            std::copy(disp_prev.begin(), disp_prev.end(), disp);
+        }
+    }
+    return rows;
+}
+
+}  // extern "C"
