@@ -1,0 +1,337 @@
+"""Benchmark of the femSolidmechanics Newton step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload large|small]
+
+A step is one full Newton iteration of the hex8 Neo-Hookean cantilever at 256(x) x 64 x 64
+(1,048,576 elements, 3,257,475 DOFs), first load step (lambda = 0.2, u = 0): fused element
+evaluation + scatter assembly, external loads, FP64 residual norm, Jacobi-PCG to the stated
+relative tolerance (PETSc KSPCG semantics) and the displacement update. Every step starts from
+the same state, so every step does identical work. The matrix (2.2 GB of FP64 values) is
+larger than L2, so no flush is needed between steps.
+
+--impl reference times the CPU restatement of the reference's path (the oracle: the
+reference itself cannot be built on this image) on the host cores, on the same workload.
+Under torchrun each rank runs an independent replica (the path has no exchange step).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+LAMBDA = 0.2
+METRIC = "Newton iters/s (FP64 assembly + Jacobi-PCG to rtol, hex8 Neo-Hookean cantilever)"
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _workload(name: str):
+    from mphyfem_b200 import meshgen
+    if name == "small":
+        return meshgen.cantilever_small()
+    return meshgen.cantilever_large()
+
+
+def _config(prob, rtol):
+    return {
+        "workload": f"{prob.name}: one Newton iteration (assembly + loads + norm + Jacobi-PCG rtol {rtol:g} "
+                    f"+ update), lambda={LAMBDA}, u=0",
+        "n_elem": prob.n_elem, "n_node": prob.n_node, "n_dof": prob.n_dof, "n_free": prob.n_free,
+        "element": "hex8, 2x2x2 Gauss, compressible Neo-Hookean mu=1 kappa=10 (Utype 3)",
+        "tangent": "reference (utilitiesmaterialHyperelastic.cpp as written)",
+        "l2_flush": "not needed: the FP64 matrix (~2.2 GB) exceeds the 126 MB L2",
+    }
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
+             "clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = [r.split(",") for r in (getattr(self, "out", "") or "").strip().splitlines() if r.count(",") >= 6]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(r[0]) for r in rows if r[0].strip().replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[3:7]) if "Active" in v and "Not" not in v})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def _read_traffic(kind: str):
+    """DRAM bytes per launch from a committed ncu summary (profiles/*.txt line 'dram_bytes_per_launch_<kind>: X')."""
+    d = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(d):
+        return None
+    key = f"dram_bytes_per_launch_{kind}:"
+    for fn in sorted(os.listdir(d)):
+        if fn.endswith(".txt"):
+            for line in open(os.path.join(d, fn)):
+                if line.strip().startswith(key):
+                    try:
+                        return float(line.split(":", 1)[1].split()[0])
+                    except ValueError:
+                        return None
+    return None
+
+
+# ------------------------------------------------------------------------------------- CPU side
+def cpu_newton_estimate(prob, gpu_its: int, rtol: float):
+    """Time the oracle (CPU restatement of the reference path) on bounded samples and scale to
+    the full workload: assembly per element on a 64x16x16 block, one CG iteration per nonzero on a
+    96x24x24 block, at the GPU's Krylov iteration count. About 10-20 s of CPU work."""
+    from mphyfem_b200 import meshgen
+    from oracle import binding
+    binding.build()
+    nthreads = os.cpu_count() or 1
+    a = meshgen.hex8_cantilever(64, 16, 16)
+    oa = binding.OracleProblem(a)
+    u0 = np.zeros(a.n_dof)
+    oa.assemble(u0, nthreads=nthreads)
+    t0 = time.perf_counter()
+    reps = 3
+    for _ in range(reps):
+        oa.assemble(u0, nthreads=nthreads, want_reac=False)
+    t_elem = (time.perf_counter() - t0) / reps / a.n_elem
+    b = meshgen.hex8_cantilever(96, 24, 24)
+    ob = binding.OracleProblem(b)
+    val, rhs, _, _ = ob.assemble(np.zeros(b.n_dof), nthreads=nthreads, want_reac=False)
+    rhs = rhs + LAMBDA * b.fnodal[np.flatnonzero(b.fixed == 0)]
+    cg_its = 60
+    t0 = time.perf_counter()
+    ob.cg(val, rhs, rtol=1e-30, maxit=cg_its, nthreads=nthreads)
+    t_cg_nnz = (time.perf_counter() - t0) / cg_its / ob.nnz
+    # nnz of the full workload from its node-block structure (3 free DOFs per free node)
+    nnz_full = _structured_nnz(prob)
+    t_asm = t_elem * prob.n_elem
+    t_iter = t_cg_nnz * nnz_full
+    t_newton = t_asm + gpu_its * t_iter
+    return {
+        "value": 1.0 / t_newton, "unit": "Newton iter/s", "cores": nthreads, "kind": "port",
+        "sample": (f"oracle (FP64 C++ restatement, OpenMP {nthreads} threads): assembly timed on "
+                   f"{a.n_elem} elements ({t_elem * 1e6:.2f} us/elem), CG timed for {cg_its} iterations on "
+                   f"{ob.nnz} nonzeros; scaled to {prob.n_elem} elements / {nnz_full} nonzeros at the GPU's "
+                   f"{gpu_its} Krylov iterations (extrapolated)"),
+        "assembly_s": t_asm, "cg_iter_s": t_iter,
+    }
+
+
+def _structured_nnz(prob):
+    nx, ny, nz = prob.meta["nx"], prob.meta["ny"], prob.meta["nz"]
+
+    def nb(n):  # neighbours of each grid index along one axis, summed over the axis
+        return np.array([min(i + 1, n) - max(i - 1, 0) + 1 for i in range(n + 1)])
+    bx, by, bz = nb(nx), nb(ny), nb(nz)
+    # free rows: nodes with i > 0; free columns: neighbours with i > 0
+    bx_free_rows = bx[1:].copy()
+    bx_free_rows[0] -= 1  # node i=1 loses its i=0 neighbour
+    blocks = int(bx_free_rows.sum()) * int(by.sum()) * int(bz.sum())
+    return 9 * blocks
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    prob = _workload(args.workload)
+    its = args.ref_its
+    samples = []
+    est = None
+    for _ in range(max(1, args.warmup)):
+        est = cpu_newton_estimate(prob, its, args.rtol)
+    for _ in range(max(1, args.steps)):
+        est = cpu_newton_estimate(prob, its, args.rtol)
+        samples.append(1.0 / est["value"])
+    t = statistics.median(samples)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": 1.0 / t, "unit": "Newton iter/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": _config(prob, args.rtol),
+        "cpu_baseline": {k: est[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": 1.0 / t, "unit": "Newton iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference (PETSc/Eigen/Boost/MPI/VTK build) cannot be built on this image; "
+                "its path is timed through the FP64 CPU restatement",
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------------------------- GPU side
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    if not torch.cuda.is_available():
+        print(json.dumps({"metric": METRIC, "error": "no CUDA device"}))
+        sys.exit(2)
+    from mphyfem_b200 import api
+
+    prob = _workload(args.workload)
+    ctx = api.Context(local)
+    mesh = api.Mesh(ctx, prob)
+    pat = api.Pattern(mesh)
+    sol = api.SolverGpu(mesh, pat, rtol=args.rtol, max_it=args.max_it)
+    stream = torch.cuda.ExternalStream(sol.stream, device=f"cuda:{local}")
+    disp = torch.zeros(prob.n_dof, dtype=torch.float64, device=f"cuda:{local}")
+    fext = torch.tensor(prob.fnodal, dtype=torch.float64, device=f"cuda:{local}")
+
+    def step():
+        disp.zero_()
+        return sol.newton_iteration(disp, fext, LAMBDA)
+
+    for _ in range(args.warmup):
+        st = step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    stats = []
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            stats.append(step())
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
+    if world > 1:
+        dist.barrier()
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    its = [s.krylov_its for s in stats]
+    asm_ms = statistics.median([s.t_assembly_ms for s in stats])
+    launches = int(sum(s.kernel_launches for s in stats))
+
+    # dominant kernel: the SpMV of the Krylov loop, timed standalone with events on its stream
+    mi = sol.matrix_info()
+    x = torch.randn(prob.n_dof, dtype=torch.float64, device=f"cuda:{local}")
+    y = torch.empty_like(x)
+    for _ in range(3):
+        sol.spmv(x, y)
+    nrep = 20
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(nrep):
+        sol.spmv(x, y)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    spmv_ms = e0.elapsed_time(e1) / nrep
+    spmv_bytes = mi["true_blocks"] * (72 + 4) + 2 * prob.n_dof * 8
+    peak, peak_kind = _peaks()
+    achieved = spmv_bytes / (spmv_ms * 1e-3) / 1e9
+    asm_bytes = pat.nnz * 8 + prob.n_free * 8 + prob.n_node * 48 + prob.n_elem * 36
+
+    # end to end through the C ABI with host buffers (H2D of u and f_ext, D2H of u every step)
+    disp_h = torch.zeros(prob.n_dof, dtype=torch.float64).pin_memory().numpy()
+    fext_h = torch.tensor(prob.fnodal, dtype=torch.float64).pin_memory().numpy()
+    e2e_steps = max(1, min(args.steps, 3))
+    sol.newton_iteration_host(disp_h, fext_h, LAMBDA)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        disp_h[:] = 0.0
+        sol.newton_iteration_host(disp_h, fext_h, LAMBDA)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / e2e_steps
+
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return
+    cpu = None
+    if world == 1 and not args.no_cpu:
+        cpu = cpu_newton_estimate(prob, int(statistics.median(its)), args.rtol)
+    line = {
+        "metric": METRIC, "value": world * args.steps / (ms * 1e-3), "unit": "Newton iter/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": dict(_config(prob, args.rtol), parallelism=f"replicas{world}" if world > 1 else "single"),
+        "krylov_its": int(statistics.median(its)),
+        "assembly": {"ms": asm_ms, "melems_per_s": prob.n_elem / (asm_ms * 1e-3) / 1e6,
+                     "algorithmic_bytes": asm_bytes, "achieved_gbs": asm_bytes / (asm_ms * 1e-3) / 1e9,
+                     "frac": asm_bytes / (asm_ms * 1e-3) / 1e9 / peak},
+        "e2e": {"value": 1e3 / e2e_ms, "unit": "Newton iter/s", "h2d_bytes_per_step": 2 * prob.n_dof * 8,
+                "d2h_bytes_per_step": prob.n_dof * 8},
+        "roofline": {"kernel": "spmv_fp64_kernel (SELL-32 3x3 FP64)", "bound": "hbm", "achieved": achieved,
+                     "peak": peak, "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": _read_traffic("spmv_fp64"), "algorithmic_bytes": spmv_bytes,
+                     "launch_ms": spmv_ms},
+        "cpu_baseline": None if cpu is None else {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "clocks": clk.summary(),
+        "gpu_launches": launches,
+    }
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="large", choices=["large", "small"])
+    ap.add_argument("--rtol", type=float, default=1e-8)
+    ap.add_argument("--max-it", dest="max_it", type=int, default=20000)
+    ap.add_argument("--ref-its", dest="ref_its", type=int, default=2000,
+                    help="Krylov iterations per Newton iteration assumed by --impl reference")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,206 @@
+/*
+ * mphy.h -- C ABI of libmphy.so, the B200 (sm_100a) implementation of mphyfem's
+ * femSolidmechanics Newton-step hot path.
+ *
+ * Every entry point replaces one interface of the reference (paths relative to the
+ * chennachaos/mphyfem source tree); the comment above each declaration names it.
+ * Plain C types only: pointers, sizes, status codes. Arguments named *_dev are device
+ * pointers on the context's device; *_host are host pointers. Calls on one context are
+ * ordered on its CUDA stream; a context must be used by one host thread at a time.
+ *
+ * Layout conventions shared with the reference:
+ *   - node-major DOF vectors: dof = 3*node + dim          (ElementBase.cpp:46-69)
+ *   - element DOF order 3*local_node + dim; element matrices row-major [3npe][3npe]
+ *   - 9-index of the material call: {(0,0),(1,0),(2,0),(0,1),(1,1),(2,1),(0,2),(1,2),(2,2)}
+ *     (utilitiesmaterialHyperelastic.cpp:192)
+ *   - free DOFs numbered node-major skipping prescribed ones (femSolidmechanics2.cpp:142-165)
+ */
+#ifndef MPHY_H
+#define MPHY_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MPHY_API_VERSION 1
+
+typedef enum mphy_status {
+    MPHY_OK = 0,
+    MPHY_ERR_INVALID_ARG = 1,
+    MPHY_ERR_CUDA = 2,
+    MPHY_ERR_NO_DEVICE = 3,
+    MPHY_ERR_OUT_OF_MEMORY = 4,
+    MPHY_ERR_UNSUPPORTED = 5,
+    /* call out of order; SolverPetsc::factoriseAndSolve returns -1 unless ASSEMBLY_OK
+     * (SolverPetsc.cpp:321-330) */
+    MPHY_ERR_STATE = 6,
+    /* det F < 0 at a Gauss point; the reference throws (Elem_Solid_3D_Disp.cpp:275-278) */
+    MPHY_ERR_NEG_JACOBIAN = 7,
+    /* Krylov iteration limit reached (KSP_DIVERGED_ITS) */
+    MPHY_ERR_NOT_CONVERGED = 8,
+    /* p.Ap <= 0 met by CG (KSP_DIVERGED_INDEFINITE_MAT) */
+    MPHY_ERR_INDEFINITE = 9,
+    /* NaN residual or divergence-tolerance exceeded */
+    MPHY_ERR_DIVERGED = 10,
+    /* load step cut below 1% of the initial step (MyTime.cpp:41-58) */
+    MPHY_ERR_TIME_STEP = 11
+} mphy_status;
+
+/* SolverEigen.h:11 status enum, mirrored for mphy_solver_state */
+enum { MPHY_SOLVER_EMPTY = 0, MPHY_PATTERN_OK = 1, MPHY_INIT_OK = 2, MPHY_ASSEMBLY_OK = 3,
+       MPHY_FACTORISE_OK = 4 };
+
+/* arithmetic of the tangent and of the Krylov solve */
+enum { MPHY_PREC_FP64 = 0,   /* FP64 element kernel, FP64 matrix, FP64 Jacobi-PCG (plain method) */
+       MPHY_PREC_MIXED = 1 };/* FP32 tangent (split-BF16 tensor-core contraction), FP32 matrix and
+                              * inner PCG, FP64 residual, FP64 iterative-refinement outer loop */
+/* preconditioner (PCJACOBI, or factorised sparse approximate inverse M = G^T G) */
+enum { MPHY_PC_JACOBI = 0, MPHY_PC_FSAI = 1, MPHY_PC_FSAI_LEARNED = 2 };
+/* MPHY_TANGENT_REFERENCE reproduces utilitiesmaterialHyperelastic.cpp:232-292 exactly
+ * (volumetric part without its geometric stress term); MPHY_TANGENT_CONSISTENT adds that
+ * term, giving the exact derivative of the residual. */
+enum { MPHY_TANGENT_REFERENCE = 0, MPHY_TANGENT_CONSISTENT = 1 };
+
+typedef struct mphy_ctx mphy_ctx;
+typedef struct mphy_mesh mphy_mesh;
+typedef struct mphy_pattern mphy_pattern;
+typedef struct mphy_solver mphy_solver;
+
+typedef struct mphy_solver_opts {
+    int32_t precision;     /* MPHY_PREC_* */
+    int32_t pc_type;       /* MPHY_PC_* */
+    int32_t tangent;       /* MPHY_TANGENT_* */
+    int32_t max_it;        /* KSP max_it (PETSc default 10000) */
+    double rtol;           /* KSP rtol on the preconditioned residual norm */
+    double abstol;         /* KSP abstol (PETSc default 1e-50) */
+    double dtol;           /* KSP dtol (PETSc default 1e5) */
+    double inner_rtol;     /* MIXED: FP32 inner PCG relative tolerance per refinement sweep */
+    int32_t max_outer;     /* MIXED: refinement sweeps */
+    int32_t chunk;         /* Krylov iterations per launched graph between host checks (0: auto) */
+} mphy_solver_opts;
+
+typedef struct mphy_newton_opts {
+    double dt;             /* Solver block timeStep */
+    double t_final;        /* finalTime */
+    int32_t max_steps;     /* maximumSteps */
+    int32_t max_newton;    /* maximumIterations (femBase.cpp:57 default 10) */
+    double tol_rel;        /* converged when ||R|| < max(tol_abs, tol_rel * ||R||_first) */
+    double tol_abs;        /* the reference's absolute `tolerance` (femSolidmechanics1.cpp:616-622) */
+} mphy_newton_opts;
+
+/* One Newton iteration's statistics (femSolidmechanics2.cpp:803 prints the norm). */
+typedef struct mphy_iter_stats {
+    int32_t step, iter, krylov_its, status;
+    double rhs_norm;
+    double t_assembly_ms, t_solve_ms;
+    int64_t kernel_launches;   /* libmphy kernels launched by this iteration */
+} mphy_iter_stats;
+
+const char* mphy_status_string(int status);
+/* Message of the last failing call on this host thread. */
+const char* mphy_last_error(void);
+int mphy_api_version(void);
+
+/* ---- context (replaces PetscInitialize + the MPI/PETSc communicator, femSolidmechanics.cpp:49) */
+int mphy_ctx_create(int device, mphy_ctx** out);
+int mphy_ctx_destroy(mphy_ctx* ctx);
+int mphy_ctx_synchronize(mphy_ctx* ctx);
+void* mphy_ctx_stream(mphy_ctx* ctx); /* the cudaStream_t all calls are ordered on */
+
+/* ---- mesh: femBase::readInput's node/element/material/BC data, held on the device
+ * (femBase.cpp:121-364, 571-614, 944-989; prescribed DOFs from setSpecifiedDOFs_Displacement,
+ * femSolidmechanics1.cpp:1479-1543). mats: [n_mat][3] = {mu, Kinv, Utype} per material
+ * (MaterialBase.cpp:91-116). fixed: [3*n_node], 1 = prescribed zero displacement.
+ * npe: 8 (hex8) or 10 (tet10). All inputs are host pointers, copied. */
+int mphy_mesh_create(mphy_ctx* ctx, int32_t n_node, const double* coords_host, int32_t n_elem,
+                     int32_t npe, const int32_t* conn_host, const int32_t* mat_id_host,
+                     int32_t n_mat, const double* mats_host, const uint8_t* fixed_host,
+                     mphy_mesh** out);
+int mphy_mesh_destroy(mphy_mesh* mesh);
+
+/* ---- material contract: MaterialBase::computeStressAndTangent (MaterialBase.h:94), Neo-Hookean
+ * (Matl_NeoHookean.cpp:45-53 -> utilitiesmaterialHyperelastic.cpp:186-295), batched.
+ * F_dev: [n][9] row-major F(i,j); stre_dev: [n][9]; cmat_dev: [n][81] row-major. */
+int mphy_material_nh_eval(mphy_ctx* ctx, int32_t n, const double* F_dev, double mu, double Kinv,
+                          int32_t utype, int32_t tangent, double* stre_dev, double* cmat_dev);
+
+/* ---- element contract: ElementBase::calcStiffnessAndResidual (ElementBase.h:149, implemented by
+ * Elem_Solid_3D_Disp.cpp:196-373), batched over every element of the mesh.
+ * disp_dev: [3*n_node]. Ke_dev: [n_elem][3npe][3npe] row-major, Re_dev: [n_elem][3npe] (= -f_int).
+ * *first_bad (host) receives the lowest element id with det F < 0, or -1; the call then returns
+ * MPHY_ERR_NEG_JACOBIAN. */
+int mphy_elem_eval(mphy_ctx* ctx, const mphy_mesh* mesh, const double* disp_dev, int32_t tangent,
+                   double* Ke_dev, double* Re_dev, int64_t* first_bad);
+
+/* ---- DOF map and sparsity: femSolidmechanics::prepareMatrixPattern (femSolidmechanics2.cpp:121-478),
+ * built on the device. */
+int mphy_pattern_build(mphy_ctx* ctx, const mphy_mesh* mesh, mphy_pattern** out);
+int mphy_pattern_info(const mphy_pattern* pat, int32_t* n_free, int64_t* nnz, int64_t* n_blocks,
+                      int64_t* stored_blocks);
+/* CSR over free DOFs, rows sorted ascending (findUnique, util.h:41-45): rowptr [n_free+1], col [nnz]. */
+int mphy_pattern_export_csr(const mphy_pattern* pat, int64_t* rowptr_host, int32_t* col_host);
+/* assyForSoln [n_free] (femSolidmechanics2.cpp:155-165); forAssyVec [n_elem][3npe] (:248-280). */
+int mphy_pattern_export_dofmap(const mphy_pattern* pat, int32_t* assy_for_soln_host,
+                               int32_t* for_assy_vec_host);
+int mphy_pattern_destroy(mphy_pattern* pat);
+
+/* ---- solver surface: SolverPetsc (SolverPetsc.h:16-96) -------------------------------------- */
+void mphy_solver_opts_default(mphy_solver_opts* opts);
+/* initialise + setSolverAndParameters (SolverPetsc.cpp:33-140). */
+int mphy_solver_create(mphy_ctx* ctx, const mphy_mesh* mesh, const mphy_pattern* pat,
+                       const mphy_solver_opts* opts, mphy_solver** out);
+int mphy_solver_destroy(mphy_solver* s);
+int mphy_solver_get_state(const mphy_solver* s, int32_t* state);
+/* zeroMtx (SolverPetsc.cpp:145-163): matrix, right-hand side and reactions to zero. */
+int mphy_solver_zero(mphy_solver* s);
+/* femSolidmechanics::calcStiffnessAndResidual (femSolidmechanics2.cpp:1047-1120): every element's
+ * calcStiffnessAndResidual fused with the ADD_VALUES scatter of assembleMatrixAndVector
+ * (SolverPetsc.cpp:357-378) and the reaction sum (:1106-1111). Zeroes first. Leaves ASSEMBLY_OK. */
+int mphy_solver_assemble(mphy_solver* s, const double* disp_dev, int64_t* first_bad);
+/* SolverPetsc::assembleMatrixAndVector for caller-supplied element matrices: element e scatters
+ * Ke_dev[e] / Re_dev[e] through forAssyVec of element elem_ids[e] (all elements when elem_ids is
+ * NULL; then n must equal n_elem). Adds to the current matrix; leaves ASSEMBLY_OK. */
+int mphy_solver_assemble_batch(mphy_solver* s, int32_t n, const int32_t* elem_ids_dev,
+                               const double* Ke_dev, const double* Re_dev);
+/* rhs += scale * Fext[assyForSoln] (femSolidmechanics2.cpp:785-789); fext_dev: [3*n_node]. */
+int mphy_solver_add_nodal_forces(mphy_solver* s, const double* fext_dev, double scale);
+/* VecNorm(rhsVec, NORM_2) in FP64 (femSolidmechanics2.cpp:798-801). */
+int mphy_solver_rhs_norm(mphy_solver* s, double* norm_host);
+/* factoriseAndSolve (SolverPetsc.cpp:250-330): KSPSolve from x = 0. Returns MPHY_ERR_STATE unless
+ * ASSEMBLY_OK; *its and *final_norm (preconditioned residual norm) on exit. */
+int mphy_solver_solve(mphy_solver* s, int32_t* its, double* final_norm);
+/* y = A x with the assembled matrix (MatMult), x_dev / y_dev: [3*n_node] FP64. */
+int mphy_solver_spmv(mphy_solver* s, const double* x_dev, double* y_dev);
+/* Sizes of the assembled operator: stored 3x3 blocks (with padding), true blocks, value bytes. */
+int mphy_solver_matrix_info(const mphy_solver* s, int64_t* stored_blocks, int64_t* true_blocks,
+                            int64_t* value_bytes);
+/* Solution increment scattered to node-major layout (femSolidmechanics2.cpp:1183-1186):
+ * dx_dev[assyForSoln[i]] = soln[i], prescribed DOFs 0. */
+int mphy_solver_get_solution(mphy_solver* s, double* dx_dev);
+/* disp_dev += solution (the update `SolnData.disp += SolnData.dispIncr`). */
+int mphy_solver_update_disp(mphy_solver* s, double* disp_dev);
+/* Copies for checks: CSR values in mphy_pattern_export_csr order [nnz], rhs over free DOFs
+ * [n_free], reactions [3*n_node]. Any pointer may be NULL. FP64 regardless of precision. */
+int mphy_solver_export(mphy_solver* s, double* val_host, double* rhs_host, double* reac_host);
+
+/* ---- Newton driver: femSolidmechanics::solveWithNewtonRaphson (femSolidmechanics2.cpp:730-851) ---- */
+/* One Newton iteration at load factor lambda on device data: assemble, rhs += lambda*fext, norm,
+ * and (unless the norm is already below tol_abs) solve and update disp_dev. */
+int mphy_newton_iteration(mphy_solver* s, double* disp_dev, const double* fext_dev, double lambda,
+                          double tol_abs, mphy_iter_stats* stats);
+/* The same iteration with host buffers: disp_host is copied in, updated and copied back. */
+int mphy_newton_iteration_host(mphy_solver* s, double* disp_host, const double* fext_host,
+                               double lambda, double tol_abs, mphy_iter_stats* stats);
+/* Full load stepping with cuts. fext_host: [3*n_node] nodal forces at lambda = 1 (lambda(t) = t);
+ * disp_host in/out. hist_host: [max_hist] rows; *n_hist rows written. */
+int mphy_newton_run(mphy_solver* s, const double* fext_host, const mphy_newton_opts* opts,
+                    double* disp_host, mphy_iter_stats* hist_host, int32_t max_hist,
+                    int32_t* n_hist);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MPHY_H */

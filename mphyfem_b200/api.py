@@ -1,0 +1,283 @@
+"""Host-side mirror of the reference's element, material and solver interfaces over libmphy.so.
+
+Names follow chennachaos/mphyfem so that a caller of the reference finds the same surface:
+
+* :class:`SolverGpu` -- ``SolverPetsc`` (src/mySolvers/SolverPetsc.h:16-96): ``initialise``,
+  ``zeroMtx``, ``assembleMatrixAndVector``, ``factoriseAndSolve``, ``currentStatus``;
+* :meth:`SolverGpu.calcStiffnessAndResidual` -- ``femSolidmechanics::calcStiffnessAndResidual``
+  (femSolidmechanics2.cpp:1047-1120), every element fused with the scatter;
+* :func:`calc_stiffness_and_residual` -- ``ElementBase::calcStiffnessAndResidual`` batched;
+* :func:`compute_stress_and_tangent` -- ``MaterialBase::computeStressAndTangent``;
+* :class:`FemSolidmechanicsGpu` -- ``femSolidmechanics::prepareMatrixPattern`` / ``setSolver`` /
+  ``solveWithNewtonRaphson``.
+
+Device arrays are torch CUDA tensors (plumbing only); all arithmetic runs in libmphy.so.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib as L
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise L.MphyError(L.ERR_NO_DEVICE, "no CUDA device visible")
+    return torch
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr())
+
+
+def _np(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+class Context:
+    """One device + one CUDA stream (replaces PetscInitialize, femSolidmechanics.cpp:49)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = L.load()
+        h = C.c_void_p()
+        L.check(self.lib.mphy_ctx_create(device, C.byref(h)))
+        self.h = h
+        self.device = device
+
+    def synchronize(self):
+        L.check(self.lib.mphy_ctx_synchronize(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mphy_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+class Mesh:
+    """Device-resident mesh of a :class:`mphyfem_b200.meshgen.Problem`."""
+
+    def __init__(self, ctx: Context, prob):
+        self.ctx, self.prob = ctx, prob
+        self.lib = ctx.lib
+        c = _np(prob.coords, np.float64)
+        cn = _np(prob.conn, np.int32)
+        mi = _np(prob.mat_id, np.int32)
+        mt = _np(prob.mats, np.float64)
+        fx = _np(prob.fixed, np.uint8)
+        h = C.c_void_p()
+        L.check(self.lib.mphy_mesh_create(ctx.h, prob.n_node, c.ctypes.data_as(L._d), prob.n_elem, prob.npe,
+                                          cn.ctypes.data_as(L._i32), mi.ctypes.data_as(L._i32), mt.shape[0],
+                                          mt.ctypes.data_as(L._d), fx.ctypes.data_as(L._u8), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mphy_mesh_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+class Pattern:
+    """DOF map + sparsity built on the device (prepareMatrixPattern, femSolidmechanics2.cpp:121-478)."""
+
+    def __init__(self, mesh: Mesh):
+        self.mesh, self.lib = mesh, mesh.lib
+        h = C.c_void_p()
+        L.check(self.lib.mphy_pattern_build(mesh.ctx.h, mesh.h, C.byref(h)))
+        self.h = h
+        nf, nnz, nb, sb = C.c_int32(), C.c_int64(), C.c_int64(), C.c_int64()
+        L.check(self.lib.mphy_pattern_info(h, C.byref(nf), C.byref(nnz), C.byref(nb), C.byref(sb)))
+        self.n_free, self.nnz, self.n_blocks, self.stored_blocks = nf.value, nnz.value, nb.value, sb.value
+
+    def export_csr(self):
+        rp = np.zeros(self.n_free + 1, np.int64)
+        col = np.zeros(self.nnz, np.int32)
+        L.check(self.lib.mphy_pattern_export_csr(self.h, rp.ctypes.data_as(L._i64), col.ctypes.data_as(L._i32)))
+        return rp, col
+
+    def export_dofmap(self):
+        p = self.mesh.prob
+        afs = np.zeros(self.n_free, np.int32)
+        fav = np.zeros((p.n_elem, 3 * p.npe), np.int32)
+        L.check(self.lib.mphy_pattern_export_dofmap(self.h, afs.ctypes.data_as(L._i32), fav.ctypes.data_as(L._i32)))
+        return afs, fav
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mphy_pattern_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+def default_solver_opts(**kw) -> L.SolverOpts:
+    o = L.SolverOpts()
+    L.load().mphy_solver_opts_default(C.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+class SolverGpu:
+    """The ``SolverPetsc`` surface on the GPU (SolverPetsc.h:16-96)."""
+
+    def __init__(self, mesh: Mesh, pattern: Pattern, **opts):
+        self.mesh, self.pattern, self.lib = mesh, pattern, mesh.lib
+        self.opts = default_solver_opts(**opts)
+        h = C.c_void_p()
+        L.check(self.lib.mphy_solver_create(mesh.ctx.h, mesh.h, pattern.h, C.byref(self.opts), C.byref(h)))
+        self.h = h
+
+    @property
+    def currentStatus(self) -> int:  # noqa: N802 (reference name)
+        s = C.c_int32()
+        L.check(self.lib.mphy_solver_get_state(self.h, C.byref(s)))
+        return s.value
+
+    def zeroMtx(self):  # noqa: N802
+        L.check(self.lib.mphy_solver_zero(self.h))
+
+    def calcStiffnessAndResidual(self, disp_dev):  # noqa: N802
+        """Fused element evaluation + scatter. Raises MphyError(ERR_NEG_JACOBIAN) on det F < 0."""
+        bad = C.c_int64(-1)
+        L.check(self.lib.mphy_solver_assemble(self.h, _ptr(disp_dev), C.byref(bad)))
+
+    def assembleMatrixAndVector(self, Ke_dev, Re_dev, elem_ids_dev=None):  # noqa: N802
+        n = Ke_dev.shape[0]
+        ids = _ptr(elem_ids_dev) if elem_ids_dev is not None else None
+        L.check(self.lib.mphy_solver_assemble_batch(self.h, n, ids, _ptr(Ke_dev), _ptr(Re_dev)))
+
+    def addExternalForces(self, fext_dev, scale: float):  # noqa: N802
+        L.check(self.lib.mphy_solver_add_nodal_forces(self.h, _ptr(fext_dev), float(scale)))
+
+    def rhsNorm(self) -> float:  # noqa: N802
+        v = C.c_double()
+        L.check(self.lib.mphy_solver_rhs_norm(self.h, C.byref(v)))
+        return v.value
+
+    def factoriseAndSolve(self, allow_fail: bool = False):  # noqa: N802
+        its, fn = C.c_int32(), C.c_double()
+        rc = self.lib.mphy_solver_solve(self.h, C.byref(its), C.byref(fn))
+        if not allow_fail:
+            L.check(rc)
+        return rc, its.value, fn.value
+
+    def spmv(self, x_dev, y_dev):
+        """y = A x with the assembled operator (MatMult); ordered on the library stream."""
+        L.check(self.lib.mphy_solver_spmv(self.h, _ptr(x_dev), _ptr(y_dev)))
+
+    def matrix_info(self):
+        a, b, c = C.c_int64(), C.c_int64(), C.c_int64()
+        L.check(self.lib.mphy_solver_matrix_info(self.h, C.byref(a), C.byref(b), C.byref(c)))
+        return {"stored_blocks": a.value, "true_blocks": b.value, "value_bytes": c.value}
+
+    @property
+    def stream(self) -> int:
+        return self.lib.mphy_ctx_stream(self.mesh.ctx.h) or 0
+
+    def solution(self):
+        torch = _torch()
+        x = torch.empty(self.mesh.prob.n_dof, dtype=torch.float64, device="cuda")
+        L.check(self.lib.mphy_solver_get_solution(self.h, _ptr(x)))
+        return x
+
+    def export(self, want_val=True, want_rhs=True, want_reac=True):
+        val = np.zeros(self.pattern.nnz) if want_val else None
+        rhs = np.zeros(self.pattern.n_free) if want_rhs else None
+        reac = np.zeros(self.mesh.prob.n_dof) if want_reac else None
+        p = lambda a: a.ctypes.data_as(L._d) if a is not None else None  # noqa: E731
+        L.check(self.lib.mphy_solver_export(self.h, p(val), p(rhs), p(reac)))
+        return val, rhs, reac
+
+    def newton_iteration(self, disp_dev, fext_dev, lam: float, tol_abs: float = 0.0) -> L.IterStats:
+        st = L.IterStats()
+        L.check(self.lib.mphy_newton_iteration(self.h, _ptr(disp_dev), _ptr(fext_dev) if fext_dev is not None else None,
+                                               float(lam), float(tol_abs), C.byref(st)))
+        return st
+
+    def newton_iteration_host(self, disp_host: np.ndarray, fext_host: np.ndarray | None, lam: float,
+                              tol_abs: float = 0.0) -> L.IterStats:
+        st = L.IterStats()
+        f = fext_host.ctypes.data_as(L._d) if fext_host is not None else None
+        L.check(self.lib.mphy_newton_iteration_host(self.h, disp_host.ctypes.data_as(L._d), f, float(lam),
+                                                    float(tol_abs), C.byref(st)))
+        return st
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mphy_solver_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+def compute_stress_and_tangent(ctx: Context, F_dev, mu: float, Kinv: float, utype: int = 3,
+                               tangent: int = L.TANGENT_REFERENCE):
+    """Batched MaterialBase::computeStressAndTangent: F [n,3,3] -> stre [n,9], Cmat [n,9,9]."""
+    torch = _torch()
+    n = F_dev.shape[0]
+    F = F_dev.contiguous().to(torch.float64)
+    s = torch.empty((n, 9), dtype=torch.float64, device=F.device)
+    Cm = torch.empty((n, 9, 9), dtype=torch.float64, device=F.device)
+    L.check(ctx.lib.mphy_material_nh_eval(ctx.h, n, _ptr(F), mu, Kinv, utype, tangent, _ptr(s), _ptr(Cm)))
+    return s, Cm
+
+
+def calc_stiffness_and_residual(mesh: Mesh, disp_dev, tangent: int = L.TANGENT_REFERENCE):
+    """Batched ElementBase::calcStiffnessAndResidual over every element: Ke, Re, first bad element."""
+    torch = _torch()
+    p = mesh.prob
+    ns = 3 * p.npe
+    Ke = torch.empty((p.n_elem, ns, ns), dtype=torch.float64, device="cuda")
+    Re = torch.empty((p.n_elem, ns), dtype=torch.float64, device="cuda")
+    bad = C.c_int64(-1)
+    rc = mesh.lib.mphy_elem_eval(mesh.ctx.h, mesh.h, _ptr(disp_dev), tangent, _ptr(Ke), _ptr(Re), C.byref(bad))
+    L.check(rc, allow=(L.ERR_NEG_JACOBIAN,))
+    return Ke, Re, bad.value
+
+
+@dataclass
+class NewtonResult:
+    disp: np.ndarray
+    hist: np.ndarray  # rows (step, iter, ||R||, krylov its, krylov status, t_assembly_ms, t_solve_ms)
+    status: int
+
+
+class FemSolidmechanicsGpu:
+    """femSolidmechanics on the GPU: setSolver (pattern + solver) and solveWithNewtonRaphson."""
+
+    def __init__(self, prob, ctx: Context | None = None, **solver_opts):
+        self.prob = prob
+        self.ctx = ctx or Context(0)
+        self.mesh = Mesh(self.ctx, prob)
+        self.pattern = Pattern(self.mesh)
+        opts = dict(rtol=prob.cg_rtol)
+        opts.update(solver_opts)
+        self.solver = SolverGpu(self.mesh, self.pattern, **opts)
+
+    def solveWithNewtonRaphson(self, max_newton: int = 10, tol_rel: float | None = None, tol_abs: float = 0.0,  # noqa: N802
+                               disp: np.ndarray | None = None, max_hist: int = 4096) -> NewtonResult:
+        p = self.prob
+        o = L.NewtonOpts(p.dt, p.t_final, p.max_steps, max_newton, p.newton_rtol if tol_rel is None else tol_rel,
+                         tol_abs)
+        u = np.zeros(p.n_dof) if disp is None else np.array(disp, np.float64)
+        f = _np(p.fnodal, np.float64)
+        hist = (L.IterStats * max_hist)()
+        n = C.c_int32(0)
+        rc = self.ctx.lib.mphy_newton_run(self.solver.h, f.ctypes.data_as(L._d), C.byref(o), u.ctypes.data_as(L._d),
+                                          hist, max_hist, C.byref(n))
+        L.check(rc, allow=(L.ERR_TIME_STEP,))
+        rows = np.array([[h.step, h.iter, h.rhs_norm, h.krylov_its, h.status, h.t_assembly_ms, h.t_solve_ms]
+                         for h in hist[:n.value]], dtype=np.float64).reshape(-1, 7)
+        return NewtonResult(disp=u, hist=rows, status=rc)

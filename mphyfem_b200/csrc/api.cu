@@ -1,0 +1,705 @@
+// api.cu -- the C ABI of libmphy.so and the host-side objects behind it.
+//
+// The host side mirrors the reference's interfaces: mphy_solver is the SolverPetsc surface
+// (initialise / zeroMtx / assembleMatrixAndVector / factoriseAndSolve with its status machine,
+// SolverPetsc.h:16-96, SolverEigen.h:11), and the Newton driver follows
+// femSolidmechanics::solveWithNewtonRaphson (femSolidmechanics2.cpp:730-851). Every failure is
+// a status code plus a thread-local message; nothing throws across the ABI.
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <new>
+
+#include "common.cuh"
+#include "elem.cuh"
+#include "krylov.cuh"
+#include "pattern.cuh"
+
+namespace mphy {
+
+thread_local std::string g_last_error;
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+template <typename F>
+int guarded(F&& f) {
+    try {
+        return f();
+    } catch (const Error& e) {
+        set_error(e.msg);
+        return e.status;
+    } catch (const std::bad_alloc&) {
+        set_error("host allocation failed");
+        return MPHY_ERR_OUT_OF_MEMORY;
+    } catch (const std::exception& e) {
+        set_error(e.what());
+        return MPHY_ERR_CUDA;
+    }
+}
+
+std::mutex g_tables_mu;
+bool g_tables_done[64] = {false};
+
+}  // namespace mphy
+
+using namespace mphy;
+
+// ------------------------------------------------------------------------------- solver struct
+struct mphy_solver {
+    mphy_ctx* ctx = nullptr;
+    const mphy_mesh* mesh = nullptr;
+    mphy_pattern* pat = nullptr;
+    mphy_solver_opts opts{};
+    int state = MPHY_SOLVER_EMPTY;
+    int64_t launches = 0;  // libmphy kernels launched (running count)
+    SellView A{};
+    DevBuf<double> val;          // SELL values, FP64
+    DevBuf<double> rhs, reac, x; // [3*n_node]
+    DevBuf<unsigned long long> bad;
+    DevBuf<double> partials, scalar;
+    DevBuf<uint32_t> counter;
+    DevBuf<double> disp_tmp, fext_tmp, disp_prev;
+    PcgFp64 pcg;
+    double* pinned = nullptr;  // [0] norm, [1] bad as bits
+};
+
+namespace {
+
+void solver_zero(mphy_solver* s) {
+    cudaStream_t st = s->ctx->stream;
+    MPHY_CUDA(cudaMemsetAsync(s->val.p, 0, s->val.bytes(), st));
+    set_prescribed_diagonal(s->A, s->mesh->fixed.p, s->val.p, st, s->ctx->sm_count);
+    s->launches += 1;
+    MPHY_CUDA(cudaMemsetAsync(s->rhs.p, 0, s->rhs.bytes(), st));
+    MPHY_CUDA(cudaMemsetAsync(s->reac.p, 0, s->reac.bytes(), st));
+    MPHY_CUDA(cudaMemsetAsync(s->bad.p, 0xff, sizeof(unsigned long long), st));
+}
+
+ElemArgs elem_args(const mphy_mesh* m, const double* disp, int tangent, unsigned long long* bad) {
+    ElemArgs a{};
+    a.n_elem = m->n_elem;
+    a.coords = m->coords.p;
+    a.conn = m->conn.p;
+    a.mat_id = m->mat_id.p;
+    a.mats = m->mats.p;
+    a.disp = disp;
+    a.tangent = tangent;
+    a.bad = bad;
+    a.fixed = m->fixed.p;
+    return a;
+}
+
+void solver_assemble(mphy_solver* s, const double* disp) {
+    solver_zero(s);
+    ElemArgs a = elem_args(s->mesh, disp, s->opts.tangent, s->bad.p);
+    a.e2v = s->pat->e2v.p;
+    a.val = s->val.p;
+    a.rhs = s->rhs.p;
+    a.reac = s->reac.p;
+    launch_elem_fp64(a, s->mesh->npe, 2, s->ctx->stream);
+    s->launches += 1;
+    s->state = MPHY_ASSEMBLY_OK;
+}
+
+// ||rhs|| and the first bad element, one synchronisation
+double solver_norm_and_bad(mphy_solver* s, int64_t* first_bad) {
+    cudaStream_t st = s->ctx->stream;
+    const int64_t n = 3 * (int64_t)s->mesh->n_node;
+    dot_fp64(s->rhs.p, s->rhs.p, n, s->partials.p, s->counter.p, s->scalar.p, st, s->ctx->sm_count);
+    s->launches += 1;
+    MPHY_CUDA(cudaMemcpyAsync(&s->pinned[0], s->scalar.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+    MPHY_CUDA(cudaMemcpyAsync(&s->pinned[1], s->bad.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    MPHY_CUDA(cudaStreamSynchronize(st));
+    unsigned long long b;
+    std::memcpy(&b, &s->pinned[1], sizeof(b));
+    if (first_bad) *first_bad = b == ULLONG_MAX ? -1 : (int64_t)b;
+    return std::sqrt(s->pinned[0]);
+}
+
+int solver_solve(mphy_solver* s, int32_t* its, double* fnorm) {
+    MPHY_REQUIRE(s->state == MPHY_ASSEMBLY_OK || s->state == MPHY_FACTORISE_OK, MPHY_ERR_STATE,
+                 "factoriseAndSolve: assemble matrix first");
+    s->state = MPHY_FACTORISE_OK;
+    const int rc = s->pcg.solve(s->val.p, s->rhs.p, s->x.p, s->opts.rtol, s->opts.abstol, s->opts.dtol,
+                                s->opts.max_it, s->ctx->stream, its, fnorm);
+    s->launches += s->pcg.launches;
+    return rc;
+}
+
+float elapsed_ms(mphy_ctx* c) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    return ms;
+}
+
+// One Newton iteration on device buffers (femSolidmechanics2.cpp:762-816).
+int newton_iteration(mphy_solver* s, double* disp, const double* fext, double lambda, double tol_abs,
+                     mphy_iter_stats* st_out, bool* solved) {
+    mphy_ctx* c = s->ctx;
+    mphy_iter_stats st{};
+    st.status = MPHY_OK;
+    const int64_t l0 = s->launches;
+    MPHY_CUDA(cudaEventRecord(c->ev0, c->stream));
+    solver_assemble(s, disp);
+    if (fext && lambda != 0.0) {
+        add_scaled_free(s->mesh->fixed.p, fext, lambda, s->rhs.p, 3 * (int64_t)s->mesh->n_node, c->stream, c->sm_count);
+        s->launches += 1;
+    }
+    MPHY_CUDA(cudaEventRecord(c->ev1, c->stream));
+    int64_t bad = -1;
+    st.rhs_norm = solver_norm_and_bad(s, &bad);
+    st.t_assembly_ms = elapsed_ms(c);
+    *solved = false;
+    if (bad >= 0) {
+        set_error("negative Jacobian in element " + std::to_string(bad));
+        if (st_out) *st_out = st;
+        return MPHY_ERR_NEG_JACOBIAN;
+    }
+    if (!(st.rhs_norm < tol_abs)) {
+        MPHY_CUDA(cudaEventRecord(c->ev0, c->stream));
+        int32_t its = 0;
+        double fn = 0.0;
+        st.status = solver_solve(s, &its, &fn);
+        axpy_inplace(disp, s->x.p, 1.0, 3 * (int64_t)s->mesh->n_node, c->stream, c->sm_count);
+        s->launches += 1;
+        MPHY_CUDA(cudaEventRecord(c->ev1, c->stream));
+        MPHY_CUDA(cudaEventSynchronize(c->ev1));
+        st.t_solve_ms = elapsed_ms(c);
+        st.krylov_its = its;
+        *solved = true;
+    }
+    st.kernel_launches = s->launches - l0;
+    if (st_out) *st_out = st;
+    return MPHY_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* mphy_status_string(int status) {
+    switch (status) {
+        case MPHY_OK: return "ok";
+        case MPHY_ERR_INVALID_ARG: return "invalid argument";
+        case MPHY_ERR_CUDA: return "CUDA error";
+        case MPHY_ERR_NO_DEVICE: return "no CUDA device";
+        case MPHY_ERR_OUT_OF_MEMORY: return "out of memory";
+        case MPHY_ERR_UNSUPPORTED: return "unsupported";
+        case MPHY_ERR_STATE: return "call out of order";
+        case MPHY_ERR_NEG_JACOBIAN: return "negative Jacobian in an element";
+        case MPHY_ERR_NOT_CONVERGED: return "Krylov iteration limit reached";
+        case MPHY_ERR_INDEFINITE: return "indefinite matrix met by CG";
+        case MPHY_ERR_DIVERGED: return "diverged";
+        case MPHY_ERR_TIME_STEP: return "time step size fell below 1% of the initial value";
+        default: return "unknown status";
+    }
+}
+
+const char* mphy_last_error(void) { return g_last_error.c_str(); }
+int mphy_api_version(void) { return MPHY_API_VERSION; }
+
+int mphy_ctx_create(int device, mphy_ctx** out) {
+    return guarded([&] {
+        MPHY_REQUIRE(out, MPHY_ERR_INVALID_ARG, "out is null");
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+            cudaGetLastError();
+            throw Error{MPHY_ERR_NO_DEVICE, "no CUDA device visible"};
+        }
+        MPHY_REQUIRE(device >= 0 && device < n, MPHY_ERR_INVALID_ARG, "device id out of range");
+        MPHY_CUDA(cudaSetDevice(device));
+        cudaDeviceProp prop;
+        MPHY_CUDA(cudaGetDeviceProperties(&prop, device));
+        MPHY_REQUIRE(prop.major == 10, MPHY_ERR_UNSUPPORTED, "libmphy.so is built for sm_100a (B200) only");
+        auto* c = new mphy_ctx;
+        c->device = device;
+        c->sm_count = prop.multiProcessorCount;
+        // a blocking stream: ordered with the legacy default stream other CUDA users of the process use
+        MPHY_CUDA(cudaStreamCreate(&c->stream));
+        MPHY_CUDA(cudaEventCreate(&c->ev0));
+        MPHY_CUDA(cudaEventCreate(&c->ev1));
+        {
+            std::lock_guard<std::mutex> lk(g_tables_mu);
+            if (device < 64 && !g_tables_done[device]) {
+                upload_shape_tables();
+                g_tables_done[device] = true;
+            }
+        }
+        *out = c;
+        return (int)MPHY_OK;
+    });
+}
+
+int mphy_ctx_destroy(mphy_ctx* c) {
+    if (!c) return MPHY_OK;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    cudaEventDestroy(c->ev0);
+    cudaEventDestroy(c->ev1);
+    cudaStreamDestroy(c->stream);
+    delete c;
+    return MPHY_OK;
+}
+
+int mphy_ctx_synchronize(mphy_ctx* c) {
+    return guarded([&] {
+        MPHY_REQUIRE(c, MPHY_ERR_INVALID_ARG, "ctx is null");
+        MPHY_CUDA(cudaStreamSynchronize(c->stream));
+        return (int)MPHY_OK;
+    });
+}
+
+void* mphy_ctx_stream(mphy_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int mphy_mesh_create(mphy_ctx* c, int32_t n_node, const double* coords, int32_t n_elem, int32_t npe,
+                     const int32_t* conn, const int32_t* mat_id, int32_t n_mat, const double* mats,
+                     const uint8_t* fixed, mphy_mesh** out) {
+    return guarded([&] {
+        MPHY_REQUIRE(c && out && coords && conn && mat_id && mats && fixed, MPHY_ERR_INVALID_ARG, "null argument");
+        MPHY_REQUIRE(npe == 8 || npe == 10, MPHY_ERR_UNSUPPORTED, "npe must be 8 (hex8) or 10 (tet10)");
+        MPHY_REQUIRE(n_node > 0 && n_elem > 0 && n_mat > 0, MPHY_ERR_INVALID_ARG, "empty mesh");
+        for (int32_t e = 0; e < n_elem; ++e)
+            MPHY_REQUIRE(mat_id[e] >= 0 && mat_id[e] < n_mat, MPHY_ERR_INVALID_ARG, "material id out of range");
+        for (int32_t m = 0; m < n_mat; ++m)
+            MPHY_REQUIRE(mats[3 * m + 1] > 0.0, MPHY_ERR_INVALID_ARG, "Kinv must be positive");
+        MPHY_CUDA(cudaSetDevice(c->device));
+        auto* m = new mphy_mesh;
+        try {
+            m->ctx = c;
+            m->n_node = n_node;
+            m->n_elem = n_elem;
+            m->npe = npe;
+            m->n_mat = n_mat;
+            cudaStream_t s = c->stream;
+            m->coords.alloc(3 * (size_t)n_node);
+            m->coords.upload(coords, 3 * (size_t)n_node, s);
+            m->conn.alloc((size_t)n_elem * npe);
+            m->conn.upload(conn, (size_t)n_elem * npe, s);
+            m->mat_id.alloc(n_elem);
+            m->mat_id.upload(mat_id, n_elem, s);
+            std::vector<double> m4(4 * (size_t)n_mat, 0.0);
+            for (int32_t k = 0; k < n_mat; ++k)
+                for (int q = 0; q < 3; ++q) m4[4 * k + q] = mats[3 * k + q];
+            m->mats.alloc(m4.size());
+            m->mats.upload(m4.data(), m4.size(), s);
+            m->fixed_host.assign(fixed, fixed + 3 * (size_t)n_node);
+            m->fixed.alloc(3 * (size_t)n_node);
+            m->fixed.upload(fixed, 3 * (size_t)n_node, s);
+            MPHY_CUDA(cudaStreamSynchronize(s));
+        } catch (...) {
+            delete m;
+            throw;
+        }
+        *out = m;
+        return (int)MPHY_OK;
+    });
+}
+
+int mphy_mesh_destroy(mphy_mesh* m) {
+    if (!m) return MPHY_OK;
+    cudaSetDevice(m->ctx->device);
+    cudaStreamSynchronize(m->ctx->stream);
+    delete m;
+    return MPHY_OK;
+}
+
+int mphy_material_nh_eval(mphy_ctx* c, int32_t n, const double* F, double mu, double Kinv, int32_t utype,
+                          int32_t tangent, double* stre, double* cmat) {
+    return guarded([&] {
+        MPHY_REQUIRE(c && F && stre && cmat && n >= 0 && Kinv > 0.0, MPHY_ERR_INVALID_ARG, "invalid argument");
+        launch_nh_eval(n, F, mu, Kinv, utype, tangent, stre, cmat, c->stream);
+        MPHY_CUDA(cudaStreamSynchronize(c->stream));
+        return (int)MPHY_OK;
+    });
+}
+
+int mphy_elem_eval(mphy_ctx* c, const mphy_mesh* m, const double* disp, int32_t tangent, double* Ke, double* Re,
+                   int64_t* first_bad) {
+    return guarded([&] {
+        MPHY_REQUIRE(c && m && disp && Ke && Re, MPHY_ERR_INVALID_ARG, "null argument");
+        DevBuf<unsigned long long> bad(1);
+        MPHY_CUDA(cudaMemsetAsync(bad.p, 0xff, sizeof(unsigned long long), c->stream));
+        ElemArgs a = elem_args(m, disp, tangent, bad.p);
+        a.Ke = Ke;
+        a.Re = Re;
+        launch_elem_fp64(a, m->npe, 1, c->stream);
+        unsigned long long h = 0;
+        MPHY_CUDA(cudaMemcpyAsync(&h, bad.p, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+        MPHY_CUDA(cudaStreamSynchronize(c->stream));
+        const int64_t b = h == ULLONG_MAX ? -1 : (int64_t)h;
+        if (first_bad) *first_bad = b;
+        if (b >= 0) {
+            set_error("negative Jacobian in element " + std::to_string(b));
+            return (int)MPHY_ERR_NEG_JACOBIAN;
+        }
+        return (int)MPHY_OK;
+    });
+}
+
+int mphy_pattern_build(mphy_ctx* c, const mphy_mesh* m, mphy_pattern** out) {
+    return guarded([&] {
+        MPHY_REQUIRE(c && m && out, MPHY_ERR_INVALID_ARG, "null argument");
+        auto* P = new mphy_pattern;
+        try {
+            build_pattern(c, m, P);
+        } catch (...) {
+            delete P;
+            throw;
+        }
+        *out = P;
+        return (int)MPHY_OK;
+    });
+}
+
+int mphy_pattern_info(const mphy_pattern* P, int32_t* n_free, int64_t* nnz, int64_t* n_blocks, int64_t* stored) {
+    if (!P) return MPHY_ERR_INVALID_ARG;
+    if (n_free) *n_free = P->n_free;
+    if (nnz) *nnz = P->nnz;
+    if (n_blocks) *n_blocks = P->n_blocks;
+    if (stored) *stored = P->sell_blocks;
+    return MPHY_OK;
+}
+
+int mphy_pattern_export_csr(const mphy_pattern* Pc, int64_t* rowptr, int32_t* col) {
+    return guarded([&] {
+        MPHY_REQUIRE(Pc, MPHY_ERR_INVALID_ARG, "null pattern");
+        auto* P = const_cast<mphy_pattern*>(Pc);
+        cudaStream_t s = P->ctx->stream;
+        if (rowptr) P->csr_rowptr.download(rowptr, P->n_free + 1, s);
+        if (col) {
+            pattern_csr_columns(P, false);
+            P->csr_col.download(col, P->nnz, s);
+        }
+        MPHY_CUDA(cudaStreamSynchronize(s));
+        return (int)MPHY_OK;
+    });
+}
+
+int mphy_pattern_export_dofmap(const mphy_pattern* P, int32_t* assy, int32_t* fav) {
+    return guarded([&] {
+        MPHY_REQUIRE(P, MPHY_ERR_INVALID_ARG, "null pattern");
+        cudaStream_t s = P->ctx->stream;
+        if (assy) P->assy_for_soln.download(assy, P->n_free, s);
+        if (fav) {
+            DevBuf<int32_t> tmp((size_t)P->n_elem * P->npe * 3);
+            pattern_elem_dofs(P, P->mesh, tmp.p);
+            tmp.download(fav, tmp.n, s);
+            MPHY_CUDA(cudaStreamSynchronize(s));
+        }
+        MPHY_CUDA(cudaStreamSynchronize(s));
+        return (int)MPHY_OK;
+    });
+}
+
+int mphy_pattern_destroy(mphy_pattern* P) {
+    if (!P) return MPHY_OK;
+    cudaSetDevice(P->ctx->device);
+    cudaStreamSynchronize(P->ctx->stream);
+    delete P;
+    return MPHY_OK;
+}
+
+void mphy_solver_opts_default(mphy_solver_opts* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->precision = MPHY_PREC_FP64;
+    o->pc_type = MPHY_PC_JACOBI;
+    o->tangent = MPHY_TANGENT_REFERENCE;
+    o->max_it = 10000;
+    o->rtol = 1e-12;
+    o->abstol = 1e-50;
+    o->dtol = 1e5;
+    o->inner_rtol = 1e-4;
+    o->max_outer = 50;
+    o->chunk = 0;
+}
+
+int mphy_solver_create(mphy_ctx* c, const mphy_mesh* m, const mphy_pattern* P, const mphy_solver_opts* opts,
+                       mphy_solver** out) {
+    return guarded([&] {
+        MPHY_REQUIRE(c && m && P && out, MPHY_ERR_INVALID_ARG, "null argument");
+        MPHY_REQUIRE(P->n_node == m->n_node && P->n_elem == m->n_elem, MPHY_ERR_INVALID_ARG, "pattern/mesh mismatch");
+        mphy_solver_opts o;
+        mphy_solver_opts_default(&o);
+        if (opts) o = *opts;
+        MPHY_REQUIRE(o.precision == MPHY_PREC_FP64, MPHY_ERR_UNSUPPORTED, "precision not available in this build");
+        MPHY_REQUIRE(o.pc_type == MPHY_PC_JACOBI, MPHY_ERR_UNSUPPORTED, "preconditioner not available in this build");
+        MPHY_CUDA(cudaSetDevice(c->device));
+        auto* s = new mphy_solver;
+        try {
+            s->ctx = c;
+            s->mesh = m;
+            s->pat = const_cast<mphy_pattern*>(P);
+            s->opts = o;
+            s->A = SellView{P->n_node, P->n_slices, P->slice_base.p, P->slice_width.p, P->sell_col.p, P->dvoff.p};
+            s->val.alloc(9 * (size_t)P->sell_blocks);
+            const size_t nd = 3 * (size_t)m->n_node;
+            s->rhs.alloc(nd);
+            s->reac.alloc(nd);
+            s->x.alloc(nd);
+            s->bad.alloc(1);
+            s->partials.alloc((size_t)c->sm_count * 8 + 8);
+            s->scalar.alloc(1);
+            s->counter.alloc(1);
+            MPHY_CUDA(cudaMemset(s->counter.p, 0, sizeof(uint32_t)));
+            s->pcg.init(s->A, c->sm_count, o.chunk);
+            MPHY_CUDA(cudaMallocHost(&s->pinned, 4 * sizeof(double)));
+            s->state = MPHY_PATTERN_OK;
+            solver_zero(s);
+            MPHY_CUDA(cudaStreamSynchronize(c->stream));
+            s->state = MPHY_INIT_OK;
+        } catch (...) {
+            if (s->pinned) cudaFreeHost(s->pinned);
+            delete s;
+            throw;
+        }
+        *out = s;
+        return (int)MPHY_OK;
+    });
+}
+
+int mphy_solver_destroy(mphy_solver* s) {
+    if (!s) return MPHY_OK;
+    cudaSetDevice(s->ctx->device);
+    cudaStreamSynchronize(s->ctx->stream);
+    if (s->pinned) cudaFreeHost(s->pinned);
+    delete s;
+    return MPHY_OK;
+}
+
+int mphy_solver_get_state(const mphy_solver* s, int32_t* state) {
+    if (!s || !state) return MPHY_ERR_INVALID_ARG;
+    *state = s->state;
+    return MPHY_OK;
+}
+
+int mphy_solver_zero(mphy_solver* s) {
+    return guarded([&] {
+        MPHY_REQUIRE(s, MPHY_ERR_INVALID_ARG, "null solver");
+        solver_zero(s);
+        MPHY_CUDA(cudaStreamSynchronize(s->ctx->stream));
+        s->state = MPHY_INIT_OK;
+        return (int)MPHY_OK;
+    });
+}
+
+int mphy_solver_assemble(mphy_solver* s, const double* disp, int64_t* first_bad) {
+    return guarded([&] {
+        MPHY_REQUIRE(s && disp, MPHY_ERR_INVALID_ARG, "null argument");
+        solver_assemble(s, disp);
+        unsigned long long h = 0;
+        MPHY_CUDA(cudaMemcpyAsync(&h, s->bad.p, sizeof(h), cudaMemcpyDeviceToHost, s->ctx->stream));
+        MPHY_CUDA(cudaStreamSynchronize(s->ctx->stream));
+        const int64_t b = h == ULLONG_MAX ? -1 : (int64_t)h;
+        if (first_bad) *first_bad = b;
+        if (b >= 0) {
+            set_error("negative Jacobian in element " + std::to_string(b));
+            return (int)MPHY_ERR_NEG_JACOBIAN;
+        }
+        return (int)MPHY_OK;
+    });
+}
+
+int mphy_solver_assemble_batch(mphy_solver* s, int32_t n, const int32_t* ids, const double* Ke, const double* Re) {
+    return guarded([&] {
+        MPHY_REQUIRE(s && Ke && Re && n >= 0, MPHY_ERR_INVALID_ARG, "invalid argument");
+        MPHY_REQUIRE(ids || n == s->mesh->n_elem, MPHY_ERR_INVALID_ARG, "without ids, n must equal n_elem");
+        launch_scatter_batch(s->mesh->npe, n, ids, s->mesh, s->pat, Ke, Re, s->val.p, s->rhs.p, s->reac.p,
+                             s->ctx->stream, s->ctx->sm_count);
+        MPHY_CUDA(cudaStreamSynchronize(s->ctx->stream));
+        s->state = MPHY_ASSEMBLY_OK;
+        return (int)MPHY_OK;
+    });
+}
+
+int mphy_solver_add_nodal_forces(mphy_solver* s, const double* fext, double scale) {
+    return guarded([&] {
+        MPHY_REQUIRE(s && fext, MPHY_ERR_INVALID_ARG, "null argument");
+        add_scaled_free(s->mesh->fixed.p, fext, scale, s->rhs.p, 3 * (int64_t)s->mesh->n_node, s->ctx->stream,
+                        s->ctx->sm_count);
+        return (int)MPHY_OK;
+    });
+}
+
+int mphy_solver_rhs_norm(mphy_solver* s, double* norm) {
+    return guarded([&] {
+        MPHY_REQUIRE(s && norm, MPHY_ERR_INVALID_ARG, "null argument");
+        *norm = solver_norm_and_bad(s, nullptr);
+        return (int)MPHY_OK;
+    });
+}
+
+int mphy_solver_solve(mphy_solver* s, int32_t* its, double* fnorm) {
+    return guarded([&] {
+        MPHY_REQUIRE(s, MPHY_ERR_INVALID_ARG, "null solver");
+        const int st = solver_solve(s, its, fnorm);
+        if (st != MPHY_OK) set_error(mphy_status_string(st));
+        return st;
+    });
+}
+
+int mphy_solver_spmv(mphy_solver* s, const double* x, double* y) {
+    return guarded([&] {
+        MPHY_REQUIRE(s && x && y, MPHY_ERR_INVALID_ARG, "null argument");
+        spmv_fp64(s->A, s->val.p, x, y, s->ctx->stream, s->ctx->sm_count);
+        s->launches += 1;
+        return (int)MPHY_OK;
+    });
+}
+
+int mphy_solver_matrix_info(const mphy_solver* s, int64_t* stored, int64_t* true_blocks, int64_t* value_bytes) {
+    if (!s) return MPHY_ERR_INVALID_ARG;
+    if (stored) *stored = s->pat->sell_blocks;
+    if (true_blocks) *true_blocks = s->pat->n_blocks;
+    if (value_bytes) *value_bytes = (int64_t)s->val.bytes();
+    return MPHY_OK;
+}
+
+int mphy_solver_get_solution(mphy_solver* s, double* dx) {
+    return guarded([&] {
+        MPHY_REQUIRE(s && dx, MPHY_ERR_INVALID_ARG, "null argument");
+        MPHY_CUDA(cudaMemcpyAsync(dx, s->x.p, s->x.bytes(), cudaMemcpyDeviceToDevice, s->ctx->stream));
+        MPHY_CUDA(cudaStreamSynchronize(s->ctx->stream));
+        return (int)MPHY_OK;
+    });
+}
+
+int mphy_solver_update_disp(mphy_solver* s, double* disp) {
+    return guarded([&] {
+        MPHY_REQUIRE(s && disp, MPHY_ERR_INVALID_ARG, "null argument");
+        axpy_inplace(disp, s->x.p, 1.0, 3 * (int64_t)s->mesh->n_node, s->ctx->stream, s->ctx->sm_count);
+        return (int)MPHY_OK;
+    });
+}
+
+int mphy_solver_export(mphy_solver* s, double* val_host, double* rhs_host, double* reac_host) {
+    return guarded([&] {
+        MPHY_REQUIRE(s, MPHY_ERR_INVALID_ARG, "null solver");
+        cudaStream_t st = s->ctx->stream;
+        const int sm = s->ctx->sm_count;
+        if (val_host && s->pat->nnz > 0) {
+            pattern_csr_columns(s->pat, true);
+            DevBuf<double> tmp(s->pat->nnz);
+            gather_values(s->val.p, s->pat->csr_src.p, tmp.p, s->pat->nnz, st, sm);
+            tmp.download(val_host, s->pat->nnz, st);
+            MPHY_CUDA(cudaStreamSynchronize(st));
+        }
+        if (rhs_host && s->pat->n_free > 0) {
+            DevBuf<double> tmp(s->pat->n_free);
+            gather_free(s->rhs.p, s->pat->assy_for_soln.p, tmp.p, s->pat->n_free, st, sm);
+            tmp.download(rhs_host, s->pat->n_free, st);
+            MPHY_CUDA(cudaStreamSynchronize(st));
+        }
+        if (reac_host) s->reac.download(reac_host, s->reac.n, st);
+        MPHY_CUDA(cudaStreamSynchronize(st));
+        return (int)MPHY_OK;
+    });
+}
+
+int mphy_newton_iteration(mphy_solver* s, double* disp, const double* fext, double lambda, double tol_abs,
+                          mphy_iter_stats* stats) {
+    return guarded([&] {
+        MPHY_REQUIRE(s && disp, MPHY_ERR_INVALID_ARG, "null argument");
+        bool solved = false;
+        return newton_iteration(s, disp, fext, lambda, tol_abs, stats, &solved);
+    });
+}
+
+int mphy_newton_iteration_host(mphy_solver* s, double* disp_host, const double* fext_host, double lambda,
+                               double tol_abs, mphy_iter_stats* stats) {
+    return guarded([&] {
+        MPHY_REQUIRE(s && disp_host, MPHY_ERR_INVALID_ARG, "null argument");
+        const size_t nd = 3 * (size_t)s->mesh->n_node;
+        cudaStream_t st = s->ctx->stream;
+        if (!s->disp_tmp.p) s->disp_tmp.alloc(nd);
+        if (fext_host && !s->fext_tmp.p) s->fext_tmp.alloc(nd);
+        s->disp_tmp.upload(disp_host, nd, st);
+        if (fext_host) s->fext_tmp.upload(fext_host, nd, st);
+        bool solved = false;
+        const int rc = newton_iteration(s, s->disp_tmp.p, fext_host ? s->fext_tmp.p : nullptr, lambda, tol_abs, stats,
+                                        &solved);
+        s->disp_tmp.download(disp_host, nd, st);
+        MPHY_CUDA(cudaStreamSynchronize(st));
+        return rc;
+    });
+}
+
+int mphy_newton_run(mphy_solver* s, const double* fext_host, const mphy_newton_opts* o, double* disp_host,
+                    mphy_iter_stats* hist, int32_t max_hist, int32_t* n_hist) {
+    return guarded([&] {
+        MPHY_REQUIRE(s && fext_host && o && disp_host, MPHY_ERR_INVALID_ARG, "null argument");
+        const size_t nd = 3 * (size_t)s->mesh->n_node;
+        cudaStream_t st = s->ctx->stream;
+        if (!s->disp_tmp.p) s->disp_tmp.alloc(nd);
+        if (!s->fext_tmp.p) s->fext_tmp.alloc(nd);
+        if (!s->disp_prev.p) s->disp_prev.alloc(nd);
+        double* disp = s->disp_tmp.p;
+        s->disp_tmp.upload(disp_host, nd, st);
+        s->fext_tmp.upload(fext_host, nd, st);
+        double t = 0.0, dt = o->dt;
+        const double dt0 = o->dt;
+        int steps_done = 1, rows = 0, rc = MPHY_OK;
+        while (t <= o->t_final - 1.0e-10 && steps_done <= o->max_steps) {
+            // timeUpdate: myTime.update, TimeFunction::update (lambda = t), saveSolution
+            t += dt;
+            const double lambda = t;
+            MPHY_CUDA(cudaMemcpyAsync(s->disp_prev.p, disp, nd * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            bool converged = false;
+            double norm = -1.0, norm_prev = -1.0, tol = o->tol_abs;
+            for (int iter = 1; iter <= o->max_newton; ++iter) {
+                mphy_iter_stats is{};
+                MPHY_CUDA(cudaEventRecord(s->ctx->ev0, st));
+                solver_assemble(s, disp);
+                add_scaled_free(s->mesh->fixed.p, s->fext_tmp.p, lambda, s->rhs.p, (int64_t)nd, st, s->ctx->sm_count);
+                MPHY_CUDA(cudaEventRecord(s->ctx->ev1, st));
+                int64_t bad = -1;
+                norm_prev = norm;
+                norm = solver_norm_and_bad(s, &bad);
+                is.t_assembly_ms = elapsed_ms(s->ctx);
+                if (bad >= 0) break;  // "Negative Jacobian encountered": the iteration loop ends
+                if (iter == 1) tol = std::fmax(o->tol_abs, o->tol_rel * norm);
+                bool stop = false;
+                if (norm < tol) {
+                    converged = true;
+                    stop = true;
+                } else if (iter > 3 && (std::isnan(norm) || (norm_prev > -0.1 && norm / norm_prev > 1.0e7))) {
+                    stop = true;  // diverging(1e7), femSolidmechanics1.cpp:627-636
+                } else {
+                    MPHY_CUDA(cudaEventRecord(s->ctx->ev0, st));
+                    int32_t its = 0;
+                    double fn = 0.0;
+                    is.status = solver_solve(s, &its, &fn);  // KSP divergence is only reported
+                    axpy_inplace(disp, s->x.p, 1.0, (int64_t)nd, st, s->ctx->sm_count);
+                    MPHY_CUDA(cudaEventRecord(s->ctx->ev1, st));
+                    MPHY_CUDA(cudaEventSynchronize(s->ctx->ev1));
+                    is.t_solve_ms = elapsed_ms(s->ctx);
+                    is.krylov_its = its;
+                }
+                is.step = steps_done;
+                is.iter = iter;
+                is.rhs_norm = norm;
+                if (hist && rows < max_hist) hist[rows++] = is;
+                if (stop) break;
+            }
+            if (converged) {
+                ++steps_done;
+            } else {
+                // MyTime::cut + SolutionDataSolid::reset
+                t -= dt;
+                dt *= 0.5;
+                if (dt < dt0 * 0.01) {
+                    rc = MPHY_ERR_TIME_STEP;
+                    set_error(mphy_status_string(rc));
+                    break;
+                }
+                MPHY_CUDA(cudaMemcpyAsync(disp, s->disp_prev.p, nd * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            }
+        }
+        s->disp_tmp.download(disp_host, nd, st);
+        MPHY_CUDA(cudaStreamSynchronize(st));
+        if (n_hist) *n_hist = rows;
+        return rc;
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,35 @@
+// elem.cuh -- K1 element kernels and the batched material call.
+#pragma once
+#include "common.cuh"
+
+namespace mphy {
+
+struct ElemArgs {
+    int64_t n_elem;
+    const double* coords;   // [n_node][3]
+    const int32_t* conn;    // [n_elem][npe]
+    const int32_t* mat_id;  // [n_elem]
+    const double* mats;     // [n_mat][4]
+    const double* disp;     // [n_node*3]
+    int tangent;
+    unsigned long long* bad;  // min element id with det F < 0 (init ULLONG_MAX)
+    // export (mode bit 1)
+    double* Ke;
+    double* Re;
+    // assembly (mode bit 2)
+    const uint8_t* fixed;
+    const uint32_t* e2v;
+    double* val;   // SELL values (FP64)
+    double* rhs;   // [n_node*3], prescribed DOFs untouched
+    double* reac;  // [n_node*3] or null
+};
+
+void upload_shape_tables();
+void launch_elem_fp64(const ElemArgs& a, int npe, int mode, cudaStream_t s);
+void launch_nh_eval(int n, const double* F, double mu, double Kinv, int utype, int tangent, double* stre,
+                    double* C, cudaStream_t s);
+void launch_scatter_batch(int npe, int32_t n, const int32_t* ids, const mphy_mesh* mesh, const mphy_pattern* P,
+                          const double* Ke, const double* Re, double* val, double* rhs, double* reac,
+                          cudaStream_t s, int sm_count);
+
+}  // namespace mphy
