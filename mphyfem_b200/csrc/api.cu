@@ -260,6 +260,8 @@ int mphy_mesh_create(mphy_ctx* c, int32_t n_node, const double* coords, int32_t 
         MPHY_REQUIRE(n_node > 0 && n_elem > 0 && n_mat > 0, MPHY_ERR_INVALID_ARG, "empty mesh");
         for (int32_t e = 0; e < n_elem; ++e)
             MPHY_REQUIRE(mat_id[e] >= 0 && mat_id[e] < n_mat, MPHY_ERR_INVALID_ARG, "material id out of range");
+        for (int64_t i = 0; i < (int64_t)n_elem * npe; ++i)
+            MPHY_REQUIRE(conn[i] >= 0 && conn[i] < n_node, MPHY_ERR_INVALID_ARG, "connectivity references a missing node");
         for (int32_t m = 0; m < n_mat; ++m)
             MPHY_REQUIRE(mats[3 * m + 1] > 0.0, MPHY_ERR_INVALID_ARG, "Kinv must be positive");
         MPHY_CUDA(cudaSetDevice(c->device));
