@@ -101,13 +101,13 @@ class ClockSampler:
 
 
 def _read_traffic(kind: str):
-    """DRAM bytes per launch from a committed ncu summary (profiles/*.txt line 'dram_bytes_per_launch_<kind>: X')."""
+    """DRAM bytes per launch from a committed ncu summary (a profiles/*.md line 'dram_bytes_per_launch_<kind>: X')."""
     d = os.path.join(ROOT, "profiles")
     if not os.path.isdir(d):
         return None
     key = f"dram_bytes_per_launch_{kind}:"
     for fn in sorted(os.listdir(d)):
-        if fn.endswith(".txt"):
+        if fn.endswith((".txt", ".md")):
             for line in open(os.path.join(d, fn)):
                 if line.strip().startswith(key):
                     try:
@@ -323,8 +323,9 @@ def main():
     ap.add_argument("--workload", default="large", choices=["large", "small"])
     ap.add_argument("--rtol", type=float, default=1e-8)
     ap.add_argument("--max-it", dest="max_it", type=int, default=20000)
-    ap.add_argument("--ref-its", dest="ref_its", type=int, default=2000,
-                    help="Krylov iterations per Newton iteration assumed by --impl reference")
+    ap.add_argument("--ref-its", dest="ref_its", type=int, default=2411,
+                    help="Krylov iterations per Newton iteration for --impl reference: the Jacobi-PCG count "
+                         "this workload needs at rtol 1e-8 (same algorithm on both arms)")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
