@@ -80,6 +80,8 @@ SIGNATURES = {
     "mphy_mesh_destroy": (C.c_int, [_vp]),
     "mphy_material_nh_eval": (C.c_int, [_vp, C.c_int32, _vp, C.c_double, C.c_double, C.c_int32, C.c_int32, _vp, _vp]),
     "mphy_elem_eval": (C.c_int, [_vp, _vp, _vp, C.c_int32, _vp, _vp, _i64]),
+    "mphy_elem_eval_noalloc": (C.c_int, [_vp, C.c_int32, _vp, C.c_int32, C.c_int32, _vp, _vp, C.c_int32, _vp, _vp,
+                                         C.c_int32, _vp, _vp, _i64]),
     "mphy_pattern_build": (C.c_int, [_vp, _vp, C.POINTER(_vp)]),
     "mphy_pattern_info": (C.c_int, [_vp, _i32, _i64, _i64, _i64]),
     "mphy_pattern_export_csr": (C.c_int, [_vp, _i64, _i32]),
