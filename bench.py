@@ -218,7 +218,11 @@ def run_ours(args):
     ctx = api.Context(local)
     mesh = api.Mesh(ctx, prob)
     pat = api.Pattern(mesh)
-    sol = api.SolverGpu(mesh, pat, rtol=args.rtol, max_it=args.max_it)
+    from mphyfem_b200 import _lib
+    prec = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED, "mixed32": _lib.PREC_MIXED_F32VEC}[args.precision]
+    pc = {"jacobi": _lib.PC_JACOBI, "fsai": _lib.PC_FSAI}[args.pc]
+    sol = api.SolverGpu(mesh, pat, rtol=args.rtol, max_it=args.max_it, precision=prec, inner_rtol=args.inner_rtol,
+                        max_outer=args.max_outer, pc_type=pc)
     stream = torch.cuda.ExternalStream(sol.stream, device=f"cuda:{local}")
     disp = torch.zeros(prob.n_dof, dtype=torch.float64, device=f"cuda:{local}")
     fext = torch.tensor(prob.fnodal, dtype=torch.float64, device=f"cuda:{local}")
@@ -265,7 +269,8 @@ def run_ours(args):
     e1.record(stream)
     torch.cuda.synchronize()
     spmv_ms = e0.elapsed_time(e1) / nrep
-    spmv_bytes = mi["true_blocks"] * (72 + 4) + 2 * prob.n_dof * 8
+    vbytes = mi["value_bytes"] // (9 * mi["stored_blocks"])  # 8 (FP64) or 4 (FP32) per value
+    spmv_bytes = mi["true_blocks"] * (9 * vbytes + 4) + 2 * prob.n_dof * 8
     peak, peak_kind = _peaks()
     achieved = spmv_bytes / (spmv_ms * 1e-3) / 1e9
     asm_bytes = pat.nnz * 8 + prob.n_free * 8 + prob.n_node * 48 + prob.n_elem * 36
@@ -301,9 +306,11 @@ def run_ours(args):
                      "frac": asm_bytes / (asm_ms * 1e-3) / 1e9 / peak},
         "e2e": {"value": 1e3 / e2e_ms, "unit": "Newton iter/s", "h2d_bytes_per_step": 2 * prob.n_dof * 8,
                 "d2h_bytes_per_step": prob.n_dof * 8},
-        "roofline": {"kernel": "spmv_fp64_kernel (SELL-32 3x3 FP64)", "bound": "hbm", "achieved": achieved,
+        "roofline": {"kernel": f"spmv_kernel (SELL-32 3x3, {'FP64' if vbytes == 8 else 'FP32'} values, FP64 vectors)",
+                     "bound": "hbm", "achieved": achieved,
                      "peak": peak, "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": _read_traffic("spmv_fp64"), "algorithmic_bytes": spmv_bytes,
+                     "traffic": _read_traffic("spmv_fp64" if vbytes == 8 else "spmv_mixed"),
+                     "algorithmic_bytes": spmv_bytes,
                      "launch_ms": spmv_ms},
         "cpu_baseline": None if cpu is None else {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
         "clocks": clk.summary(),
@@ -322,6 +329,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="large", choices=["large", "small"])
     ap.add_argument("--rtol", type=float, default=1e-8)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed", "mixed32"])
+    ap.add_argument("--inner-rtol", dest="inner_rtol", type=float, default=0.0)
+    ap.add_argument("--max-outer", dest="max_outer", type=int, default=1)
+    ap.add_argument("--pc", default="jacobi", choices=["jacobi", "fsai"])
     ap.add_argument("--max-it", dest="max_it", type=int, default=20000)
     ap.add_argument("--ref-its", dest="ref_its", type=int, default=2411,
                     help="Krylov iterations per Newton iteration for --impl reference: the Jacobi-PCG count "

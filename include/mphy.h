@@ -6,7 +6,9 @@
  * chennachaos/mphyfem source tree); the comment above each declaration names it.
  * Plain C types only: pointers, sizes, status codes. Arguments named *_dev are device
  * pointers on the context's device; *_host are host pointers. Calls on one context are
- * ordered on its CUDA stream; a context must be used by one host thread at a time.
+ * ordered on its CUDA stream; a context must be used by one host thread at a time. Meshes,
+ * patterns and solvers may be destroyed in any order, before or after their context; no other
+ * call may use an object after its context is destroyed.
  *
  * Layout conventions shared with the reference:
  *   - node-major DOF vectors: dof = 3*node + dim          (ElementBase.cpp:46-69)
@@ -53,9 +55,10 @@ enum { MPHY_SOLVER_EMPTY = 0, MPHY_PATTERN_OK = 1, MPHY_INIT_OK = 2, MPHY_ASSEMB
        MPHY_FACTORISE_OK = 4 };
 
 /* arithmetic of the tangent and of the Krylov solve */
-enum { MPHY_PREC_FP64 = 0,   /* FP64 element kernel, FP64 matrix, FP64 Jacobi-PCG (plain method) */
-       MPHY_PREC_MIXED = 1 };/* FP32 tangent (split-BF16 tensor-core contraction), FP32 matrix and
-                              * inner PCG, FP64 residual, FP64 iterative-refinement outer loop */
+enum { MPHY_PREC_FP64 = 0,        /* FP64 element kernel, FP64 matrix, FP64 PCG (plain method) */
+       MPHY_PREC_MIXED = 1,       /* FP32 tangent and matrix values; Krylov vectors, dot products,
+                                   * residual and the iterative-refinement outer loop in FP64 */
+       MPHY_PREC_MIXED_F32VEC = 2 /* as MIXED, with FP32 Krylov vectors (FP64 reductions) */ };
 /* preconditioner (PCJACOBI, or factorised sparse approximate inverse M = G^T G) */
 enum { MPHY_PC_JACOBI = 0, MPHY_PC_FSAI = 1, MPHY_PC_FSAI_LEARNED = 2 };
 /* MPHY_TANGENT_REFERENCE reproduces utilitiesmaterialHyperelastic.cpp:232-292 exactly
@@ -76,8 +79,9 @@ typedef struct mphy_solver_opts {
     double rtol;           /* KSP rtol on the preconditioned residual norm */
     double abstol;         /* KSP abstol (PETSc default 1e-50) */
     double dtol;           /* KSP dtol (PETSc default 1e5) */
-    double inner_rtol;     /* MIXED: FP32 inner PCG relative tolerance per refinement sweep */
-    int32_t max_outer;     /* MIXED: refinement sweeps */
+    double inner_rtol;     /* MIXED*: inner PCG rtol per refinement sweep (<= 0: use rtol) */
+    int32_t max_outer;     /* MIXED*: refinement sweeps, each ending with the FP64 residual
+                            * b - A x; stops early once ||b - A x|| <= rtol ||b|| (default 1) */
     int32_t chunk;         /* Krylov iterations per launched graph between host checks (0: auto) */
 } mphy_solver_opts;
 
@@ -191,6 +195,21 @@ int mphy_solver_spmv(mphy_solver* s, const double* x_dev, double* y_dev);
 /* Sizes of the assembled operator: stored 3x3 blocks (with padding), true blocks, value bytes. */
 int mphy_solver_matrix_info(const mphy_solver* s, int64_t* stored_blocks, int64_t* true_blocks,
                             int64_t* value_bytes);
+/* ---- factorised preconditioner M = G^T G (MPHY_PC_FSAI, MPHY_PC_FSAI_LEARNED). No counterpart
+ * in the reference, whose PC comes from PETSc options (SolverPetsc.cpp:117-140). G is lower
+ * block-triangular on the matrix's lower block pattern: block row n holds the neighbour nodes
+ * m <= n ascending (n last, at most 16 blocks). Blocks are 3x3 row-major FP32. */
+/* Lower pattern: rowptr [n_node+1], col [n_lower_blocks]. Either pointer may be NULL. */
+int mphy_solver_pc_pattern(mphy_solver* s, int64_t* n_lower_blocks, int64_t* rowptr_host, int32_t* col_host);
+/* Current G blocks in pattern order, [n_lower_blocks][9] FP32 device memory. With MPHY_PC_FSAI
+ * they are the exact block FSAI of the last solved operator (or of the assembled one after
+ * mphy_solver_pc_setup). */
+int mphy_solver_pc_get_blocks(mphy_solver* s, float* blocks_dev);
+/* Install G blocks (MPHY_PC_FSAI_LEARNED: the next solves use them as they are). */
+int mphy_solver_pc_set_blocks(mphy_solver* s, const float* blocks_dev);
+/* Exact block FSAI of the currently assembled operator; *n_fallback rows were not positive
+ * definite and use the inverse square root of their diagonal. */
+int mphy_solver_pc_setup(mphy_solver* s, int32_t* n_fallback);
 /* Solution increment scattered to node-major layout (femSolidmechanics2.cpp:1183-1186):
  * dx_dev[assyForSoln[i]] = soln[i], prescribed DOFs 0. */
 int mphy_solver_get_solution(mphy_solver* s, double* dx_dev);

@@ -32,7 +32,7 @@ ERR_DIVERGED = 10
 ERR_TIME_STEP = 11
 
 SOLVER_EMPTY, PATTERN_OK, INIT_OK, ASSEMBLY_OK, FACTORISE_OK = range(5)
-PREC_FP64, PREC_MIXED = 0, 1
+PREC_FP64, PREC_MIXED, PREC_MIXED_F32VEC = 0, 1, 2
 PC_JACOBI, PC_FSAI, PC_FSAI_LEARNED = 0, 1, 2
 TANGENT_REFERENCE, TANGENT_CONSISTENT = 0, 1
 
@@ -99,6 +99,10 @@ SIGNATURES = {
     "mphy_solver_solve": (C.c_int, [_vp, _i32, _d]),
     "mphy_solver_spmv": (C.c_int, [_vp, _vp, _vp]),
     "mphy_solver_matrix_info": (C.c_int, [_vp, _i64, _i64, _i64]),
+    "mphy_solver_pc_pattern": (C.c_int, [_vp, _i64, _i64, _i32]),
+    "mphy_solver_pc_get_blocks": (C.c_int, [_vp, _vp]),
+    "mphy_solver_pc_set_blocks": (C.c_int, [_vp, _vp]),
+    "mphy_solver_pc_setup": (C.c_int, [_vp, _i32]),
     "mphy_solver_get_solution": (C.c_int, [_vp, _vp]),
     "mphy_solver_update_disp": (C.c_int, [_vp, _vp]),
     "mphy_solver_export": (C.c_int, [_vp, _d, _d, _d]),

@@ -185,6 +185,32 @@ class SolverGpu:
     def stream(self) -> int:
         return self.lib.mphy_ctx_stream(self.mesh.ctx.h) or 0
 
+    # ---- factorised preconditioner M = G^T G (pc_type FSAI / FSAI_LEARNED)
+    def pc_pattern(self):
+        n = C.c_int64()
+        L.check(self.lib.mphy_solver_pc_pattern(self.h, C.byref(n), None, None))
+        rp = np.zeros(self.mesh.prob.n_node + 1, np.int64)
+        col = np.zeros(n.value, np.int32)
+        L.check(self.lib.mphy_solver_pc_pattern(self.h, None, rp.ctypes.data_as(L._i64), col.ctypes.data_as(L._i32)))
+        return rp, col
+
+    def pc_setup(self) -> int:
+        nf = C.c_int32()
+        L.check(self.lib.mphy_solver_pc_setup(self.h, C.byref(nf)))
+        return nf.value
+
+    def pc_get_blocks(self):
+        torch = _torch()
+        rp, _ = self.pc_pattern()
+        out = torch.empty((int(rp[-1]), 3, 3), dtype=torch.float32, device="cuda")
+        L.check(self.lib.mphy_solver_pc_get_blocks(self.h, _ptr(out)))
+        return out
+
+    def pc_set_blocks(self, blocks_dev):
+        torch = _torch()
+        b = blocks_dev.contiguous().to(torch.float32)
+        L.check(self.lib.mphy_solver_pc_set_blocks(self.h, _ptr(b)))
+
     def solution(self):
         torch = _torch()
         x = torch.empty(self.mesh.prob.n_dof, dtype=torch.float64, device="cuda")

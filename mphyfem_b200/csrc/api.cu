@@ -13,6 +13,7 @@
 
 #include "common.cuh"
 #include "elem.cuh"
+#include "fsai.cuh"
 #include "krylov.cuh"
 #include "pattern.cuh"
 
@@ -47,19 +48,28 @@ using namespace mphy;
 // ------------------------------------------------------------------------------- solver struct
 struct mphy_solver {
     mphy_ctx* ctx = nullptr;
+    int device = 0;
     const mphy_mesh* mesh = nullptr;
     mphy_pattern* pat = nullptr;
     mphy_solver_opts opts{};
     int state = MPHY_SOLVER_EMPTY;
     int64_t launches = 0;  // libmphy kernels launched (running count)
     SellView A{};
-    DevBuf<double> val;          // SELL values, FP64
+    bool mixed = false;          // MPHY_PREC_MIXED: FP32 values + FP64 iterative refinement
+    DevBuf<double> val;          // SELL values, FP64 (plain method)
+    DevBuf<float> valf;          // SELL values, FP32 (mixed precision)
     DevBuf<double> rhs, reac, x; // [3*n_node]
     DevBuf<unsigned long long> bad;
     DevBuf<double> partials, scalar;
     DevBuf<uint32_t> counter;
     DevBuf<double> disp_tmp, fext_tmp, disp_prev;
     PcgFp64 pcg;
+    IterativeRefinement<double> ir;       // MIXED
+    IterativeRefinement<float> ir32;      // MIXED_F32VEC
+    Fsai fsai;                            // MPHY_PC_FSAI*
+    bool use_fsai = false;
+    double t_pc_ms = 0.0;                 // last preconditioner setup time
+    int32_t last_sweeps = 0;
     double* pinned = nullptr;  // [0] norm, [1] bad as bits
 };
 
@@ -67,8 +77,13 @@ namespace {
 
 void solver_zero(mphy_solver* s) {
     cudaStream_t st = s->ctx->stream;
-    MPHY_CUDA(cudaMemsetAsync(s->val.p, 0, s->val.bytes(), st));
-    set_prescribed_diagonal(s->A, s->mesh->fixed.p, s->val.p, st, s->ctx->sm_count);
+    if (s->mixed) {
+        MPHY_CUDA(cudaMemsetAsync(s->valf.p, 0, s->valf.bytes(), st));
+        set_prescribed_diagonal<float>(s->A, s->mesh->fixed.p, s->valf.p, st, s->ctx->sm_count);
+    } else {
+        MPHY_CUDA(cudaMemsetAsync(s->val.p, 0, s->val.bytes(), st));
+        set_prescribed_diagonal<double>(s->A, s->mesh->fixed.p, s->val.p, st, s->ctx->sm_count);
+    }
     s->launches += 1;
     MPHY_CUDA(cudaMemsetAsync(s->rhs.p, 0, s->rhs.bytes(), st));
     MPHY_CUDA(cudaMemsetAsync(s->reac.p, 0, s->reac.bytes(), st));
@@ -94,6 +109,7 @@ void solver_assemble(mphy_solver* s, const double* disp) {
     ElemArgs a = elem_args(s->mesh, disp, s->opts.tangent, s->bad.p);
     a.e2v = s->pat->e2v.p;
     a.val = s->val.p;
+    a.valf = s->mixed ? s->valf.p : nullptr;
     a.rhs = s->rhs.p;
     a.reac = s->reac.p;
     launch_elem_fp64(a, s->mesh->npe, 2, s->ctx->stream);
@@ -120,6 +136,32 @@ int solver_solve(mphy_solver* s, int32_t* its, double* fnorm) {
     MPHY_REQUIRE(s->state == MPHY_ASSEMBLY_OK || s->state == MPHY_FACTORISE_OK, MPHY_ERR_STATE,
                  "factoriseAndSolve: assemble matrix first");
     s->state = MPHY_FACTORISE_OK;
+    if (s->use_fsai && s->opts.pc_type == MPHY_PC_FSAI) {
+        // the preconditioner follows the operator: rebuilt for every solve (KSPSetReusePreconditioner false)
+        MPHY_CUDA(cudaEventRecord(s->ctx->ev0, s->ctx->stream));
+        if (s->mixed) s->fsai.compute<float>(s->valf.p, s->ctx->stream);
+        else s->fsai.compute<double>(s->val.p, s->ctx->stream);
+        MPHY_CUDA(cudaEventRecord(s->ctx->ev1, s->ctx->stream));
+        MPHY_CUDA(cudaEventSynchronize(s->ctx->ev1));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, s->ctx->ev0, s->ctx->ev1);
+        s->t_pc_ms = ms;
+        s->launches += s->fsai.launches;
+    }
+    if (s->mixed) {
+        // FP32 inner PCG inside an FP64 refinement loop; *fnorm is ||b - A x|| / ||b|| in FP64
+        if (s->opts.precision == MPHY_PREC_MIXED_F32VEC) {
+            const int rc = s->ir32.solve(s->valf.p, s->rhs.p, s->x.p, s->opts.rtol, s->opts.inner_rtol,
+                                         s->opts.max_outer, s->opts.max_it, s->ctx->stream, its, &s->last_sweeps,
+                                         fnorm);
+            s->launches += s->ir32.launches;
+            return rc;
+        }
+        const int rc = s->ir.solve(s->valf.p, s->rhs.p, s->x.p, s->opts.rtol, s->opts.inner_rtol, s->opts.max_outer,
+                                   s->opts.max_it, s->ctx->stream, its, &s->last_sweeps, fnorm);
+        s->launches += s->ir.launches;
+        return rc;
+    }
     const int rc = s->pcg.solve(s->val.p, s->rhs.p, s->x.p, s->opts.rtol, s->opts.abstol, s->opts.dtol,
                                 s->opts.max_it, s->ctx->stream, its, fnorm);
     s->launches += s->pcg.launches;
@@ -268,6 +310,7 @@ int mphy_mesh_create(mphy_ctx* c, int32_t n_node, const double* coords, int32_t 
         auto* m = new mphy_mesh;
         try {
             m->ctx = c;
+            m->device = c->device;
             m->n_node = n_node;
             m->n_elem = n_elem;
             m->npe = npe;
@@ -299,8 +342,9 @@ int mphy_mesh_create(mphy_ctx* c, int32_t n_node, const double* coords, int32_t 
 
 int mphy_mesh_destroy(mphy_mesh* m) {
     if (!m) return MPHY_OK;
-    cudaSetDevice(m->ctx->device);
-    cudaStreamSynchronize(m->ctx->stream);
+    // objects may be destroyed in any order relative to their context: no ctx access here
+    cudaSetDevice(m->device);
+    cudaDeviceSynchronize();
     delete m;
     return MPHY_OK;
 }
@@ -395,8 +439,8 @@ int mphy_pattern_export_dofmap(const mphy_pattern* P, int32_t* assy, int32_t* fa
 
 int mphy_pattern_destroy(mphy_pattern* P) {
     if (!P) return MPHY_OK;
-    cudaSetDevice(P->ctx->device);
-    cudaStreamSynchronize(P->ctx->stream);
+    cudaSetDevice(P->device);
+    cudaDeviceSynchronize();
     delete P;
     return MPHY_OK;
 }
@@ -411,8 +455,8 @@ void mphy_solver_opts_default(mphy_solver_opts* o) {
     o->rtol = 1e-12;
     o->abstol = 1e-50;
     o->dtol = 1e5;
-    o->inner_rtol = 1e-4;
-    o->max_outer = 50;
+    o->inner_rtol = 0.0;  // inner sweep uses rtol (PETSc semantics on the preconditioned norm)
+    o->max_outer = 1;
     o->chunk = 0;
 }
 
@@ -424,17 +468,23 @@ int mphy_solver_create(mphy_ctx* c, const mphy_mesh* m, const mphy_pattern* P, c
         mphy_solver_opts o;
         mphy_solver_opts_default(&o);
         if (opts) o = *opts;
-        MPHY_REQUIRE(o.precision == MPHY_PREC_FP64, MPHY_ERR_UNSUPPORTED, "precision not available in this build");
-        MPHY_REQUIRE(o.pc_type == MPHY_PC_JACOBI, MPHY_ERR_UNSUPPORTED, "preconditioner not available in this build");
+        MPHY_REQUIRE(o.precision == MPHY_PREC_FP64 || o.precision == MPHY_PREC_MIXED ||
+                         o.precision == MPHY_PREC_MIXED_F32VEC,
+                     MPHY_ERR_INVALID_ARG, "unknown precision");
+        MPHY_REQUIRE(o.pc_type == MPHY_PC_JACOBI || o.pc_type == MPHY_PC_FSAI || o.pc_type == MPHY_PC_FSAI_LEARNED,
+                     MPHY_ERR_INVALID_ARG, "unknown preconditioner");
         MPHY_CUDA(cudaSetDevice(c->device));
         auto* s = new mphy_solver;
         try {
             s->ctx = c;
+            s->device = c->device;
             s->mesh = m;
             s->pat = const_cast<mphy_pattern*>(P);
             s->opts = o;
             s->A = SellView{P->n_node, P->n_slices, P->slice_base.p, P->slice_width.p, P->sell_col.p, P->dvoff.p};
-            s->val.alloc(9 * (size_t)P->sell_blocks);
+            s->mixed = o.precision != MPHY_PREC_FP64;
+            if (s->mixed) s->valf.alloc(9 * (size_t)P->sell_blocks);
+            else s->val.alloc(9 * (size_t)P->sell_blocks);
             const size_t nd = 3 * (size_t)m->n_node;
             s->rhs.alloc(nd);
             s->reac.alloc(nd);
@@ -444,7 +494,17 @@ int mphy_solver_create(mphy_ctx* c, const mphy_mesh* m, const mphy_pattern* P, c
             s->scalar.alloc(1);
             s->counter.alloc(1);
             MPHY_CUDA(cudaMemset(s->counter.p, 0, sizeof(uint32_t)));
-            s->pcg.init(s->A, c->sm_count, o.chunk);
+            if (o.precision == MPHY_PREC_MIXED) s->ir.init(s->A, c->sm_count, o.chunk);
+            else if (o.precision == MPHY_PREC_MIXED_F32VEC) s->ir32.init(s->A, c->sm_count, o.chunk);
+            else s->pcg.init(s->A, c->sm_count, o.chunk);
+            if (o.pc_type != MPHY_PC_JACOBI) {
+                s->use_fsai = true;
+                s->fsai.init(c, P, 16);
+                const FactorView<float> fv = s->fsai.view();
+                if (o.precision == MPHY_PREC_MIXED) s->ir.inner().set_factor(fv);
+                else if (o.precision == MPHY_PREC_MIXED_F32VEC) s->ir32.inner().set_factor(fv);
+                else s->pcg.set_factor(fv);
+            }
             MPHY_CUDA(cudaMallocHost(&s->pinned, 4 * sizeof(double)));
             s->state = MPHY_PATTERN_OK;
             solver_zero(s);
@@ -462,8 +522,8 @@ int mphy_solver_create(mphy_ctx* c, const mphy_mesh* m, const mphy_pattern* P, c
 
 int mphy_solver_destroy(mphy_solver* s) {
     if (!s) return MPHY_OK;
-    cudaSetDevice(s->ctx->device);
-    cudaStreamSynchronize(s->ctx->stream);
+    cudaSetDevice(s->device);
+    cudaDeviceSynchronize();
     if (s->pinned) cudaFreeHost(s->pinned);
     delete s;
     return MPHY_OK;
@@ -506,8 +566,8 @@ int mphy_solver_assemble_batch(mphy_solver* s, int32_t n, const int32_t* ids, co
     return guarded([&] {
         MPHY_REQUIRE(s && Ke && Re && n >= 0, MPHY_ERR_INVALID_ARG, "invalid argument");
         MPHY_REQUIRE(ids || n == s->mesh->n_elem, MPHY_ERR_INVALID_ARG, "without ids, n must equal n_elem");
-        launch_scatter_batch(s->mesh->npe, n, ids, s->mesh, s->pat, Ke, Re, s->val.p, s->rhs.p, s->reac.p,
-                             s->ctx->stream, s->ctx->sm_count);
+        launch_scatter_batch(s->mesh->npe, n, ids, s->mesh, s->pat, Ke, Re, s->val.p, s->mixed ? s->valf.p : nullptr,
+                             s->rhs.p, s->reac.p, s->ctx->stream, s->ctx->sm_count);
         MPHY_CUDA(cudaStreamSynchronize(s->ctx->stream));
         s->state = MPHY_ASSEMBLY_OK;
         return (int)MPHY_OK;
@@ -543,7 +603,8 @@ int mphy_solver_solve(mphy_solver* s, int32_t* its, double* fnorm) {
 int mphy_solver_spmv(mphy_solver* s, const double* x, double* y) {
     return guarded([&] {
         MPHY_REQUIRE(s && x && y, MPHY_ERR_INVALID_ARG, "null argument");
-        spmv_fp64(s->A, s->val.p, x, y, s->ctx->stream, s->ctx->sm_count);
+        if (s->mixed) spmv<float, double>(s->A, s->valf.p, x, y, s->ctx->stream, s->ctx->sm_count);
+        else spmv<double, double>(s->A, s->val.p, x, y, s->ctx->stream, s->ctx->sm_count);
         s->launches += 1;
         return (int)MPHY_OK;
     });
@@ -553,8 +614,54 @@ int mphy_solver_matrix_info(const mphy_solver* s, int64_t* stored, int64_t* true
     if (!s) return MPHY_ERR_INVALID_ARG;
     if (stored) *stored = s->pat->sell_blocks;
     if (true_blocks) *true_blocks = s->pat->n_blocks;
-    if (value_bytes) *value_bytes = (int64_t)s->val.bytes();
+    if (value_bytes) *value_bytes = (int64_t)(s->mixed ? s->valf.bytes() : s->val.bytes());
     return MPHY_OK;
+}
+
+int mphy_solver_pc_pattern(mphy_solver* s, int64_t* n_lower, int64_t* rowptr, int32_t* col) {
+    return guarded([&] {
+        MPHY_REQUIRE(s && s->use_fsai, MPHY_ERR_STATE, "the solver has no factorised preconditioner");
+        const SellPattern& L = s->fsai.lower();
+        if (n_lower) *n_lower = L.n_blocks;
+        if (rowptr) L.rowptr.download(rowptr, (size_t)L.n_node + 1, s->ctx->stream);
+        if (col) L.col.download(col, (size_t)L.n_blocks, s->ctx->stream);
+        MPHY_CUDA(cudaStreamSynchronize(s->ctx->stream));
+        return (int)MPHY_OK;
+    });
+}
+
+int mphy_solver_pc_get_blocks(mphy_solver* s, float* blocks) {
+    return guarded([&] {
+        MPHY_REQUIRE(s && blocks, MPHY_ERR_INVALID_ARG, "null argument");
+        MPHY_REQUIRE(s->use_fsai, MPHY_ERR_STATE, "the solver has no factorised preconditioner");
+        s->fsai.get_lower_values(blocks, s->ctx->stream);
+        MPHY_CUDA(cudaStreamSynchronize(s->ctx->stream));
+        return (int)MPHY_OK;
+    });
+}
+
+int mphy_solver_pc_set_blocks(mphy_solver* s, const float* blocks) {
+    return guarded([&] {
+        MPHY_REQUIRE(s && blocks, MPHY_ERR_INVALID_ARG, "null argument");
+        MPHY_REQUIRE(s->use_fsai, MPHY_ERR_STATE, "the solver has no factorised preconditioner");
+        s->fsai.set_lower_values(blocks, s->ctx->stream);
+        MPHY_CUDA(cudaStreamSynchronize(s->ctx->stream));
+        return (int)MPHY_OK;
+    });
+}
+
+int mphy_solver_pc_setup(mphy_solver* s, int32_t* n_fallback) {
+    return guarded([&] {
+        MPHY_REQUIRE(s, MPHY_ERR_INVALID_ARG, "null solver");
+        MPHY_REQUIRE(s->use_fsai, MPHY_ERR_STATE, "the solver has no factorised preconditioner");
+        MPHY_REQUIRE(s->state == MPHY_ASSEMBLY_OK || s->state == MPHY_FACTORISE_OK, MPHY_ERR_STATE,
+                     "assemble the matrix first");
+        if (s->mixed) s->fsai.compute<float>(s->valf.p, s->ctx->stream);
+        else s->fsai.compute<double>(s->val.p, s->ctx->stream);
+        const int32_t nf = s->fsai.fallback_rows(s->ctx->stream);
+        if (n_fallback) *n_fallback = nf;
+        return (int)MPHY_OK;
+    });
 }
 
 int mphy_solver_get_solution(mphy_solver* s, double* dx) {
@@ -582,7 +689,8 @@ int mphy_solver_export(mphy_solver* s, double* val_host, double* rhs_host, doubl
         if (val_host && s->pat->nnz > 0) {
             pattern_csr_columns(s->pat, true);
             DevBuf<double> tmp(s->pat->nnz);
-            gather_values(s->val.p, s->pat->csr_src.p, tmp.p, s->pat->nnz, st, sm);
+            if (s->mixed) gather_values<float>(s->valf.p, s->pat->csr_src.p, tmp.p, s->pat->nnz, st, sm);
+            else gather_values<double>(s->val.p, s->pat->csr_src.p, tmp.p, s->pat->nnz, st, sm);
             tmp.download(val_host, s->pat->nnz, st);
             MPHY_CUDA(cudaStreamSynchronize(st));
         }

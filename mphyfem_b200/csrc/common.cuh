@@ -87,6 +87,7 @@ struct mphy_ctx {
 // Device-resident mesh: the SoA replacement of GeomDataLagrange / elems[] / MaterialBase objects.
 struct mphy_mesh {
     mphy_ctx* ctx = nullptr;
+    int device = 0;  // kept so that destroy never touches the context (it may be gone)
     int32_t n_node = 0, n_elem = 0, npe = 0, n_mat = 0;
     mphy::DevBuf<double> coords;   // [n_node][3]
     mphy::DevBuf<int32_t> conn;    // [n_elem][npe]
@@ -107,6 +108,7 @@ struct mphy_mesh {
 struct mphy_pattern {
     mphy_ctx* ctx = nullptr;
     const mphy_mesh* mesh = nullptr;
+    int device = 0;
     int32_t n_node = 0, n_elem = 0, npe = 0, n_free = 0;
     int64_t n_blocks = 0;       // true blocks (sum of row lengths)
     int64_t sell_blocks = 0;    // stored blocks incl. padding

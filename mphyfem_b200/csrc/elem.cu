@@ -376,8 +376,11 @@ __global__ void __launch_bounds__(kEpb * NPE) elem_fp64_kernel(ElemArgs a) {
                 for (int bb = 0; bb < 3; ++bb) {
                     if (a.fixed[3 * (int64_t)nJ + bb]) continue;
 #pragma unroll
-                    for (int aa = 0; aa < 3; ++aa)
-                        if (freeI[aa]) atomicAdd(&a.val[off + 32u * (3 * aa + bb)], acc[j][3 * aa + bb]);
+                    for (int aa = 0; aa < 3; ++aa) {
+                        if (!freeI[aa]) continue;
+                        if (a.valf) atomicAdd(&a.valf[off + 32u * (3 * aa + bb)], (float)acc[j][3 * aa + bb]);
+                        else atomicAdd(&a.val[off + 32u * (3 * aa + bb)], acc[j][3 * aa + bb]);
+                    }
                 }
             }
         }
@@ -423,7 +426,8 @@ template <int NPE>
 __global__ void scatter_batch_kernel(int32_t n, const int32_t* __restrict__ ids, const int32_t* __restrict__ conn,
                                      const uint32_t* __restrict__ e2v, const uint8_t* __restrict__ fixed,
                                      const double* __restrict__ Ke, const double* __restrict__ Re,
-                                     double* __restrict__ val, double* __restrict__ rhs, double* __restrict__ reac) {
+                                     double* __restrict__ val, float* __restrict__ valf, double* __restrict__ rhs,
+                                     double* __restrict__ reac) {
     constexpr int NS = 3 * NPE;
     const int64_t total = (int64_t)n * NPE * NPE;
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
@@ -437,7 +441,9 @@ __global__ void scatter_batch_kernel(int32_t n, const int32_t* __restrict__ ids,
             if (fixed[3 * (int64_t)nI + aa]) continue;
             for (int bb = 0; bb < 3; ++bb) {
                 if (fixed[3 * (int64_t)nJ + bb]) continue;
-                atomicAdd(&val[off + 32u * (3 * aa + bb)], Ke[(k * NS + 3 * I + aa) * NS + 3 * J + bb]);
+                const double v = Ke[(k * NS + 3 * I + aa) * NS + 3 * J + bb];
+                if (valf) atomicAdd(&valf[off + 32u * (3 * aa + bb)], (float)v);
+                else atomicAdd(&val[off + 32u * (3 * aa + bb)], v);
             }
         }
         if (J == 0) {
@@ -451,16 +457,18 @@ __global__ void scatter_batch_kernel(int32_t n, const int32_t* __restrict__ ids,
 }
 
 void launch_scatter_batch(int npe, int32_t n, const int32_t* ids, const mphy_mesh* mesh, const mphy_pattern* P,
-                          const double* Ke, const double* Re, double* val, double* rhs, double* reac,
+                          const double* Ke, const double* Re, double* val, float* valf, double* rhs, double* reac,
                           cudaStream_t s, int sm_count) {
     if (n <= 0) return;
     const int64_t total = (int64_t)n * npe * npe;
     unsigned grid = ceil_div(total, 256);
     if (grid > (unsigned)sm_count * 16) grid = sm_count * 16;
     if (npe == 8)
-        scatter_batch_kernel<8><<<grid, 256, 0, s>>>(n, ids, mesh->conn.p, P->e2v.p, mesh->fixed.p, Ke, Re, val, rhs, reac);
+        scatter_batch_kernel<8><<<grid, 256, 0, s>>>(n, ids, mesh->conn.p, P->e2v.p, mesh->fixed.p, Ke, Re, val, valf,
+                                                     rhs, reac);
     else
-        scatter_batch_kernel<10><<<grid, 256, 0, s>>>(n, ids, mesh->conn.p, P->e2v.p, mesh->fixed.p, Ke, Re, val, rhs, reac);
+        scatter_batch_kernel<10><<<grid, 256, 0, s>>>(n, ids, mesh->conn.p, P->e2v.p, mesh->fixed.p, Ke, Re, val, valf,
+                                                      rhs, reac);
     MPHY_CUDA(cudaGetLastError());
 }
 

@@ -19,7 +19,8 @@ struct ElemArgs {
     // assembly (mode bit 2)
     const uint8_t* fixed;
     const uint32_t* e2v;
-    double* val;   // SELL values (FP64)
+    double* val;   // SELL values (FP64), or
+    float* valf;   // SELL values (FP32) when non-null
     double* rhs;   // [n_node*3], prescribed DOFs untouched
     double* reac;  // [n_node*3] or null
 };
@@ -29,7 +30,7 @@ void launch_elem_fp64(const ElemArgs& a, int npe, int mode, cudaStream_t s);
 void launch_nh_eval(int n, const double* F, double mu, double Kinv, int utype, int tangent, double* stre,
                     double* C, cudaStream_t s);
 void launch_scatter_batch(int npe, int32_t n, const int32_t* ids, const mphy_mesh* mesh, const mphy_pattern* P,
-                          const double* Ke, const double* Re, double* val, double* rhs, double* reac,
+                          const double* Ke, const double* Re, double* val, float* valf, double* rhs, double* reac,
                           cudaStream_t s, int sm_count);
 
 }  // namespace mphy

@@ -1,16 +1,21 @@
-// krylov.cu -- K4/K5: SpMV over the SELL-32 3x3 layout, Jacobi-PCG, FP64 vector kernels.
+// krylov.cu -- K4/K5: SpMV over the SELL-32 3x3 layout, preconditioned CG, FP64 iterative
+// refinement, vector kernels.
 //
-// Replaces KSPSolve with KSPCG + PCJACOBI (SolverPetsc.cpp:250-314 with the options
-// -ksp_type cg -pc_type jacobi). The iteration follows PETSc's documented KSPCG
-// (Hestenes-Stiefel, preconditioned-residual norm, KSPConvergedDefault): x0 = 0,
-// converged when ||z_k|| <= max(rtol ||z_0||, abstol), diverged when ||z_k|| >= dtol ||z_0||,
-// indefinite when p.Ap <= 0, its = iterations performed.
+// Replaces KSPSolve with KSPCG (SolverPetsc.cpp:250-314; -ksp_type cg -pc_type jacobi for the
+// plain method). The iteration follows PETSc's documented KSPCG (Hestenes-Stiefel,
+// preconditioned-residual norm, KSPConvergedDefault): x0 = 0, converged when
+// ||z_k|| <= max(rtol ||z_0||, abstol), diverged when ||z_k|| >= dtol ||z_0||, indefinite when
+// p.Ap <= 0, its = iterations performed.
 //
-// One CG iteration is three kernels: SpMV with the fused p.q reduction; the x/r/z update with
-// the fused (r,z) and (z,z) reductions; the p update. Reductions are deterministic: every CTA
-// writes a partial sum, and the CTA that finishes last (an atomic ticket, no waiting) adds the
-// partials in a fixed order and advances the shared scalar state. Chunks of iterations are
-// replayed from a captured CUDA graph; kernels return immediately once the state says done.
+// One CG iteration is three kernels with Jacobi (SpMV + fused p.q; x/r/z update + fused (r,z),
+// (z,z); p update) or five with the factorised preconditioner M = G^T G (the update splits into
+// the x/r update and two SpMVs, the second fusing the reductions). Reductions are
+// deterministic: every CTA writes a partial sum, and the CTA that finishes last (an atomic
+// ticket, no waiting) adds the partials in a fixed order and advances the shared scalar state.
+// Chunks of iterations are replayed from a captured CUDA graph; kernels return immediately once
+// the state says done. FP32 vectors keep every reduction in FP64.
+#include <cmath>
+
 #include "krylov.cuh"
 
 namespace mphy {
@@ -24,6 +29,11 @@ unsigned stride_grid(int64_t n, int threads, int sm_count, int per_sm) {
 }
 
 namespace {
+
+template <typename T>
+struct AccOf {
+    using type = T;
+};
 
 // Deterministic block sum (fixed butterfly per warp, fixed order across warps); valid in all
 // threads of warp 0.
@@ -60,13 +70,70 @@ __device__ __forceinline__ double reduce_partials(const double* partials, int n,
     return block_sum(v, sh);
 }
 
+// State after the initial residual (KSPConvergedDefault at n = 0).
+__device__ void finish_init(PcgState* st, double rz, double zz, double rtol, double abstol, double dtol, int maxit) {
+    const double dp = sqrt(zz);
+    st->rz = rz;
+    st->dp = dp;
+    st->dp0 = dp;
+    st->ttol = fmax(rtol * dp, abstol);
+    st->dtol = dtol;
+    st->maxit = maxit;
+    st->its = 0;
+    st->status = MPHY_OK;
+    st->done = 0;
+    if (dp != dp) {
+        st->status = MPHY_ERR_DIVERGED;
+        st->done = 1;
+    } else if (dp <= st->ttol) {
+        st->done = 1;
+    } else if (rz == 0.0) {
+        st->its = 1;
+        st->done = 1;
+    } else if (maxit <= 0) {
+        st->status = MPHY_ERR_NOT_CONVERGED;
+        st->done = 1;
+    }
+}
+
+// State after iteration its+1 (convergence, divergence, limit, next beta).
+__device__ void finish_iter(PcgState* st, double rz, double zz) {
+    st->its += 1;
+    const double dp = sqrt(zz);
+    st->dp = dp;
+    if (dp != dp) {
+        st->status = MPHY_ERR_DIVERGED;
+        st->done = 1;
+    } else if (dp <= st->ttol) {
+        st->status = MPHY_OK;
+        st->done = 1;
+    } else if (dp >= st->dtol * st->dp0) {
+        st->status = MPHY_ERR_DIVERGED;
+        st->done = 1;
+    } else if (st->its >= st->maxit) {
+        st->status = MPHY_ERR_NOT_CONVERGED;
+        st->done = 1;
+    } else if (rz == 0.0) {
+        // the next iteration would stop at once with beta == 0 (KSP_CONVERGED_ATOL)
+        st->its += 1;
+        st->status = MPHY_OK;
+        st->done = 1;
+    } else {
+        st->beta = rz / st->rz;
+        st->rz = rz;
+    }
+}
+
 // ---------------------------------------------------------------- SpMV
-template <bool DOT>
-__global__ void __launch_bounds__(kThreads) spmv_fp64_kernel(SellView A, const double* __restrict__ val,
-                                                             const double* __restrict__ x, double* __restrict__ y,
-                                                             double* __restrict__ partials, PcgState* st) {
+// One thread per block row; a warp is one 32-row slice, so every value load is 32 consecutive
+// entries. DOT: fuse p.q (x = p, y = q) and, in the last CTA, alpha = (r,z) / p.q.
+template <typename VT, typename XT, bool DOT>
+__global__ void __launch_bounds__(kThreads) spmv_kernel(SellView A, const VT* __restrict__ val,
+                                                        const XT* __restrict__ x, XT* __restrict__ y,
+                                                        double* __restrict__ partials, PcgState* st) {
+    using Acc = typename AccOf<XT>::type;
     __shared__ double sh[32];
-    if (DOT && st->done) return;
+    if (st && st->done) return;  // inside a CG iteration: nothing left to do
     double acc = 0.0;
     const int64_t rows = (int64_t)A.n_slices * 32;
     for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < rows;
@@ -75,23 +142,25 @@ __global__ void __launch_bounds__(kThreads) spmv_fp64_kernel(SellView A, const d
         const int lane = (int)(row & 31);
         const int64_t base = A.slice_base[s];
         const int w = A.slice_width[s];
-        double y0 = 0.0, y1 = 0.0, y2 = 0.0;
+        Acc y0 = 0, y1 = 0, y2 = 0;
         const int32_t* cp = A.col + base + lane;
-        const double* vp = val + 9 * base + lane;
+        const VT* vp = val + 9 * base + lane;
 #pragma unroll 2
         for (int k = 0; k < w; ++k) {
             const int64_t c = cp[32 * k];
-            const double x0 = x[3 * c], x1 = x[3 * c + 1], x2 = x[3 * c + 2];
-            const double* v = vp + 288 * (int64_t)k;
-            y0 += v[0] * x0 + v[32] * x1 + v[64] * x2;
-            y1 += v[96] * x0 + v[128] * x1 + v[160] * x2;
-            y2 += v[192] * x0 + v[224] * x1 + v[256] * x2;
+            const Acc x0 = (Acc)x[3 * c], x1 = (Acc)x[3 * c + 1], x2 = (Acc)x[3 * c + 2];
+            const VT* v = vp + 288 * (int64_t)k;
+            y0 += (Acc)v[0] * x0 + (Acc)v[32] * x1 + (Acc)v[64] * x2;
+            y1 += (Acc)v[96] * x0 + (Acc)v[128] * x1 + (Acc)v[160] * x2;
+            y2 += (Acc)v[192] * x0 + (Acc)v[224] * x1 + (Acc)v[256] * x2;
         }
         if (row < A.n_node) {
-            y[3 * row] = y0;
-            y[3 * row + 1] = y1;
-            y[3 * row + 2] = y2;
-            if (DOT) acc += x[3 * row] * y0 + x[3 * row + 1] * y1 + x[3 * row + 2] * y2;
+            y[3 * row] = (XT)y0;
+            y[3 * row + 1] = (XT)y1;
+            y[3 * row + 2] = (XT)y2;
+            if (DOT)
+                acc += (double)x[3 * row] * (double)(XT)y0 + (double)x[3 * row + 1] * (double)(XT)y1 +
+                       (double)x[3 * row + 2] * (double)(XT)y2;
         }
     }
     if (!DOT) return;
@@ -113,25 +182,47 @@ __global__ void __launch_bounds__(kThreads) spmv_fp64_kernel(SellView A, const d
     }
 }
 
-// x += alpha p, r -= alpha q, z = D^-1 r, then (r, z) and (z, z)
-__global__ void __launch_bounds__(kThreads) pcg_update_kernel(int64_t n, double* __restrict__ x, double* __restrict__ r,
-                                                              double* __restrict__ z, const double* __restrict__ p,
-                                                              const double* __restrict__ q,
-                                                              const double* __restrict__ dinv,
-                                                              double* __restrict__ part_rz, double* __restrict__ part_zz,
-                                                              PcgState* st) {
+// z = G^T t with the fused (r, z), (z, z); INIT also sets p = z and the initial state.
+template <typename XT, bool INIT>
+__global__ void __launch_bounds__(kThreads) factor_apply_kernel(SellView A, const float* __restrict__ val,
+                                                                const XT* __restrict__ t, XT* __restrict__ z,
+                                                                const XT* __restrict__ r, XT* __restrict__ p,
+                                                                double* __restrict__ part_rz,
+                                                                double* __restrict__ part_zz, PcgState* st,
+                                                                double rtol, double abstol, double dtol, int maxit) {
+    using Acc = typename AccOf<XT>::type;
     __shared__ double sh[32];
-    if (st->done) return;
-    const double alpha = st->alpha;
+    if (!INIT && st->done) return;
     double a1 = 0.0, a2 = 0.0;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        x[i] += alpha * p[i];
-        const double ri = r[i] - alpha * q[i];
-        r[i] = ri;
-        const double zi = dinv[i] * ri;
-        z[i] = zi;
-        a1 += ri * zi;
-        a2 += zi * zi;
+    const int64_t rows = (int64_t)A.n_slices * 32;
+    for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < rows;
+         row += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = row >> 5;
+        const int lane = (int)(row & 31);
+        const int64_t base = A.slice_base[s];
+        const int w = A.slice_width[s];
+        Acc y0 = 0, y1 = 0, y2 = 0;
+        const int32_t* cp = A.col + base + lane;
+        const float* vp = val + 9 * base + lane;
+#pragma unroll 2
+        for (int k = 0; k < w; ++k) {
+            const int64_t c = cp[32 * k];
+            const Acc x0 = t[3 * c], x1 = t[3 * c + 1], x2 = t[3 * c + 2];
+            const float* v = vp + 288 * (int64_t)k;
+            y0 += (Acc)v[0] * x0 + (Acc)v[32] * x1 + (Acc)v[64] * x2;
+            y1 += (Acc)v[96] * x0 + (Acc)v[128] * x1 + (Acc)v[160] * x2;
+            y2 += (Acc)v[192] * x0 + (Acc)v[224] * x1 + (Acc)v[256] * x2;
+        }
+        if (row < A.n_node) {
+            const XT zz[3] = {(XT)y0, (XT)y1, (XT)y2};
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                z[3 * row + c] = zz[c];
+                if (INIT) p[3 * row + c] = zz[c];
+                a1 += (double)r[3 * row + c] * (double)zz[c];
+                a2 += (double)zz[c] * (double)zz[c];
+            }
+        }
     }
     a1 = block_sum(a1, sh);
     if (threadIdx.x == 0) part_rz[blockIdx.x] = a1;
@@ -142,60 +233,124 @@ __global__ void __launch_bounds__(kThreads) pcg_update_kernel(int64_t n, double*
     const double zz = reduce_partials(part_zz, gridDim.x, sh);
     if (threadIdx.x == 0) {
         st->counter = 0;
-        st->its += 1;
-        const double dp = sqrt(zz);
-        st->dp = dp;
-        if (dp != dp) {
-            st->status = MPHY_ERR_DIVERGED;
-            st->done = 1;
-        } else if (dp <= st->ttol) {
-            st->status = MPHY_OK;
-            st->done = 1;
-        } else if (dp >= st->dtol * st->dp0) {
-            st->status = MPHY_ERR_DIVERGED;
-            st->done = 1;
-        } else if (st->its >= st->maxit) {
-            st->status = MPHY_ERR_NOT_CONVERGED;
-            st->done = 1;
-        } else if (rz == 0.0) {
-            // the next iteration would stop at once with beta == 0 (KSP_CONVERGED_ATOL)
-            st->its += 1;
-            st->status = MPHY_OK;
-            st->done = 1;
-        } else {
-            st->beta = rz / st->rz;
-            st->rz = rz;
-        }
+        if (INIT) finish_init(st, rz, zz, rtol, abstol, dtol, maxit);
+        else finish_iter(st, rz, zz);
     }
 }
 
-__global__ void __launch_bounds__(kThreads) pcg_direction_kernel(int64_t n, double* __restrict__ p,
-                                                                 const double* __restrict__ z, const PcgState* st) {
+// r = b - A x in FP64 with the fused ||r||^2
+template <typename VT>
+__global__ void __launch_bounds__(kThreads) residual_kernel(SellView A, const VT* __restrict__ val,
+                                                            const double* __restrict__ x, const double* __restrict__ b,
+                                                            double* __restrict__ r, double* __restrict__ partials,
+                                                            uint32_t* counter, double* out) {
+    __shared__ double sh[32];
+    double acc = 0.0;
+    const int64_t rows = (int64_t)A.n_slices * 32;
+    for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < rows;
+         row += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = row >> 5;
+        const int lane = (int)(row & 31);
+        const int64_t base = A.slice_base[s];
+        const int w = A.slice_width[s];
+        double y0 = 0, y1 = 0, y2 = 0;
+        const int32_t* cp = A.col + base + lane;
+        const VT* vp = val + 9 * base + lane;
+#pragma unroll 2
+        for (int k = 0; k < w; ++k) {
+            const int64_t c = cp[32 * k];
+            const double x0 = x[3 * c], x1 = x[3 * c + 1], x2 = x[3 * c + 2];
+            const VT* v = vp + 288 * (int64_t)k;
+            y0 += (double)v[0] * x0 + (double)v[32] * x1 + (double)v[64] * x2;
+            y1 += (double)v[96] * x0 + (double)v[128] * x1 + (double)v[160] * x2;
+            y2 += (double)v[192] * x0 + (double)v[224] * x1 + (double)v[256] * x2;
+        }
+        if (row < A.n_node) {
+            const double ri[3] = {b[3 * row] - y0, b[3 * row + 1] - y1, b[3 * row + 2] - y2};
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                r[3 * row + c] = ri[c];
+                acc += ri[c] * ri[c];
+            }
+        }
+    }
+    acc = block_sum(acc, sh);
+    if (threadIdx.x == 0) partials[blockIdx.x] = acc;
+    if (!arrive_last(counter)) return;
+    const double t = reduce_partials(partials, gridDim.x, sh);
+    if (threadIdx.x == 0) {
+        *counter = 0;
+        *out = t;
+    }
+}
+
+// x += alpha p, r -= alpha q; JAC: z = D^-1 r and the fused (r, z), (z, z)
+template <typename XT, bool JAC>
+__global__ void __launch_bounds__(kThreads) pcg_update_kernel(int64_t n, XT* __restrict__ x, XT* __restrict__ r,
+                                                              XT* __restrict__ z, const XT* __restrict__ p,
+                                                              const XT* __restrict__ q, const XT* __restrict__ dinv,
+                                                              double* __restrict__ part_rz,
+                                                              double* __restrict__ part_zz, PcgState* st) {
+    __shared__ double sh[32];
     if (st->done) return;
-    const double beta = st->beta;
+    const XT alpha = (XT)st->alpha;
+    double a1 = 0.0, a2 = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        x[i] += alpha * p[i];
+        const XT ri = r[i] - alpha * q[i];
+        r[i] = ri;
+        if (JAC) {
+            const XT zi = dinv[i] * ri;
+            z[i] = zi;
+            a1 += (double)ri * (double)zi;
+            a2 += (double)zi * (double)zi;
+        }
+    }
+    if (!JAC) return;
+    a1 = block_sum(a1, sh);
+    if (threadIdx.x == 0) part_rz[blockIdx.x] = a1;
+    a2 = block_sum(a2, sh);
+    if (threadIdx.x == 0) part_zz[blockIdx.x] = a2;
+    if (!arrive_last(&st->counter)) return;
+    const double rz = reduce_partials(part_rz, gridDim.x, sh);
+    const double zz = reduce_partials(part_zz, gridDim.x, sh);
+    if (threadIdx.x == 0) {
+        st->counter = 0;
+        finish_iter(st, rz, zz);
+    }
+}
+
+template <typename XT>
+__global__ void __launch_bounds__(kThreads) pcg_direction_kernel(int64_t n, XT* __restrict__ p, const XT* __restrict__ z,
+                                                                 const PcgState* st) {
+    if (st->done) return;
+    const XT beta = (XT)st->beta;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         p[i] = z[i] + beta * p[i];
 }
 
-// r = b, x = 0, z = D^-1 b, p = z; then (r, z), (z, z) and the initial state
-__global__ void __launch_bounds__(kThreads) pcg_init_kernel(int64_t n, const double* __restrict__ b, double* __restrict__ x,
-                                                            double* __restrict__ r, double* __restrict__ z,
-                                                            double* __restrict__ p, const double* __restrict__ dinv,
-                                                            double* __restrict__ part_rz, double* __restrict__ part_zz,
-                                                            PcgState* st, double rtol, double abstol, double dtol,
-                                                            int maxit) {
+// r = b, x = 0; JAC: z = D^-1 b, p = z, the fused (r, z), (z, z) and the initial state
+template <typename XT, bool JAC>
+__global__ void __launch_bounds__(kThreads) pcg_init_kernel(int64_t n, const XT* __restrict__ b, XT* __restrict__ x,
+                                                            XT* __restrict__ r, XT* __restrict__ z, XT* __restrict__ p,
+                                                            const XT* __restrict__ dinv, double* __restrict__ part_rz,
+                                                            double* __restrict__ part_zz, PcgState* st, double rtol,
+                                                            double abstol, double dtol, int maxit) {
     __shared__ double sh[32];
     double a1 = 0.0, a2 = 0.0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const double ri = b[i];
-        const double zi = dinv[i] * ri;
-        x[i] = 0.0;
+        const XT ri = b[i];
+        x[i] = 0;
         r[i] = ri;
-        z[i] = zi;
-        p[i] = zi;
-        a1 += ri * zi;
-        a2 += zi * zi;
+        if (JAC) {
+            const XT zi = dinv[i] * ri;
+            z[i] = zi;
+            p[i] = zi;
+            a1 += (double)ri * (double)zi;
+            a2 += (double)zi * (double)zi;
+        }
     }
+    if (!JAC) return;
     a1 = block_sum(a1, sh);
     if (threadIdx.x == 0) part_rz[blockIdx.x] = a1;
     a2 = block_sum(a2, sh);
@@ -205,39 +360,19 @@ __global__ void __launch_bounds__(kThreads) pcg_init_kernel(int64_t n, const dou
     const double zz = reduce_partials(part_zz, gridDim.x, sh);
     if (threadIdx.x == 0) {
         st->counter = 0;
-        const double dp = sqrt(zz);
-        st->rz = rz;
-        st->dp = dp;
-        st->dp0 = dp;
-        st->ttol = fmax(rtol * dp, abstol);
-        st->dtol = dtol;
-        st->maxit = maxit;
-        st->its = 0;
-        st->status = MPHY_OK;
-        st->done = 0;
-        if (dp != dp) {
-            st->status = MPHY_ERR_DIVERGED;
-            st->done = 1;
-        } else if (dp <= st->ttol) {
-            st->done = 1;
-        } else if (rz == 0.0) {
-            st->its = 1;
-            st->done = 1;
-        } else if (maxit <= 0) {
-            st->status = MPHY_ERR_NOT_CONVERGED;
-            st->done = 1;
-        }
+        finish_init(st, rz, zz, rtol, abstol, dtol, maxit);
     }
 }
 
-// PCJACOBI: inverse diagonal, a zero diagonal entry is replaced by 1
-__global__ void jacobi_kernel(SellView A, const double* __restrict__ val, double* __restrict__ dinv) {
+// PCJACOBI: inverse diagonal, a zero diagonal entry (or a node without blocks) gives 1
+template <typename VT, typename XT>
+__global__ void jacobi_kernel(SellView A, const VT* __restrict__ val, XT* __restrict__ dinv) {
     for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < A.n_node; n += (int64_t)gridDim.x * blockDim.x) {
         const uint32_t o = A.dvoff[n];
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-            const double d = o != 0xffffffffu ? val[o + 32u * (4 * a)] : 0.0;
-            dinv[3 * n + a] = d != 0.0 ? 1.0 / d : 1.0;
+            const double d = o != 0xffffffffu ? (double)val[o + 32u * (4 * a)] : 0.0;
+            dinv[3 * n + a] = (XT)(d != 0.0 ? 1.0 / d : 1.0);
         }
     }
 }
@@ -258,13 +393,14 @@ __global__ void dot_kernel(const double* __restrict__ a, const double* __restric
     }
 }
 
-__global__ void prescribed_diag_kernel(SellView A, const uint8_t* __restrict__ fixed, double* __restrict__ val) {
+template <typename VT>
+__global__ void prescribed_diag_kernel(SellView A, const uint8_t* __restrict__ fixed, VT* __restrict__ val) {
     for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < A.n_node; n += (int64_t)gridDim.x * blockDim.x) {
         const uint32_t o = A.dvoff[n];
         if (o == 0xffffffffu) continue;
 #pragma unroll
         for (int a = 0; a < 3; ++a)
-            if (fixed[3 * n + a]) val[o + 32u * (4 * a)] = 1.0;
+            if (fixed[3 * n + a]) val[o + 32u * (4 * a)] = (VT)1;
     }
 }
 
@@ -274,15 +410,22 @@ __global__ void add_scaled_free_kernel(const uint8_t* __restrict__ fixed, const 
         if (!fixed[i]) rhs[i] += scale * f[i];
 }
 
-__global__ void axpy_kernel(double* __restrict__ y, const double* __restrict__ x, double a, int64_t n) {
+template <typename XT>
+__global__ void axpy_kernel(double* __restrict__ y, const XT* __restrict__ x, double a, int64_t n) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        y[i] += a * x[i];
+        y[i] += a * (double)x[i];
 }
 
-__global__ void gather_values_kernel(const double* __restrict__ val, const int64_t* __restrict__ src,
+__global__ void to_f32_kernel(const double* __restrict__ in, float* __restrict__ out, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = (float)in[i];
+}
+
+template <typename VT>
+__global__ void gather_values_kernel(const VT* __restrict__ val, const int64_t* __restrict__ src,
                                      double* __restrict__ out, int64_t n) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        out[i] = val[src[i]];
+        out[i] = (double)val[src[i]];
 }
 
 __global__ void gather_free_kernel(const double* __restrict__ v, const int32_t* __restrict__ assy,
@@ -293,11 +436,28 @@ __global__ void gather_free_kernel(const double* __restrict__ v, const int32_t* 
 
 }  // namespace
 
-void spmv_fp64(const SellView& A, const double* val, const double* x, double* y, cudaStream_t s, int sm) {
-    spmv_fp64_kernel<false><<<stride_grid((int64_t)A.n_slices * 32, kThreads, sm), kThreads, 0, s>>>(
+// ---------------------------------------------------------------- host wrappers
+template <typename VT, typename XT>
+void spmv(const SellView& A, const VT* val, const XT* x, XT* y, cudaStream_t s, int sm) {
+    spmv_kernel<VT, XT, false><<<stride_grid((int64_t)A.n_slices * 32, kThreads, sm), kThreads, 0, s>>>(
         A, val, x, y, nullptr, nullptr);
     MPHY_CUDA(cudaGetLastError());
 }
+template void spmv<double, double>(const SellView&, const double*, const double*, double*, cudaStream_t, int);
+template void spmv<float, float>(const SellView&, const float*, const float*, float*, cudaStream_t, int);
+template void spmv<float, double>(const SellView&, const float*, const double*, double*, cudaStream_t, int);
+
+template <typename VT>
+void residual_fp64(const SellView& A, const VT* val, const double* x, const double* b, double* r, double* partials,
+                   uint32_t* counter, double* out_dev, cudaStream_t s, int sm) {
+    residual_kernel<VT><<<stride_grid((int64_t)A.n_slices * 32, kThreads, sm), kThreads, 0, s>>>(
+        A, val, x, b, r, partials, counter, out_dev);
+    MPHY_CUDA(cudaGetLastError());
+}
+template void residual_fp64<double>(const SellView&, const double*, const double*, const double*, double*, double*,
+                                    uint32_t*, double*, cudaStream_t, int);
+template void residual_fp64<float>(const SellView&, const float*, const double*, const double*, double*, double*,
+                                   uint32_t*, double*, cudaStream_t, int);
 
 void dot_fp64(const double* a, const double* b, int64_t n, double* partials, uint32_t* counter, double* out_dev,
               cudaStream_t s, int sm) {
@@ -305,10 +465,13 @@ void dot_fp64(const double* a, const double* b, int64_t n, double* partials, uin
     MPHY_CUDA(cudaGetLastError());
 }
 
-void set_prescribed_diagonal(const SellView& A, const uint8_t* fixed, double* val, cudaStream_t s, int sm) {
-    prescribed_diag_kernel<<<stride_grid(A.n_node, kThreads, sm), kThreads, 0, s>>>(A, fixed, val);
+template <typename VT>
+void set_prescribed_diagonal(const SellView& A, const uint8_t* fixed, VT* val, cudaStream_t s, int sm) {
+    prescribed_diag_kernel<VT><<<stride_grid(A.n_node, kThreads, sm), kThreads, 0, s>>>(A, fixed, val);
     MPHY_CUDA(cudaGetLastError());
 }
+template void set_prescribed_diagonal<double>(const SellView&, const uint8_t*, double*, cudaStream_t, int);
+template void set_prescribed_diagonal<float>(const SellView&, const uint8_t*, float*, cudaStream_t, int);
 
 void add_scaled_free(const uint8_t* fixed, const double* f, double scale, double* rhs, int64_t n, cudaStream_t s,
                      int sm) {
@@ -317,15 +480,18 @@ void add_scaled_free(const uint8_t* fixed, const double* f, double scale, double
 }
 
 void axpy_inplace(double* y, const double* x, double a, int64_t n, cudaStream_t s, int sm) {
-    axpy_kernel<<<stride_grid(n, kThreads, sm), kThreads, 0, s>>>(y, x, a, n);
+    axpy_kernel<double><<<stride_grid(n, kThreads, sm), kThreads, 0, s>>>(y, x, a, n);
     MPHY_CUDA(cudaGetLastError());
 }
 
-void gather_values(const double* val, const int64_t* src, double* out, int64_t n, cudaStream_t s, int sm) {
+template <typename VT>
+void gather_values(const VT* val, const int64_t* src, double* out, int64_t n, cudaStream_t s, int sm) {
     if (n <= 0) return;
-    gather_values_kernel<<<stride_grid(n, kThreads, sm), kThreads, 0, s>>>(val, src, out, n);
+    gather_values_kernel<VT><<<stride_grid(n, kThreads, sm), kThreads, 0, s>>>(val, src, out, n);
     MPHY_CUDA(cudaGetLastError());
 }
+template void gather_values<double>(const double*, const int64_t*, double*, int64_t, cudaStream_t, int);
+template void gather_values<float>(const float*, const int64_t*, double*, int64_t, cudaStream_t, int);
 
 void gather_free(const double* v, const int32_t* assy, double* out, int64_t n_free, cudaStream_t s, int sm) {
     if (n_free <= 0) return;
@@ -334,7 +500,8 @@ void gather_free(const double* v, const int32_t* assy, double* out, int64_t n_fr
 }
 
 // ---------------------------------------------------------------- PCG driver
-void PcgFp64::init(const SellView& A, int sm_count, int chunk) {
+template <typename VT, typename XT>
+void Pcg<VT, XT>::init(const SellView& A, int sm_count, int chunk) {
     A_ = A;
     sm_ = sm_count;
     chunk_ = chunk > 0 ? chunk : 32;
@@ -343,6 +510,7 @@ void PcgFp64::init(const SellView& A, int sm_count, int chunk) {
     z_.alloc(n_);
     p_.alloc(n_);
     q_.alloc(n_);
+    t_.alloc(n_);
     dinv_.alloc(n_);
     const size_t np = (size_t)sm_ * 8 + 8;
     partials_.alloc(np);
@@ -351,29 +519,55 @@ void PcgFp64::init(const SellView& A, int sm_count, int chunk) {
     MPHY_CUDA(cudaMemset(st_.p, 0, sizeof(PcgState)));
 }
 
-PcgFp64::~PcgFp64() {
+template <typename VT, typename XT>
+Pcg<VT, XT>::~Pcg() {
     if (graph_) cudaGraphExecDestroy(graph_);
 }
 
-void PcgFp64::record_iterations(const double* val, double* x, cudaStream_t s, int n_iter) {
+template <typename VT, typename XT>
+void Pcg<VT, XT>::record_iterations(const VT* val, XT* x, cudaStream_t s, int n_iter) {
     const unsigned gs = stride_grid((int64_t)A_.n_slices * 32, kThreads, sm_);
     const unsigned gv = stride_grid(n_, kThreads, sm_);
     for (int it = 0; it < n_iter; ++it) {
-        spmv_fp64_kernel<true><<<gs, kThreads, 0, s>>>(A_, val, p_.p, q_.p, partials_.p, st_.p);
-        pcg_update_kernel<<<gv, kThreads, 0, s>>>(n_, x, r_.p, z_.p, p_.p, q_.p, dinv_.p, partials_.p, partials2_.p,
-                                                   st_.p);
-        pcg_direction_kernel<<<gv, kThreads, 0, s>>>(n_, p_.p, z_.p, st_.p);
+        spmv_kernel<VT, XT, true><<<gs, kThreads, 0, s>>>(A_, val, p_.p, q_.p, partials_.p, st_.p);
+        if (kind_ == PcKind::Jacobi) {
+            pcg_update_kernel<XT, true><<<gv, kThreads, 0, s>>>(n_, x, r_.p, z_.p, p_.p, q_.p, dinv_.p, partials_.p,
+                                                                 partials2_.p, st_.p);
+        } else {
+            pcg_update_kernel<XT, false><<<gv, kThreads, 0, s>>>(n_, x, r_.p, z_.p, p_.p, q_.p, nullptr, nullptr,
+                                                                  nullptr, st_.p);
+            const unsigned gg = stride_grid((int64_t)factor_.G.n_slices * 32, kThreads, sm_);
+            spmv_kernel<float, XT, false><<<gg, kThreads, 0, s>>>(factor_.G, factor_.gval, r_.p, t_.p, nullptr, st_.p);
+            factor_apply_kernel<XT, false><<<gg, kThreads, 0, s>>>(factor_.GT, factor_.gtval, t_.p, z_.p, r_.p, p_.p,
+                                                                    partials_.p, partials2_.p, st_.p, 0, 0, 0, 0);
+        }
+        pcg_direction_kernel<XT><<<gv, kThreads, 0, s>>>(n_, p_.p, z_.p, st_.p);
     }
 }
 
-int PcgFp64::solve(const double* val, const double* b, double* x, double rtol, double abstol, double dtol, int maxit,
-                   cudaStream_t s, int32_t* its, double* final_norm) {
-    jacobi_kernel<<<stride_grid(A_.n_node, kThreads, sm_), kThreads, 0, s>>>(A_, val, dinv_.p);
-    pcg_init_kernel<<<stride_grid(n_, kThreads, sm_), kThreads, 0, s>>>(n_, b, x, r_.p, z_.p, p_.p, dinv_.p,
-                                                                        partials_.p, partials2_.p, st_.p, rtol, abstol,
-                                                                        dtol, maxit);
+template <typename VT, typename XT>
+int Pcg<VT, XT>::solve(const VT* val, const XT* b, XT* x, double rtol, double abstol, double dtol, int maxit,
+                       cudaStream_t s, int32_t* its, double* final_norm) {
+    const unsigned gv = stride_grid(n_, kThreads, sm_);
+    launches = 0;
+    if (kind_ == PcKind::Jacobi) {
+        jacobi_kernel<VT, XT><<<stride_grid(A_.n_node, kThreads, sm_), kThreads, 0, s>>>(A_, val, dinv_.p);
+        pcg_init_kernel<XT, true><<<gv, kThreads, 0, s>>>(n_, b, x, r_.p, z_.p, p_.p, dinv_.p, partials_.p,
+                                                           partials2_.p, st_.p, rtol, abstol, dtol, maxit);
+        launches += 2;
+    } else {
+        pcg_init_kernel<XT, false><<<gv, kThreads, 0, s>>>(n_, b, x, r_.p, z_.p, p_.p, nullptr, nullptr, nullptr,
+                                                            st_.p, rtol, abstol, dtol, maxit);
+        const unsigned gg = stride_grid((int64_t)factor_.G.n_slices * 32, kThreads, sm_);
+        spmv_kernel<float, XT, false><<<gg, kThreads, 0, s>>>(factor_.G, factor_.gval, r_.p, t_.p, nullptr, nullptr);
+        factor_apply_kernel<XT, true><<<gg, kThreads, 0, s>>>(factor_.GT, factor_.gtval, t_.p, z_.p, r_.p, p_.p,
+                                                               partials_.p, partials2_.p, st_.p, rtol, abstol, dtol,
+                                                               maxit);
+        launches += 3;
+    }
     MPHY_CUDA(cudaGetLastError());
-    if (!graph_ || graph_val_ != val || graph_x_ != x || graph_stream_ != s) {
+    if (!graph_ || graph_val_ != (const void*)val || graph_x_ != (void*)x || graph_stream_ != s ||
+        graph_kind_ != kind_) {
         if (graph_) {
             cudaGraphExecDestroy(graph_);
             graph_ = nullptr;
@@ -387,22 +581,103 @@ int PcgFp64::solve(const double* val, const double* b, double* x, double rtol, d
         graph_val_ = val;
         graph_x_ = x;
         graph_stream_ = s;
+        graph_kind_ = kind_;
     }
-    launches = 2;
+    const int per_iter = kind_ == PcKind::Jacobi ? 3 : 5;
     PcgState h{};
     // every replay advances at most chunk_ iterations; the device stops at maxit
-    const int64_t max_replays = (int64_t)maxit / chunk_ + 2;
+    const int64_t max_replays = (int64_t)(maxit > 0 ? maxit : 0) / chunk_ + 2;
     for (int64_t rep = 0;; ++rep) {
         MPHY_CUDA(cudaMemcpyAsync(&h, st_.p, sizeof(PcgState), cudaMemcpyDeviceToHost, s));
         MPHY_CUDA(cudaStreamSynchronize(s));
         if (h.done) break;
         MPHY_REQUIRE(rep < max_replays, MPHY_ERR_CUDA, "internal: CG state never reached done");
         MPHY_CUDA(cudaGraphLaunch(graph_, s));
-        launches += 3 * (int64_t)chunk_;
+        launches += (int64_t)per_iter * chunk_;
     }
     if (its) *its = h.its;
     if (final_norm) *final_norm = h.dp;
     return h.status;
 }
+
+template class Pcg<double, double>;
+template class Pcg<float, float>;
+
+// ---------------------------------------------------------------- iterative refinement
+namespace {
+__global__ void copy_f64_kernel(const double* __restrict__ in, double* __restrict__ out, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = in[i];
+}
+void to_inner(const double* in, float* out, int64_t n, unsigned g, cudaStream_t s) {
+    to_f32_kernel<<<g, kThreads, 0, s>>>(in, out, n);
+}
+void to_inner(const double* in, double* out, int64_t n, unsigned g, cudaStream_t s) {
+    copy_f64_kernel<<<g, kThreads, 0, s>>>(in, out, n);
+}
+}  // namespace
+
+template <typename XT>
+void IterativeRefinement<XT>::init(const SellView& A, int sm_count, int chunk) {
+    A_ = A;
+    sm_ = sm_count;
+    n_ = 3 * (int64_t)A.n_node;
+    inner_.init(A, sm_count, chunk);
+    r64_.alloc(n_);
+    rin_.alloc(n_);
+    d_.alloc(n_);
+    partials_.alloc((size_t)sm_count * 8 + 8);
+    scalars_.alloc(2);
+    counter_.alloc(1);
+    MPHY_CUDA(cudaMemset(counter_.p, 0, sizeof(uint32_t)));
+}
+
+template <typename XT>
+int IterativeRefinement<XT>::solve(const float* val, const double* b, double* x, double rtol, double inner_rtol,
+                                   int max_outer, int maxit, cudaStream_t s, int32_t* its, int32_t* sweeps,
+                                   double* relres) {
+    const unsigned gv = stride_grid(n_, kThreads, sm_);
+    launches = 0;
+    MPHY_CUDA(cudaMemsetAsync(x, 0, n_ * sizeof(double), s));
+    MPHY_CUDA(cudaMemcpyAsync(r64_.p, b, n_ * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    dot_fp64(b, b, n_, partials_.p, counter_.p, scalars_.p, s, sm_);
+    double bb = 0.0;
+    MPHY_CUDA(cudaMemcpyAsync(&bb, scalars_.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+    MPHY_CUDA(cudaStreamSynchronize(s));
+    launches += 1;
+    const double bnorm = std::sqrt(bb);
+    int total = 0, k = 0, status = MPHY_OK;
+    double rel = bnorm > 0.0 ? 1.0 : 0.0;
+    while (rel > rtol && k < max_outer && total < maxit) {
+        to_inner(r64_.p, rin_.p, n_, gv, s);
+        int32_t it = 0;
+        double dn = 0.0;
+        const int st = inner_.solve(val, rin_.p, d_.p, inner_rtol > 0.0 ? inner_rtol : rtol, 0.0, 1e5, maxit - total,
+                                    s, &it, &dn);
+        launches += inner_.launches + 1;
+        total += it;
+        axpy_kernel<XT><<<gv, kThreads, 0, s>>>(x, d_.p, 1.0, n_);
+        residual_fp64<float>(A_, val, x, b, r64_.p, partials_.p, counter_.p, scalars_.p, s, sm_);
+        launches += 2;
+        double rr = 0.0;
+        MPHY_CUDA(cudaMemcpyAsync(&rr, scalars_.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+        MPHY_CUDA(cudaStreamSynchronize(s));
+        rel = std::sqrt(rr) / bnorm;
+        ++k;
+        if (st == MPHY_ERR_INDEFINITE || st == MPHY_ERR_DIVERGED) {
+            status = st;
+            break;
+        }
+    }
+    if (status == MPHY_OK && rel > rtol) status = MPHY_ERR_NOT_CONVERGED;
+    if (its) *its = total;
+    if (sweeps) *sweeps = k;
+    if (relres) *relres = rel;
+    return status;
+}
+
+template class Pcg<float, double>;
+template class IterativeRefinement<double>;
+template class IterativeRefinement<float>;
 
 }  // namespace mphy

@@ -1,5 +1,5 @@
-// krylov.cuh -- K4/K5: SELL-32 3x3 SpMV, Jacobi-preconditioned CG with PETSc KSPCG semantics,
-// and the FP64 vector operations around it.
+// krylov.cuh -- K4/K5: SELL-32 3x3 SpMV, preconditioned CG with PETSc KSPCG semantics (FP64, or
+// FP32 vectors with FP64 reductions), FP64 iterative refinement, and the vector operations.
 #pragma once
 #include "common.cuh"
 
@@ -33,45 +33,97 @@ struct SellView {
     const uint32_t* dvoff;
 };
 
+// Factorised preconditioner M = G^T G: G lower block-triangular and G^T, both in SELL layout
+// with FP32 values.
+template <typename VT>
+struct FactorView {
+    SellView G, GT;
+    const VT* gval;
+    const VT* gtval;
+};
+
 // Grid of a grid-stride kernel over n items with the given block size.
 unsigned stride_grid(int64_t n, int threads, int sm_count, int per_sm = 8);
 
-// y = A x (FP64 values and vectors).
-void spmv_fp64(const SellView& A, const double* val, const double* x, double* y, cudaStream_t s, int sm);
+// y = A x.
+template <typename VT, typename XT>
+void spmv(const SellView& A, const VT* val, const XT* x, XT* y, cudaStream_t s, int sm);
+
+// r = b - A x in FP64 (A in VT), and ||r||^2 into *out_dev; partials [sm*8+8], counter zeroed.
+template <typename VT>
+void residual_fp64(const SellView& A, const VT* val, const double* x, const double* b, double* r, double* partials,
+                   uint32_t* counter, double* out_dev, cudaStream_t s, int sm);
 
 // Deterministic FP64 dot product of two device vectors; result left in *out_dev.
 void dot_fp64(const double* a, const double* b, int64_t n, double* partials, uint32_t* counter, double* out_dev,
               cudaStream_t s, int sm);
 
-// Jacobi-PCG driver, FP64. Holds its work vectors; solve() runs from x = 0.
-class PcgFp64 {
+enum class PcKind { Jacobi, Factor };
+
+// Preconditioned CG, VT = matrix values, XT = vector precision (double, or float with FP64
+// reductions). solve() runs from x = 0 on b (XT), PETSc KSPCG semantics.
+template <typename VT, typename XT>
+class Pcg {
   public:
     void init(const SellView& A, int sm_count, int chunk);
-    // b: [3*n_node] FP64 (prescribed DOFs zero). x: [3*n_node] output.
-    int solve(const double* val, const double* b, double* x, double rtol, double abstol, double dtol, int maxit,
-              cudaStream_t s, int32_t* its, double* final_norm);
-    ~PcgFp64();
+    void set_factor(const FactorView<float>& f) { factor_ = f; kind_ = PcKind::Factor; }
+    void set_jacobi() { kind_ = PcKind::Jacobi; }
+    int solve(const VT* val, const XT* b, XT* x, double rtol, double abstol, double dtol, int maxit, cudaStream_t s,
+              int32_t* its, double* final_norm);
+    ~Pcg();
     int64_t launches = 0;  // kernels launched by the last solve()
 
   private:
-    void record_iterations(const double* val, double* x, cudaStream_t s, int n_iter);
+    void record_iterations(const VT* val, XT* x, cudaStream_t s, int n_iter);
     SellView A_{};
+    PcKind kind_ = PcKind::Jacobi;
+    FactorView<float> factor_{};
     int sm_ = 148, chunk_ = 32;
     int64_t n_ = 0;
-    DevBuf<double> r_, z_, p_, q_, dinv_, partials_, partials2_;
+    DevBuf<XT> r_, z_, p_, q_, t_, dinv_;
+    DevBuf<double> partials_, partials2_;
     DevBuf<PcgState> st_;
     cudaGraphExec_t graph_ = nullptr;
-    const double* graph_val_ = nullptr;
-    double* graph_x_ = nullptr;
+    const void* graph_val_ = nullptr;
+    void* graph_x_ = nullptr;
     cudaStream_t graph_stream_ = nullptr;
+    PcKind graph_kind_ = PcKind::Jacobi;
+};
+
+using PcgFp64 = Pcg<double, double>;
+
+// FP64 iterative refinement around a PCG on the FP32-stored operator A32:
+//   x = 0, r = b; repeat { d = PCG(A32, r, inner_rtol); x += d; r = b - A32 x (FP64) }
+// until ||r|| <= rtol ||b|| or max_outer sweeps. XT is the inner Krylov vector precision:
+// double (FP32 values, FP64 vectors and reductions) or float (FP32 vectors, FP64 reductions).
+// x: FP64 output. Returns an mphy_status.
+template <typename XT>
+class IterativeRefinement {
+  public:
+    void init(const SellView& A, int sm_count, int chunk);
+    Pcg<float, XT>& inner() { return inner_; }
+    int solve(const float* val, const double* b, double* x, double rtol, double inner_rtol, int max_outer, int maxit,
+              cudaStream_t s, int32_t* its, int32_t* sweeps, double* relres);
+    int64_t launches = 0;
+
+  private:
+    SellView A_{};
+    int sm_ = 148;
+    int64_t n_ = 0;
+    Pcg<float, XT> inner_;
+    DevBuf<double> r64_, partials_, scalars_;
+    DevBuf<XT> rin_, d_;
+    DevBuf<uint32_t> counter_;
 };
 
 // small kernels of the solver surface
-void set_prescribed_diagonal(const SellView& A, const uint8_t* fixed, double* val, cudaStream_t s, int sm);
+template <typename VT>
+void set_prescribed_diagonal(const SellView& A, const uint8_t* fixed, VT* val, cudaStream_t s, int sm);
 void add_scaled_free(const uint8_t* fixed, const double* f, double scale, double* rhs, int64_t n, cudaStream_t s,
                      int sm);
 void axpy_inplace(double* y, const double* x, double a, int64_t n, cudaStream_t s, int sm);
-void gather_values(const double* val, const int64_t* src, double* out, int64_t n, cudaStream_t s, int sm);
+template <typename VT>
+void gather_values(const VT* val, const int64_t* src, double* out, int64_t n, cudaStream_t s, int sm);
 void gather_free(const double* v, const int32_t* assy, double* out, int64_t n_free, cudaStream_t s, int sm);
 
 }  // namespace mphy

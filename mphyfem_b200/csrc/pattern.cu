@@ -367,6 +367,7 @@ void build_pattern(mphy_ctx* ctx, const mphy_mesh* mesh, mphy_pattern* P) {
     const int32_t nn = mesh->n_node, ne = mesh->n_elem, npe = mesh->npe;
     P->ctx = ctx;
     P->mesh = mesh;
+    P->device = ctx->device;
     P->n_node = nn;
     P->n_elem = ne;
     P->npe = npe;

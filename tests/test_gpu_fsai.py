@@ -1,0 +1,74 @@
+"""Block FSAI preconditioner (M = G^T G) against its numpy restatement, and FSAI-PCG against the
+FP64 oracle solve. G is stored in FP32: blocks agree within 1e-5 of the row's largest entry;
+FSAI-PCG solutions agree with the oracle's to 1e-9 at rtol 1e-12 and need fewer iterations
+than Jacobi-PCG."""
+import numpy as np
+import pytest
+
+from mphyfem_b200 import meshgen
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def env():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no GPU")
+    from mphyfem_b200 import _lib, api, build
+    build.build()
+    return torch, api, _lib, api.Context(0)
+
+
+@pytest.mark.parametrize("mk", [lambda: meshgen.hex8_cantilever(10, 3, 3),
+                                lambda: meshgen.tet10_kuhn(3, 2, 2, lx=1.5)])
+def test_fsai_blocks_match_restatement(env, mk):
+    from oracle import fsai_ref
+    torch, api, _lib, ctx = env
+    p = mk()
+    mesh = api.Mesh(ctx, p)
+    pat = api.Pattern(mesh)
+    # the consistent tangent: with kappa = 100 the reference tangent is locally indefinite here
+    sol = api.SolverGpu(mesh, pat, pc_type=_lib.PC_FSAI, tangent=1)
+    rng = np.random.default_rng(2)
+    u = 0.01 * rng.standard_normal(p.n_dof) * (p.fixed == 0)
+    sol.calcStiffnessAndResidual(torch.tensor(u, device="cuda"))
+    assert sol.pc_setup() == 0
+    G = sol.pc_get_blocks().cpu().numpy()
+    rp, col = sol.pc_pattern()
+    val, _, _ = sol.export(want_rhs=False, want_reac=False)
+    crp, ccol = pat.export_csr()
+    A = fsai_ref.full_operator(p.n_node, p.fixed, crp, ccol, val)
+    nbrs = fsai_ref.node_neighbours(p.conn, p.n_node)
+    orp, ocol, oblk = fsai_ref.block_fsai(A, nbrs, max_lower=16)
+    assert np.array_equal(rp, orp) and np.array_equal(col, ocol)
+    for n in range(p.n_node):
+        g, o = G[rp[n]:rp[n + 1]], oblk[orp[n]:orp[n + 1]]
+        assert np.abs(g - o).max() <= 1e-5 * np.abs(o).max()
+
+
+@pytest.mark.parametrize("prec", ["PREC_FP64", "PREC_MIXED"])
+def test_fsai_pcg_matches_oracle_with_fewer_iterations(env, oracle, prec):
+    torch, api, _lib, ctx = env
+    p = meshgen.cantilever_small()
+    mesh = api.Mesh(ctx, p)
+    pat = api.Pattern(mesh)
+    zero = torch.zeros(p.n_dof, dtype=torch.float64, device="cuda")
+    f = torch.tensor(p.fnodal, device="cuda")
+    its = {}
+    xs = {}
+    for pc in ("PC_JACOBI", "PC_FSAI"):
+        sol = api.SolverGpu(mesh, pat, pc_type=getattr(_lib, pc), precision=getattr(_lib, prec), rtol=1e-12)
+        sol.calcStiffnessAndResidual(zero)
+        sol.addExternalForces(f, 0.2)
+        rc, its[pc], _ = sol.factoriseAndSolve()
+        assert rc == 0
+        xs[pc] = sol.solution().cpu().numpy()
+    op = oracle.OracleProblem(p)
+    val, _, _, _ = op.assemble(np.zeros(p.n_dof))
+    free = np.flatnonzero(p.fixed == 0)
+    xo, _, _, _ = op.cg(val, 0.2 * p.fnodal[free], rtol=1e-13)
+    tol = 1e-9 if prec == "PREC_FP64" else 1e-2  # FP32-stored operator: cond(A) * 6e-8
+    assert np.linalg.norm(xs["PC_FSAI"][free] - xo) <= tol * np.linalg.norm(xo)
+    assert np.linalg.norm(xs["PC_FSAI"] - xs["PC_JACOBI"]) <= 1e-8 * np.linalg.norm(xs["PC_JACOBI"])
+    assert its["PC_FSAI"] < 0.7 * its["PC_JACOBI"], its
