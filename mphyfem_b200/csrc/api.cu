@@ -57,7 +57,8 @@ struct mphy_solver {
     SellView A{};
     bool mixed = false;          // MPHY_PREC_MIXED: FP32 values + FP64 iterative refinement
     DevBuf<double> val;          // SELL values, FP64 (plain method)
-    DevBuf<float> valf;          // SELL values, FP32 (mixed precision)
+    DevBuf<float> valf;          // SELL values, FP32 (mixed precision): off-diagonal blocks, unmasked
+    DevBuf<double> diag64;       // [n_node][9] FP64 diagonal blocks = -sum of the stored off-diagonals
     DevBuf<double> rhs, reac, x; // [3*n_node]
     DevBuf<unsigned long long> bad;
     DevBuf<double> partials, scalar;
@@ -79,7 +80,7 @@ void solver_zero(mphy_solver* s) {
     cudaStream_t st = s->ctx->stream;
     if (s->mixed) {
         MPHY_CUDA(cudaMemsetAsync(s->valf.p, 0, s->valf.bytes(), st));
-        set_prescribed_diagonal<float>(s->A, s->mesh->fixed.p, s->valf.p, st, s->ctx->sm_count);
+        MPHY_CUDA(cudaMemsetAsync(s->diag64.p, 0, s->diag64.bytes(), st));
     } else {
         MPHY_CUDA(cudaMemsetAsync(s->val.p, 0, s->val.bytes(), st));
         set_prescribed_diagonal<double>(s->A, s->mesh->fixed.p, s->val.p, st, s->ctx->sm_count);
@@ -114,6 +115,10 @@ void solver_assemble(mphy_solver* s, const double* disp) {
     a.reac = s->reac.p;
     launch_elem_fp64(a, s->mesh->npe, 2, s->ctx->stream);
     s->launches += 1;
+    if (s->mixed) {
+        diag_from_offdiag(s->A, s->valf.p, s->diag64.p, s->ctx->stream, s->ctx->sm_count);
+        s->launches += 1;
+    }
     s->state = MPHY_ASSEMBLY_OK;
 }
 
@@ -139,8 +144,8 @@ int solver_solve(mphy_solver* s, int32_t* its, double* fnorm) {
     if (s->use_fsai && s->opts.pc_type == MPHY_PC_FSAI) {
         // the preconditioner follows the operator: rebuilt for every solve (KSPSetReusePreconditioner false)
         MPHY_CUDA(cudaEventRecord(s->ctx->ev0, s->ctx->stream));
-        if (s->mixed) s->fsai.compute<float>(s->valf.p, s->ctx->stream);
-        else s->fsai.compute<double>(s->val.p, s->ctx->stream);
+        if (s->mixed) s->fsai.compute<float>(s->valf.p, s->diag64.p, s->mesh->fixed.p, s->ctx->stream);
+        else s->fsai.compute<double>(s->val.p, nullptr, nullptr, s->ctx->stream);
         MPHY_CUDA(cudaEventRecord(s->ctx->ev1, s->ctx->stream));
         MPHY_CUDA(cudaEventSynchronize(s->ctx->ev1));
         float ms = 0.f;
@@ -483,8 +488,14 @@ int mphy_solver_create(mphy_ctx* c, const mphy_mesh* m, const mphy_pattern* P, c
             s->opts = o;
             s->A = SellView{P->n_node, P->n_slices, P->slice_base.p, P->slice_width.p, P->sell_col.p, P->dvoff.p};
             s->mixed = o.precision != MPHY_PREC_FP64;
-            if (s->mixed) s->valf.alloc(9 * (size_t)P->sell_blocks);
-            else s->val.alloc(9 * (size_t)P->sell_blocks);
+            if (s->mixed) {
+                s->valf.alloc(9 * (size_t)P->sell_blocks);
+                s->diag64.alloc(9 * (size_t)P->n_node);
+                s->A.diag64 = s->diag64.p;
+                s->A.fixed = m->fixed.p;
+            } else {
+                s->val.alloc(9 * (size_t)P->sell_blocks);
+            }
             const size_t nd = 3 * (size_t)m->n_node;
             s->rhs.alloc(nd);
             s->reac.alloc(nd);
@@ -568,6 +579,7 @@ int mphy_solver_assemble_batch(mphy_solver* s, int32_t n, const int32_t* ids, co
         MPHY_REQUIRE(ids || n == s->mesh->n_elem, MPHY_ERR_INVALID_ARG, "without ids, n must equal n_elem");
         launch_scatter_batch(s->mesh->npe, n, ids, s->mesh, s->pat, Ke, Re, s->val.p, s->mixed ? s->valf.p : nullptr,
                              s->rhs.p, s->reac.p, s->ctx->stream, s->ctx->sm_count);
+        if (s->mixed) diag_from_offdiag(s->A, s->valf.p, s->diag64.p, s->ctx->stream, s->ctx->sm_count);
         MPHY_CUDA(cudaStreamSynchronize(s->ctx->stream));
         s->state = MPHY_ASSEMBLY_OK;
         return (int)MPHY_OK;
@@ -656,8 +668,8 @@ int mphy_solver_pc_setup(mphy_solver* s, int32_t* n_fallback) {
         MPHY_REQUIRE(s->use_fsai, MPHY_ERR_STATE, "the solver has no factorised preconditioner");
         MPHY_REQUIRE(s->state == MPHY_ASSEMBLY_OK || s->state == MPHY_FACTORISE_OK, MPHY_ERR_STATE,
                      "assemble the matrix first");
-        if (s->mixed) s->fsai.compute<float>(s->valf.p, s->ctx->stream);
-        else s->fsai.compute<double>(s->val.p, s->ctx->stream);
+        if (s->mixed) s->fsai.compute<float>(s->valf.p, s->diag64.p, s->mesh->fixed.p, s->ctx->stream);
+        else s->fsai.compute<double>(s->val.p, nullptr, nullptr, s->ctx->stream);
         const int32_t nf = s->fsai.fallback_rows(s->ctx->stream);
         if (n_fallback) *n_fallback = nf;
         return (int)MPHY_OK;
@@ -689,8 +701,13 @@ int mphy_solver_export(mphy_solver* s, double* val_host, double* rhs_host, doubl
         if (val_host && s->pat->nnz > 0) {
             pattern_csr_columns(s->pat, true);
             DevBuf<double> tmp(s->pat->nnz);
-            if (s->mixed) gather_values<float>(s->valf.p, s->pat->csr_src.p, tmp.p, s->pat->nnz, st, sm);
-            else gather_values<double>(s->val.p, s->pat->csr_src.p, tmp.p, s->pat->nnz, st, sm);
+            if (s->mixed) {
+                gather_values<float>(s->valf.p, s->pat->csr_src.p, tmp.p, s->pat->nnz, st, sm);
+                export_fix_diagonal(s->diag64.p, s->pat->csr_rowptr.p, s->pat->csr_col.p, s->pat->assy_for_soln.p,
+                                    s->pat->n_free, tmp.p, st, sm);
+            } else {
+                gather_values<double>(s->val.p, s->pat->csr_src.p, tmp.p, s->pat->nnz, st, sm);
+            }
             tmp.download(val_host, s->pat->nnz, st);
             MPHY_CUDA(cudaStreamSynchronize(st));
         }

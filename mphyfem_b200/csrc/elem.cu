@@ -372,14 +372,19 @@ __global__ void __launch_bounds__(kEpb * NPE) elem_fp64_kernel(ElemArgs a) {
             if (MODE & 2) {
                 const int32_t nJ = a.conn[e * NPE + J];
                 const uint32_t off = a.e2v[(e * NPE + I) * NPE + J];
+                if (a.valf) {
+                    // FP32 storage: off-diagonal blocks, unmasked; the diagonal is rebuilt from them
+                    if (nJ != node) {
 #pragma unroll
-                for (int bb = 0; bb < 3; ++bb) {
-                    if (a.fixed[3 * (int64_t)nJ + bb]) continue;
+                        for (int v = 0; v < 9; ++v) atomicAdd(&a.valf[off + 32u * v], (float)acc[j][v]);
+                    }
+                } else {
 #pragma unroll
-                    for (int aa = 0; aa < 3; ++aa) {
-                        if (!freeI[aa]) continue;
-                        if (a.valf) atomicAdd(&a.valf[off + 32u * (3 * aa + bb)], (float)acc[j][3 * aa + bb]);
-                        else atomicAdd(&a.val[off + 32u * (3 * aa + bb)], acc[j][3 * aa + bb]);
+                    for (int bb = 0; bb < 3; ++bb) {
+                        if (a.fixed[3 * (int64_t)nJ + bb]) continue;
+#pragma unroll
+                        for (int aa = 0; aa < 3; ++aa)
+                            if (freeI[aa]) atomicAdd(&a.val[off + 32u * (3 * aa + bb)], acc[j][3 * aa + bb]);
                     }
                 }
             }
@@ -437,13 +442,18 @@ __global__ void scatter_batch_kernel(int32_t n, const int32_t* __restrict__ ids,
         const int64_t e = ids ? ids[k] : k;
         const int32_t nI = conn[e * NPE + I], nJ = conn[e * NPE + J];
         const uint32_t off = e2v[e * NPE * NPE + IJ];
-        for (int aa = 0; aa < 3; ++aa) {
-            if (fixed[3 * (int64_t)nI + aa]) continue;
-            for (int bb = 0; bb < 3; ++bb) {
-                if (fixed[3 * (int64_t)nJ + bb]) continue;
-                const double v = Ke[(k * NS + 3 * I + aa) * NS + 3 * J + bb];
-                if (valf) atomicAdd(&valf[off + 32u * (3 * aa + bb)], (float)v);
-                else atomicAdd(&val[off + 32u * (3 * aa + bb)], v);
+        if (valf) {
+            // FP32 storage: off-diagonal blocks, unmasked; the diagonal is rebuilt from them
+            if (nI != nJ)
+                for (int v = 0; v < 9; ++v)
+                    atomicAdd(&valf[off + 32u * v], (float)Ke[(k * NS + 3 * I + v / 3) * NS + 3 * J + v % 3]);
+        } else {
+            for (int aa = 0; aa < 3; ++aa) {
+                if (fixed[3 * (int64_t)nI + aa]) continue;
+                for (int bb = 0; bb < 3; ++bb) {
+                    if (fixed[3 * (int64_t)nJ + bb]) continue;
+                    atomicAdd(&val[off + 32u * (3 * aa + bb)], Ke[(k * NS + 3 * I + aa) * NS + 3 * J + bb]);
+                }
             }
         }
         if (J == 0) {

@@ -20,7 +20,8 @@ struct ElemArgs {
     const uint8_t* fixed;
     const uint32_t* e2v;
     double* val;   // SELL values (FP64), or
-    float* valf;   // SELL values (FP32) when non-null
+    float* valf;   // SELL values (FP32) when non-null; then the scatter stores off-diagonal blocks
+                   // only, without Dirichlet masking (null-space-preserving storage)
     double* rhs;   // [n_node*3], prescribed DOFs untouched
     double* reac;  // [n_node*3] or null
 };

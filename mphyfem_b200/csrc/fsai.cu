@@ -160,6 +160,8 @@ struct SetupArgs {
     const int32_t* abcol;
     const int64_t* aslice;
     const VT* aval;
+    const double* diag64;  // mixed storage: FP64 diagonal blocks
+    const uint8_t* fixed;  // mixed storage: prescribed DOFs are identity rows / zero columns
     float* gval;
     float* gtval;
     int32_t* nfail;
@@ -167,6 +169,9 @@ struct SetupArgs {
 
 template <typename VT>
 __device__ __forceinline__ double a_block_entry(const SetupArgs<VT>& a, int32_t m1, int32_t m2, int v) {
+    if (a.fixed && (a.fixed[3 * (int64_t)m1 + v / 3] || a.fixed[3 * (int64_t)m2 + v % 3]))
+        return (m1 == m2 && v / 3 == v % 3) ? 1.0 : 0.0;
+    if (a.diag64 && m1 == m2) return a.diag64[9 * (int64_t)m1 + v];
     const int64_t b = a.abrow[m1], e = a.abrow[m1 + 1];
     const int64_t q = find_in_row(a.abcol, b, e, m2);
     if (q >= e || a.abcol[q] != m2) return 0.0;
@@ -359,7 +364,7 @@ void Fsai::init(mphy_ctx* ctx, const mphy_pattern* A, int max_lower) {
 }
 
 template <typename VT>
-void Fsai::compute(const VT* aval, cudaStream_t s) {
+void Fsai::compute(const VT* aval, const double* diag64, const uint8_t* fixed, cudaStream_t s) {
     SetupArgs<VT> a{};
     a.n_node = A_->n_node;
     a.max_lower = max_lower_;
@@ -371,6 +376,8 @@ void Fsai::compute(const VT* aval, cudaStream_t s) {
     a.abcol = A_->bcol.p;
     a.aslice = A_->slice_base.p;
     a.aval = aval;
+    a.diag64 = diag64;
+    a.fixed = fixed;
     a.gval = gval_.p;
     a.gtval = gtval_.p;
     a.nfail = err_.p;
@@ -384,8 +391,8 @@ void Fsai::compute(const VT* aval, cudaStream_t s) {
     launches = 1;
 }
 
-template void Fsai::compute<double>(const double*, cudaStream_t);
-template void Fsai::compute<float>(const float*, cudaStream_t);
+template void Fsai::compute<double>(const double*, const double*, const uint8_t*, cudaStream_t);
+template void Fsai::compute<float>(const float*, const double*, const uint8_t*, cudaStream_t);
 
 void Fsai::set_lower_values(const float* gblocks, cudaStream_t s) {
     set_lower_kernel<<<stride_grid(9 * L_.n_blocks, 256, ctx_->sm_count), 256, 0, s>>>(L_.n_blocks, gblocks,

@@ -28,8 +28,9 @@ class Fsai {
     void init(mphy_ctx* ctx, const mphy_pattern* A, int max_lower = 16);
     // Exact block FSAI of the assembled operator (values VT: double or float), FP64 local
     // Cholesky per block row, G and G^T stored in FP32.
+    // diag64 / fixed: the null-space-preserving storage of the mixed path (null for FP64).
     template <typename VT>
-    void compute(const VT* aval, cudaStream_t s);
+    void compute(const VT* aval, const double* diag64, const uint8_t* fixed, cudaStream_t s);
     // Install externally predicted G blocks (lower pattern order, [n_blocks][9] row-major FP32)
     // and mirror them into G^T.
     void set_lower_values(const float* gblocks, cudaStream_t s);

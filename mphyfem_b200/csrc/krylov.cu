@@ -155,6 +155,18 @@ __global__ void __launch_bounds__(kThreads) spmv_kernel(SellView A, const VT* __
             y2 += (Acc)v[192] * x0 + (Acc)v[224] * x1 + (Acc)v[256] * x2;
         }
         if (row < A.n_node) {
+            if (A.diag64) {
+                const double* D = A.diag64 + 9 * row;
+                const double x0 = (double)x[3 * row], x1 = (double)x[3 * row + 1], x2 = (double)x[3 * row + 2];
+                y0 = (Acc)((double)y0 + D[0] * x0 + D[1] * x1 + D[2] * x2);
+                y1 = (Acc)((double)y1 + D[3] * x0 + D[4] * x1 + D[5] * x2);
+                y2 = (Acc)((double)y2 + D[6] * x0 + D[7] * x1 + D[8] * x2);
+            }
+            if (A.fixed) {
+                if (A.fixed[3 * row]) y0 = (Acc)x[3 * row];
+                if (A.fixed[3 * row + 1]) y1 = (Acc)x[3 * row + 1];
+                if (A.fixed[3 * row + 2]) y2 = (Acc)x[3 * row + 2];
+            }
             y[3 * row] = (XT)y0;
             y[3 * row + 1] = (XT)y1;
             y[3 * row + 2] = (XT)y2;
@@ -266,6 +278,18 @@ __global__ void __launch_bounds__(kThreads) residual_kernel(SellView A, const VT
             y2 += (double)v[192] * x0 + (double)v[224] * x1 + (double)v[256] * x2;
         }
         if (row < A.n_node) {
+            if (A.diag64) {
+                const double* D = A.diag64 + 9 * row;
+                const double x0 = x[3 * row], x1 = x[3 * row + 1], x2 = x[3 * row + 2];
+                y0 += D[0] * x0 + D[1] * x1 + D[2] * x2;
+                y1 += D[3] * x0 + D[4] * x1 + D[5] * x2;
+                y2 += D[6] * x0 + D[7] * x1 + D[8] * x2;
+            }
+            if (A.fixed) {
+                if (A.fixed[3 * row]) y0 = x[3 * row];
+                if (A.fixed[3 * row + 1]) y1 = x[3 * row + 1];
+                if (A.fixed[3 * row + 2]) y2 = x[3 * row + 2];
+            }
             const double ri[3] = {b[3 * row] - y0, b[3 * row + 1] - y1, b[3 * row + 2] - y2};
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
@@ -371,8 +395,43 @@ __global__ void jacobi_kernel(SellView A, const VT* __restrict__ val, XT* __rest
         const uint32_t o = A.dvoff[n];
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-            const double d = o != 0xffffffffu ? (double)val[o + 32u * (4 * a)] : 0.0;
+            double d = A.diag64 ? A.diag64[9 * n + 4 * a] : (o != 0xffffffffu ? (double)val[o + 32u * (4 * a)] : 0.0);
+            if (A.fixed && A.fixed[3 * n + a]) d = 1.0;
             dinv[3 * n + a] = (XT)(d != 0.0 ? 1.0 / d : 1.0);
+        }
+    }
+}
+
+__global__ void diag_rowsum_kernel(SellView A, const float* __restrict__ val, double* __restrict__ D) {
+    const int64_t rows = (int64_t)A.n_slices * 32;
+    for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < rows;
+         row += (int64_t)gridDim.x * blockDim.x) {
+        if (row >= A.n_node) continue;
+        const int64_t s = row >> 5;
+        const int lane = (int)(row & 31);
+        const int64_t base = A.slice_base[s];
+        const int w = A.slice_width[s];
+        double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        const float* vp = val + 9 * base + lane;
+        for (int k = 0; k < w; ++k) {
+            const float* v = vp + 288 * (int64_t)k;
+#pragma unroll
+            for (int q = 0; q < 9; ++q) acc[q] += (double)v[32 * q];
+        }
+#pragma unroll
+        for (int q = 0; q < 9; ++q) D[9 * row + q] = -acc[q];
+    }
+}
+
+__global__ void export_fix_diag_kernel(const double* __restrict__ D, const int64_t* __restrict__ rowptr,
+                                       const int32_t* __restrict__ col, const int32_t* __restrict__ assy, int32_t n_free,
+                                       double* __restrict__ out) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n_free; r += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t dr = assy[r];
+        const int32_t n = dr / 3, a = dr % 3;
+        for (int64_t k = rowptr[r]; k < rowptr[r + 1]; ++k) {
+            const int32_t dc = assy[col[k]];
+            if (dc / 3 == n) out[k] = D[9 * (int64_t)n + 3 * a + dc % 3];
         }
     }
 }
@@ -458,6 +517,19 @@ template void residual_fp64<double>(const SellView&, const double*, const double
                                     uint32_t*, double*, cudaStream_t, int);
 template void residual_fp64<float>(const SellView&, const float*, const double*, const double*, double*, double*,
                                    uint32_t*, double*, cudaStream_t, int);
+
+void diag_from_offdiag(const SellView& A, const float* val, double* diag64, cudaStream_t s, int sm) {
+    diag_rowsum_kernel<<<stride_grid((int64_t)A.n_slices * 32, kThreads, sm), kThreads, 0, s>>>(A, val, diag64);
+    MPHY_CUDA(cudaGetLastError());
+}
+
+void export_fix_diagonal(const double* diag64, const int64_t* rowptr, const int32_t* col, const int32_t* assy,
+                         int32_t n_free, double* out, cudaStream_t s, int sm) {
+    if (n_free <= 0) return;
+    export_fix_diag_kernel<<<stride_grid(n_free, kThreads, sm), kThreads, 0, s>>>(diag64, rowptr, col, assy, n_free,
+                                                                                  out);
+    MPHY_CUDA(cudaGetLastError());
+}
 
 void dot_fp64(const double* a, const double* b, int64_t n, double* partials, uint32_t* counter, double* out_dev,
               cudaStream_t s, int sm) {
@@ -646,7 +718,7 @@ int IterativeRefinement<XT>::solve(const float* val, const double* b, double* x,
     MPHY_CUDA(cudaStreamSynchronize(s));
     launches += 1;
     const double bnorm = std::sqrt(bb);
-    int total = 0, k = 0, status = MPHY_OK;
+    int total = 0, k = 0, status = MPHY_OK, inner_status = MPHY_OK;
     double rel = bnorm > 0.0 ? 1.0 : 0.0;
     while (rel > rtol && k < max_outer && total < maxit) {
         to_inner(r64_.p, rin_.p, n_, gv, s);
@@ -654,6 +726,7 @@ int IterativeRefinement<XT>::solve(const float* val, const double* b, double* x,
         double dn = 0.0;
         const int st = inner_.solve(val, rin_.p, d_.p, inner_rtol > 0.0 ? inner_rtol : rtol, 0.0, 1e5, maxit - total,
                                     s, &it, &dn);
+        inner_status = st;
         launches += inner_.launches + 1;
         total += it;
         axpy_kernel<XT><<<gv, kThreads, 0, s>>>(x, d_.p, 1.0, n_);
@@ -669,7 +742,9 @@ int IterativeRefinement<XT>::solve(const float* val, const double* b, double* x,
             break;
         }
     }
-    if (status == MPHY_OK && rel > rtol) status = MPHY_ERR_NOT_CONVERGED;
+    // one sweep: the inner solve's KSP status decides (its stopping rule is PETSc's); more sweeps:
+    // the FP64 true residual does
+    if (status == MPHY_OK) status = max_outer <= 1 ? inner_status : (rel > rtol ? MPHY_ERR_NOT_CONVERGED : MPHY_OK);
     if (its) *its = total;
     if (sweeps) *sweeps = k;
     if (relres) *relres = rel;

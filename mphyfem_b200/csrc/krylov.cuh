@@ -31,6 +31,11 @@ struct SellView {
     const int32_t* slice_width;
     const int32_t* col;
     const uint32_t* dvoff;
+    // Null-space-preserving storage (mixed precision): when diag64 is set, the stored diagonal
+    // blocks are zero and block row n adds diag64[n] (FP64, [9]) times x_n; when fixed is set,
+    // prescribed DOFs are identity rows (the stored rows and columns are unmasked).
+    const double* diag64 = nullptr;
+    const uint8_t* fixed = nullptr;
 };
 
 // Factorised preconditioner M = G^T G: G lower block-triangular and G^T, both in SELL layout
@@ -115,6 +120,13 @@ class IterativeRefinement {
     DevBuf<XT> rin_, d_;
     DevBuf<uint32_t> counter_;
 };
+
+// D_n = -sum_{m != n} A_nm over the stored FP32 blocks (the stored diagonal blocks are zero):
+// the diagonal that makes the stored operator exactly translation invariant.
+void diag_from_offdiag(const SellView& A, const float* val, double* diag64, cudaStream_t s, int sm);
+// CSR export fix-up for that storage: entries of diagonal blocks come from diag64.
+void export_fix_diagonal(const double* diag64, const int64_t* rowptr, const int32_t* col, const int32_t* assy,
+                         int32_t n_free, double* out, cudaStream_t s, int sm);
 
 // small kernels of the solver surface
 template <typename VT>

@@ -226,16 +226,20 @@ def two_phase_inclusions(nx: int, ny: int, nz: int, seed: int = 23, vol_frac: fl
         centers.append(c)
         radii.append(r)
         vol += 4.0 / 3.0 * np.pi * r ** 3
-    cent = p.coords[p.conn].mean(axis=1)
-    inside = np.zeros(p.n_elem, dtype=bool)
-    C, R = np.asarray(centers), np.asarray(radii)
-    # bucket the spheres by cell to keep the centroid test linear in the element count
-    for c, r in zip(C, R):
-        lo, hi = c - r, c + r
-        m = np.all((cent >= lo) & (cent <= hi), axis=1)
-        idx = np.nonzero(m)[0]
-        if idx.size:
-            inside[idx[np.sum((cent[idx] - c) ** 2, axis=1) <= r * r]] = True
+    # element (i, j, k) of the structured grid has its centroid at ((i+.5)hx, (j+.5)hy, (k+.5)hz);
+    # test only the cells inside each sphere's bounding box
+    h = np.array([lx / nx, ly / ny, lz / nz])
+    dims = np.array([nx, ny, nz])
+    inside = np.zeros((nz, ny, nx), dtype=bool)
+    for c, r in zip(centers, radii):
+        lo = np.maximum(np.floor((c - r) / h - 0.5).astype(int), 0)
+        hi = np.minimum(np.ceil((c + r) / h - 0.5).astype(int), dims - 1)
+        ii = (np.arange(lo[0], hi[0] + 1) + 0.5) * h[0] - c[0]
+        jj = (np.arange(lo[1], hi[1] + 1) + 0.5) * h[1] - c[1]
+        kk = (np.arange(lo[2], hi[2] + 1) + 0.5) * h[2] - c[2]
+        d2 = kk[:, None, None] ** 2 + jj[None, :, None] ** 2 + ii[None, None, :] ** 2
+        inside[lo[2]:hi[2] + 1, lo[1]:hi[1] + 1, lo[0]:hi[0] + 1] |= d2 <= r * r
+    inside = inside.ravel()  # cells are numbered x-fastest, like the elements
     p.mat_id = inside.astype(np.int32)
     p.mats = np.stack([nh_material(1.0, kappa_over_mu), nh_material(mu_ratio, kappa_over_mu * mu_ratio)])
     p.newton_rtol = 1e-8
