@@ -226,7 +226,7 @@ def run_ours(args):
     prec = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED, "mixed32": _lib.PREC_MIXED_F32VEC}[args.precision]
     pc = {"jacobi": _lib.PC_JACOBI, "fsai": _lib.PC_FSAI}[args.pc]
     sol = api.SolverGpu(mesh, pat, rtol=args.rtol, max_it=args.max_it, precision=prec, inner_rtol=args.inner_rtol,
-                        max_outer=args.max_outer, pc_type=pc)
+                        max_outer=args.max_outer, pc_type=pc, coarse_aggregates=args.coarse)
     stream = torch.cuda.ExternalStream(sol.stream, device=f"cuda:{local}")
     disp = torch.zeros(prob.n_dof, dtype=torch.float64, device=f"cuda:{local}")
     fext = torch.tensor(prob.fnodal, dtype=torch.float64, device=f"cuda:{local}")
@@ -341,6 +341,7 @@ def main():
     ap.add_argument("--inner-rtol", dest="inner_rtol", type=float, default=0.0)
     ap.add_argument("--max-outer", dest="max_outer", type=int, default=1)
     ap.add_argument("--pc", default="jacobi", choices=["jacobi", "fsai"])
+    ap.add_argument("--coarse", type=int, default=0, help="aggregates of the two-level coarse correction (0: off)")
     ap.add_argument("--max-it", dest="max_it", type=int, default=20000)
     ap.add_argument("--ref-its", dest="ref_its", type=int, default=2411,
                     help="Krylov iterations per Newton iteration for --impl reference: the Jacobi-PCG count "

@@ -83,6 +83,9 @@ typedef struct mphy_solver_opts {
     int32_t max_outer;     /* MIXED*: refinement sweeps, each ending with the FP64 residual
                             * b - A x; stops early once ||b - A x|| <= rtol ||b|| (default 1) */
     int32_t chunk;         /* Krylov iterations per launched graph between host checks (0: auto) */
+    int32_t coarse_aggregates; /* > 0: add the two-level rigid-body coarse correction
+                                * M^{-1} = D^{-1} + Z (Z^T A Z)^{-1} Z^T over about this many
+                                * geometric aggregates (6 modes each) to MPHY_PC_JACOBI */
 } mphy_solver_opts;
 
 typedef struct mphy_newton_opts {
@@ -210,6 +213,10 @@ int mphy_solver_pc_set_blocks(mphy_solver* s, const float* blocks_dev);
 /* Exact block FSAI of the currently assembled operator; *n_fallback rows were not positive
  * definite and use the inverse square root of their diagonal. */
 int mphy_solver_pc_setup(mphy_solver* s, int32_t* n_fallback);
+/* Coarse space of the two-level correction: aggregate grid (boxes along x, y, z of the reference
+ * bounding box) and coarse size (6 modes per box). *setup_ms: time of the last E setup.
+ * No counterpart in the reference. */
+int mphy_solver_coarse_info(const mphy_solver* s, int32_t* grid3, int32_t* coarse_size, float* setup_ms);
 /* Solution increment scattered to node-major layout (femSolidmechanics2.cpp:1183-1186):
  * dx_dev[assyForSoln[i]] = soln[i], prescribed DOFs 0. */
 int mphy_solver_get_solution(mphy_solver* s, double* dx_dev);

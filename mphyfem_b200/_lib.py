@@ -41,7 +41,7 @@ class SolverOpts(C.Structure):
     _fields_ = [
         ("precision", C.c_int32), ("pc_type", C.c_int32), ("tangent", C.c_int32), ("max_it", C.c_int32),
         ("rtol", C.c_double), ("abstol", C.c_double), ("dtol", C.c_double), ("inner_rtol", C.c_double),
-        ("max_outer", C.c_int32), ("chunk", C.c_int32),
+        ("max_outer", C.c_int32), ("chunk", C.c_int32), ("coarse_aggregates", C.c_int32),
     ]
 
 
@@ -103,6 +103,7 @@ SIGNATURES = {
     "mphy_solver_pc_get_blocks": (C.c_int, [_vp, _vp]),
     "mphy_solver_pc_set_blocks": (C.c_int, [_vp, _vp]),
     "mphy_solver_pc_setup": (C.c_int, [_vp, _i32]),
+    "mphy_solver_coarse_info": (C.c_int, [_vp, _i32, _i32, C.POINTER(C.c_float)]),
     "mphy_solver_get_solution": (C.c_int, [_vp, _vp]),
     "mphy_solver_update_disp": (C.c_int, [_vp, _vp]),
     "mphy_solver_export": (C.c_int, [_vp, _d, _d, _d]),

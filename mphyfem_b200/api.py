@@ -211,6 +211,13 @@ class SolverGpu:
         b = blocks_dev.contiguous().to(torch.float32)
         L.check(self.lib.mphy_solver_pc_set_blocks(self.h, _ptr(b)))
 
+    def coarse_info(self):
+        g = (C.c_int32 * 3)()
+        k = C.c_int32()
+        ms = C.c_float()
+        L.check(self.lib.mphy_solver_coarse_info(self.h, g, C.byref(k), C.byref(ms)))
+        return {"grid": tuple(g), "coarse_size": k.value, "setup_ms": ms.value}
+
     def solution(self):
         torch = _torch()
         x = torch.empty(self.mesh.prob.n_dof, dtype=torch.float64, device="cuda")

@@ -12,6 +12,7 @@
 #include <new>
 
 #include "common.cuh"
+#include "coarse.cuh"
 #include "elem.cuh"
 #include "fsai.cuh"
 #include "krylov.cuh"
@@ -68,6 +69,8 @@ struct mphy_solver {
     IterativeRefinement<double> ir;       // MIXED
     IterativeRefinement<float> ir32;      // MIXED_F32VEC
     Fsai fsai;                            // MPHY_PC_FSAI*
+    CoarseSpace coarse;                   // coarse_aggregates > 0
+    bool use_coarse = false;
     bool use_fsai = false;
     double t_pc_ms = 0.0;                 // last preconditioner setup time
     int32_t last_sweeps = 0;
@@ -152,6 +155,13 @@ int solver_solve(mphy_solver* s, int32_t* its, double* fnorm) {
         cudaEventElapsedTime(&ms, s->ctx->ev0, s->ctx->ev1);
         s->t_pc_ms = ms;
         s->launches += s->fsai.launches;
+    }
+    if (s->use_coarse) {
+        // the coarse operator follows the assembled matrix
+        if (s->mixed) s->coarse.setup<float>(s->A, s->valf.p, nullptr, s->ctx->stream);
+        else s->coarse.setup<double>(s->A, s->val.p, nullptr, s->ctx->stream);
+        s->t_pc_ms = s->coarse.last_setup_ms;
+        s->launches += s->coarse.launches;
     }
     if (s->mixed) {
         // FP32 inner PCG inside an FP64 refinement loop; *fnorm is ||b - A x|| / ||b|| in FP64
@@ -333,6 +343,7 @@ int mphy_mesh_create(mphy_ctx* c, int32_t n_node, const double* coords, int32_t 
             m->mats.alloc(m4.size());
             m->mats.upload(m4.data(), m4.size(), s);
             m->fixed_host.assign(fixed, fixed + 3 * (size_t)n_node);
+            m->coords_host.assign(coords, coords + 3 * (size_t)n_node);
             m->fixed.alloc(3 * (size_t)n_node);
             m->fixed.upload(fixed, 3 * (size_t)n_node, s);
             MPHY_CUDA(cudaStreamSynchronize(s));
@@ -508,6 +519,16 @@ int mphy_solver_create(mphy_ctx* c, const mphy_mesh* m, const mphy_pattern* P, c
             if (o.precision == MPHY_PREC_MIXED) s->ir.init(s->A, c->sm_count, o.chunk);
             else if (o.precision == MPHY_PREC_MIXED_F32VEC) s->ir32.init(s->A, c->sm_count, o.chunk);
             else s->pcg.init(s->A, c->sm_count, o.chunk);
+            if (o.coarse_aggregates > 0) {
+                MPHY_REQUIRE(o.pc_type == MPHY_PC_JACOBI, MPHY_ERR_UNSUPPORTED,
+                             "the coarse correction combines with MPHY_PC_JACOBI");
+                s->use_coarse = true;
+                s->coarse.init(c, m, P, o.coarse_aggregates);
+                const CoarseView cv = s->coarse.view();
+                if (o.precision == MPHY_PREC_MIXED) s->ir.inner().set_coarse(cv);
+                else if (o.precision == MPHY_PREC_MIXED_F32VEC) s->ir32.inner().set_coarse(cv);
+                else s->pcg.set_coarse(cv);
+            }
             if (o.pc_type != MPHY_PC_JACOBI) {
                 s->use_fsai = true;
                 s->fsai.init(c, P, 16);
@@ -674,6 +695,19 @@ int mphy_solver_pc_setup(mphy_solver* s, int32_t* n_fallback) {
         if (n_fallback) *n_fallback = nf;
         return (int)MPHY_OK;
     });
+}
+
+int mphy_solver_coarse_info(const mphy_solver* s, int32_t* grid3, int32_t* k, float* setup_ms) {
+    if (!s) return MPHY_ERR_INVALID_ARG;
+    if (!s->use_coarse) {
+        set_error("the solver has no coarse correction");
+        return MPHY_ERR_STATE;
+    }
+    if (grid3)
+        for (int d = 0; d < 3; ++d) grid3[d] = s->coarse.grid()[d];
+    if (k) *k = s->coarse.coarse_size();
+    if (setup_ms) *setup_ms = s->coarse.last_setup_ms;
+    return MPHY_OK;
 }
 
 int mphy_solver_get_solution(mphy_solver* s, double* dx) {

@@ -1,0 +1,469 @@
+// coarse.cu -- rigid-body coarse space on geometric aggregates (setup side; the per-iteration
+// restriction, coarse GEMV and prolongation live in krylov.cu next to the CG state).
+//
+// Setup per operator:
+//   1. centroids of the current coordinates per aggregate and scaled offsets d_n = (x_n - c_a)/H;
+//   2. E = Z^T A Z: one CTA per aggregate walks its nodes' matrix rows and accumulates the 6x6
+//      blocks E[a][b] for its (at most 27) neighbour aggregates in shared memory -- every block
+//      of E is written by exactly one CTA, no atomics in global memory;
+//   3. E = L L^T by a right-looking blocked Cholesky (64x64 tiles, FP64), W = L^{-1} by blocked
+//      forward substitution, E^{-1} = W^T W, stored in FP32 for the per-iteration GEMV.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "coarse.cuh"
+
+namespace mphy {
+namespace {
+
+constexpr int T = 64;   // dense tile
+constexpr int TP = 65;  // padded shared-memory row
+
+// ---------------------------------------------------------------- modes
+__global__ void centroid_kernel(int32_t n_agg, const int64_t* __restrict__ agg_ptr, const int32_t* __restrict__ nodes,
+                                const double* __restrict__ X, const double* __restrict__ u, double* __restrict__ cent) {
+    __shared__ double sh[3][256];
+    for (int a = blockIdx.x; a < n_agg; a += gridDim.x) {
+        double s[3] = {0, 0, 0};
+        for (int64_t i = agg_ptr[a] + threadIdx.x; i < agg_ptr[a + 1]; i += blockDim.x) {
+            const int64_t n = nodes[i];
+            for (int d = 0; d < 3; ++d) s[d] += X[3 * n + d] + (u ? u[3 * n + d] : 0.0);
+        }
+        for (int d = 0; d < 3; ++d) sh[d][threadIdx.x] = s[d];
+        __syncthreads();
+        for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+            if ((int)threadIdx.x < o)
+                for (int d = 0; d < 3; ++d) sh[d][threadIdx.x] += sh[d][threadIdx.x + o];
+            __syncthreads();
+        }
+        const double cnt = (double)(agg_ptr[a + 1] - agg_ptr[a]);
+        if (threadIdx.x == 0)
+            for (int d = 0; d < 3; ++d) cent[3 * a + d] = cnt > 0 ? sh[d][0] / cnt : 0.0;
+        __syncthreads();
+    }
+}
+
+__global__ void offsets_kernel(int32_t n_node, const int32_t* __restrict__ agg, const double* __restrict__ X,
+                               const double* __restrict__ u, const double* __restrict__ cent, double inv_h,
+                               double* __restrict__ d) {
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < n_node; n += (int64_t)gridDim.x * blockDim.x) {
+        const int a = agg[n];
+        for (int k = 0; k < 3; ++k) d[3 * n + k] = (X[3 * n + k] + (u ? u[3 * n + k] : 0.0) - cent[3 * a + k]) * inv_h;
+    }
+}
+
+// Z_n (3 x 6) of node n: translations, then rotations about z, x, y; zero rows on prescribed DOFs
+__device__ __forceinline__ void node_modes(const double* d, const uint8_t* fixed, int64_t n, double Z[3][6]) {
+    const double dx = d[3 * n], dy = d[3 * n + 1], dz = d[3 * n + 2];
+    const double m[3][6] = {{1, 0, 0, -dy, 0, dz}, {0, 1, 0, dx, -dz, 0}, {0, 0, 1, 0, dy, -dx}};
+    for (int i = 0; i < 3; ++i) {
+        const bool fx = fixed[3 * n + i] != 0;
+        for (int j = 0; j < 6; ++j) Z[i][j] = fx ? 0.0 : m[i][j];
+    }
+}
+
+// ---------------------------------------------------------------- E = Z^T A Z
+template <typename VT>
+__global__ void __launch_bounds__(256) coarse_matrix_kernel(SellView A, const VT* __restrict__ aval, CoarseView cv,
+                                                            int ngx, int ngy, int ngz, double* __restrict__ E,
+                                                            int32_t* err) {
+    __shared__ double Eloc[27][36];
+    for (int a = blockIdx.x; a < cv.n_agg; a += gridDim.x) {
+        for (int i = threadIdx.x; i < 27 * 36; i += blockDim.x) (&Eloc[0][0])[i] = 0.0;
+        __syncthreads();
+        const int ax = a % ngx, ay = (a / ngx) % ngy, az = a / (ngx * ngy);
+        for (int64_t i = cv.agg_ptr[a] + threadIdx.x; i < cv.agg_ptr[a + 1]; i += blockDim.x) {
+            const int64_t n = cv.agg_nodes[i];
+            double Zn[3][6];
+            node_modes(cv.d, cv.fixed, n, Zn);
+            const int64_t s = n >> 5;
+            const int lane = (int)(n & 31);
+            const int64_t base = A.slice_base[s];
+            const int w = A.slice_width[s];
+            for (int k = 0; k <= w; ++k) {
+                double blk[9];
+                int64_t m;
+                if (k < w) {
+                    m = A.col[base + 32 * (int64_t)k + lane];
+                    const VT* v = aval + 9 * (base + 32 * (int64_t)k) + lane;
+                    bool any = false;
+                    for (int q = 0; q < 9; ++q) {
+                        blk[q] = (double)v[32 * q];
+                        any |= blk[q] != 0.0;
+                    }
+                    if (!any) continue;
+                } else {
+                    if (!A.diag64) break;  // the FP32 storage keeps the diagonal blocks apart
+                    m = n;
+                    for (int q = 0; q < 9; ++q) blk[q] = A.diag64[9 * n + q];
+                }
+                if (A.fixed) {  // the FP32 storage is unmasked: prescribed DOFs act as identity rows
+                    for (int q = 0; q < 9; ++q)
+                        if (A.fixed[3 * n + q / 3] || A.fixed[3 * m + q % 3]) blk[q] = 0.0;
+                }
+                const int b = cv.agg[m];
+                const int dx = b % ngx - ax, dy = (b / ngx) % ngy - ay, dz = b / (ngx * ngy) - az;
+                if (dx < -1 || dx > 1 || dy < -1 || dy > 1 || dz < -1 || dz > 1) {
+                    atomicExch(err, 1);
+                    continue;
+                }
+                const int slot = (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1);
+                double Zm[3][6];
+                node_modes(cv.d, cv.fixed, m, Zm);
+                double Tm[3][6];
+                for (int r = 0; r < 3; ++r)
+                    for (int j = 0; j < 6; ++j) Tm[r][j] = blk[3 * r] * Zm[0][j] + blk[3 * r + 1] * Zm[1][j] + blk[3 * r + 2] * Zm[2][j];
+                for (int i2 = 0; i2 < 6; ++i2)
+                    for (int j = 0; j < 6; ++j) {
+                        const double v = Zn[0][i2] * Tm[0][j] + Zn[1][i2] * Tm[1][j] + Zn[2][i2] * Tm[2][j];
+                        if (v != 0.0) atomicAdd(&Eloc[slot][6 * i2 + j], v);
+                    }
+            }
+        }
+        __syncthreads();
+        for (int t = threadIdx.x; t < 27 * 36; t += blockDim.x) {
+            const int slot = t / 36, q = t % 36;
+            const int bx = ax + slot % 3 - 1, by = ay + (slot / 3) % 3 - 1, bz = az + slot / 9 - 1;
+            if (bx < 0 || bx >= ngx || by < 0 || by >= ngy || bz < 0 || bz >= ngz) continue;
+            const int b = bx + ngx * (by + ngy * bz);
+            E[(int64_t)(6 * a + q / 6) * cv.kp + 6 * b + q % 6] = Eloc[slot][q];
+        }
+        __syncthreads();
+    }
+}
+
+// modes that vanish on the free DOFs (an aggregate of prescribed nodes) and the padding become
+// identity rows: their correction is zero
+__global__ void drop_null_modes(double* __restrict__ E, int kp, int k) {
+    __shared__ double mx;
+    if (threadIdx.x == 0) {
+        double m = 0.0;
+        for (int j = 0; j < k; ++j) m = fmax(m, fabs(E[(int64_t)j * kp + j]));
+        mx = m;
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < kp; j += blockDim.x) {
+        const bool drop = j >= k || !(E[(int64_t)j * kp + j] > 1e-13 * mx);
+        if (!drop) continue;
+        for (int i = 0; i < kp; ++i) {
+            E[(int64_t)j * kp + i] = 0.0;
+            E[(int64_t)i * kp + j] = 0.0;
+        }
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < kp; j += blockDim.x)
+        if (E[(int64_t)j * kp + j] == 0.0) E[(int64_t)j * kp + j] = 1.0;
+}
+
+// ---------------------------------------------------------------- dense Cholesky + inverse
+__device__ __forceinline__ void load_tile(double (*S)[TP], const double* M, int kp, int ti, int tj) {
+    for (int t = threadIdx.x; t < T * T; t += blockDim.x) S[t / T][t % T] = M[(int64_t)(ti * T + t / T) * kp + tj * T + t % T];
+}
+__device__ __forceinline__ void store_tile(const double (*S)[TP], double* M, int kp, int ti, int tj) {
+    for (int t = threadIdx.x; t < T * T; t += blockDim.x) M[(int64_t)(ti * T + t / T) * kp + tj * T + t % T] = S[t / T][t % T];
+}
+
+// factor the diagonal tile (j, j) in place (lower triangle; upper zeroed)
+__global__ void __launch_bounds__(256) potrf_tile(double* E, int kp, int j, int32_t* err) {
+    __shared__ double S[T][TP];
+    load_tile(S, E, kp, j, j);
+    __syncthreads();
+    for (int c = 0; c < T; ++c) {
+        double p = S[c][c];
+        if (!(p > 0.0)) {
+            if (threadIdx.x == 0) atomicExch(err, 2);
+            p = 1e-300;
+        }
+        const double l = sqrt(p);
+        __syncthreads();
+        if (threadIdx.x == 0) S[c][c] = l;
+        for (int i = c + 1 + threadIdx.x; i < T; i += blockDim.x) S[i][c] /= l;
+        __syncthreads();
+        const int rem = T - c - 1;
+        for (int t = threadIdx.x; t < rem * rem; t += blockDim.x) {
+            const int i = c + 1 + t / rem, q = c + 1 + t % rem;
+            if (q <= i) S[i][q] -= S[i][c] * S[q][c];
+        }
+        __syncthreads();
+    }
+    for (int t = threadIdx.x; t < T * T; t += blockDim.x)
+        if (t % T > t / T) S[t / T][t % T] = 0.0;
+    __syncthreads();
+    store_tile(S, E, kp, j, j);
+}
+
+// tiles below the diagonal: L_ij = A_ij L_jj^{-T}
+__global__ void __launch_bounds__(256) trsm_tiles(double* E, int kp, int j) {
+    extern __shared__ double sm[];
+    double (*L)[TP] = reinterpret_cast<double (*)[TP]>(sm);
+    double (*X)[TP] = reinterpret_cast<double (*)[TP]>(sm + T * TP);
+    const int i = j + 1 + blockIdx.x;
+    load_tile(L, E, kp, j, j);
+    load_tile(X, E, kp, i, j);
+    __syncthreads();
+    if (threadIdx.x < T) {
+        const int r = threadIdx.x;
+        for (int c = 0; c < T; ++c) {
+            double s = X[r][c];
+            for (int t = 0; t < c; ++t) s -= X[r][t] * L[c][t];
+            X[r][c] = s / L[c][c];
+        }
+    }
+    __syncthreads();
+    store_tile(X, E, kp, i, j);
+}
+
+// C (tile ci, cj of M) += alpha * sum_t A[r][t] * B[c][t]  with A, B 64x64 tiles in shared memory
+__device__ __forceinline__ void tile_abt(const double (*A)[TP], const double (*B)[TP], double acc[4][4]) {
+    const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;
+    for (int t = 0; t < T; ++t) {
+        double a[4], b[4];
+        for (int q = 0; q < 4; ++q) {
+            a[q] = A[ty + 16 * q][t];
+            b[q] = B[tx + 16 * q][t];
+        }
+        for (int q = 0; q < 4; ++q)
+            for (int r = 0; r < 4; ++r) acc[q][r] += a[q] * b[r];
+    }
+}
+
+// trailing update A_ik -= L_ij L_kj^T for j < k <= i
+__global__ void __launch_bounds__(256) syrk_tiles(double* E, int kp, int j) {
+    extern __shared__ double sm[];
+    double (*Li)[TP] = reinterpret_cast<double (*)[TP]>(sm);
+    double (*Lk)[TP] = reinterpret_cast<double (*)[TP]>(sm + T * TP);
+    const int idx = blockIdx.x;
+    const int ii = (int)((sqrt(8.0 * idx + 1.0) - 1.0) / 2.0);
+    int a = ii, b = idx - ii * (ii + 1) / 2;
+    if (b > a) { ++a; b = idx - a * (a + 1) / 2; }  // guard the float square root
+    if (b < 0) { --a; b = idx - a * (a + 1) / 2; }
+    const int i = j + 1 + a, k = j + 1 + b;
+    load_tile(Li, E, kp, i, j);
+    load_tile(Lk, E, kp, k, j);
+    __syncthreads();
+    double acc[4][4] = {{0}};
+    tile_abt(Li, Lk, acc);
+    const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;
+    for (int q = 0; q < 4; ++q)
+        for (int r = 0; r < 4; ++r) E[(int64_t)(i * T + ty + 16 * q) * kp + k * T + tx + 16 * r] -= acc[q][r];
+}
+
+// W_ii = L_ii^{-1}
+__global__ void __launch_bounds__(256) trtri_tile(const double* E, double* W, int kp, int i) {
+    extern __shared__ double sm[];
+    double (*L)[TP] = reinterpret_cast<double (*)[TP]>(sm);
+    double (*X)[TP] = reinterpret_cast<double (*)[TP]>(sm + T * TP);
+    load_tile(L, E, kp, i, i);
+    __syncthreads();
+    if (threadIdx.x < T) {
+        const int c = threadIdx.x;  // column c of the inverse: L x = e_c
+        for (int r = 0; r < T; ++r) {
+            double s = r == c ? 1.0 : 0.0;
+            for (int t = c; t < r; ++t) s -= L[r][t] * X[t][c];
+            X[r][c] = r < c ? 0.0 : s / L[r][r];
+        }
+    }
+    __syncthreads();
+    store_tile(X, W, kp, i, i);
+}
+
+// W_ij = -W_ii sum_{k=j}^{i-1} L_ik W_kj   (j < i)
+__global__ void __launch_bounds__(256) trtri_row(const double* E, double* W, int kp, int i) {
+    extern __shared__ double sm[];
+    double (*A)[TP] = reinterpret_cast<double (*)[TP]>(sm);
+    double (*B)[TP] = reinterpret_cast<double (*)[TP]>(sm + T * TP);
+    const int j = blockIdx.x;
+    const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;
+    double acc[4][4] = {{0}};
+    for (int k = j; k < i; ++k) {
+        load_tile(A, E, kp, i, k);  // L_ik
+        // B = W_kj^T so that tile_abt gives L_ik W_kj
+        for (int t = threadIdx.x; t < T * T; t += blockDim.x) B[t % T][t / T] = W[(int64_t)(k * T + t / T) * kp + j * T + t % T];
+        __syncthreads();
+        tile_abt(A, B, acc);
+        __syncthreads();
+    }
+    // S -> shared, then W_ij = -W_ii S
+    for (int q = 0; q < 4; ++q)
+        for (int r = 0; r < 4; ++r) B[tx + 16 * r][ty + 16 * q] = acc[q][r];  // B = S^T
+    load_tile(A, W, kp, i, i);
+    __syncthreads();
+    double o[4][4] = {{0}};
+    tile_abt(A, B, o);
+    for (int q = 0; q < 4; ++q)
+        for (int r = 0; r < 4; ++r) W[(int64_t)(i * T + ty + 16 * q) * kp + j * T + tx + 16 * r] = -o[q][r];
+}
+
+// E^{-1} = W^T W (tile (i, j) = sum_{k >= max(i,j)} W_ki^T W_kj), stored FP32
+__global__ void __launch_bounds__(256) inverse_tiles(const double* W, float* einv, int kp, int nb) {
+    extern __shared__ double sm[];
+    double (*A)[TP] = reinterpret_cast<double (*)[TP]>(sm);
+    double (*B)[TP] = reinterpret_cast<double (*)[TP]>(sm + T * TP);
+    const int i = blockIdx.x / nb, j = blockIdx.x % nb;
+    const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;
+    double acc[4][4] = {{0}};
+    for (int k = max(i, j); k < nb; ++k) {
+        // A = W_ki^T, B = W_kj^T: tile_abt gives sum_t W_ki[t][r] W_kj[t][c]
+        for (int t = threadIdx.x; t < T * T; t += blockDim.x) {
+            A[t % T][t / T] = W[(int64_t)(k * T + t / T) * kp + i * T + t % T];
+            B[t % T][t / T] = W[(int64_t)(k * T + t / T) * kp + j * T + t % T];
+        }
+        __syncthreads();
+        tile_abt(A, B, acc);
+        __syncthreads();
+    }
+    for (int q = 0; q < 4; ++q)
+        for (int r = 0; r < 4; ++r) einv[(int64_t)(i * T + ty + 16 * q) * kp + j * T + tx + 16 * r] = (float)acc[q][r];
+}
+
+}  // namespace
+
+void CoarseSpace::init(mphy_ctx* ctx, const mphy_mesh* mesh, const mphy_pattern* pat, int target) {
+    ctx_ = ctx;
+    mesh_ = mesh;
+    pat_ = pat;
+    const int32_t nn = mesh->n_node;
+    const std::vector<double>& X = mesh->coords_host;
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int32_t n = 0; n < nn; ++n)
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = std::min(lo[d], X[3 * n + d]);
+            hi[d] = std::max(hi[d], X[3 * n + d]);
+        }
+    double L[3], vol = 1.0;
+    for (int d = 0; d < 3; ++d) {
+        L[d] = std::max(hi[d] - lo[d], 1e-30);
+        vol *= L[d];
+    }
+    // boxes as close to cubes as the bounding box allows, never thinner than ~2 elements
+    const double h = std::cbrt(vol / std::max(target, 1));
+    const double helem = std::cbrt(vol / std::max(mesh->n_elem, 1)) * 2.0;
+    for (int d = 0; d < 3; ++d) {
+        int g = (int)std::lround(L[d] / h);
+        g = std::max(1, std::min(g, (int)(L[d] / helem)));
+        ng_[d] = std::max(g, 1);
+    }
+    n_agg_ = ng_[0] * ng_[1] * ng_[2];
+    kp_ = ((6 * n_agg_ + T - 1) / T) * T;
+    MPHY_REQUIRE(kp_ <= 16384, MPHY_ERR_UNSUPPORTED, "coarse space larger than 16384");
+    std::vector<int32_t> agg(nn), cnt(n_agg_, 0);
+    for (int32_t n = 0; n < nn; ++n) {
+        int c[3];
+        for (int d = 0; d < 3; ++d) c[d] = std::min(ng_[d] - 1, (int)((X[3 * n + d] - lo[d]) / L[d] * ng_[d]));
+        agg[n] = c[0] + ng_[0] * (c[1] + ng_[1] * c[2]);
+        ++cnt[agg[n]];
+    }
+    std::vector<int64_t> ptr(n_agg_ + 1, 0);
+    for (int a = 0; a < n_agg_; ++a) ptr[a + 1] = ptr[a] + cnt[a];
+    std::vector<int32_t> nodes(nn);
+    std::vector<int64_t> cur(ptr.begin(), ptr.end() - 1);
+    for (int32_t n = 0; n < nn; ++n) nodes[cur[agg[n]]++] = n;
+    cudaStream_t s = ctx->stream;
+    agg_.alloc(nn);
+    agg_.upload(agg.data(), nn, s);
+    agg_ptr_.alloc(n_agg_ + 1);
+    agg_ptr_.upload(ptr.data(), n_agg_ + 1, s);
+    agg_nodes_.alloc(nn);
+    agg_nodes_.upload(nodes.data(), nn, s);
+    d_.alloc(3 * (size_t)nn);
+    cent_.alloc(3 * (size_t)n_agg_);
+    E_.alloc((size_t)kp_ * kp_);
+    W_.alloc((size_t)kp_ * kp_);
+    einv_.alloc((size_t)kp_ * kp_);
+    w_.alloc(kp_);
+    c_.alloc(kp_);
+    err_.alloc(1);
+    MPHY_CUDA(cudaMemsetAsync(w_.p, 0, w_.bytes(), s));
+    MPHY_CUDA(cudaMemsetAsync(c_.p, 0, c_.bytes(), s));
+    MPHY_CUDA(cudaStreamSynchronize(s));
+}
+
+template <typename VT>
+void CoarseSpace::setup(const SellView& A, const VT* aval, const double* disp, cudaStream_t s) {
+    MPHY_CUDA(cudaEventRecord(ctx_->ev0, s));
+    const int sm = ctx_->sm_count;
+    launches = 0;
+    centroid_kernel<<<std::min(n_agg_, sm * 8), 256, 0, s>>>(n_agg_, agg_ptr_.p, agg_nodes_.p, mesh_->coords.p, disp,
+                                                             cent_.p);
+    double boxd = 0.0;  // box diagonal of the reference grid scales the rotation modes to O(1)
+    {
+        const std::vector<double>& X = mesh_->coords_host;
+        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+        for (size_t n = 0; n < X.size() / 3; ++n)
+            for (int d = 0; d < 3; ++d) {
+                lo[d] = std::min(lo[d], X[3 * n + d]);
+                hi[d] = std::max(hi[d], X[3 * n + d]);
+            }
+        for (int d = 0; d < 3; ++d) boxd += std::pow((hi[d] - lo[d]) / ng_[d], 2);
+        boxd = std::sqrt(std::max(boxd, 1e-300));
+    }
+    offsets_kernel<<<stride_grid(mesh_->n_node, 256, sm), 256, 0, s>>>(mesh_->n_node, agg_.p, mesh_->coords.p, disp,
+                                                                      cent_.p, 1.0 / boxd, d_.p);
+    MPHY_CUDA(cudaMemsetAsync(E_.p, 0, E_.bytes(), s));
+    MPHY_CUDA(cudaMemsetAsync(W_.p, 0, W_.bytes(), s));
+    MPHY_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(int32_t), s));
+    CoarseView cv = view();
+    coarse_matrix_kernel<VT><<<std::min(n_agg_, sm * 8), 256, 0, s>>>(A, aval, cv, ng_[0], ng_[1], ng_[2], E_.p,
+                                                                       err_.p);
+    drop_null_modes<<<1, 1024, 0, s>>>(E_.p, kp_, 6 * n_agg_);
+    MPHY_CUDA(cudaGetLastError());
+    launches += 4;
+    const int nb = kp_ / T;
+    const size_t sm2 = 2 * (size_t)T * TP * sizeof(double);
+    static bool attr = false;
+    if (!attr) {
+        MPHY_CUDA(cudaFuncSetAttribute(syrk_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
+        MPHY_CUDA(cudaFuncSetAttribute(trsm_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
+        MPHY_CUDA(cudaFuncSetAttribute(trtri_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
+        MPHY_CUDA(cudaFuncSetAttribute(trtri_row, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
+        MPHY_CUDA(cudaFuncSetAttribute(inverse_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
+        attr = true;
+    }
+    for (int j = 0; j < nb; ++j) {
+        potrf_tile<<<1, 256, 0, s>>>(E_.p, kp_, j, err_.p);
+        const int m = nb - j - 1;
+        if (m > 0) {
+            trsm_tiles<<<m, 256, sm2, s>>>(E_.p, kp_, j);
+            syrk_tiles<<<m * (m + 1) / 2, 256, sm2, s>>>(E_.p, kp_, j);
+            launches += 2;
+        }
+        launches += 1;
+    }
+    for (int i = 0; i < nb; ++i) {
+        trtri_tile<<<1, 256, sm2, s>>>(E_.p, W_.p, kp_, i);
+        if (i > 0) trtri_row<<<i, 256, sm2, s>>>(E_.p, W_.p, kp_, i);
+        launches += i > 0 ? 2 : 1;
+    }
+    inverse_tiles<<<nb * nb, 256, sm2, s>>>(W_.p, einv_.p, kp_, nb);
+    launches += 1;
+    MPHY_CUDA(cudaGetLastError());
+    MPHY_CUDA(cudaEventRecord(ctx_->ev1, s));
+    int32_t h = 0;
+    MPHY_CUDA(cudaMemcpyAsync(&h, err_.p, sizeof(h), cudaMemcpyDeviceToHost, s));
+    MPHY_CUDA(cudaStreamSynchronize(s));
+    cudaEventElapsedTime(&last_setup_ms, ctx_->ev0, ctx_->ev1);
+    MPHY_REQUIRE(h != 1, MPHY_ERR_UNSUPPORTED, "coarse space: an element spans more than two aggregates");
+    MPHY_REQUIRE(h != 2, MPHY_ERR_INDEFINITE, "coarse space: Z^T A Z is not positive definite");
+}
+
+template void CoarseSpace::setup<double>(const SellView&, const double*, const double*, cudaStream_t);
+template void CoarseSpace::setup<float>(const SellView&, const float*, const double*, cudaStream_t);
+
+CoarseView CoarseSpace::view() const {
+    CoarseView v;
+    v.n_agg = n_agg_;
+    v.k = 6 * n_agg_;
+    v.kp = kp_;
+    v.agg = agg_.p;
+    v.agg_ptr = agg_ptr_.p;
+    v.agg_nodes = agg_nodes_.p;
+    v.d = d_.p;
+    v.fixed = mesh_->fixed.p;
+    v.einv = einv_.p;
+    v.w = w_.p;
+    v.c = c_.p;
+    return v;
+}
+
+}  // namespace mphy

@@ -1,0 +1,44 @@
+// coarse.cuh -- two-level preconditioner: a rigid-body coarse space on geometric aggregates.
+//
+//   M^{-1} r = D^{-1} r + Z E^{-1} Z^T r,   E = Z^T A Z,
+// Z holding, for every box of a regular grid of boxes over the mesh, the six rigid-body modes
+// (three translations, three rotations about the box centroid) of its nodes, zero on prescribed
+// DOFs. M^{-1} is symmetric positive definite, so CG keeps its guarantees; the coarse term takes
+// care of the global, smooth modes (beam bending) that no local preconditioner reaches.
+#pragma once
+#include "common.cuh"
+#include "coarse_view.cuh"
+#include "krylov.cuh"
+
+namespace mphy {
+
+class CoarseSpace {
+  public:
+    // Aggregates: a grid of boxes over the bounding box of the reference coordinates with about
+    // target_aggregates boxes, as close to cubes as the box allows.
+    void init(mphy_ctx* ctx, const mphy_mesh* mesh, const mphy_pattern* pat, int target_aggregates);
+    // Modes from the current coordinates X + disp (disp may be null), E = Z^T A Z, its Cholesky
+    // factor and inverse (FP64), stored in FP32.
+    template <typename VT>
+    void setup(const SellView& A, const VT* aval, const double* disp, cudaStream_t s);
+    CoarseView view() const;
+    int n_agg() const { return n_agg_; }
+    int coarse_size() const { return 6 * n_agg_; }
+    const int* grid() const { return ng_; }
+    int64_t launches = 0;
+    float last_setup_ms = 0.f;
+
+  private:
+    mphy_ctx* ctx_ = nullptr;
+    const mphy_mesh* mesh_ = nullptr;
+    const mphy_pattern* pat_ = nullptr;
+    int ng_[3] = {1, 1, 1};
+    int n_agg_ = 0, kp_ = 0;
+    DevBuf<int32_t> agg_, agg_nodes_, err_;
+    DevBuf<int64_t> agg_ptr_;
+    DevBuf<double> d_, cent_, E_, W_, w_, c_;
+    DevBuf<float> einv_;
+    DevBuf<uint8_t> drop_;
+};
+
+}  // namespace mphy

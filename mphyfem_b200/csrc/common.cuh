@@ -95,6 +95,7 @@ struct mphy_mesh {
     mphy::DevBuf<double> mats;     // [n_mat][4] = mu, Kinv, Utype, 0
     mphy::DevBuf<uint8_t> fixed;   // [n_node*3]
     std::vector<uint8_t> fixed_host;
+    std::vector<double> coords_host;  // reference coordinates (aggregation of the coarse space)
 };
 
 // Node-block sparsity. Block rows are nodes; a block row holds the nodes that share an element

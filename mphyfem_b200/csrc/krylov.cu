@@ -14,6 +14,7 @@
 // ticket, no waiting) adds the partials in a fixed order and advances the shared scalar state.
 // Chunks of iterations are replayed from a captured CUDA graph; kernels return immediately once
 // the state says done. FP32 vectors keep every reduction in FP64.
+#include <algorithm>
 #include <cmath>
 
 #include "krylov.cuh"
@@ -388,6 +389,90 @@ __global__ void __launch_bounds__(kThreads) pcg_init_kernel(int64_t n, const XT*
     }
 }
 
+// ---------------------------------------------------------------- two-level (coarse) apply
+// w = Z^T r per aggregate (one CTA per aggregate, fixed-order reduction)
+template <typename XT>
+__global__ void __launch_bounds__(kThreads) coarse_restrict_kernel(CoarseView cv, const XT* __restrict__ r,
+                                                                   const PcgState* st) {
+    __shared__ double sh[32];
+    if (st && st->done) return;
+    for (int a = blockIdx.x; a < cv.n_agg; a += gridDim.x) {
+        double w[6] = {0, 0, 0, 0, 0, 0};
+        for (int64_t i = cv.agg_ptr[a] + threadIdx.x; i < cv.agg_ptr[a + 1]; i += blockDim.x) {
+            const int64_t n = cv.agg_nodes[i];
+            const double rx = cv.fixed[3 * n] ? 0.0 : (double)r[3 * n];
+            const double ry = cv.fixed[3 * n + 1] ? 0.0 : (double)r[3 * n + 1];
+            const double rz = cv.fixed[3 * n + 2] ? 0.0 : (double)r[3 * n + 2];
+            const double dx = cv.d[3 * n], dy = cv.d[3 * n + 1], dz = cv.d[3 * n + 2];
+            w[0] += rx;
+            w[1] += ry;
+            w[2] += rz;
+            w[3] += -dy * rx + dx * ry;
+            w[4] += -dz * ry + dy * rz;
+            w[5] += dz * rx - dx * rz;
+        }
+        for (int j = 0; j < 6; ++j) {
+            const double t = block_sum(w[j], sh);
+            if (threadIdx.x == 0) cv.w[6 * a + j] = t;
+        }
+    }
+}
+
+// c = E^{-1} w: one warp per row of the FP32 inverse, FP64 accumulation
+__global__ void __launch_bounds__(kThreads) coarse_gemv_kernel(CoarseView cv, const PcgState* st) {
+    if (st && st->done) return;
+    const int lane = threadIdx.x & 31;
+    for (int64_t row = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; row < cv.kp;
+         row += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        const float* e = cv.einv + row * cv.kp;
+        double acc = 0.0;
+        for (int col = lane; col < cv.kp; col += 32) acc += (double)e[col] * cv.w[col];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) cv.c[row] = acc;
+    }
+}
+
+// z = D^{-1} r + Z c with the fused (r, z), (z, z); INIT also sets p = z and the initial state
+template <typename XT, bool INIT>
+__global__ void __launch_bounds__(kThreads) coarse_final_kernel(int32_t n_node, CoarseView cv, const XT* __restrict__ r,
+                                                                XT* __restrict__ z, XT* __restrict__ p,
+                                                                const XT* __restrict__ dinv,
+                                                                double* __restrict__ part_rz,
+                                                                double* __restrict__ part_zz, PcgState* st,
+                                                                double rtol, double abstol, double dtol, int maxit) {
+    __shared__ double sh[32];
+    if (!INIT && st->done) return;
+    double a1 = 0.0, a2 = 0.0;
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < n_node; n += (int64_t)gridDim.x * blockDim.x) {
+        const double* c = cv.c + 6 * (int64_t)cv.agg[n];
+        const double dx = cv.d[3 * n], dy = cv.d[3 * n + 1], dz = cv.d[3 * n + 2];
+        const double zc[3] = {c[0] - dy * c[3] + dz * c[5], c[1] + dx * c[3] - dz * c[4], c[2] + dy * c[4] - dx * c[5]};
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const int64_t i = 3 * n + a;
+            const XT ri = r[i];
+            const XT zi = (XT)((double)dinv[i] * (double)ri + (cv.fixed[i] ? 0.0 : zc[a]));
+            z[i] = zi;
+            if (INIT) p[i] = zi;
+            a1 += (double)ri * (double)zi;
+            a2 += (double)zi * (double)zi;
+        }
+    }
+    a1 = block_sum(a1, sh);
+    if (threadIdx.x == 0) part_rz[blockIdx.x] = a1;
+    a2 = block_sum(a2, sh);
+    if (threadIdx.x == 0) part_zz[blockIdx.x] = a2;
+    if (!arrive_last(&st->counter)) return;
+    const double rz = reduce_partials(part_rz, gridDim.x, sh);
+    const double zz = reduce_partials(part_zz, gridDim.x, sh);
+    if (threadIdx.x == 0) {
+        st->counter = 0;
+        if (INIT) finish_init(st, rz, zz, rtol, abstol, dtol, maxit);
+        else finish_iter(st, rz, zz);
+    }
+}
+
 // PCJACOBI: inverse diagonal, a zero diagonal entry (or a node without blocks) gives 1
 template <typename VT, typename XT>
 __global__ void jacobi_kernel(SellView A, const VT* __restrict__ val, XT* __restrict__ dinv) {
@@ -605,6 +690,14 @@ void Pcg<VT, XT>::record_iterations(const VT* val, XT* x, cudaStream_t s, int n_
         if (kind_ == PcKind::Jacobi) {
             pcg_update_kernel<XT, true><<<gv, kThreads, 0, s>>>(n_, x, r_.p, z_.p, p_.p, q_.p, dinv_.p, partials_.p,
                                                                  partials2_.p, st_.p);
+        } else if (kind_ == PcKind::JacobiCoarse) {
+            pcg_update_kernel<XT, false><<<gv, kThreads, 0, s>>>(n_, x, r_.p, z_.p, p_.p, q_.p, nullptr, nullptr,
+                                                                  nullptr, st_.p);
+            coarse_restrict_kernel<XT><<<std::min(coarse_.n_agg, sm_ * 8), kThreads, 0, s>>>(coarse_, r_.p, st_.p);
+            coarse_gemv_kernel<<<stride_grid((int64_t)coarse_.kp * 32, kThreads, sm_), kThreads, 0, s>>>(coarse_,
+                                                                                                          st_.p);
+            coarse_final_kernel<XT, false><<<stride_grid(A_.n_node, kThreads, sm_), kThreads, 0, s>>>(
+                A_.n_node, coarse_, r_.p, z_.p, p_.p, dinv_.p, partials_.p, partials2_.p, st_.p, 0, 0, 0, 0);
         } else {
             pcg_update_kernel<XT, false><<<gv, kThreads, 0, s>>>(n_, x, r_.p, z_.p, p_.p, q_.p, nullptr, nullptr,
                                                                   nullptr, st_.p);
@@ -627,6 +720,16 @@ int Pcg<VT, XT>::solve(const VT* val, const XT* b, XT* x, double rtol, double ab
         pcg_init_kernel<XT, true><<<gv, kThreads, 0, s>>>(n_, b, x, r_.p, z_.p, p_.p, dinv_.p, partials_.p,
                                                            partials2_.p, st_.p, rtol, abstol, dtol, maxit);
         launches += 2;
+    } else if (kind_ == PcKind::JacobiCoarse) {
+        jacobi_kernel<VT, XT><<<stride_grid(A_.n_node, kThreads, sm_), kThreads, 0, s>>>(A_, val, dinv_.p);
+        pcg_init_kernel<XT, false><<<gv, kThreads, 0, s>>>(n_, b, x, r_.p, z_.p, p_.p, nullptr, nullptr, nullptr,
+                                                            st_.p, rtol, abstol, dtol, maxit);
+        coarse_restrict_kernel<XT><<<std::min(coarse_.n_agg, sm_ * 8), kThreads, 0, s>>>(coarse_, r_.p, nullptr);
+        coarse_gemv_kernel<<<stride_grid((int64_t)coarse_.kp * 32, kThreads, sm_), kThreads, 0, s>>>(coarse_, nullptr);
+        coarse_final_kernel<XT, true><<<stride_grid(A_.n_node, kThreads, sm_), kThreads, 0, s>>>(
+            A_.n_node, coarse_, r_.p, z_.p, p_.p, dinv_.p, partials_.p, partials2_.p, st_.p, rtol, abstol, dtol,
+            maxit);
+        launches += 5;
     } else {
         pcg_init_kernel<XT, false><<<gv, kThreads, 0, s>>>(n_, b, x, r_.p, z_.p, p_.p, nullptr, nullptr, nullptr,
                                                             st_.p, rtol, abstol, dtol, maxit);
@@ -655,7 +758,7 @@ int Pcg<VT, XT>::solve(const VT* val, const XT* b, XT* x, double rtol, double ab
         graph_stream_ = s;
         graph_kind_ = kind_;
     }
-    const int per_iter = kind_ == PcKind::Jacobi ? 3 : 5;
+    const int per_iter = kind_ == PcKind::Jacobi ? 3 : (kind_ == PcKind::Factor ? 5 : 6);
     PcgState h{};
     // every replay advances at most chunk_ iterations; the device stops at maxit
     const int64_t max_replays = (int64_t)(maxit > 0 ? maxit : 0) / chunk_ + 2;

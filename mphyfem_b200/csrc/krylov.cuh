@@ -3,6 +3,8 @@
 #pragma once
 #include "common.cuh"
 
+#include "coarse_view.cuh"
+
 namespace mphy {
 
 // Device-side CG state. Written only by the last CTA of a kernel (after every CTA has
@@ -63,7 +65,7 @@ void residual_fp64(const SellView& A, const VT* val, const double* x, const doub
 void dot_fp64(const double* a, const double* b, int64_t n, double* partials, uint32_t* counter, double* out_dev,
               cudaStream_t s, int sm);
 
-enum class PcKind { Jacobi, Factor };
+enum class PcKind { Jacobi, Factor, JacobiCoarse };
 
 // Preconditioned CG, VT = matrix values, XT = vector precision (double, or float with FP64
 // reductions). solve() runs from x = 0 on b (XT), PETSc KSPCG semantics.
@@ -73,6 +75,7 @@ class Pcg {
     void init(const SellView& A, int sm_count, int chunk);
     void set_factor(const FactorView<float>& f) { factor_ = f; kind_ = PcKind::Factor; }
     void set_jacobi() { kind_ = PcKind::Jacobi; }
+    void set_coarse(const CoarseView& c) { coarse_ = c; kind_ = PcKind::JacobiCoarse; }
     int solve(const VT* val, const XT* b, XT* x, double rtol, double abstol, double dtol, int maxit, cudaStream_t s,
               int32_t* its, double* final_norm);
     ~Pcg();
@@ -83,6 +86,7 @@ class Pcg {
     SellView A_{};
     PcKind kind_ = PcKind::Jacobi;
     FactorView<float> factor_{};
+    CoarseView coarse_{};
     int sm_ = 148, chunk_ = 32;
     int64_t n_ = 0;
     DevBuf<XT> r_, z_, p_, q_, t_, dinv_;
