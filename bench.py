@@ -29,7 +29,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 LAMBDA = 0.2
-METRIC = "Newton iters/s (FP64 assembly + Jacobi-PCG to rtol, hex8 Neo-Hookean cantilever)"
+METRIC = "Newton iters/s (hex8 Neo-Hookean cantilever 256x64x64, 3.26M DOFs, PCG to rtol 1e-8)"
 
 
 def _peaks():
@@ -52,7 +52,7 @@ def _workload(name: str):
 
 def _config(prob, rtol):
     return {
-        "workload": f"{prob.name}: one Newton iteration (assembly + loads + norm + Jacobi-PCG rtol {rtol:g} "
+        "workload": f"{prob.name}: one Newton iteration (assembly + loads + norm + PCG to rtol {rtol:g} "
                     f"+ update), lambda={LAMBDA}, u=0",
         "n_elem": prob.n_elem, "n_node": prob.n_node, "n_dof": prob.n_dof, "n_free": prob.n_free,
         "element": ("hex8, 2x2x2 Gauss, compressible Neo-Hookean mu=1 kappa=10 (Utype 3)" if prob.mats.shape[0] == 1
@@ -203,6 +203,36 @@ def run_reference(args):
 
 
 # ------------------------------------------------------------------------------------- GPU side
+def _method_name(args):
+    parts = [{"fp64": "FP64", "mixed": "mixed FP32/FP64", "mixed32": "mixed FP32 vectors"}[args.precision],
+             {"jacobi": "Jacobi", "fsai": "FSAI"}[args.pc]]
+    if args.coarse > 0:
+        parts.append(f"+ rigid-body coarse space ({args.coarse} aggregates)")
+    return " ".join(parts) + "-PCG"
+
+
+def _make_solver(api, _lib, mesh, pat, args, precision, pc, coarse):
+    return api.SolverGpu(mesh, pat, rtol=args.rtol, max_it=args.max_it,
+                         precision={"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED,
+                                    "mixed32": _lib.PREC_MIXED_F32VEC}[precision],
+                         pc_type={"jacobi": _lib.PC_JACOBI, "fsai": _lib.PC_FSAI}[pc],
+                         inner_rtol=args.inner_rtol, max_outer=args.max_outer, coarse_aggregates=coarse)
+
+
+def _time_steps(torch, stream, step, steps, warmup):
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stats = []
+    ev0.record(stream)
+    for _ in range(steps):
+        stats.append(step())
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    return ev0.elapsed_time(ev1), stats
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -216,53 +246,45 @@ def run_ours(args):
     if not torch.cuda.is_available():
         print(json.dumps({"metric": METRIC, "error": "no CUDA device"}))
         sys.exit(2)
-    from mphyfem_b200 import api
+    from mphyfem_b200 import _lib, api
 
+    dev = f"cuda:{local}"
     prob = _workload(args.workload)
     ctx = api.Context(local)
     mesh = api.Mesh(ctx, prob)
     pat = api.Pattern(mesh)
-    from mphyfem_b200 import _lib
-    prec = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED, "mixed32": _lib.PREC_MIXED_F32VEC}[args.precision]
-    pc = {"jacobi": _lib.PC_JACOBI, "fsai": _lib.PC_FSAI}[args.pc]
-    sol = api.SolverGpu(mesh, pat, rtol=args.rtol, max_it=args.max_it, precision=prec, inner_rtol=args.inner_rtol,
-                        max_outer=args.max_outer, pc_type=pc, coarse_aggregates=args.coarse)
-    stream = torch.cuda.ExternalStream(sol.stream, device=f"cuda:{local}")
-    disp = torch.zeros(prob.n_dof, dtype=torch.float64, device=f"cuda:{local}")
-    fext = torch.tensor(prob.fnodal, dtype=torch.float64, device=f"cuda:{local}")
+    sol = _make_solver(api, _lib, mesh, pat, args, args.precision, args.pc, args.coarse)
+    stream = torch.cuda.ExternalStream(sol.stream, device=dev)
+    disp = torch.zeros(prob.n_dof, dtype=torch.float64, device=dev)
+    fext = torch.tensor(prob.fnodal, dtype=torch.float64, device=dev)
 
     def step():
         disp.zero_()
         return sol.newton_iteration(disp, fext, LAMBDA)
 
     for _ in range(args.warmup):
-        st = step()
+        step()
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    stats = []
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
-        torch.cuda.synchronize()
-        ev0.record(stream)
-        for _ in range(args.steps):
-            stats.append(step())
-        ev1.record(stream)
-        torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1)
-    t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
+        ms, stats = _time_steps(torch, stream, step, args.steps, 0)
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
     if world > 1:
         dist.barrier()
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms = float(t.item())
     its = [s.krylov_its for s in stats]
-    kstatus = [int(s.status) for s in stats]
+    kstatus = sorted({int(s.status) for s in stats})
     asm_ms = statistics.median([s.t_assembly_ms for s in stats])
+    solve_ms = statistics.median([s.t_solve_ms for s in stats])
     launches = int(sum(s.kernel_launches for s in stats))
+    relres = sol.true_residual()
+    coarse = sol.coarse_info() if args.coarse > 0 else None
 
     # dominant kernel: the SpMV of the Krylov loop, timed standalone with events on its stream
     mi = sol.matrix_info()
-    x = torch.randn(prob.n_dof, dtype=torch.float64, device=f"cuda:{local}")
+    x = torch.randn(prob.n_dof, dtype=torch.float64, device=dev)
     y = torch.empty_like(x)
     for _ in range(3):
         sol.spmv(x, y)
@@ -280,7 +302,7 @@ def run_ours(args):
         spmv_bytes += prob.n_node * (72 + 3)
     peak, peak_kind = _peaks()
     achieved = spmv_bytes / (spmv_ms * 1e-3) / 1e9
-    asm_bytes = pat.nnz * 8 + prob.n_free * 8 + prob.n_node * 48 + prob.n_elem * 36
+    asm_bytes = pat.nnz * (8 if vbytes == 8 else 4) + prob.n_free * 8 + prob.n_node * 48 + prob.n_elem * 36
 
     # end to end through the C ABI with host buffers (H2D of u and f_ext, D2H of u every step)
     disp_h = torch.zeros(prob.n_dof, dtype=torch.float64).pin_memory().numpy()
@@ -295,31 +317,55 @@ def run_ours(args):
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1) / e2e_steps
 
+    # the plain GPU method (FP64 Jacobi-PCG, the drop-in for the reference's KSPCG + PCJACOBI),
+    # same workload and step, measured in the same run
+    plain = None
+    if world == 1 and not args.no_plain and (args.precision, args.pc, args.coarse) != ("fp64", "jacobi", 0):
+        sol.close()
+        psol = _make_solver(api, _lib, mesh, pat, args, "fp64", "jacobi", 0)
+        pstream = torch.cuda.ExternalStream(psol.stream, device=dev)
+
+        def pstep():
+            disp.zero_()
+            return psol.newton_iteration(disp, fext, LAMBDA)
+
+        pms, pst = _time_steps(torch, pstream, pstep, max(1, min(args.steps, 2)), 1)
+        plain = {"method": "FP64 Jacobi-PCG (plain)", "ms_per_newton_iter": pms / len(pst),
+                 "krylov_its": int(statistics.median([q.krylov_its for q in pst])),
+                 "true_relres": psol.true_residual(),
+                 "speedup_of_this_method": (pms / len(pst)) / (ms / args.steps)}
+        psol.close()
+
     if rank != 0:
         if world > 1:
             dist.destroy_process_group()
         return
     cpu = None
     if world == 1 and not args.no_cpu:
-        cpu = cpu_newton_estimate(prob, int(statistics.median(its)), args.rtol)
+        cpu = cpu_newton_estimate(prob, args.ref_its, args.rtol)
     line = {
         "metric": METRIC, "value": world * args.steps / (ms * 1e-3), "unit": "Newton iter/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": dict(_config(prob, args.rtol), parallelism=f"replicas{world}" if world > 1 else "single"),
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+        "data": "synthetic",
+        "config": dict(_config(prob, args.rtol), method=_method_name(args),
+                       parallelism=f"replicas{world}" if world > 1 else "single"),
         "krylov_its": int(statistics.median(its)),
-        "krylov_status": [_lib.status_string(k) for k in sorted(set(kstatus))],
+        "krylov_status": [_lib.status_string(k) for k in kstatus],
+        "true_relres": relres,
+        "solve_ms": solve_ms,
+        "coarse": coarse,
         "assembly": {"ms": asm_ms, "melems_per_s": prob.n_elem / (asm_ms * 1e-3) / 1e6,
                      "algorithmic_bytes": asm_bytes, "achieved_gbs": asm_bytes / (asm_ms * 1e-3) / 1e9,
                      "frac": asm_bytes / (asm_ms * 1e-3) / 1e9 / peak},
+        "plain_gpu": plain,
         "e2e": {"value": 1e3 / e2e_ms, "unit": "Newton iter/s", "h2d_bytes_per_step": 2 * prob.n_dof * 8,
                 "d2h_bytes_per_step": prob.n_dof * 8},
         "roofline": {"kernel": f"spmv_kernel (SELL-32 3x3, {'FP64' if vbytes == 8 else 'FP32'} values, FP64 vectors)",
-                     "bound": "hbm", "achieved": achieved,
-                     "peak": peak, "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                     "bound": "hbm", "achieved": achieved, "peak": peak, "peak_source": peak_kind, "unit": "GB/s",
+                     "frac": achieved / peak,
                      "traffic": _read_traffic("spmv_fp64" if vbytes == 8 else "spmv_mixed"),
-                     "algorithmic_bytes": spmv_bytes,
-                     "launch_ms": spmv_ms},
+                     "algorithmic_bytes": spmv_bytes, "launch_ms": spmv_ms},
         "cpu_baseline": None if cpu is None else {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
         "clocks": clk.summary(),
         "gpu_launches": launches,
@@ -337,11 +383,13 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="large", choices=["large", "small", "two_phase"])
     ap.add_argument("--rtol", type=float, default=1e-8)
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed", "mixed32"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed", "mixed32"])
     ap.add_argument("--inner-rtol", dest="inner_rtol", type=float, default=0.0)
     ap.add_argument("--max-outer", dest="max_outer", type=int, default=1)
     ap.add_argument("--pc", default="jacobi", choices=["jacobi", "fsai"])
-    ap.add_argument("--coarse", type=int, default=0, help="aggregates of the two-level coarse correction (0: off)")
+    ap.add_argument("--coarse", type=int, default=512, help="aggregates of the two-level coarse correction (0: off)")
+    ap.add_argument("--no-plain", dest="no_plain", action="store_true",
+                    help="skip the same-run measurement of the plain FP64 Jacobi-PCG method")
     ap.add_argument("--max-it", dest="max_it", type=int, default=20000)
     ap.add_argument("--ref-its", dest="ref_its", type=int, default=2411,
                     help="Krylov iterations per Newton iteration for --impl reference: the Jacobi-PCG count "

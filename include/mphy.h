@@ -217,6 +217,8 @@ int mphy_solver_pc_setup(mphy_solver* s, int32_t* n_fallback);
  * bounding box) and coarse size (6 modes per box). *setup_ms: time of the last E setup.
  * No counterpart in the reference. */
 int mphy_solver_coarse_info(const mphy_solver* s, int32_t* grid3, int32_t* coarse_size, float* setup_ms);
+/* ||b - A x|| / ||b|| in FP64 for the last solve (A as stored: FP64, or the FP32 storage). */
+int mphy_solver_true_residual(mphy_solver* s, double* relres);
 /* Solution increment scattered to node-major layout (femSolidmechanics2.cpp:1183-1186):
  * dx_dev[assyForSoln[i]] = soln[i], prescribed DOFs 0. */
 int mphy_solver_get_solution(mphy_solver* s, double* dx_dev);

@@ -103,6 +103,7 @@ SIGNATURES = {
     "mphy_solver_pc_get_blocks": (C.c_int, [_vp, _vp]),
     "mphy_solver_pc_set_blocks": (C.c_int, [_vp, _vp]),
     "mphy_solver_pc_setup": (C.c_int, [_vp, _i32]),
+    "mphy_solver_true_residual": (C.c_int, [_vp, _d]),
     "mphy_solver_coarse_info": (C.c_int, [_vp, _i32, _i32, C.POINTER(C.c_float)]),
     "mphy_solver_get_solution": (C.c_int, [_vp, _vp]),
     "mphy_solver_update_disp": (C.c_int, [_vp, _vp]),

@@ -211,6 +211,12 @@ class SolverGpu:
         b = blocks_dev.contiguous().to(torch.float32)
         L.check(self.lib.mphy_solver_pc_set_blocks(self.h, _ptr(b)))
 
+    def true_residual(self) -> float:
+        """||b - A x|| / ||b|| of the last solve, FP64."""
+        v = C.c_double()
+        L.check(self.lib.mphy_solver_true_residual(self.h, C.byref(v)))
+        return v.value
+
     def coarse_info(self):
         g = (C.c_int32 * 3)()
         k = C.c_int32()

@@ -697,6 +697,28 @@ int mphy_solver_pc_setup(mphy_solver* s, int32_t* n_fallback) {
     });
 }
 
+int mphy_solver_true_residual(mphy_solver* s, double* relres) {
+    return guarded([&] {
+        MPHY_REQUIRE(s && relres, MPHY_ERR_INVALID_ARG, "null argument");
+        cudaStream_t st = s->ctx->stream;
+        const int sm = s->ctx->sm_count;
+        const int64_t n = 3 * (int64_t)s->mesh->n_node;
+        DevBuf<double> r(n);
+        if (s->mixed) residual_fp64<float>(s->A, s->valf.p, s->x.p, s->rhs.p, r.p, s->partials.p, s->counter.p,
+                                           s->scalar.p, st, sm);
+        else residual_fp64<double>(s->A, s->val.p, s->x.p, s->rhs.p, r.p, s->partials.p, s->counter.p, s->scalar.p,
+                                   st, sm);
+        double rr = 0.0, bb = 0.0;
+        MPHY_CUDA(cudaMemcpyAsync(&rr, s->scalar.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+        MPHY_CUDA(cudaStreamSynchronize(st));
+        dot_fp64(s->rhs.p, s->rhs.p, n, s->partials.p, s->counter.p, s->scalar.p, st, sm);
+        MPHY_CUDA(cudaMemcpyAsync(&bb, s->scalar.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+        MPHY_CUDA(cudaStreamSynchronize(st));
+        *relres = bb > 0.0 ? std::sqrt(rr / bb) : 0.0;
+        return (int)MPHY_OK;
+    });
+}
+
 int mphy_solver_coarse_info(const mphy_solver* s, int32_t* grid3, int32_t* k, float* setup_ms) {
     if (!s) return MPHY_ERR_INVALID_ARG;
     if (!s->use_coarse) {
