@@ -85,7 +85,10 @@ typedef struct mphy_solver_opts {
     int32_t chunk;         /* Krylov iterations per launched graph between host checks (0: auto) */
     int32_t coarse_aggregates; /* > 0: add the two-level rigid-body coarse correction
                                 * M^{-1} = D^{-1} + Z (Z^T A Z)^{-1} Z^T over about this many
-                                * geometric aggregates (6 modes each) to MPHY_PC_JACOBI */
+                                * geometric aggregates (6 modes each) to the local
+                                * preconditioner (Jacobi: D^{-1}, FSAI: G^T G) */
+    int32_t norm_type;     /* KSP norm of the convergence test: 0 = preconditioned ||z|| (PETSc's
+                            * CG default), 1 = unpreconditioned ||r|| (true residual vs ||b||) */
 } mphy_solver_opts;
 
 typedef struct mphy_newton_opts {

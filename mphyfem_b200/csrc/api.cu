@@ -519,16 +519,6 @@ int mphy_solver_create(mphy_ctx* c, const mphy_mesh* m, const mphy_pattern* P, c
             if (o.precision == MPHY_PREC_MIXED) s->ir.init(s->A, c->sm_count, o.chunk);
             else if (o.precision == MPHY_PREC_MIXED_F32VEC) s->ir32.init(s->A, c->sm_count, o.chunk);
             else s->pcg.init(s->A, c->sm_count, o.chunk);
-            if (o.coarse_aggregates > 0) {
-                MPHY_REQUIRE(o.pc_type == MPHY_PC_JACOBI, MPHY_ERR_UNSUPPORTED,
-                             "the coarse correction combines with MPHY_PC_JACOBI");
-                s->use_coarse = true;
-                s->coarse.init(c, m, P, o.coarse_aggregates);
-                const CoarseView cv = s->coarse.view();
-                if (o.precision == MPHY_PREC_MIXED) s->ir.inner().set_coarse(cv);
-                else if (o.precision == MPHY_PREC_MIXED_F32VEC) s->ir32.inner().set_coarse(cv);
-                else s->pcg.set_coarse(cv);
-            }
             if (o.pc_type != MPHY_PC_JACOBI) {
                 s->use_fsai = true;
                 s->fsai.init(c, P, 16);
@@ -537,6 +527,17 @@ int mphy_solver_create(mphy_ctx* c, const mphy_mesh* m, const mphy_pattern* P, c
                 else if (o.precision == MPHY_PREC_MIXED_F32VEC) s->ir32.inner().set_factor(fv);
                 else s->pcg.set_factor(fv);
             }
+            if (o.coarse_aggregates > 0) {
+                s->use_coarse = true;
+                s->coarse.init(c, m, P, o.coarse_aggregates);
+                const CoarseView cv = s->coarse.view();
+                if (o.precision == MPHY_PREC_MIXED) s->ir.inner().set_coarse(cv);
+                else if (o.precision == MPHY_PREC_MIXED_F32VEC) s->ir32.inner().set_coarse(cv);
+                else s->pcg.set_coarse(cv);
+            }
+            s->pcg.norm_type = o.norm_type;
+            s->ir.inner().norm_type = o.norm_type;
+            s->ir32.inner().norm_type = o.norm_type;
             MPHY_CUDA(cudaMallocHost(&s->pinned, 4 * sizeof(double)));
             s->state = MPHY_PATTERN_OK;
             solver_zero(s);

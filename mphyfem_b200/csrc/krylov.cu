@@ -72,8 +72,10 @@ __device__ __forceinline__ double reduce_partials(const double* partials, int n,
 }
 
 // State after the initial residual (KSPConvergedDefault at n = 0).
-__device__ void finish_init(PcgState* st, double rz, double zz, double rtol, double abstol, double dtol, int maxit) {
+__device__ void finish_init(PcgState* st, double rz, double zz, double rtol, double abstol, double dtol, int maxit,
+                            int norm_type) {
     const double dp = sqrt(zz);
+    st->norm_type = norm_type;
     st->rz = rz;
     st->dp = dp;
     st->dp0 = dp;
@@ -197,15 +199,17 @@ __global__ void __launch_bounds__(kThreads) spmv_kernel(SellView A, const VT* __
 
 // z = G^T t with the fused (r, z), (z, z); INIT also sets p = z and the initial state.
 template <typename XT, bool INIT>
-__global__ void __launch_bounds__(kThreads) factor_apply_kernel(SellView A, const float* __restrict__ val,
+__global__ void __launch_bounds__(kThreads) factor_apply_kernel(SellView A, CoarseView cv, const float* __restrict__ val,
                                                                 const XT* __restrict__ t, XT* __restrict__ z,
                                                                 const XT* __restrict__ r, XT* __restrict__ p,
                                                                 double* __restrict__ part_rz,
                                                                 double* __restrict__ part_zz, PcgState* st,
-                                                                double rtol, double abstol, double dtol, int maxit) {
+                                                                double rtol, double abstol, double dtol, int maxit,
+                                                                int norm_type) {
     using Acc = typename AccOf<XT>::type;
     __shared__ double sh[32];
     if (!INIT && st->done) return;
+    const bool unprec = INIT ? norm_type == 1 : st->norm_type == 1;
     double a1 = 0.0, a2 = 0.0;
     const int64_t rows = (int64_t)A.n_slices * 32;
     for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < rows;
@@ -227,13 +231,20 @@ __global__ void __launch_bounds__(kThreads) factor_apply_kernel(SellView A, cons
             y2 += (Acc)v[192] * x0 + (Acc)v[224] * x1 + (Acc)v[256] * x2;
         }
         if (row < A.n_node) {
+            if (cv.n_agg > 0) {  // two-level: + Z c
+                const double* c = cv.c + 6 * (int64_t)cv.agg[row];
+                const double dx = cv.d[3 * row], dy = cv.d[3 * row + 1], dz = cv.d[3 * row + 2];
+                if (!cv.fixed[3 * row]) y0 += (Acc)(c[0] - dy * c[3] + dz * c[5]);
+                if (!cv.fixed[3 * row + 1]) y1 += (Acc)(c[1] + dx * c[3] - dz * c[4]);
+                if (!cv.fixed[3 * row + 2]) y2 += (Acc)(c[2] + dy * c[4] - dx * c[5]);
+            }
             const XT zz[3] = {(XT)y0, (XT)y1, (XT)y2};
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
                 z[3 * row + c] = zz[c];
                 if (INIT) p[3 * row + c] = zz[c];
                 a1 += (double)r[3 * row + c] * (double)zz[c];
-                a2 += (double)zz[c] * (double)zz[c];
+                a2 += unprec ? (double)r[3 * row + c] * (double)r[3 * row + c] : (double)zz[c] * (double)zz[c];
             }
         }
     }
@@ -246,7 +257,7 @@ __global__ void __launch_bounds__(kThreads) factor_apply_kernel(SellView A, cons
     const double zz = reduce_partials(part_zz, gridDim.x, sh);
     if (threadIdx.x == 0) {
         st->counter = 0;
-        if (INIT) finish_init(st, rz, zz, rtol, abstol, dtol, maxit);
+        if (INIT) finish_init(st, rz, zz, rtol, abstol, dtol, maxit, norm_type);
         else finish_iter(st, rz, zz);
     }
 }
@@ -319,6 +330,7 @@ __global__ void __launch_bounds__(kThreads) pcg_update_kernel(int64_t n, XT* __r
     __shared__ double sh[32];
     if (st->done) return;
     const XT alpha = (XT)st->alpha;
+    const bool unprec = st->norm_type == 1;
     double a1 = 0.0, a2 = 0.0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         x[i] += alpha * p[i];
@@ -328,7 +340,7 @@ __global__ void __launch_bounds__(kThreads) pcg_update_kernel(int64_t n, XT* __r
             const XT zi = dinv[i] * ri;
             z[i] = zi;
             a1 += (double)ri * (double)zi;
-            a2 += (double)zi * (double)zi;
+            a2 += unprec ? (double)ri * (double)ri : (double)zi * (double)zi;
         }
     }
     if (!JAC) return;
@@ -360,7 +372,7 @@ __global__ void __launch_bounds__(kThreads) pcg_init_kernel(int64_t n, const XT*
                                                             XT* __restrict__ r, XT* __restrict__ z, XT* __restrict__ p,
                                                             const XT* __restrict__ dinv, double* __restrict__ part_rz,
                                                             double* __restrict__ part_zz, PcgState* st, double rtol,
-                                                            double abstol, double dtol, int maxit) {
+                                                            double abstol, double dtol, int maxit, int norm_type) {
     __shared__ double sh[32];
     double a1 = 0.0, a2 = 0.0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -372,7 +384,7 @@ __global__ void __launch_bounds__(kThreads) pcg_init_kernel(int64_t n, const XT*
             z[i] = zi;
             p[i] = zi;
             a1 += (double)ri * (double)zi;
-            a2 += (double)zi * (double)zi;
+            a2 += norm_type == 1 ? (double)ri * (double)ri : (double)zi * (double)zi;
         }
     }
     if (!JAC) return;
@@ -385,7 +397,7 @@ __global__ void __launch_bounds__(kThreads) pcg_init_kernel(int64_t n, const XT*
     const double zz = reduce_partials(part_zz, gridDim.x, sh);
     if (threadIdx.x == 0) {
         st->counter = 0;
-        finish_init(st, rz, zz, rtol, abstol, dtol, maxit);
+        finish_init(st, rz, zz, rtol, abstol, dtol, maxit, norm_type);
     }
 }
 
@@ -440,9 +452,11 @@ __global__ void __launch_bounds__(kThreads) coarse_final_kernel(int32_t n_node, 
                                                                 const XT* __restrict__ dinv,
                                                                 double* __restrict__ part_rz,
                                                                 double* __restrict__ part_zz, PcgState* st,
-                                                                double rtol, double abstol, double dtol, int maxit) {
+                                                                double rtol, double abstol, double dtol, int maxit,
+                                                                int norm_type) {
     __shared__ double sh[32];
     if (!INIT && st->done) return;
+    const bool unprec = INIT ? norm_type == 1 : st->norm_type == 1;
     double a1 = 0.0, a2 = 0.0;
     for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < n_node; n += (int64_t)gridDim.x * blockDim.x) {
         const double* c = cv.c + 6 * (int64_t)cv.agg[n];
@@ -456,7 +470,7 @@ __global__ void __launch_bounds__(kThreads) coarse_final_kernel(int32_t n_node, 
             z[i] = zi;
             if (INIT) p[i] = zi;
             a1 += (double)ri * (double)zi;
-            a2 += (double)zi * (double)zi;
+            a2 += unprec ? (double)ri * (double)ri : (double)zi * (double)zi;
         }
     }
     a1 = block_sum(a1, sh);
@@ -468,7 +482,7 @@ __global__ void __launch_bounds__(kThreads) coarse_final_kernel(int32_t n_node, 
     const double zz = reduce_partials(part_zz, gridDim.x, sh);
     if (threadIdx.x == 0) {
         st->counter = 0;
-        if (INIT) finish_init(st, rz, zz, rtol, abstol, dtol, maxit);
+        if (INIT) finish_init(st, rz, zz, rtol, abstol, dtol, maxit, norm_type);
         else finish_iter(st, rz, zz);
     }
 }
@@ -697,14 +711,20 @@ void Pcg<VT, XT>::record_iterations(const VT* val, XT* x, cudaStream_t s, int n_
             coarse_gemv_kernel<<<stride_grid((int64_t)coarse_.kp * 32, kThreads, sm_), kThreads, 0, s>>>(coarse_,
                                                                                                           st_.p);
             coarse_final_kernel<XT, false><<<stride_grid(A_.n_node, kThreads, sm_), kThreads, 0, s>>>(
-                A_.n_node, coarse_, r_.p, z_.p, p_.p, dinv_.p, partials_.p, partials2_.p, st_.p, 0, 0, 0, 0);
+                A_.n_node, coarse_, r_.p, z_.p, p_.p, dinv_.p, partials_.p, partials2_.p, st_.p, 0, 0, 0, 0, norm_type);
         } else {
             pcg_update_kernel<XT, false><<<gv, kThreads, 0, s>>>(n_, x, r_.p, z_.p, p_.p, q_.p, nullptr, nullptr,
                                                                   nullptr, st_.p);
             const unsigned gg = stride_grid((int64_t)factor_.G.n_slices * 32, kThreads, sm_);
             spmv_kernel<float, XT, false><<<gg, kThreads, 0, s>>>(factor_.G, factor_.gval, r_.p, t_.p, nullptr, st_.p);
-            factor_apply_kernel<XT, false><<<gg, kThreads, 0, s>>>(factor_.GT, factor_.gtval, t_.p, z_.p, r_.p, p_.p,
-                                                                    partials_.p, partials2_.p, st_.p, 0, 0, 0, 0);
+            if (kind_ == PcKind::FactorCoarse) {
+                coarse_restrict_kernel<XT><<<std::min(coarse_.n_agg, sm_ * 8), kThreads, 0, s>>>(coarse_, r_.p, st_.p);
+                coarse_gemv_kernel<<<stride_grid((int64_t)coarse_.kp * 32, kThreads, sm_), kThreads, 0, s>>>(coarse_,
+                                                                                                              st_.p);
+            }
+            factor_apply_kernel<XT, false><<<gg, kThreads, 0, s>>>(factor_.GT, kind_ == PcKind::FactorCoarse ? coarse_ : CoarseView{},
+                                                                    factor_.gtval, t_.p, z_.p, r_.p, p_.p,
+                                                                    partials_.p, partials2_.p, st_.p, 0, 0, 0, 0, norm_type);
         }
         pcg_direction_kernel<XT><<<gv, kThreads, 0, s>>>(n_, p_.p, z_.p, st_.p);
     }
@@ -718,26 +738,33 @@ int Pcg<VT, XT>::solve(const VT* val, const XT* b, XT* x, double rtol, double ab
     if (kind_ == PcKind::Jacobi) {
         jacobi_kernel<VT, XT><<<stride_grid(A_.n_node, kThreads, sm_), kThreads, 0, s>>>(A_, val, dinv_.p);
         pcg_init_kernel<XT, true><<<gv, kThreads, 0, s>>>(n_, b, x, r_.p, z_.p, p_.p, dinv_.p, partials_.p,
-                                                           partials2_.p, st_.p, rtol, abstol, dtol, maxit);
+                                                           partials2_.p, st_.p, rtol, abstol, dtol, maxit, norm_type);
         launches += 2;
     } else if (kind_ == PcKind::JacobiCoarse) {
         jacobi_kernel<VT, XT><<<stride_grid(A_.n_node, kThreads, sm_), kThreads, 0, s>>>(A_, val, dinv_.p);
         pcg_init_kernel<XT, false><<<gv, kThreads, 0, s>>>(n_, b, x, r_.p, z_.p, p_.p, nullptr, nullptr, nullptr,
-                                                            st_.p, rtol, abstol, dtol, maxit);
+                                                            st_.p, rtol, abstol, dtol, maxit, norm_type);
         coarse_restrict_kernel<XT><<<std::min(coarse_.n_agg, sm_ * 8), kThreads, 0, s>>>(coarse_, r_.p, nullptr);
         coarse_gemv_kernel<<<stride_grid((int64_t)coarse_.kp * 32, kThreads, sm_), kThreads, 0, s>>>(coarse_, nullptr);
         coarse_final_kernel<XT, true><<<stride_grid(A_.n_node, kThreads, sm_), kThreads, 0, s>>>(
             A_.n_node, coarse_, r_.p, z_.p, p_.p, dinv_.p, partials_.p, partials2_.p, st_.p, rtol, abstol, dtol,
-            maxit);
+            maxit, norm_type);
         launches += 5;
     } else {
         pcg_init_kernel<XT, false><<<gv, kThreads, 0, s>>>(n_, b, x, r_.p, z_.p, p_.p, nullptr, nullptr, nullptr,
-                                                            st_.p, rtol, abstol, dtol, maxit);
+                                                            st_.p, rtol, abstol, dtol, maxit, norm_type);
         const unsigned gg = stride_grid((int64_t)factor_.G.n_slices * 32, kThreads, sm_);
         spmv_kernel<float, XT, false><<<gg, kThreads, 0, s>>>(factor_.G, factor_.gval, r_.p, t_.p, nullptr, nullptr);
-        factor_apply_kernel<XT, true><<<gg, kThreads, 0, s>>>(factor_.GT, factor_.gtval, t_.p, z_.p, r_.p, p_.p,
+        if (kind_ == PcKind::FactorCoarse) {
+            coarse_restrict_kernel<XT><<<std::min(coarse_.n_agg, sm_ * 8), kThreads, 0, s>>>(coarse_, r_.p, nullptr);
+            coarse_gemv_kernel<<<stride_grid((int64_t)coarse_.kp * 32, kThreads, sm_), kThreads, 0, s>>>(coarse_,
+                                                                                                          nullptr);
+            launches += 2;
+        }
+        factor_apply_kernel<XT, true><<<gg, kThreads, 0, s>>>(factor_.GT, kind_ == PcKind::FactorCoarse ? coarse_ : CoarseView{},
+                                                               factor_.gtval, t_.p, z_.p, r_.p, p_.p,
                                                                partials_.p, partials2_.p, st_.p, rtol, abstol, dtol,
-                                                               maxit);
+                                                               maxit, norm_type);
         launches += 3;
     }
     MPHY_CUDA(cudaGetLastError());
@@ -758,7 +785,7 @@ int Pcg<VT, XT>::solve(const VT* val, const XT* b, XT* x, double rtol, double ab
         graph_stream_ = s;
         graph_kind_ = kind_;
     }
-    const int per_iter = kind_ == PcKind::Jacobi ? 3 : (kind_ == PcKind::Factor ? 5 : 6);
+    const int per_iter = kind_ == PcKind::Jacobi ? 3 : (kind_ == PcKind::Factor ? 5 : (kind_ == PcKind::FactorCoarse ? 7 : 6));
     PcgState h{};
     // every replay advances at most chunk_ iterations; the device stops at maxit
     const int64_t max_replays = (int64_t)(maxit > 0 ? maxit : 0) / chunk_ + 2;

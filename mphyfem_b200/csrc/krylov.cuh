@@ -23,7 +23,7 @@ struct PcgState {
     int32_t status;  // mphy_status of the solve
     int32_t maxit;
     uint32_t counter;  // last-CTA detection, reset by the last CTA
-    uint32_t pad;
+    int32_t norm_type; // 0: ||z|| (KSP_NORM_PRECONDITIONED), 1: ||r|| (KSP_NORM_UNPRECONDITIONED)
 };
 
 struct SellView {
@@ -65,7 +65,7 @@ void residual_fp64(const SellView& A, const VT* val, const double* x, const doub
 void dot_fp64(const double* a, const double* b, int64_t n, double* partials, uint32_t* counter, double* out_dev,
               cudaStream_t s, int sm);
 
-enum class PcKind { Jacobi, Factor, JacobiCoarse };
+enum class PcKind { Jacobi, Factor, JacobiCoarse, FactorCoarse };
 
 // Preconditioned CG, VT = matrix values, XT = vector precision (double, or float with FP64
 // reductions). solve() runs from x = 0 on b (XT), PETSc KSPCG semantics.
@@ -75,10 +75,15 @@ class Pcg {
     void init(const SellView& A, int sm_count, int chunk);
     void set_factor(const FactorView<float>& f) { factor_ = f; kind_ = PcKind::Factor; }
     void set_jacobi() { kind_ = PcKind::Jacobi; }
-    void set_coarse(const CoarseView& c) { coarse_ = c; kind_ = PcKind::JacobiCoarse; }
+    // the coarse correction adds to the current local part (Jacobi or G^T G)
+    void set_coarse(const CoarseView& c) {
+        coarse_ = c;
+        kind_ = kind_ == PcKind::Factor ? PcKind::FactorCoarse : PcKind::JacobiCoarse;
+    }
     int solve(const VT* val, const XT* b, XT* x, double rtol, double abstol, double dtol, int maxit, cudaStream_t s,
               int32_t* its, double* final_norm);
     ~Pcg();
+    int norm_type = 0;  // KSP norm type of the convergence test (see PcgState)
     int64_t launches = 0;  // kernels launched by the last solve()
 
   private:

@@ -67,6 +67,8 @@ def lib():
         L.orc_problem_assemble.restype = C.c_int64
         L.orc_cg_jacobi.argtypes = [C.c_void_p, _d, _d, _d, C.c_double, C.c_double, C.c_int, C.c_int,
                                     C.POINTER(C.c_int), _d]
+        L.orc_cg_jacobi_norm.argtypes = [C.c_void_p, _d, _d, _d, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int,
+                                         C.POINTER(C.c_int), _d]
         L.orc_newton_run.argtypes = [C.c_void_p, _d, C.POINTER(NewtonOpts), _d, _d, C.c_int]
         _lib = L
     return _lib
@@ -153,12 +155,12 @@ class OracleProblem:
         bad = lib().orc_problem_assemble(self.h, _p(disp, _d), _p(val, _d), _p(rhs, _d), _p(reac, _d), nthreads)
         return val, rhs, reac, int(bad)
 
-    def cg(self, val, b, rtol=1e-12, abstol=1e-50, maxit=10000, nthreads=1):
+    def cg(self, val, b, rtol=1e-12, abstol=1e-50, maxit=10000, nthreads=1, norm_type=0):
         b = np.ascontiguousarray(b, np.float64)
         x = np.zeros(self.n_free)
         its, fn = C.c_int(0), C.c_double(0.0)
-        st = lib().orc_cg_jacobi(self.h, _p(val, _d), _p(b, _d), _p(x, _d), rtol, abstol, maxit, nthreads,
-                                 C.byref(its), C.byref(fn))
+        st = lib().orc_cg_jacobi_norm(self.h, _p(val, _d), _p(b, _d), _p(x, _d), rtol, abstol, maxit, nthreads,
+                                      norm_type, C.byref(its), C.byref(fn))
         return x, its.value, fn.value, st
 
     def newton(self, tol_rel=None, tol_abs=0.0, cg_rtol=None, cg_maxit=10000, max_newton=10,

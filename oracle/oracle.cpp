@@ -557,6 +557,11 @@ int64_t orc_problem_assemble(const orc_problem* p, const double* disp, double* v
 // max(rtol * ||z_0||, abstol).
 int orc_cg_jacobi(const orc_problem* p, const double* val, const double* b, double* x, double rtol,
                   double abstol, int maxit, int nthreads, int* its_out, double* final_norm) {
+    return orc_cg_jacobi_norm(p, val, b, x, rtol, abstol, maxit, nthreads, 0, its_out, final_norm);
+}
+
+int orc_cg_jacobi_norm(const orc_problem* p, const double* val, const double* b, double* x, double rtol,
+                       double abstol, int maxit, int nthreads, int norm_type, int* its_out, double* final_norm) {
     const CsrPattern& P = p->pat;
     const int n = P.n_free;
     set_threads(nthreads);
@@ -578,7 +583,7 @@ int orc_cg_jacobi(const orc_problem* p, const double* val, const double* b, doub
     };
 #pragma omp parallel for if (par)
     for (int i = 0; i < n; ++i) z[i] = dinv[i] * r[i];
-    double dp = std::sqrt(dot(z, z));
+    double dp = std::sqrt(norm_type == 1 ? dot(r, r) : dot(z, z));
     const double ttol = std::max(rtol * dp, abstol);
     int its = 0, status = 1;
     if (final_norm) *final_norm = dp;
@@ -613,7 +618,7 @@ int orc_cg_jacobi(const orc_problem* p, const double* val, const double* b, doub
             r[k] -= a * q[k];
             z[k] = dinv[k] * r[k];
         }
-        dp = std::sqrt(dot(z, z));
+        dp = std::sqrt(norm_type == 1 ? dot(r, r) : dot(z, z));
         if (final_norm) *final_norm = dp;
         if (std::isnan(dp)) { status = 3; break; }
         if (dp <= ttol) { status = 0; break; }

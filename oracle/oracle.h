@@ -92,6 +92,11 @@ int64_t orc_problem_assemble(const orc_problem* p, const double* disp, double* v
 int orc_cg_jacobi(const orc_problem* p, const double* val, const double* b, double* x,
                   double rtol, double abstol, int maxit, int nthreads, int* its,
                   double* final_norm);
+/* The same with the norm type: 0 = KSP_NORM_PRECONDITIONED (||z||, PETSc's CG default),
+ * 1 = KSP_NORM_UNPRECONDITIONED (||r||, the true residual relative to ||b||). */
+int orc_cg_jacobi_norm(const orc_problem* p, const double* val, const double* b, double* x,
+                       double rtol, double abstol, int maxit, int nthreads, int norm_type, int* its,
+                       double* final_norm);
 
 /* Newton-Raphson load stepping (femSolidmechanics2.cpp:730-851, STATIC scheme, nodal forces
  * scaled by the load factor lambda(t) = t).
