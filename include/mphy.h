@@ -70,6 +70,7 @@ typedef struct mphy_ctx mphy_ctx;
 typedef struct mphy_mesh mphy_mesh;
 typedef struct mphy_pattern mphy_pattern;
 typedef struct mphy_solver mphy_solver;
+typedef struct mphy_gnn mphy_gnn;
 
 typedef struct mphy_solver_opts {
     int32_t precision;     /* MPHY_PREC_* */
@@ -216,6 +217,33 @@ int mphy_solver_pc_set_blocks(mphy_solver* s, const float* blocks_dev);
 /* Exact block FSAI of the currently assembled operator; *n_fallback rows were not positive
  * definite and use the inverse square root of their diagonal. */
 int mphy_solver_pc_setup(mphy_solver* s, int32_t* n_fallback);
+/* ---- learned factorised preconditioner (MPHY_PC_FSAI_LEARNED). No counterpart in the reference.
+ * A message-passing network (3 layers of width 64, BF16 weights, FP32 accumulation) predicts the
+ * blocks of G from the Jacobi-scaled operator; it is trained on the GPU against the exact block
+ * FSAI of operators the solver assembles. Parameters: a flat FP32 vector of
+ * mphy_gnn_param_count() values. */
+int mphy_gnn_param_count(void);
+int mphy_gnn_create(mphy_ctx* ctx, const float* params_host, mphy_gnn** out);
+int mphy_gnn_destroy(mphy_gnn* g);
+int mphy_gnn_get_params(mphy_gnn* g, float* params_host);
+int mphy_gnn_set_params(mphy_gnn* g, const float* params_host);
+/* Loss (mean squared error of the scaled blocks against the exact FSAI of the solver's assembled
+ * operator) and its gradient, without changing the parameters; grads_host may be NULL. */
+int mphy_gnn_loss_and_grads(mphy_gnn* g, mphy_solver* s, double* loss, float* grads_host);
+/* One Adam step on the solver's assembled operator; *loss before the step. */
+int mphy_gnn_train_step(mphy_gnn* g, mphy_solver* s, float lr, double* loss);
+/* Predict G for the solver's assembled operator and install it (then solves use it). */
+int mphy_gnn_predict(mphy_gnn* g, mphy_solver* s, float* ms);
+/* With MPHY_PC_FSAI_LEARNED, run the network before every solve (NULL detaches). Such solves stop
+ * on the true residual (norm_type 1) and are accepted only with ||b - A x|| <= 100 rtol ||b|| in
+ * FP64; otherwise they are repeated with the Jacobi local part (see mphy_solver_pc_last). */
+int mphy_solver_attach_gnn(mphy_solver* s, mphy_gnn* g);
+/* Last solve: *fallback = 1 when a learned preconditioner failed the FP64 true-residual check and
+ * the solve was repeated with the Jacobi local part; *setup_ms = the preconditioner's setup time
+ * (FSAI, network inference or coarse operator); first_*: status, iterations and true relative
+ * residual of the learned attempt. Any pointer may be NULL. */
+int mphy_solver_pc_last(const mphy_solver* s, int32_t* fallback, float* setup_ms, int32_t* first_status,
+                        int32_t* first_its, double* first_relres);
 /* Coarse space of the two-level correction: aggregate grid (boxes along x, y, z of the reference
  * bounding box) and coarse size (6 modes per box). *setup_ms: time of the last E setup.
  * No counterpart in the reference. */

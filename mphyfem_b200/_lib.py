@@ -104,6 +104,16 @@ SIGNATURES = {
     "mphy_solver_pc_set_blocks": (C.c_int, [_vp, _vp]),
     "mphy_solver_pc_setup": (C.c_int, [_vp, _i32]),
     "mphy_solver_true_residual": (C.c_int, [_vp, _d]),
+    "mphy_gnn_param_count": (C.c_int, []),
+    "mphy_gnn_create": (C.c_int, [_vp, C.POINTER(C.c_float), C.POINTER(_vp)]),
+    "mphy_gnn_destroy": (C.c_int, [_vp]),
+    "mphy_gnn_get_params": (C.c_int, [_vp, C.POINTER(C.c_float)]),
+    "mphy_gnn_set_params": (C.c_int, [_vp, C.POINTER(C.c_float)]),
+    "mphy_gnn_loss_and_grads": (C.c_int, [_vp, _vp, _d, C.POINTER(C.c_float)]),
+    "mphy_gnn_train_step": (C.c_int, [_vp, _vp, C.c_float, _d]),
+    "mphy_gnn_predict": (C.c_int, [_vp, _vp, C.POINTER(C.c_float)]),
+    "mphy_solver_attach_gnn": (C.c_int, [_vp, _vp]),
+    "mphy_solver_pc_last": (C.c_int, [_vp, _i32, C.POINTER(C.c_float), _i32, _i32, _d]),
     "mphy_solver_coarse_info": (C.c_int, [_vp, _i32, _i32, C.POINTER(C.c_float)]),
     "mphy_solver_get_solution": (C.c_int, [_vp, _vp]),
     "mphy_solver_update_disp": (C.c_int, [_vp, _vp]),

@@ -217,6 +217,12 @@ class SolverGpu:
         L.check(self.lib.mphy_solver_true_residual(self.h, C.byref(v)))
         return v.value
 
+    def pc_last(self):
+        fb, ms, st, it, rr = C.c_int32(), C.c_float(), C.c_int32(), C.c_int32(), C.c_double()
+        L.check(self.lib.mphy_solver_pc_last(self.h, C.byref(fb), C.byref(ms), C.byref(st), C.byref(it), C.byref(rr)))
+        return {"fallback": bool(fb.value), "setup_ms": ms.value, "first_status": st.value, "first_its": it.value,
+                "first_relres": rr.value}
+
     def coarse_info(self):
         g = (C.c_int32 * 3)()
         k = C.c_int32()

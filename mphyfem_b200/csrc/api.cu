@@ -15,6 +15,7 @@
 #include "coarse.cuh"
 #include "elem.cuh"
 #include "fsai.cuh"
+#include "gnn.cuh"
 #include "krylov.cuh"
 #include "pattern.cuh"
 
@@ -70,11 +71,22 @@ struct mphy_solver {
     IterativeRefinement<float> ir32;      // MIXED_F32VEC
     Fsai fsai;                            // MPHY_PC_FSAI*
     CoarseSpace coarse;                   // coarse_aggregates > 0
+    mphy_gnn* gnn = nullptr;              // MPHY_PC_FSAI_LEARNED: network run before every solve
+    int32_t last_fallback = 0;            // the last solve fell back to Jacobi
+    int32_t first_status = 0, first_its = 0;  // the learned attempt of the last solve
+    double first_relres = 0.0;
+    GnnGraph graph;
     bool use_coarse = false;
     bool use_fsai = false;
     double t_pc_ms = 0.0;                 // last preconditioner setup time
     int32_t last_sweeps = 0;
     double* pinned = nullptr;  // [0] norm, [1] bad as bits
+};
+
+struct mphy_gnn {
+    mphy_ctx* ctx = nullptr;
+    int device = 0;
+    Gnn net;
 };
 
 namespace {
@@ -140,7 +152,44 @@ double solver_norm_and_bad(mphy_solver* s, int64_t* first_bad) {
     return std::sqrt(s->pinned[0]);
 }
 
+int solver_solve_once(mphy_solver* s, int32_t* its, double* fnorm);
+double true_relres(mphy_solver* s);
+
+// A learned preconditioner is checked by the FP64 true residual: a failed or useless solve is
+// repeated with the Jacobi local part (the coarse correction, if any, kept).
 int solver_solve(mphy_solver* s, int32_t* its, double* fnorm) {
+    s->last_fallback = 0;
+    const int rc = solver_solve_once(s, its, fnorm);
+    if (!(s->use_fsai && s->opts.pc_type == MPHY_PC_FSAI_LEARNED)) return rc;
+    const double rel = true_relres(s);
+    s->first_status = rc;
+    s->first_its = its ? *its : 0;
+    s->first_relres = rel;
+    // 100 rtol: room for the drift of the recurrence residual from the true one on stiff
+    // operators; a poor prediction shows up as divergence or an order-of-magnitude miss.
+    if (rc == MPHY_OK && rel == rel && rel <= 100.0 * s->opts.rtol) return rc;
+    s->last_fallback = 1;
+    auto local_jacobi = [&](auto& pcg) {
+        pcg.set_jacobi();
+        if (s->use_coarse) pcg.set_coarse(s->coarse.view());
+    };
+    auto local_factor = [&](auto& pcg) {
+        pcg.set_factor(s->fsai.view());
+        if (s->use_coarse) pcg.set_coarse(s->coarse.view());
+    };
+    if (s->opts.precision == MPHY_PREC_MIXED) local_jacobi(s->ir.inner());
+    else if (s->opts.precision == MPHY_PREC_MIXED_F32VEC) local_jacobi(s->ir32.inner());
+    else local_jacobi(s->pcg);
+    int32_t its2 = 0;
+    const int rc2 = solver_solve_once(s, &its2, fnorm);
+    if (its) *its += its2;
+    if (s->opts.precision == MPHY_PREC_MIXED) local_factor(s->ir.inner());
+    else if (s->opts.precision == MPHY_PREC_MIXED_F32VEC) local_factor(s->ir32.inner());
+    else local_factor(s->pcg);
+    return rc2;
+}
+
+int solver_solve_once(mphy_solver* s, int32_t* its, double* fnorm) {
     MPHY_REQUIRE(s->state == MPHY_ASSEMBLY_OK || s->state == MPHY_FACTORISE_OK, MPHY_ERR_STATE,
                  "factoriseAndSolve: assemble matrix first");
     s->state = MPHY_FACTORISE_OK;
@@ -155,6 +204,12 @@ int solver_solve(mphy_solver* s, int32_t* its, double* fnorm) {
         cudaEventElapsedTime(&ms, s->ctx->ev0, s->ctx->ev1);
         s->t_pc_ms = ms;
         s->launches += s->fsai.launches;
+    }
+    if (s->use_fsai && s->opts.pc_type == MPHY_PC_FSAI_LEARNED && s->gnn) {
+        float ms = 0.f;
+        const int rc = mphy_gnn_predict(s->gnn, s, &ms);
+        MPHY_REQUIRE(rc == MPHY_OK, rc, "learned preconditioner: prediction failed");
+        s->t_pc_ms = ms;
     }
     if (s->use_coarse) {
         // the coarse operator follows the assembled matrix
@@ -181,6 +236,24 @@ int solver_solve(mphy_solver* s, int32_t* its, double* fnorm) {
                                 s->opts.max_it, s->ctx->stream, its, fnorm);
     s->launches += s->pcg.launches;
     return rc;
+}
+
+double true_relres(mphy_solver* s) {
+    cudaStream_t st = s->ctx->stream;
+    const int sm = s->ctx->sm_count;
+    const int64_t n = 3 * (int64_t)s->mesh->n_node;
+    DevBuf<double> r(n);
+    if (s->mixed)
+        residual_fp64<float>(s->A, s->valf.p, s->x.p, s->rhs.p, r.p, s->partials.p, s->counter.p, s->scalar.p, st, sm);
+    else
+        residual_fp64<double>(s->A, s->val.p, s->x.p, s->rhs.p, r.p, s->partials.p, s->counter.p, s->scalar.p, st, sm);
+    double rr = 0.0, bb = 0.0;
+    MPHY_CUDA(cudaMemcpyAsync(&rr, s->scalar.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+    MPHY_CUDA(cudaStreamSynchronize(st));
+    dot_fp64(s->rhs.p, s->rhs.p, n, s->partials.p, s->counter.p, s->scalar.p, st, sm);
+    MPHY_CUDA(cudaMemcpyAsync(&bb, s->scalar.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+    MPHY_CUDA(cudaStreamSynchronize(st));
+    return bb > 0.0 ? std::sqrt(rr / bb) : 0.0;
 }
 
 float elapsed_ms(mphy_ctx* c) {
@@ -535,9 +608,11 @@ int mphy_solver_create(mphy_ctx* c, const mphy_mesh* m, const mphy_pattern* P, c
                 else if (o.precision == MPHY_PREC_MIXED_F32VEC) s->ir32.inner().set_coarse(cv);
                 else s->pcg.set_coarse(cv);
             }
-            s->pcg.norm_type = o.norm_type;
-            s->ir.inner().norm_type = o.norm_type;
-            s->ir32.inner().norm_type = o.norm_type;
+            // a learned local part is judged by the true residual, so it also stops on it
+            const int nt = o.pc_type == MPHY_PC_FSAI_LEARNED ? 1 : o.norm_type;
+            s->pcg.norm_type = nt;
+            s->ir.inner().norm_type = nt;
+            s->ir32.inner().norm_type = nt;
             MPHY_CUDA(cudaMallocHost(&s->pinned, 4 * sizeof(double)));
             s->state = MPHY_PATTERN_OK;
             solver_zero(s);
@@ -701,23 +776,20 @@ int mphy_solver_pc_setup(mphy_solver* s, int32_t* n_fallback) {
 int mphy_solver_true_residual(mphy_solver* s, double* relres) {
     return guarded([&] {
         MPHY_REQUIRE(s && relres, MPHY_ERR_INVALID_ARG, "null argument");
-        cudaStream_t st = s->ctx->stream;
-        const int sm = s->ctx->sm_count;
-        const int64_t n = 3 * (int64_t)s->mesh->n_node;
-        DevBuf<double> r(n);
-        if (s->mixed) residual_fp64<float>(s->A, s->valf.p, s->x.p, s->rhs.p, r.p, s->partials.p, s->counter.p,
-                                           s->scalar.p, st, sm);
-        else residual_fp64<double>(s->A, s->val.p, s->x.p, s->rhs.p, r.p, s->partials.p, s->counter.p, s->scalar.p,
-                                   st, sm);
-        double rr = 0.0, bb = 0.0;
-        MPHY_CUDA(cudaMemcpyAsync(&rr, s->scalar.p, sizeof(double), cudaMemcpyDeviceToHost, st));
-        MPHY_CUDA(cudaStreamSynchronize(st));
-        dot_fp64(s->rhs.p, s->rhs.p, n, s->partials.p, s->counter.p, s->scalar.p, st, sm);
-        MPHY_CUDA(cudaMemcpyAsync(&bb, s->scalar.p, sizeof(double), cudaMemcpyDeviceToHost, st));
-        MPHY_CUDA(cudaStreamSynchronize(st));
-        *relres = bb > 0.0 ? std::sqrt(rr / bb) : 0.0;
+        *relres = true_relres(s);
         return (int)MPHY_OK;
     });
+}
+
+int mphy_solver_pc_last(const mphy_solver* s, int32_t* fallback, float* setup_ms, int32_t* first_status,
+                        int32_t* first_its, double* first_relres) {
+    if (!s) return MPHY_ERR_INVALID_ARG;
+    if (fallback) *fallback = s->last_fallback;
+    if (setup_ms) *setup_ms = (float)s->t_pc_ms;
+    if (first_status) *first_status = s->first_status;
+    if (first_its) *first_its = s->first_its;
+    if (first_relres) *first_relres = s->first_relres;
+    return MPHY_OK;
 }
 
 int mphy_solver_coarse_info(const mphy_solver* s, int32_t* grid3, int32_t* k, float* setup_ms) {
@@ -886,4 +958,118 @@ int mphy_newton_run(mphy_solver* s, const double* fext_host, const mphy_newton_o
     });
 }
 
+
+// ------------------------------------------------------------------------------- learned FSAI
+int mphy_gnn_param_count(void) { return GnnLayout::total; }
+
+int mphy_gnn_create(mphy_ctx* c, const float* params, mphy_gnn** out) {
+    return guarded([&] {
+        MPHY_REQUIRE(c && params && out, MPHY_ERR_INVALID_ARG, "null argument");
+        MPHY_CUDA(cudaSetDevice(c->device));
+        auto* g = new mphy_gnn;
+        try {
+            g->ctx = c;
+            g->device = c->device;
+            g->net.init(c, params);
+        } catch (...) {
+            delete g;
+            throw;
+        }
+        *out = g;
+        return (int)MPHY_OK;
+    });
+}
+
+int mphy_gnn_destroy(mphy_gnn* g) {
+    if (!g) return MPHY_OK;
+    cudaSetDevice(g->device);
+    cudaDeviceSynchronize();
+    delete g;
+    return MPHY_OK;
+}
+
+int mphy_gnn_get_params(mphy_gnn* g, float* p) {
+    return guarded([&] {
+        MPHY_REQUIRE(g && p, MPHY_ERR_INVALID_ARG, "null argument");
+        g->net.get_params(p);
+        return (int)MPHY_OK;
+    });
+}
+
+int mphy_gnn_set_params(mphy_gnn* g, const float* p) {
+    return guarded([&] {
+        MPHY_REQUIRE(g && p, MPHY_ERR_INVALID_ARG, "null argument");
+        g->net.set_params(p);
+        return (int)MPHY_OK;
+    });
+}
+
+namespace {
+// exact block FSAI of the assembled operator as the training target, features, forward/backward
+double gnn_loss(mphy_gnn* g, mphy_solver* s, bool grad) {
+    MPHY_REQUIRE(s->use_fsai, MPHY_ERR_STATE, "the solver needs pc_type MPHY_PC_FSAI or MPHY_PC_FSAI_LEARNED");
+    MPHY_REQUIRE(s->state == MPHY_ASSEMBLY_OK || s->state == MPHY_FACTORISE_OK, MPHY_ERR_STATE,
+                 "assemble the matrix first");
+    cudaStream_t st = s->ctx->stream;
+    const void* aval = s->mixed ? (const void*)s->valf.p : (const void*)s->val.p;
+    if (s->mixed) s->fsai.compute<float>(s->valf.p, s->diag64.p, s->mesh->fixed.p, st);
+    else s->fsai.compute<double>(s->val.p, nullptr, nullptr, st);
+    DevBuf<float> blocks(9 * (size_t)s->fsai.lower().n_blocks);
+    s->fsai.get_lower_values(blocks.p, st);
+    g->net.build_graph(s->graph, s->pat, s->fsai, s->A, aval, s->mixed, s->mesh->fixed.p, blocks.p, st);
+    if (grad) g->net.zero_grads(st);
+    const double loss = g->net.run(s->graph, s->pat, s->fsai, s->A, aval, s->mixed, s->mesh->fixed.p, nullptr, grad, st);
+    MPHY_CUDA(cudaStreamSynchronize(st));
+    return loss;
+}
+}  // namespace
+
+int mphy_gnn_loss_and_grads(mphy_gnn* g, mphy_solver* s, double* loss, float* grads) {
+    return guarded([&] {
+        MPHY_REQUIRE(g && s && loss, MPHY_ERR_INVALID_ARG, "null argument");
+        *loss = gnn_loss(g, s, true);
+        if (grads) g->net.get_grads(grads);
+        return (int)MPHY_OK;
+    });
+}
+
+int mphy_gnn_train_step(mphy_gnn* g, mphy_solver* s, float lr, double* loss) {
+    return guarded([&] {
+        MPHY_REQUIRE(g && s, MPHY_ERR_INVALID_ARG, "null argument");
+        const double l = gnn_loss(g, s, true);
+        g->net.adam_step(lr, 0.9f, 0.999f, 1e-8f, s->ctx->stream);
+        MPHY_CUDA(cudaStreamSynchronize(s->ctx->stream));
+        if (loss) *loss = l;
+        return (int)MPHY_OK;
+    });
+}
+
+int mphy_gnn_predict(mphy_gnn* g, mphy_solver* s, float* ms) {
+    return guarded([&] {
+        MPHY_REQUIRE(g && s, MPHY_ERR_INVALID_ARG, "null argument");
+        MPHY_REQUIRE(s->use_fsai, MPHY_ERR_STATE, "the solver needs pc_type MPHY_PC_FSAI or MPHY_PC_FSAI_LEARNED");
+        MPHY_REQUIRE(s->state == MPHY_ASSEMBLY_OK || s->state == MPHY_FACTORISE_OK, MPHY_ERR_STATE,
+                     "assemble the matrix first");
+        cudaStream_t st = s->ctx->stream;
+        const void* aval = s->mixed ? (const void*)s->valf.p : (const void*)s->val.p;
+        MPHY_CUDA(cudaEventRecord(s->ctx->ev0, st));
+        g->net.build_graph(s->graph, s->pat, s->fsai, s->A, aval, s->mixed, s->mesh->fixed.p, nullptr, st);
+        DevBuf<float> blocks(9 * (size_t)s->fsai.lower().n_blocks);
+        g->net.run(s->graph, s->pat, s->fsai, s->A, aval, s->mixed, s->mesh->fixed.p, blocks.p, false, st);
+        s->fsai.set_lower_values(blocks.p, st);
+        MPHY_CUDA(cudaEventRecord(s->ctx->ev1, st));
+        MPHY_CUDA(cudaEventSynchronize(s->ctx->ev1));
+        float t = 0.f;
+        cudaEventElapsedTime(&t, s->ctx->ev0, s->ctx->ev1);
+        if (ms) *ms = t;
+        s->launches += g->net.launches + 5;
+        return (int)MPHY_OK;
+    });
+}
+
+int mphy_solver_attach_gnn(mphy_solver* s, mphy_gnn* g) {
+    if (!s) return MPHY_ERR_INVALID_ARG;
+    s->gnn = g;
+    return MPHY_OK;
+}
 }  // extern "C"

@@ -1,0 +1,102 @@
+"""FP64 restatement of the learned-FSAI network (mphyfem_b200/csrc/gnn.cu) with torch autograd on
+the CPU. Test infrastructure only: the checker for the GPU forward and backward kernels.
+
+Features follow the GPU: A^ = D^{-1/2} A D^{-1/2} with prescribed DOFs as identity rows; node
+input = A^_nn (9), prescribed flags (3), (neighbours - 1) / 27; edge input = A^_nm; targets the
+exact FSAI blocks scaled by the column's sqrt(diag). Weights are rounded to BF16 as on the GPU.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+H, L, NIN = 64, 3, 13
+
+
+def layout():
+    off = {}
+    o = 0
+
+    def add(name, n):
+        nonlocal o
+        off[name] = (o, n)
+        o += n
+    add("w_in", H * NIN)
+    add("b_in", H)
+    for l in range(L):
+        add(f"U{l}", H * H)
+        add(f"V{l}", H * 9)
+        add(f"c{l}", H)
+        add(f"S{l}", H * H)
+        add(f"T{l}", H * H)
+        add(f"d{l}", H)
+    add("Wa", 9 * H)
+    add("Wb", 9 * H)
+    add("Wc", 81)
+    add("bo", 9)
+    return off, o
+
+
+def loss_and_grads(params, A_full, fixed, nbrs, lrow, lcol, gblocks):
+    """params: flat float32; A_full: scipy node-major operator; nbrs: ascending neighbour lists;
+    (lrow, lcol): lower pattern; gblocks: [n_lower, 3, 3] exact FSAI (unscaled).
+    Returns (loss, flat gradient, predicted unscaled blocks)."""
+    off, total = layout()
+    p32 = torch.tensor(np.asarray(params, np.float32))
+    pb = p32.to(torch.bfloat16).to(torch.float64).detach().requires_grad_(True)
+
+    def W(name, shape):
+        o, n = off[name]
+        return pb[o:o + n].view(*shape)
+
+    A = A_full.tocsr()
+    n_node = len(nbrs)
+    d = np.abs(A.diagonal())
+    s = np.where(d > 0, np.sqrt(d), 1.0)
+    fx = np.asarray(fixed).reshape(-1, 3).astype(np.float64)
+
+    def blk(n, m):
+        b = A[3 * n:3 * n + 3, 3 * m:3 * m + 3].toarray()
+        return b / np.outer(s[3 * n:3 * n + 3], s[3 * m:3 * m + 3])
+
+    x = np.zeros((n_node, NIN))
+    src, dst, e = [], [], []
+    for n in range(n_node):
+        x[n, :9] = blk(n, n).ravel()
+        x[n, 9:12] = fx[n]
+        x[n, 12] = (len(nbrs[n]) - 1) / 27.0
+        for m in nbrs[n]:
+            if m != n:
+                src.append(m)
+                dst.append(n)
+                e.append(blk(n, m).ravel())
+    deg = torch.tensor(np.maximum(np.array([len(nb) - 1 for nb in nbrs]), 1), dtype=torch.float64)
+    X = torch.tensor(x)
+    src_t, dst_t = torch.tensor(src), torch.tensor(dst)
+    E = torch.tensor(np.array(e))
+    h = torch.relu(X @ W("w_in", (H, NIN)).T + W("b_in", (H,)))
+    for l in range(L):
+        P = h @ W(f"U{l}", (H, H)).T
+        pre = P[src_t] + E @ W(f"V{l}", (H, 9)).T + W(f"c{l}", (H,))
+        msg = torch.zeros_like(h).index_add_(0, dst_t, torch.relu(pre)) / deg[:, None]
+        q = h @ W(f"S{l}", (H, H)).T + msg @ W(f"T{l}", (H, H)).T + W(f"d{l}", (H,))
+        h = h + torch.relu(q)
+    rows = np.repeat(np.arange(n_node), np.diff(lrow))
+    el = torch.tensor(np.array([blk(n, m).ravel() for n, m in zip(rows, lcol)]))
+    out = (h[torch.tensor(rows)] @ W("Wa", (9, H)).T + h[torch.tensor(lcol.astype(np.int64))] @ W("Wb", (9, H)).T
+           + el @ W("Wc", (9, 9)).T + W("bo", (9,)))
+    # entries with a prescribed row or column DOF are fixed to the identity (gnn.cu dec_fwd)
+    keep = np.ones((len(rows), 3, 3))
+    ident = np.zeros((len(rows), 3, 3))
+    for j, (n, m) in enumerate(zip(rows, lcol)):
+        keep[j] = 1.0 - np.maximum(fx[n][:, None], fx[m][None, :])
+        if n == m:
+            ident[j] = np.diag(fx[n])
+    keep_t, ident_t = torch.tensor(keep.reshape(-1, 9)), torch.tensor(ident.reshape(-1, 9))
+    out = out * keep_t + ident_t
+    scol = torch.tensor(np.stack([s[3 * m:3 * m + 3] for m in lcol]))          # [n_lower, 3]
+    tgt = torch.tensor(np.asarray(gblocks, np.float64).reshape(-1, 3, 3)) * scol[:, None, :]
+    loss = ((out.view(-1, 3, 3) - tgt) ** 2).mean()
+    loss.backward()
+    pred = (out.view(-1, 3, 3) / scol[:, None, :]).detach().numpy()
+    return float(loss.detach()), pb.grad.numpy().copy(), pred
