@@ -273,6 +273,57 @@ int mphy_newton_run(mphy_solver* s, const double* fext_host, const mphy_newton_o
                     double* disp_host, mphy_iter_stats* hist_host, int32_t max_hist,
                     int32_t* n_hist);
 
+/* ------------------------------------------------------------------ batched form
+ * Many independent problems as one block-diagonal union mesh: instance i owns the contiguous
+ * nodes [node_ptr[i], node_ptr[i+1]) and only elements among them. The solver s (Jacobi-PCG,
+ * FP64 or MPHY_PREC_MIXED values, FP64 vectors) is created on the union; assembly runs over the
+ * union, and the linear solves of all instances run in one persistent launch: each thread-block
+ * cluster takes instances from a work queue, largest first, and runs Jacobi-PCG (KSPCG semantics,
+ * s's rtol / abstol / dtol / norm_type) on each with cluster-wide reductions in distributed
+ * shared memory. The reference solves one problem per run (femSolidmechanics2.cpp:730-851); every
+ * instance here follows that loop on its own. */
+typedef struct mphy_batch mphy_batch;
+
+typedef struct mphy_batch_stats {
+    int32_t steps;            /* load steps completed */
+    int32_t graph_replays;    /* batch Newton iterations (one CUDA graph replay each) */
+    int64_t kernel_launches;  /* libmphy kernels in those replays */
+    float t_ms;               /* device time of the load stepping */
+} mphy_batch_stats;
+
+/* node_ptr_host: [n_inst+1], 0 = node_ptr[0] < ... < node_ptr[n_inst] = n_node. Fails with
+ * MPHY_ERR_INVALID_ARG when an element couples two instances. */
+int mphy_batch_create(mphy_solver* s, int32_t n_inst, const int32_t* node_ptr_host, mphy_batch** out);
+int mphy_batch_destroy(mphy_batch* b);
+/* Schedule of the persistent solve: CTAs per cluster (1, 2, 4, 8) and threads per CTA (128, 256,
+ * 512). The default is (1, 256); mphy_batch_autotune picks one by measurement. */
+int mphy_batch_set_schedule(mphy_batch* b, int32_t cluster, int32_t threads);
+int mphy_batch_get_schedule(const mphy_batch* b, int32_t* cluster, int32_t* threads);
+/* Times every schedule on the assembled system (solves capped at maxit iterations; maxit <= 0:
+ * complete solves, which also measures the load balance of the slowest instances) and keeps the
+ * fastest. Writes up to max_candidates rows (cluster, threads, ms); *n_candidates = rows tried. */
+int mphy_batch_autotune(mphy_batch* b, int32_t maxit, int32_t max_candidates, int32_t* n_candidates,
+                        int32_t* clusters, int32_t* threads, float* ms);
+/* Solve every instance on the assembled system (x = 0 start, solution in the solver's x) in one
+ * launch. Per instance (host arrays, each may be NULL): iterations, status, final / initial norm
+ * of the convergence test. maxit <= 0: the solver's max_it. *ms: device time. */
+int mphy_batch_solve(mphy_batch* b, int32_t maxit, int32_t* its_host, int32_t* status_host,
+                     double* relres_host, float* ms);
+/* Load stepping of every instance (lambda = t, steps of o->dt up to o->t_final / o->max_steps),
+ * each instance following mphy_newton_run on its own: its own load factor, Newton iterations,
+ * step cuts (halving dt and restoring the last converged state after det F < 0, divergence or
+ * max_newton iterations) and MPHY_ERR_TIME_STEP when dt falls below 1% of o->dt. One CUDA graph
+ * replay per batch Newton iteration. fext_host, disp_host: [3*n_node] union vectors (disp
+ * in/out). newton_its_host: [max_steps][n_inst] Newton solves of each converged step;
+ * krylov_its_host, status_host: [n_inst]. Any output may be NULL. */
+int mphy_batch_newton_run(mphy_batch* b, const double* fext_host, const mphy_newton_opts* o,
+                          double* disp_host, int32_t* newton_its_host, int32_t* krylov_its_host,
+                          int32_t* status_host, mphy_batch_stats* stats);
+/* After mphy_batch_newton_run, per instance: Newton solves in all steps (failed tries included),
+ * step cuts, converged steps, load factor reached. Any pointer may be NULL. */
+int mphy_batch_instance_info(mphy_batch* b, int32_t* newton_total_host, int32_t* cuts_host,
+                             int32_t* steps_done_host, double* t_host);
+
 #ifdef __cplusplus
 }
 #endif

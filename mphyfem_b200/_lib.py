@@ -60,6 +60,12 @@ class IterStats(C.Structure):
     ]
 
 
+class BatchStats(C.Structure):
+    _fields_ = [
+        ("steps", C.c_int32), ("graph_replays", C.c_int32), ("kernel_launches", C.c_int64), ("t_ms", C.c_float),
+    ]
+
+
 class MphyError(RuntimeError):
     def __init__(self, status: int, message: str):
         super().__init__(f"mphy status {status} ({status_string(status)}): {message}")
@@ -121,6 +127,14 @@ SIGNATURES = {
     "mphy_newton_iteration": (C.c_int, [_vp, _vp, _vp, C.c_double, C.c_double, C.POINTER(IterStats)]),
     "mphy_newton_iteration_host": (C.c_int, [_vp, _d, _d, C.c_double, C.c_double, C.POINTER(IterStats)]),
     "mphy_newton_run": (C.c_int, [_vp, _d, C.POINTER(NewtonOpts), _d, C.POINTER(IterStats), C.c_int32, _i32]),
+    "mphy_batch_create": (C.c_int, [_vp, C.c_int32, _i32, C.POINTER(_vp)]),
+    "mphy_batch_destroy": (C.c_int, [_vp]),
+    "mphy_batch_set_schedule": (C.c_int, [_vp, C.c_int32, C.c_int32]),
+    "mphy_batch_get_schedule": (C.c_int, [_vp, _i32, _i32]),
+    "mphy_batch_autotune": (C.c_int, [_vp, C.c_int32, C.c_int32, _i32, _i32, _i32, C.POINTER(C.c_float)]),
+    "mphy_batch_solve": (C.c_int, [_vp, C.c_int32, _i32, _i32, _d, C.POINTER(C.c_float)]),
+    "mphy_batch_instance_info": (C.c_int, [_vp, _i32, _i32, _i32, _d]),
+    "mphy_batch_newton_run": (C.c_int, [_vp, _d, C.POINTER(NewtonOpts), _d, _i32, _i32, _i32, C.POINTER(BatchStats)]),
 }
 
 _lib = None

@@ -326,3 +326,90 @@ class FemSolidmechanicsGpu:
         rows = np.array([[h.step, h.iter, h.rhs_norm, h.krylov_its, h.status, h.t_assembly_ms, h.t_solve_ms]
                          for h in hist[:n.value]], dtype=np.float64).reshape(-1, 7)
         return NewtonResult(disp=u, hist=rows, status=rc)
+
+
+class BatchGpu:
+    """The batched form: independent problems as one block-diagonal union (meshgen.batch_union),
+    assembled together and solved in one persistent launch (mphy_batch_*)."""
+
+    def __init__(self, problems, ctx: Context | None = None, union=None, **solver_opts):
+        from . import meshgen
+        self.ctx = ctx or Context(0)
+        self.problems = list(problems)
+        self.union = union if union is not None else meshgen.batch_union(self.problems)
+        self.node_ptr = np.ascontiguousarray(self.union.meta["inst_node_ptr"], np.int32)
+        self.mesh = Mesh(self.ctx, self.union)
+        self.pattern = Pattern(self.mesh)
+        opts = dict(rtol=1e-10, norm_type=1)
+        opts.update(solver_opts)
+        self.solver = SolverGpu(self.mesh, self.pattern, **opts)
+        self.lib = self.ctx.lib
+        h = C.c_void_p()
+        L.check(self.lib.mphy_batch_create(self.solver.h, len(self.node_ptr) - 1,
+                                           self.node_ptr.ctypes.data_as(L._i32), C.byref(h)))
+        self.h = h
+        self.n_inst = len(self.node_ptr) - 1
+
+    def schedule(self):
+        c, t = C.c_int32(), C.c_int32()
+        L.check(self.lib.mphy_batch_get_schedule(self.h, C.byref(c), C.byref(t)))
+        return c.value, t.value
+
+    def set_schedule(self, cluster: int, threads: int):
+        L.check(self.lib.mphy_batch_set_schedule(self.h, cluster, threads))
+
+    def autotune(self, maxit: int = 0):
+        """Times every schedule on the assembled system (maxit <= 0: complete solves); keeps the
+        fastest. Returns rows (cluster, threads, ms)."""
+        n = C.c_int32()
+        cl, th, ms = (C.c_int32 * 32)(), (C.c_int32 * 32)(), (C.c_float * 32)()
+        L.check(self.lib.mphy_batch_autotune(self.h, maxit, 32, C.byref(n), cl, th, ms))
+        return [(cl[i], th[i], ms[i]) for i in range(min(n.value, 32))]
+
+    def solve(self, maxit: int = 0):
+        """All instances' linear solves on the assembled system. Returns (its, status, relres, ms)."""
+        its = np.zeros(self.n_inst, np.int32)
+        st = np.zeros(self.n_inst, np.int32)
+        rel = np.zeros(self.n_inst, np.float64)
+        ms = C.c_float()
+        L.check(self.lib.mphy_batch_solve(self.h, maxit, its.ctypes.data_as(L._i32), st.ctypes.data_as(L._i32),
+                                          rel.ctypes.data_as(L._d), C.byref(ms)))
+        return its, st, rel, ms.value
+
+    def newton_run(self, max_newton: int = 10, tol_rel: float | None = None, tol_abs: float = 0.0,
+                   disp: np.ndarray | None = None):
+        """Load stepping of every instance. Returns dict(disp, newton_its [steps, n_inst],
+        krylov_its, status, stats)."""
+        p = self.union
+        o = L.NewtonOpts(p.dt, p.t_final, p.max_steps, max_newton, p.newton_rtol if tol_rel is None else tol_rel,
+                         tol_abs)
+        u = np.zeros(p.n_dof) if disp is None else np.array(disp, np.float64)
+        f = _np(p.fnodal, np.float64)
+        nits = np.zeros((p.max_steps, self.n_inst), np.int32)
+        kits = np.zeros(self.n_inst, np.int32)
+        st = np.zeros(self.n_inst, np.int32)
+        bs = L.BatchStats()
+        rc = self.lib.mphy_batch_newton_run(self.h, f.ctypes.data_as(L._d), C.byref(o), u.ctypes.data_as(L._d),
+                                            nits.ctypes.data_as(L._i32), kits.ctypes.data_as(L._i32),
+                                            st.ctypes.data_as(L._i32), C.byref(bs))
+        L.check(rc)
+        tot, cuts, done = (np.zeros(self.n_inst, np.int32) for _ in range(3))
+        tr = np.zeros(self.n_inst, np.float64)
+        L.check(self.lib.mphy_batch_instance_info(self.h, tot.ctypes.data_as(L._i32), cuts.ctypes.data_as(L._i32),
+                                                  done.ctypes.data_as(L._i32), tr.ctypes.data_as(L._d)))
+        return dict(disp=u, newton_its=nits[:bs.steps], krylov_its=kits, status=st, newton_total=tot, cuts=cuts,
+                    steps_done=done, t=tr,
+                    stats=dict(steps=bs.steps, graph_replays=bs.graph_replays, kernel_launches=bs.kernel_launches,
+                               t_ms=bs.t_ms))
+
+    def instance_slice(self, i: int):
+        """DOF range of instance i in the union vectors."""
+        return slice(3 * int(self.node_ptr[i]), 3 * int(self.node_ptr[i + 1]))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mphy_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()

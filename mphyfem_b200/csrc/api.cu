@@ -18,27 +18,12 @@
 #include "gnn.cuh"
 #include "krylov.cuh"
 #include "pattern.cuh"
+#include "solver.cuh"
 
 namespace mphy {
 
 thread_local std::string g_last_error;
 void set_error(const std::string& msg) { g_last_error = msg; }
-
-template <typename F>
-int guarded(F&& f) {
-    try {
-        return f();
-    } catch (const Error& e) {
-        set_error(e.msg);
-        return e.status;
-    } catch (const std::bad_alloc&) {
-        set_error("host allocation failed");
-        return MPHY_ERR_OUT_OF_MEMORY;
-    } catch (const std::exception& e) {
-        set_error(e.what());
-        return MPHY_ERR_CUDA;
-    }
-}
 
 std::mutex g_tables_mu;
 bool g_tables_done[64] = {false};
@@ -47,49 +32,7 @@ bool g_tables_done[64] = {false};
 
 using namespace mphy;
 
-// ------------------------------------------------------------------------------- solver struct
-struct mphy_solver {
-    mphy_ctx* ctx = nullptr;
-    int device = 0;
-    const mphy_mesh* mesh = nullptr;
-    mphy_pattern* pat = nullptr;
-    mphy_solver_opts opts{};
-    int state = MPHY_SOLVER_EMPTY;
-    int64_t launches = 0;  // libmphy kernels launched (running count)
-    SellView A{};
-    bool mixed = false;          // MPHY_PREC_MIXED: FP32 values + FP64 iterative refinement
-    DevBuf<double> val;          // SELL values, FP64 (plain method)
-    DevBuf<float> valf;          // SELL values, FP32 (mixed precision): off-diagonal blocks, unmasked
-    DevBuf<double> diag64;       // [n_node][9] FP64 diagonal blocks = -sum of the stored off-diagonals
-    DevBuf<double> rhs, reac, x; // [3*n_node]
-    DevBuf<unsigned long long> bad;
-    DevBuf<double> partials, scalar;
-    DevBuf<uint32_t> counter;
-    DevBuf<double> disp_tmp, fext_tmp, disp_prev;
-    PcgFp64 pcg;
-    IterativeRefinement<double> ir;       // MIXED
-    IterativeRefinement<float> ir32;      // MIXED_F32VEC
-    Fsai fsai;                            // MPHY_PC_FSAI*
-    CoarseSpace coarse;                   // coarse_aggregates > 0
-    mphy_gnn* gnn = nullptr;              // MPHY_PC_FSAI_LEARNED: network run before every solve
-    int32_t last_fallback = 0;            // the last solve fell back to Jacobi
-    int32_t first_status = 0, first_its = 0;  // the learned attempt of the last solve
-    double first_relres = 0.0;
-    GnnGraph graph;
-    bool use_coarse = false;
-    bool use_fsai = false;
-    double t_pc_ms = 0.0;                 // last preconditioner setup time
-    int32_t last_sweeps = 0;
-    double* pinned = nullptr;  // [0] norm, [1] bad as bits
-};
-
-struct mphy_gnn {
-    mphy_ctx* ctx = nullptr;
-    int device = 0;
-    Gnn net;
-};
-
-namespace {
+namespace mphy {
 
 void solver_zero(mphy_solver* s) {
     cudaStream_t st = s->ctx->stream;
@@ -120,9 +63,10 @@ ElemArgs elem_args(const mphy_mesh* m, const double* disp, int tangent, unsigned
     return a;
 }
 
-void solver_assemble(mphy_solver* s, const double* disp) {
+void solver_assemble(mphy_solver* s, const double* disp, uint8_t* bad_elem) {
     solver_zero(s);
     ElemArgs a = elem_args(s->mesh, disp, s->opts.tangent, s->bad.p);
+    a.bad_elem = bad_elem;
     a.e2v = s->pat->e2v.p;
     a.val = s->val.p;
     a.valf = s->mixed ? s->valf.p : nullptr;
@@ -151,6 +95,10 @@ double solver_norm_and_bad(mphy_solver* s, int64_t* first_bad) {
     if (first_bad) *first_bad = b == ULLONG_MAX ? -1 : (int64_t)b;
     return std::sqrt(s->pinned[0]);
 }
+
+}  // namespace mphy
+
+namespace {
 
 int solver_solve_once(mphy_solver* s, int32_t* its, double* fnorm);
 double true_relres(mphy_solver* s);

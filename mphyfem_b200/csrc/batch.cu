@@ -1,0 +1,823 @@
+// batch.cu -- the batched form: many independent problems solved together.
+//
+// The instances are one block-diagonal union mesh: instance i owns the contiguous nodes
+// [node_ptr[i], node_ptr[i+1]) and only elements among them. Assembly therefore runs over the
+// union in the single-problem kernels (one element launch for all instances), and the SELL
+// operator is block diagonal by construction.
+//
+// The linear solves of all instances run in ONE persistent launch (batch_pcg_kernel): a
+// thread-block cluster takes instances from a work queue (largest first), splits each
+// instance's block rows over its CTAs and runs Jacobi-PCG on it with KSPCG semantics per
+// instance (SolverPetsc.cpp:250-330 with -ksp_type cg -pc_type jacobi). The two reductions of an
+// iteration are cluster-wide: every CTA sums its rows, the partials meet in distributed shared
+// memory and every CTA adds them in rank order, so all CTAs hold bitwise the same scalars and
+// take the same branches. No grid-wide synchronisation, no per-iteration launches, and an
+// instance's iteration count does not hold up the others.
+//
+// Newton control is per instance and stays on the device (batch_check_kernel applies the
+// load-step loop's test of femSolidmechanics2.cpp:762-816 / femSolidmechanics1.cpp:616-636 to
+// every instance), so one Newton iteration of the whole batch -- assembly, forces, checks, solves,
+// update -- is a single CUDA graph replay with one small read-back.
+#include <cooperative_groups.h>
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+#include "solver.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace mphy {
+namespace {
+
+// Deterministic block sum (fixed butterfly per warp, fixed order across warps); valid in all
+// threads of warp 0.
+__device__ __forceinline__ double bsum(double v, double* sh) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        v = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    }
+    return v;
+}
+
+// Two sums over the whole cluster, returned identically in every thread of every CTA: each
+// CTA's partial goes to its shared slot, and after the cluster barrier every thread adds the
+// CTAs' slots in rank order. Slots alternate so that a slot is rewritten only after the next
+// barrier, by which time every CTA has read it.
+__device__ __forceinline__ void cluster_sum2(cg::cluster_group& cl, double& a, double& b, double (*slot)[2], int& par,
+                                             double* sh) {
+    a = bsum(a, sh);
+    b = bsum(b, sh);
+    if (threadIdx.x == 0) {
+        slot[par][0] = a;
+        slot[par][1] = b;
+    }
+    cl.sync();
+    double sa = 0.0, sb = 0.0;
+    const unsigned nb = cl.num_blocks();
+    for (unsigned c = 0; c < nb; ++c) {
+        const double* rs = cl.map_shared_rank(&slot[par][0], c);
+        sa += rs[0];
+        sb += rs[1];
+    }
+    par ^= 1;
+    a = sa;
+    b = sb;
+}
+
+struct BatchView {
+    const int32_t* node_ptr;  // [n_inst+1]
+    const int32_t* order;     // [n_inst] instances, largest first
+    int32_t n_inst;
+    const uint8_t* active;    // [n_inst] or null (all)
+    const double* b;
+    double *x, *r, *z, *p, *q, *dinv;
+    int32_t* its;             // [n_inst]
+    int32_t* status;
+    double* dp;               // final and initial residual norms of the convergence test
+    double* dp0;
+    int32_t* its_total;       // [n_inst] running sum over solves, or null
+    uint32_t* work;           // work-queue head, zero at launch
+    double rtol, abstol, dtol;
+    int32_t maxit, norm_type;
+};
+
+// y = (A p)_row, FP64 accumulation; p is read through L2 (written by other CTAs of the cluster)
+template <typename VT>
+__device__ __forceinline__ void row_apply(const SellView& A, const VT* __restrict__ val, const double* p, int64_t row,
+                                          double& y0, double& y1, double& y2) {
+    const int64_t s = row >> 5;
+    const int lane = (int)(row & 31);
+    const int64_t base = A.slice_base[s];
+    const int w = A.slice_width[s];
+    const int32_t* cp = A.col + base + lane;
+    const VT* vp = val + 9 * base + lane;
+    y0 = y1 = y2 = 0.0;
+#pragma unroll 2
+    for (int k = 0; k < w; ++k) {
+        const int64_t c = cp[32 * k];
+        const double x0 = __ldcg(p + 3 * c), x1 = __ldcg(p + 3 * c + 1), x2 = __ldcg(p + 3 * c + 2);
+        const VT* v = vp + 288 * (int64_t)k;
+        y0 += (double)v[0] * x0 + (double)v[32] * x1 + (double)v[64] * x2;
+        y1 += (double)v[96] * x0 + (double)v[128] * x1 + (double)v[160] * x2;
+        y2 += (double)v[192] * x0 + (double)v[224] * x1 + (double)v[256] * x2;
+    }
+    if (A.diag64) {
+        const double* D = A.diag64 + 9 * row;
+        const double x0 = __ldcg(p + 3 * row), x1 = __ldcg(p + 3 * row + 1), x2 = __ldcg(p + 3 * row + 2);
+        y0 += D[0] * x0 + D[1] * x1 + D[2] * x2;
+        y1 += D[3] * x0 + D[4] * x1 + D[5] * x2;
+        y2 += D[6] * x0 + D[7] * x1 + D[8] * x2;
+    }
+    if (A.fixed) {
+        if (A.fixed[3 * row]) y0 = __ldcg(p + 3 * row);
+        if (A.fixed[3 * row + 1]) y1 = __ldcg(p + 3 * row + 1);
+        if (A.fixed[3 * row + 2]) y2 = __ldcg(p + 3 * row + 2);
+    }
+}
+
+template <typename VT>
+__global__ void __launch_bounds__(512) batch_pcg_kernel(SellView A, const VT* __restrict__ val, BatchView v) {
+    cg::cluster_group cl = cg::this_cluster();
+    const int rank = (int)cl.block_rank(), nb = (int)cl.num_blocks();
+    __shared__ int job[2];
+    __shared__ double slot[2][2];
+    __shared__ double sh[32];
+    int jpar = 0, rpar = 0;
+    for (;;) {
+        if (rank == 0 && threadIdx.x == 0) job[jpar] = (int)atomicAdd(v.work, 1u);
+        cl.sync();
+        const int k = *cl.map_shared_rank(&job[jpar], 0);
+        jpar ^= 1;
+        if (k >= v.n_inst) break;
+        const int inst = v.order[k];
+        const int64_t n0 = v.node_ptr[inst], n1 = v.node_ptr[inst + 1];
+        // this CTA's rows: a multiple of 32 each, so a warp's rows are one slice where possible
+        const int64_t per = (((n1 - n0) + nb - 1) / nb + 31) & ~(int64_t)31;
+        const int64_t a0 = min(n1, n0 + per * rank), a1 = min(n1, a0 + per);
+        const int64_t d0 = 3 * a0, d1 = 3 * a1;
+        if (v.active && !v.active[inst]) {
+            for (int64_t i = d0 + threadIdx.x; i < d1; i += blockDim.x) v.x[i] = 0.0;
+            if (rank == 0 && threadIdx.x == 0) {
+                v.its[inst] = 0;
+                v.status[inst] = MPHY_OK;
+                v.dp[inst] = 0.0;
+                v.dp0[inst] = 0.0;
+            }
+            continue;
+        }
+        // x = 0, r = b, z = D^-1 r, p = z (PCJACOBI: a zero diagonal entry gives 1)
+        double rz = 0.0, nn = 0.0;
+        for (int64_t n = a0 + threadIdx.x; n < a1; n += blockDim.x) {
+            const uint32_t o = A.dvoff[n];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                double d = A.diag64 ? A.diag64[9 * n + 4 * c] : (o != 0xffffffffu ? (double)val[o + 32u * (4 * c)] : 0.0);
+                if (A.fixed && A.fixed[3 * n + c]) d = 1.0;
+                const double di = d != 0.0 ? 1.0 / d : 1.0;
+                const double bi = v.b[3 * n + c];
+                const double zi = di * bi;
+                v.dinv[3 * n + c] = di;
+                v.x[3 * n + c] = 0.0;
+                v.r[3 * n + c] = bi;
+                v.z[3 * n + c] = zi;
+                v.p[3 * n + c] = zi;
+                rz += bi * zi;
+                nn += v.norm_type ? bi * bi : zi * zi;
+            }
+        }
+        cluster_sum2(cl, rz, nn, slot, rpar, sh);  // also publishes p to the cluster
+        double dp = sqrt(nn);
+        const double dp0 = dp, ttol = fmax(v.rtol * dp, v.abstol);
+        int its = 0, status = MPHY_OK;
+        bool done = false;
+        if (dp != dp) {
+            status = MPHY_ERR_DIVERGED;
+            done = true;
+        } else if (dp <= ttol) {
+            done = true;
+        } else if (rz == 0.0) {
+            its = 1;
+            done = true;
+        } else if (v.maxit <= 0) {
+            status = MPHY_ERR_NOT_CONVERGED;
+            done = true;
+        }
+        while (!done) {
+            double pq = 0.0, unused = 0.0;
+            for (int64_t n = a0 + threadIdx.x; n < a1; n += blockDim.x) {
+                double y0, y1, y2;
+                row_apply<VT>(A, val, v.p, n, y0, y1, y2);
+                v.q[3 * n] = y0;
+                v.q[3 * n + 1] = y1;
+                v.q[3 * n + 2] = y2;
+                pq += v.p[3 * n] * y0 + v.p[3 * n + 1] * y1 + v.p[3 * n + 2] * y2;
+            }
+            cluster_sum2(cl, pq, unused, slot, rpar, sh);
+            if (!(pq > 0.0)) {  // KSP_DIVERGED_INDEFINITE_MAT (or NaN); the iteration counts
+                its += 1;
+                status = pq != pq ? MPHY_ERR_DIVERGED : MPHY_ERR_INDEFINITE;
+                break;
+            }
+            const double alpha = rz / pq;
+            double rz1 = 0.0, nn1 = 0.0;
+            for (int64_t i = d0 + threadIdx.x; i < d1; i += blockDim.x) {
+                const double ri = v.r[i] - alpha * v.q[i];
+                const double zi = v.dinv[i] * ri;
+                v.x[i] += alpha * v.p[i];
+                v.r[i] = ri;
+                v.z[i] = zi;
+                rz1 += ri * zi;
+                nn1 += v.norm_type ? ri * ri : zi * zi;
+            }
+            cluster_sum2(cl, rz1, nn1, slot, rpar, sh);
+            its += 1;
+            dp = sqrt(nn1);
+            if (dp != dp) {
+                status = MPHY_ERR_DIVERGED;
+                break;
+            }
+            if (dp <= ttol) break;
+            if (dp >= v.dtol * dp0) {
+                status = MPHY_ERR_DIVERGED;
+                break;
+            }
+            if (its >= v.maxit) {
+                status = MPHY_ERR_NOT_CONVERGED;
+                break;
+            }
+            if (rz1 == 0.0) {  // the next iteration would stop at once with beta == 0
+                its += 1;
+                break;
+            }
+            const double beta = rz1 / rz;
+            rz = rz1;
+            for (int64_t i = d0 + threadIdx.x; i < d1; i += blockDim.x) v.p[i] = v.z[i] + beta * v.p[i];
+            cl.sync();  // the new direction, visible to every CTA of the cluster
+        }
+        if (rank == 0 && threadIdx.x == 0) {
+            v.its[inst] = its;
+            v.status[inst] = status;
+            v.dp[inst] = dp;
+            v.dp0[inst] = dp0;
+            if (v.its_total) v.its_total[inst] += its;
+        }
+    }
+    cl.sync();  // no CTA leaves while another may still read its shared memory
+}
+
+// Per-instance load stepping, one CTA per instance: the loop of femSolidmechanics2.cpp:730-851
+// (as mphy_newton_run runs it) as a state machine advanced once per batch Newton iteration.
+//   RUNNING, iteration it of the step at load factor t:
+//     forces: R += t Fext (free DOFs); ||R||
+//     it > max_newton, det F < 0 in an element, or divergence (it > 3, NaN or ratio > 1e7)
+//         -> failed step: disp = last converged state, t -= dt, dt /= 2 (MyTime::cut), below
+//            1% of the first dt the instance stops with MPHY_ERR_TIME_STEP; else retry at t + dt
+//     ||R|| < max(tol_abs, tol_rel ||R||_it=1)  -> converged step: the next one starts at t + dt
+//            while t <= t_final - 1e-10 and fewer than max_steps steps are done
+//     otherwise                                 -> solve this iteration (active)
+enum : int32_t { kRunning = 0, kDone = 1, kFailed = 2 };
+
+struct NewtonView {
+    const int32_t* node_ptr;
+    const int32_t* elem_ptr;
+    const uint8_t* fixed;
+    const double* fext;
+    double* rhs;
+    double* disp;
+    double* disp_prev;
+    const uint8_t* bad_elem;
+    double* t;             // load factor of the current step
+    double* dt;
+    int32_t* steps_done;   // starts at 1, as the reference's counter
+    int32_t* it;           // Newton iterations solved in the current step
+    int32_t* phase;
+    int32_t* status;
+    double* tol;
+    double* norm;
+    int32_t* newton_total;
+    int32_t* cuts;
+    int32_t* step_rec;     // [max_steps][n_inst] solves of each completed step
+    uint8_t* active;
+    uint32_t* n_running;
+    uint32_t* n_active;
+    int32_t n_inst;
+    double dt0, t_final, tol_rel, tol_abs;
+    int32_t max_steps, max_newton;
+};
+
+__global__ void __launch_bounds__(256) batch_step_kernel(NewtonView v) {
+    __shared__ double sh[32];
+    __shared__ int action;  // 0 solve, 1 converged, 2 failed, 3 inactive
+    const int i = blockIdx.x;
+    if (v.phase[i] != kRunning) {
+        if (threadIdx.x == 0) v.active[i] = 0;
+        return;
+    }
+    const int64_t d0 = 3 * (int64_t)v.node_ptr[i], d1 = 3 * (int64_t)v.node_ptr[i + 1];
+    const double ti = v.t[i];
+    double s = 0.0;
+    for (int64_t k = d0 + threadIdx.x; k < d1; k += blockDim.x) {
+        const double r = v.fixed[k] ? v.rhs[k] : v.rhs[k] + ti * v.fext[k];
+        v.rhs[k] = r;
+        s += r * r;
+    }
+    int bad = 0;
+    for (int64_t e = v.elem_ptr[i] + threadIdx.x; e < v.elem_ptr[i + 1]; e += blockDim.x) bad |= v.bad_elem[e];
+    bad = __syncthreads_or(bad);
+    s = bsum(s, sh);
+    if (threadIdx.x == 0) {
+        const double norm = sqrt(s);
+        const int it = v.it[i] + 1;
+        const double prev = it == 1 ? -1.0 : v.norm[i];
+        v.norm[i] = norm;
+        int act;
+        if (it > v.max_newton || bad) {
+            act = 2;
+        } else {
+            if (it == 1) v.tol[i] = fmax(v.tol_abs, v.tol_rel * norm);
+            if (norm < v.tol[i]) act = 1;
+            else if (it > 3 && (norm != norm || (prev > -0.1 && norm / prev > 1.0e7))) act = 2;
+            else act = 0;
+        }
+        action = act;
+        if (act == 0) {
+            v.it[i] = it;
+            v.newton_total[i] += 1;
+        } else if (act == 1) {
+            const int done = v.steps_done[i];
+            if (done - 1 < v.max_steps) v.step_rec[(int64_t)(done - 1) * v.n_inst + i] = it - 1;
+            v.steps_done[i] = done + 1;
+            if (ti <= v.t_final - 1.0e-10 && done + 1 <= v.max_steps) {
+                v.t[i] = ti + v.dt[i];
+                v.it[i] = 0;
+            } else {
+                v.phase[i] = kDone;
+                action = 3;
+            }
+        } else {
+            const double dt_old = v.dt[i], dt = 0.5 * dt_old;
+            v.cuts[i] += 1;
+            v.dt[i] = dt;
+            if (dt < v.dt0 * 0.01) {
+                v.phase[i] = kFailed;
+                v.status[i] = MPHY_ERR_TIME_STEP;
+                action = 4;  // restore the last converged state and stop
+            } else {
+                v.t[i] = (ti - dt_old) + dt;  // t -= dt; dt *= 0.5; then the next try's t += dt
+                v.it[i] = 0;
+            }
+        }
+        v.active[i] = act == 0;
+        if (act == 0) atomicAdd(v.n_active, 1u);
+        if (v.phase[i] == kRunning) atomicAdd(v.n_running, 1u);
+    }
+    __syncthreads();
+    const int act = action;
+    if (act == 1) {  // a new step starts from the converged state (saveSolution)
+        for (int64_t k = d0 + threadIdx.x; k < d1; k += blockDim.x) v.disp_prev[k] = v.disp[k];
+    } else if (act == 2 || act == 4) {  // SolutionDataSolid::reset
+        for (int64_t k = d0 + threadIdx.x; k < d1; k += blockDim.x) v.disp[k] = v.disp_prev[k];
+    }
+}
+
+}  // namespace
+}  // namespace mphy
+
+// ------------------------------------------------------------------------------- batch handle
+struct mphy_batch {
+    mphy_solver* s = nullptr;
+    int32_t n_inst = 0;
+    std::vector<int32_t> node_ptr_host;
+    DevBuf<int32_t> node_ptr, order;
+    DevBuf<double> r, z, p, q, dinv;
+    DevBuf<int32_t> its, status, its_total;
+    DevBuf<double> dp, dp0;
+    DevBuf<uint32_t> work;
+    // load-stepping state (NewtonView)
+    DevBuf<int32_t> steps_done, it, phase, nstatus, newton_total, cuts, step_rec;
+    DevBuf<double> t, dt, tol, norm;
+    DevBuf<uint8_t> active, bad_elem;
+    DevBuf<uint32_t> counters;  // [0] running, [1] active
+    DevBuf<double> disp, disp_prev, fext;
+    DevBuf<int32_t> elem_ptr;
+    int32_t rec_steps = 0;
+    int32_t cluster = 1, threads = 256;
+    cudaGraphExec_t graph = nullptr;
+    int graph_cluster = 0, graph_threads = 0;
+    double graph_key[6] = {0, 0, 0, 0, 0, 0};
+    int64_t launches = 0;
+    uint32_t* pinned = nullptr;  // [0] instances still running, [1] instances solved in the last iteration
+};
+
+namespace {
+
+using namespace mphy;
+
+BatchView batch_view(mphy_batch* b, const uint8_t* active, bool totals, int maxit) {
+    mphy_solver* s = b->s;
+    BatchView v{};
+    v.node_ptr = b->node_ptr.p;
+    v.order = b->order.p;
+    v.n_inst = b->n_inst;
+    v.active = active;
+    v.b = s->rhs.p;
+    v.x = s->x.p;
+    v.r = b->r.p;
+    v.z = b->z.p;
+    v.p = b->p.p;
+    v.q = b->q.p;
+    v.dinv = b->dinv.p;
+    v.its = b->its.p;
+    v.status = b->status.p;
+    v.dp = b->dp.p;
+    v.dp0 = b->dp0.p;
+    v.its_total = totals ? b->its_total.p : nullptr;
+    v.work = b->work.p;
+    v.rtol = s->opts.rtol;
+    v.abstol = s->opts.abstol;
+    v.dtol = s->opts.dtol;
+    v.maxit = maxit;
+    v.norm_type = s->opts.norm_type;
+    return v;
+}
+
+template <typename VT>
+void launch_pcg(mphy_batch* b, const VT* val, const BatchView& v, cudaStream_t st, int cluster, int threads) {
+    cudaLaunchConfig_t cfg{};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.blockDim = dim3(threads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cfg.gridDim = dim3(cluster);
+    int max_clusters = 0;
+    MPHY_CUDA(cudaOccupancyMaxActiveClusters(&max_clusters, batch_pcg_kernel<VT>, &cfg));
+    MPHY_REQUIRE(max_clusters > 0, MPHY_ERR_UNSUPPORTED, "batched solve: this cluster shape cannot be resident");
+    const int n_clusters = std::min(max_clusters, b->n_inst);
+    cfg.gridDim = dim3((unsigned)(n_clusters * cluster));
+    MPHY_CUDA(cudaMemsetAsync(b->work.p, 0, sizeof(uint32_t), st));
+    MPHY_CUDA(cudaLaunchKernelEx(&cfg, batch_pcg_kernel<VT>, b->s->A, val, v));
+    b->launches += 1;
+}
+
+void run_pcg(mphy_batch* b, const uint8_t* active, bool totals, int maxit, cudaStream_t st, int cluster, int threads) {
+    const BatchView v = batch_view(b, active, totals, maxit);
+    if (b->s->mixed) launch_pcg<float>(b, b->s->valf.p, v, st, cluster, threads);
+    else launch_pcg<double>(b, b->s->val.p, v, st, cluster, threads);
+}
+
+bool schedule_ok(int cluster, int threads) {
+    return (cluster == 1 || cluster == 2 || cluster == 4 || cluster == 8) && (threads == 128 || threads == 256 || threads == 512);
+}
+
+// One Newton iteration of every instance: assembly, per-instance forces / tests / step
+// control, the persistent solve of the active instances, disp += x.
+void newton_body(mphy_batch* b, const NewtonView& nv, cudaStream_t st) {
+    mphy_solver* s = b->s;
+    const int64_t nd = 3 * (int64_t)s->mesh->n_node;
+    MPHY_CUDA(cudaMemsetAsync(b->bad_elem.p, 0, b->bad_elem.bytes(), st));
+    solver_assemble(s, b->disp.p, b->bad_elem.p);
+    MPHY_CUDA(cudaMemsetAsync(b->counters.p, 0, 2 * sizeof(uint32_t), st));
+    batch_step_kernel<<<b->n_inst, 256, 0, st>>>(nv);
+    run_pcg(b, b->active.p, true, s->opts.max_it, st, b->cluster, b->threads);
+    axpy_inplace(b->disp.p, s->x.p, 1.0, nd, st, s->ctx->sm_count);
+    MPHY_CUDA(cudaGetLastError());
+}
+
+}  // namespace
+
+extern "C" {
+
+int mphy_batch_create(mphy_solver* s, int32_t n_inst, const int32_t* node_ptr, mphy_batch** out) {
+    return guarded([&] {
+        MPHY_REQUIRE(s && node_ptr && out, MPHY_ERR_INVALID_ARG, "null argument");
+        MPHY_REQUIRE(n_inst > 0, MPHY_ERR_INVALID_ARG, "no instances");
+        MPHY_REQUIRE(s->opts.pc_type == MPHY_PC_JACOBI && s->opts.coarse_aggregates <= 0 &&
+                         s->opts.precision != MPHY_PREC_MIXED_F32VEC,
+                     MPHY_ERR_UNSUPPORTED, "batched solves use Jacobi-PCG with FP64 vectors");
+        MPHY_REQUIRE(s->mesh->n_node < INT32_MAX / 3, MPHY_ERR_UNSUPPORTED, "union mesh too large");
+        MPHY_REQUIRE(node_ptr[0] == 0 && node_ptr[n_inst] == s->mesh->n_node, MPHY_ERR_INVALID_ARG,
+                     "node_ptr must start at 0 and end at the node count");
+        for (int32_t i = 0; i < n_inst; ++i)
+            MPHY_REQUIRE(node_ptr[i + 1] > node_ptr[i], MPHY_ERR_INVALID_ARG, "empty or unordered instance");
+        // every element's nodes lie in one instance (the operator is block diagonal)
+        MPHY_CUDA(cudaSetDevice(s->device));
+        const mphy_mesh* m = s->mesh;
+        {
+            std::vector<int32_t> conn((size_t)m->n_elem * m->npe);
+            MPHY_CUDA(cudaMemcpy(conn.data(), m->conn.p, conn.size() * sizeof(int32_t), cudaMemcpyDeviceToHost));
+            std::vector<int32_t> inst_of(m->n_node);
+            for (int32_t i = 0; i < n_inst; ++i)
+                for (int32_t n = node_ptr[i]; n < node_ptr[i + 1]; ++n) inst_of[n] = i;
+            for (int64_t e = 0; e < m->n_elem; ++e) {
+                const int32_t i0 = inst_of[conn[e * m->npe]];
+                for (int a = 1; a < m->npe; ++a)
+                    MPHY_REQUIRE(inst_of[conn[e * m->npe + a]] == i0, MPHY_ERR_INVALID_ARG,
+                                 "an element couples two instances");
+            }
+        }
+        auto* b = new mphy_batch;
+        try {
+            b->s = s;
+            b->n_inst = n_inst;
+            b->node_ptr_host.assign(node_ptr, node_ptr + n_inst + 1);
+            std::vector<int32_t> order(n_inst);
+            std::iota(order.begin(), order.end(), 0);
+            std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t c) {
+                return node_ptr[a + 1] - node_ptr[a] > node_ptr[c + 1] - node_ptr[c];
+            });
+            cudaStream_t st = s->ctx->stream;
+            const size_t nd = 3 * (size_t)m->n_node, ni = (size_t)n_inst;
+            b->node_ptr.alloc(ni + 1);
+            b->node_ptr.upload(node_ptr, ni + 1, st);
+            b->order.alloc(ni);
+            b->order.upload(order.data(), ni, st);
+            for (DevBuf<double>* v : {&b->r, &b->z, &b->p, &b->q, &b->dinv}) v->alloc(nd);
+            for (DevBuf<int32_t>* v : {&b->its, &b->status, &b->its_total, &b->steps_done, &b->it, &b->phase,
+                                       &b->nstatus, &b->newton_total, &b->cuts})
+                v->alloc(ni);
+            for (DevBuf<double>* v : {&b->dp, &b->dp0, &b->t, &b->dt, &b->tol, &b->norm}) v->alloc(ni);
+            b->active.alloc(ni);
+            b->bad_elem.alloc((size_t)m->n_elem);
+            b->work.alloc(1);
+            b->counters.alloc(2);
+            {
+                // element ranges of the instances (elements of an instance need not be contiguous
+                // in general; the union generator makes them so, and the check below enforces it)
+                std::vector<int32_t> conn((size_t)m->n_elem * m->npe), eptr(ni + 1, 0);
+                MPHY_CUDA(cudaMemcpy(conn.data(), m->conn.p, conn.size() * sizeof(int32_t), cudaMemcpyDeviceToHost));
+                int32_t cur = 0;
+                for (int64_t e = 0; e < m->n_elem; ++e) {
+                    const int32_t n = conn[e * m->npe];
+                    while (cur < n_inst && n >= node_ptr[cur + 1]) eptr[++cur] = (int32_t)e;
+                    MPHY_REQUIRE(n >= node_ptr[cur], MPHY_ERR_INVALID_ARG,
+                                 "the elements of an instance must be contiguous and in instance order");
+                }
+                while (cur < n_inst) eptr[++cur] = m->n_elem;
+                b->elem_ptr.alloc(ni + 1);
+                b->elem_ptr.upload(eptr.data(), ni + 1, st);
+            }
+            MPHY_CUDA(cudaMemsetAsync(b->its_total.p, 0, ni * sizeof(int32_t), st));
+            MPHY_CUDA(cudaMallocHost(&b->pinned, 4 * sizeof(uint32_t)));
+            MPHY_CUDA(cudaStreamSynchronize(st));
+        } catch (...) {
+            if (b->pinned) cudaFreeHost(b->pinned);
+            delete b;
+            throw;
+        }
+        *out = b;
+        return (int)MPHY_OK;
+    });
+}
+
+int mphy_batch_destroy(mphy_batch* b) {
+    if (!b) return MPHY_OK;
+    cudaSetDevice(b->s->device);
+    cudaDeviceSynchronize();
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    if (b->pinned) cudaFreeHost(b->pinned);
+    delete b;
+    return MPHY_OK;
+}
+
+int mphy_batch_set_schedule(mphy_batch* b, int32_t cluster, int32_t threads) {
+    if (!b) return MPHY_ERR_INVALID_ARG;
+    if (!schedule_ok(cluster, threads)) {
+        set_error("schedule: cluster in {1,2,4,8}, threads in {128,256,512}");
+        return MPHY_ERR_INVALID_ARG;
+    }
+    b->cluster = cluster;
+    b->threads = threads;
+    return MPHY_OK;
+}
+
+int mphy_batch_get_schedule(const mphy_batch* b, int32_t* cluster, int32_t* threads) {
+    if (!b) return MPHY_ERR_INVALID_ARG;
+    if (cluster) *cluster = b->cluster;
+    if (threads) *threads = b->threads;
+    return MPHY_OK;
+}
+
+int mphy_batch_solve(mphy_batch* b, int32_t maxit, int32_t* its, int32_t* status, double* relres, float* ms) {
+    return guarded([&] {
+        MPHY_REQUIRE(b, MPHY_ERR_INVALID_ARG, "null argument");
+        mphy_solver* s = b->s;
+        MPHY_REQUIRE(s->state == MPHY_ASSEMBLY_OK || s->state == MPHY_FACTORISE_OK, MPHY_ERR_STATE,
+                     "batched solve: assemble first");
+        MPHY_CUDA(cudaSetDevice(s->device));
+        cudaStream_t st = s->ctx->stream;
+        MPHY_CUDA(cudaEventRecord(s->ctx->ev0, st));
+        run_pcg(b, nullptr, false, maxit > 0 ? maxit : s->opts.max_it, st, b->cluster, b->threads);
+        MPHY_CUDA(cudaEventRecord(s->ctx->ev1, st));
+        MPHY_CUDA(cudaEventSynchronize(s->ctx->ev1));
+        s->state = MPHY_FACTORISE_OK;
+        if (ms) cudaEventElapsedTime(ms, s->ctx->ev0, s->ctx->ev1);
+        const size_t ni = (size_t)b->n_inst;
+        if (its) b->its.download(its, ni, st);
+        if (status) b->status.download(status, ni, st);
+        if (relres) {
+            std::vector<double> dp(ni), dp0(ni);
+            b->dp.download(dp.data(), ni, st);
+            b->dp0.download(dp0.data(), ni, st);
+            MPHY_CUDA(cudaStreamSynchronize(st));
+            for (size_t i = 0; i < ni; ++i) relres[i] = dp0[i] > 0.0 ? dp[i] / dp0[i] : 0.0;
+        }
+        MPHY_CUDA(cudaStreamSynchronize(st));
+        return (int)MPHY_OK;
+    });
+}
+
+int mphy_batch_autotune(mphy_batch* b, int32_t maxit, int32_t max_candidates, int32_t* n_candidates,
+                        int32_t* clusters, int32_t* threads, float* ms) {
+    return guarded([&] {
+        MPHY_REQUIRE(b, MPHY_ERR_INVALID_ARG, "null argument");
+        mphy_solver* s = b->s;
+        MPHY_REQUIRE(s->state == MPHY_ASSEMBLY_OK || s->state == MPHY_FACTORISE_OK, MPHY_ERR_STATE,
+                     "autotune: assemble first (the candidates are timed on the assembled system)");
+        MPHY_CUDA(cudaSetDevice(s->device));
+        cudaStream_t st = s->ctx->stream;
+        const int cand_cl[4] = {1, 2, 4, 8}, cand_th[3] = {128, 256, 512};
+        float best = 1e30f;
+        int bc = b->cluster, bt = b->threads, k = 0;
+        for (int ci = 0; ci < 4; ++ci)
+            for (int ti = 0; ti < 3; ++ti) {
+                const int c = cand_cl[ci], t = cand_th[ti];
+                float t_ms = 0.f;
+                const int mi = maxit > 0 ? maxit : s->opts.max_it;
+                run_pcg(b, nullptr, false, mi, st, c, t);  // warm-up
+                MPHY_CUDA(cudaEventRecord(s->ctx->ev0, st));
+                run_pcg(b, nullptr, false, mi, st, c, t);
+                MPHY_CUDA(cudaEventRecord(s->ctx->ev1, st));
+                MPHY_CUDA(cudaEventSynchronize(s->ctx->ev1));
+                cudaEventElapsedTime(&t_ms, s->ctx->ev0, s->ctx->ev1);
+                if (k < max_candidates) {
+                    if (clusters) clusters[k] = c;
+                    if (threads) threads[k] = t;
+                    if (ms) ms[k] = t_ms;
+                }
+                ++k;
+                if (t_ms < best) {
+                    best = t_ms;
+                    bc = c;
+                    bt = t;
+                }
+            }
+        if (n_candidates) *n_candidates = k;
+        b->cluster = bc;
+        b->threads = bt;
+        s->state = MPHY_FACTORISE_OK;
+        return (int)MPHY_OK;
+    });
+}
+
+int mphy_batch_newton_run(mphy_batch* b, const double* fext_host, const mphy_newton_opts* o, double* disp_host,
+                          int32_t* newton_its, int32_t* krylov_its, int32_t* status, mphy_batch_stats* stats) {
+    return guarded([&] {
+        MPHY_REQUIRE(b && fext_host && o && disp_host, MPHY_ERR_INVALID_ARG, "null argument");
+        MPHY_REQUIRE(o->dt > 0.0 && o->max_steps > 0 && o->max_newton > 0, MPHY_ERR_INVALID_ARG, "bad Newton options");
+        mphy_solver* s = b->s;
+        MPHY_CUDA(cudaSetDevice(s->device));
+        cudaStream_t st = s->ctx->stream;
+        const size_t nd = 3 * (size_t)s->mesh->n_node, ni = (size_t)b->n_inst;
+        if (!b->disp.p) {
+            b->disp.alloc(nd);
+            b->disp_prev.alloc(nd);
+            b->fext.alloc(nd);
+        }
+        if (b->rec_steps != o->max_steps) {
+            b->step_rec.alloc((size_t)o->max_steps * ni);
+            b->rec_steps = o->max_steps;
+        }
+        b->disp.upload(disp_host, nd, st);
+        b->fext.upload(fext_host, nd, st);
+        MPHY_CUDA(cudaMemcpyAsync(b->disp_prev.p, b->disp.p, nd * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        {
+            // every instance starts its first step: t = dt, steps_done = 1
+            const std::vector<double> t0(ni, o->dt);
+            const std::vector<int32_t> one(ni, 1);
+            b->t.upload(t0.data(), ni, st);
+            b->dt.upload(t0.data(), ni, st);
+            b->steps_done.upload(one.data(), ni, st);
+            MPHY_CUDA(cudaStreamSynchronize(st));  // the host vectors above are about to go
+        }
+        const int32_t first_phase = o->t_final >= 1.0e-10 ? kRunning : kDone;
+        {
+            const std::vector<int32_t> ph(ni, first_phase);
+            b->phase.upload(ph.data(), ni, st);
+            MPHY_CUDA(cudaStreamSynchronize(st));
+        }
+        for (DevBuf<int32_t>* v : {&b->it, &b->nstatus, &b->newton_total, &b->cuts, &b->its_total})
+            MPHY_CUDA(cudaMemsetAsync(v->p, 0, ni * sizeof(int32_t), st));
+        MPHY_CUDA(cudaMemsetAsync(b->step_rec.p, 0, b->step_rec.bytes(), st));
+        NewtonView nv{};
+        nv.node_ptr = b->node_ptr.p;
+        nv.elem_ptr = b->elem_ptr.p;
+        nv.fixed = s->mesh->fixed.p;
+        nv.fext = b->fext.p;
+        nv.rhs = s->rhs.p;
+        nv.disp = b->disp.p;
+        nv.disp_prev = b->disp_prev.p;
+        nv.bad_elem = b->bad_elem.p;
+        nv.t = b->t.p;
+        nv.dt = b->dt.p;
+        nv.steps_done = b->steps_done.p;
+        nv.it = b->it.p;
+        nv.phase = b->phase.p;
+        nv.status = b->nstatus.p;
+        nv.tol = b->tol.p;
+        nv.norm = b->norm.p;
+        nv.newton_total = b->newton_total.p;
+        nv.cuts = b->cuts.p;
+        nv.step_rec = b->step_rec.p;
+        nv.active = b->active.p;
+        nv.n_running = b->counters.p;
+        nv.n_active = b->counters.p + 1;
+        nv.n_inst = b->n_inst;
+        nv.dt0 = o->dt;
+        nv.t_final = o->t_final;
+        nv.tol_rel = o->tol_rel;
+        nv.tol_abs = o->tol_abs;
+        nv.max_steps = o->max_steps;
+        nv.max_newton = o->max_newton;
+        const double key[6] = {o->dt, o->t_final, o->tol_rel, o->tol_abs, (double)o->max_steps, (double)o->max_newton};
+        // the graph of one batch Newton iteration (rebuilt when the schedule or the options change)
+        if (b->graph && (b->graph_cluster != b->cluster || b->graph_threads != b->threads ||
+                         std::memcmp(b->graph_key, key, sizeof(key)) != 0)) {
+            MPHY_CUDA(cudaGraphExecDestroy(b->graph));
+            b->graph = nullptr;
+        }
+        if (!b->graph) {
+            solver_assemble(s, b->disp.p, b->bad_elem.p);  // outside the capture: first-use kernel attributes
+            cudaGraph_t g = nullptr;
+            MPHY_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            try {
+                newton_body(b, nv, st);
+            } catch (...) {
+                cudaStreamEndCapture(st, &g);
+                if (g) cudaGraphDestroy(g);
+                throw;
+            }
+            MPHY_CUDA(cudaStreamEndCapture(st, &g));
+            const cudaError_t e = cudaGraphInstantiate(&b->graph, g, 0);
+            cudaGraphDestroy(g);
+            MPHY_CUDA(e);
+            b->graph_cluster = b->cluster;
+            b->graph_threads = b->threads;
+            std::memcpy(b->graph_key, key, sizeof(key));
+        }
+        // prescribed diagonal (FP64) or diagonal rebuild (mixed), element, step control, solve, update
+        const int64_t body_launches = 5;
+        // every instance needs at most max_steps converged steps and 7 consecutive cuts per step,
+        // each costing at most max_newton + 1 iterations
+        const int64_t cap = 8LL * o->max_steps * (o->max_newton + 1) + 8;
+        mphy_batch_stats bs{};
+        int rc = MPHY_OK;
+        MPHY_CUDA(cudaEventRecord(s->ctx->ev0, st));
+        if (first_phase == kRunning) {
+            for (int64_t round = 0;; ++round) {
+                if (round >= cap) {
+                    rc = MPHY_ERR_NOT_CONVERGED;
+                    set_error("batched load stepping: iteration cap reached");
+                    break;
+                }
+                MPHY_CUDA(cudaGraphLaunch(b->graph, st));
+                bs.graph_replays += 1;
+                bs.kernel_launches += body_launches;
+                MPHY_CUDA(cudaMemcpyAsync(b->pinned, b->counters.p, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+                MPHY_CUDA(cudaStreamSynchronize(st));
+                if (b->pinned[0] == 0) break;
+            }
+        }
+        MPHY_CUDA(cudaEventRecord(s->ctx->ev1, st));
+        MPHY_CUDA(cudaEventSynchronize(s->ctx->ev1));
+        cudaEventElapsedTime(&bs.t_ms, s->ctx->ev0, s->ctx->ev1);
+        b->disp.download(disp_host, nd, st);
+        if (newton_its) b->step_rec.download(newton_its, (size_t)o->max_steps * ni, st);
+        if (krylov_its) b->its_total.download(krylov_its, ni, st);
+        if (status) b->nstatus.download(status, ni, st);
+        std::vector<int32_t> sd(ni);
+        b->steps_done.download(sd.data(), ni, st);
+        MPHY_CUDA(cudaStreamSynchronize(st));
+        bs.steps = sd.empty() ? 0 : *std::max_element(sd.begin(), sd.end()) - 1;
+        s->state = MPHY_FACTORISE_OK;
+        if (stats) *stats = bs;
+        return rc;
+    });
+}
+
+int mphy_batch_instance_info(mphy_batch* b, int32_t* newton_total, int32_t* cuts, int32_t* steps_done, double* t) {
+    return guarded([&] {
+        MPHY_REQUIRE(b, MPHY_ERR_INVALID_ARG, "null argument");
+        MPHY_CUDA(cudaSetDevice(b->s->device));
+        cudaStream_t st = b->s->ctx->stream;
+        const size_t ni = (size_t)b->n_inst;
+        if (newton_total) b->newton_total.download(newton_total, ni, st);
+        if (cuts) b->cuts.download(cuts, ni, st);
+        if (steps_done) {
+            b->steps_done.download(steps_done, ni, st);
+            MPHY_CUDA(cudaStreamSynchronize(st));
+            for (size_t i = 0; i < ni; ++i) steps_done[i] -= 1;
+        }
+        if (t) b->t.download(t, ni, st);
+        MPHY_CUDA(cudaStreamSynchronize(st));
+        return (int)MPHY_OK;
+    });
+}
+
+}  // extern "C"

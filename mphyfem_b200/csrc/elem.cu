@@ -259,7 +259,10 @@ __global__ void __launch_bounds__(kEpb * NPE) elem_fp64_kernel(ElemArgs a) {
                 for (int m = 0; m < 3; ++m) F[i][m] += s.u[I][i] * g0[m];
         }
         const double J = det3(F);
-        if (J < 0.0) atomicMin(a.bad, (unsigned long long)e);
+        if (J < 0.0) {
+            atomicMin(a.bad, (unsigned long long)e);
+            if (a.bad_elem) a.bad_elem[e] = 1;
+        }
         double b[3][3];
 #pragma unroll
         for (int i = 0; i < 3; ++i)

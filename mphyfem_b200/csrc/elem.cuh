@@ -13,6 +13,7 @@ struct ElemArgs {
     const double* disp;     // [n_node*3]
     int tangent;
     unsigned long long* bad;  // min element id with det F < 0 (init ULLONG_MAX)
+    uint8_t* bad_elem = nullptr;  // optional per-element flag (set to 1) for det F < 0
     // export (mode bit 1)
     double* Ke;
     double* Re;

@@ -267,3 +267,32 @@ def batched_blocks(n_inst: int = 512, seed: int = 11):
         q.meta.update({"mu": mu, "nu": nu, "traction_mag": tmag, "kappa": kappa})
         out.append(q)
     return out
+
+
+def batch_union(problems, name: str = "batch"):
+    """Disjoint union of problems as one mesh: instance i owns nodes
+    [inst_node_ptr[i], inst_node_ptr[i+1]), elements [inst_elem_ptr[i], inst_elem_ptr[i+1]) and
+    material rows [inst_mat_ptr[i], inst_mat_ptr[i+1]). The load stepping (dt, t_final,
+    max_steps) and tolerances are the first problem's; the instances must share npe."""
+    problems = list(problems)
+    assert problems and len({q.npe for q in problems}) == 1
+    nptr = np.zeros(len(problems) + 1, np.int64)
+    eptr = np.zeros(len(problems) + 1, np.int64)
+    mptr = np.zeros(len(problems) + 1, np.int64)
+    for i, q in enumerate(problems):
+        nptr[i + 1] = nptr[i] + q.n_node
+        eptr[i + 1] = eptr[i] + q.n_elem
+        mptr[i + 1] = mptr[i] + len(q.mats)
+    assert nptr[-1] < 2**31 // 3
+    coords = np.concatenate([q.coords for q in problems])
+    conn = np.concatenate([q.conn.astype(np.int64) + nptr[i] for i, q in enumerate(problems)]).astype(np.int32)
+    mat_id = np.concatenate([q.mat_id.astype(np.int64) + mptr[i] for i, q in enumerate(problems)]).astype(np.int32)
+    mats = np.concatenate([q.mats for q in problems])
+    fixed = np.concatenate([q.fixed for q in problems]).astype(np.uint8)
+    fnodal = np.concatenate([q.fnodal for q in problems])
+    q0 = problems[0]
+    return Problem(name=name, coords=coords, conn=conn, mat_id=mat_id, mats=mats, fixed=fixed, fnodal=fnodal,
+                   dt=q0.dt, t_final=q0.t_final, max_steps=q0.max_steps, newton_rtol=q0.newton_rtol,
+                   cg_rtol=q0.cg_rtol,
+                   meta={"inst_node_ptr": nptr.astype(np.int32), "inst_elem_ptr": eptr.astype(np.int32),
+                         "inst_mat_ptr": mptr.astype(np.int32), "n_inst": len(problems)})

@@ -1,0 +1,128 @@
+"""Batched form on the GPU: one persistent launch solves every instance of a block-diagonal
+union; each instance must get what it gets when solved alone (same Jacobi-PCG, same Newton
+rules), for every schedule the autotuner may pick.
+
+Tolerances: linear solves to rtol 1e-10 (true-residual norm), solutions within 1e-7 of the
+single-instance GPU solve and iteration counts within 2 (reduction order differs); Newton runs
+(to 1e-8) against the FP64 oracle within 1e-8 relative displacement, same Newton solves and cuts."""
+import numpy as np
+import pytest
+
+from mphyfem_b200 import meshgen
+
+pytestmark = pytest.mark.gpu
+
+SCHEDULES = [(1, 256), (2, 128), (4, 256), (8, 512)]
+
+
+@pytest.fixture(scope="module")
+def env():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no GPU")
+    from mphyfem_b200 import _lib, api, build
+    build.build()
+    return torch, api, _lib, api.Context(0)
+
+
+def small_batch(n, seed):
+    """Uneven cantilever blocks (a tiny one included: fewer block rows than CTAs in a cluster)."""
+    rng = np.random.default_rng(seed)
+    out = [meshgen.hex8_cantilever(2, 1, 1, mu=2.0, kappa=30.0, traction=(0, 0, -0.01))]
+    for i in range(n - 1):
+        nx, ny = (int(v) for v in rng.integers(2, 5, size=2))
+        nz = int(rng.integers(6, 17))
+        mu = float(np.exp(rng.uniform(np.log(0.1), np.log(10.0))))
+        nu = float(rng.uniform(0.30, 0.49))
+        kappa = 2.0 * mu * (1.0 + nu) / (3.0 * (1.0 - 2.0 * nu))
+        t = float(rng.uniform(0.01, 0.08)) * mu
+        out.append(meshgen.hex8_cantilever(nz, nx, ny, mu=mu, kappa=kappa, traction=(0.0, 0.0, -t)))
+    return out
+
+
+def _assemble(torch, sol, prob, lam=0.2):
+    sol.calcStiffnessAndResidual(torch.zeros(prob.n_dof, dtype=torch.float64, device="cuda"))
+    sol.addExternalForces(torch.tensor(prob.fnodal, device="cuda"), lam)
+
+
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "mixed"])
+def test_batch_solve_matches_single_instances(env, precision):
+    torch, api, _lib, ctx = env
+    probs = small_batch(12, seed=5)
+    b = api.BatchGpu(probs, ctx, precision=precision, rtol=1e-10, norm_type=1)
+    _assemble(torch, b.solver, b.union)
+    ref_its, ref_x = [], []
+    for q in probs:
+        mesh = api.Mesh(ctx, q)
+        s = api.SolverGpu(mesh, api.Pattern(mesh), precision=precision, rtol=1e-10, norm_type=1)
+        _assemble(torch, s, q)
+        rc, its, _ = s.factoriseAndSolve()
+        assert rc == 0
+        ref_its.append(its)
+        ref_x.append(s.solution().cpu().numpy())
+    for cl, th in SCHEDULES:
+        b.set_schedule(cl, th)
+        its, st, rel, ms = b.solve()
+        assert (st == 0).all(), st
+        assert (rel <= 1e-10).all()
+        x = b.solver.solution().cpu().numpy()
+        for i in range(len(probs)):
+            xi = x[b.instance_slice(i)]
+            assert abs(int(its[i]) - ref_its[i]) <= 2, (cl, th, i, its[i], ref_its[i])
+            assert np.linalg.norm(xi - ref_x[i]) <= 1e-7 * np.linalg.norm(ref_x[i]), (cl, th, i)
+
+
+def test_batch_newton_matches_oracle(env):
+    torch, api, _lib, ctx = env
+    from oracle.binding import OracleProblem, set_consistent_tangent
+    probs = small_batch(5, seed=9)
+    for q in probs:
+        q.newton_rtol = 1e-8  # the batched form's target; 1e-10 sits on the round-off floor here
+    # consistent tangent: quadratic Newton, so both sides converge in a few iterations per step
+    b = api.BatchGpu(probs, ctx, rtol=1e-12, norm_type=0, tangent=_lib.TANGENT_CONSISTENT)
+    out = b.newton_run(max_newton=15)
+    assert (out["status"] == 0).all(), out["status"]
+    assert out["stats"]["steps"] == 5
+    set_consistent_tangent(True)
+    try:
+        refs = [OracleProblem(q).newton(cg_rtol=1e-12, max_newton=15) for q in probs]
+    finally:
+        set_consistent_tangent(False)
+    for i, (u_ref, hist) in enumerate(refs):
+        ui = out["disp"][b.instance_slice(i)]
+        assert np.linalg.norm(ui - u_ref) <= 1e-8 * np.linalg.norm(u_ref), i
+        assert out["steps_done"][i] == 5
+        # Newton solves of the converged try of every step: the oracle records one row per
+        # iteration, a try restarts at iter 1, and its last row is the converged check. (A failed
+        # try wanders far from the solution, so where it ends depends on round-off: not compared.)
+        for step in range(1, 6):
+            rows = hist[hist[:, 0] == step]
+            last_try = rows[np.nonzero(rows[:, 1] == 1)[0][-1]:]
+            assert out["newton_its"][step - 1, i] == len(last_try) - 1, (i, step)
+        if i == 1:
+            assert out["cuts"][i] >= 1  # this instance's first try of step 1 ends in det F < 0
+
+
+def test_autotune_and_graph_rebuild(env):
+    torch, api, _lib, ctx = env
+    probs = small_batch(8, seed=3)
+    b = api.BatchGpu(probs, ctx, rtol=1e-10, norm_type=1, tangent=_lib.TANGENT_CONSISTENT)
+    _assemble(torch, b.solver, b.union)
+    rows = b.autotune(maxit=50)
+    assert len(rows) == 12 and all(ms > 0 for _, _, ms in rows)
+    best = min(rows, key=lambda r: r[2])
+    assert b.schedule() == best[:2]
+    ref = b.newton_run(max_newton=10)
+    b.set_schedule(1, 128)
+    other = b.newton_run(max_newton=10)
+    assert (ref["status"] == 0).all() and (other["status"] == 0).all()
+    assert np.linalg.norm(ref["disp"] - other["disp"]) <= 1e-9 * np.linalg.norm(ref["disp"])
+
+
+def test_coupled_instances_rejected(env):
+    torch, api, _lib, ctx = env
+    q = meshgen.hex8_cantilever(4, 1, 1)
+    u = meshgen.batch_union([q])
+    u.meta["inst_node_ptr"] = np.array([0, q.n_node // 2, q.n_node], np.int32)  # splits elements
+    with pytest.raises(_lib.MphyError):
+        api.BatchGpu([q], ctx, union=u)
