@@ -205,19 +205,29 @@ def run_reference(args):
 # ------------------------------------------------------------------------------------- GPU side
 def _method_name(args):
     parts = [{"fp64": "FP64", "mixed": "mixed FP32/FP64", "mixed32": "mixed FP32 vectors"}[args.precision],
-             {"jacobi": "Jacobi", "fsai": "FSAI"}[args.pc]]
+             {"jacobi": "Jacobi", "fsai": "FSAI", "learned": "learned FSAI"}[args.pc]]
     if args.coarse > 0:
         parts.append(f"+ rigid-body coarse space ({args.coarse} aggregates)")
     return " ".join(parts) + "-PCG"
 
 
+_GNN = []
+
+
 def _make_solver(api, _lib, mesh, pat, args, precision, pc, coarse):
-    return api.SolverGpu(mesh, pat, rtol=args.rtol, max_it=args.max_it,
-                         precision={"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED,
-                                    "mixed32": _lib.PREC_MIXED_F32VEC}[precision],
-                         pc_type={"jacobi": _lib.PC_JACOBI, "fsai": _lib.PC_FSAI}[pc],
-                         inner_rtol=args.inner_rtol, max_outer=args.max_outer, coarse_aggregates=coarse,
-                         norm_type=args.norm)
+    sol = api.SolverGpu(mesh, pat, rtol=args.rtol, max_it=args.max_it,
+                        precision={"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED,
+                                   "mixed32": _lib.PREC_MIXED_F32VEC}[precision],
+                        pc_type={"jacobi": _lib.PC_JACOBI, "fsai": _lib.PC_FSAI,
+                                 "learned": _lib.PC_FSAI_LEARNED}[pc],
+                        inner_rtol=args.inner_rtol, max_outer=args.max_outer, coarse_aggregates=coarse,
+                        norm_type=args.norm)
+    if pc == "learned":
+        from mphyfem_b200 import learned
+        if not _GNN:
+            _GNN.append(learned.Gnn(mesh.ctx, learned.load_params(args.gnn or learned.DEFAULT_WEIGHTS)))
+        _GNN[0].attach(sol)
+    return sol
 
 
 def _time_steps(torch, stream, step, steps, warmup):
@@ -282,6 +292,7 @@ def run_ours(args):
     launches = int(sum(s.kernel_launches for s in stats))
     relres = sol.true_residual()
     coarse = sol.coarse_info() if args.coarse > 0 else None
+    pc_info = sol.pc_last() if args.pc != "jacobi" else None
 
     # dominant kernel: the SpMV of the Krylov loop, timed standalone with events on its stream
     mi = sol.matrix_info()
@@ -356,6 +367,7 @@ def run_ours(args):
         "true_relres": relres,
         "solve_ms": solve_ms,
         "coarse": coarse,
+        "preconditioner_setup": pc_info,
         "assembly": {"ms": asm_ms, "melems_per_s": prob.n_elem / (asm_ms * 1e-3) / 1e6,
                      "algorithmic_bytes": asm_bytes, "achieved_gbs": asm_bytes / (asm_ms * 1e-3) / 1e9,
                      "frac": asm_bytes / (asm_ms * 1e-3) / 1e9 / peak},
@@ -386,8 +398,9 @@ def main():
     ap.add_argument("--rtol", type=float, default=1e-8)
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed", "mixed32"])
     ap.add_argument("--inner-rtol", dest="inner_rtol", type=float, default=0.0)
-    ap.add_argument("--max-outer", dest="max_outer", type=int, default=1)
-    ap.add_argument("--pc", default="jacobi", choices=["jacobi", "fsai"])
+    ap.add_argument("--max-outer", dest="max_outer", type=int, default=4)
+    ap.add_argument("--pc", default="jacobi", choices=["jacobi", "fsai", "learned"])
+    ap.add_argument("--gnn", default=None, help="weights of the learned FSAI (default: the packaged ones)")
     ap.add_argument("--norm", type=int, default=1, choices=[0, 1],
                     help="Krylov stopping norm: 1 = true residual ||b - Ax|| <= rtol ||b|| (every method compared "
                          "at the same accuracy), 0 = PETSc's preconditioned-residual default")

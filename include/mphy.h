@@ -80,9 +80,13 @@ typedef struct mphy_solver_opts {
     double rtol;           /* KSP rtol on the preconditioned residual norm */
     double abstol;         /* KSP abstol (PETSc default 1e-50) */
     double dtol;           /* KSP dtol (PETSc default 1e5) */
-    double inner_rtol;     /* MIXED*: inner PCG rtol per refinement sweep (<= 0: use rtol) */
-    int32_t max_outer;     /* MIXED*: refinement sweeps, each ending with the FP64 residual
-                            * b - A x; stops early once ||b - A x|| <= rtol ||b|| (default 1) */
+    double inner_rtol;     /* MIXED*: inner PCG rtol per refinement sweep (<= 0: rtol for the
+                            * first sweep, then what the sweep must remove to reach rtol ||b||
+                            * with a factor 2 to spare, capped at 0.5) */
+    int32_t max_outer;     /* refinement sweeps, each ending with the FP64 residual b - A x
+                            * (FP64 path too: against the drift of the CG recurrence residual);
+                            * stops early once ||b - A x|| <= rtol ||b|| (default 1: the KSP
+                            * solve alone, PETSc's behaviour) */
     int32_t chunk;         /* Krylov iterations per launched graph between host checks (0: auto) */
     int32_t coarse_aggregates; /* > 0: add the two-level rigid-body coarse correction
                                 * M^{-1} = D^{-1} + Z (Z^T A Z)^{-1} Z^T over about this many

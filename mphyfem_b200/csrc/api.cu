@@ -180,9 +180,53 @@ int solver_solve_once(mphy_solver* s, int32_t* its, double* fnorm) {
         s->launches += s->ir.launches;
         return rc;
     }
-    const int rc = s->pcg.solve(s->val.p, s->rhs.p, s->x.p, s->opts.rtol, s->opts.abstol, s->opts.dtol,
-                                s->opts.max_it, s->ctx->stream, its, fnorm);
+    int rc = s->pcg.solve(s->val.p, s->rhs.p, s->x.p, s->opts.rtol, s->opts.abstol, s->opts.dtol,
+                          s->opts.max_it, s->ctx->stream, its, fnorm);
     s->launches += s->pcg.launches;
+    s->last_sweeps = 1;
+    if (s->opts.max_outer <= 1 || rc == MPHY_ERR_INDEFINITE || rc == MPHY_ERR_DIVERGED) return rc;
+    // FP64 refinement sweeps: the recurrence residual of a long CG run drifts away from b - A x;
+    // x += PCG(A, b - A x) until the FP64 true residual meets rtol (the same loop as the mixed
+    // path, on the FP64 operator)
+    cudaStream_t st = s->ctx->stream;
+    const int sm = s->ctx->sm_count;
+    const int64_t n = 3 * (int64_t)s->mesh->n_node;
+    if (s->ref_r.n != (size_t)n) {
+        s->ref_r.alloc(n);
+        s->ref_d.alloc(n);
+    }
+    double bb = 0.0, rr = 0.0;
+    dot_fp64(s->rhs.p, s->rhs.p, n, s->partials.p, s->counter.p, s->scalar.p, st, sm);
+    MPHY_CUDA(cudaMemcpyAsync(&bb, s->scalar.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+    MPHY_CUDA(cudaStreamSynchronize(st));
+    const double bnorm = std::sqrt(bb);
+    int32_t total = its ? *its : 0;
+    double rel = 0.0;
+    for (int k = 1;; ++k) {
+        residual_fp64<double>(s->A, s->val.p, s->x.p, s->rhs.p, s->ref_r.p, s->partials.p, s->counter.p, s->scalar.p,
+                              st, sm);
+        s->launches += 1;
+        MPHY_CUDA(cudaMemcpyAsync(&rr, s->scalar.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+        MPHY_CUDA(cudaStreamSynchronize(st));
+        rel = bnorm > 0.0 ? std::sqrt(rr) / bnorm : 0.0;
+        if (!(rel > s->opts.rtol) || k >= s->opts.max_outer || total >= s->opts.max_it) break;
+        const double tol_in = std::fmin(0.5, std::fmax(s->opts.rtol, 0.5 * s->opts.rtol / rel));
+        int32_t it = 0;
+        double dn = 0.0;
+        const int rc2 = s->pcg.solve(s->val.p, s->ref_r.p, s->ref_d.p, tol_in, 0.0, s->opts.dtol,
+                                     s->opts.max_it - total, st, &it, &dn);
+        s->launches += s->pcg.launches + 1;
+        total += it;
+        axpy_inplace(s->x.p, s->ref_d.p, 1.0, n, st, sm);
+        s->last_sweeps = k + 1;
+        if (rc2 == MPHY_ERR_INDEFINITE || rc2 == MPHY_ERR_DIVERGED) {
+            rc = rc2;
+            break;
+        }
+    }
+    if (its) *its = total;
+    if (fnorm) *fnorm = rel;
+    if (rc == MPHY_OK || rc == MPHY_ERR_NOT_CONVERGED) rc = rel > s->opts.rtol ? MPHY_ERR_NOT_CONVERGED : MPHY_OK;
     return rc;
 }
 

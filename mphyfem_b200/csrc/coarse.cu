@@ -7,7 +7,8 @@
 //      blocks E[a][b] for its (at most 27) neighbour aggregates in shared memory -- every block
 //      of E is written by exactly one CTA, no atomics in global memory;
 //   3. E = L L^T by a right-looking blocked Cholesky (64x64 tiles, FP64), W = L^{-1} by blocked
-//      forward substitution, E^{-1} = W^T W, stored in FP32 for the per-iteration GEMV.
+//      forward substitution, E^{-1} = W^T W, kept in FP64 for the per-iteration GEMV (FP32
+//      rounding of the inverse of an ill-conditioned E can make it indefinite).
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -295,8 +296,8 @@ __global__ void __launch_bounds__(256) trtri_row(const double* E, double* W, int
         for (int r = 0; r < 4; ++r) W[(int64_t)(i * T + ty + 16 * q) * kp + j * T + tx + 16 * r] = -o[q][r];
 }
 
-// E^{-1} = W^T W (tile (i, j) = sum_{k >= max(i,j)} W_ki^T W_kj), stored FP32
-__global__ void __launch_bounds__(256) inverse_tiles(const double* W, float* einv, int kp, int nb) {
+// E^{-1} = W^T W (tile (i, j) = sum_{k >= max(i,j)} W_ki^T W_kj), stored FP64
+__global__ void __launch_bounds__(256) inverse_tiles(const double* W, double* einv, int kp, int nb) {
     extern __shared__ double sm[];
     double (*A)[TP] = reinterpret_cast<double (*)[TP]>(sm);
     double (*B)[TP] = reinterpret_cast<double (*)[TP]>(sm + T * TP);
@@ -314,7 +315,7 @@ __global__ void __launch_bounds__(256) inverse_tiles(const double* W, float* ein
         __syncthreads();
     }
     for (int q = 0; q < 4; ++q)
-        for (int r = 0; r < 4; ++r) einv[(int64_t)(i * T + ty + 16 * q) * kp + j * T + tx + 16 * r] = (float)acc[q][r];
+        for (int r = 0; r < 4; ++r) einv[(int64_t)(i * T + ty + 16 * q) * kp + j * T + tx + 16 * r] = acc[q][r];
 }
 
 }  // namespace

@@ -18,7 +18,7 @@ class CoarseSpace {
     // target_aggregates boxes, as close to cubes as the box allows.
     void init(mphy_ctx* ctx, const mphy_mesh* mesh, const mphy_pattern* pat, int target_aggregates);
     // Modes from the current coordinates X + disp (disp may be null), E = Z^T A Z, its Cholesky
-    // factor and inverse (FP64), stored in FP32.
+    // factor and inverse, all FP64.
     template <typename VT>
     void setup(const SellView& A, const VT* aval, const double* disp, cudaStream_t s);
     CoarseView view() const;
@@ -37,7 +37,7 @@ class CoarseSpace {
     DevBuf<int32_t> agg_, agg_nodes_, err_;
     DevBuf<int64_t> agg_ptr_;
     DevBuf<double> d_, cent_, E_, W_, w_, c_;
-    DevBuf<float> einv_;
+    DevBuf<double> einv_;
     DevBuf<uint8_t> drop_;
 };
 

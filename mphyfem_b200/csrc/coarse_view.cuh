@@ -13,7 +13,10 @@ struct CoarseView {
     const int32_t* agg_nodes;
     const double* d;         // [n_node][3] (x_n - c_agg) / H_agg at setup
     const uint8_t* fixed;    // [3 n_node]
-    const float* einv;       // [kp][kp] FP32 inverse of E (row-major)
+    // [kp][kp] inverse of E (row-major), FP64: with a large stiffness contrast E is so
+    // ill-conditioned that rounding its inverse to FP32 makes the coarse term indefinite, and CG
+    // on an indefinite preconditioner stalls
+    const double* einv;
     double* w;               // [kp] restriction Z^T r
     double* c;               // [kp] coarse correction E^{-1} w
 };

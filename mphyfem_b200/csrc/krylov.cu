@@ -430,15 +430,15 @@ __global__ void __launch_bounds__(kThreads) coarse_restrict_kernel(CoarseView cv
     }
 }
 
-// c = E^{-1} w: one warp per row of the FP32 inverse, FP64 accumulation
+// c = E^{-1} w: one warp per row of the FP64 inverse
 __global__ void __launch_bounds__(kThreads) coarse_gemv_kernel(CoarseView cv, const PcgState* st) {
     if (st && st->done) return;
     const int lane = threadIdx.x & 31;
     for (int64_t row = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; row < cv.kp;
          row += ((int64_t)gridDim.x * blockDim.x) >> 5) {
-        const float* e = cv.einv + row * cv.kp;
+        const double* e = cv.einv + row * cv.kp;
         double acc = 0.0;
-        for (int col = lane; col < cv.kp; col += 32) acc += (double)e[col] * cv.w[col];
+        for (int col = lane; col < cv.kp; col += 32) acc += e[col] * cv.w[col];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
         if (lane == 0) cv.c[row] = acc;
@@ -854,8 +854,11 @@ int IterativeRefinement<XT>::solve(const float* val, const double* b, double* x,
         to_inner(r64_.p, rin_.p, n_, gv, s);
         int32_t it = 0;
         double dn = 0.0;
-        const int st = inner_.solve(val, rin_.p, d_.p, inner_rtol > 0.0 ? inner_rtol : rtol, 0.0, 1e5, maxit - total,
-                                    s, &it, &dn);
+        // default inner tolerance: what this sweep must remove to reach rtol ||b|| (with a factor
+        // 2 to spare), never tighter than rtol: the first sweep solves to rtol, later sweeps only
+        // correct the drift of the recurrence residual
+        const double tol_in = inner_rtol > 0.0 ? inner_rtol : std::fmin(0.5, std::fmax(rtol, 0.5 * rtol / rel));
+        const int st = inner_.solve(val, rin_.p, d_.p, tol_in, 0.0, 1e5, maxit - total, s, &it, &dn);
         inner_status = st;
         launches += inner_.launches + 1;
         total += it;

@@ -213,19 +213,25 @@ def two_phase_inclusions(nx: int, ny: int, nz: int, seed: int = 23, vol_frac: fl
                         name=name or f"hex8_two_phase_{nx}x{ny}x{nz}")
     lx, ly, lz = 4.0, 1.0, 1.0
     rng = np.random.Generator(np.random.PCG64(seed))
-    centers, radii = [], []
+    cap = 1024
+    cen, rad, n = np.empty((cap, 3)), np.empty(cap), 0
     vol, target, tries = 0.0, vol_frac * lx * ly * lz, 0
     while vol < target and tries < max_tries:
         tries += 1
         r = rng.uniform(*r_range)
         c = rng.uniform([r, r, r], [lx - r, ly - r, lz - r])
-        if centers:
-            d = np.linalg.norm(np.asarray(centers) - c, axis=1)
-            if np.any(d < np.asarray(radii) + r):
+        if n:
+            d = np.linalg.norm(cen[:n] - c, axis=1)
+            if np.any(d < rad[:n] + r):
                 continue
-        centers.append(c)
-        radii.append(r)
+        if n == cap:
+            cap *= 2
+            cen = np.concatenate([cen, np.empty((cap - n, 3))])
+            rad = np.concatenate([rad, np.empty(cap - n)])
+        cen[n], rad[n] = c, r
+        n += 1
         vol += 4.0 / 3.0 * np.pi * r ** 3
+    centers, radii = list(cen[:n]), list(rad[:n])
     # element (i, j, k) of the structured grid has its centroid at ((i+.5)hx, (j+.5)hy, (k+.5)hz);
     # test only the cells inside each sphere's bounding box
     h = np.array([lx / nx, ly / ny, lz / nz])

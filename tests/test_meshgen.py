@@ -58,3 +58,27 @@ def test_batched_blocks_ranges():
         nz, nx, ny = q.meta["nx"], q.meta["ny"], q.meta["nz"]
         assert 16 <= nz <= 64 and 4 <= nx <= 16 and 4 <= ny <= 16
         assert 0.1 <= q.mats[0, 0] <= 10.0 and 0.30 <= q.meta["nu"] <= 0.49
+
+
+def _rsa_plain(seed, vol_frac, r_range, lx=4.0, ly=1.0, lz=1.0):
+    """List-based random sequential addition: the generator's placement, restated plainly."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    centers, radii, vol = [], [], 0.0
+    while vol < vol_frac * lx * ly * lz:
+        r = rng.uniform(*r_range)
+        c = rng.uniform([r, r, r], [lx - r, ly - r, lz - r])
+        if centers and np.any(np.linalg.norm(np.asarray(centers) - c, axis=1) < np.asarray(radii) + r):
+            continue
+        centers.append(c)
+        radii.append(r)
+        vol += 4.0 / 3.0 * np.pi * r ** 3
+    return len(radii), vol
+
+
+def test_two_phase_placement_is_the_seeded_rsa():
+    # the two-phase workload's layout (seed 23) and a training layout (seed 1000)
+    for seed in (23, 1000):
+        p = meshgen.two_phase_inclusions(32, 8, 8, seed=seed)
+        n, vol = _rsa_plain(seed, 0.2, (0.03, 0.08))
+        assert p.meta["n_spheres"] == n
+        assert abs(p.meta["vol_frac"] - vol / 4.0) < 1e-15
