@@ -28,7 +28,6 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-LAMBDA = 0.2
 METRIC = "Newton iters/s (hex8 Neo-Hookean cantilever 256x64x64, 3.26M DOFs, PCG to rtol 1e-8)"
 
 
@@ -47,15 +46,20 @@ def _workload(name: str):
         return meshgen.cantilever_small()
     if name == "two_phase":
         return meshgen.two_phase_inclusions(256, 64, 64, seed=23)
+    if name == "tet10":
+        # 10-node tets, Kuhn split of a 96(x) x 48 x 48 grid, kappa = 100, traction 0.02, dt 0.1
+        return meshgen.tet10_kuhn(96, 48, 48)
     return meshgen.cantilever_large()
 
 
 def _config(prob, rtol):
     return {
         "workload": f"{prob.name}: one Newton iteration (assembly + loads + norm + PCG to true relative residual {rtol:g} "
-                    f"+ update), lambda={LAMBDA}, u=0",
+                    f"+ update), lambda={prob.dt:g} (the first load step), u=0",
         "n_elem": prob.n_elem, "n_node": prob.n_node, "n_dof": prob.n_dof, "n_free": prob.n_free,
-        "element": ("hex8, 2x2x2 Gauss, compressible Neo-Hookean mu=1 kappa=10 (Utype 3)" if prob.mats.shape[0] == 1
+        "element": ("tet10, 4-point rule, near-incompressible Neo-Hookean mu=1 kappa=100 (Utype 3), jitter 0.1h seed 7"
+                    if prob.npe == 10 else
+                    "hex8, 2x2x2 Gauss, compressible Neo-Hookean mu=1 kappa=10 (Utype 3)" if prob.mats.shape[0] == 1
                     else "hex8, two-phase Neo-Hookean: matrix mu=1 kappa=10, spherical inclusions mu=1000 "
                          f"kappa=10000 ({prob.meta.get('stiff_elems')} elements, seed 23)"),
         "tangent": "reference (utilitiesmaterialHyperelastic.cpp as written)",
@@ -142,7 +146,7 @@ def cpu_newton_estimate(prob, gpu_its: int, rtol: float):
     b = meshgen.hex8_cantilever(96, 24, 24)
     ob = binding.OracleProblem(b)
     val, rhs, _, _ = ob.assemble(np.zeros(b.n_dof), nthreads=nthreads, want_reac=False)
-    rhs = rhs + LAMBDA * b.fnodal[np.flatnonzero(b.fixed == 0)]
+    rhs = rhs + b.dt * b.fnodal[np.flatnonzero(b.fixed == 0)]
     cg_its = 60
     t0 = time.perf_counter()
     ob.cg(val, rhs, rtol=1e-30, maxit=cg_its, nthreads=nthreads)
@@ -204,7 +208,8 @@ def run_reference(args):
 
 # ------------------------------------------------------------------------------------- GPU side
 def _method_name(args):
-    parts = [{"fp64": "FP64", "mixed": "mixed FP32/FP64", "mixed32": "mixed FP32 vectors"}[args.precision],
+    parts = [{"fp64": "FP64", "mixed": "mixed FP32/FP64", "mixed32": "mixed FP32 vectors",
+              "mixed_tc": "mixed FP32/FP64 (tensor-core split-BF16 tangent)"}[args.precision],
              {"jacobi": "Jacobi", "fsai": "FSAI", "learned": "learned FSAI"}[args.pc]]
     if args.coarse > 0:
         parts.append(f"+ rigid-body coarse space ({args.coarse} aggregates)")
@@ -217,7 +222,7 @@ _GNN = []
 def _make_solver(api, _lib, mesh, pat, args, precision, pc, coarse):
     sol = api.SolverGpu(mesh, pat, rtol=args.rtol, max_it=args.max_it,
                         precision={"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED,
-                                   "mixed32": _lib.PREC_MIXED_F32VEC}[precision],
+                                   "mixed32": _lib.PREC_MIXED_F32VEC, "mixed_tc": _lib.PREC_MIXED_TC}[precision],
                         pc_type={"jacobi": _lib.PC_JACOBI, "fsai": _lib.PC_FSAI,
                                  "learned": _lib.PC_FSAI_LEARNED}[pc],
                         inner_rtol=args.inner_rtol, max_outer=args.max_outer, coarse_aggregates=coarse,
@@ -271,7 +276,7 @@ def run_ours(args):
 
     def step():
         disp.zero_()
-        return sol.newton_iteration(disp, fext, LAMBDA)
+        return sol.newton_iteration(disp, fext, prob.dt)
 
     for _ in range(args.warmup):
         step()
@@ -320,11 +325,11 @@ def run_ours(args):
     disp_h = torch.zeros(prob.n_dof, dtype=torch.float64).pin_memory().numpy()
     fext_h = torch.tensor(prob.fnodal, dtype=torch.float64).pin_memory().numpy()
     e2e_steps = max(1, min(args.steps, 3))
-    sol.newton_iteration_host(disp_h, fext_h, LAMBDA)
+    sol.newton_iteration_host(disp_h, fext_h, prob.dt)
     e0.record(stream)
     for _ in range(e2e_steps):
         disp_h[:] = 0.0
-        sol.newton_iteration_host(disp_h, fext_h, LAMBDA)
+        sol.newton_iteration_host(disp_h, fext_h, prob.dt)
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1) / e2e_steps
@@ -339,7 +344,7 @@ def run_ours(args):
 
         def pstep():
             disp.zero_()
-            return psol.newton_iteration(disp, fext, LAMBDA)
+            return psol.newton_iteration(disp, fext, prob.dt)
 
         pms, pst = _time_steps(torch, pstream, pstep, max(1, min(args.steps, 2)), 1)
         plain = {"method": "FP64 Jacobi-PCG (plain)", "ms_per_newton_iter": pms / len(pst),
@@ -394,9 +399,9 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="large", choices=["large", "small", "two_phase"])
+    ap.add_argument("--workload", default="large", choices=["large", "small", "two_phase", "tet10"])
     ap.add_argument("--rtol", type=float, default=1e-8)
-    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed", "mixed32"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed", "mixed32", "mixed_tc"])
     ap.add_argument("--inner-rtol", dest="inner_rtol", type=float, default=0.0)
     ap.add_argument("--max-outer", dest="max_outer", type=int, default=4)
     ap.add_argument("--pc", default="jacobi", choices=["jacobi", "fsai", "learned"])

@@ -58,7 +58,10 @@ enum { MPHY_SOLVER_EMPTY = 0, MPHY_PATTERN_OK = 1, MPHY_INIT_OK = 2, MPHY_ASSEMB
 enum { MPHY_PREC_FP64 = 0,        /* FP64 element kernel, FP64 matrix, FP64 PCG (plain method) */
        MPHY_PREC_MIXED = 1,       /* FP32 tangent and matrix values; Krylov vectors, dot products,
                                    * residual and the iterative-refinement outer loop in FP64 */
-       MPHY_PREC_MIXED_F32VEC = 2 /* as MIXED, with FP32 Krylov vectors (FP64 reductions) */ };
+       MPHY_PREC_MIXED_F32VEC = 2,/* as MIXED, with FP32 Krylov vectors (FP64 reductions) */
+       MPHY_PREC_MIXED_TC = 3     /* as MIXED, with the element tangent's contraction on tensor
+                                   * cores: split-BF16 operands, FP32 accumulation (about 1e-5
+                                   * relative per entry); kinematics, stress and residual FP64 */ };
 /* preconditioner (PCJACOBI, or factorised sparse approximate inverse M = G^T G) */
 enum { MPHY_PC_JACOBI = 0, MPHY_PC_FSAI = 1, MPHY_PC_FSAI_LEARNED = 2 };
 /* MPHY_TANGENT_REFERENCE reproduces utilitiesmaterialHyperelastic.cpp:232-292 exactly
@@ -148,6 +151,10 @@ int mphy_material_nh_eval(mphy_ctx* ctx, int32_t n, const double* F_dev, double 
  * MPHY_ERR_NEG_JACOBIAN. */
 int mphy_elem_eval(mphy_ctx* ctx, const mphy_mesh* mesh, const double* disp_dev, int32_t tangent,
                    double* Ke_dev, double* Re_dev, int64_t* first_bad);
+/* The same contract computed by the MPHY_PREC_MIXED_TC element kernel: residual in FP64, tangent
+ * contracted on tensor cores (split-BF16, FP32 accumulation), widened to FP64 on export. */
+int mphy_elem_eval_tc(mphy_ctx* ctx, const mphy_mesh* mesh, const double* disp_dev, int32_t tangent,
+                      double* Ke_dev, double* Re_dev, int64_t* first_bad);
 
 /* Allocation-free variant of mphy_elem_eval for callers that cannot let the library call
  * cudaMalloc (their mesh already lives in device memory under their own allocator, or they run

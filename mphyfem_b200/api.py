@@ -279,15 +279,17 @@ def compute_stress_and_tangent(ctx: Context, F_dev, mu: float, Kinv: float, utyp
     return s, Cm
 
 
-def calc_stiffness_and_residual(mesh: Mesh, disp_dev, tangent: int = L.TANGENT_REFERENCE):
-    """Batched ElementBase::calcStiffnessAndResidual over every element: Ke, Re, first bad element."""
+def calc_stiffness_and_residual(mesh: Mesh, disp_dev, tangent: int = L.TANGENT_REFERENCE, tensor_cores: bool = False):
+    """Batched ElementBase::calcStiffnessAndResidual over every element: Ke, Re, first bad element.
+    tensor_cores: the MPHY_PREC_MIXED_TC kernel (FP64 residual, split-BF16 tangent contraction)."""
     torch = _torch()
     p = mesh.prob
     ns = 3 * p.npe
     Ke = torch.empty((p.n_elem, ns, ns), dtype=torch.float64, device="cuda")
     Re = torch.empty((p.n_elem, ns), dtype=torch.float64, device="cuda")
     bad = C.c_int64(-1)
-    rc = mesh.lib.mphy_elem_eval(mesh.ctx.h, mesh.h, _ptr(disp_dev), tangent, _ptr(Ke), _ptr(Re), C.byref(bad))
+    fn = mesh.lib.mphy_elem_eval_tc if tensor_cores else mesh.lib.mphy_elem_eval
+    rc = fn(mesh.ctx.h, mesh.h, _ptr(disp_dev), tangent, _ptr(Ke), _ptr(Re), C.byref(bad))
     L.check(rc, allow=(L.ERR_NEG_JACOBIAN,))
     return Ke, Re, bad.value
 

@@ -72,7 +72,8 @@ void solver_assemble(mphy_solver* s, const double* disp, uint8_t* bad_elem) {
     a.valf = s->mixed ? s->valf.p : nullptr;
     a.rhs = s->rhs.p;
     a.reac = s->reac.p;
-    launch_elem_fp64(a, s->mesh->npe, 2, s->ctx->stream);
+    if (s->opts.precision == MPHY_PREC_MIXED_TC) launch_elem_tc(a, s->mesh->npe, 2, s->ctx->stream);
+    else launch_elem_fp64(a, s->mesh->npe, 2, s->ctx->stream);
     s->launches += 1;
     if (s->mixed) {
         diag_from_offdiag(s->A, s->valf.p, s->diag64.p, s->ctx->stream, s->ctx->sm_count);
@@ -125,13 +126,13 @@ int solver_solve(mphy_solver* s, int32_t* its, double* fnorm) {
         pcg.set_factor(s->fsai.view());
         if (s->use_coarse) pcg.set_coarse(s->coarse.view());
     };
-    if (s->opts.precision == MPHY_PREC_MIXED) local_jacobi(s->ir.inner());
+    if (s->opts.precision == MPHY_PREC_MIXED || s->opts.precision == MPHY_PREC_MIXED_TC) local_jacobi(s->ir.inner());
     else if (s->opts.precision == MPHY_PREC_MIXED_F32VEC) local_jacobi(s->ir32.inner());
     else local_jacobi(s->pcg);
     int32_t its2 = 0;
     const int rc2 = solver_solve_once(s, &its2, fnorm);
     if (its) *its += its2;
-    if (s->opts.precision == MPHY_PREC_MIXED) local_factor(s->ir.inner());
+    if (s->opts.precision == MPHY_PREC_MIXED || s->opts.precision == MPHY_PREC_MIXED_TC) local_factor(s->ir.inner());
     else if (s->opts.precision == MPHY_PREC_MIXED_F32VEC) local_factor(s->ir32.inner());
     else local_factor(s->pcg);
     return rc2;
@@ -297,6 +298,32 @@ int newton_iteration(mphy_solver* s, double* disp, const double* fext, double la
 
 }  // namespace
 
+namespace {
+int elem_eval(mphy_ctx* c, const mphy_mesh* m, const double* disp, int32_t tangent, double* Ke, double* Re,
+              int64_t* first_bad, bool tc) {
+    return guarded([&] {
+        MPHY_REQUIRE(c && m && disp && Ke && Re, MPHY_ERR_INVALID_ARG, "null argument");
+        DevBuf<unsigned long long> bad(1);
+        MPHY_CUDA(cudaMemsetAsync(bad.p, 0xff, sizeof(unsigned long long), c->stream));
+        ElemArgs a = elem_args(m, disp, tangent, bad.p);
+        a.Ke = Ke;
+        a.Re = Re;
+        if (tc) launch_elem_tc(a, m->npe, 1, c->stream);
+        else launch_elem_fp64(a, m->npe, 1, c->stream);
+        unsigned long long h = 0;
+        MPHY_CUDA(cudaMemcpyAsync(&h, bad.p, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+        MPHY_CUDA(cudaStreamSynchronize(c->stream));
+        const int64_t b = h == ULLONG_MAX ? -1 : (int64_t)h;
+        if (first_bad) *first_bad = b;
+        if (b >= 0) {
+            set_error("negative Jacobian in element " + std::to_string(b));
+            return (int)MPHY_ERR_NEG_JACOBIAN;
+        }
+        return (int)MPHY_OK;
+    });
+}
+}  // namespace
+
 extern "C" {
 
 const char* mphy_status_string(int status) {
@@ -440,27 +467,15 @@ int mphy_material_nh_eval(mphy_ctx* c, int32_t n, const double* F, double mu, do
     });
 }
 
+
 int mphy_elem_eval(mphy_ctx* c, const mphy_mesh* m, const double* disp, int32_t tangent, double* Ke, double* Re,
                    int64_t* first_bad) {
-    return guarded([&] {
-        MPHY_REQUIRE(c && m && disp && Ke && Re, MPHY_ERR_INVALID_ARG, "null argument");
-        DevBuf<unsigned long long> bad(1);
-        MPHY_CUDA(cudaMemsetAsync(bad.p, 0xff, sizeof(unsigned long long), c->stream));
-        ElemArgs a = elem_args(m, disp, tangent, bad.p);
-        a.Ke = Ke;
-        a.Re = Re;
-        launch_elem_fp64(a, m->npe, 1, c->stream);
-        unsigned long long h = 0;
-        MPHY_CUDA(cudaMemcpyAsync(&h, bad.p, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
-        MPHY_CUDA(cudaStreamSynchronize(c->stream));
-        const int64_t b = h == ULLONG_MAX ? -1 : (int64_t)h;
-        if (first_bad) *first_bad = b;
-        if (b >= 0) {
-            set_error("negative Jacobian in element " + std::to_string(b));
-            return (int)MPHY_ERR_NEG_JACOBIAN;
-        }
-        return (int)MPHY_OK;
-    });
+    return elem_eval(c, m, disp, tangent, Ke, Re, first_bad, false);
+}
+
+int mphy_elem_eval_tc(mphy_ctx* c, const mphy_mesh* m, const double* disp, int32_t tangent, double* Ke, double* Re,
+                      int64_t* first_bad) {
+    return elem_eval(c, m, disp, tangent, Ke, Re, first_bad, true);
 }
 
 int mphy_pattern_build(mphy_ctx* c, const mphy_mesh* m, mphy_pattern** out) {
@@ -550,7 +565,7 @@ int mphy_solver_create(mphy_ctx* c, const mphy_mesh* m, const mphy_pattern* P, c
         mphy_solver_opts_default(&o);
         if (opts) o = *opts;
         MPHY_REQUIRE(o.precision == MPHY_PREC_FP64 || o.precision == MPHY_PREC_MIXED ||
-                         o.precision == MPHY_PREC_MIXED_F32VEC,
+                         o.precision == MPHY_PREC_MIXED_F32VEC || o.precision == MPHY_PREC_MIXED_TC,
                      MPHY_ERR_INVALID_ARG, "unknown precision");
         MPHY_REQUIRE(o.pc_type == MPHY_PC_JACOBI || o.pc_type == MPHY_PC_FSAI || o.pc_type == MPHY_PC_FSAI_LEARNED,
                      MPHY_ERR_INVALID_ARG, "unknown preconditioner");
@@ -581,14 +596,14 @@ int mphy_solver_create(mphy_ctx* c, const mphy_mesh* m, const mphy_pattern* P, c
             s->scalar.alloc(1);
             s->counter.alloc(1);
             MPHY_CUDA(cudaMemset(s->counter.p, 0, sizeof(uint32_t)));
-            if (o.precision == MPHY_PREC_MIXED) s->ir.init(s->A, c->sm_count, o.chunk);
+            if (o.precision == MPHY_PREC_MIXED || o.precision == MPHY_PREC_MIXED_TC) s->ir.init(s->A, c->sm_count, o.chunk);
             else if (o.precision == MPHY_PREC_MIXED_F32VEC) s->ir32.init(s->A, c->sm_count, o.chunk);
             else s->pcg.init(s->A, c->sm_count, o.chunk);
             if (o.pc_type != MPHY_PC_JACOBI) {
                 s->use_fsai = true;
                 s->fsai.init(c, P, 16);
                 const FactorView<float> fv = s->fsai.view();
-                if (o.precision == MPHY_PREC_MIXED) s->ir.inner().set_factor(fv);
+                if (o.precision == MPHY_PREC_MIXED || o.precision == MPHY_PREC_MIXED_TC) s->ir.inner().set_factor(fv);
                 else if (o.precision == MPHY_PREC_MIXED_F32VEC) s->ir32.inner().set_factor(fv);
                 else s->pcg.set_factor(fv);
             }
@@ -596,7 +611,7 @@ int mphy_solver_create(mphy_ctx* c, const mphy_mesh* m, const mphy_pattern* P, c
                 s->use_coarse = true;
                 s->coarse.init(c, m, P, o.coarse_aggregates);
                 const CoarseView cv = s->coarse.view();
-                if (o.precision == MPHY_PREC_MIXED) s->ir.inner().set_coarse(cv);
+                if (o.precision == MPHY_PREC_MIXED || o.precision == MPHY_PREC_MIXED_TC) s->ir.inner().set_coarse(cv);
                 else if (o.precision == MPHY_PREC_MIXED_F32VEC) s->ir32.inner().set_coarse(cv);
                 else s->pcg.set_coarse(cv);
             }

@@ -28,7 +28,11 @@ struct ElemArgs {
 };
 
 void upload_shape_tables();
+void upload_shape_tables_tc(const double* h8, const double* w8, const double* t10, const double* w4);
 void launch_elem_fp64(const ElemArgs& a, int npe, int mode, cudaStream_t s);
+// Mixed-precision element kernel (elem_tc.cu): FP64 residual, tangent contraction on tensor
+// cores (split-BF16, FP32 accumulation), FP32 off-diagonal scatter (a.valf) or Ke export.
+void launch_elem_tc(const ElemArgs& a, int npe, int mode, cudaStream_t s);
 void launch_nh_eval(int n, const double* F, double mu, double Kinv, int utype, int tangent, double* stre,
                     double* C, cudaStream_t s);
 void launch_scatter_batch(int npe, int32_t n, const int32_t* ids, const mphy_mesh* mesh, const mphy_pattern* P,

@@ -80,6 +80,48 @@ __global__ void diag_scale_kernel(SellView A, const void* aval, bool f32, const 
     }
 }
 
+// Block-Jacobi FSAI in the network's scaled units: with only the diagonal block in the pattern,
+// the block FSAI of fsai.cu is G_nn = L^T with L L^T = (A^_nn)^{-1}. The network predicts a
+// correction to it, so an untrained (zero-output) network is block-Jacobi. A block that is not
+// positive definite gives the identity (fsai.cu's fallback row, 1/sqrt|a_ii| unscaled).
+__global__ void base_kernel(int32_t n_node, const float* __restrict__ x, float* __restrict__ base) {
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < n_node; n += (int64_t)gridDim.x * blockDim.x) {
+        double A[3][3];
+        for (int v = 0; v < 9; ++v) A[v / 3][v % 3] = 0.5 * ((double)x[13 * n + v] + (double)x[13 * n + 3 * (v % 3) + v / 3]);
+        const double det = A[0][0] * (A[1][1] * A[2][2] - A[1][2] * A[2][1]) -
+                           A[0][1] * (A[1][0] * A[2][2] - A[1][2] * A[2][0]) +
+                           A[0][2] * (A[1][0] * A[2][1] - A[1][1] * A[2][0]);
+        float out[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+        if (det > 0.0) {
+            const double r = 1.0 / det;
+            double Y[3][3];  // (A^_nn)^{-1}, symmetric
+            Y[0][0] = (A[1][1] * A[2][2] - A[1][2] * A[2][1]) * r;
+            Y[0][1] = (A[0][2] * A[2][1] - A[0][1] * A[2][2]) * r;
+            Y[0][2] = (A[0][1] * A[1][2] - A[0][2] * A[1][1]) * r;
+            Y[1][1] = (A[0][0] * A[2][2] - A[0][2] * A[2][0]) * r;
+            Y[1][2] = (A[0][2] * A[1][0] - A[0][0] * A[1][2]) * r;
+            Y[2][2] = (A[0][0] * A[1][1] - A[0][1] * A[1][0]) * r;
+            const double l00s = Y[0][0];
+            if (l00s > 0.0) {
+                const double l00 = sqrt(l00s), l10 = Y[0][1] / l00, l20 = Y[0][2] / l00;
+                const double l11s = Y[1][1] - l10 * l10;
+                if (l11s > 0.0) {
+                    const double l11 = sqrt(l11s), l21 = (Y[1][2] - l20 * l10) / l11;
+                    const double l22s = Y[2][2] - l20 * l20 - l21 * l21;
+                    if (l22s > 0.0) {
+                        const double l22 = sqrt(l22s);
+                        // G_nn = L^T (row-major)
+                        const float g[9] = {(float)l00, (float)l10, (float)l20, 0.f, (float)l11, (float)l21,
+                                            0.f, 0.f, (float)l22};
+                        for (int v = 0; v < 9; ++v) out[v] = g[v];
+                    }
+                }
+            }
+        }
+        for (int v = 0; v < 9; ++v) base[9 * n + v] = out[v];
+    }
+}
+
 // prescribed flags for the FP64 storage (its rows are already identity): from the pattern's mask
 __global__ void fixed_flags_kernel(int32_t n_node, const uint8_t* __restrict__ fixed, float* __restrict__ x) {
     for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < n_node; n += (int64_t)gridDim.x * blockDim.x)
@@ -361,13 +403,14 @@ __global__ void relu_mask_kernel(int64_t n, const float* __restrict__ dh, const 
         dq[i] = q[i] > 0.f ? dh[i] : 0.f;
 }
 
-// decoder on lower edges: out = an_n + bn_m + Wc e_nm + bo; loss, dout, predicted blocks.
+// decoder on lower edges: out = [m == n] base_n + an_n + bn_m + Wc e_nm + bo; loss, dout,
+// predicted blocks.
 // Entries whose row or column DOF is prescribed are not predicted: they take the identity (1 on a
 // prescribed DOF's own diagonal, 0 elsewhere), the structure of the exact FSAI of an operator with
 // identity rows and columns there. M = G^T G then leaves prescribed components of the residual
 // alone, which the mixed operator (couplings to prescribed DOFs stored, masked in SpMV) requires.
 __global__ void __launch_bounds__(256) dec_fwd(SellView A, const void* aval, bool f32, const uint8_t* __restrict__ fixed,
-                                               int64_t n_lower,
+                                               const float* __restrict__ base, int64_t n_lower,
                                                const int32_t* __restrict__ lrow_of, const int32_t* __restrict__ lcol,
                                                const int32_t* __restrict__ lslot, const float* __restrict__ sqrt_s,
                                                const float* __restrict__ an, const float* __restrict__ bn,
@@ -387,6 +430,7 @@ __global__ void __launch_bounds__(256) dec_fwd(SellView A, const void* aval, boo
         for (int o = 0; o < 9; ++o) {
             float v = an[9 * n + o] + bn[9 * m + o] + B[o];
             for (int i = 0; i < 9; ++i) v += W[9 * o + i] * e[i];
+            if (m == n) v += base[9 * n + o];  // correction to block-Jacobi FSAI
             const bool masked = fixed && (fixed[3 * n + o / 3] || fixed[3 * m + o % 3]);
             if (masked) v = (m == n && o / 3 == o % 3) ? 1.f : 0.f;
             if (tgt) {
@@ -559,6 +603,8 @@ void Gnn::build_graph(GnnGraph& g, const mphy_pattern* P, const Fsai& F, const S
     diag_scale_kernel<<<stride_grid(nn, 256, sm), 256, 0, s>>>(A, aval, f32, P->brow_ptr.p, P->bcol.p, g.sqrt_s.p,
                                                                g.xnode.p, g.deg.p);
     fixed_flags_kernel<<<stride_grid(nn, 256, sm), 256, 0, s>>>(nn, fixed, g.xnode.p);
+    if (g.base.n != 9 * (size_t)nn) g.base.alloc(9 * (size_t)nn);
+    base_kernel<<<stride_grid(nn, 256, sm), 256, 0, s>>>(nn, g.xnode.p, g.base.p);
     lower_slots_kernel<<<stride_grid(nn, 256, sm), 256, 0, s>>>(nn, L.rowptr.p, L.col.p, P->brow_ptr.p, P->bcol.p,
                                                                 g.lslot.p, g.lrow_of.p);
     upper_to_lower_kernel<<<stride_grid(nn, 256, sm), 256, 0, s>>>(nn, U.rowptr.p, U.col.p, L.rowptr.p, L.col.p,
@@ -609,7 +655,7 @@ double Gnn::run(const GnnGraph& g, const mphy_pattern* Pt, const Fsai& F, const 
     lin_fwd<H, 9, false><<<gn, 256, 0, s>>>(nn, hL, W + GnnLayout::Wb, nullptr, bn_.p);
     if (train) MPHY_CUDA(cudaMemsetAsync(loss_.p, 0, sizeof(double), s));
     const float inv_count = 1.f / (9.f * (float)nl);
-    dec_fwd<<<stride_grid(nl, 256, sm), 256, 0, s>>>(A, aval, f32, fixed, nl, g.lrow_of.p, L.col.p, g.lslot.p, g.sqrt_s.p, an_.p,
+    dec_fwd<<<stride_grid(nl, 256, sm), 256, 0, s>>>(A, aval, f32, fixed, g.base.p, nl, g.lrow_of.p, L.col.p, g.lslot.p, g.sqrt_s.p, an_.p,
                                                      bn_.p, W + GnnLayout::Wc, W + GnnLayout::bo,
                                                      train ? g.target.p : nullptr, inv_count,
                                                      (train && compute_grad) ? dout_.p : nullptr, out_blocks,

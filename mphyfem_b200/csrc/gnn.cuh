@@ -38,6 +38,7 @@ struct GnnGraph {
     DevBuf<int32_t> lrow_of;  // [n_lower] row n of every lower block
     DevBuf<int64_t> u2l;      // [n_lower] compact lower index of the k-th upper entry (G^T rows)
     DevBuf<float> target;     // [n_lower][9] scaled exact FSAI blocks (training only)
+    DevBuf<float> base;       // [n_node][9] block-Jacobi FSAI diagonal blocks (scaled units)
     bool has_target = false;
 };
 

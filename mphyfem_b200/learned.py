@@ -1,8 +1,9 @@
 """Learned factorised preconditioner (MPHY_PC_FSAI_LEARNED): parameter initialisation, GPU
 training on operators the solver assembles, and persistence of the trained weights.
 
-The network (csrc/gnn.cu) predicts the blocks of G in M = G^T G from the Jacobi-scaled operator;
-the targets are the exact block FSAI the library computes for the same operator. Training runs
+The network (csrc/gnn.cu) predicts the blocks of G in M = G^T G from the Jacobi-scaled operator,
+as a correction to block-Jacobi FSAI (so an untrained network is block-Jacobi); the targets are
+the exact block FSAI the library computes for the same operator. Training runs
 entirely in libmphy.so's forward/backward/Adam kernels; this module only orders the steps.
 """
 from __future__ import annotations
@@ -43,7 +44,7 @@ def init_params(seed: int = 0) -> np.ndarray:
         zeros(H)           # d
     lin(9, H, 0.1)         # Wa
     lin(9, H, 0.1)         # Wb
-    parts.append(np.eye(9).ravel() * 0.5)  # Wc: start near a scaled copy of the operator block
+    zeros(81)              # Wc: the network starts as block-Jacobi FSAI (its correction is small)
     zeros(9)
     p = np.concatenate(parts).astype(np.float32)
     assert p.size == param_count(), (p.size, param_count())

@@ -1,12 +1,15 @@
 """Small, self-terminating workloads for ncu captures of single kernels.
 
     python -m mphyfem_b200.profile_driver --op spmv --nx 128 --ny 32 --nz 32 --reps 4
+    python -m mphyfem_b200.profile_driver --op spmv --precision mixed --reps 4
     python -m mphyfem_b200.profile_driver --op assemble --nx 128 --ny 32 --nz 32 --reps 3
-    python -m mphyfem_b200.profile_driver --op newton --nx 128 --ny 32 --nz 32 --reps 1
+    python -m mphyfem_b200.profile_driver --op newton --precision mixed --coarse 64 --reps 1
+    python -m mphyfem_b200.profile_driver --op batch --instances 48 --reps 2
 
-Each run builds the hex8 cantilever of the given size, assembles it once at u = 0 and then
-repeats the chosen operation: SpMV with the assembled matrix, the fused assembly, or one Newton
-iteration (assembly + Jacobi-PCG + update).
+Each run builds the hex8 cantilever of the given size (or, for ``batch``, the first blocks of
+the 512-block batched set), assembles it once at u = 0 and then repeats the chosen operation:
+SpMV with the assembled matrix, the fused assembly, one Newton iteration (assembly + PCG +
+update), or the batched persistent solve of all instances.
 """
 from __future__ import annotations
 
@@ -16,22 +19,44 @@ import sys
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--op", choices=["spmv", "assemble", "newton"], default="spmv")
+    ap.add_argument("--op", choices=["spmv", "assemble", "newton", "batch"], default="spmv")
     ap.add_argument("--nx", type=int, default=128)
     ap.add_argument("--ny", type=int, default=32)
     ap.add_argument("--nz", type=int, default=32)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--rtol", type=float, default=1e-8)
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--pc", choices=["jacobi", "fsai"], default="jacobi")
+    ap.add_argument("--coarse", type=int, default=0)
+    ap.add_argument("--instances", type=int, default=48)
+    ap.add_argument("--cluster", type=int, default=4)
+    ap.add_argument("--threads", type=int, default=512)
     args = ap.parse_args(argv)
 
     import torch
 
-    from . import api, meshgen
-    p = meshgen.hex8_cantilever(args.nx, args.ny, args.nz)
+    from . import _lib, api, meshgen
+    prec = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED}[args.precision]
     ctx = api.Context(0)
+    if args.op == "batch":
+        probs = meshgen.batched_blocks(512, seed=11)[:args.instances]
+        b = api.BatchGpu(probs, ctx, precision=prec, rtol=args.rtol, norm_type=1, max_it=20000)
+        u = b.union
+        b.solver.calcStiffnessAndResidual(torch.zeros(u.n_dof, dtype=torch.float64, device="cuda"))
+        b.solver.addExternalForces(torch.tensor(u.fnodal, device="cuda"), 0.2)
+        b.set_schedule(args.cluster, args.threads)
+        for _ in range(args.reps):
+            its, st, _, ms = b.solve()
+        torch.cuda.synchronize()
+        print(f"batch of {args.instances}: n_node={u.n_node} its mean {its.mean():.0f} max {its.max()} "
+              f"ms {ms:.2f}", file=sys.stderr)
+        return
+    p = meshgen.hex8_cantilever(args.nx, args.ny, args.nz)
     mesh = api.Mesh(ctx, p)
     pat = api.Pattern(mesh)
-    sol = api.SolverGpu(mesh, pat, rtol=args.rtol, max_it=20000)
+    sol = api.SolverGpu(mesh, pat, rtol=args.rtol, max_it=20000, precision=prec,
+                        pc_type={"jacobi": _lib.PC_JACOBI, "fsai": _lib.PC_FSAI}[args.pc],
+                        coarse_aggregates=args.coarse, norm_type=1)
     disp = torch.zeros(p.n_dof, dtype=torch.float64, device="cuda")
     fext = torch.tensor(p.fnodal, dtype=torch.float64, device="cuda")
     sol.calcStiffnessAndResidual(disp)

@@ -85,6 +85,21 @@ def loss_and_grads(params, A_full, fixed, nbrs, lrow, lcol, gblocks):
     el = torch.tensor(np.array([blk(n, m).ravel() for n, m in zip(rows, lcol)]))
     out = (h[torch.tensor(rows)] @ W("Wa", (9, H)).T + h[torch.tensor(lcol.astype(np.int64))] @ W("Wb", (9, H)).T
            + el @ W("Wc", (9, 9)).T + W("bo", (9,)))
+    # the network corrects block-Jacobi FSAI (gnn.cu base_kernel): G_nn = L^T, L L^T = (A^_nn)^-1
+    base = np.zeros((len(rows), 9))
+    for j, (n, m) in enumerate(zip(rows, lcol)):
+        if n != m:
+            continue
+        B = blk(n, n)
+        B = 0.5 * (B + B.T)
+        g = np.eye(3)
+        if np.linalg.det(B) > 0:
+            try:
+                g = np.linalg.cholesky(np.linalg.inv(B)).T
+            except np.linalg.LinAlgError:
+                g = np.eye(3)
+        base[j] = g.ravel()
+    out = out + torch.tensor(base)
     # entries with a prescribed row or column DOF are fixed to the identity (gnn.cu dec_fwd)
     keep = np.ones((len(rows), 3, 3))
     ident = np.zeros((len(rows), 3, 3))

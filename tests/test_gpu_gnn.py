@@ -92,10 +92,38 @@ def test_learned_beats_jacobi(env, trained, precision, rtol):
         assert np.linalg.norm(xs["learned"] - xs["jacobi"]) <= 1e-7 * np.linalg.norm(xs["jacobi"])
 
 
+def test_untrained_network_is_block_jacobi(env):
+    """Zero weights: the prediction is block-Jacobi FSAI, the exact block FSAI on the diagonal
+    pattern (G_nn = L^T, L L^T = A_nn^-1), so G A G^T has identity diagonal blocks."""
+    torch, api, _lib, learned, ctx = env
+    q = meshgen.hex8_cantilever(8, 2, 2)
+    mesh, pat, sol = _assembled(torch, api, _lib, ctx, q, _lib.PREC_FP64)
+    gnn = learned.Gnn(ctx, np.zeros(learned.param_count(), np.float32))
+    gnn.predict(sol)
+    G = sol.pc_get_blocks().cpu().numpy().reshape(-1, 3, 3)
+    lrow, lcol = sol.pc_pattern()
+    rows = np.repeat(np.arange(q.n_node), np.diff(lrow))
+    val, _, _ = sol.export(want_rhs=False, want_reac=False)
+    rp, col = pat.export_csr()
+    from oracle import fsai_ref
+    A = fsai_ref.full_operator(q.n_node, q.fixed, rp, col, val).tocsr()
+    for j, (n, m) in enumerate(zip(rows, lcol)):
+        if n != m:
+            assert np.abs(G[j]).max() < 1e-6
+            continue
+        Ann = A[3 * n:3 * n + 3, 3 * n:3 * n + 3].toarray()
+        np.testing.assert_allclose(G[j] @ Ann @ G[j].T, np.eye(3), atol=1e-4)
+
+
 def test_useless_network_falls_back_to_jacobi(env):
     torch, api, _lib, learned, ctx = env
     q = meshgen.hex8_cantilever(12, 3, 3)
-    gnn = learned.Gnn(ctx, np.zeros(learned.param_count(), np.float32))  # predicts G = 0
+    from oracle import gnn_ref
+    off, _ = gnn_ref.layout()
+    p = np.zeros(learned.param_count(), np.float32)
+    o, n = off["bo"]
+    p[o:o + n] = np.nan  # a corrupted weights file: every predicted block is NaN
+    gnn = learned.Gnn(ctx, p)
     mesh = api.Mesh(ctx, q)
     sol = api.SolverGpu(mesh, api.Pattern(mesh), pc_type=_lib.PC_FSAI_LEARNED, rtol=1e-10)
     gnn.attach(sol)
