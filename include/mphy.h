@@ -238,8 +238,10 @@ int mphy_gnn_create(mphy_ctx* ctx, const float* params_host, mphy_gnn** out);
 int mphy_gnn_destroy(mphy_gnn* g);
 int mphy_gnn_get_params(mphy_gnn* g, float* params_host);
 int mphy_gnn_set_params(mphy_gnn* g, const float* params_host);
-/* Loss (mean squared error of the scaled blocks against the exact FSAI of the solver's assembled
- * operator) and its gradient, without changing the parameters; grads_host may be NULL. */
+/* Loss and its gradient on the solver's assembled operator, without changing the parameters;
+ * grads_host may be NULL. The loss is Kaporin's condition number of the preconditioned operator,
+ * log( tr(G A G^T) / N ) - (2/N) sum_n log|det G_nn| in the Jacobi-scaled units (N = 3 n_node),
+ * whose minimiser over the pattern is the exact block FSAI; it needs no target. */
 int mphy_gnn_loss_and_grads(mphy_gnn* g, mphy_solver* s, double* loss, float* grads_host);
 /* One Adam step on the solver's assembled operator; *loss before the step. */
 int mphy_gnn_train_step(mphy_gnn* g, mphy_solver* s, float lr, double* loss);

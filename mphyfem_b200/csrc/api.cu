@@ -1012,18 +1012,14 @@ int mphy_gnn_set_params(mphy_gnn* g, const float* p) {
 }
 
 namespace {
-// exact block FSAI of the assembled operator as the training target, features, forward/backward
+// features of the assembled operator, forward, the Kaporin loss and (grad) the backward pass
 double gnn_loss(mphy_gnn* g, mphy_solver* s, bool grad) {
     MPHY_REQUIRE(s->use_fsai, MPHY_ERR_STATE, "the solver needs pc_type MPHY_PC_FSAI or MPHY_PC_FSAI_LEARNED");
     MPHY_REQUIRE(s->state == MPHY_ASSEMBLY_OK || s->state == MPHY_FACTORISE_OK, MPHY_ERR_STATE,
                  "assemble the matrix first");
     cudaStream_t st = s->ctx->stream;
     const void* aval = s->mixed ? (const void*)s->valf.p : (const void*)s->val.p;
-    if (s->mixed) s->fsai.compute<float>(s->valf.p, s->diag64.p, s->mesh->fixed.p, st);
-    else s->fsai.compute<double>(s->val.p, nullptr, nullptr, st);
-    DevBuf<float> blocks(9 * (size_t)s->fsai.lower().n_blocks);
-    s->fsai.get_lower_values(blocks.p, st);
-    g->net.build_graph(s->graph, s->pat, s->fsai, s->A, aval, s->mixed, s->mesh->fixed.p, blocks.p, st);
+    g->net.build_graph(s->graph, s->pat, s->fsai, s->A, aval, s->mixed, s->mesh->fixed.p, true, st);
     if (grad) g->net.zero_grads(st);
     const double loss = g->net.run(s->graph, s->pat, s->fsai, s->A, aval, s->mixed, s->mesh->fixed.p, nullptr, grad, st);
     MPHY_CUDA(cudaStreamSynchronize(st));
@@ -1060,7 +1056,7 @@ int mphy_gnn_predict(mphy_gnn* g, mphy_solver* s, float* ms) {
         cudaStream_t st = s->ctx->stream;
         const void* aval = s->mixed ? (const void*)s->valf.p : (const void*)s->val.p;
         MPHY_CUDA(cudaEventRecord(s->ctx->ev0, st));
-        g->net.build_graph(s->graph, s->pat, s->fsai, s->A, aval, s->mixed, s->mesh->fixed.p, nullptr, st);
+        g->net.build_graph(s->graph, s->pat, s->fsai, s->A, aval, s->mixed, s->mesh->fixed.p, false, st);
         DevBuf<float> blocks(9 * (size_t)s->fsai.lower().n_blocks);
         g->net.run(s->graph, s->pat, s->fsai, s->A, aval, s->mixed, s->mesh->fixed.p, blocks.p, false, st);
         s->fsai.set_lower_values(blocks.p, st);

@@ -163,12 +163,139 @@ __global__ void upper_to_lower_kernel(int32_t n_node, const int64_t* __restrict_
     }
 }
 
-__global__ void target_kernel(int64_t n_lower, const int32_t* __restrict__ lcol, const float* __restrict__ G,
-                              const float* __restrict__ sqrt_s, float* __restrict__ tgt) {
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < 9 * n_lower; t += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t j = t / 9;
-        const int v = (int)(t % 9);
-        tgt[t] = G[t] * sqrt_s[3 * (int64_t)lcol[j] + v % 3];
+// ---------------------------------------------------------------- training loss
+// Kaporin's K-condition number of the preconditioned operator, whose minimiser over the pattern
+// is exact FSAI and which bounds CG's iteration count:
+//   K = (tr(G^ A^ G^T) / N) / det(G^ A^ G^T)^{1/N},
+//   loss = log K + (1/N) log det A^ = log(tr(G^ A^ G^T) / N) - (2/N) sum_n log|det G^_nn|
+// (N = 3 n_node; G^ lower block-triangular, so det G^ is the product of its diagonal blocks'
+// determinants). The trace is a sum over block rows of local quadratic forms,
+//   tr_n = sum_{j, j' in row n} tr(G^_j A^_{m_j m_j'} G^_j'^T),
+// and d tr / d G^_j = 2 T_j with T_j = sum_{j'} G^_j' A^_{m_j' m_j}.
+__device__ __forceinline__ int64_t slot_in_row(const int64_t* brow, const int32_t* bcol, int64_t r, int32_t c) {
+    int64_t lo = brow[r], hi = brow[r + 1];
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (bcol[mid] < c) lo = mid + 1;
+        else hi = mid;
+    }
+    return (lo < brow[r + 1] && bcol[lo] == c) ? lo - brow[r] : -1;
+}
+
+// One warp per block row; lane j of the row (at most 32 lower blocks) forms T_j.
+__global__ void __launch_bounds__(256) kaporin_rows(SellView A, const void* aval, bool f32, int32_t n_node,
+                                                    const int64_t* __restrict__ brow, const int32_t* __restrict__ bcol,
+                                                    const int64_t* __restrict__ lrow, const int32_t* __restrict__ lcol,
+                                                    const float* __restrict__ sqrt_s, const float* __restrict__ ghat,
+                                                    float* __restrict__ tbuf, double* __restrict__ part_tr,
+                                                    double* __restrict__ part_ld) {
+    const int lane = threadIdx.x & 31;
+    for (int64_t n = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; n < n_node;
+         n += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        const int64_t r0 = lrow[n], len = lrow[n + 1] - r0;
+        double tr = 0.0, ld = 0.0;
+        if (lane < len) {
+            const int64_t j = r0 + lane;
+            const int32_t m = lcol[j];
+            float T[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+            for (int64_t jp = r0; jp < r0 + len; ++jp) {
+                const int32_t mp = lcol[jp];
+                const int64_t k = slot_in_row(brow, bcol, mp, m);
+                if (k < 0) continue;  // m and m' are not neighbours: A^_{m' m} = 0
+                float e[9];
+                scaled_block(A, aval, f32, sqrt_s, mp, (int)k, m, e);
+                const float* g = ghat + 9 * jp;
+#pragma unroll
+                for (int r = 0; r < 3; ++r)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) T[3 * r + c] += g[3 * r] * e[c] + g[3 * r + 1] * e[3 + c] + g[3 * r + 2] * e[6 + c];
+            }
+            const float* gj = ghat + 9 * j;
+#pragma unroll
+            for (int v = 0; v < 9; ++v) {
+                tbuf[9 * j + v] = T[v];
+                tr += (double)T[v] * (double)gj[v];
+            }
+            if (m == (int32_t)n) {
+                const double d = (double)gj[0] * ((double)gj[4] * gj[8] - (double)gj[5] * gj[7]) -
+                                 (double)gj[1] * ((double)gj[3] * gj[8] - (double)gj[5] * gj[6]) +
+                                 (double)gj[2] * ((double)gj[3] * gj[7] - (double)gj[4] * gj[6]);
+                ld = log(fmax(fabs(d), 1e-300));
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            tr += __shfl_xor_sync(0xffffffffu, tr, o);
+            ld += __shfl_xor_sync(0xffffffffu, ld, o);
+        }
+        if (lane == 0) {
+            part_tr[n] = tr;
+            part_ld[n] = ld;
+        }
+    }
+}
+
+// One CTA: fixed-order sums of the row partials; red = {tr, sum log|det|, loss}.
+__global__ void __launch_bounds__(1024) kaporin_reduce(int32_t n_node, const double* __restrict__ part_tr,
+                                                       const double* __restrict__ part_ld, double* __restrict__ red,
+                                                       double* __restrict__ loss) {
+    __shared__ double s1[1024], s2[1024];
+    double a = 0.0, b = 0.0;
+    for (int64_t i = threadIdx.x; i < n_node; i += blockDim.x) {
+        a += part_tr[i];
+        b += part_ld[i];
+    }
+    s1[threadIdx.x] = a;
+    s2[threadIdx.x] = b;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) {
+            s1[threadIdx.x] += s1[threadIdx.x + o];
+            s2[threadIdx.x] += s2[threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const double N = 3.0 * n_node;
+        red[0] = s1[0];
+        red[1] = s2[0];
+        red[2] = log(s1[0] / N) - 2.0 / N * s2[0];
+        *loss = red[2];
+    }
+}
+
+// dL/dG^_j = (2 / tr) T_j - (2 / N) [m == n] G^_nn^{-T}, zero on entries fixed to the identity;
+// dout_j = dL/dP_j = base_n^T dL/dG^_j (the decoder's P, see dec_fwd).
+__global__ void kaporin_grad(int64_t n_lower, int32_t n_node, const int32_t* __restrict__ lrow_of,
+                             const int32_t* __restrict__ lcol, const uint8_t* __restrict__ fixed,
+                             const float* __restrict__ base, const float* __restrict__ ghat,
+                             const float* __restrict__ tbuf, const double* __restrict__ red, float* __restrict__ dout) {
+    const double tr = red[0], N = 3.0 * n_node;
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n_lower; j += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t n = lrow_of[j], m = lcol[j];
+        float dg[9];
+        for (int v = 0; v < 9; ++v) dg[v] = (float)(2.0 / tr * tbuf[9 * j + v]);
+        if (m == n) {
+            const float* g = ghat + 9 * j;
+            const double d = (double)g[0] * ((double)g[4] * g[8] - (double)g[5] * g[7]) -
+                             (double)g[1] * ((double)g[3] * g[8] - (double)g[5] * g[6]) +
+                             (double)g[2] * ((double)g[3] * g[7] - (double)g[4] * g[6]);
+            if (fabs(d) > 1e-300) {
+                // G^{-T}[r][c] = cof(G)[r][c] / det
+                const double cof[9] = {g[4] * g[8] - g[5] * g[7], g[5] * g[6] - g[3] * g[8], g[3] * g[7] - g[4] * g[6],
+                                       g[2] * g[7] - g[1] * g[8], g[0] * g[8] - g[2] * g[6], g[1] * g[6] - g[0] * g[7],
+                                       g[1] * g[5] - g[2] * g[4], g[2] * g[3] - g[0] * g[5], g[0] * g[4] - g[1] * g[3]};
+                for (int v = 0; v < 9; ++v) dg[v] -= (float)(2.0 / N * cof[v] / d);
+            }
+        }
+        if (fixed)
+            for (int v = 0; v < 9; ++v)
+                if (fixed[3 * n + v / 3] || fixed[3 * m + v % 3]) dg[v] = 0.f;
+        const float* B = base + 9 * n;
+        for (int o = 0; o < 9; ++o) {
+            const int k = o / 3, c = o % 3;
+            dout[9 * j + o] = B[k] * dg[c] + B[3 + k] * dg[3 + c] + B[6 + k] * dg[6 + c];
+        }
     }
 }
 
@@ -403,8 +530,12 @@ __global__ void relu_mask_kernel(int64_t n, const float* __restrict__ dh, const 
         dq[i] = q[i] > 0.f ? dh[i] : 0.f;
 }
 
-// decoder on lower edges: out = [m == n] base_n + an_n + bn_m + Wc e_nm + bo; loss, dout,
-// predicted blocks.
+// decoder on lower edges: P = [m == n] I + an_n + bn_m + [m != n] Wc e_nm + bo, and the predicted
+// block is
+// G^_nm = base_n P (3x3 product): block-Jacobi FSAI times a learned factor, so an untrained
+// network (P = I on the diagonal, 0 elsewhere) is block-Jacobi, and the structure of exact FSAI's
+// off-diagonal blocks, G_nm ~ -G_nn A^_nm, is linear in the decoder. The loss kernels (kaporin_*) give
+// dout = dL/dP.
 // Entries whose row or column DOF is prescribed are not predicted: they take the identity (1 on a
 // prescribed DOF's own diagonal, 0 elsewhere), the structure of the exact FSAI of an operator with
 // identity rows and columns there. M = G^T G then leaves prescribed components of the residual
@@ -415,40 +546,31 @@ __global__ void __launch_bounds__(256) dec_fwd(SellView A, const void* aval, boo
                                                const int32_t* __restrict__ lslot, const float* __restrict__ sqrt_s,
                                                const float* __restrict__ an, const float* __restrict__ bn,
                                                const __nv_bfloat16* __restrict__ Wc, const __nv_bfloat16* __restrict__ bo,
-                                               const float* __restrict__ tgt, float inv_count, float* __restrict__ dout,
-                                               float* __restrict__ pred, double* loss) {
+                                               float* __restrict__ ghat, float* __restrict__ pred) {
     __shared__ float W[81], B[9];
-    __shared__ double red[256];
     for (int i = threadIdx.x; i < 81; i += blockDim.x) W[i] = bf(Wc, i);
     for (int i = threadIdx.x; i < 9; i += blockDim.x) B[i] = bf(bo, i);
     __syncthreads();
-    double l = 0.0;
     for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n_lower; j += (int64_t)gridDim.x * blockDim.x) {
         const int64_t n = lrow_of[j], m = lcol[j];
-        float e[9];
+        float e[9], P[9], Bn[9];
         scaled_block(A, aval, f32, sqrt_s, n, lslot[j], m, e);
         for (int o = 0; o < 9; ++o) {
             float v = an[9 * n + o] + bn[9 * m + o] + B[o];
-            for (int i = 0; i < 9; ++i) v += W[9 * o + i] * e[i];
-            if (m == n) v += base[9 * n + o];  // correction to block-Jacobi FSAI
-            const bool masked = fixed && (fixed[3 * n + o / 3] || fixed[3 * m + o % 3]);
-            if (masked) v = (m == n && o / 3 == o % 3) ? 1.f : 0.f;
-            if (tgt) {
-                const float df = v - tgt[9 * j + o];
-                l += (double)df * df;
-                if (dout) dout[9 * j + o] = masked ? 0.f : 2.f * df * inv_count;
-            }
-            if (pred) pred[9 * j + o] = v / sqrt_s[3 * m + o % 3];
+            if (m != n)
+                for (int i = 0; i < 9; ++i) v += W[9 * o + i] * e[i];
+            P[o] = v + ((m == n && o / 3 == o % 3) ? 1.f : 0.f);
+            Bn[o] = base[9 * n + o];
+        }
+        for (int o = 0; o < 9; ++o) {
+            const int r = o / 3, c = o % 3;
+            float v = Bn[3 * r] * P[c] + Bn[3 * r + 1] * P[3 + c] + Bn[3 * r + 2] * P[6 + c];
+            const bool masked = fixed && (fixed[3 * n + r] || fixed[3 * m + c]);
+            if (masked) v = (m == n && r == c) ? 1.f : 0.f;
+            if (ghat) ghat[9 * j + o] = v;
+            if (pred) pred[9 * j + o] = v / sqrt_s[3 * m + c];
         }
     }
-    if (!loss) return;
-    red[threadIdx.x] = l;
-    __syncthreads();
-    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-        if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) atomicAdd(loss, red[0] * (double)inv_count);
 }
 
 // dan_n = sum over lower edges of row n; dbn_m = sum over lower edges with column m (via G^T rows)
@@ -483,10 +605,12 @@ __global__ void __launch_bounds__(256) dec_bwd_weights(SellView A, const void* a
     for (int i = 0; i < 90; ++i) acc[i] = 0.f;
     for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n_lower; j += (int64_t)gridDim.x * blockDim.x) {
         float e[9];
+        const bool self = lrow_of[j] == lcol[j];  // the edge term acts on off-diagonal blocks only
         scaled_block(A, aval, f32, sqrt_s, lrow_of[j], lslot[j], lcol[j], e);
         for (int o = 0; o < 9; ++o) {
             const float d = dout[9 * j + o];
-            for (int i = 0; i < 9; ++i) acc[9 * o + i] += d * e[i];
+            if (!self)
+                for (int i = 0; i < 9; ++i) acc[9 * o + i] += d * e[i];
             acc[81 + o] += d;
         }
     }
@@ -582,10 +706,15 @@ void Gnn::ensure_workspace(int32_t nn, int64_t nl) {
     dan_.alloc(9 * (size_t)nn);
     dbn_.alloc(9 * (size_t)nn);
     dout_.alloc(9 * (size_t)nl);
+    ghat_.alloc(9 * (size_t)nl);
+    tbuf_.alloc(9 * (size_t)nl);
+    part_tr_.alloc(nn);
+    part_ld_.alloc(nn);
+    red_.alloc(3);
 }
 
 void Gnn::build_graph(GnnGraph& g, const mphy_pattern* P, const Fsai& F, const SellView& A, const void* aval,
-                      bool f32, const uint8_t* fixed, const float* fsai_blocks, cudaStream_t s) {
+                      bool f32, const uint8_t* fixed, bool training, cudaStream_t s) {
     const int sm = ctx_->sm_count;
     const int32_t nn = P->n_node;
     const SellPattern& L = F.lower();
@@ -609,12 +738,7 @@ void Gnn::build_graph(GnnGraph& g, const mphy_pattern* P, const Fsai& F, const S
                                                                 g.lslot.p, g.lrow_of.p);
     upper_to_lower_kernel<<<stride_grid(nn, 256, sm), 256, 0, s>>>(nn, U.rowptr.p, U.col.p, L.rowptr.p, L.col.p,
                                                                    g.u2l.p);
-    g.has_target = fsai_blocks != nullptr;
-    if (g.has_target) {
-        if (g.target.n != 9 * (size_t)L.n_blocks) g.target.alloc(9 * (size_t)L.n_blocks);
-        target_kernel<<<stride_grid(9 * L.n_blocks, 256, sm), 256, 0, s>>>(L.n_blocks, L.col.p, fsai_blocks, g.sqrt_s.p,
-                                                                          g.target.p);
-    }
+    g.training = training;
     MPHY_CUDA(cudaGetLastError());
 }
 
@@ -630,7 +754,8 @@ double Gnn::run(const GnnGraph& g, const mphy_pattern* Pt, const Fsai& F, const 
     const unsigned gn = node_grid(nn, sm);
     const SellPattern& L = F.lower();
     const SellPattern& U = F.upper();
-    const bool train = g.has_target;
+    const bool train = g.training;
+    MPHY_REQUIRE(F.max_lower() <= 32, MPHY_ERR_UNSUPPORTED, "learned FSAI: at most 32 lower blocks per row");
     launches = 0;
     // forward
     lin_fwd<kGnnNodeIn, H, true><<<gn, 256, 0, s>>>(nn, g.xnode.p, W + GnnLayout::w_in, W + GnnLayout::b_in, h_.p);
@@ -653,14 +778,22 @@ double Gnn::run(const GnnGraph& g, const mphy_pattern* Pt, const Fsai& F, const 
     float* hL = h_.p + kGnnLayers * nh;
     lin_fwd<H, 9, false><<<gn, 256, 0, s>>>(nn, hL, W + GnnLayout::Wa, nullptr, an_.p);
     lin_fwd<H, 9, false><<<gn, 256, 0, s>>>(nn, hL, W + GnnLayout::Wb, nullptr, bn_.p);
-    if (train) MPHY_CUDA(cudaMemsetAsync(loss_.p, 0, sizeof(double), s));
-    const float inv_count = 1.f / (9.f * (float)nl);
-    dec_fwd<<<stride_grid(nl, 256, sm), 256, 0, s>>>(A, aval, f32, fixed, g.base.p, nl, g.lrow_of.p, L.col.p, g.lslot.p, g.sqrt_s.p, an_.p,
-                                                     bn_.p, W + GnnLayout::Wc, W + GnnLayout::bo,
-                                                     train ? g.target.p : nullptr, inv_count,
-                                                     (train && compute_grad) ? dout_.p : nullptr, out_blocks,
-                                                     train ? loss_.p : nullptr);
+    dec_fwd<<<stride_grid(nl, 256, sm), 256, 0, s>>>(A, aval, f32, fixed, g.base.p, nl, g.lrow_of.p, L.col.p,
+                                                     g.lslot.p, g.sqrt_s.p, an_.p, bn_.p, W + GnnLayout::Wc,
+                                                     W + GnnLayout::bo, train ? ghat_.p : nullptr, out_blocks);
     launches += 4;
+    if (train) {
+        kaporin_rows<<<stride_grid((int64_t)nn * 32, 256, sm, 16), 256, 0, s>>>(
+            A, aval, f32, nn, Pt->brow_ptr.p, Pt->bcol.p, L.rowptr.p, L.col.p, g.sqrt_s.p, ghat_.p, tbuf_.p,
+            part_tr_.p, part_ld_.p);
+        kaporin_reduce<<<1, 1024, 0, s>>>(nn, part_tr_.p, part_ld_.p, red_.p, loss_.p);
+        launches += 2;
+        if (compute_grad) {
+            kaporin_grad<<<stride_grid(nl, 256, sm), 256, 0, s>>>(nl, nn, g.lrow_of.p, L.col.p, fixed, g.base.p,
+                                                                  ghat_.p, tbuf_.p, red_.p, dout_.p);
+            launches += 1;
+        }
+    }
     MPHY_CUDA(cudaGetLastError());
     double loss = 0.0;
     if (train && compute_grad) {

@@ -37,9 +37,8 @@ struct GnnGraph {
     DevBuf<int32_t> lslot;    // [n_lower] position of the lower block (n, m) in A's row n
     DevBuf<int32_t> lrow_of;  // [n_lower] row n of every lower block
     DevBuf<int64_t> u2l;      // [n_lower] compact lower index of the k-th upper entry (G^T rows)
-    DevBuf<float> target;     // [n_lower][9] scaled exact FSAI blocks (training only)
     DevBuf<float> base;       // [n_node][9] block-Jacobi FSAI diagonal blocks (scaled units)
-    bool has_target = false;
+    bool training = false;    // run() evaluates the loss (and gradients)
 };
 
 class Gnn {
@@ -48,12 +47,12 @@ class Gnn {
     void set_params(const float* host);
     void get_params(float* host) const;
     void get_grads(float* host) const;
-    // Features of the assembled operator of `s` (and, when fsai_target is given, the scaled exact
-    // FSAI blocks as training targets).
+    // Features of the assembled operator (training: run() also evaluates the loss).
     void build_graph(GnnGraph& g, const mphy_pattern* P, const Fsai& F, const SellView& A, const void* aval,
-                     bool fp32_values, const uint8_t* fixed, const float* fsai_blocks, cudaStream_t s);
+                     bool fp32_values, const uint8_t* fixed, bool training, cudaStream_t s);
     // Forward pass; writes predicted G blocks (unscaled, FP32) into out_blocks when non-null.
-    // With a target, returns the loss and (compute_grad) accumulates gradients.
+    // For a training graph, returns the Kaporin loss log K(G A G^T) - (1/N) log det A^ and
+    // (compute_grad) accumulates its gradients.
     double run(const GnnGraph& g, const mphy_pattern* P, const Fsai& F, const SellView& A, const void* aval,
                bool fp32_values, const uint8_t* fixed, float* out_blocks, bool compute_grad, cudaStream_t s);
     void zero_grads(cudaStream_t s);
@@ -71,6 +70,8 @@ class Gnn {
     int64_t ws_lower_ = 0;
     // activations: h_l for l = 0..L ([n][H] each), P, msg, q per layer, decoder partials
     DevBuf<float> h_, P_, msg_, q_, dh_, dP_, dmsg_, dq_, an_, bn_, dout_, dan_, dbn_;
+    DevBuf<float> ghat_, tbuf_;        // predicted scaled blocks, T_j of the loss
+    DevBuf<double> part_tr_, part_ld_, red_;
 };
 
 }  // namespace mphy

@@ -2,8 +2,9 @@
 training on operators the solver assembles, and persistence of the trained weights.
 
 The network (csrc/gnn.cu) predicts the blocks of G in M = G^T G from the Jacobi-scaled operator,
-as a correction to block-Jacobi FSAI (so an untrained network is block-Jacobi); the targets are
-the exact block FSAI the library computes for the same operator. Training runs
+as a correction to block-Jacobi FSAI (so an untrained network is block-Jacobi). Training minimises
+Kaporin's condition number of G A G^T (the functional exact FSAI minimises), so it needs no
+targets. Training runs
 entirely in libmphy.so's forward/backward/Adam kernels; this module only orders the steps.
 """
 from __future__ import annotations
@@ -44,7 +45,8 @@ def init_params(seed: int = 0) -> np.ndarray:
         zeros(H)           # d
     lin(9, H, 0.1)         # Wa
     lin(9, H, 0.1)         # Wb
-    zeros(81)              # Wc: the network starts as block-Jacobi FSAI (its correction is small)
+    zeros(81)              # Wc
+    # zero decoder weights: the network starts as block-Jacobi FSAI (a valid SPD preconditioner)
     zeros(9)
     p = np.concatenate(parts).astype(np.float32)
     assert p.size == param_count(), (p.size, param_count())

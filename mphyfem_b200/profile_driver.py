@@ -3,6 +3,7 @@
     python -m mphyfem_b200.profile_driver --op spmv --nx 128 --ny 32 --nz 32 --reps 4
     python -m mphyfem_b200.profile_driver --op spmv --precision mixed --reps 4
     python -m mphyfem_b200.profile_driver --op assemble --nx 128 --ny 32 --nz 32 --reps 3
+    python -m mphyfem_b200.profile_driver --op assemble --precision mixed_tc --reps 3
     python -m mphyfem_b200.profile_driver --op newton --precision mixed --coarse 64 --reps 1
     python -m mphyfem_b200.profile_driver --op batch --instances 48 --reps 2
 
@@ -25,7 +26,7 @@ def main(argv=None):
     ap.add_argument("--nz", type=int, default=32)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--rtol", type=float, default=1e-8)
-    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--precision", choices=["fp64", "mixed", "mixed_tc"], default="fp64")
     ap.add_argument("--pc", choices=["jacobi", "fsai"], default="jacobi")
     ap.add_argument("--coarse", type=int, default=0)
     ap.add_argument("--instances", type=int, default=48)
@@ -36,7 +37,7 @@ def main(argv=None):
     import torch
 
     from . import _lib, api, meshgen
-    prec = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED}[args.precision]
+    prec = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED, "mixed_tc": _lib.PREC_MIXED_TC}[args.precision]
     ctx = api.Context(0)
     if args.op == "batch":
         probs = meshgen.batched_blocks(512, seed=11)[:args.instances]

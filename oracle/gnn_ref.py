@@ -2,8 +2,9 @@
 the CPU. Test infrastructure only: the checker for the GPU forward and backward kernels.
 
 Features follow the GPU: A^ = D^{-1/2} A D^{-1/2} with prescribed DOFs as identity rows; node
-input = A^_nn (9), prescribed flags (3), (neighbours - 1) / 27; edge input = A^_nm; targets the
-exact FSAI blocks scaled by the column's sqrt(diag). Weights are rounded to BF16 as on the GPU.
+input = A^_nn (9), prescribed flags (3), (neighbours - 1) / 27; edge input = A^_nm (off-diagonal
+blocks); prediction base_n P with base_n the block-Jacobi FSAI block; loss Kaporin's condition
+number of G^ A^ G^T (dense, small problems only). Weights are rounded to BF16 as on the GPU.
 """
 from __future__ import annotations
 
@@ -37,9 +38,10 @@ def layout():
     return off, o
 
 
-def loss_and_grads(params, A_full, fixed, nbrs, lrow, lcol, gblocks):
+def loss_and_grads(params, A_full, fixed, nbrs, lrow, lcol):
     """params: flat float32; A_full: scipy node-major operator; nbrs: ascending neighbour lists;
-    (lrow, lcol): lower pattern; gblocks: [n_lower, 3, 3] exact FSAI (unscaled).
+    (lrow, lcol): lower pattern. Loss: Kaporin's log K of G^ A^ G^T up to the constant
+    (1/N) log det A^, i.e. log(tr(G^ A^ G^T) / N) - (2/N) sum_n log|det G^_nn| (N = 3 n_node).
     Returns (loss, flat gradient, predicted unscaled blocks)."""
     off, total = layout()
     p32 = torch.tensor(np.asarray(params, np.float32))
@@ -82,14 +84,14 @@ def loss_and_grads(params, A_full, fixed, nbrs, lrow, lcol, gblocks):
         q = h @ W(f"S{l}", (H, H)).T + msg @ W(f"T{l}", (H, H)).T + W(f"d{l}", (H,))
         h = h + torch.relu(q)
     rows = np.repeat(np.arange(n_node), np.diff(lrow))
-    el = torch.tensor(np.array([blk(n, m).ravel() for n, m in zip(rows, lcol)]))
+    # the edge term acts on off-diagonal blocks only
+    el = torch.tensor(np.array([blk(n, m).ravel() if n != m else np.zeros(9) for n, m in zip(rows, lcol)]))
     out = (h[torch.tensor(rows)] @ W("Wa", (9, H)).T + h[torch.tensor(lcol.astype(np.int64))] @ W("Wb", (9, H)).T
            + el @ W("Wc", (9, 9)).T + W("bo", (9,)))
-    # the network corrects block-Jacobi FSAI (gnn.cu base_kernel): G_nn = L^T, L L^T = (A^_nn)^-1
-    base = np.zeros((len(rows), 9))
-    for j, (n, m) in enumerate(zip(rows, lcol)):
-        if n != m:
-            continue
+    # the prediction is base_n P with P = decoder + [n == m] I, base_n the block-Jacobi FSAI
+    # (gnn.cu base_kernel): G_nn = L^T, L L^T = (A^_nn)^-1
+    base_node = np.zeros((n_node, 3, 3))
+    for n in range(n_node):
         B = blk(n, n)
         B = 0.5 * (B + B.T)
         g = np.eye(3)
@@ -98,8 +100,10 @@ def loss_and_grads(params, A_full, fixed, nbrs, lrow, lcol, gblocks):
                 g = np.linalg.cholesky(np.linalg.inv(B)).T
             except np.linalg.LinAlgError:
                 g = np.eye(3)
-        base[j] = g.ravel()
-    out = out + torch.tensor(base)
+        base_node[n] = g
+    eye_rows = np.array([np.eye(3).ravel() if n == m else np.zeros(9) for n, m in zip(rows, lcol)])
+    P = (out + torch.tensor(eye_rows)).view(-1, 3, 3)
+    out = torch.bmm(torch.tensor(base_node[rows]), P).reshape(-1, 9)
     # entries with a prescribed row or column DOF are fixed to the identity (gnn.cu dec_fwd)
     keep = np.ones((len(rows), 3, 3))
     ident = np.zeros((len(rows), 3, 3))
@@ -110,8 +114,19 @@ def loss_and_grads(params, A_full, fixed, nbrs, lrow, lcol, gblocks):
     keep_t, ident_t = torch.tensor(keep.reshape(-1, 9)), torch.tensor(ident.reshape(-1, 9))
     out = out * keep_t + ident_t
     scol = torch.tensor(np.stack([s[3 * m:3 * m + 3] for m in lcol]))          # [n_lower, 3]
-    tgt = torch.tensor(np.asarray(gblocks, np.float64).reshape(-1, 3, 3)) * scol[:, None, :]
-    loss = ((out.view(-1, 3, 3) - tgt) ** 2).mean()
+    N = 3 * n_node
+    Gd = torch.zeros((N, N), dtype=torch.float64)
+    blocks = out.view(-1, 3, 3)
+    for j, (n, m) in enumerate(zip(rows, lcol)):
+        Gd[3 * n:3 * n + 3, 3 * m:3 * m + 3] = blocks[j]
+    Ah = np.zeros((N, N))
+    for n in range(n_node):
+        for m in nbrs[n]:
+            Ah[3 * n:3 * n + 3, 3 * m:3 * m + 3] = blk(n, m)
+    tr = torch.trace(Gd @ torch.tensor(Ah) @ Gd.T)
+    diag = [j for j, (n, m) in enumerate(zip(rows, lcol)) if n == m]
+    logdet = sum(torch.log(torch.abs(torch.det(blocks[j]))) for j in diag)
+    loss = torch.log(tr / N) - 2.0 / N * logdet
     loss.backward()
-    pred = (out.view(-1, 3, 3) / scol[:, None, :]).detach().numpy()
+    pred = (blocks / scol[:, None, :]).detach().numpy()
     return float(loss.detach()), pb.grad.numpy().copy(), pred

@@ -1,8 +1,9 @@
 """Learned FSAI: GPU forward/backward against the FP64 torch restatement, training, and what the
 trained network gains over Jacobi-PCG (the method without it), with the true-residual fallback.
 
-Tolerances: loss within 1e-4 relative; every parameter tensor's gradient within 2e-3 relative
-(FP32 atomics and FP32 features on the GPU against FP64 on the CPU, same BF16 weights)."""
+Loss: Kaporin's condition number of the preconditioned operator. Tolerances: loss within 1e-4
+relative; every parameter tensor's gradient within 2e-3 relative (FP32 atomics and FP32 features
+on the GPU against FP64 on the CPU, same BF16 weights)."""
 import numpy as np
 import pytest
 
@@ -38,14 +39,13 @@ def test_gnn_loss_and_gradients_match_oracle(env, prec):
     params = learned.init_params(seed=1)
     gnn = learned.Gnn(ctx, params)
     loss, grads = gnn.loss_and_grads(sol)
-    G = sol.pc_get_blocks().cpu().numpy()            # the exact FSAI targets the GPU used
     lrow, lcol = sol.pc_pattern()
     val, _, _ = sol.export(want_rhs=False, want_reac=False)
     rp, col = pat.export_csr()
     A = fsai_ref.full_operator(p.n_node, p.fixed, rp, col, val)
     nbrs = fsai_ref.node_neighbours(p.conn, p.n_node)
-    loss_ref, grads_ref, _ = gnn_ref.loss_and_grads(params, A, p.fixed, nbrs, lrow, lcol, G)
-    assert abs(loss - loss_ref) <= 1e-4 * loss_ref
+    loss_ref, grads_ref, _ = gnn_ref.loss_and_grads(params, A, p.fixed, nbrs, lrow, lcol)
+    assert abs(loss - loss_ref) <= 1e-4 * max(abs(loss_ref), 1.0)
     off, _ = gnn_ref.layout()
     for name, (o, n) in off.items():
         g, r = grads[o:o + n], grads_ref[o:o + n]
@@ -61,7 +61,8 @@ def trained(env):
 
 def test_training_reduces_loss(trained):
     _, losses = trained
-    assert losses[-20:].mean() < 0.5 * losses[:4].mean(), (losses[:4], losses[-20:])
+    # log K falls from its block-Jacobi start (zero decoder weights)
+    assert losses[-20:].mean() < losses[:4].mean() - 0.02, (losses[:4], losses[-20:])
 
 
 # FP64: rtol 1e-10. Mixed: the FP32-stored operator bounds the FP64 true residual near 1e-9 without
