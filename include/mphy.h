@@ -252,8 +252,9 @@ int mphy_gnn_predict(mphy_gnn* g, mphy_solver* s, float* ms);
  * FP64; otherwise they are repeated with the Jacobi local part (see mphy_solver_pc_last). */
 int mphy_solver_attach_gnn(mphy_solver* s, mphy_gnn* g);
 /* Last solve: *fallback = 1 when a learned preconditioner failed the FP64 true-residual check and
- * the solve was repeated with the Jacobi local part; *setup_ms = the preconditioner's setup time
- * (FSAI, network inference or coarse operator); first_*: status, iterations and true relative
+ * the solve was repeated with the Jacobi local part; *setup_ms = the local preconditioner's setup
+ * time (exact FSAI or network inference; the coarse operator's is in mphy_solver_coarse_info);
+ * first_*: status, iterations and true relative
  * residual of the learned attempt. Any pointer may be NULL. */
 int mphy_solver_pc_last(const mphy_solver* s, int32_t* fallback, float* setup_ms, int32_t* first_status,
                         int32_t* first_its, double* first_relres);

@@ -164,7 +164,6 @@ int solver_solve_once(mphy_solver* s, int32_t* its, double* fnorm) {
         // the coarse operator follows the assembled matrix
         if (s->mixed) s->coarse.setup<float>(s->A, s->valf.p, nullptr, s->ctx->stream);
         else s->coarse.setup<double>(s->A, s->val.p, nullptr, s->ctx->stream);
-        s->t_pc_ms = s->coarse.last_setup_ms;
         s->launches += s->coarse.launches;
     }
     if (s->mixed) {

@@ -82,6 +82,20 @@ __global__ void __launch_bounds__(256) coarse_matrix_kernel(SellView A, const VT
             const int lane = (int)(n & 31);
             const int64_t base = A.slice_base[s];
             const int w = A.slice_width[s];
+            // T = sum_m A_nm Z_m accumulated per neighbour aggregate (a node's neighbours are
+            // ascending, so they change aggregate rarely); E[a][slot] += Z_n^T T flushed once per
+            // aggregate run instead of once per block
+            double T[3][6] = {{0}};
+            int cur = -1;
+            auto flush = [&](int slot) {
+                for (int i2 = 0; i2 < 6; ++i2)
+                    for (int j = 0; j < 6; ++j) {
+                        const double v = Zn[0][i2] * T[0][j] + Zn[1][i2] * T[1][j] + Zn[2][i2] * T[2][j];
+                        if (v != 0.0) atomicAdd(&Eloc[slot][6 * i2 + j], v);
+                    }
+                for (int r = 0; r < 3; ++r)
+                    for (int j = 0; j < 6; ++j) T[r][j] = 0.0;
+            };
             for (int k = 0; k <= w; ++k) {
                 double blk[9];
                 int64_t m;
@@ -110,17 +124,17 @@ __global__ void __launch_bounds__(256) coarse_matrix_kernel(SellView A, const VT
                     continue;
                 }
                 const int slot = (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1);
+                if (slot != cur) {
+                    if (cur >= 0) flush(cur);
+                    cur = slot;
+                }
                 double Zm[3][6];
                 node_modes(cv.d, cv.fixed, m, Zm);
-                double Tm[3][6];
                 for (int r = 0; r < 3; ++r)
-                    for (int j = 0; j < 6; ++j) Tm[r][j] = blk[3 * r] * Zm[0][j] + blk[3 * r + 1] * Zm[1][j] + blk[3 * r + 2] * Zm[2][j];
-                for (int i2 = 0; i2 < 6; ++i2)
-                    for (int j = 0; j < 6; ++j) {
-                        const double v = Zn[0][i2] * Tm[0][j] + Zn[1][i2] * Tm[1][j] + Zn[2][i2] * Tm[2][j];
-                        if (v != 0.0) atomicAdd(&Eloc[slot][6 * i2 + j], v);
-                    }
+                    for (int j = 0; j < 6; ++j)
+                        T[r][j] += blk[3 * r] * Zm[0][j] + blk[3 * r + 1] * Zm[1][j] + blk[3 * r + 2] * Zm[2][j];
             }
+            if (cur >= 0) flush(cur);
         }
         __syncthreads();
         for (int t = threadIdx.x; t < 27 * 36; t += blockDim.x) {
@@ -269,31 +283,39 @@ __global__ void __launch_bounds__(256) trtri_tile(const double* E, double* W, in
     store_tile(X, W, kp, i, i);
 }
 
-// W_ij = -W_ii sum_{k=j}^{i-1} L_ik W_kj   (j < i)
-__global__ void __launch_bounds__(256) trtri_row(const double* E, double* W, int kp, int i) {
+// Right-looking W = L^{-1}: the strictly lower tiles of W first accumulate
+// S_ij = sum_{k < i} L_ik W_kj; once tile row i is complete, W_ij = -W_ii S_ij. Step k finalises
+// tile row k (k CTAs, one tile product each) and adds L_ik W_kj to every S_ij with i > k, j <= k
+// (one CTA per tile, all independent), so no CTA runs a chain of products.
+__global__ void __launch_bounds__(256) trtri_finalize(double* W, int kp, int k) {
     extern __shared__ double sm[];
     double (*A)[TP] = reinterpret_cast<double (*)[TP]>(sm);
     double (*B)[TP] = reinterpret_cast<double (*)[TP]>(sm + T * TP);
     const int j = blockIdx.x;
     const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;
-    double acc[4][4] = {{0}};
-    for (int k = j; k < i; ++k) {
-        load_tile(A, E, kp, i, k);  // L_ik
-        // B = W_kj^T so that tile_abt gives L_ik W_kj
-        for (int t = threadIdx.x; t < T * T; t += blockDim.x) B[t % T][t / T] = W[(int64_t)(k * T + t / T) * kp + j * T + t % T];
-        __syncthreads();
-        tile_abt(A, B, acc);
-        __syncthreads();
-    }
-    // S -> shared, then W_ij = -W_ii S
-    for (int q = 0; q < 4; ++q)
-        for (int r = 0; r < 4; ++r) B[tx + 16 * r][ty + 16 * q] = acc[q][r];  // B = S^T
-    load_tile(A, W, kp, i, i);
+    load_tile(A, W, kp, k, k);  // W_kk
+    for (int t = threadIdx.x; t < T * T; t += blockDim.x) B[t % T][t / T] = W[(int64_t)(k * T + t / T) * kp + j * T + t % T];
     __syncthreads();
-    double o[4][4] = {{0}};
-    tile_abt(A, B, o);
+    double acc[4][4] = {{0}};
+    tile_abt(A, B, acc);  // W_kk S_kj
     for (int q = 0; q < 4; ++q)
-        for (int r = 0; r < 4; ++r) W[(int64_t)(i * T + ty + 16 * q) * kp + j * T + tx + 16 * r] = -o[q][r];
+        for (int r = 0; r < 4; ++r) W[(int64_t)(k * T + ty + 16 * q) * kp + j * T + tx + 16 * r] = -acc[q][r];
+}
+
+__global__ void __launch_bounds__(256) trtri_update(const double* E, double* W, int kp, int k, int nb) {
+    extern __shared__ double sm[];
+    double (*A)[TP] = reinterpret_cast<double (*)[TP]>(sm);
+    double (*B)[TP] = reinterpret_cast<double (*)[TP]>(sm + T * TP);
+    const int rows = nb - k - 1;
+    const int i = k + 1 + (int)(blockIdx.x % rows), j = (int)(blockIdx.x / rows);
+    const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;
+    load_tile(A, E, kp, i, k);  // L_ik
+    for (int t = threadIdx.x; t < T * T; t += blockDim.x) B[t % T][t / T] = W[(int64_t)(k * T + t / T) * kp + j * T + t % T];
+    __syncthreads();
+    double acc[4][4] = {{0}};
+    tile_abt(A, B, acc);  // L_ik W_kj
+    for (int q = 0; q < 4; ++q)
+        for (int r = 0; r < 4; ++r) W[(int64_t)(i * T + ty + 16 * q) * kp + j * T + tx + 16 * r] += acc[q][r];
 }
 
 // E^{-1} = W^T W (tile (i, j) = sum_{k >= max(i,j)} W_ki^T W_kj), stored FP64
@@ -417,7 +439,8 @@ void CoarseSpace::setup(const SellView& A, const VT* aval, const double* disp, c
         MPHY_CUDA(cudaFuncSetAttribute(syrk_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
         MPHY_CUDA(cudaFuncSetAttribute(trsm_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
         MPHY_CUDA(cudaFuncSetAttribute(trtri_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
-        MPHY_CUDA(cudaFuncSetAttribute(trtri_row, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
+        MPHY_CUDA(cudaFuncSetAttribute(trtri_finalize, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
+        MPHY_CUDA(cudaFuncSetAttribute(trtri_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
         MPHY_CUDA(cudaFuncSetAttribute(inverse_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
         attr = true;
     }
@@ -431,10 +454,17 @@ void CoarseSpace::setup(const SellView& A, const VT* aval, const double* disp, c
         }
         launches += 1;
     }
-    for (int i = 0; i < nb; ++i) {
-        trtri_tile<<<1, 256, sm2, s>>>(E_.p, W_.p, kp_, i);
-        if (i > 0) trtri_row<<<i, 256, sm2, s>>>(E_.p, W_.p, kp_, i);
-        launches += i > 0 ? 2 : 1;
+    for (int k = 0; k < nb; ++k) {
+        trtri_tile<<<1, 256, sm2, s>>>(E_.p, W_.p, kp_, k);
+        launches += 1;
+        if (k > 0) {
+            trtri_finalize<<<k, 256, sm2, s>>>(W_.p, kp_, k);
+            launches += 1;
+        }
+        if (k < nb - 1) {
+            trtri_update<<<(nb - k - 1) * (k + 1), 256, sm2, s>>>(E_.p, W_.p, kp_, k, nb);
+            launches += 1;
+        }
     }
     inverse_tiles<<<nb * nb, 256, sm2, s>>>(W_.p, einv_.p, kp_, nb);
     launches += 1;
