@@ -191,10 +191,8 @@ int solver_solve_once(mphy_solver* s, int32_t* its, double* fnorm) {
     cudaStream_t st = s->ctx->stream;
     const int sm = s->ctx->sm_count;
     const int64_t n = 3 * (int64_t)s->mesh->n_node;
-    if (s->ref_r.n != (size_t)n) {
-        s->ref_r.alloc(n);
-        s->ref_d.alloc(n);
-    }
+    if (s->ref_r.n != (size_t)n) s->ref_r.alloc(n);
+    if (s->ref_d.n != (size_t)n) s->ref_d.alloc(n);
     double bb = 0.0, rr = 0.0;
     dot_fp64(s->rhs.p, s->rhs.p, n, s->partials.p, s->counter.p, s->scalar.p, st, sm);
     MPHY_CUDA(cudaMemcpyAsync(&bb, s->scalar.p, sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -234,7 +232,8 @@ double true_relres(mphy_solver* s) {
     cudaStream_t st = s->ctx->stream;
     const int sm = s->ctx->sm_count;
     const int64_t n = 3 * (int64_t)s->mesh->n_node;
-    DevBuf<double> r(n);
+    if (s->ref_r.n != (size_t)n) s->ref_r.alloc(n);  // kept: no allocation per check
+    DevBuf<double>& r = s->ref_r;
     if (s->mixed)
         residual_fp64<float>(s->A, s->valf.p, s->x.p, s->rhs.p, r.p, s->partials.p, s->counter.p, s->scalar.p, st, sm);
     else
@@ -601,7 +600,7 @@ int mphy_solver_create(mphy_ctx* c, const mphy_mesh* m, const mphy_pattern* P, c
             if (o.pc_type != MPHY_PC_JACOBI) {
                 s->use_fsai = true;
                 s->fsai.init(c, P, 16);
-                const FactorView<float> fv = s->fsai.view();
+                const FactorView<FactorT> fv = s->fsai.view();
                 if (o.precision == MPHY_PREC_MIXED || o.precision == MPHY_PREC_MIXED_TC) s->ir.inner().set_factor(fv);
                 else if (o.precision == MPHY_PREC_MIXED_F32VEC) s->ir32.inner().set_factor(fv);
                 else s->pcg.set_factor(fv);
@@ -1056,9 +1055,10 @@ int mphy_gnn_predict(mphy_gnn* g, mphy_solver* s, float* ms) {
         const void* aval = s->mixed ? (const void*)s->valf.p : (const void*)s->val.p;
         MPHY_CUDA(cudaEventRecord(s->ctx->ev0, st));
         g->net.build_graph(s->graph, s->pat, s->fsai, s->A, aval, s->mixed, s->mesh->fixed.p, false, st);
-        DevBuf<float> blocks(9 * (size_t)s->fsai.lower().n_blocks);
-        g->net.run(s->graph, s->pat, s->fsai, s->A, aval, s->mixed, s->mesh->fixed.p, blocks.p, false, st);
-        s->fsai.set_lower_values(blocks.p, st);
+        const size_t nb = 9 * (size_t)s->fsai.lower().n_blocks;
+        if (s->pred_blocks.n != nb) s->pred_blocks.alloc(nb);  // kept: no allocation per solve
+        g->net.run(s->graph, s->pat, s->fsai, s->A, aval, s->mixed, s->mesh->fixed.p, s->pred_blocks.p, false, st);
+        s->fsai.set_lower_values(s->pred_blocks.p, st);
         MPHY_CUDA(cudaEventRecord(s->ctx->ev1, st));
         MPHY_CUDA(cudaEventSynchronize(s->ctx->ev1));
         float t = 0.f;

@@ -162,8 +162,8 @@ struct SetupArgs {
     const VT* aval;
     const double* diag64;  // mixed storage: FP64 diagonal blocks
     const uint8_t* fixed;  // mixed storage: prescribed DOFs are identity rows / zero columns
-    float* gval;
-    float* gtval;
+    FactorT* gval;
+    FactorT* gtval;
     int32_t* nfail;
 };
 
@@ -296,30 +296,30 @@ __global__ void __launch_bounds__(kWarps * 32) fsai_setup_kernel(SetupArgs<VT> a
         for (int t = lane; t < 9 * p; t += 32) {
             const int k = t / 9, v = t % 9, r = v / 3, c = v % 3;
             const float g = (float)Gr[r * NMAX + 3 * k + c];
-            a.gval[a.l2s[r0 + k] + 32 * (3 * r + c)] = g;
-            a.gtval[a.l2u[r0 + k] + 32 * (3 * c + r)] = g;
+            a.gval[a.l2s[r0 + k] + 32 * (3 * r + c)] = __float2bfloat16_rn((float)g);
+            a.gtval[a.l2u[r0 + k] + 32 * (3 * c + r)] = __float2bfloat16_rn((float)g);
         }
         __syncwarp();
     }
 }
 
 __global__ void set_lower_kernel(int64_t n_lower, const float* __restrict__ blocks, const int64_t* __restrict__ l2s,
-                                 const int64_t* __restrict__ l2u, float* __restrict__ gval, float* __restrict__ gtval) {
+                                 const int64_t* __restrict__ l2u, FactorT* __restrict__ gval, FactorT* __restrict__ gtval) {
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < 9 * n_lower; t += (int64_t)gridDim.x * blockDim.x) {
         const int64_t j = t / 9;
         const int v = (int)(t % 9), r = v / 3, c = v % 3;
         const float g = blocks[t];
-        gval[l2s[j] + 32 * (3 * r + c)] = g;
-        gtval[l2u[j] + 32 * (3 * c + r)] = g;
+        gval[l2s[j] + 32 * (3 * r + c)] = __float2bfloat16_rn(g);
+        gtval[l2u[j] + 32 * (3 * c + r)] = __float2bfloat16_rn(g);
     }
 }
 
-__global__ void get_lower_kernel(int64_t n_lower, const float* __restrict__ gval, const int64_t* __restrict__ l2s,
+__global__ void get_lower_kernel(int64_t n_lower, const FactorT* __restrict__ gval, const int64_t* __restrict__ l2s,
                                  float* __restrict__ out) {
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < 9 * n_lower; t += (int64_t)gridDim.x * blockDim.x) {
         const int64_t j = t / 9;
         const int v = (int)(t % 9);
-        out[t] = gval[l2s[j] + 32 * v];
+        out[t] = __bfloat162float(gval[l2s[j] + 32 * v]);
     }
 }
 
@@ -414,8 +414,8 @@ int32_t Fsai::fallback_rows(cudaStream_t s) const {
     return h;
 }
 
-FactorView<float> Fsai::view() const {
-    FactorView<float> f;
+FactorView<FactorT> Fsai::view() const {
+    FactorView<FactorT> f;
     f.G = L_.view();
     f.GT = U_.view();
     f.gval = gval_.p;

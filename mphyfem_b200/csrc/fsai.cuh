@@ -27,7 +27,7 @@ class Fsai {
     // (the nearest, i.e. largest indices, are kept) so the local systems fit shared memory.
     void init(mphy_ctx* ctx, const mphy_pattern* A, int max_lower = 16);
     // Exact block FSAI of the assembled operator (values VT: double or float), FP64 local
-    // Cholesky per block row, G and G^T stored in FP32.
+    // Cholesky per block row, G and G^T stored in BF16 (FactorT).
     // diag64 / fixed: the null-space-preserving storage of the mixed path (null for FP64).
     template <typename VT>
     void compute(const VT* aval, const double* diag64, const uint8_t* fixed, cudaStream_t s);
@@ -36,7 +36,7 @@ class Fsai {
     void set_lower_values(const float* gblocks, cudaStream_t s);
     // lower-pattern blocks of G in compact order [n_blocks][9] (for training and checks)
     void get_lower_values(float* out_dev, cudaStream_t s) const;
-    FactorView<float> view() const;
+    FactorView<FactorT> view() const;
     const SellPattern& lower() const { return L_; }
     const SellPattern& upper() const { return U_; }
     int max_lower() const { return max_lower_; }
@@ -48,7 +48,7 @@ class Fsai {
     const mphy_pattern* A_ = nullptr;
     int max_lower_ = 16;
     SellPattern L_, U_;
-    DevBuf<float> gval_, gtval_;       // SELL values of G and G^T
+    DevBuf<FactorT> gval_, gtval_;     // SELL values of G and G^T
     DevBuf<int64_t> l2sell_;           // compact lower block -> SELL value offset in G
     DevBuf<int64_t> l2usell_;          // compact lower block (n, m) -> SELL value offset of (m, n) in G^T
     DevBuf<int32_t> err_;

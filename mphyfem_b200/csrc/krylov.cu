@@ -36,6 +36,11 @@ struct AccOf {
     using type = T;
 };
 
+// matrix value -> arithmetic (FP64 / FP32 values as they are, BF16 factor values widened)
+__device__ __forceinline__ double mval(double x) { return x; }
+__device__ __forceinline__ float mval(float x) { return x; }
+__device__ __forceinline__ float mval(__nv_bfloat16 x) { return __bfloat162float(x); }
+
 // Deterministic block sum (fixed butterfly per warp, fixed order across warps); valid in all
 // threads of warp 0.
 __device__ __forceinline__ double block_sum(double v, double* sh) {
@@ -153,9 +158,9 @@ __global__ void __launch_bounds__(kThreads) spmv_kernel(SellView A, const VT* __
             const int64_t c = cp[32 * k];
             const Acc x0 = (Acc)x[3 * c], x1 = (Acc)x[3 * c + 1], x2 = (Acc)x[3 * c + 2];
             const VT* v = vp + 288 * (int64_t)k;
-            y0 += (Acc)v[0] * x0 + (Acc)v[32] * x1 + (Acc)v[64] * x2;
-            y1 += (Acc)v[96] * x0 + (Acc)v[128] * x1 + (Acc)v[160] * x2;
-            y2 += (Acc)v[192] * x0 + (Acc)v[224] * x1 + (Acc)v[256] * x2;
+            y0 += (Acc)mval(v[0]) * x0 + (Acc)mval(v[32]) * x1 + (Acc)mval(v[64]) * x2;
+            y1 += (Acc)mval(v[96]) * x0 + (Acc)mval(v[128]) * x1 + (Acc)mval(v[160]) * x2;
+            y2 += (Acc)mval(v[192]) * x0 + (Acc)mval(v[224]) * x1 + (Acc)mval(v[256]) * x2;
         }
         if (row < A.n_node) {
             if (A.diag64) {
@@ -199,7 +204,7 @@ __global__ void __launch_bounds__(kThreads) spmv_kernel(SellView A, const VT* __
 
 // z = G^T t with the fused (r, z), (z, z); INIT also sets p = z and the initial state.
 template <typename XT, bool INIT>
-__global__ void __launch_bounds__(kThreads) factor_apply_kernel(SellView A, CoarseView cv, const float* __restrict__ val,
+__global__ void __launch_bounds__(kThreads) factor_apply_kernel(SellView A, CoarseView cv, const FactorT* __restrict__ val,
                                                                 const XT* __restrict__ t, XT* __restrict__ z,
                                                                 const XT* __restrict__ r, XT* __restrict__ p,
                                                                 double* __restrict__ part_rz,
@@ -220,15 +225,15 @@ __global__ void __launch_bounds__(kThreads) factor_apply_kernel(SellView A, Coar
         const int w = A.slice_width[s];
         Acc y0 = 0, y1 = 0, y2 = 0;
         const int32_t* cp = A.col + base + lane;
-        const float* vp = val + 9 * base + lane;
+        const FactorT* vp = val + 9 * base + lane;
 #pragma unroll 2
         for (int k = 0; k < w; ++k) {
             const int64_t c = cp[32 * k];
             const Acc x0 = t[3 * c], x1 = t[3 * c + 1], x2 = t[3 * c + 2];
-            const float* v = vp + 288 * (int64_t)k;
-            y0 += (Acc)v[0] * x0 + (Acc)v[32] * x1 + (Acc)v[64] * x2;
-            y1 += (Acc)v[96] * x0 + (Acc)v[128] * x1 + (Acc)v[160] * x2;
-            y2 += (Acc)v[192] * x0 + (Acc)v[224] * x1 + (Acc)v[256] * x2;
+            const FactorT* v = vp + 288 * (int64_t)k;
+            y0 += (Acc)mval(v[0]) * x0 + (Acc)mval(v[32]) * x1 + (Acc)mval(v[64]) * x2;
+            y1 += (Acc)mval(v[96]) * x0 + (Acc)mval(v[128]) * x1 + (Acc)mval(v[160]) * x2;
+            y2 += (Acc)mval(v[192]) * x0 + (Acc)mval(v[224]) * x1 + (Acc)mval(v[256]) * x2;
         }
         if (row < A.n_node) {
             if (cv.n_agg > 0) {  // two-level: + Z c
@@ -716,7 +721,7 @@ void Pcg<VT, XT>::record_iterations(const VT* val, XT* x, cudaStream_t s, int n_
             pcg_update_kernel<XT, false><<<gv, kThreads, 0, s>>>(n_, x, r_.p, z_.p, p_.p, q_.p, nullptr, nullptr,
                                                                   nullptr, st_.p);
             const unsigned gg = stride_grid((int64_t)factor_.G.n_slices * 32, kThreads, sm_);
-            spmv_kernel<float, XT, false><<<gg, kThreads, 0, s>>>(factor_.G, factor_.gval, r_.p, t_.p, nullptr, st_.p);
+            spmv_kernel<FactorT, XT, false><<<gg, kThreads, 0, s>>>(factor_.G, factor_.gval, r_.p, t_.p, nullptr, st_.p);
             if (kind_ == PcKind::FactorCoarse) {
                 coarse_restrict_kernel<XT><<<std::min(coarse_.n_agg, sm_ * 8), kThreads, 0, s>>>(coarse_, r_.p, st_.p);
                 coarse_gemv_kernel<<<stride_grid((int64_t)coarse_.kp * 32, kThreads, sm_), kThreads, 0, s>>>(coarse_,
@@ -754,7 +759,7 @@ int Pcg<VT, XT>::solve(const VT* val, const XT* b, XT* x, double rtol, double ab
         pcg_init_kernel<XT, false><<<gv, kThreads, 0, s>>>(n_, b, x, r_.p, z_.p, p_.p, nullptr, nullptr, nullptr,
                                                             st_.p, rtol, abstol, dtol, maxit, norm_type);
         const unsigned gg = stride_grid((int64_t)factor_.G.n_slices * 32, kThreads, sm_);
-        spmv_kernel<float, XT, false><<<gg, kThreads, 0, s>>>(factor_.G, factor_.gval, r_.p, t_.p, nullptr, nullptr);
+        spmv_kernel<FactorT, XT, false><<<gg, kThreads, 0, s>>>(factor_.G, factor_.gval, r_.p, t_.p, nullptr, nullptr);
         if (kind_ == PcKind::FactorCoarse) {
             coarse_restrict_kernel<XT><<<std::min(coarse_.n_agg, sm_ * 8), kThreads, 0, s>>>(coarse_, r_.p, nullptr);
             coarse_gemv_kernel<<<stride_grid((int64_t)coarse_.kp * 32, kThreads, sm_), kThreads, 0, s>>>(coarse_,

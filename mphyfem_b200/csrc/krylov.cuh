@@ -1,6 +1,8 @@
 // krylov.cuh -- K4/K5: SELL-32 3x3 SpMV, preconditioned CG with PETSc KSPCG semantics (FP64, or
 // FP32 vectors with FP64 reductions), FP64 iterative refinement, and the vector operations.
 #pragma once
+#include <cuda_bf16.h>
+
 #include "common.cuh"
 
 #include "coarse_view.cuh"
@@ -40,8 +42,11 @@ struct SellView {
     const uint8_t* fixed = nullptr;
 };
 
-// Factorised preconditioner M = G^T G: G lower block-triangular and G^T, both in SELL layout
-// with FP32 values.
+// Factorised preconditioner M = G^T G: G lower block-triangular and G^T, both in SELL layout.
+// The factor is stored in BF16: M = G^T G is symmetric positive definite for every nonsingular
+// G, so rounding G changes the preconditioner's quality by its 2^-9 relative error, never its
+// validity, and the two factor SpMVs of every iteration stream half the bytes of FP32.
+using FactorT = __nv_bfloat16;
 template <typename VT>
 struct FactorView {
     SellView G, GT;
@@ -73,7 +78,7 @@ template <typename VT, typename XT>
 class Pcg {
   public:
     void init(const SellView& A, int sm_count, int chunk);
-    void set_factor(const FactorView<float>& f) { factor_ = f; kind_ = PcKind::Factor; }
+    void set_factor(const FactorView<FactorT>& f) { factor_ = f; kind_ = PcKind::Factor; }
     void set_jacobi() { kind_ = PcKind::Jacobi; }
     // the coarse correction adds to the current local part (Jacobi or G^T G)
     void set_coarse(const CoarseView& c) {
@@ -90,7 +95,7 @@ class Pcg {
     void record_iterations(const VT* val, XT* x, cudaStream_t s, int n_iter);
     SellView A_{};
     PcKind kind_ = PcKind::Jacobi;
-    FactorView<float> factor_{};
+    FactorView<FactorT> factor_{};
     CoarseView coarse_{};
     int sm_ = 148, chunk_ = 32;
     int64_t n_ = 0;

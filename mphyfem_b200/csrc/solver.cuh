@@ -52,7 +52,8 @@ struct mphy_solver {
     DevBuf<double> partials, scalar;
     DevBuf<uint32_t> counter;
     DevBuf<double> disp_tmp, fext_tmp, disp_prev;
-    DevBuf<double> ref_r, ref_d;          // FP64 refinement sweeps (max_outer > 1)
+    DevBuf<double> ref_r, ref_d;          // FP64 refinement sweeps (max_outer > 1), true residual
+    DevBuf<float> pred_blocks;            // network-predicted G blocks (learned FSAI)
     PcgFp64 pcg;
     IterativeRefinement<double> ir;       // MIXED
     IterativeRefinement<float> ir32;      // MIXED_F32VEC

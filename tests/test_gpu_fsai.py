@@ -1,5 +1,6 @@
 """Block FSAI preconditioner (M = G^T G) against its numpy restatement, and FSAI-PCG against the
-FP64 oracle solve. G is stored in FP32: blocks agree within 1e-5 of the row's largest entry;
+FP64 oracle solve. G is stored in BF16 (8-bit mantissa): blocks agree within 4e-3 of the row's
+largest entry (one rounding, 2^-9 relative, of the FP64-computed blocks);
 FSAI-PCG solutions agree with the oracle's to 1e-9 at rtol 1e-12 and need fewer iterations
 than Jacobi-PCG."""
 import numpy as np
@@ -45,7 +46,7 @@ def test_fsai_blocks_match_restatement(env, mk, amp):
     assert np.array_equal(rp, orp) and np.array_equal(col, ocol)
     for n in range(p.n_node):
         g, o = G[rp[n]:rp[n + 1]], oblk[orp[n]:orp[n + 1]]
-        assert np.abs(g - o).max() <= 1e-5 * np.abs(o).max()
+        assert np.abs(g - o).max() <= 4e-3 * np.abs(o).max()
 
 
 @pytest.mark.parametrize("prec", ["PREC_FP64", "PREC_MIXED"])

@@ -113,7 +113,8 @@ def test_untrained_network_is_block_jacobi(env):
             assert np.abs(G[j]).max() < 1e-6
             continue
         Ann = A[3 * n:3 * n + 3, 3 * n:3 * n + 3].toarray()
-        np.testing.assert_allclose(G[j] @ Ann @ G[j].T, np.eye(3), atol=1e-4)
+        # G is stored in BF16 (2^-9 relative rounding)
+        np.testing.assert_allclose(G[j] @ Ann @ G[j].T, np.eye(3), atol=2e-2)
 
 
 def test_useless_network_falls_back_to_jacobi(env):
