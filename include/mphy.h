@@ -313,6 +313,11 @@ int mphy_batch_destroy(mphy_batch* b);
  * 512). The default is (1, 256); mphy_batch_autotune picks one by measurement. */
 int mphy_batch_set_schedule(mphy_batch* b, int32_t cluster, int32_t threads);
 int mphy_batch_get_schedule(const mphy_batch* b, int32_t* cluster, int32_t* threads);
+/* Two-level variant of the persistent solve: every instance is cut into `slabs` (1..8; 0 turns
+ * it off) slabs along its longest axis, and z = D^{-1} r + Z E^{-1} Z^T r with Z the six
+ * rigid-body modes of every slab (zero on prescribed DOFs) and E = Z^T A Z assembled, summed over
+ * the cluster and inverted in shared memory at the start of each instance's solve. */
+int mphy_batch_set_coarse(mphy_batch* b, int32_t slabs);
 /* Times every schedule on the assembled system (solves capped at maxit iterations; maxit <= 0:
  * complete solves, which also measures the load balance of the slowest instances) and keeps the
  * fastest. Writes up to max_candidates rows (cluster, threads, ms); *n_candidates = rows tried. */

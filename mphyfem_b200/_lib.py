@@ -132,6 +132,7 @@ SIGNATURES = {
     "mphy_batch_destroy": (C.c_int, [_vp]),
     "mphy_batch_set_schedule": (C.c_int, [_vp, C.c_int32, C.c_int32]),
     "mphy_batch_get_schedule": (C.c_int, [_vp, _i32, _i32]),
+    "mphy_batch_set_coarse": (C.c_int, [_vp, C.c_int32]),
     "mphy_batch_autotune": (C.c_int, [_vp, C.c_int32, C.c_int32, _i32, _i32, _i32, C.POINTER(C.c_float)]),
     "mphy_batch_solve": (C.c_int, [_vp, C.c_int32, _i32, _i32, _d, C.POINTER(C.c_float)]),
     "mphy_batch_instance_info": (C.c_int, [_vp, _i32, _i32, _i32, _d]),

@@ -360,6 +360,10 @@ class BatchGpu:
     def set_schedule(self, cluster: int, threads: int):
         L.check(self.lib.mphy_batch_set_schedule(self.h, cluster, threads))
 
+    def set_coarse(self, slabs: int):
+        """Two-level persistent solve: `slabs` rigid-body slabs per instance (0: Jacobi only)."""
+        L.check(self.lib.mphy_batch_set_coarse(self.h, slabs))
+
     def autotune(self, maxit: int = 0):
         """Times every schedule on the assembled system (maxit <= 0: complete solves); keeps the
         fastest. Returns rows (cluster, threads, ms)."""

@@ -25,6 +25,7 @@
 #include <cmath>
 #include <cstring>
 #include <numeric>
+#include <vector>
 
 #include "solver.cuh"
 
@@ -90,7 +91,213 @@ struct BatchView {
     uint32_t* work;           // work-queue head, zero at launch
     double rtol, abstol, dtol;
     int32_t maxit, norm_type;
+    // two-level variant: ns slabs per instance along its long axis, 6 rigid-body modes each
+    int32_t ns;
+    const double* slab_geo;   // [n_inst][4]: long axis, lo, hi, length scale of the offsets
+    const double* slab_cent;  // [n_inst][kMaxSlabs][3] slab centroids (reference coordinates)
+    const double* coords;     // [n_node][3] reference coordinates
+    const uint8_t* fixed;     // [3 n_node] prescribed DOFs (zero rows of Z)
 };
+
+constexpr int kMaxSlabs = 8;
+constexpr int kMaxCoarse = 6 * kMaxSlabs;
+constexpr int kMaxWarps = 16;
+
+// Shared workspace of the two-level variant (dynamic shared memory, per CTA).
+struct CoarseSmem {
+    double Epart[kMaxCoarse * kMaxCoarse];  // this CTA's rows' share of E = Z^T A Z
+    double E[kMaxCoarse * kMaxCoarse];      // E, then E^{-1} (Gauss-Jordan in place)
+    double wacc[kMaxWarps][kMaxCoarse];     // per-warp partials of Z^T r
+    double vec[2][kMaxCoarse + 1];          // cluster-reduction slots (w and r.r)
+    double w[kMaxCoarse + 1];               // reduced Z^T r (and r.r)
+    double c[kMaxCoarse];                   // E^{-1} Z^T r
+    double col[kMaxCoarse];
+    int drop[kMaxCoarse];
+};
+
+__device__ __forceinline__ int slab_of(const BatchView& v, int inst, int64_t n) {
+    const double* g = v.slab_geo + 4 * inst;
+    const int ax = (int)g[0];
+    const double t = (v.coords[3 * n + ax] - g[1]) / (g[2] - g[1]);
+    int s = (int)floor(t * v.ns);
+    return s < 0 ? 0 : (s >= v.ns ? v.ns - 1 : s);
+}
+
+// Z_n (3 x 6): translations and rotations about the slab centroid, zero rows on prescribed DOFs
+__device__ __forceinline__ void slab_modes(const BatchView& v, int inst, int64_t n, int s, double Z[3][6]) {
+    const double* cen = v.slab_cent + 3 * ((int64_t)inst * kMaxSlabs + s);
+    const double h = v.slab_geo[4 * inst + 3];
+    const double dx = (v.coords[3 * n] - cen[0]) / h, dy = (v.coords[3 * n + 1] - cen[1]) / h,
+                 dz = (v.coords[3 * n + 2] - cen[2]) / h;
+    const double m[3][6] = {{1, 0, 0, -dy, 0, dz}, {0, 1, 0, dx, -dz, 0}, {0, 0, 1, 0, dy, -dx}};
+    for (int i = 0; i < 3; ++i) {
+        const bool fx = v.fixed[3 * n + i] != 0;
+        for (int j = 0; j < 6; ++j) Z[i][j] = fx ? 0.0 : m[i][j];
+    }
+}
+
+// Sum of the per-CTA vectors vec[par][0..len) over the cluster in rank order into w[0..len),
+// identical in every CTA.
+__device__ __forceinline__ void cluster_sum_vec(cg::cluster_group& cl, CoarseSmem& cs, int len, int& par) {
+    cl.sync();
+    const unsigned nb = cl.num_blocks();
+    for (int t = threadIdx.x; t < len; t += blockDim.x) {
+        double acc = 0.0;
+        for (unsigned c = 0; c < nb; ++c) acc += cl.map_shared_rank(&cs.vec[par][0], c)[t];
+        cs.w[t] = acc;
+    }
+    par ^= 1;
+    __syncthreads();
+}
+
+// This CTA's rows' Z^T r (per-warp shared accumulators, then fixed warp order) and r.r into
+// vec[par]; then the cluster sum into w.
+__device__ __forceinline__ void coarse_restrict(cg::cluster_group& cl, CoarseSmem& cs, const BatchView& v, int inst,
+                                                int64_t a0, int64_t a1, double rr, double* sh, int& par) {
+    const int K = 6 * v.ns, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int t = threadIdx.x; t < kMaxWarps * kMaxCoarse; t += blockDim.x) (&cs.wacc[0][0])[t] = 0.0;
+    __syncthreads();
+    for (int64_t n = a0 + threadIdx.x; n < a1; n += blockDim.x) {
+        const int s = slab_of(v, inst, n);
+        double Z[3][6];
+        slab_modes(v, inst, n, s, Z);
+        const double r0 = v.r[3 * n], r1 = v.r[3 * n + 1], r2 = v.r[3 * n + 2];
+        for (int j = 0; j < 6; ++j) {
+            const double t = Z[0][j] * r0 + Z[1][j] * r1 + Z[2][j] * r2;
+            if (t != 0.0) atomicAdd(&cs.wacc[warp][6 * s + j], t);
+        }
+    }
+    rr = bsum(rr, sh);
+    __syncthreads();
+    for (int t = threadIdx.x; t < K; t += blockDim.x) {
+        double acc = 0.0;
+        for (int w = 0; w < nw; ++w) acc += cs.wacc[w][t];
+        cs.vec[par][t] = acc;
+    }
+    if (threadIdx.x == 0) cs.vec[par][K] = rr;
+    cluster_sum_vec(cl, cs, K + 1, par);
+}
+
+// c = E^{-1} w (every CTA, from its own copy of E^{-1}); 8 threads per row. The loop runs over
+// whole warps (8 K rounded up to 32, blockDim a multiple of 32) so every lane of a warp takes
+// part in the shuffles; lanes past the last row add zeros.
+__device__ __forceinline__ void coarse_solve(CoarseSmem& cs, int K) {
+    const int T8 = (8 * K + 31) & ~31;
+    for (int t = threadIdx.x; t < T8; t += blockDim.x) {
+        const int row = t >> 3, part = t & 7;
+        double acc = 0.0;
+        if (row < K)
+            for (int j = part; j < K; j += 8) acc += cs.E[row * kMaxCoarse + j] * cs.w[j];
+        acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+        acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+        acc += __shfl_xor_sync(0xffffffffu, acc, 4);
+        if (part == 0 && row < K) cs.c[row] = acc;
+    }
+    __syncthreads();
+}
+
+// E = Z^T A Z of the instance (this CTA's rows, then the cluster sum), its inverse in place
+template <typename VT>
+__device__ void coarse_setup(cg::cluster_group& cl, CoarseSmem& cs, const SellView& A, const VT* __restrict__ val,
+                             const BatchView& v, int inst, int64_t a0, int64_t a1) {
+    const int K = 6 * v.ns;
+    for (int t = threadIdx.x; t < kMaxCoarse * kMaxCoarse; t += blockDim.x) cs.Epart[t] = 0.0;
+    __syncthreads();
+    for (int64_t n = a0 + threadIdx.x; n < a1; n += blockDim.x) {
+        const int sn = slab_of(v, inst, n);
+        double Zn[3][6];
+        slab_modes(v, inst, n, sn, Zn);
+        const int64_t sl = n >> 5;
+        const int lane = (int)(n & 31);
+        const int64_t base = A.slice_base[sl];
+        const int w = A.slice_width[sl];
+        double T[3][6] = {{0}};
+        int cur = -1;
+        auto flush = [&](int sm) {
+            for (int i = 0; i < 6; ++i)
+                for (int j = 0; j < 6; ++j) {
+                    const double e = Zn[0][i] * T[0][j] + Zn[1][i] * T[1][j] + Zn[2][i] * T[2][j];
+                    if (e != 0.0) atomicAdd(&cs.Epart[(6 * sn + i) * kMaxCoarse + 6 * sm + j], e);
+                }
+            for (int r = 0; r < 3; ++r)
+                for (int j = 0; j < 6; ++j) T[r][j] = 0.0;
+        };
+        for (int k = 0; k <= w; ++k) {
+            double blk[9];
+            int64_t m;
+            if (k < w) {
+                m = A.col[base + 32 * (int64_t)k + lane];
+                const VT* p = val + 9 * (base + 32 * (int64_t)k) + lane;
+                bool any = false;
+                for (int q = 0; q < 9; ++q) {
+                    blk[q] = (double)p[32 * q];
+                    any |= blk[q] != 0.0;
+                }
+                if (!any) continue;
+            } else {
+                if (!A.diag64) break;  // the FP32 storage keeps the diagonal blocks apart
+                m = n;
+                for (int q = 0; q < 9; ++q) blk[q] = A.diag64[9 * n + q];
+            }
+            if (A.fixed)
+                for (int q = 0; q < 9; ++q)
+                    if (A.fixed[3 * n + q / 3] || A.fixed[3 * m + q % 3]) blk[q] = 0.0;
+            const int sm = slab_of(v, inst, m);
+            if (sm != cur) {
+                if (cur >= 0) flush(cur);
+                cur = sm;
+            }
+            double Zm[3][6];
+            slab_modes(v, inst, m, sm, Zm);
+            for (int r = 0; r < 3; ++r)
+                for (int j = 0; j < 6; ++j)
+                    T[r][j] += blk[3 * r] * Zm[0][j] + blk[3 * r + 1] * Zm[1][j] + blk[3 * r + 2] * Zm[2][j];
+        }
+        if (cur >= 0) flush(cur);
+    }
+    cl.sync();
+    const unsigned nb = cl.num_blocks();
+    for (int t = threadIdx.x; t < K * K; t += blockDim.x) {
+        const int i = t / K, j = t % K;
+        double acc = 0.0;
+        for (unsigned c = 0; c < nb; ++c) acc += cl.map_shared_rank(cs.Epart, c)[i * kMaxCoarse + j];
+        cs.E[i * kMaxCoarse + j] = acc;
+    }
+    __syncthreads();
+    // modes without free DOFs (a slab of prescribed nodes) become identity rows, dropped below
+    if (threadIdx.x == 0) {
+        double mx = 0.0;
+        for (int i = 0; i < K; ++i) mx = fmax(mx, fabs(cs.E[i * kMaxCoarse + i]));
+        for (int i = 0; i < K; ++i) cs.drop[i] = !(cs.E[i * kMaxCoarse + i] > 1e-13 * mx);
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < K * K; t += blockDim.x) {
+        const int i = t / K, j = t % K;
+        if (cs.drop[i] || cs.drop[j]) cs.E[i * kMaxCoarse + j] = i == j ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    // Gauss-Jordan inversion without pivoting (E is symmetric positive definite)
+    for (int k = 0; k < K; ++k) {
+        for (int i = threadIdx.x; i < K; i += blockDim.x) cs.col[i] = cs.E[i * kMaxCoarse + k];
+        __syncthreads();
+        const double piv = 1.0 / cs.col[k];
+        for (int j = threadIdx.x; j < K; j += blockDim.x)
+            cs.E[k * kMaxCoarse + j] = (j == k ? 1.0 : cs.E[k * kMaxCoarse + j]) * piv;
+        __syncthreads();
+        for (int t = threadIdx.x; t < K * K; t += blockDim.x) {
+            const int i = t / K, j = t % K;
+            if (i == k) continue;
+            const double e = j == k ? 0.0 : cs.E[i * kMaxCoarse + j];
+            cs.E[i * kMaxCoarse + j] = e - cs.col[i] * cs.E[k * kMaxCoarse + j];
+        }
+        __syncthreads();
+    }
+    for (int t = threadIdx.x; t < K * K; t += blockDim.x) {
+        const int i = t / K, j = t % K;
+        if (cs.drop[i] || cs.drop[j]) cs.E[i * kMaxCoarse + j] = 0.0;
+    }
+    __syncthreads();
+}
 
 // y = (A p)_row, FP64 accumulation; p is read through L2 (written by other CTAs of the cluster)
 template <typename VT>
@@ -126,14 +333,19 @@ __device__ __forceinline__ void row_apply(const SellView& A, const VT* __restric
     }
 }
 
-template <typename VT>
+// COARSE: the two-level preconditioner z = D^{-1} r + Z E^{-1} Z^T r on the instance's slabs (one
+// more cluster reduction per iteration: Z^T r together with r.r).
+template <typename VT, bool COARSE>
 __global__ void __launch_bounds__(512) batch_pcg_kernel(SellView A, const VT* __restrict__ val, BatchView v) {
     cg::cluster_group cl = cg::this_cluster();
     const int rank = (int)cl.block_rank(), nb = (int)cl.num_blocks();
     __shared__ int job[2];
     __shared__ double slot[2][2];
     __shared__ double sh[32];
-    int jpar = 0, rpar = 0;
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    CoarseSmem& cs = *reinterpret_cast<CoarseSmem*>(dyn_smem);  // COARSE only
+    const int K = COARSE ? 6 * v.ns : 0;
+    int jpar = 0, rpar = 0, vpar = 0;
     for (;;) {
         if (rank == 0 && threadIdx.x == 0) job[jpar] = (int)atomicAdd(v.work, 1u);
         cl.sync();
@@ -156,8 +368,9 @@ __global__ void __launch_bounds__(512) batch_pcg_kernel(SellView A, const VT* __
             }
             continue;
         }
-        // x = 0, r = b, z = D^-1 r, p = z (PCJACOBI: a zero diagonal entry gives 1)
-        double rz = 0.0, nn = 0.0;
+        if constexpr (COARSE) coarse_setup<VT>(cl, cs, A, val, v, inst, a0, a1);
+        // x = 0, r = b, z = D^-1 r (+ Z E^-1 Z^T r), p = z (PCJACOBI: a zero diagonal entry gives 1)
+        double rz = 0.0, nn = 0.0, rr0 = 0.0;
         for (int64_t n = a0 + threadIdx.x; n < a1; n += blockDim.x) {
             const uint32_t o = A.dvoff[n];
 #pragma unroll
@@ -170,13 +383,39 @@ __global__ void __launch_bounds__(512) batch_pcg_kernel(SellView A, const VT* __
                 v.dinv[3 * n + c] = di;
                 v.x[3 * n + c] = 0.0;
                 v.r[3 * n + c] = bi;
-                v.z[3 * n + c] = zi;
-                v.p[3 * n + c] = zi;
-                rz += bi * zi;
-                nn += v.norm_type ? bi * bi : zi * zi;
+                rr0 += bi * bi;
+                if constexpr (!COARSE) {
+                    v.z[3 * n + c] = zi;
+                    v.p[3 * n + c] = zi;
+                    rz += bi * zi;
+                    nn += v.norm_type ? bi * bi : zi * zi;
+                }
+            }
+        }
+        if constexpr (COARSE) {
+            coarse_restrict(cl, cs, v, inst, a0, a1, rr0, sh, vpar);
+            coarse_solve(cs, K);
+            for (int64_t n = a0 + threadIdx.x; n < a1; n += blockDim.x) {
+                const int sl = slab_of(v, inst, n);
+                double Z[3][6];
+                slab_modes(v, inst, n, sl, Z);
+                const double* cc = cs.c + 6 * sl;
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    double zc = 0.0;
+                    for (int j = 0; j < 6; ++j) zc += Z[c][j] * cc[j];
+                    const double ri = v.r[3 * n + c], zi = v.dinv[3 * n + c] * ri + zc;
+                    v.z[3 * n + c] = zi;
+                    v.p[3 * n + c] = zi;
+                    rz += ri * zi;
+                    nn += zi * zi;
+                }
             }
         }
         cluster_sum2(cl, rz, nn, slot, rpar, sh);  // also publishes p to the cluster
+        if constexpr (COARSE) {
+            if (v.norm_type) nn = cs.w[K];
+        }
         double dp = sqrt(nn);
         const double dp0 = dp, ttol = fmax(v.rtol * dp, v.abstol);
         int its = 0, status = MPHY_OK;
@@ -211,16 +450,45 @@ __global__ void __launch_bounds__(512) batch_pcg_kernel(SellView A, const VT* __
             }
             const double alpha = rz / pq;
             double rz1 = 0.0, nn1 = 0.0;
-            for (int64_t i = d0 + threadIdx.x; i < d1; i += blockDim.x) {
-                const double ri = v.r[i] - alpha * v.q[i];
-                const double zi = v.dinv[i] * ri;
-                v.x[i] += alpha * v.p[i];
-                v.r[i] = ri;
-                v.z[i] = zi;
-                rz1 += ri * zi;
-                nn1 += v.norm_type ? ri * ri : zi * zi;
+            if constexpr (!COARSE) {
+                for (int64_t i = d0 + threadIdx.x; i < d1; i += blockDim.x) {
+                    const double ri = v.r[i] - alpha * v.q[i];
+                    const double zi = v.dinv[i] * ri;
+                    v.x[i] += alpha * v.p[i];
+                    v.r[i] = ri;
+                    v.z[i] = zi;
+                    rz1 += ri * zi;
+                    nn1 += v.norm_type ? ri * ri : zi * zi;
+                }
+                cluster_sum2(cl, rz1, nn1, slot, rpar, sh);
+            } else {
+                double rr1 = 0.0;
+                for (int64_t i = d0 + threadIdx.x; i < d1; i += blockDim.x) {
+                    const double ri = v.r[i] - alpha * v.q[i];
+                    v.x[i] += alpha * v.p[i];
+                    v.r[i] = ri;
+                    rr1 += ri * ri;
+                }
+                coarse_restrict(cl, cs, v, inst, a0, a1, rr1, sh, vpar);
+                coarse_solve(cs, K);
+                for (int64_t n = a0 + threadIdx.x; n < a1; n += blockDim.x) {
+                    const int sl = slab_of(v, inst, n);
+                    double Z[3][6];
+                    slab_modes(v, inst, n, sl, Z);
+                    const double* cc = cs.c + 6 * sl;
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        double zc = 0.0;
+                        for (int j = 0; j < 6; ++j) zc += Z[c][j] * cc[j];
+                        const double ri = v.r[3 * n + c], zi = v.dinv[3 * n + c] * ri + zc;
+                        v.z[3 * n + c] = zi;
+                        rz1 += ri * zi;
+                        nn1 += zi * zi;
+                    }
+                }
+                cluster_sum2(cl, rz1, nn1, slot, rpar, sh);
+                if (v.norm_type) nn1 = cs.w[K];
             }
-            cluster_sum2(cl, rz1, nn1, slot, rpar, sh);
             its += 1;
             dp = sqrt(nn1);
             if (dp != dp) {
@@ -393,8 +661,10 @@ struct mphy_batch {
     DevBuf<int32_t> elem_ptr;
     int32_t rec_steps = 0;
     int32_t cluster = 1, threads = 256;
+    int32_t ns = 0;                          // slabs per instance of the two-level variant (0: off)
+    DevBuf<double> slab_geo, slab_cent;
     cudaGraphExec_t graph = nullptr;
-    int graph_cluster = 0, graph_threads = 0;
+    int graph_cluster = 0, graph_threads = 0, graph_ns = 0;
     double graph_key[6] = {0, 0, 0, 0, 0, 0};
     int64_t launches = 0;
     uint32_t* pinned = nullptr;  // [0] instances still running, [1] instances solved in the last iteration
@@ -429,11 +699,23 @@ BatchView batch_view(mphy_batch* b, const uint8_t* active, bool totals, int maxi
     v.dtol = s->opts.dtol;
     v.maxit = maxit;
     v.norm_type = s->opts.norm_type;
+    v.ns = b->ns;
+    v.slab_geo = b->slab_geo.p;
+    v.slab_cent = b->slab_cent.p;
+    v.coords = s->mesh->coords.p;
+    v.fixed = s->mesh->fixed.p;
     return v;
 }
 
-template <typename VT>
+template <typename VT, bool COARSE>
 void launch_pcg(mphy_batch* b, const VT* val, const BatchView& v, cudaStream_t st, int cluster, int threads) {
+    const size_t dyn = COARSE ? sizeof(CoarseSmem) : 0;
+    static bool smem_set = false;
+    if (COARSE && !smem_set) {
+        MPHY_CUDA(cudaFuncSetAttribute(batch_pcg_kernel<VT, COARSE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)dyn));
+        smem_set = true;
+    }
     cudaLaunchConfig_t cfg{};
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -441,25 +723,30 @@ void launch_pcg(mphy_batch* b, const VT* val, const BatchView& v, cudaStream_t s
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
     cfg.blockDim = dim3(threads);
-    cfg.dynamicSmemBytes = 0;
+    cfg.dynamicSmemBytes = dyn;
     cfg.stream = st;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     cfg.gridDim = dim3(cluster);
     int max_clusters = 0;
-    MPHY_CUDA(cudaOccupancyMaxActiveClusters(&max_clusters, batch_pcg_kernel<VT>, &cfg));
+    MPHY_CUDA(cudaOccupancyMaxActiveClusters(&max_clusters, batch_pcg_kernel<VT, COARSE>, &cfg));
     MPHY_REQUIRE(max_clusters > 0, MPHY_ERR_UNSUPPORTED, "batched solve: this cluster shape cannot be resident");
     const int n_clusters = std::min(max_clusters, b->n_inst);
     cfg.gridDim = dim3((unsigned)(n_clusters * cluster));
     MPHY_CUDA(cudaMemsetAsync(b->work.p, 0, sizeof(uint32_t), st));
-    MPHY_CUDA(cudaLaunchKernelEx(&cfg, batch_pcg_kernel<VT>, b->s->A, val, v));
+    MPHY_CUDA(cudaLaunchKernelEx(&cfg, batch_pcg_kernel<VT, COARSE>, b->s->A, val, v));
     b->launches += 1;
 }
 
 void run_pcg(mphy_batch* b, const uint8_t* active, bool totals, int maxit, cudaStream_t st, int cluster, int threads) {
     const BatchView v = batch_view(b, active, totals, maxit);
-    if (b->s->mixed) launch_pcg<float>(b, b->s->valf.p, v, st, cluster, threads);
-    else launch_pcg<double>(b, b->s->val.p, v, st, cluster, threads);
+    if (b->s->mixed) {
+        if (b->ns > 0) launch_pcg<float, true>(b, b->s->valf.p, v, st, cluster, threads);
+        else launch_pcg<float, false>(b, b->s->valf.p, v, st, cluster, threads);
+    } else {
+        if (b->ns > 0) launch_pcg<double, true>(b, b->s->val.p, v, st, cluster, threads);
+        else launch_pcg<double, false>(b, b->s->val.p, v, st, cluster, threads);
+    }
 }
 
 bool schedule_ok(int cluster, int threads) {
@@ -585,6 +872,61 @@ int mphy_batch_set_schedule(mphy_batch* b, int32_t cluster, int32_t threads) {
     b->cluster = cluster;
     b->threads = threads;
     return MPHY_OK;
+}
+
+int mphy_batch_set_coarse(mphy_batch* b, int32_t slabs) {
+    return guarded([&] {
+        MPHY_REQUIRE(b, MPHY_ERR_INVALID_ARG, "null argument");
+        MPHY_REQUIRE(slabs >= 0 && slabs <= kMaxSlabs, MPHY_ERR_INVALID_ARG,
+                     "batched coarse space: 0 (off) to 8 slabs per instance");
+        if (slabs == 0) {
+            b->ns = 0;
+            return (int)MPHY_OK;
+        }
+        const mphy_mesh* m = b->s->mesh;
+        const std::vector<double>& X = m->coords_host;
+        const size_t ni = (size_t)b->n_inst;
+        std::vector<double> geo(4 * ni), cen(3 * ni * kMaxSlabs, 0.0);
+        for (size_t i = 0; i < ni; ++i) {
+            const int32_t n0 = b->node_ptr_host[i], n1 = b->node_ptr_host[i + 1];
+            double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+            for (int32_t n = n0; n < n1; ++n)
+                for (int d = 0; d < 3; ++d) {
+                    lo[d] = std::min(lo[d], X[3 * (size_t)n + d]);
+                    hi[d] = std::max(hi[d], X[3 * (size_t)n + d]);
+                }
+            int ax = 0;
+            for (int d = 1; d < 3; ++d)
+                if (hi[d] - lo[d] > hi[ax] - lo[ax]) ax = d;
+            const double len = std::max(hi[ax] - lo[ax], 1e-300);
+            // offsets scaled by a slab's diagonal: the rotation modes are O(1) like the translations
+            double diag = 0.0;
+            for (int d = 0; d < 3; ++d) diag += std::pow(d == ax ? len / slabs : hi[d] - lo[d], 2);
+            geo[4 * i] = ax;
+            geo[4 * i + 1] = lo[ax];
+            geo[4 * i + 2] = lo[ax] + len;
+            geo[4 * i + 3] = std::sqrt(std::max(diag, 1e-300));
+            std::vector<double> cnt(slabs, 0.0);
+            for (int32_t n = n0; n < n1; ++n) {
+                int sl = (int)std::floor((X[3 * (size_t)n + ax] - lo[ax]) / len * slabs);
+                sl = sl < 0 ? 0 : (sl >= slabs ? slabs - 1 : sl);
+                cnt[sl] += 1.0;
+                for (int d = 0; d < 3; ++d) cen[3 * (i * kMaxSlabs + sl) + d] += X[3 * (size_t)n + d];
+            }
+            for (int sl = 0; sl < slabs; ++sl)
+                for (int d = 0; d < 3; ++d)
+                    if (cnt[sl] > 0.0) cen[3 * (i * kMaxSlabs + sl) + d] /= cnt[sl];
+        }
+        MPHY_CUDA(cudaSetDevice(b->s->device));
+        cudaStream_t st = b->s->ctx->stream;
+        b->slab_geo.alloc(geo.size());
+        b->slab_geo.upload(geo.data(), geo.size(), st);
+        b->slab_cent.alloc(cen.size());
+        b->slab_cent.upload(cen.data(), cen.size(), st);
+        MPHY_CUDA(cudaStreamSynchronize(st));
+        b->ns = slabs;
+        return (int)MPHY_OK;
+    });
 }
 
 int mphy_batch_get_schedule(const mphy_batch* b, int32_t* cluster, int32_t* threads) {
@@ -737,7 +1079,7 @@ int mphy_batch_newton_run(mphy_batch* b, const double* fext_host, const mphy_new
         nv.max_newton = o->max_newton;
         const double key[6] = {o->dt, o->t_final, o->tol_rel, o->tol_abs, (double)o->max_steps, (double)o->max_newton};
         // the graph of one batch Newton iteration (rebuilt when the schedule or the options change)
-        if (b->graph && (b->graph_cluster != b->cluster || b->graph_threads != b->threads ||
+        if (b->graph && (b->graph_cluster != b->cluster || b->graph_threads != b->threads || b->graph_ns != b->ns ||
                          std::memcmp(b->graph_key, key, sizeof(key)) != 0)) {
             MPHY_CUDA(cudaGraphExecDestroy(b->graph));
             b->graph = nullptr;
@@ -759,6 +1101,7 @@ int mphy_batch_newton_run(mphy_batch* b, const double* fext_host, const mphy_new
             MPHY_CUDA(e);
             b->graph_cluster = b->cluster;
             b->graph_threads = b->threads;
+            b->graph_ns = b->ns;
             std::memcpy(b->graph_key, key, sizeof(key));
         }
         // prescribed diagonal (FP64) or diagonal rebuild (mixed), element, step control, solve, update
