@@ -313,6 +313,20 @@ class FemSolidmechanicsGpu:
         opts.update(solver_opts)
         self.solver = SolverGpu(self.mesh, self.pattern, **opts)
 
+    @classmethod
+    def from_reference_inputs(cls, config_path, ctx: Context | None = None, **solver_opts):
+        """The reference's inputs (a config file and the Gmsh 2.2 mesh it names, see
+        reference_io); solve_reference() then applies its Solver block."""
+        from . import reference_io
+        return cls(reference_io.read_config(config_path), ctx, **solver_opts)
+
+    def solve_reference(self) -> "NewtonResult":
+        """solveWithNewtonRaphson with the config's absolute `tolerance` and `maximumIterations`
+        (femSolidmechanics1.cpp:616-622: converged when ||R|| < tolerance)."""
+        m = self.prob.meta
+        return self.solveWithNewtonRaphson(max_newton=int(m["maximumIterations"]), tol_rel=0.0,
+                                           tol_abs=float(m["tolerance"]))
+
     def solveWithNewtonRaphson(self, max_newton: int = 10, tol_rel: float | None = None, tol_abs: float = 0.0,  # noqa: N802
                                disp: np.ndarray | None = None, max_hist: int = 4096) -> NewtonResult:
         p = self.prob

@@ -1,0 +1,147 @@
+"""The reference's input formats (Gmsh 2.2 + config): round trips of the generated workloads,
+traction quadrature against closed forms, and the config reader's rules and limits."""
+import numpy as np
+import pytest
+
+from mphyfem_b200 import meshgen
+from mphyfem_b200 import reference_io as rio
+
+
+def _write(tmp_path, prob, patches, fixed=("clamp",), **kw):
+    rio.write_gmsh22(tmp_path / "m.msh", prob, patches)
+    rio.write_config(tmp_path / "config", "m.msh", prob, fixed_patches=fixed, **kw)
+    return rio.read_config(tmp_path / "config")
+
+
+@pytest.mark.parametrize("make", [lambda: meshgen.hex8_cantilever(8, 2, 3),
+                                  lambda: meshgen.two_phase_inclusions(16, 4, 4, seed=3, r_range=(0.2, 0.3)),
+                                  lambda: meshgen.tet10_kuhn(4, 2, 2)], ids=["hex8", "two_phase", "tet10"])
+def test_round_trip(tmp_path, make):
+    p = make()
+    clamp = rio.boundary_faces(p, lambda X: np.isclose(X[:, 0], 0.0))
+    q = _write(tmp_path, p, {"clamp": clamp})
+    assert np.array_equal(q.coords, p.coords) and np.array_equal(q.conn, p.conn)
+    assert np.array_equal(q.fixed, p.fixed)
+    assert np.array_equal(q.fnodal, p.fnodal)
+    # materials are renumbered by first use; the per-element rows must agree
+    assert np.array_equal(q.mats[q.mat_id], p.mats[p.mat_id])
+    assert (q.dt, q.t_final, q.max_steps) == (p.dt, p.t_final, p.max_steps)
+
+
+def test_quad4_traction_closed_form():
+    p = meshgen.hex8_cantilever(2, 2, 2, lx=2.0, ly=1.0, lz=3.0)
+    face = rio.boundary_faces(p, lambda X: np.isclose(X[:, 0], 2.0))
+    F = rio.traction_forces(p.coords, face, [0.7, 0.0, 9.0]).sum(axis=0)
+    # normal = (dv x du)/|.| with the faces in the element's outward corner order (counter-
+    # clockwise seen from outside): dv x du points into the body, here -x; s2 is not used
+    assert np.allclose(F, [-0.7 * 3.0, 0.0, 0.0], rtol=1e-13, atol=1e-13)
+    # tangential part: s1 du with du = dx/dxi1 not normalised (half the face edge per face)
+    for fc in face:
+        X = p.coords[fc]
+        du = (X[1] - X[0]) / 2.0
+        Ff = rio.traction_forces(p.coords, [fc], [0.0, 2.0, 0.0]).sum(axis=0)
+        area = np.linalg.norm(np.cross(X[1] - X[0], X[3] - X[0]))
+        assert np.allclose(Ff, 2.0 * du * area, rtol=1e-13)
+
+
+def test_traction_matches_consistent_nodal_forces():
+    """The cantilever's load, t = (0, 0, -0.05) on x = 4, given as a Tractions block with the
+    faces ordered so that dx/dxi1 runs along z: identical nodal forces."""
+    p = meshgen.hex8_cantilever(4, 2, 2)
+    faces = [[fc[0], fc[3], fc[2], fc[1]] for fc in rio.boundary_faces(p, lambda X: np.isclose(X[:, 0], 4.0))]
+    hz = 1.0 / 2
+    F = rio.traction_forces(p.coords, faces, [0.0, -0.05 / (hz / 2.0), 0.0])
+    assert np.allclose(F.ravel(), p.fnodal, rtol=1e-13, atol=1e-16)
+
+
+def test_tri6_face_area_and_normal():
+    X = np.array([[0, 0, 0], [2, 0, 0], [0, 3, 0], [1, 0, 0], [1, 1.5, 0], [0, 1.5, 0]], dtype=float)
+    F = rio.traction_forces(X, [[0, 1, 2, 3, 4, 5]], [1.0, 0.0, 0.0])
+    assert np.allclose(F.sum(axis=0), [0, 0, -3.0], rtol=1e-13)   # area 3, normal dv x du = -z
+    assert np.allclose(F[:3].sum(axis=0), 0.0, atol=1e-13)         # vertex shares vanish for tri6
+
+
+CONFIG = """
+Files
+{
+  mesh : m.msh
+}
+
+Domains
+{
+  phase0
+  {
+    Material   : 2
+    Element    : 1
+  }
+}
+
+! a comment line
+Material
+{
+  id : 2
+  name : Matl_NeoHookean
+  density : 1.0
+  data_deviatoric :  3.5
+  data_volumetric :  3  0.02
+}
+
+Boundary Conditions
+{
+    clamp
+    {
+        type   :  specified
+        dof    :  X
+        value  :  0.0
+    }
+}
+
+Nodal Forces
+{
+  timefunction 1
+  count 1
+  9 3 -1.5
+}
+
+Time Functions
+{
+   1   0.0   1000.0  0.0  2.0    0.0   0.0   0.0   0.0   0.0   0.0
+}
+
+Solver
+{
+finalTime          1.0
+timeStep           0.25
+maximumSteps       4
+maximumIterations  12
+tolerance          1.0e-9
+}
+"""
+
+
+def test_config_reader_rules(tmp_path):
+    p = meshgen.hex8_cantilever(2, 1, 1)
+    clamp = rio.boundary_faces(p, lambda X: np.isclose(X[:, 0], 0.0))
+    rio.write_gmsh22(tmp_path / "m.msh", p, {"clamp": clamp})
+    (tmp_path / "config").write_text(CONFIG)
+    q = rio.read_config(tmp_path / "config")
+    assert np.allclose(q.mats, [[3.5, 0.02, 3.0]])
+    fx = q.fixed.reshape(-1, 3)
+    clamped = np.isclose(p.coords[:, 0], 0.0)
+    assert (fx[clamped, 0] == 1).all() and (fx[:, 1:] == 0).all() and (fx[~clamped] == 0).all()
+    F = q.fnodal.reshape(-1, 3)
+    assert F[8, 2] == -3.0 and np.count_nonzero(F) == 1          # lam = 2 t: the slope scales the load
+    assert (q.dt, q.t_final, q.max_steps) == (0.25, 1.0, 4)
+    assert q.meta["tolerance"] == 1e-9 and q.meta["maximumIterations"] == 12
+    (tmp_path / "config").write_text(CONFIG.replace("0.0  2.0    0.0   0.0", "1.0  0.0    0.0   0.0"))
+    with pytest.raises(NotImplementedError):
+        rio.read_config(tmp_path / "config")                     # constant load: not lam = c t
+    (tmp_path / "config").write_text(CONFIG.replace("value  :  0.0", "value  :  0.1"))
+    with pytest.raises(NotImplementedError):
+        rio.read_config(tmp_path / "config")                     # nonzero prescribed value
+    (tmp_path / "config").write_text(CONFIG.replace("Matl_NeoHookean", "Matl_LinearElastic"))
+    with pytest.raises(NotImplementedError):
+        rio.read_config(tmp_path / "config")
+    (tmp_path / "config").write_text(CONFIG.replace("Solver", "Solvr"))
+    with pytest.raises(ValueError):
+        rio.read_config(tmp_path / "config")                     # unknown block key
