@@ -138,6 +138,38 @@ int mphy_mesh_create(mphy_ctx* ctx, int32_t n_node, const double* coords_host, i
                      mphy_mesh** out);
 int mphy_mesh_destroy(mphy_mesh* mesh);
 
+/* ---- hyperelastic models (the compressible branch of utilitiesmaterialHyperelastic.cpp) and
+ * their deviatoric parameters, as the reference's material blocks give them:
+ *   MPHY_MAT_NEOHOOKEAN   Matl_NeoHookean    data_deviatoric : mu          (:186-295)
+ *   MPHY_MAT_MOONEYRIVLIN Matl_MooneyRivlin  data_deviatoric : c1 c2       (:300-420)
+ *   MPHY_MAT_GENT         Matl_Gent          data_deviatoric : mu Im       (:423-548)
+ *   MPHY_MAT_ARRUDABOYCE  Matl_ArrudaBoyce   data            : mu N        (:551-677)
+ * Each takes the volumetric energy Utype and Kinv = 1/K of data_volumetric.
+ * Tangent modes: MPHY_TANGENT_REFERENCE gives each model's tangent as the reference writes it.
+ * MPHY_TANGENT_CONSISTENT gives the exact derivative of the residual for Neo-Hookean, Gent and
+ * Arruda-Boyce (whose reference tangent is a symmetrised form). Mooney-Rivlin keeps the written
+ * tangent in both modes: the reference's stress carries J^{-5/3} where J^{-7/3} belongs (r7d3 =
+ * 5/3, :303), and its exact derivative is not symmetric. */
+enum { MPHY_MAT_NEOHOOKEAN = 0, MPHY_MAT_MOONEYRIVLIN = 1, MPHY_MAT_GENT = 2, MPHY_MAT_ARRUDABOYCE = 3 };
+enum { MPHY_MAT_NDATA = 4 };
+
+/* Sets the model and parameters of every material of the mesh (the Matl_* object that
+ * MaterialBase's factory makes per material id). model: [n_mat] MPHY_MAT_*; data: [n_mat][4],
+ * the model's parameters above, unused slots ignored. Kinv and Utype stay those of
+ * mphy_mesh_create. n_mat must equal the mesh's; Gent needs Im > 0 and Arruda-Boyce N > 0
+ * (MPHY_ERR_INVALID_ARG otherwise). Without this call every material is Neo-Hookean with mu =
+ * mats[3k]. A mesh with any model other than Neo-Hookean assembles with the dense-tangent
+ * element kernel (FP64; FP32 storage in the mixed precisions, MPHY_PREC_MIXED_TC included, whose
+ * tensor-core kernel is Neo-Hookean only), and mphy_elem_eval_tc returns MPHY_ERR_UNSUPPORTED for
+ * it. Host pointers, copied; affects assemblies issued after the call. */
+int mphy_mesh_set_materials(mphy_mesh* mesh, int32_t n_mat, const int32_t* model_host, const double* data_host);
+
+/* Batched stress and tangent of any model above at n deformation gradients (the material
+ * contract of MaterialBase::computeStressAndTangent). data_host: [4]. Device arrays as in
+ * mphy_material_nh_eval. */
+int mphy_material_eval(mphy_ctx* ctx, int32_t n, const double* F_dev, int32_t model, const double* data_host,
+                       double Kinv, int32_t utype, int32_t tangent, double* stre_dev, double* cmat_dev);
+
 /* ---- material contract: MaterialBase::computeStressAndTangent (MaterialBase.h:94), Neo-Hookean
  * (Matl_NeoHookean.cpp:45-53 -> utilitiesmaterialHyperelastic.cpp:186-295), batched.
  * F_dev: [n][9] row-major F(i,j); stre_dev: [n][9]; cmat_dev: [n][81] row-major. */

@@ -35,6 +35,8 @@ SOLVER_EMPTY, PATTERN_OK, INIT_OK, ASSEMBLY_OK, FACTORISE_OK = range(5)
 PREC_FP64, PREC_MIXED, PREC_MIXED_F32VEC, PREC_MIXED_TC = 0, 1, 2, 3
 PC_JACOBI, PC_FSAI, PC_FSAI_LEARNED = 0, 1, 2
 TANGENT_REFERENCE, TANGENT_CONSISTENT = 0, 1
+MAT_NEOHOOKEAN, MAT_MOONEYRIVLIN, MAT_GENT, MAT_ARRUDABOYCE = 0, 1, 2, 3
+MAT_NDATA = 4
 
 
 class SolverOpts(C.Structure):
@@ -85,6 +87,9 @@ SIGNATURES = {
                                    C.POINTER(_vp)]),
     "mphy_mesh_destroy": (C.c_int, [_vp]),
     "mphy_material_nh_eval": (C.c_int, [_vp, C.c_int32, _vp, C.c_double, C.c_double, C.c_int32, C.c_int32, _vp, _vp]),
+    "mphy_mesh_set_materials": (C.c_int, [_vp, C.c_int32, _i32, _d]),
+    "mphy_material_eval": (C.c_int, [_vp, C.c_int32, _vp, C.c_int32, _d, C.c_double, C.c_int32, C.c_int32, _vp,
+                                     _vp]),
     "mphy_elem_eval_tc": (C.c_int, [_vp, _vp, _vp, C.c_int32, _vp, _vp, _i64]),
     "mphy_elem_eval": (C.c_int, [_vp, _vp, _vp, C.c_int32, _vp, _vp, _i64]),
     "mphy_elem_eval_noalloc": (C.c_int, [_vp, C.c_int32, _vp, C.c_int32, C.c_int32, _vp, _vp, C.c_int32, _vp, _vp,

@@ -76,6 +76,18 @@ class Mesh:
                                           cn.ctypes.data_as(L._i32), mi.ctypes.data_as(L._i32), mt.shape[0],
                                           mt.ctypes.data_as(L._d), fx.ctypes.data_as(L._u8), C.byref(h)))
         self.h = h
+        if getattr(prob, "mat_model", None) is not None:
+            self.set_materials(prob.mat_model, prob.mat_data)
+
+    def set_materials(self, model, data):
+        """Per-material hyperelastic model (MAT_*) and parameters [n_mat, MAT_NDATA]
+        (mphy_mesh_set_materials); Kinv and Utype stay those of the mesh's material rows."""
+        mdl = _np(model, np.int32)
+        dat = np.zeros((mdl.shape[0], L.MAT_NDATA))
+        d = np.asarray(data, np.float64).reshape(mdl.shape[0], -1)
+        dat[:, :d.shape[1]] = d
+        L.check(self.lib.mphy_mesh_set_materials(self.h, mdl.shape[0], mdl.ctypes.data_as(L._i32),
+                                                 dat.ctypes.data_as(L._d)))
 
     def close(self):
         if getattr(self, "h", None):
@@ -276,6 +288,22 @@ def compute_stress_and_tangent(ctx: Context, F_dev, mu: float, Kinv: float, utyp
     s = torch.empty((n, 9), dtype=torch.float64, device=F.device)
     Cm = torch.empty((n, 9, 9), dtype=torch.float64, device=F.device)
     L.check(ctx.lib.mphy_material_nh_eval(ctx.h, n, _ptr(F), mu, Kinv, utype, tangent, _ptr(s), _ptr(Cm)))
+    return s, Cm
+
+
+def material_stress_and_tangent(ctx: Context, F_dev, model: int, data, Kinv: float, utype: int = 3,
+                                tangent: int = L.TANGENT_REFERENCE):
+    """Batched computeStressAndTangent of any hyperelastic model (MAT_*): F [n,3,3] -> stre [n,9],
+    Cmat [n,9,9]. data: the model's parameters (mu; c1 c2; mu Im; mu N)."""
+    torch = _torch()
+    n = F_dev.shape[0]
+    F = F_dev.contiguous().to(torch.float64)
+    d = np.zeros(L.MAT_NDATA)
+    d[:len(data)] = data
+    s = torch.empty((n, 9), dtype=torch.float64, device=F.device)
+    Cm = torch.empty((n, 9, 9), dtype=torch.float64, device=F.device)
+    L.check(ctx.lib.mphy_material_eval(ctx.h, n, _ptr(F), int(model), d.ctypes.data_as(L._d), Kinv, utype, tangent,
+                                       _ptr(s), _ptr(Cm)))
     return s, Cm
 
 

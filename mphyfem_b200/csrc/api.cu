@@ -16,6 +16,7 @@
 #include "elem.cuh"
 #include "fsai.cuh"
 #include "gnn.cuh"
+#include "mat.cuh"
 #include "krylov.cuh"
 #include "pattern.cuh"
 #include "solver.cuh"
@@ -56,6 +57,7 @@ ElemArgs elem_args(const mphy_mesh* m, const double* disp, int tangent, unsigned
     a.conn = m->conn.p;
     a.mat_id = m->mat_id.p;
     a.mats = m->mats.p;
+    a.matx = m->matx.p;
     a.disp = disp;
     a.tangent = tangent;
     a.bad = bad;
@@ -72,7 +74,8 @@ void solver_assemble(mphy_solver* s, const double* disp, uint8_t* bad_elem) {
     a.valf = s->mixed ? s->valf.p : nullptr;
     a.rhs = s->rhs.p;
     a.reac = s->reac.p;
-    if (s->opts.precision == MPHY_PREC_MIXED_TC) launch_elem_tc(a, s->mesh->npe, 2, s->ctx->stream);
+    if (s->mesh->general) launch_elem_gen(a, s->mesh->npe, 2, s->ctx->stream);
+    else if (s->opts.precision == MPHY_PREC_MIXED_TC) launch_elem_tc(a, s->mesh->npe, 2, s->ctx->stream);
     else launch_elem_fp64(a, s->mesh->npe, 2, s->ctx->stream);
     s->launches += 1;
     if (s->mixed) {
@@ -306,7 +309,10 @@ int elem_eval(mphy_ctx* c, const mphy_mesh* m, const double* disp, int32_t tange
         ElemArgs a = elem_args(m, disp, tangent, bad.p);
         a.Ke = Ke;
         a.Re = Re;
-        if (tc) launch_elem_tc(a, m->npe, 1, c->stream);
+        MPHY_REQUIRE(!(tc && m->general), MPHY_ERR_UNSUPPORTED,
+                     "the tensor-core element kernel supports Neo-Hookean materials only");
+        if (m->general) launch_elem_gen(a, m->npe, 1, c->stream);
+        else if (tc) launch_elem_tc(a, m->npe, 1, c->stream);
         else launch_elem_fp64(a, m->npe, 1, c->stream);
         unsigned long long h = 0;
         MPHY_CUDA(cudaMemcpyAsync(&h, bad.p, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
@@ -432,6 +438,16 @@ int mphy_mesh_create(mphy_ctx* c, int32_t n_node, const double* coords, int32_t 
                 for (int q = 0; q < 3; ++q) m4[4 * k + q] = mats[3 * k + q];
             m->mats.alloc(m4.size());
             m->mats.upload(m4.data(), m4.size(), s);
+            m->matx_host.assign(kMatRow * (size_t)n_mat, 0.0);
+            for (int32_t k = 0; k < n_mat; ++k) {
+                double* r = &m->matx_host[kMatRow * (size_t)k];
+                r[0] = MPHY_MAT_NEOHOOKEAN;
+                r[1] = mats[3 * k];
+                r[5] = mats[3 * k + 1];
+                r[6] = mats[3 * k + 2];
+            }
+            m->matx.alloc(m->matx_host.size());
+            m->matx.upload(m->matx_host.data(), m->matx_host.size(), s);
             m->fixed_host.assign(fixed, fixed + 3 * (size_t)n_node);
             m->coords_host.assign(coords, coords + 3 * (size_t)n_node);
             m->fixed.alloc(3 * (size_t)n_node);
@@ -453,6 +469,55 @@ int mphy_mesh_destroy(mphy_mesh* m) {
     cudaDeviceSynchronize();
     delete m;
     return MPHY_OK;
+}
+
+int mphy_mesh_set_materials(mphy_mesh* m, int32_t n_mat, const int32_t* model, const double* data) {
+    return guarded([&] {
+        MPHY_REQUIRE(m && model && data, MPHY_ERR_INVALID_ARG, "null argument");
+        MPHY_REQUIRE(n_mat == m->n_mat, MPHY_ERR_INVALID_ARG, "n_mat differs from the mesh's material count");
+        for (int32_t k = 0; k < n_mat; ++k) {
+            MPHY_REQUIRE(model[k] >= MPHY_MAT_NEOHOOKEAN && model[k] <= MPHY_MAT_ARRUDABOYCE, MPHY_ERR_INVALID_ARG,
+                         "unknown material model");
+            const double* d = data + MPHY_MAT_NDATA * (size_t)k;
+            MPHY_REQUIRE(model[k] != MPHY_MAT_GENT || d[1] > 0.0, MPHY_ERR_INVALID_ARG, "Gent needs Im > 0");
+            MPHY_REQUIRE(model[k] != MPHY_MAT_ARRUDABOYCE || d[1] > 0.0, MPHY_ERR_INVALID_ARG,
+                         "Arruda-Boyce needs N > 0");
+        }
+        MPHY_CUDA(cudaSetDevice(m->device));
+        std::vector<double> m4(4 * (size_t)n_mat);
+        MPHY_CUDA(cudaMemcpy(m4.data(), m->mats.p, m4.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        bool general = false;
+        for (int32_t k = 0; k < n_mat; ++k) {
+            double* r = &m->matx_host[kMatRow * (size_t)k];
+            r[0] = model[k];
+            for (int q = 0; q < MPHY_MAT_NDATA; ++q) r[1 + q] = data[MPHY_MAT_NDATA * (size_t)k + q];
+            m4[4 * (size_t)k] = data[MPHY_MAT_NDATA * (size_t)k];
+            general = general || model[k] != MPHY_MAT_NEOHOOKEAN;
+        }
+        // ordered after every assembly already issued on the mesh's stream
+        cudaStream_t s = m->ctx ? m->ctx->stream : nullptr;
+        m->matx.upload(m->matx_host.data(), m->matx_host.size(), s);
+        m->mats.upload(m4.data(), m4.size(), s);
+        MPHY_CUDA(cudaStreamSynchronize(s));
+        m->general = general;
+        return (int)MPHY_OK;
+    });
+}
+
+int mphy_material_eval(mphy_ctx* c, int32_t n, const double* F, int32_t model, const double* data, double Kinv,
+                       int32_t utype, int32_t tangent, double* stre, double* cmat) {
+    return guarded([&] {
+        MPHY_REQUIRE(c && F && data && stre && cmat && n >= 0 && Kinv > 0.0, MPHY_ERR_INVALID_ARG,
+                     "invalid argument");
+        MPHY_REQUIRE(model >= MPHY_MAT_NEOHOOKEAN && model <= MPHY_MAT_ARRUDABOYCE, MPHY_ERR_INVALID_ARG,
+                     "unknown material model");
+        double row[kMatRow] = {(double)model, data[0], data[1], data[2], data[3], Kinv, (double)utype, 0.0};
+        DevBuf<double> drow(kMatRow);
+        drow.upload(row, kMatRow, c->stream);
+        launch_material_eval(n, F, drow.p, tangent, stre, cmat, c->stream);
+        MPHY_CUDA(cudaStreamSynchronize(c->stream));
+        return (int)MPHY_OK;
+    });
 }
 
 int mphy_material_nh_eval(mphy_ctx* c, int32_t n, const double* F, double mu, double Kinv, int32_t utype,

@@ -93,6 +93,9 @@ struct mphy_mesh {
     mphy::DevBuf<int32_t> conn;    // [n_elem][npe]
     mphy::DevBuf<int32_t> mat_id;  // [n_elem]
     mphy::DevBuf<double> mats;     // [n_mat][4] = mu, Kinv, Utype, 0
+    mphy::DevBuf<double> matx;     // [n_mat][8] = model, data0..3, Kinv, Utype, 0
+    std::vector<double> matx_host;
+    bool general = false;          // some material is not Neo-Hookean: dense-tangent element kernel
     mphy::DevBuf<uint8_t> fixed;   // [n_node*3]
     std::vector<uint8_t> fixed_host;
     std::vector<double> coords_host;  // reference coordinates (aggregation of the coarse space)

@@ -16,6 +16,7 @@
 // That is 30 FMAs per 3x3 block per Gauss point instead of the dense contraction's 108.
 #include "common.cuh"
 #include "elem.cuh"
+#include "elem_store.cuh"
 #include "nh.cuh"
 
 namespace mphy {
@@ -83,6 +84,7 @@ void upload_shape_tables() {
     MPHY_CUDA(cudaMemcpyToSymbol(c_tet10_dN, t10, sizeof(t10)));
     MPHY_CUDA(cudaMemcpyToSymbol(c_tet10_w, w4, sizeof(w4)));
     upload_shape_tables_tc(h8, w8, t10, w4);
+    upload_shape_tables_gen(h8, w8, t10, w4);
 }
 
 __device__ __forceinline__ double det3(const double A[3][3]) {
@@ -267,17 +269,7 @@ __global__ void __launch_bounds__(kEpb * NPE) elem_fp64_kernel(ElemArgs a) {
         for (int gp = 0; gp < NGP; ++gp)
 #pragma unroll
             for (int c = 0; c < 3; ++c) R[c] += s.r[gp][I][c];
-        if (MODE & 1) {
-#pragma unroll
-            for (int c = 0; c < 3; ++c) a.Re[e * NS + 3 * I + c] = R[c];
-        }
-        if (MODE & 2) {
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                if (a.reac) atomicAdd(&a.reac[3 * (int64_t)node + c], R[c]);
-                if (freeI[c]) atomicAdd(&a.rhs[3 * (int64_t)node + c], R[c]);
-            }
-        }
+        store_residual<NPE, MODE>(a, e, I, node, freeI, R);
     }
     constexpr int CH = 4;
 #pragma unroll 1
@@ -325,31 +317,7 @@ __global__ void __launch_bounds__(kEpb * NPE) elem_fp64_kernel(ElemArgs a) {
         for (int j = 0; j < CH; ++j) {
             const int J = J0 + j;
             if (J >= NPE) break;
-            if (MODE & 1) {
-#pragma unroll
-                for (int aa = 0; aa < 3; ++aa)
-#pragma unroll
-                    for (int bb = 0; bb < 3; ++bb) a.Ke[(e * NS + 3 * I + aa) * NS + 3 * J + bb] = acc[j][3 * aa + bb];
-            }
-            if (MODE & 2) {
-                const int32_t nJ = a.conn[e * NPE + J];
-                const uint32_t off = a.e2v[(e * NPE + I) * NPE + J];
-                if (a.valf) {
-                    // FP32 storage: off-diagonal blocks, unmasked; the diagonal is rebuilt from them
-                    if (nJ != node) {
-#pragma unroll
-                        for (int v = 0; v < 9; ++v) atomicAdd(&a.valf[off + 32u * v], (float)acc[j][v]);
-                    }
-                } else {
-#pragma unroll
-                    for (int bb = 0; bb < 3; ++bb) {
-                        if (a.fixed[3 * (int64_t)nJ + bb]) continue;
-#pragma unroll
-                        for (int aa = 0; aa < 3; ++aa)
-                            if (freeI[aa]) atomicAdd(&a.val[off + 32u * (3 * aa + bb)], acc[j][3 * aa + bb]);
-                    }
-                }
-            }
+            store_block<NPE, MODE>(a, e, I, J, node, freeI, acc[j]);
         }
     }
 }

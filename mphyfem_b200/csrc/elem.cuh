@@ -9,7 +9,8 @@ struct ElemArgs {
     const double* coords;   // [n_node][3]
     const int32_t* conn;    // [n_elem][npe]
     const int32_t* mat_id;  // [n_elem]
-    const double* mats;     // [n_mat][4]
+    const double* mats;     // [n_mat][4] = mu, Kinv, Utype, 0 (Neo-Hookean kernels)
+    const double* matx = nullptr;  // [n_mat][8] = model, data0..3, Kinv, Utype, 0 (general kernel)
     const double* disp;     // [n_node*3]
     int tangent;
     unsigned long long* bad;  // min element id with det F < 0 (init ULLONG_MAX)
@@ -33,6 +34,11 @@ void launch_elem_fp64(const ElemArgs& a, int npe, int mode, cudaStream_t s);
 // Mixed-precision element kernel (elem_tc.cu): FP64 residual, tangent contraction on tensor
 // cores (split-BF16, FP32 accumulation), FP32 off-diagonal scatter (a.valf) or Ke export.
 void launch_elem_tc(const ElemArgs& a, int npe, int mode, cudaStream_t s);
+// Element kernel for any material model of the table a.matx (elem_gen.cu).
+void launch_elem_gen(const ElemArgs& a, int npe, int mode, cudaStream_t s);
+void upload_shape_tables_gen(const double* h8, const double* w8, const double* t10, const double* w4);
+void launch_material_eval(int n, const double* F, const double* row_dev, int tangent, double* stre, double* C,
+                          cudaStream_t s);
 void launch_nh_eval(int n, const double* F, double mu, double Kinv, int utype, int tangent, double* stre,
                     double* C, cudaStream_t s);
 void launch_scatter_batch(int npe, int32_t n, const int32_t* ids, const mphy_mesh* mesh, const mphy_pattern* P,

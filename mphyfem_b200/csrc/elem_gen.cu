@@ -1,0 +1,292 @@
+// elem_gen.cu -- element kernel for any hyperelastic model of the material table, and the batched
+// material call over the same models.
+//
+// Replaces Elem_Solid_3D_Disp::calcStiffnessAndResidual (Elem_Solid_3D_Disp.cpp:196-373) with
+// MaterialBase::computeStressAndTangent dispatched to Matl_NeoHookean, Matl_MooneyRivlin,
+// Matl_Gent or Matl_ArrudaBoyce per element (utilitiesmaterialHyperelastic.cpp:186-677). The
+// reference's contraction with the dense 9x9 tangent is kept:
+//     K_IJ(a, b) = sum_gp dvol sum_{m,n} h_mI C(a + 3m, b + 3n) h_nJ
+// evaluated per Gauss point as Gc_I(a, q) = sum_m h_mI C(a + 3m, q) (81 FMAs per row node), then
+// K_IJ(a, b) += sum_n Gc_I(a, b + 3n) h_nJ (27 FMAs per block).
+//
+// Layout: one element per group of NPE * NCH threads. Phase 1: one thread per Gauss point builds
+// F, the spatial gradients h and dvol * {sigma, C} in shared memory. Phase 2: thread (I, ch) owns
+// row node I and the column nodes J of chunk ch (4 per chunk), so the 9 * 4 accumulators stay in
+// registers; chunk 0 also forms the residual of node I.
+#include "common.cuh"
+#include "elem.cuh"
+#include "elem_store.cuh"
+#include "mat.cuh"
+
+namespace mphy {
+
+namespace {
+
+// This translation unit's copy of the shape tables (dN/dxi at the Gauss points and the weights),
+// filled by upload_shape_tables_gen from the host tables of elem.cu.
+__constant__ double g_hex8_dN[8 * 3 * 8];
+__constant__ double g_hex8_w[8];
+__constant__ double g_tet10_dN[4 * 3 * 10];
+__constant__ double g_tet10_w[4];
+
+template <int NPE>
+struct GenTraits;
+template <>
+struct GenTraits<8> {
+    static constexpr int NGP = 8;
+    static constexpr int PAD = 2;  // element stride 962 doubles: two elements of a warp on distinct banks
+    __device__ static const double* dN(int gp) { return g_hex8_dN + gp * 3 * 8; }
+    __device__ static double w(int gp) { return g_hex8_w[gp]; }
+};
+template <>
+struct GenTraits<10> {
+    static constexpr int NGP = 4;
+    static constexpr int PAD = 6;  // element stride 546 doubles
+    __device__ static const double* dN(int gp) { return g_tet10_dN + gp * 3 * 10; }
+    __device__ static double w(int gp) { return g_tet10_w[gp]; }
+};
+
+constexpr int kGenEpb = 8;  // elements per CTA
+constexpr int kGenCh = 4;   // column nodes per thread
+
+template <int NPE>
+struct GenSmem {
+    static constexpr int NGP = GenTraits<NPE>::NGP;
+    double x0[NPE][3];
+    double u[NPE][3];
+    double h[NGP][NPE][3];
+    double C[NGP][81];   // dvol * C
+    double sig[NGP][9];  // dvol * sigma
+    double pad[GenTraits<NPE>::PAD];
+};
+
+__device__ __forceinline__ double det3g(const double A[3][3]) {
+    return A[0][0] * (A[1][1] * A[2][2] - A[1][2] * A[2][1]) - A[0][1] * (A[1][0] * A[2][2] - A[1][2] * A[2][0]) +
+           A[0][2] * (A[1][0] * A[2][1] - A[1][1] * A[2][0]);
+}
+
+__device__ __forceinline__ void inv3g(const double A[3][3], double det, double Ai[3][3]) {
+    const double r = 1.0 / det;
+    Ai[0][0] = (A[1][1] * A[2][2] - A[1][2] * A[2][1]) * r;
+    Ai[0][1] = (A[0][2] * A[2][1] - A[0][1] * A[2][2]) * r;
+    Ai[0][2] = (A[0][1] * A[1][2] - A[0][2] * A[1][1]) * r;
+    Ai[1][0] = (A[1][2] * A[2][0] - A[1][0] * A[2][2]) * r;
+    Ai[1][1] = (A[0][0] * A[2][2] - A[0][2] * A[2][0]) * r;
+    Ai[1][2] = (A[0][2] * A[1][0] - A[0][0] * A[1][2]) * r;
+    Ai[2][0] = (A[1][0] * A[2][1] - A[1][1] * A[2][0]) * r;
+    Ai[2][1] = (A[0][1] * A[2][0] - A[0][0] * A[2][1]) * r;
+    Ai[2][2] = (A[0][0] * A[1][1] - A[0][1] * A[1][0]) * r;
+}
+
+__device__ __forceinline__ void square3(const double b[3][3], double b2[3][3]) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) b2[i][j] = b[i][0] * b[0][j] + b[i][1] * b[1][j] + b[i][2] * b[2][j];
+}
+
+// MODE bit 1: export Ke/Re; bit 2: scatter into the matrix / rhs / reactions.
+template <int NPE, int MODE>
+__global__ void __launch_bounds__(kGenEpb * NPE * ((NPE + kGenCh - 1) / kGenCh))
+    elem_gen_kernel(ElemArgs a) {
+    using T = GenTraits<NPE>;
+    constexpr int NGP = T::NGP;
+    constexpr int NCH = (NPE + kGenCh - 1) / kGenCh;
+    constexpr int TPE = NPE * NCH;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    auto* S = reinterpret_cast<GenSmem<NPE>*>(smem_raw);
+    const int el = threadIdx.x / TPE, loc = threadIdx.x % TPE;
+    const int I = loc % NPE, ch = loc / NPE;
+    const int64_t e = (int64_t)blockIdx.x * kGenEpb + el;
+    const bool live = e < a.n_elem;
+    GenSmem<NPE>& s = S[el];
+
+    int32_t node = 0;
+    if (live) {
+        node = a.conn[e * NPE + I];
+        if (ch == 0) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                s.x0[I][d] = a.coords[3 * (int64_t)node + d];
+                s.u[I][d] = a.disp[3 * (int64_t)node + d];
+            }
+        }
+    }
+    __syncthreads();
+
+    // ---- phase 1: one thread per Gauss point
+    if (live && loc < NGP) {
+        const int gp = loc;
+        const double* dN = T::dN(gp);
+        double G[3][3] = {{0}}, Gc[3][3] = {{0}};
+#pragma unroll
+        for (int n = 0; n < NPE; ++n)
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                const double d = dN[r * NPE + n];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    G[r][c] += s.x0[n][c] * d;
+                    Gc[r][c] += (s.x0[n][c] + s.u[n][c]) * d;
+                }
+            }
+        double Gi[3][3], Gci[3][3];
+        inv3g(G, det3g(G), Gi);
+        const double jac = det3g(Gc);
+        inv3g(Gc, jac, Gci);
+        const double dvol = T::w(gp) * jac;
+        // F = I + sum_n u_n (x) grad0 N_n   (ElementBase.cpp:334-361)
+        double F[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+#pragma unroll
+        for (int n = 0; n < NPE; ++n) {
+            double g0[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+                g0[c] = dN[n] * Gi[c][0] + dN[NPE + n] * Gi[c][1] + dN[2 * NPE + n] * Gi[c][2];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int m = 0; m < 3; ++m) F[i][m] += s.u[n][i] * g0[m];
+            double h[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                h[c] = dN[n] * Gci[c][0] + dN[NPE + n] * Gci[c][1] + dN[2 * NPE + n] * Gci[c][2];
+                s.h[gp][n][c] = h[c];
+            }
+        }
+        const double J = det3g(F);
+        if (J < 0.0) {
+            atomicMin(a.bad, (unsigned long long)e);
+            if (a.bad_elem) a.bad_elem[e] = 1;
+        }
+        double b[3][3], b2[3][3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) b[i][j] = F[i][0] * F[j][0] + F[i][1] * F[j][1] + F[i][2] * F[j][2];
+        square3(b, b2);
+        double row[kMatRow];
+#pragma unroll
+        for (int q = 0; q < kMatRow; ++q) row[q] = a.matx[kMatRow * (int64_t)a.mat_id[e] + q];
+        const MatScalars m = material_scalars(row, a.tangent, b, b2, J);
+        material_fill(m, b, b2, dvol, s.sig[gp], s.C[gp]);
+    }
+    __syncthreads();
+    if (!live) return;
+
+    // ---- phase 2: thread (I, ch)
+    bool freeI[3] = {true, true, true};
+    if (MODE & 2) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) freeI[c] = a.fixed[3 * (int64_t)node + c] == 0;
+    }
+    if (ch == 0) {
+        // R_I(a) = -sum_gp dvol sum_m h_mI sigma(a, m)   (Elem_Solid_3D_Disp.cpp:328-334)
+        double R[3] = {0, 0, 0};
+#pragma unroll
+        for (int gp = 0; gp < NGP; ++gp)
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+                R[c] -= s.h[gp][I][0] * s.sig[gp][c] + s.h[gp][I][1] * s.sig[gp][3 + c] +
+                        s.h[gp][I][2] * s.sig[gp][6 + c];
+        store_residual<NPE, MODE>(a, e, I, node, freeI, R);
+    }
+    const int J0 = ch * kGenCh;
+    double acc[kGenCh][9];
+#pragma unroll
+    for (int j = 0; j < kGenCh; ++j)
+#pragma unroll
+        for (int v = 0; v < 9; ++v) acc[j][v] = 0.0;
+#pragma unroll 1
+    for (int gp = 0; gp < NGP; ++gp) {
+        const double h0 = s.h[gp][I][0], h1 = s.h[gp][I][1], h2 = s.h[gp][I][2];
+        const double* C = s.C[gp];
+        double Gc[3][9];
+#pragma unroll
+        for (int aa = 0; aa < 3; ++aa)
+#pragma unroll
+            for (int q = 0; q < 9; ++q) Gc[aa][q] = h0 * C[9 * aa + q] + h1 * C[9 * (3 + aa) + q] + h2 * C[9 * (6 + aa) + q];
+#pragma unroll
+        for (int j = 0; j < kGenCh; ++j) {
+            if (J0 + j < NPE) {
+                const double g0 = s.h[gp][J0 + j][0], g1 = s.h[gp][J0 + j][1], g2 = s.h[gp][J0 + j][2];
+#pragma unroll
+                for (int aa = 0; aa < 3; ++aa)
+#pragma unroll
+                    for (int bb = 0; bb < 3; ++bb)
+                        acc[j][3 * aa + bb] += Gc[aa][bb] * g0 + Gc[aa][3 + bb] * g1 + Gc[aa][6 + bb] * g2;
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < kGenCh; ++j) {
+        const int J = J0 + j;
+        if (J < NPE) store_block<NPE, MODE>(a, e, I, J, node, freeI, acc[j]);
+    }
+}
+
+template <int NPE, int MODE>
+void launch_gen(const ElemArgs& a, cudaStream_t s) {
+    constexpr int TPE = NPE * ((NPE + kGenCh - 1) / kGenCh);
+    const size_t smem = kGenEpb * sizeof(GenSmem<NPE>);
+    static bool configured = false;
+    if (!configured) {
+        MPHY_CUDA(cudaFuncSetAttribute(elem_gen_kernel<NPE, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
+        configured = true;
+    }
+    const unsigned grid = ceil_div((size_t)a.n_elem, kGenEpb);
+    if (grid == 0) return;
+    elem_gen_kernel<NPE, MODE><<<grid, kGenEpb * TPE, smem, s>>>(a);
+    MPHY_CUDA(cudaGetLastError());
+}
+
+// Batched material call: F [n][9] row-major -> sigma [n][9], C [n][81] (reference index order).
+__global__ void material_eval_kernel(int n, const double* __restrict__ Fm, const double* __restrict__ row_in,
+                                     int tangent, double* __restrict__ stre, double* __restrict__ Cout) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    double F[3][3], b[3][3], b2[3][3];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) F[i / 3][i % 3] = Fm[9 * (int64_t)t + i];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) b[i][j] = F[i][0] * F[j][0] + F[i][1] * F[j][1] + F[i][2] * F[j][2];
+    square3(b, b2);
+    double row[kMatRow];
+#pragma unroll
+    for (int q = 0; q < kMatRow; ++q) row[q] = row_in[q];
+    const MatScalars m = material_scalars(row, tangent, b, b2, det3g(F));
+    material_fill(m, b, b2, 1.0, stre + 9 * (int64_t)t, Cout + 81 * (int64_t)t);
+}
+
+}  // namespace
+
+void upload_shape_tables_gen(const double* h8, const double* w8, const double* t10, const double* w4) {
+    MPHY_CUDA(cudaMemcpyToSymbol(g_hex8_dN, h8, sizeof(g_hex8_dN)));
+    MPHY_CUDA(cudaMemcpyToSymbol(g_hex8_w, w8, sizeof(g_hex8_w)));
+    MPHY_CUDA(cudaMemcpyToSymbol(g_tet10_dN, t10, sizeof(g_tet10_dN)));
+    MPHY_CUDA(cudaMemcpyToSymbol(g_tet10_w, w4, sizeof(g_tet10_w)));
+}
+
+void launch_elem_gen(const ElemArgs& a, int npe, int mode, cudaStream_t s) {
+    if (npe == 8) {
+        if (mode == 1) launch_gen<8, 1>(a, s);
+        else if (mode == 2) launch_gen<8, 2>(a, s);
+        else launch_gen<8, 3>(a, s);
+    } else {
+        if (mode == 1) launch_gen<10, 1>(a, s);
+        else if (mode == 2) launch_gen<10, 2>(a, s);
+        else launch_gen<10, 3>(a, s);
+    }
+}
+
+void launch_material_eval(int n, const double* F, const double* row_dev, int tangent, double* stre, double* C,
+                          cudaStream_t s) {
+    if (n <= 0) return;
+    material_eval_kernel<<<ceil_div(n, 128), 128, 0, s>>>(n, F, row_dev, tangent, stre, C);
+    MPHY_CUDA(cudaGetLastError());
+}
+
+}  // namespace mphy

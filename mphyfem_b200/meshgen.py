@@ -55,6 +55,8 @@ class Problem:
     newton_rtol: float = 1e-10
     cg_rtol: float = 1e-12
     meta: dict = field(default_factory=dict)
+    mat_model: np.ndarray | None = None  # [n_mat] int32 hyperelastic model per material (None: Neo-Hookean)
+    mat_data: np.ndarray | None = None  # [n_mat, 4] float64 model parameters (mu; c1 c2; mu Im; mu N)
 
     @property
     def n_node(self) -> int:
@@ -297,8 +299,32 @@ def batch_union(problems, name: str = "batch"):
     fixed = np.concatenate([q.fixed for q in problems]).astype(np.uint8)
     fnodal = np.concatenate([q.fnodal for q in problems])
     q0 = problems[0]
+    model = data = None
+    if any(q.mat_model is not None for q in problems):
+        model = np.concatenate([q.mat_model if q.mat_model is not None else np.zeros(len(q.mats), np.int32)
+                                for q in problems]).astype(np.int32)
+        data = np.concatenate([_material_data(q) for q in problems])
     return Problem(name=name, coords=coords, conn=conn, mat_id=mat_id, mats=mats, fixed=fixed, fnodal=fnodal,
                    dt=q0.dt, t_final=q0.t_final, max_steps=q0.max_steps, newton_rtol=q0.newton_rtol,
                    cg_rtol=q0.cg_rtol,
                    meta={"inst_node_ptr": nptr.astype(np.int32), "inst_elem_ptr": eptr.astype(np.int32),
-                         "inst_mat_ptr": mptr.astype(np.int32), "n_inst": len(problems)})
+                         "inst_mat_ptr": mptr.astype(np.int32), "n_inst": len(problems)},
+                   mat_model=model, mat_data=data)
+
+
+def _material_data(q) -> np.ndarray:
+    """[n_mat, 4] model parameters of a problem (Neo-Hookean rows: mu from mats)."""
+    if q.mat_data is not None:
+        return np.asarray(q.mat_data, np.float64).reshape(len(q.mats), 4)
+    d = np.zeros((len(q.mats), 4))
+    d[:, 0] = q.mats[:, 0]
+    return d
+
+
+def hyperelastic_material(model: int, data, kappa: float, utype: int = 3):
+    """(mats row, model, data row) of one material: model 0 Neo-Hookean (mu), 1 Mooney-Rivlin
+    (c1, c2), 2 Gent (mu, Im), 3 Arruda-Boyce (mu, N); data_volumetric Utype 1/kappa. The mats row
+    carries data[0] in its first slot."""
+    d = np.zeros(4)
+    d[:len(data)] = data
+    return np.array([d[0], 1.0 / kappa, float(utype)]), int(model), d

@@ -6,16 +6,21 @@
     python -m mphyfem_b200.profile_driver --op assemble --precision mixed_tc --reps 3
     python -m mphyfem_b200.profile_driver --op newton --precision mixed --coarse 64 --reps 1
     python -m mphyfem_b200.profile_driver --op batch --instances 48 --reps 2
+    python -m mphyfem_b200.profile_driver --op assemble --model 2 --reps 3
 
 Each run builds the hex8 cantilever of the given size (or, for ``batch``, the first blocks of
 the 512-block batched set), assembles it once at u = 0 and then repeats the chosen operation:
 SpMV with the assembled matrix, the fused assembly, one Newton iteration (assembly + PCG +
-update), or the batched persistent solve of all instances.
+update), or the batched persistent solve of all instances. ``--model`` gives every element one
+hyperelastic model (1 Mooney-Rivlin, 2 Gent, 3 Arruda-Boyce: the dense-tangent element kernel).
+The mean device time per repetition (CUDA events on the library's stream) goes to stderr.
 """
 from __future__ import annotations
 
 import argparse
 import sys
+
+import numpy as np
 
 
 def main(argv=None):
@@ -32,6 +37,7 @@ def main(argv=None):
     ap.add_argument("--instances", type=int, default=48)
     ap.add_argument("--cluster", type=int, default=4)
     ap.add_argument("--threads", type=int, default=512)
+    ap.add_argument("--model", type=int, default=0, choices=[0, 1, 2, 3])
     args = ap.parse_args(argv)
 
     import torch
@@ -53,6 +59,10 @@ def main(argv=None):
               f"ms {ms:.2f}", file=sys.stderr)
         return
     p = meshgen.hex8_cantilever(args.nx, args.ny, args.nz)
+    if args.model:
+        p.mat_model = np.array([args.model], np.int32)
+        p.mat_data = np.array([{1: [0.5, 0.1, 0, 0], 2: [1.0, 12.0, 0, 0], 3: [1.0, 5.0, 0, 0]}[args.model]])
+        p.mats[0, 0] = p.mat_data[0, 0]
     mesh = api.Mesh(ctx, p)
     pat = api.Pattern(mesh)
     sol = api.SolverGpu(mesh, pat, rtol=args.rtol, max_it=20000, precision=prec,
@@ -63,6 +73,10 @@ def main(argv=None):
     sol.calcStiffnessAndResidual(disp)
     x = torch.randn(p.n_dof, dtype=torch.float64, device="cuda")
     y = torch.empty_like(x)
+    stream = torch.cuda.ExternalStream(sol.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
     for _ in range(args.reps):
         if args.op == "spmv":
             sol.spmv(x, y)
@@ -72,7 +86,9 @@ def main(argv=None):
             disp.zero_()
             st = sol.newton_iteration(disp, fext, 0.2)
             print(f"krylov_its={st.krylov_its}", file=sys.stderr)
+    e1.record(stream)
     torch.cuda.synchronize()
+    print(f"{args.op}: {e0.elapsed_time(e1) / max(1, args.reps):.3f} ms per repetition", file=sys.stderr)
     mi = sol.matrix_info()
     print(f"{p.name}: n_dof={p.n_dof} nnz={pat.nnz} blocks={mi['true_blocks']} stored={mi['stored_blocks']} "
           f"value_bytes={mi['value_bytes']}")

@@ -12,8 +12,11 @@ Restated behaviour (host-side, as in the reference):
   ``Time Functions``, ``Solver``, ``Boundary Conditions``, ``Tractions``, ``Nodal Forces``,
   ``Output``, ``Nodal Data Output``; lines starting with ``!``, ``#`` or ``%`` are comments.
   ``Domains`` (Domain.cpp:32-72): per domain label ``Material : id`` and ``Element : id``
-  (1-based). ``Material`` (MaterialBase.cpp:91-116): ``Matl_NeoHookean`` with
-  ``data_deviatoric : mu`` and ``data_volumetric : Utype Kinv``. ``Boundary Conditions``
+  (1-based). ``Material`` (MaterialBase.cpp:91-116; names of myIDmaps.h:233-236, objects of
+  NewMaterial.h:48-54): ``Matl_NeoHookean`` (``data_deviatoric : mu``), ``Matl_MooneyRivlin``
+  (``data_deviatoric : c1 c2``), ``Matl_Gent`` (``data_deviatoric : mu Im``) and
+  ``Matl_ArrudaBoyce`` (``data : mu N``, the line its computeStressAndTangent reads,
+  Matl_ArrudaBoyce.cpp:28), each with ``data_volumetric : Utype Kinv``. ``Boundary Conditions``
   (femBase.cpp:670-771, femSolidmechanics1.cpp:813-915): ``type : fixed`` prescribes every DOF
   of the patch's nodes to zero; ``type : specified`` prescribes ``dof`` to ``value``.
   ``Nodal Forces`` (femBase.cpp:876-919): ``timefunction n``, ``count m``, then m lines
@@ -31,8 +34,8 @@ Restated behaviour (host-side, as in the reference):
 
 Limits of this build's Newton driver, checked with clear errors: the load factor must be
 proportional to time (lam(t) = c t on [0, finalTime]: the driver steps lam = t and the forces are
-scaled by c); prescribed values must be zero; no body force; Neo-Hookean materials; hex8 or
-tet10 volumes. The ``Solver`` block also accepts ``key value`` lines without the colon, the
+scaled by c); prescribed values must be zero; no body force; the four hyperelastic materials
+above; hex8 or tet10 volumes. The ``Solver`` block also accepts ``key value`` lines without the colon, the
 form the reference's own sample config uses (its reader splits on ``:`` only).
 """
 from __future__ import annotations
@@ -44,6 +47,10 @@ import numpy as np
 from .meshgen import Problem
 
 GMSH_VOLUME = {5: 8, 11: 10}          # hex8, tet10
+# material name -> (model code of mphy.h, config line holding its parameters, parameter count)
+MATERIALS = {"Matl_NeoHookean": (0, "data_deviatoric", 1), "Matl_MooneyRivlin": (1, "data_deviatoric", 2),
+             "Matl_Gent": (2, "data_deviatoric", 2), "Matl_ArrudaBoyce": (3, "data", 2)}
+MATERIAL_NAME = {code: name for name, (code, _, _) in MATERIALS.items()}
 GMSH_FACE = {3: 4, 2: 3, 9: 6}        # quad4, tri3, tri6
 GMSH_TYPE_OF = {8: 5, 10: 11, 4: 3, 3: 2, 6: 9}
 DOF_NAMES = {"x": 0, "y": 1, "z": 2, "ux": 0, "uy": 1, "uz": 2, "0": 0, "1": 1, "2": 2}
@@ -359,16 +366,25 @@ def read_config(config_path, mesh_path=None):
             raise ValueError(f"config: domain {label!r} of the mesh has no Domains entry")
         tag_mat[tag] = domains[label][0]
     used = sorted(set(tag_mat.values()))
-    rows = []
+    rows, models, mdata = [], [], []
     for mid in used:
         kv = materials.get(mid)
         if kv is None:
             raise ValueError(f"config: material {mid + 1} is not defined")
-        if kv.get("name") != "Matl_NeoHookean":
-            raise NotImplementedError(f"config: material {kv.get('name')!r}: Matl_NeoHookean is supported")
-        mu = float(kv["data_deviatoric"].split()[0])
+        if kv.get("name") not in MATERIALS:
+            raise NotImplementedError(f"config: material {kv.get('name')!r}: supported are {sorted(MATERIALS)}")
+        code, line, npar = MATERIALS[kv["name"]]
+        if line not in kv:
+            raise ValueError(f"config: material {mid + 1} ({kv['name']}) has no {line} line")
+        par = [float(x) for x in kv[line].split()]
+        if len(par) < npar:
+            raise ValueError(f"config: {kv['name']} needs {npar} values on its {line} line")
         ut, kinv = kv["data_volumetric"].split()[:2]
-        rows.append([mu, float(kinv), float(int(ut))])
+        rows.append([par[0], float(kinv), float(int(ut))])
+        d = np.zeros(4)
+        d[:npar] = par[:npar]
+        models.append(code)
+        mdata.append(d)
     row_of = {mid: k for k, mid in enumerate(used)}
     conn = np.array([c for _, _, c in vol], dtype=np.int32)
     mat_id = np.array([row_of[tag_mat[tag]] for _, tag, _ in vol], dtype=np.int32)
@@ -417,6 +433,9 @@ def read_config(config_path, mesh_path=None):
                    dt=dt, t_final=tfin, max_steps=solver["maximumSteps"],
                    meta={"tolerance": solver["tolerance"], "maximumIterations": solver["maximumIterations"],
                          "domains": m["domains"], "patches": list(m["patches"])})
+    if any(models):
+        prob.mat_model = np.array(models, dtype=np.int32)
+        prob.mat_data = np.array(mdata, dtype=np.float64)
     return prob
 
 
@@ -432,9 +451,13 @@ def write_config(path, mesh_name, prob: Problem, fixed_patches=(), domain_names=
         out += [f"  {domain_names[m]}", "  {", f"    Material : {m + 1}", "    Element  : 1", "  }"]
     out += ["}", ""]
     for m, (mu, kinv, ut) in enumerate(prob.mats):
-        out += ["Material", "{", f"  id              : {m + 1}", "  name            : Matl_NeoHookean",
-                "  density         : 1.0", f"  data_deviatoric : {float(mu)!r}", f"  data_volumetric : {int(ut)} {float(kinv)!r}",
-                "}", ""]
+        code = int(prob.mat_model[m]) if prob.mat_model is not None else 0
+        name = MATERIAL_NAME[code]
+        _, line, npar = MATERIALS[name]
+        par = prob.mat_data[m][:npar] if prob.mat_model is not None else [mu]
+        out += ["Material", "{", f"  id              : {m + 1}", f"  name            : {name}",
+                "  density         : 1.0", f"  {line:<15} : " + " ".join(repr(float(v)) for v in par),
+                f"  data_volumetric : {int(ut)} {float(kinv)!r}", "}", ""]
     etype = "ELEM_SOLID_3D_DISP"
     out += ["Element", "{", "  id   : 1", f"  type : {etype}", "}", ""]
     if fixed_patches:

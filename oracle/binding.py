@@ -54,6 +54,9 @@ def lib():
         L.orc_vol_d2U.restype = C.c_double
         L.orc_elem_stiffness_residual.argtypes = [C.c_int, _d, _d, C.c_double, C.c_double, C.c_int, _d, _d]
         L.orc_gauss_rule.argtypes = [C.c_int, _d, _d, _d, _d]
+        L.orc_material_stress_tangent.argtypes = [C.c_int, _d, C.c_double, C.c_int, _d, _d, _d]
+        L.orc_elem_stiffness_residual_mat.argtypes = [C.c_int, _d, _d, C.c_int, _d, C.c_double, C.c_int, _d, _d]
+        L.orc_problem_set_materials.argtypes = [C.c_void_p, C.c_int, _i32, _d]
         L.orc_problem_create.argtypes = [C.c_int, _d, C.c_int, C.c_int, _i32, _i32, C.c_int, _d, _u8]
         L.orc_problem_create.restype = C.c_void_p
         L.orc_problem_destroy.argtypes = [C.c_void_p]
@@ -102,6 +105,38 @@ def elem_stiffness_residual(X, u, mu, Kinv, utype=3):
     return K, R, bad
 
 
+MAT_NEOHOOKEAN, MAT_MOONEYRIVLIN, MAT_GENT, MAT_ARRUDABOYCE = 0, 1, 2, 3
+MAT_NDATA = 4
+
+
+def _mat_data(data):
+    d = np.zeros(MAT_NDATA)
+    d[:len(data)] = data
+    return d
+
+
+def material_stress_tangent(model, data, F, Kinv, utype=3):
+    """Stress (9) and tangent (9x9) of any hyperelastic model, reference index order."""
+    F = np.ascontiguousarray(F, dtype=np.float64).reshape(9)
+    d = _mat_data(data)
+    s, Cm = np.zeros(9), np.zeros(81)
+    rc = lib().orc_material_stress_tangent(int(model), _p(d, _d), Kinv, utype, _p(F, _d), _p(s, _d), _p(Cm, _d))
+    if rc:
+        raise ValueError(f"oracle: unknown material model {model}")
+    return s, Cm.reshape(9, 9)
+
+
+def elem_stiffness_residual_mat(X, u, model, data, Kinv, utype=3):
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    d = _mat_data(data)
+    npe = X.shape[0]
+    K, R = np.zeros((3 * npe, 3 * npe)), np.zeros(3 * npe)
+    bad = lib().orc_elem_stiffness_residual_mat(npe, _p(X, _d), _p(u, _d), int(model), _p(d, _d), Kinv, utype,
+                                                _p(K, _d), _p(R, _d))
+    return K, R, bad
+
+
 def gauss_rule(npe):
     xi, w = np.zeros((8, 3)), np.zeros(8)
     N, dN = np.zeros((8, npe)), np.zeros((8, 3, npe))
@@ -122,6 +157,13 @@ class OracleProblem:
                                           _p(m, _i32), mt.shape[0], _p(mt, _d), _p(fx, _u8))
         if not self.h:
             raise ValueError("oracle: unsupported element type")
+        models = getattr(prob, "mat_model", None)
+        if models is not None:
+            mdl = np.ascontiguousarray(models, np.int32)
+            dat = np.ascontiguousarray(prob.mat_data, np.float64).reshape(len(mdl), MAT_NDATA)
+            self._keep += [mdl, dat]
+            if lib().orc_problem_set_materials(self.h, len(mdl), _p(mdl, _i32), _p(dat, _d)):
+                raise ValueError("oracle: invalid material models")
         self.n_free = lib().orc_problem_nfree(self.h)
         self.nnz = lib().orc_problem_nnz(self.h)
 

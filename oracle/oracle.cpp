@@ -171,7 +171,9 @@ struct orc_problem {
     int n_node, n_elem, npe;
     std::vector<double> coords;
     std::vector<int32_t> conn, mat_id;
-    std::vector<double> mats;  // [n_mat][3]
+    std::vector<double> mats;  // [n_mat][3] = {mu, Kinv, Utype}
+    std::vector<int32_t> model;  // [n_mat] ORC_MAT_* (Neo-Hookean unless set)
+    std::vector<double> data;    // [n_mat][ORC_MAT_NDATA] model parameters (data[0] = mu by default)
     std::vector<uint8_t> fixed;
     CsrPattern pat;
     // position of each (element row i, element col j) entry in the CSR value array, -1 if
@@ -260,6 +262,166 @@ int orc_nh_stress_tangent(const double* Fm, double mu, double Kinv, int Utype, d
     return 0;
 }
 
+namespace {
+
+// Shared pieces of the three b-invariant models below: b = F F^T, b^2, J, the trace, the
+// deviatoric part of b, U'(J), U''(J).
+struct Kin {
+    double b[3][3], b2[3][3], bdev[3][3];
+    double J, Ib, dU, d2U;
+};
+
+Kin kinematics(const double* Fm, double Kinv, int Utype) {
+    Kin k;
+    double F[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) F[i][j] = Fm[3 * i + j];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) k.b[i][j] = F[i][0] * F[j][0] + F[i][1] * F[j][1] + F[i][2] * F[j][2];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            k.b2[i][j] = k.b[i][0] * k.b[0][j] + k.b[i][1] * k.b[1][j] + k.b[i][2] * k.b[2][j];
+    k.J = det3(F);
+    k.Ib = k.b[0][0] + k.b[1][1] + k.b[2][2];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) k.bdev[i][j] = k.b[i][j] - (i == j ? k.Ib / 3.0 : 0.0);
+    const double K = 1.0 / Kinv;
+    k.dU = orc_vol_dU(Utype, K, k.J);
+    k.d2U = orc_vol_d2U(Utype, K, k.J);
+    return k;
+}
+
+// Mooney-Rivlin, utilitiesmaterialHyperelastic.cpp:300-420, compressible branch. data = {c1, c2}.
+// The reference sets r7d3 = 5.0/3.0 (:303), so its "J^{-7/3}" factor is J^{-5/3}; restated as
+// written (the c2 terms of stress and tangent both carry J^{-5/3}). With that factor the c2 stress
+// is J^{2/3} times an energy's stress, and its exact linearisation adds (2/3) sigma_c2 (x) I to
+// the tangent below: a non-symmetric term that a CG solve cannot take, so both tangent modes
+// give the symmetric tangent as written.
+void mooney_rivlin(const double* Fm, const double* data, double Kinv, int Utype, double* stre, double* C) {
+    const Kin k = kinematics(Fm, Kinv, Utype);
+    const double c1 = data[0], c2 = data[1];
+    const double Jm5d3 = std::pow(k.J, -2.0 / 3.0) / k.J;
+    const double Jm7d3 = std::pow(k.J, -5.0 / 3.0);
+    const double I1 = k.Ib;
+    const double I2 = 0.5 * (I1 * I1 - (k.b2[0][0] + k.b2[1][1] + k.b2[2][2]));
+    const double s1 = 2.0 * c1 * Jm5d3 + 2.0 * c2 * Jm7d3 * I1;
+    const double s2 = -c1 * (2.0 / 3.0) * Jm5d3 * I1 - c2 * (4.0 / 3.0) * Jm7d3 * I2 + k.dU;
+    const double s3 = -2.0 * c2 * Jm7d3;
+    for (int q = 0; q < 9; ++q) {
+        const int i = kPairI[q], j = kPairJ[q];
+        stre[q] = s1 * k.b[i][j] + s3 * k.b2[i][j] + (i == j ? s2 : 0.0);
+    }
+    const double f1 = 2.0 * c1 * Jm5d3, f2 = 2.0 * c2 * Jm7d3, f3 = (4.0 / 3.0) * c2 * Jm7d3;
+    const double f7 = k.J * k.d2U + k.dU, f8 = -k.dU;
+    const auto& b = k.b;
+    const auto& b2 = k.b2;
+    for (int p = 0; p < 9; ++p) {
+        const int i = kPairI[p], j = kPairJ[p];
+        for (int q = 0; q < 9; ++q) {
+            const int kk = kPairI[q], l = kPairJ[q];
+            const double dij = kd(i, j), dik = kd(i, kk), dil = kd(i, l), djk = kd(j, kk), dkl = kd(kk, l);
+            double v = f1 * (dik * b[j][l] + (1.0 / 3.0) * I1 * dil * djk + (2.0 / 9.0) * I1 * dij * dkl -
+                             (2.0 / 3.0) * b[i][j] * dkl - (2.0 / 3.0) * b[kk][l] * dij);
+            v += f2 * (2.0 * b[i][j] * b[kk][l] + I1 * dik * b[j][l] - b[i][kk] * b[j][l] - b[i][l] * b[kk][j] -
+                       dik * b2[j][l]);
+            v += f3 * (I2 * dil * djk + (4.0 / 3.0) * I2 * dkl * dij + 2.0 * dij * b2[kk][l] + 2.0 * dkl * b2[i][j] -
+                       2.0 * I1 * dkl * b[i][j] - 2.0 * I1 * dij * b[kk][l]);
+            v += f7 * (dij * dkl) + f8 * (dil * djk);
+            C[9 * p + q] = v;
+        }
+    }
+}
+
+// Gent, utilitiesmaterialHyperelastic.cpp:423-548, compressible branch. data = {mu, Im}.
+void gent(const double* Fm, const double* data, double Kinv, int Utype, double* stre, double* C) {
+    const Kin k = kinematics(Fm, Kinv, Utype);
+    const double mu = data[0], Im = data[1];
+    const double Jm2d3 = std::pow(k.J, -2.0 / 3.0);
+    const double Jm5d3 = Jm2d3 / k.J;
+    const double Jm7d3 = std::pow(k.J, -7.0 / 3.0);
+    const double gf = 1.0 / (1.0 - (Jm2d3 * k.Ib - 3.0) / Im);
+    const double s1 = mu * Jm5d3 * gf;
+    const double s2 = -s1 * (1.0 / 3.0) * k.Ib + k.dU;
+    for (int q = 0; q < 9; ++q) {
+        const int i = kPairI[q], j = kPairJ[q];
+        stre[q] = s1 * k.b[i][j] + (i == j ? s2 : 0.0);
+    }
+    const double f1 = -(2.0 / 3.0) * mu * Jm5d3 * gf, f2 = 2.0 * mu * Jm7d3 * gf * gf / Im, f3 = mu * Jm5d3 * gf;
+    const double f7 = k.J * k.d2U + k.dU, f8 = -k.dU;
+    const auto& b = k.b;
+    const auto& bd = k.bdev;
+    for (int p = 0; p < 9; ++p) {
+        const int i = kPairI[p], j = kPairJ[p];
+        for (int q = 0; q < 9; ++q) {
+            const int kk = kPairI[q], l = kPairJ[q];
+            const double dij = kd(i, j), dik = kd(i, kk), dil = kd(i, l), djk = kd(j, kk), dkl = kd(kk, l);
+            double v = f1 * (bd[i][j] * dkl);
+            v += f2 * (bd[i][j] * bd[kk][l]);
+            v += f3 * (dik * b[j][l] - (2.0 / 3.0) * b[kk][l] * dij + (1.0 / 3.0) * k.Ib * dil * djk);
+            v += f7 * (dij * dkl) + f8 * (dil * djk);
+            C[9 * p + q] = v;
+        }
+    }
+}
+
+// Arruda-Boyce (five-term inverse-Langevin series), utilitiesmaterialHyperelastic.cpp:551-677,
+// compressible branch. data = {mu, N}.
+void arruda_boyce(const double* Fm, const double* data, double Kinv, int Utype, double* stre, double* C) {
+    const Kin k = kinematics(Fm, Kinv, Utype);
+    const double mu = data[0], N = data[1];
+    const double c1 = mu / 2.0, c2 = mu / 20.0 / N, c3 = mu * 11.0 / 1050.0 / N / N,
+                 c4 = mu * 19.0 / 7000.0 / N / N / N, c5 = mu * 519.0 / 673750.0 / N / N / N / N;
+    const double Jm2d3 = std::pow(k.J, -2.0 / 3.0);
+    const double Jm5d3 = std::pow(k.J, -5.0 / 3.0);
+    const double Jm7d3 = std::pow(k.J, -7.0 / 3.0);
+    const double Ibb = Jm2d3 * k.Ib;
+    const double a1 = c1 + 2.0 * c2 * Ibb + 3.0 * c3 * Ibb * Ibb + 4.0 * c4 * Ibb * Ibb * Ibb +
+                      5.0 * c5 * Ibb * Ibb * Ibb * Ibb;
+    const double a2 = 2.0 * c2 + 6.0 * c3 * Ibb + 12.0 * c4 * Ibb * Ibb + 20.0 * c5 * Ibb * Ibb * Ibb;
+    const double s1 = 2.0 * a1 * Jm5d3;
+    const double s2 = -s1 * (1.0 / 3.0) * k.Ib + k.dU;
+    for (int q = 0; q < 9; ++q) {
+        const int i = kPairI[q], j = kPairJ[q];
+        stre[q] = s1 * k.b[i][j] + (i == j ? s2 : 0.0);
+    }
+    const double f1 = 4.0 * Jm7d3 * a2, f2 = -4.0 * (1.0 / 3.0) * a1 * Jm5d3, f3 = (2.0 / 3.0) * a1 * Jm5d3 * k.Ib,
+                 f4 = 4.0 * (1.0 / 3.0) * (1.0 / 3.0) * a1 * Jm5d3 * k.Ib;
+    const double f7 = k.J * k.d2U + k.dU, f8 = -k.dU;
+    const auto& b = k.b;
+    const auto& bd = k.bdev;
+    for (int p = 0; p < 9; ++p) {
+        const int i = kPairI[p], j = kPairJ[p];
+        for (int q = 0; q < 9; ++q) {
+            const int kk = kPairI[q], l = kPairJ[q];
+            const double dij = kd(i, j), dik = kd(i, kk), dil = kd(i, l), djk = kd(j, kk), djl = kd(j, l),
+                         dkl = kd(kk, l);
+            double v = f1 * (bd[i][j] * bd[kk][l]);
+            v += f2 * (b[i][j] * dkl + b[kk][l] * dij);
+            v += f3 * (dik * djl + dil * djk);
+            v += f4 * (dij * dkl);
+            v += f7 * (dij * dkl) + f8 * (dil * djk);
+            // The deviatoric part above is the symmetrised form "without stress terms" (:655-660):
+            // it has (2/3) a1 J^{-5/3} Ib d_ik d_jl where the exact linearisation of the stress
+            // has 2 a1 J^{-5/3} d_ik b_jl. The consistent tangent swaps them.
+            if (g_consistent_tangent) v += 2.0 * a1 * Jm5d3 * dik * (b[j][l] - (1.0 / 3.0) * k.Ib * djl);
+            C[9 * p + q] = v;
+        }
+    }
+}
+
+}  // namespace
+
+int orc_material_stress_tangent(int model, const double* data, double Kinv, int Utype, const double* F,
+                                double* stre, double* C) {
+    switch (model) {
+        case ORC_MAT_NEOHOOKEAN: return orc_nh_stress_tangent(F, data[0], Kinv, Utype, stre, C);
+        case ORC_MAT_MOONEYRIVLIN: mooney_rivlin(F, data, Kinv, Utype, stre, C); return 0;
+        case ORC_MAT_GENT: gent(F, data, Kinv, Utype, stre, C); return 0;
+        case ORC_MAT_ARRUDABOYCE: arruda_boyce(F, data, Kinv, Utype, stre, C); return 0;
+        default: return 2;
+    }
+}
+
 void orc_set_consistent_tangent(int on) { g_consistent_tangent = on ? 1 : 0; }
 void orc_set_pattern_mode(int mode) { g_pattern_mode = mode; }
 
@@ -285,6 +447,11 @@ int orc_gauss_rule(int npe, double* xi, double* w, double* N, double* dNdxi) {
 // then gradients and volume in the current configuration x = X + u.
 int orc_elem_stiffness_residual(int npe, const double* X, const double* u, double mu, double Kinv,
                                 int Utype, double* K, double* R) {
+    return orc_elem_stiffness_residual_mat(npe, X, u, ORC_MAT_NEOHOOKEAN, &mu, Kinv, Utype, K, R);
+}
+
+int orc_elem_stiffness_residual_mat(int npe, const double* X, const double* u, int model, const double* data,
+                                    double Kinv, int Utype, double* K, double* R) {
     GaussRule rule;
     if (!element_rule(npe, rule)) return 2;
     const int ns = 3 * npe;
@@ -306,7 +473,7 @@ int orc_elem_stiffness_residual(int npe, const double* X, const double* u, doubl
         if (det3(Fa) < 0.0) bad = 1;
         const double dvol = rule.w[q] * spatial_gradients(npe, x, dN, g);
         double stre[9], C[81];
-        orc_nh_stress_tangent(F, mu, Kinv, Utype, stre, C);
+        if (orc_material_stress_tangent(model, data, Kinv, Utype, F, stre, C) != 0) return 2;
         for (int I = 0; I < npe; ++I) {
             const double bb[3] = {dvol * g[0][I], dvol * g[1][I], dvol * g[2][I]};
             double Gc[3][9];
@@ -438,8 +605,10 @@ void gather_element(const orc_problem* p, int64_t e, const double* disp, double*
 void elem_eval(const orc_problem* p, int64_t e, const double* disp, double* K, double* R, int* bad) {
     double X[3 * kMaxNpe], u[3 * kMaxNpe];
     gather_element(p, e, disp, X, u);
-    const double* m = &p->mats[3 * (size_t)p->mat_id[e]];
-    *bad = orc_elem_stiffness_residual(p->npe, X, u, m[0], m[1], (int)m[2], K, R);
+    const size_t id = (size_t)p->mat_id[e];
+    const double* m = &p->mats[3 * id];
+    *bad = orc_elem_stiffness_residual_mat(p->npe, X, u, p->model[id], &p->data[ORC_MAT_NDATA * id], m[1], (int)m[2],
+                                           K, R);
 }
 
 }  // namespace
@@ -458,12 +627,24 @@ orc_problem* orc_problem_create(int n_node, const double* coords, int n_elem, in
     p->conn.assign(conn, conn + (size_t)n_elem * npe);
     p->mat_id.assign(mat_id, mat_id + n_elem);
     p->mats.assign(mats, mats + 3 * (size_t)n_mat);
+    p->model.assign(n_mat, ORC_MAT_NEOHOOKEAN);
+    p->data.assign(ORC_MAT_NDATA * (size_t)n_mat, 0.0);
+    for (int k = 0; k < n_mat; ++k) p->data[ORC_MAT_NDATA * (size_t)k] = mats[3 * k];
     p->fixed.assign(fixed, fixed + 3 * (size_t)n_node);
     build_pattern(p);
     return p;
 }
 
 void orc_problem_destroy(orc_problem* p) { delete p; }
+
+int orc_problem_set_materials(orc_problem* p, int n_mat, const int32_t* model, const double* data) {
+    if (n_mat != (int)p->model.size()) return 1;
+    for (int k = 0; k < n_mat; ++k)
+        if (model[k] < ORC_MAT_NEOHOOKEAN || model[k] > ORC_MAT_ARRUDABOYCE) return 2;
+    p->model.assign(model, model + n_mat);
+    p->data.assign(data, data + ORC_MAT_NDATA * (size_t)n_mat);
+    return 0;
+}
 int orc_problem_nfree(const orc_problem* p) { return p->pat.n_free; }
 int64_t orc_problem_nnz(const orc_problem* p) { return p->pat.rowptr.back(); }
 

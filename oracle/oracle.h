@@ -34,6 +34,21 @@ extern "C" {
 int orc_nh_stress_tangent(const double* F, double mu, double Kinv, int Utype,
                           double* stre, double* Cmat);
 
+/* Hyperelastic models of the reference's MaterialBase family and their parameters:
+ *   ORC_MAT_NEOHOOKEAN   Matl_NeoHookean,   data_deviatoric = {mu}
+ *   ORC_MAT_MOONEYRIVLIN Matl_MooneyRivlin, data_deviatoric = {c1, c2}
+ *                        (utilitiesmaterialHyperelastic.cpp:300-420)
+ *   ORC_MAT_GENT         Matl_Gent,         data_deviatoric = {mu, Im}  (:423-548)
+ *   ORC_MAT_ARRUDABOYCE  Matl_ArrudaBoyce,  data = {mu, N}              (:551-677)
+ * each with the volumetric energy Utype and Kinv = 1/K of data_volumetric. */
+enum { ORC_MAT_NEOHOOKEAN = 0, ORC_MAT_MOONEYRIVLIN = 1, ORC_MAT_GENT = 2, ORC_MAT_ARRUDABOYCE = 3 };
+enum { ORC_MAT_NDATA = 4 };
+
+/* Stress and tangent of any model above, same conventions as orc_nh_stress_tangent.
+ * Returns 0, or 2 for an unknown model. */
+int orc_material_stress_tangent(int model, const double* data, double Kinv, int Utype, const double* F,
+                                double* stre, double* Cmat);
+
 /* Test-only switch: 0 (default) = the reference's tangent; 1 = add the volumetric geometric
  * term U'(J) d_ik d_jl that the reference omits, giving the consistent tangent -dR/du. */
 void orc_set_consistent_tangent(int on);
@@ -54,6 +69,10 @@ double orc_vol_d2U(int Utype, double K, double J);
 int orc_elem_stiffness_residual(int npe, const double* X, const double* u, double mu,
                                 double Kinv, int Utype, double* K, double* R);
 
+/* orc_elem_stiffness_residual with any material model (data: [ORC_MAT_NDATA]). */
+int orc_elem_stiffness_residual_mat(int npe, const double* X, const double* u, int model, const double* data,
+                                    double Kinv, int Utype, double* K, double* R);
+
 /* Gauss points and shape functions used by the element (for cross-checks). Writes ngp and
  * xi[ngp][3], w[ngp]; N[ngp][npe]; dNdxi[ngp][3][npe]. Returns ngp. */
 int orc_gauss_rule(int npe, double* xi, double* w, double* N, double* dNdxi);
@@ -68,6 +87,10 @@ orc_problem* orc_problem_create(int n_node, const double* coords, int n_elem, in
                                 const int32_t* conn, const int32_t* mat_id, int n_mat,
                                 const double* mats, const uint8_t* fixed);
 void orc_problem_destroy(orc_problem* p);
+/* Per-material model codes [n_mat] and parameters [n_mat][ORC_MAT_NDATA]; Kinv and Utype stay
+ * those of orc_problem_create. Without this call every material is Neo-Hookean with mu =
+ * mats[3k]. Returns 0, 1 when n_mat differs from the problem's, 2 for an unknown model. */
+int orc_problem_set_materials(orc_problem* p, int n_mat, const int32_t* model, const double* data);
 int orc_problem_nfree(const orc_problem* p);
 int64_t orc_problem_nnz(const orc_problem* p);
 /* assy_for_soln: [n_free]; for_assy_vec: [n_elem][3npe]; rowptr: [n_free+1]; col: [nnz] */

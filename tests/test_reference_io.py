@@ -145,3 +145,33 @@ def test_config_reader_rules(tmp_path):
     (tmp_path / "config").write_text(CONFIG.replace("Solver", "Solvr"))
     with pytest.raises(ValueError):
         rio.read_config(tmp_path / "config")                     # unknown block key
+
+
+def test_material_models_round_trip(tmp_path):
+    # Matl_MooneyRivlin / Matl_Gent read data_deviatoric; Matl_ArrudaBoyce reads its data line
+    p = meshgen.two_phase_inclusions(16, 4, 4, seed=3, r_range=(0.2, 0.3))
+    n_mat = len(p.mats)
+    p.mat_model = np.array([1, 3][:n_mat], np.int32)
+    p.mat_data = np.array([[0.4, 0.15, 0, 0], [0.7, 5.0, 0, 0]][:n_mat])
+    p.mats[:, 0] = p.mat_data[:, 0]
+    clamp = rio.boundary_faces(p, lambda X: np.isclose(X[:, 0], 0.0))
+    q = _write(tmp_path, p, {"clamp": clamp})
+    text = (tmp_path / "config").read_text()
+    assert "Matl_MooneyRivlin" in text and "data_deviatoric : 0.4 0.15" in text
+    assert "Matl_ArrudaBoyce" in text and "data            : 0.7 5.0" in text
+    assert np.array_equal(q.mat_model[q.mat_id], p.mat_model[p.mat_id])
+    assert np.array_equal(q.mat_data[q.mat_id], p.mat_data[p.mat_id])
+    assert np.array_equal(q.mats[q.mat_id], p.mats[p.mat_id])
+
+
+def test_gent_block(tmp_path):
+    p = meshgen.hex8_cantilever(2, 1, 1)
+    clamp = rio.boundary_faces(p, lambda X: np.isclose(X[:, 0], 0.0))
+    rio.write_gmsh22(tmp_path / "m.msh", p, {"clamp": clamp})
+    (tmp_path / "config").write_text(CONFIG.replace("Matl_NeoHookean", "Matl_Gent")
+                                     .replace("data_deviatoric :  3.5", "data_deviatoric :  3.5 40.0"))
+    q = rio.read_config(tmp_path / "config")
+    assert q.mat_model.tolist() == [2] and np.allclose(q.mat_data, [[3.5, 40.0, 0, 0]])
+    (tmp_path / "config").write_text(CONFIG.replace("Matl_NeoHookean", "Matl_Gent"))
+    with pytest.raises(ValueError):
+        rio.read_config(tmp_path / "config")                     # Gent needs mu and Im
