@@ -319,6 +319,28 @@ int mphy_newton_run(mphy_solver* s, const double* fext_host, const mphy_newton_o
                     double* disp_host, mphy_iter_stats* hist_host, int32_t max_hist,
                     int32_t* n_hist);
 
+/* ---- arc-length continuation: femSolidmechanics::solveWithArclength (femSolidmechanics2.cpp:855-1039)
+ * with SolverPetsc::solveArclengthSystem (SolverPetsc.cpp:671-757), psi = 1.
+ * opts: dt = the first step's load factor (loadFactor = myTime.dt) and the time increment of every
+ * attempt; t_final; max_steps = converged steps; max_newton = iterationsMax (iterations
+ * 1..max_newton-1 per step, the reference's bound); converged when ||R|| < max(tol_abs,
+ * tol_rel ||R||_first of the step) (the reference: tol_abs = tolerance, tol_rel = 0).
+ * Per iteration: assemble, R += lambda F, then two solves on the one assembled K (x1 = K^-1 R,
+ * x2 = K^-1 F; the preconditioner is set up once), dl from the linearised spherical constraint
+ * (Du.Du + Dl^2 F.F = Ds^2; dl = 0 in the first step, a Newton solve at lambda = dt), disp +=
+ * x1 + dl x2, lambda += dl. Steps after the first start from the extrapolation of the two last
+ * converged steps. Ds after the first step is sqrt(Du.Du + lambda^2 F.F), bounded to
+ * [Ds/1024, Ds]; doubled after two converged steps in a row; halved on a failure after a
+ * converged step, quartered after a failed one.
+ * fext_host, disp_host (in/out): [3*n_node]. step_lambda_host: load factor of each converged
+ * step [max_steps_out]; hist_host / hist_lambda_host: one row and the load factor after the
+ * update per iteration [max_hist] (either may be NULL). Returns MPHY_ERR_NOT_CONVERGED when the
+ * first step does not converge (the reference would go on with an unset arc length). */
+int mphy_arclength_run(mphy_solver* s, const double* fext_host, const mphy_newton_opts* opts,
+                       double* disp_host, double* step_lambda_host, int32_t max_steps_out,
+                       int32_t* n_steps, mphy_iter_stats* hist_host, double* hist_lambda_host,
+                       int32_t max_hist, int32_t* n_hist);
+
 /* ------------------------------------------------------------------ batched form
  * Many independent problems as one block-diagonal union mesh: instance i owns the contiguous
  * nodes [node_ptr[i], node_ptr[i+1]) and only elements among them. The solver s (Jacobi-PCG,

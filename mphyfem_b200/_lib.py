@@ -133,6 +133,8 @@ SIGNATURES = {
     "mphy_newton_iteration": (C.c_int, [_vp, _vp, _vp, C.c_double, C.c_double, C.POINTER(IterStats)]),
     "mphy_newton_iteration_host": (C.c_int, [_vp, _d, _d, C.c_double, C.c_double, C.POINTER(IterStats)]),
     "mphy_newton_run": (C.c_int, [_vp, _d, C.POINTER(NewtonOpts), _d, C.POINTER(IterStats), C.c_int32, _i32]),
+    "mphy_arclength_run": (C.c_int, [_vp, _d, C.POINTER(NewtonOpts), _d, _d, C.c_int32, _i32, C.POINTER(IterStats),
+                                     _d, C.c_int32, _i32]),
     "mphy_batch_create": (C.c_int, [_vp, C.c_int32, _i32, C.POINTER(_vp)]),
     "mphy_batch_destroy": (C.c_int, [_vp]),
     "mphy_batch_set_schedule": (C.c_int, [_vp, C.c_int32, C.c_int32]),

@@ -371,6 +371,43 @@ class FemSolidmechanicsGpu:
                          for h in hist[:n.value]], dtype=np.float64).reshape(-1, 7)
         return NewtonResult(disp=u, hist=rows, status=rc)
 
+    def solveWithArclength(self, max_newton: int = 10, tol_rel: float = 0.0, tol_abs: float | None = None,  # noqa: N802
+                           disp: np.ndarray | None = None, max_hist: int = 4096) -> "ArclengthResult":
+        """Arc-length continuation (femSolidmechanics2.cpp:855-1039): see solve_with_arclength."""
+        return solve_with_arclength(self, max_newton, tol_rel, tol_abs, disp, max_hist)
+
+
+@dataclass
+class ArclengthResult:
+    disp: np.ndarray
+    load_factors: np.ndarray  # load factor of each converged step
+    hist: np.ndarray  # rows (step, iter, ||R||, krylov its of both solves, status, load factor after the update)
+    status: int
+
+
+def solve_with_arclength(fem: "FemSolidmechanicsGpu", max_newton: int = 10, tol_rel: float = 0.0,
+                         tol_abs: float | None = None, disp: np.ndarray | None = None,
+                         max_hist: int = 4096) -> ArclengthResult:
+    """femSolidmechanics::solveWithArclength (mphy_arclength_run) on fem's solver. The first
+    step is a Newton solve at load factor prob.dt; max_newton is iterationsMax (iterations
+    1..max_newton-1); tol_abs defaults to the config's tolerance (0 when absent)."""
+    p = fem.prob
+    tol_abs = float(p.meta.get("tolerance", 0.0)) if tol_abs is None else tol_abs
+    o = L.NewtonOpts(p.dt, p.t_final, p.max_steps, max_newton, tol_rel, tol_abs)
+    u = np.zeros(p.n_dof) if disp is None else np.array(disp, np.float64)
+    f = _np(p.fnodal, np.float64)
+    lam = np.zeros(max(1, p.max_steps))
+    hl = np.zeros(max_hist)
+    hist = (L.IterStats * max_hist)()
+    nl, n = C.c_int32(0), C.c_int32(0)
+    rc = fem.ctx.lib.mphy_arclength_run(fem.solver.h, f.ctypes.data_as(L._d), C.byref(o), u.ctypes.data_as(L._d),
+                                        lam.ctypes.data_as(L._d), len(lam), C.byref(nl), hist,
+                                        hl.ctypes.data_as(L._d), max_hist, C.byref(n))
+    L.check(rc, allow=(L.ERR_NOT_CONVERGED,))
+    rows = np.array([[h.step, h.iter, h.rhs_norm, h.krylov_its, h.status, hl[k]]
+                     for k, h in enumerate(hist[:n.value])], dtype=np.float64).reshape(-1, 6)
+    return ArclengthResult(disp=u, load_factors=lam[:min(nl.value, len(lam))], hist=rows, status=rc)
+
 
 class BatchGpu:
     """The batched form: independent problems as one block-diagonal union (meshgen.batch_union),

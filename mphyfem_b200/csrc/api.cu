@@ -144,8 +144,12 @@ int solver_solve(mphy_solver* s, int32_t* its, double* fnorm) {
 int solver_solve_once(mphy_solver* s, int32_t* its, double* fnorm) {
     MPHY_REQUIRE(s->state == MPHY_ASSEMBLY_OK || s->state == MPHY_FACTORISE_OK, MPHY_ERR_STATE,
                  "factoriseAndSolve: assemble matrix first");
+    // The preconditioner follows the operator (KSPSetReusePreconditioner false): it is built by
+    // the first solve after an assembly and reused by further solves with the same matrix
+    // (PETSc's PCSetUp runs only when the operator has changed).
+    const bool setup = s->state == MPHY_ASSEMBLY_OK;
     s->state = MPHY_FACTORISE_OK;
-    if (s->use_fsai && s->opts.pc_type == MPHY_PC_FSAI) {
+    if (setup && s->use_fsai && s->opts.pc_type == MPHY_PC_FSAI) {
         // the preconditioner follows the operator: rebuilt for every solve (KSPSetReusePreconditioner false)
         MPHY_CUDA(cudaEventRecord(s->ctx->ev0, s->ctx->stream));
         if (s->mixed) s->fsai.compute<float>(s->valf.p, s->diag64.p, s->mesh->fixed.p, s->ctx->stream);
@@ -157,13 +161,13 @@ int solver_solve_once(mphy_solver* s, int32_t* its, double* fnorm) {
         s->t_pc_ms = ms;
         s->launches += s->fsai.launches;
     }
-    if (s->use_fsai && s->opts.pc_type == MPHY_PC_FSAI_LEARNED && s->gnn) {
+    if (setup && s->use_fsai && s->opts.pc_type == MPHY_PC_FSAI_LEARNED && s->gnn) {
         float ms = 0.f;
         const int rc = mphy_gnn_predict(s->gnn, s, &ms);
         MPHY_REQUIRE(rc == MPHY_OK, rc, "learned preconditioner: prediction failed");
         s->t_pc_ms = ms;
     }
-    if (s->use_coarse) {
+    if (setup && s->use_coarse) {
         // the coarse operator follows the assembled matrix
         if (s->mixed) s->coarse.setup<float>(s->A, s->valf.p, nullptr, s->ctx->stream);
         else s->coarse.setup<double>(s->A, s->val.p, nullptr, s->ctx->stream);
@@ -1028,6 +1032,155 @@ int mphy_newton_run(mphy_solver* s, const double* fext_host, const mphy_newton_o
     });
 }
 
+
+int mphy_arclength_run(mphy_solver* s, const double* fext_host, const mphy_newton_opts* o, double* disp_host,
+                       double* step_lambda, int32_t max_steps_out, int32_t* n_steps, mphy_iter_stats* hist,
+                       double* hist_lambda, int32_t max_hist, int32_t* n_hist) {
+    return guarded([&] {
+        MPHY_REQUIRE(s && fext_host && o && disp_host, MPHY_ERR_INVALID_ARG, "null argument");
+        MPHY_REQUIRE(o->dt > 0.0 && o->max_newton >= 2, MPHY_ERR_INVALID_ARG,
+                     "arc-length needs dt > 0 and max_newton >= 2 (iterations 1..max_newton-1)");
+        const size_t nd = 3 * (size_t)s->mesh->n_node;
+        const int64_t n = (int64_t)nd;
+        cudaStream_t st = s->ctx->stream;
+        const int sm = s->ctx->sm_count;
+        for (DevBuf<double>* b : {&s->disp_tmp, &s->fext_tmp, &s->disp_prev, &s->disp_prev2, &s->du_full, &s->x_first})
+            if (!b->p) b->alloc(nd);
+        if (!s->arc_dots.p) s->arc_dots.alloc(4);
+        double* disp = s->disp_tmp.p;
+        s->disp_tmp.upload(disp_host, nd, st);
+        s->fext_tmp.upload(fext_host, nd, st);
+        MPHY_CUDA(cudaMemcpyAsync(s->disp_prev.p, disp, nd * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        MPHY_CUDA(cudaMemcpyAsync(s->disp_prev2.p, disp, nd * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        double h[4];
+        // F.F over every DOF (the full Fext of SolverPetsc.cpp:674)
+        dot_fp64(s->fext_tmp.p, s->fext_tmp.p, n, s->partials.p, s->counter.p, s->arc_dots.p, st, sm);
+        s->arc_dots.download(h, 1, st);
+        MPHY_CUDA(cudaStreamSynchronize(st));
+        const double FtF = h[0];
+        double t = 0.0;
+        double lam = o->dt, lam_prev = 0.0, lam_prev2 = 0.0;  // femBase.cpp:65; loadFactor = myTime.dt
+        double ds = 0.0, ds_prev = 0.0, ds_max = 0.0, ds_min = 0.0;
+        bool conv = false, conv_prev = false;
+        int steps_done = 1, rows = 0, nl = 0, rc = MPHY_OK;
+        while (t <= o->t_final - 1.0e-10 && steps_done <= o->max_steps) {
+            t += o->dt;  // timeUpdate: myTime.update
+            conv_prev = conv;
+            conv = false;
+            if (steps_done > 1) {
+                // disp = (1 + f) dispPrev - f dispPrev2, lambda likewise, f = Ds / Ds_prev
+                const double f = ds / ds_prev;
+                MPHY_CUDA(cudaMemcpyAsync(disp, s->disp_prev.p, nd * sizeof(double), cudaMemcpyDeviceToDevice, st));
+                axpy_inplace(disp, s->disp_prev.p, f, n, st, sm);
+                axpy_inplace(disp, s->disp_prev2.p, -f, n, st, sm);
+                lam = (1.0 + f) * lam_prev - f * lam_prev2;
+            }
+            // DuFull = disp - dispPrev
+            MPHY_CUDA(cudaMemcpyAsync(s->du_full.p, disp, nd * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            axpy_inplace(s->du_full.p, s->disp_prev.p, -1.0, n, st, sm);
+            double dlam = lam - lam_prev;
+            double norm = -1.0, tol = o->tol_abs;
+            for (int iter = 1; iter < o->max_newton; ++iter) {
+                mphy_iter_stats is{};
+                const int64_t l0 = s->launches;
+                MPHY_CUDA(cudaEventRecord(s->ctx->ev0, st));
+                solver_assemble(s, disp);
+                add_scaled_free(s->mesh->fixed.p, s->fext_tmp.p, lam, s->rhs.p, n, st, sm);
+                MPHY_CUDA(cudaEventRecord(s->ctx->ev1, st));
+                int64_t bad = -1;
+                norm = solver_norm_and_bad(s, &bad);
+                is.t_assembly_ms = elapsed_ms(s->ctx);
+                if (bad >= 0) break;  // the element throws; the iteration loop ends
+                if (iter == 1) tol = std::fmax(o->tol_abs, o->tol_rel * norm);
+                const bool done = norm < tol;
+                if (!done) {
+                    // SolverPetsc::solveArclengthSystem: x1 = K^-1 R (du2 = -x1), x2 = K^-1 F on one
+                    // assembled K, dl from the linearised spherical constraint, soln = x1 + dl x2
+                    MPHY_CUDA(cudaEventRecord(s->ctx->ev0, st));
+                    int32_t its1 = 0, its2 = 0;
+                    double fn = 0.0;
+                    const int st1 = solver_solve(s, &its1, &fn);
+                    MPHY_CUDA(cudaMemcpyAsync(s->x_first.p, s->x.p, nd * sizeof(double), cudaMemcpyDeviceToDevice, st));
+                    MPHY_CUDA(cudaMemsetAsync(s->rhs.p, 0, nd * sizeof(double), st));
+                    add_scaled_free(s->mesh->fixed.p, s->fext_tmp.p, 1.0, s->rhs.p, n, st, sm);
+                    const int st2 = solver_solve(s, &its2, &fn);
+                    double A = 0.0, b = 1.0, adu2 = 0.0, adu1 = 0.0;
+                    if (steps_done > 1) {
+                        dot_fp64(s->du_full.p, s->du_full.p, n, s->partials.p, s->counter.p, s->arc_dots.p, st, sm);
+                        dot_fp64(s->du_full.p, s->x_first.p, n, s->partials.p, s->counter.p, s->arc_dots.p + 1, st, sm);
+                        dot_fp64(s->du_full.p, s->x.p, n, s->partials.p, s->counter.p, s->arc_dots.p + 2, st, sm);
+                        s->launches += 3;
+                        s->arc_dots.download(h, 3, st);
+                        MPHY_CUDA(cudaStreamSynchronize(st));
+                        A = h[0] + dlam * dlam * FtF - ds * ds;
+                        b = 2.0 * dlam * FtF;
+                        adu2 = -2.0 * h[1];
+                        adu1 = 2.0 * h[2];
+                    }
+                    const double dl = (adu2 - A) / (b + adu1);
+                    axpy_inplace(disp, s->x_first.p, 1.0, n, st, sm);
+                    axpy_inplace(disp, s->x.p, dl, n, st, sm);
+                    axpy_inplace(s->du_full.p, s->x_first.p, 1.0, n, st, sm);
+                    axpy_inplace(s->du_full.p, s->x.p, dl, n, st, sm);
+                    s->launches += 4;
+                    lam += dl;
+                    dlam += dl;
+                    MPHY_CUDA(cudaEventRecord(s->ctx->ev1, st));
+                    MPHY_CUDA(cudaEventSynchronize(s->ctx->ev1));
+                    is.t_solve_ms = elapsed_ms(s->ctx);
+                    is.krylov_its = its1 + its2;
+                    is.status = st1 != MPHY_OK ? st1 : st2;
+                }
+                is.step = steps_done;
+                is.iter = iter;
+                is.rhs_norm = norm;
+                is.kernel_launches = s->launches - l0;
+                if (rows < max_hist) {
+                    if (hist) hist[rows] = is;
+                    if (hist_lambda) hist_lambda[rows] = lam;
+                    ++rows;
+                }
+                if (done) {
+                    conv = true;
+                    break;
+                }
+            }
+            if (conv) {
+                if (steps_done == 1) {
+                    dot_fp64(s->du_full.p, s->du_full.p, n, s->partials.p, s->counter.p, s->arc_dots.p, st, sm);
+                    s->arc_dots.download(h, 1, st);
+                    MPHY_CUDA(cudaStreamSynchronize(st));
+                    ds = std::sqrt(h[0] + lam * lam * FtF);
+                    ds_max = ds;
+                    ds_min = ds / 1024.0;
+                }
+                lam_prev2 = lam_prev;
+                lam_prev = lam;
+                MPHY_CUDA(cudaMemcpyAsync(s->disp_prev2.p, s->disp_prev.p, nd * sizeof(double),
+                                          cudaMemcpyDeviceToDevice, st));
+                MPHY_CUDA(cudaMemcpyAsync(s->disp_prev.p, disp, nd * sizeof(double), cudaMemcpyDeviceToDevice, st));
+                ds_prev = ds;
+                if (conv_prev) ds = std::fmin(std::fmax(2.0 * ds, ds_min), ds_max);
+                if (step_lambda && nl < max_steps_out) step_lambda[nl] = lam;
+                ++nl;
+                ++steps_done;
+            } else {
+                if (steps_done == 1) {
+                    // the reference reads its arc length before the first step sets it
+                    rc = MPHY_ERR_NOT_CONVERGED;
+                    set_error("arc-length: the first step (a Newton solve at lambda = dt) did not converge");
+                    break;
+                }
+                ds = std::fmax(ds * (conv_prev ? 0.5 : 0.25), ds_min);
+            }
+        }
+        s->disp_tmp.download(disp_host, nd, st);
+        MPHY_CUDA(cudaStreamSynchronize(st));
+        if (n_hist) *n_hist = rows;
+        if (n_steps) *n_steps = nl;
+        return rc;
+    });
+}
 
 // ------------------------------------------------------------------------------- learned FSAI
 int mphy_gnn_param_count(void) { return GnnLayout::total; }

@@ -52,6 +52,7 @@ struct mphy_solver {
     DevBuf<double> partials, scalar;
     DevBuf<uint32_t> counter;
     DevBuf<double> disp_tmp, fext_tmp, disp_prev;
+    DevBuf<double> disp_prev2, du_full, x_first, arc_dots;  // arc-length continuation
     DevBuf<double> ref_r, ref_d;          // FP64 refinement sweeps (max_outer > 1), true residual
     DevBuf<float> pred_blocks;            // network-predicted G blocks (learned FSAI)
     PcgFp64 pcg;

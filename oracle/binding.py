@@ -73,6 +73,8 @@ def lib():
         L.orc_cg_jacobi_norm.argtypes = [C.c_void_p, _d, _d, _d, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int,
                                          C.POINTER(C.c_int), _d]
         L.orc_newton_run.argtypes = [C.c_void_p, _d, C.POINTER(NewtonOpts), _d, _d, C.c_int]
+        L.orc_arclength_run.argtypes = [C.c_void_p, _d, C.POINTER(NewtonOpts), _d, _d, C.c_int,
+                                        C.POINTER(C.c_int), _d, C.c_int]
         _lib = L
     return _lib
 
@@ -218,3 +220,22 @@ class OracleProblem:
         if rows < 0:
             raise RuntimeError("oracle Newton: time step size fell below 1% of the initial value")
         return u, hist[:rows]
+
+    def arclength(self, tol_rel=0.0, tol_abs=None, cg_rtol=None, cg_maxit=10000, max_newton=10, nthreads=1,
+                  disp=None, max_hist=4096):
+        """solveWithArclength: (disp, load factors of the converged steps, history rows
+        [step, iter, ||R||, CG its of both solves, load factor])."""
+        p = self.prob
+        o = NewtonOpts(p.dt, p.t_final, p.max_steps, max_newton, tol_rel,
+                       p.meta.get("tolerance", 0.0) if tol_abs is None else tol_abs,
+                       p.cg_rtol if cg_rtol is None else cg_rtol, cg_maxit, nthreads)
+        u = np.zeros(p.n_dof) if disp is None else np.array(disp, np.float64)
+        f = np.ascontiguousarray(p.fnodal, np.float64)
+        lam = np.zeros(max(1, p.max_steps))
+        nl = C.c_int(0)
+        hist = np.zeros((max_hist, 5))
+        rows = lib().orc_arclength_run(self.h, _p(f, _d), C.byref(o), _p(u, _d), _p(lam, _d), len(lam), C.byref(nl),
+                                       _p(hist, _d), max_hist)
+        if rows < 0:
+            raise RuntimeError("oracle arc-length: the first step did not converge")
+        return u, lam[:min(nl.value, len(lam))], hist[:rows]

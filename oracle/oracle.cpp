@@ -872,4 +872,122 @@ int orc_newton_run(const orc_problem* p, const double* fnodal, const orc_newton_
     return rows;
 }
 
+// femSolidmechanics::solveWithArclength (femSolidmechanics2.cpp:855-1039) with
+// SolverPetsc::solveArclengthSystem (SolverPetsc.cpp:671-757), psi = 1, static scheme.
+// Per step: extrapolate disp and the load factor from the two last converged steps (after the
+// first), then iterations 1..max_newton-1 of: assemble, R += lambda F, stop when ||R|| < tol;
+// du2 = -K^{-1} R, du1 = K^{-1} F, dl = (a.du2 - A) / (b + a.du1) with the spherical constraint
+// (A = Du.Du + Dl^2 F.F - Ds^2, a = 2 Du, b = 2 Dl F.F; step 1: A = 0, a = 0, b = 1, so dl = 0),
+// disp += -du2 + dl du1, lambda += dl. F.F runs over every DOF (the full Fext), Du over the free
+// ones. Arc length after step 1: Ds = sqrt(Du.Du + lambda^2 F.F), its bounds [Ds/1024, Ds];
+// doubled after two converged steps in a row, halved (quartered after a failure) on failure.
+// Returns the history rows, or -1 when the first step does not converge (the reference then
+// reads its arc length before setting it).
+int orc_arclength_run(const orc_problem* p, const double* fnodal, const orc_newton_opts* o, double* disp,
+                      double* lambdas, int max_lambdas, int* n_lambdas, double* hist, int max_hist) {
+    const CsrPattern& P = p->pat;
+    const int n = P.n_free;
+    const size_t nd = 3 * (size_t)p->n_node;
+    std::vector<double> val(P.rowptr.back()), rhs(n), fshort(n), du1(n), x1(n), du_full(nd, 0.0);
+    std::vector<double> disp_prev(disp, disp + nd), disp_prev2(disp, disp + nd);
+    double FtF = 0.0;
+    for (size_t i = 0; i < nd; ++i) FtF += fnodal[i] * fnodal[i];
+    for (int i = 0; i < n; ++i) fshort[i] = fnodal[P.assy_for_soln[i]];
+    auto dot_free = [&](const std::vector<double>& a_full, const std::vector<double>& b) {
+        double s = 0.0;
+        for (int i = 0; i < n; ++i) s += a_full[P.assy_for_soln[i]] * b[i];
+        return s;
+    };
+    double t = 0.0;
+    double lam = o->dt, lam_prev = 0.0, lam_prev2 = 0.0;
+    double ds = 0.0, ds_prev = 0.0, ds_max = 0.0, ds_min = 0.0;
+    bool conv = false, conv_prev = false;
+    int steps_done = 1, rows = 0, nl = 0;
+    while (t <= o->t_final - 1.0e-10 && steps_done <= o->max_steps) {
+        t += o->dt;  // timeUpdate: myTime.update
+        conv_prev = conv;
+        conv = false;
+        if (steps_done > 1) {
+            const double f = ds / ds_prev;
+            for (size_t i = 0; i < nd; ++i) disp[i] = (1.0 + f) * disp_prev[i] - f * disp_prev2[i];
+            lam = (1.0 + f) * lam_prev - f * lam_prev2;
+        }
+        for (size_t i = 0; i < nd; ++i) du_full[i] = disp[i] - disp_prev[i];
+        double dlam = lam - lam_prev;
+        double norm = -1.0, tol = o->tol_abs;
+        for (int iter = 1; iter < o->max_newton; ++iter) {
+            const int64_t bad = orc_problem_assemble(p, disp, val.data(), rhs.data(), nullptr, o->nthreads);
+            if (bad >= 0) break;  // the element throws; the iteration loop ends
+            for (int i = 0; i < n; ++i) rhs[i] += lam * fshort[i];
+            double s2 = 0.0;
+            for (int i = 0; i < n; ++i) s2 += rhs[i] * rhs[i];
+            norm = std::sqrt(s2);
+            if (iter == 1) tol = std::max(o->tol_abs, o->tol_rel * norm);
+            int its1 = 0, its2 = 0;
+            const bool done = norm < tol;
+            if (!done) {
+                double A = 0.0, b = 1.0, adu2 = 0.0, adu1 = 0.0, fn = 0.0;
+                orc_cg_jacobi(p, val.data(), rhs.data(), x1.data(), o->cg_rtol, 1.0e-50, o->cg_maxit, o->nthreads,
+                              &its1, &fn);  // du2 = -x1
+                orc_cg_jacobi(p, val.data(), fshort.data(), du1.data(), o->cg_rtol, 1.0e-50, o->cg_maxit,
+                              o->nthreads, &its2, &fn);
+                if (steps_done > 1) {
+                    double dd = 0.0;
+                    for (int i = 0; i < n; ++i) dd += du_full[P.assy_for_soln[i]] * du_full[P.assy_for_soln[i]];
+                    A = dd + dlam * dlam * FtF - ds * ds;
+                    b = 2.0 * dlam * FtF;
+                    adu2 = -2.0 * dot_free(du_full, x1);
+                    adu1 = 2.0 * dot_free(du_full, du1);
+                }
+                const double dl = (adu2 - A) / (b + adu1);
+                for (int i = 0; i < n; ++i) {
+                    const double d = x1[i] + dl * du1[i];
+                    disp[P.assy_for_soln[i]] += d;
+                    du_full[P.assy_for_soln[i]] += d;
+                }
+                lam += dl;
+                dlam += dl;
+            }
+            if (rows < max_hist && hist) {
+                hist[5 * rows + 0] = steps_done;
+                hist[5 * rows + 1] = iter;
+                hist[5 * rows + 2] = norm;
+                hist[5 * rows + 3] = its1 + its2;
+                hist[5 * rows + 4] = lam;
+                ++rows;
+            }
+            if (done) {
+                conv = true;
+                break;
+            }
+        }
+        if (conv) {
+            if (steps_done == 1) {
+                double dd = 0.0;
+                for (size_t i = 0; i < nd; ++i) dd += du_full[i] * du_full[i];
+                ds = std::sqrt(dd + lam * lam * FtF);
+                ds_max = ds;
+                ds_min = ds / 1024.0;
+            }
+            lam_prev2 = lam_prev;
+            lam_prev = lam;
+            disp_prev2 = disp_prev;
+            std::copy(disp, disp + nd, disp_prev.begin());
+            ds_prev = ds;
+            if (conv_prev) ds = std::min(std::max(2.0 * ds, ds_min), ds_max);
+            if (nl < max_lambdas && lambdas) lambdas[nl] = lam;
+            ++nl;
+            ++steps_done;
+        } else {
+            if (steps_done == 1) {
+                if (n_lambdas) *n_lambdas = nl;
+                return -1;
+            }
+            ds = std::max(ds * (conv_prev ? 0.5 : 0.25), ds_min);
+        }
+    }
+    if (n_lambdas) *n_lambdas = nl;
+    return rows;
+}
+
 }  // extern "C"

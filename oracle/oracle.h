@@ -142,6 +142,17 @@ typedef struct {
 int orc_newton_run(const orc_problem* p, const double* fnodal, const orc_newton_opts* opts,
                    double* disp, double* hist, int max_hist);
 
+/* Arc-length continuation: femSolidmechanics::solveWithArclength (femSolidmechanics2.cpp:855-1039)
+ * with SolverPetsc::solveArclengthSystem (SolverPetsc.cpp:671-757). opts: dt = the first load
+ * factor and the time increment of every attempt, t_final, max_steps (converged steps),
+ * max_newton = iterationsMax (iterations 1..max_newton-1), tol_abs / tol_rel as in
+ * orc_newton_run. disp: [3*n_node] in/out. lambdas: load factor of each converged step.
+ * hist rows: step, iter, ||R||, CG iterations of both solves, load factor after the update.
+ * Returns the number of rows, or -1 when the first step does not converge. */
+int orc_arclength_run(const orc_problem* p, const double* fnodal, const orc_newton_opts* opts,
+                      double* disp, double* lambdas, int max_lambdas, int* n_lambdas, double* hist,
+                      int max_hist);
+
 #ifdef __cplusplus
 }
 #endif
