@@ -57,6 +57,10 @@ def lib():
         L.orc_material_stress_tangent.argtypes = [C.c_int, _d, C.c_double, C.c_int, _d, _d, _d]
         L.orc_elem_stiffness_residual_mat.argtypes = [C.c_int, _d, _d, C.c_int, _d, C.c_double, C.c_int, _d, _d]
         L.orc_problem_set_materials.argtypes = [C.c_void_p, C.c_int, _i32, _d]
+        L.orc_material_stress_tangent_mixed.argtypes = [C.c_int, _d, C.c_double, C.c_int, _d, C.c_double, _d, _d]
+        L.orc_mixed_constants.argtypes = [C.c_int, C.c_double, C.c_double, _d, _d]
+        L.orc_elem_mixed.argtypes = [C.c_int, _d, _d, _d, _d, C.c_int, _d, C.c_double, C.c_int, _d, _d, _d, _d,
+                                     _d, _d]
         L.orc_problem_create.argtypes = [C.c_int, _d, C.c_int, C.c_int, _i32, _i32, C.c_int, _d, _u8]
         L.orc_problem_create.restype = C.c_void_p
         L.orc_problem_destroy.argtypes = [C.c_void_p]
@@ -137,6 +141,30 @@ def elem_stiffness_residual_mat(X, u, model, data, Kinv, utype=3):
     bad = lib().orc_elem_stiffness_residual_mat(npe, _p(X, _d), _p(u, _d), int(model), _p(d, _d), Kinv, utype,
                                                 _p(K, _d), _p(R, _d))
     return K, R, bad
+
+
+def material_stress_tangent_mixed(model, data, F, Kinv, pres, utype=3):
+    """Mixed (u-p) branch: the pressure replaces U'(J) in the stress and tangent."""
+    F = np.ascontiguousarray(F, dtype=np.float64).reshape(9)
+    d = _mat_data(data)
+    s, Cm = np.zeros(9), np.zeros(81)
+    if lib().orc_material_stress_tangent_mixed(int(model), _p(d, _d), Kinv, utype, _p(F, _d), pres, _p(s, _d),
+                                               _p(Cm, _d)):
+        raise ValueError(f"oracle: unknown material model {model}")
+    return s, Cm.reshape(9, 9)
+
+
+def elem_mixed(X, u, u_prev, pn, model, data, Kinv, utype=3):
+    """Mixed u-p tet10 element (linear vertex pressure): Kuu, Kup, Kpu, Kpp, FU, FP, bad."""
+    X, u, up, pn = (np.ascontiguousarray(a, dtype=np.float64) for a in (X, u, u_prev, pn))
+    d = _mat_data(data)
+    Kuu, Kup, Kpu, Kpp = np.zeros((30, 30)), np.zeros((30, 4)), np.zeros((4, 30)), np.zeros((4, 4))
+    FU, FP = np.zeros(30), np.zeros(4)
+    bad = lib().orc_elem_mixed(X.shape[0], _p(X, _d), _p(u, _d), _p(up, _d), _p(pn, _d), int(model), _p(d, _d), Kinv,
+                               utype, _p(Kuu, _d), _p(Kup, _d), _p(Kpu, _d), _p(Kpp, _d), _p(FU, _d), _p(FP, _d))
+    if bad == 2:
+        raise ValueError("oracle: the mixed element is tet10 only")
+    return Kuu, Kup, Kpu, Kpp, FU, FP, bad
 
 
 def gauss_rule(npe):

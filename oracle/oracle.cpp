@@ -218,8 +218,10 @@ double orc_vol_d2U(int type, double K, double J) {
 //   C_{ijkl} = (mu J^{-5/3} Ib/3) d_il d_jk - (2/3) mu J^{-5/3} (b_ij d_kl + d_ij b_kl)
 //            + (2/9) mu J^{-5/3} Ib d_ij d_kl + mu J^{-5/3} b_jl d_ik
 //            + (J U'' + U') d_ij d_kl - U' d_il d_jk - U' d_jl d_ik
-int orc_nh_stress_tangent(const double* Fm, double mu, double Kinv, int Utype, double* stre,
-                          double* C) {
+// Mixed (u-p) branch, :218-221 and :275-281: the pressure unknown p replaces U'(J) in the stress
+// and p (d_ij d_kl - d_jk d_il) replaces the volumetric tangent.
+static int nh_impl(const double* Fm, double mu, double Kinv, int Utype, bool mixed, double pres, double* stre,
+                   double* C) {
     const double K = 1.0 / Kinv;
     double F[3][3], b[3][3];
     for (int i = 0; i < 3; ++i)
@@ -234,7 +236,7 @@ int orc_nh_stress_tangent(const double* Fm, double mu, double Kinv, int Utype, d
     const double d2U = orc_vol_d2U(Utype, K, J);
 
     const double s1 = mu * Jm5d3;
-    const double s2 = -s1 * (1.0 / 3.0) * Ib + dU;
+    const double s2 = -s1 * (1.0 / 3.0) * Ib + (mixed ? pres : dU);
     for (int q = 0; q < 9; ++q) {
         const int i = kPairI[q], j = kPairJ[q];
         stre[q] = s1 * b[i][j] + (i == j ? s2 : 0.0);
@@ -254,12 +256,20 @@ int orc_nh_stress_tangent(const double* Fm, double mu, double Kinv, int Utype, d
             v += c_bdd * (b[i][j] * kd(k, l) + kd(i, j) * b[k][l]);
             v += c_dd * (kd(i, j) * kd(k, l));
             v += c_bjl * (b[j][l] * kd(i, k));
-            v += c_vol * (kd(i, j) * kd(k, l)) - dU * (kd(i, l) * kd(j, k)) - dU * (kd(j, l) * kd(i, k));
-            if (g_consistent_tangent) v += dU * (kd(j, l) * kd(i, k));
+            if (mixed) {
+                v += pres * (kd(i, j) * kd(k, l) - kd(j, k) * kd(i, l));
+            } else {
+                v += c_vol * (kd(i, j) * kd(k, l)) - dU * (kd(i, l) * kd(j, k)) - dU * (kd(j, l) * kd(i, k));
+                if (g_consistent_tangent) v += dU * (kd(j, l) * kd(i, k));
+            }
             C[9 * p + q] = v;
         }
     }
     return 0;
+}
+
+int orc_nh_stress_tangent(const double* Fm, double mu, double Kinv, int Utype, double* stre, double* C) {
+    return nh_impl(Fm, mu, Kinv, Utype, false, 0.0, stre, C);
 }
 
 namespace {
@@ -297,7 +307,8 @@ Kin kinematics(const double* Fm, double Kinv, int Utype) {
 // is J^{2/3} times an energy's stress, and its exact linearisation adds (2/3) sigma_c2 (x) I to
 // the tangent below: a non-symmetric term that a CG solve cannot take, so both tangent modes
 // give the symmetric tangent as written.
-void mooney_rivlin(const double* Fm, const double* data, double Kinv, int Utype, double* stre, double* C) {
+void mooney_rivlin(const double* Fm, const double* data, double Kinv, int Utype, bool mixed, double pres,
+                   double* stre, double* C) {
     const Kin k = kinematics(Fm, Kinv, Utype);
     const double c1 = data[0], c2 = data[1];
     const double Jm5d3 = std::pow(k.J, -2.0 / 3.0) / k.J;
@@ -305,7 +316,7 @@ void mooney_rivlin(const double* Fm, const double* data, double Kinv, int Utype,
     const double I1 = k.Ib;
     const double I2 = 0.5 * (I1 * I1 - (k.b2[0][0] + k.b2[1][1] + k.b2[2][2]));
     const double s1 = 2.0 * c1 * Jm5d3 + 2.0 * c2 * Jm7d3 * I1;
-    const double s2 = -c1 * (2.0 / 3.0) * Jm5d3 * I1 - c2 * (4.0 / 3.0) * Jm7d3 * I2 + k.dU;
+    const double s2 = -c1 * (2.0 / 3.0) * Jm5d3 * I1 - c2 * (4.0 / 3.0) * Jm7d3 * I2 + (mixed ? pres : k.dU);
     const double s3 = -2.0 * c2 * Jm7d3;
     for (int q = 0; q < 9; ++q) {
         const int i = kPairI[q], j = kPairJ[q];
@@ -326,14 +337,15 @@ void mooney_rivlin(const double* Fm, const double* data, double Kinv, int Utype,
                        dik * b2[j][l]);
             v += f3 * (I2 * dil * djk + (4.0 / 3.0) * I2 * dkl * dij + 2.0 * dij * b2[kk][l] + 2.0 * dkl * b2[i][j] -
                        2.0 * I1 * dkl * b[i][j] - 2.0 * I1 * dij * b[kk][l]);
-            v += f7 * (dij * dkl) + f8 * (dil * djk);
+            v += mixed ? pres * (dij * dkl - djk * dil) : f7 * (dij * dkl) + f8 * (dil * djk);
             C[9 * p + q] = v;
         }
     }
 }
 
 // Gent, utilitiesmaterialHyperelastic.cpp:423-548, compressible branch. data = {mu, Im}.
-void gent(const double* Fm, const double* data, double Kinv, int Utype, double* stre, double* C) {
+void gent(const double* Fm, const double* data, double Kinv, int Utype, bool mixed, double pres, double* stre,
+          double* C) {
     const Kin k = kinematics(Fm, Kinv, Utype);
     const double mu = data[0], Im = data[1];
     const double Jm2d3 = std::pow(k.J, -2.0 / 3.0);
@@ -341,7 +353,7 @@ void gent(const double* Fm, const double* data, double Kinv, int Utype, double* 
     const double Jm7d3 = std::pow(k.J, -7.0 / 3.0);
     const double gf = 1.0 / (1.0 - (Jm2d3 * k.Ib - 3.0) / Im);
     const double s1 = mu * Jm5d3 * gf;
-    const double s2 = -s1 * (1.0 / 3.0) * k.Ib + k.dU;
+    const double s2 = -s1 * (1.0 / 3.0) * k.Ib + (mixed ? pres : k.dU);
     for (int q = 0; q < 9; ++q) {
         const int i = kPairI[q], j = kPairJ[q];
         stre[q] = s1 * k.b[i][j] + (i == j ? s2 : 0.0);
@@ -358,7 +370,7 @@ void gent(const double* Fm, const double* data, double Kinv, int Utype, double* 
             double v = f1 * (bd[i][j] * dkl);
             v += f2 * (bd[i][j] * bd[kk][l]);
             v += f3 * (dik * b[j][l] - (2.0 / 3.0) * b[kk][l] * dij + (1.0 / 3.0) * k.Ib * dil * djk);
-            v += f7 * (dij * dkl) + f8 * (dil * djk);
+            v += mixed ? pres * (dij * dkl - djk * dil) : f7 * (dij * dkl) + f8 * (dil * djk);
             C[9 * p + q] = v;
         }
     }
@@ -366,7 +378,8 @@ void gent(const double* Fm, const double* data, double Kinv, int Utype, double* 
 
 // Arruda-Boyce (five-term inverse-Langevin series), utilitiesmaterialHyperelastic.cpp:551-677,
 // compressible branch. data = {mu, N}.
-void arruda_boyce(const double* Fm, const double* data, double Kinv, int Utype, double* stre, double* C) {
+void arruda_boyce(const double* Fm, const double* data, double Kinv, int Utype, bool mixed, double pres,
+                  double* stre, double* C) {
     const Kin k = kinematics(Fm, Kinv, Utype);
     const double mu = data[0], N = data[1];
     const double c1 = mu / 2.0, c2 = mu / 20.0 / N, c3 = mu * 11.0 / 1050.0 / N / N,
@@ -379,7 +392,7 @@ void arruda_boyce(const double* Fm, const double* data, double Kinv, int Utype, 
                       5.0 * c5 * Ibb * Ibb * Ibb * Ibb;
     const double a2 = 2.0 * c2 + 6.0 * c3 * Ibb + 12.0 * c4 * Ibb * Ibb + 20.0 * c5 * Ibb * Ibb * Ibb;
     const double s1 = 2.0 * a1 * Jm5d3;
-    const double s2 = -s1 * (1.0 / 3.0) * k.Ib + k.dU;
+    const double s2 = -s1 * (1.0 / 3.0) * k.Ib + (mixed ? pres : k.dU);
     for (int q = 0; q < 9; ++q) {
         const int i = kPairI[q], j = kPairJ[q];
         stre[q] = s1 * k.b[i][j] + (i == j ? s2 : 0.0);
@@ -399,7 +412,10 @@ void arruda_boyce(const double* Fm, const double* data, double Kinv, int Utype, 
             v += f2 * (b[i][j] * dkl + b[kk][l] * dij);
             v += f3 * (dik * djl + dil * djk);
             v += f4 * (dij * dkl);
-            v += f7 * (dij * dkl) + f8 * (dil * djk);
+            // mixed: the pressure term as written at :661-664 (with d_jl d_ik, which the
+            // consistent tangent drops); displacement form: the volumetric terms
+            if (mixed) v += pres * (dij * dkl - djk * dil - (g_consistent_tangent ? 0.0 : djl * dik));
+            else v += f7 * (dij * dkl) + f8 * (dil * djk);
             // The deviatoric part above is the symmetrised form "without stress terms" (:655-660):
             // it has (2/3) a1 J^{-5/3} Ib d_ik d_jl where the exact linearisation of the stress
             // has 2 a1 J^{-5/3} d_ik b_jl. The consistent tangent swaps them.
@@ -411,15 +427,25 @@ void arruda_boyce(const double* Fm, const double* data, double Kinv, int Utype, 
 
 }  // namespace
 
-int orc_material_stress_tangent(int model, const double* data, double Kinv, int Utype, const double* F,
-                                double* stre, double* C) {
+static int material_impl(int model, const double* data, double Kinv, int Utype, const double* F, bool mixed,
+                         double pres, double* stre, double* C) {
     switch (model) {
-        case ORC_MAT_NEOHOOKEAN: return orc_nh_stress_tangent(F, data[0], Kinv, Utype, stre, C);
-        case ORC_MAT_MOONEYRIVLIN: mooney_rivlin(F, data, Kinv, Utype, stre, C); return 0;
-        case ORC_MAT_GENT: gent(F, data, Kinv, Utype, stre, C); return 0;
-        case ORC_MAT_ARRUDABOYCE: arruda_boyce(F, data, Kinv, Utype, stre, C); return 0;
+        case ORC_MAT_NEOHOOKEAN: return nh_impl(F, data[0], Kinv, Utype, mixed, pres, stre, C);
+        case ORC_MAT_MOONEYRIVLIN: mooney_rivlin(F, data, Kinv, Utype, mixed, pres, stre, C); return 0;
+        case ORC_MAT_GENT: gent(F, data, Kinv, Utype, mixed, pres, stre, C); return 0;
+        case ORC_MAT_ARRUDABOYCE: arruda_boyce(F, data, Kinv, Utype, mixed, pres, stre, C); return 0;
         default: return 2;
     }
+}
+
+int orc_material_stress_tangent(int model, const double* data, double Kinv, int Utype, const double* F,
+                                double* stre, double* C) {
+    return material_impl(model, data, Kinv, Utype, F, false, 0.0, stre, C);
+}
+
+int orc_material_stress_tangent_mixed(int model, const double* data, double Kinv, int Utype, const double* F,
+                                      double pres, double* stre, double* C) {
+    return material_impl(model, data, Kinv, Utype, F, true, pres, stre, C);
 }
 
 void orc_set_consistent_tangent(int on) { g_consistent_tangent = on ? 1 : 0; }
@@ -672,6 +698,27 @@ int64_t orc_problem_elements(const orc_problem* p, const double* disp, double* K
     return first_bad == p->n_elem ? -1 : first_bad;
 }
 
+int64_t orc_problem_elements_mixed(const orc_problem* p, const double* disp, const double* disp_prev,
+                                   const double* pres, double* Kuu, double* Kup, double* Kpp, double* FU, double* FP,
+                                   int nthreads) {
+    if (p->npe != 10) return -2;
+    int64_t first_bad = p->n_elem;
+    set_threads(nthreads);
+#pragma omp parallel for schedule(static) reduction(min : first_bad) if (nthreads > 1)
+    for (int64_t e = 0; e < p->n_elem; ++e) {
+        double X[30], u[30], up[30], pn[4], Kpu[120];
+        gather_element(p, e, disp, X, u);
+        gather_element(p, e, disp_prev, X, up);
+        for (int i = 0; i < 4; ++i) pn[i] = pres[p->conn[e * 10 + i]];
+        const size_t id = (size_t)p->mat_id[e];
+        const double* m = &p->mats[3 * id];
+        const int bad = orc_elem_mixed(10, X, u, up, pn, p->model[id], &p->data[ORC_MAT_NDATA * id], m[1], (int)m[2],
+                                       Kuu + e * 900, Kup + e * 120, Kpu, Kpp + e * 16, FU + e * 30, FP + e * 4);
+        if (bad && e < first_bad) first_bad = e;
+    }
+    return first_bad == p->n_elem ? -1 : first_bad;
+}
+
 int64_t orc_problem_assemble(const orc_problem* p, const double* disp, double* val, double* rhs,
                              double* reac, int nthreads) {
     const CsrPattern& P = p->pat;
@@ -870,6 +917,99 @@ int orc_newton_run(const orc_problem* p, const double* fnodal, const orc_newton_
         }
     }
     return rows;
+}
+
+// compute_constants_volumetric_functions (utilitiesmaterialHyperelastic.cpp:144-173), finite
+// strain: Jhat = Jn - U'(Jn)/U''(Jn), thetahat = 1/U''(Jn) (Utype -1: 1 and 0).
+void orc_mixed_constants(int Utype, double Jn, double K, double* Jhat, double* thetahat) {
+    if (Utype == -1) {
+        *Jhat = 1.0;
+        *thetahat = 0.0;
+        return;
+    }
+    const double d1 = orc_vol_dU(Utype, K, Jn), d2 = orc_vol_d2U(Utype, K, Jn);
+    *Jhat = Jn - d1 / d2;
+    *thetahat = 1.0 / d2;
+}
+
+// ElementBase::calcStiffnessAndResidualMixed3D (ElementBase2.cpp:278-553) for
+// Elem_Solid_3D_Mixed1 with the tet10 displacement and the linear (vertex) pressure of
+// Elem_Solid_3D_Mixed1.cpp:55-75, STATIC scheme (af = 1, no inertia or body force). X, u, u_prev:
+// [10][3]; pn: the 4 vertex pressures. Kuu [30][30], Kup [30][4], Kpu [4][30], Kpp [4][4], FU [30],
+// FP [4], row-major. Returns 0, 1 when some Gauss point has det F < 0, 2 for npe != 10.
+int orc_elem_mixed(int npe, const double* X, const double* u, const double* u_prev, const double* pn, int model,
+                   const double* data, double Kinv, int Utype, double* Kuu, double* Kup, double* Kpu, double* Kpp,
+                   double* FU, double* FP) {
+    if (npe != 10) return 2;
+    constexpr int NP = 4, NS = 30;
+    GaussRule rule;
+    element_rule(npe, rule);
+    std::fill(Kuu, Kuu + NS * NS, 0.0);
+    std::fill(Kup, Kup + NS * NP, 0.0);
+    std::fill(Kpu, Kpu + NP * NS, 0.0);
+    std::fill(Kpp, Kpp + NP * NP, 0.0);
+    std::fill(FU, FU + NS, 0.0);
+    std::fill(FP, FP + NP, 0.0);
+    const double BULK = 1.0 / Kinv;
+    double x[3 * kMaxNpe];
+    for (int a = 0; a < 3 * npe; ++a) x[a] = X[a] + u[a];
+    int bad = 0;
+    for (int q = 0; q < rule.ngp; ++q) {
+        double N[kMaxNpe], dN[3][kMaxNpe], g0[3][kMaxNpe], g[3][kMaxNpe];
+        shape(npe, rule.xi[q], N, dN);
+        const double dvol0 = rule.w[q] * spatial_gradients(npe, X, dN, g0);
+        double F[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, Fn[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+        for (int I = 0; I < npe; ++I)
+            for (int a = 0; a < 3; ++a)
+                for (int m = 0; m < 3; ++m) {
+                    F[3 * a + m] += u[3 * I + a] * g0[m][I];
+                    Fn[3 * a + m] += u_prev[3 * I + a] * g0[m][I];
+                }
+        double Fa[3][3], Fna[3][3];
+        for (int i = 0; i < 9; ++i) {
+            Fa[i / 3][i % 3] = F[i];
+            Fna[i / 3][i % 3] = Fn[i];
+        }
+        double Jhat, thetahat;
+        orc_mixed_constants(Utype, det3(Fna), BULK, &Jhat, &thetahat);
+        const double J = det3(Fa);
+        if (J < 0.0) bad = 1;
+        const double dvol = rule.w[q] * spatial_gradients(npe, x, dN, g);
+        // LagrangeBasisFunsTetra(4): the barycentric coordinates, vertex order
+        const double* xi = rule.xi[q];
+        const double Np[NP] = {1.0 - xi[0] - xi[1] - xi[2], xi[0], xi[1], xi[2]};
+        double pres = 0.0;
+        for (int i = 0; i < NP; ++i) pres += Np[i] * pn[i];
+        double stre[9], C[81];
+        if (orc_material_stress_tangent_mixed(model, data, Kinv, Utype, F, pres, stre, C) != 0) return 2;
+        for (int I = 0; I < npe; ++I) {
+            const double bb[3] = {dvol * g[0][I], dvol * g[1][I], dvol * g[2][I]};
+            double Gc[3][9];
+            for (int kk = 0; kk < 9; ++kk)
+                for (int a = 0; a < 3; ++a)
+                    Gc[a][kk] = bb[0] * C[9 * a + kk] + bb[1] * C[9 * (3 + a) + kk] + bb[2] * C[9 * (6 + a) + kk];
+            for (int a = 0; a < 3; ++a)
+                FU[3 * I + a] -= bb[0] * stre[a] + bb[1] * stre[3 + a] + bb[2] * stre[6 + a];
+            for (int Jn = 0; Jn < npe; ++Jn) {
+                const double c[3] = {g[0][Jn], g[1][Jn], g[2][Jn]};
+                for (int a = 0; a < 3; ++a)
+                    for (int b = 0; b < 3; ++b)
+                        Kuu[(3 * I + a) * NS + 3 * Jn + b] +=
+                            Gc[a][b] * c[0] + Gc[a][3 + b] * c[1] + Gc[a][6 + b] * c[2];
+            }
+            for (int j = 0; j < NP; ++j)
+                for (int a = 0; a < 3; ++a) Kup[(3 * I + a) * NP + j] += bb[a] * Np[j];
+        }
+        const double resip = J - Jhat - thetahat * pres;
+        for (int i = 0; i < NP; ++i) {
+            const double b4 = dvol * Np[i];
+            FP[i] -= dvol0 * Np[i] * resip;
+            for (int Jn = 0; Jn < npe; ++Jn)
+                for (int b = 0; b < 3; ++b) Kpu[i * NS + 3 * Jn + b] += b4 * g[b][Jn];
+            for (int j = 0; j < NP; ++j) Kpp[i * NP + j] -= dvol0 * Np[i] * thetahat * Np[j];
+        }
+    }
+    return bad;
 }
 
 // femSolidmechanics::solveWithArclength (femSolidmechanics2.cpp:855-1039) with

@@ -49,6 +49,33 @@ enum { ORC_MAT_NDATA = 4 };
 int orc_material_stress_tangent(int model, const double* data, double Kinv, int Utype, const double* F,
                                 double* stre, double* Cmat);
 
+/* Mixed (u-p) branch of the same models: the pressure pres replaces U'(J) in the stress and the
+ * pressure term replaces the volumetric tangent (utilitiesmaterialHyperelastic.cpp, the
+ * MIXED_ELEMENT branches). Returns 0, or 2 for an unknown model. */
+int orc_material_stress_tangent_mixed(int model, const double* data, double Kinv, int Utype, const double* F,
+                                      double pres, double* stre, double* Cmat);
+
+/* compute_constants_volumetric_functions, finite strain (utilitiesmaterialHyperelastic.cpp:144-173). */
+void orc_mixed_constants(int Utype, double Jn, double K, double* Jhat, double* thetahat);
+
+/* Mixed u-p tet10 element with linear vertex pressure (Elem_Solid_3D_Mixed1 with npElem = 10,
+ * ElementBase::calcStiffnessAndResidualMixed3D, ElementBase2.cpp:278-553), STATIC scheme.
+ * X, u, u_prev (the last converged step's displacement, for Jn): [10][3]; pn: [4] vertex
+ * pressures. Kuu [30][30], Kup [30][4], Kpu [4][30], Kpp [4][4], FU [30], FP [4], row-major.
+ * Returns 0, 1 when some Gauss point has det F < 0, 2 for npe != 10 or an unknown model. */
+int orc_elem_mixed(int npe, const double* X, const double* u, const double* u_prev, const double* pn, int model,
+                   const double* data, double Kinv, int Utype, double* Kuu, double* Kup, double* Kpu, double* Kpp,
+                   double* FU, double* FP);
+
+/* ---- see orc_problem_create below: every element of a tet10 problem as a mixed u-p element.
+ * disp, disp_prev: [3*n_node]; pres: [n_node] nodal pressures (vertex nodes used). Outputs per
+ * element: Kuu [30][30], Kup [30][4] (Kpu = Kup^T), Kpp [4][4], FU [30], FP [4]. Returns the
+ * first element with det F < 0, -1, or -2 when the mesh is not tet10. */
+typedef struct orc_problem orc_problem;
+int64_t orc_problem_elements_mixed(const orc_problem* p, const double* disp, const double* disp_prev,
+                                   const double* pres, double* Kuu, double* Kup, double* Kpp, double* FU, double* FP,
+                                   int nthreads);
+
 /* Test-only switch: 0 (default) = the reference's tangent; 1 = add the volumetric geometric
  * term U'(J) d_ik d_jl that the reference omits, giving the consistent tangent -dR/du. */
 void orc_set_consistent_tangent(int on);
