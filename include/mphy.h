@@ -341,6 +341,56 @@ int mphy_arclength_run(mphy_solver* s, const double* fext_host, const mphy_newto
                        int32_t* n_steps, mphy_iter_stats* hist_host, double* hist_lambda_host,
                        int32_t max_hist, int32_t* n_hist);
 
+/* ---- mixed u-p elements: Elem_Solid_3D_Mixed1 with npElem = 10 (tet10 displacement, linear
+ * pressure on the vertex nodes), ElementBase::calcStiffnessAndResidualMixed3D
+ * (ElementBase2.cpp:278-553), STATIC scheme, every material model above through its mixed
+ * branch. Pressure DOFs: the vertex nodes in ascending node order (prepareDataForMixedElements,
+ * femSolidmechanics1.cpp:274-380), no prescribed pressures. The two-field vectors are
+ * [3 n_node displacements | n_pres pressures]; prescribed displacement rows and columns are
+ * left out of the coupling blocks and hold identity rows in Kuu (SolverPetsc.cpp:434-502 leaves
+ * them out of the matrix). The solve is preconditioned MINRES (the reference's sample inputs run
+ * MUMPS LU): relative tolerance rtol on the preconditioned residual, at most max_it iterations. */
+typedef struct mphy_mixed mphy_mixed;
+typedef struct mphy_mixed_opts {
+    int32_t tangent;  /* MPHY_TANGENT_* */
+    int32_t max_it;   /* MINRES iterations per solve */
+    double rtol;      /* MINRES relative tolerance */
+} mphy_mixed_opts;
+void mphy_mixed_opts_default(mphy_mixed_opts* opts); /* reference tangent, 20000, 1e-10 */
+/* mesh: tet10 (npe = 10); pattern: mphy_pattern_build of the same mesh. opts may be NULL. */
+int mphy_mixed_create(mphy_ctx* ctx, const mphy_mesh* mesh, const mphy_pattern* pattern,
+                      const mphy_mixed_opts* opts, mphy_mixed** out);
+int mphy_mixed_destroy(mphy_mixed* m);
+/* pressure DOF count; entries of the coupling block B = Kup (node rows) and of C = Kpp */
+int mphy_mixed_info(mphy_mixed* m, int32_t* n_pres, int64_t* nnz_coupling, int64_t* nnz_pp);
+/* the global node of each pressure DOF (assyForSolnPres) [n_pres], host */
+int mphy_mixed_pressure_nodes(mphy_mixed* m, int32_t* nodes_host);
+/* calcStiffnessAndResidualMixed for every element. Device arrays: disp, disp_prev (the last
+ * converged step, for Jn) [3 n_node], pres [n_node] nodal pressures (vertex nodes used);
+ * outputs Kuu [n_elem][30][30], FU [n_elem][30], Kup [n_elem][30][4] (Kpu = Kup^T),
+ * Kpp [n_elem][4][4], FP [n_elem][4]. MPHY_ERR_NEG_JACOBIAN as mphy_elem_eval. */
+int mphy_mixed_elem_eval(mphy_mixed* m, const double* disp_dev, const double* disp_prev_dev,
+                         const double* pres_dev, double* Kuu_dev, double* FU_dev, double* Kup_dev,
+                         double* Kpp_dev, double* FP_dev, int64_t* first_bad);
+/* femSolidmechanics::calcStiffnessAndResidual for a mixed mesh plus rhs_u += lambda fext_dev on
+ * the free DOFs (fext_dev may be NULL); *rhs_norm = ||rhs|| over both fields. */
+int mphy_mixed_assemble(mphy_mixed* m, const double* disp_dev, const double* disp_prev_dev,
+                        const double* pres_dev, double lambda, const double* fext_dev, double* rhs_norm,
+                        int64_t* first_bad);
+/* y = A x with the assembled two-field operator, device vectors [3 n_node + n_pres]. */
+int mphy_mixed_apply(mphy_mixed* m, const double* x_dev, double* y_dev);
+/* Copies (device, any may be NULL): rhs [3 n_node + n_pres], reactions [3 n_node], the last
+ * solution [3 n_node + n_pres]. */
+int mphy_mixed_vectors(mphy_mixed* m, double* rhs_dev, double* reac_dev, double* solution_dev);
+/* MINRES on the assembled system from x = 0; *relres = ||rhs - A x|| / ||rhs|| (FP64). */
+int mphy_mixed_solve(mphy_mixed* m, int32_t* its, double* relres);
+/* solveWithNewtonRaphson for the mixed mesh (load stepping and cuts as mphy_newton_run; a cut
+ * restores displacements and pressures). fext_host, disp_host: [3 n_node]; pres_host: [n_node]
+ * nodal pressures; both in/out. hist: one row per Newton iteration (krylov_its = MINRES). */
+int mphy_mixed_newton_run(mphy_mixed* m, const double* fext_host, const mphy_newton_opts* opts,
+                          double* disp_host, double* pres_host, mphy_iter_stats* hist_host,
+                          int32_t max_hist, int32_t* n_hist);
+
 /* ------------------------------------------------------------------ batched form
  * Many independent problems as one block-diagonal union mesh: instance i owns the contiguous
  * nodes [node_ptr[i], node_ptr[i+1]) and only elements among them. The solver s (Jacobi-PCG,

@@ -62,6 +62,10 @@ class IterStats(C.Structure):
     ]
 
 
+class MixedOpts(C.Structure):
+    _fields_ = [("tangent", C.c_int32), ("max_it", C.c_int32), ("rtol", C.c_double)]
+
+
 class BatchStats(C.Structure):
     _fields_ = [
         ("steps", C.c_int32), ("graph_replays", C.c_int32), ("kernel_launches", C.c_int64), ("t_ms", C.c_float),
@@ -135,6 +139,18 @@ SIGNATURES = {
     "mphy_newton_run": (C.c_int, [_vp, _d, C.POINTER(NewtonOpts), _d, C.POINTER(IterStats), C.c_int32, _i32]),
     "mphy_arclength_run": (C.c_int, [_vp, _d, C.POINTER(NewtonOpts), _d, _d, C.c_int32, _i32, C.POINTER(IterStats),
                                      _d, C.c_int32, _i32]),
+    "mphy_mixed_opts_default": (None, [C.POINTER(MixedOpts)]),
+    "mphy_mixed_create": (C.c_int, [_vp, _vp, _vp, C.POINTER(MixedOpts), C.POINTER(_vp)]),
+    "mphy_mixed_destroy": (C.c_int, [_vp]),
+    "mphy_mixed_info": (C.c_int, [_vp, _i32, _i64, _i64]),
+    "mphy_mixed_pressure_nodes": (C.c_int, [_vp, _i32]),
+    "mphy_mixed_elem_eval": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64]),
+    "mphy_mixed_assemble": (C.c_int, [_vp, _vp, _vp, _vp, C.c_double, _vp, _d, _i64]),
+    "mphy_mixed_apply": (C.c_int, [_vp, _vp, _vp]),
+    "mphy_mixed_vectors": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "mphy_mixed_solve": (C.c_int, [_vp, _i32, _d]),
+    "mphy_mixed_newton_run": (C.c_int, [_vp, _d, C.POINTER(NewtonOpts), _d, _d, C.POINTER(IterStats), C.c_int32,
+                                        _i32]),
     "mphy_batch_create": (C.c_int, [_vp, C.c_int32, _i32, C.POINTER(_vp)]),
     "mphy_batch_destroy": (C.c_int, [_vp]),
     "mphy_batch_set_schedule": (C.c_int, [_vp, C.c_int32, C.c_int32]),

@@ -378,6 +378,110 @@ class FemSolidmechanicsGpu:
 
 
 @dataclass
+class MixedNewtonResult:
+    disp: np.ndarray
+    pres: np.ndarray  # nodal pressures [n_node] (vertex nodes carry the pressure DOFs)
+    hist: np.ndarray  # rows (step, iter, ||R||, MINRES its, status, t_assembly_ms, t_solve_ms)
+    status: int
+
+
+class MixedSolidGpu:
+    """A mixed u-p problem (tet10 displacement, linear vertex pressure; Elem_Solid_3D_Mixed1) on
+    the GPU: two-field assembly, MINRES solve and Newton load stepping (mphy_mixed_*)."""
+
+    def __init__(self, prob, ctx: Context | None = None, tangent: int = L.TANGENT_REFERENCE, rtol: float = 1e-10,
+                 max_it: int = 20000):
+        self.prob = prob
+        self.ctx = ctx or Context(0)
+        self.lib = self.ctx.lib
+        self.mesh = Mesh(self.ctx, prob)
+        self.pattern = Pattern(self.mesh)
+        o = L.MixedOpts()
+        self.lib.mphy_mixed_opts_default(C.byref(o))
+        o.tangent, o.rtol, o.max_it = tangent, rtol, max_it
+        h = C.c_void_p()
+        L.check(self.lib.mphy_mixed_create(self.ctx.h, self.mesh.h, self.pattern.h, C.byref(o), C.byref(h)))
+        self.h = h
+        npres, nb, nc = C.c_int32(), C.c_int64(), C.c_int64()
+        L.check(self.lib.mphy_mixed_info(h, C.byref(npres), C.byref(nb), C.byref(nc)))
+        self.n_pres, self.nnz_coupling, self.nnz_pp = npres.value, nb.value, nc.value
+        self.n = prob.n_dof + self.n_pres
+
+    def pressure_nodes(self) -> np.ndarray:
+        out = np.zeros(self.n_pres, np.int32)
+        L.check(self.lib.mphy_mixed_pressure_nodes(self.h, out.ctypes.data_as(L._i32)))
+        return out
+
+    def elements(self, disp, disp_prev, pres):
+        """(Kuu, FU, Kup, Kpp, FP, first bad) per element, device tensors."""
+        torch = _torch()
+        ne = self.prob.n_elem
+        dev = dict(dtype=torch.float64, device="cuda")
+        Kuu, FU = torch.empty((ne, 30, 30), **dev), torch.empty((ne, 30), **dev)
+        Kup, Kpp, FP = torch.empty((ne, 30, 4), **dev), torch.empty((ne, 4, 4), **dev), torch.empty((ne, 4), **dev)
+        bad = C.c_int64(-1)
+        rc = self.lib.mphy_mixed_elem_eval(self.h, _ptr(disp), _ptr(disp_prev), _ptr(pres), _ptr(Kuu), _ptr(FU),
+                                           _ptr(Kup), _ptr(Kpp), _ptr(FP), C.byref(bad))
+        L.check(rc, allow=(L.ERR_NEG_JACOBIAN,))
+        return Kuu, FU, Kup, Kpp, FP, bad.value
+
+    def assemble(self, disp, disp_prev, pres, lam: float = 0.0, fext=None) -> float:
+        nrm, bad = C.c_double(), C.c_int64(-1)
+        L.check(self.lib.mphy_mixed_assemble(self.h, _ptr(disp), _ptr(disp_prev), _ptr(pres), float(lam),
+                                             _ptr(fext) if fext is not None else None, C.byref(nrm), C.byref(bad)))
+        return nrm.value
+
+    def apply(self, x):
+        torch = _torch()
+        y = torch.empty_like(x)
+        L.check(self.lib.mphy_mixed_apply(self.h, _ptr(x), _ptr(y)))
+        return y
+
+    def vectors(self):
+        """(rhs [3 n_node + n_pres], reactions [3 n_node], solution [3 n_node + n_pres])."""
+        torch = _torch()
+        dev = dict(dtype=torch.float64, device="cuda")
+        rhs, reac, x = torch.empty(self.n, **dev), torch.empty(self.prob.n_dof, **dev), torch.empty(self.n, **dev)
+        L.check(self.lib.mphy_mixed_vectors(self.h, _ptr(rhs), _ptr(reac), _ptr(x)))
+        return rhs, reac, x
+
+    def solve(self, allow_fail: bool = False):
+        its, rr = C.c_int32(), C.c_double()
+        rc = self.lib.mphy_mixed_solve(self.h, C.byref(its), C.byref(rr))
+        if not allow_fail:
+            L.check(rc)
+        return rc, its.value, rr.value
+
+    def solveWithNewtonRaphson(self, max_newton: int = 10, tol_rel: float | None = None,  # noqa: N802
+                               tol_abs: float = 0.0, max_hist: int = 4096) -> MixedNewtonResult:
+        p = self.prob
+        o = L.NewtonOpts(p.dt, p.t_final, p.max_steps, max_newton, p.newton_rtol if tol_rel is None else tol_rel,
+                         tol_abs)
+        u, pres = np.zeros(p.n_dof), np.zeros(p.n_node)
+        f = _np(p.fnodal, np.float64)
+        hist = (L.IterStats * max_hist)()
+        n = C.c_int32(0)
+        rc = self.lib.mphy_mixed_newton_run(self.h, f.ctypes.data_as(L._d), C.byref(o), u.ctypes.data_as(L._d),
+                                            pres.ctypes.data_as(L._d), hist, max_hist, C.byref(n))
+        L.check(rc, allow=(L.ERR_TIME_STEP,))
+        rows = np.array([[h.step, h.iter, h.rhs_norm, h.krylov_its, h.status, h.t_assembly_ms, h.t_solve_ms]
+                         for h in hist[:n.value]], dtype=np.float64).reshape(-1, 7)
+        return MixedNewtonResult(disp=u, pres=pres, hist=rows, status=rc)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mphy_mixed_destroy(self.h)
+            self.h = None
+        for obj in ("pattern", "mesh"):
+            o = getattr(self, obj, None)
+            if o is not None:
+                o.close()
+
+    def __del__(self):
+        self.close()
+
+
+@dataclass
 class ArclengthResult:
     disp: np.ndarray
     load_factors: np.ndarray  # load factor of each converged step

@@ -17,6 +17,7 @@
 #include "elem.cuh"
 #include "elem_store.cuh"
 #include "mat.cuh"
+#include "mixed.cuh"
 
 namespace mphy {
 
@@ -241,6 +242,242 @@ void launch_gen(const ElemArgs& a, cudaStream_t s) {
     MPHY_CUDA(cudaGetLastError());
 }
 
+// ---------------------------------------------------------------- mixed u-p tet10 element
+// ElementBase::calcStiffnessAndResidualMixed3D (ElementBase2.cpp:278-553) for Elem_Solid_3D_Mixed1
+// with npElem = 10: quadratic displacement, linear pressure on the four vertex nodes (basis the
+// barycentric coordinates, LagrangeBasisFunsTetra(4)), the displacement element's 4-point rule.
+// Per Gauss point: F from u, Fn from the last converged step (Jn, then Jhat = Jn - U'(Jn)/U''(Jn),
+// thetahat = 1/U''(Jn)), p = sum Np_i p_i, the mixed material branch, and
+//   Kup(3I+a, j) = sum dvol h_aI Np_j = Kpu(j, 3I+a),   Kpp(i, j) = -sum dvol0 thetahat Np_i Np_j,
+//   FP(i) = -sum dvol0 Np_i (J - Jhat - thetahat p),    Kuu and FU as the displacement element.
+struct MixedSmem {
+    double x0[10][3];
+    double u[10][3];
+    double up[10][3];
+    double h[4][10][3];
+    double C[4][81];
+    double sig[4][9];
+    double dvol[4], dvol0[4], th[4], resip[4];
+    double pad[8];  // element stride 594 doubles
+};
+
+// tet 4-point rule (QuadratureUtil.cpp:690-712) points in barycentric form: Np(gp, i)
+__device__ __forceinline__ double tet4_np(int gp, int i) {
+    const double a = 0.1381966011250105, b = 0.5854101966249685;
+    if (i == 0) return gp == 0 ? 1.0 - 3.0 * a : 1.0 - b - 2.0 * a;
+    return gp == i ? b : a;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kGenEpb * 30) elem_mixed_kernel(MixedElemArgs ma) {
+    const ElemArgs& a = ma.base;
+    using T = GenTraits<10>;
+    constexpr int NPE = 10, NGP = 4, TPE = 30, NS = 30;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    auto* S = reinterpret_cast<MixedSmem*>(smem_raw);
+    const int el = threadIdx.x / TPE, loc = threadIdx.x % TPE;
+    const int I = loc % NPE, ch = loc / NPE;
+    const int64_t e = (int64_t)blockIdx.x * kGenEpb + el;
+    const bool live = e < a.n_elem;
+    MixedSmem& s = S[el];
+
+    int32_t node = 0;
+    if (live) {
+        node = a.conn[e * NPE + I];
+        if (ch == 0) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                s.x0[I][d] = a.coords[3 * (int64_t)node + d];
+                s.u[I][d] = a.disp[3 * (int64_t)node + d];
+                s.up[I][d] = ma.disp_prev[3 * (int64_t)node + d];
+            }
+        }
+    }
+    __syncthreads();
+
+    if (live && loc < NGP) {
+        const int gp = loc;
+        const double* dN = T::dN(gp);
+        double G[3][3] = {{0}}, Gc[3][3] = {{0}};
+#pragma unroll
+        for (int n = 0; n < NPE; ++n)
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                const double d = dN[r * NPE + n];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    G[r][c] += s.x0[n][c] * d;
+                    Gc[r][c] += (s.x0[n][c] + s.u[n][c]) * d;
+                }
+            }
+        double Gi[3][3], Gci[3][3];
+        const double jac0 = det3g(G);
+        inv3g(G, jac0, Gi);
+        const double jac = det3g(Gc);
+        inv3g(Gc, jac, Gci);
+        const double dvol = T::w(gp) * jac, dvol0 = T::w(gp) * jac0;
+        double F[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}}, Fn[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+#pragma unroll
+        for (int n = 0; n < NPE; ++n) {
+            double g0[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+                g0[c] = dN[n] * Gi[c][0] + dN[NPE + n] * Gi[c][1] + dN[2 * NPE + n] * Gi[c][2];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int m = 0; m < 3; ++m) {
+                    F[i][m] += s.u[n][i] * g0[m];
+                    Fn[i][m] += s.up[n][i] * g0[m];
+                }
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+                s.h[gp][n][c] = dN[n] * Gci[c][0] + dN[NPE + n] * Gci[c][1] + dN[2 * NPE + n] * Gci[c][2];
+        }
+        const double J = det3g(F);
+        if (J < 0.0) {
+            atomicMin(a.bad, (unsigned long long)e);
+            if (a.bad_elem) a.bad_elem[e] = 1;
+        }
+        double row[kMatRow];
+#pragma unroll
+        for (int q = 0; q < kMatRow; ++q) row[q] = a.matx[kMatRow * (int64_t)a.mat_id[e] + q];
+        // compute_constants_volumetric_functions (utilitiesmaterialHyperelastic.cpp:144-173)
+        double Jhat = 1.0, th = 0.0;
+        const int utype = (int)row[6];
+        if (utype != -1) {
+            double d1, d2;
+            const double Jn = det3g(Fn);
+            vol_derivs(utype, 1.0 / row[5], Jn, d1, d2);
+            Jhat = Jn - d1 / d2;
+            th = 1.0 / d2;
+        }
+        double pres = 0.0;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) pres += tet4_np(gp, i) * ma.pres[a.conn[e * NPE + i]];
+        double b[3][3], b2[3][3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) b[i][j] = F[i][0] * F[j][0] + F[i][1] * F[j][1] + F[i][2] * F[j][2];
+        square3(b, b2);
+        const MatScalars m = material_scalars(row, a.tangent, b, b2, J, true, pres);
+        material_fill(m, b, b2, dvol, s.sig[gp], s.C[gp]);
+        s.dvol[gp] = dvol;
+        s.dvol0[gp] = dvol0;
+        s.th[gp] = th;
+        s.resip[gp] = J - Jhat - th * pres;
+    }
+    __syncthreads();
+    if (!live) return;
+
+    bool freeI[3] = {true, true, true};
+    if (MODE & 2) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) freeI[c] = a.fixed[3 * (int64_t)node + c] == 0;
+    }
+    if (ch == 0) {
+        double R[3] = {0, 0, 0};
+        double kup[3][4] = {{0}};
+#pragma unroll
+        for (int gp = 0; gp < NGP; ++gp) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                R[c] -= s.h[gp][I][0] * s.sig[gp][c] + s.h[gp][I][1] * s.sig[gp][3 + c] +
+                        s.h[gp][I][2] * s.sig[gp][6 + c];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) kup[c][j] += s.dvol[gp] * s.h[gp][I][c] * tet4_np(gp, j);
+            }
+        }
+        store_residual<NPE, MODE>(a, e, I, node, freeI, R);
+        if (MODE & 1) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) ma.Kup[(e * NS + 3 * I + c) * 4 + j] = kup[c][j];
+        }
+        if (MODE & 2) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const uint32_t ib = ma.e2b[(e * NPE + I) * 4 + j], it = ma.e2bt[(e * 4 + j) * NPE + I];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    if (!freeI[c]) continue;
+                    atomicAdd(&ma.bval[3 * (int64_t)ib + c], kup[c][j]);
+                    atomicAdd(&ma.btval[3 * (int64_t)it + c], kup[c][j]);
+                }
+            }
+        }
+    } else if (ch == 1 && I < 4) {
+        // pressure row i = I (vertex node)
+        double fp = 0.0, kpp[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (int gp = 0; gp < NGP; ++gp) {
+            const double w = s.dvol0[gp] * tet4_np(gp, I);
+            fp -= w * s.resip[gp];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) kpp[j] -= w * s.th[gp] * tet4_np(gp, j);
+        }
+        if (MODE & 1) {
+            ma.FP[e * 4 + I] = fp;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) ma.Kpp[(e * 4 + I) * 4 + j] = kpp[j];
+        }
+        if (MODE & 2) {
+            atomicAdd(&ma.rhs_p[ma.pres_id[node]], fp);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) atomicAdd(&ma.cval[ma.e2c[(e * 4 + I) * 4 + j]], kpp[j]);
+        }
+    }
+    // Kuu: thread (I, ch), column nodes 4 ch .. 4 ch + 3
+    const int J0 = ch * kGenCh;
+    double acc[kGenCh][9];
+#pragma unroll
+    for (int j = 0; j < kGenCh; ++j)
+#pragma unroll
+        for (int v = 0; v < 9; ++v) acc[j][v] = 0.0;
+#pragma unroll 1
+    for (int gp = 0; gp < NGP; ++gp) {
+        const double h0 = s.h[gp][I][0], h1 = s.h[gp][I][1], h2 = s.h[gp][I][2];
+        const double* C = s.C[gp];
+        double Gc[3][9];
+#pragma unroll
+        for (int aa = 0; aa < 3; ++aa)
+#pragma unroll
+            for (int q = 0; q < 9; ++q) Gc[aa][q] = h0 * C[9 * aa + q] + h1 * C[9 * (3 + aa) + q] + h2 * C[9 * (6 + aa) + q];
+#pragma unroll
+        for (int j = 0; j < kGenCh; ++j) {
+            if (J0 + j < NPE) {
+                const double g0 = s.h[gp][J0 + j][0], g1 = s.h[gp][J0 + j][1], g2 = s.h[gp][J0 + j][2];
+#pragma unroll
+                for (int aa = 0; aa < 3; ++aa)
+#pragma unroll
+                    for (int bb = 0; bb < 3; ++bb)
+                        acc[j][3 * aa + bb] += Gc[aa][bb] * g0 + Gc[aa][3 + bb] * g1 + Gc[aa][6 + bb] * g2;
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < kGenCh; ++j) {
+        const int J = J0 + j;
+        if (J < NPE) store_block<NPE, MODE>(a, e, I, J, node, freeI, acc[j]);
+    }
+}
+
+template <int MODE>
+void launch_mixed(const MixedElemArgs& a, cudaStream_t s) {
+    const size_t smem = kGenEpb * sizeof(MixedSmem);
+    static bool configured = false;
+    if (!configured) {
+        MPHY_CUDA(cudaFuncSetAttribute(elem_mixed_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        configured = true;
+    }
+    const unsigned grid = ceil_div((size_t)a.base.n_elem, kGenEpb);
+    if (grid == 0) return;
+    elem_mixed_kernel<MODE><<<grid, kGenEpb * 30, smem, s>>>(a);
+    MPHY_CUDA(cudaGetLastError());
+}
+
 // Batched material call: F [n][9] row-major -> sigma [n][9], C [n][81] (reference index order).
 __global__ void material_eval_kernel(int n, const double* __restrict__ Fm, const double* __restrict__ row_in,
                                      int tangent, double* __restrict__ stre, double* __restrict__ Cout) {
@@ -280,6 +517,12 @@ void launch_elem_gen(const ElemArgs& a, int npe, int mode, cudaStream_t s) {
         else if (mode == 2) launch_gen<10, 2>(a, s);
         else launch_gen<10, 3>(a, s);
     }
+}
+
+void launch_elem_mixed(const MixedElemArgs& a, int mode, cudaStream_t s) {
+    if (mode == 1) launch_mixed<1>(a, s);
+    else if (mode == 2) launch_mixed<2>(a, s);
+    else launch_mixed<3>(a, s);
 }
 
 void launch_material_eval(int n, const double* F, const double* row_dev, int tangent, double* stre, double* C,

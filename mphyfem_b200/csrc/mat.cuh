@@ -29,18 +29,20 @@ __device__ __forceinline__ double pow_m23(double J) {
     return r * r;
 }
 
-// Neo-Hookean (:186-295) from the factors the structured kernel uses.
-__device__ __forceinline__ void nh_scalars(const double b[3][3], double J, double mu, double Kinv, int utype,
-                                           int tangent, MatScalars& m) {
-    const NhFactors f = nh_factors(b, J, mu, Kinv, utype, tangent);
-    m.s[0] = f.s1;
-    m.s[1] = f.s2;
-    m.k[0] = f.c1;
-    m.k[1] = f.c2;
-    m.k[2] = f.c2;
-    m.k[3] = f.c3;
-    m.k[4] = f.f4;
-    m.k[5] = f.f9;
+// Neo-Hookean (:186-295), the factors of the structured kernel (nh.cuh) with U'(J), U''(J) given:
+// the mixed branch passes dU = p, d2U = 0 and has no d_jl d_ik term.
+__device__ __forceinline__ void nh_scalars(const double b[3][3], double J, double mu, double dU, double d2U,
+                                           double f9, MatScalars& m) {
+    const double Ib = b[0][0] + b[1][1] + b[2][2];
+    const double jm53 = pow_m23(J) / J;
+    m.s[0] = mu * jm53;
+    m.s[1] = -m.s[0] * (1.0 / 3.0) * Ib + dU;
+    m.k[0] = (1.0 / 3.0) * mu * jm53 * Ib - dU;
+    m.k[1] = -(2.0 / 3.0) * mu * jm53;
+    m.k[2] = m.k[1];
+    m.k[3] = (2.0 / 3.0) * (1.0 / 3.0) * mu * jm53 * Ib + (J * d2U + dU);
+    m.k[4] = mu * jm53;
+    m.k[5] = f9;
 }
 
 // Mooney-Rivlin (:300-420). The reference's r7d3 is 5/3 (:303), so its J^{-7/3} factor is
@@ -122,9 +124,14 @@ __device__ __forceinline__ void ab_scalars(double J, double Ib, double mu, doubl
     }
 }
 
-// Stress and tangent scalars of material row `row` at deformation gradient F.
+// Stress and tangent scalars of material row `row` at deformation gradient F. Mixed (u-p)
+// elements pass mixed = true and the Gauss-point pressure: p replaces U'(J) in the stress and
+// p (d_ij d_kl - d_jk d_il) replaces the volumetric tangent (the MIXED_ELEMENT branches), which
+// is U' = p, U'' = 0 in the factors below; Arruda-Boyce's written branch adds -p d_jl d_ik
+// (:661-664), which the consistent tangent leaves out.
 __device__ __forceinline__ MatScalars material_scalars(const double* row, int tangent, const double b[3][3],
-                                                       const double b2[3][3], double J) {
+                                                       const double b2[3][3], double J, bool mixed = false,
+                                                       double pres = 0.0) {
     MatScalars m;
 #pragma unroll
     for (int i = 0; i < 3; ++i) m.s[i] = 0.0;
@@ -134,15 +141,18 @@ __device__ __forceinline__ MatScalars material_scalars(const double* row, int ta
     const double Kinv = row[5];
     const int utype = (int)row[6];
     const double Ib = b[0][0] + b[1][1] + b[2][2];
+    double dU = pres, d2U = 0.0;
+    if (!mixed) vol_derivs(utype, 1.0 / Kinv, J, dU, d2U);
     if (model == MPHY_MAT_NEOHOOKEAN) {
-        nh_scalars(b, J, row[1], Kinv, utype, tangent, m);
-        return m;
+        nh_scalars(b, J, row[1], dU, d2U, (mixed || tangent == MPHY_TANGENT_CONSISTENT) ? 0.0 : -dU, m);
+    } else if (model == MPHY_MAT_MOONEYRIVLIN) {
+        mr_scalars(b, b2, J, Ib, row[1], row[2], dU, d2U, m);
+    } else if (model == MPHY_MAT_GENT) {
+        gent_scalars(J, Ib, row[1], row[2], dU, d2U, m);
+    } else {
+        ab_scalars(J, Ib, row[1], row[2], dU, d2U, tangent, m);
+        if (mixed && tangent != MPHY_TANGENT_CONSISTENT) m.k[5] -= pres;
     }
-    double dU, d2U;
-    vol_derivs(utype, 1.0 / Kinv, J, dU, d2U);
-    if (model == MPHY_MAT_MOONEYRIVLIN) mr_scalars(b, b2, J, Ib, row[1], row[2], dU, d2U, m);
-    else if (model == MPHY_MAT_GENT) gent_scalars(J, Ib, row[1], row[2], dU, d2U, m);
-    else ab_scalars(J, Ib, row[1], row[2], dU, d2U, tangent, m);
     return m;
 }
 

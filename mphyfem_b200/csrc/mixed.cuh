@@ -1,0 +1,33 @@
+// mixed.cuh -- the mixed u-p (tet10 displacement, linear vertex pressure) element and its
+// two-field system: pressure DOFs at the vertex nodes, the coupling blocks B = Kup (u rows),
+// B^T = Kpu (pressure rows) and C = Kpp, each in compressed rows.
+#pragma once
+#include "elem.cuh"
+
+namespace mphy {
+
+// Element evaluation (elem_gen.cu). MODE bit 1 exports per element Ke (= Kuu), Re (= FU), Kup
+// [30][4], Kpp [4][4], FP [4]; bit 2 scatters Kuu / FU / reactions through `base` (FP64 masked
+// SELL) and the coupling blocks through the element maps.
+struct MixedElemArgs {
+    ElemArgs base;
+    const double* disp_prev;  // [3 n_node] last converged step: Jn of compute_constants_volumetric_functions
+    const double* pres;       // [n_node] nodal pressures (vertex nodes)
+    const int32_t* pres_id;   // [n_node] pressure DOF or -1
+    // export
+    double* Kup = nullptr;
+    double* Kpp = nullptr;
+    double* FP = nullptr;
+    // assembly: entry indices of element pairs, values (3 per B / B^T entry, 1 per C entry)
+    const uint32_t* e2b = nullptr;   // [n_elem][10][4]
+    const uint32_t* e2bt = nullptr;  // [n_elem][4][10]
+    const uint32_t* e2c = nullptr;   // [n_elem][4][4]
+    double* bval = nullptr;
+    double* btval = nullptr;
+    double* cval = nullptr;
+    double* rhs_p = nullptr;  // [n_pres]
+};
+
+void launch_elem_mixed(const MixedElemArgs& a, int mode, cudaStream_t s);
+
+}  // namespace mphy
