@@ -352,11 +352,13 @@ int mphy_arclength_run(mphy_solver* s, const double* fext_host, const mphy_newto
  * MUMPS LU): relative tolerance rtol on the preconditioned residual, at most max_it iterations. */
 typedef struct mphy_mixed mphy_mixed;
 typedef struct mphy_mixed_opts {
-    int32_t tangent;  /* MPHY_TANGENT_* */
-    int32_t max_it;   /* MINRES iterations per solve */
-    double rtol;      /* MINRES relative tolerance */
+    int32_t tangent;            /* MPHY_TANGENT_* */
+    int32_t max_it;             /* MINRES iterations per solve */
+    double rtol;                /* MINRES relative tolerance */
+    int32_t coarse_aggregates;  /* > 0: the displacement block of the preconditioner adds the
+                                 * rigid-body coarse space over about this many aggregates */
 } mphy_mixed_opts;
-void mphy_mixed_opts_default(mphy_mixed_opts* opts); /* reference tangent, 20000, 1e-10 */
+void mphy_mixed_opts_default(mphy_mixed_opts* opts); /* reference tangent, 20000, 1e-10, 0 */
 /* mesh: tet10 (npe = 10); pattern: mphy_pattern_build of the same mesh. opts may be NULL. */
 int mphy_mixed_create(mphy_ctx* ctx, const mphy_mesh* mesh, const mphy_pattern* pattern,
                       const mphy_mixed_opts* opts, mphy_mixed** out);

@@ -63,7 +63,8 @@ class IterStats(C.Structure):
 
 
 class MixedOpts(C.Structure):
-    _fields_ = [("tangent", C.c_int32), ("max_it", C.c_int32), ("rtol", C.c_double)]
+    _fields_ = [("tangent", C.c_int32), ("max_it", C.c_int32), ("rtol", C.c_double),
+                ("coarse_aggregates", C.c_int32)]
 
 
 class BatchStats(C.Structure):

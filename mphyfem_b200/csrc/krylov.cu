@@ -622,6 +622,27 @@ template void residual_fp64<double>(const SellView&, const double*, const double
 template void residual_fp64<float>(const SellView&, const float*, const double*, const double*, double*, double*,
                                    uint32_t*, double*, cudaStream_t, int);
 
+namespace {
+// z_u += Z c on the free displacement DOFs (the prolongation of the coarse correction)
+__global__ void __launch_bounds__(kThreads) coarse_prolong_add_kernel(int32_t n_node, CoarseView cv, double* z) {
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < n_node; n += (int64_t)gridDim.x * blockDim.x) {
+        const double* c = cv.c + 6 * (int64_t)cv.agg[n];
+        const double dx = cv.d[3 * n], dy = cv.d[3 * n + 1], dz = cv.d[3 * n + 2];
+        const double zc[3] = {c[0] - dy * c[3] + dz * c[5], c[1] + dx * c[3] - dz * c[4], c[2] + dy * c[4] - dx * c[5]};
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+            if (!cv.fixed[3 * n + a]) z[3 * n + a] += zc[a];
+    }
+}
+}  // namespace
+
+void coarse_apply_add(const CoarseView& cv, int32_t n_node, const double* r, double* z, cudaStream_t s, int sm) {
+    coarse_restrict_kernel<double><<<std::min(cv.n_agg, sm * 8), kThreads, 0, s>>>(cv, r, nullptr);
+    coarse_gemv_kernel<<<stride_grid((int64_t)cv.kp * 32, kThreads, sm), kThreads, 0, s>>>(cv, nullptr);
+    coarse_prolong_add_kernel<<<stride_grid(n_node, kThreads, sm), kThreads, 0, s>>>(n_node, cv, z);
+    MPHY_CUDA(cudaGetLastError());
+}
+
 void diag_from_offdiag(const SellView& A, const float* val, double* diag64, cudaStream_t s, int sm) {
     diag_rowsum_kernel<<<stride_grid((int64_t)A.n_slices * 32, kThreads, sm), kThreads, 0, s>>>(A, val, diag64);
     MPHY_CUDA(cudaGetLastError());

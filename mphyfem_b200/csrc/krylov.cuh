@@ -142,6 +142,10 @@ void diag_from_offdiag(const SellView& A, const float* val, double* diag64, cuda
 void export_fix_diagonal(const double* diag64, const int64_t* rowptr, const int32_t* col, const int32_t* assy,
                          int32_t n_free, double* out, cudaStream_t s, int sm);
 
+// z_u += Z E^{-1} Z^T r_u: the coarse correction of a set-up coarse space added to z over the
+// first 3 n_node entries (restriction, coarse solve, prolongation; FP64).
+void coarse_apply_add(const CoarseView& cv, int32_t n_node, const double* r, double* z, cudaStream_t s, int sm);
+
 // small kernels of the solver surface
 template <typename VT>
 void set_prescribed_diagonal(const SellView& A, const uint8_t* fixed, VT* val, cudaStream_t s, int sm);

@@ -18,14 +18,16 @@
 // Solve. The reference's sample inputs factorise the indefinite system with MUMPS LU
 // (-ksp_type preonly -pc_type lu). Here: MINRES (Paige-Saunders recurrences in the preconditioned
 // form of Elman, Silvester and Wathen) with the symmetric positive definite block-diagonal
-// preconditioner diag(Kuu)^-1 (+) S^-1, S_ii = sum_k (B^T_ik)^2 / Kuu_kk + |C_ii| (the diagonal of
-// the Schur complement's approximation). All scalars stay on the device; the host reads the
-// residual estimate every kCheck iterations.
+// preconditioner P_u^-1 (+) S^-1: P_u^-1 = diag(Kuu)^-1, plus Z E^-1 Z^T with the rigid-body
+// coarse space of the displacement solver when coarse_aggregates > 0; S_ii = sum_k (B^T_ik)^2 /
+// Kuu_kk + |C_ii| (the diagonal of the Schur complement's approximation). All scalars stay on
+// the device; the host reads the residual estimate every kCheck iterations.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
 
+#include "coarse.cuh"
 #include "common.cuh"
 #include "elem.cuh"
 #include "krylov.cuh"
@@ -58,6 +60,8 @@ struct mphy_mixed {
     DevBuf<double> disp, disp_prev, pres, pres_prev, fext;
     std::vector<int32_t> pres_node_host;
     bool assembled = false;
+    CoarseSpace coarse;  // opts.coarse_aggregates > 0: two-level displacement block
+    bool use_coarse = false;
 };
 
 namespace {
@@ -328,6 +332,10 @@ void assemble(mphy_mixed* m, const double* disp, const double* disp_prev, const 
                                                                       m->dinv.p);
     MPHY_CUDA(cudaGetLastError());
     m->launches += 10;
+    if (m->use_coarse) {
+        m->coarse.setup<double>(m->A, m->val.p, nullptr, st);
+        m->launches += m->coarse.launches;
+    }
     m->assembled = true;
 }
 
@@ -358,6 +366,7 @@ int minres(mphy_mixed* m, int32_t* its_out, double* relres) {
     MPHY_CUDA(cudaMemsetAsync(m->v[0].p, 0, n * sizeof(double), st));
     MPHY_CUDA(cudaMemcpyAsync(m->v[1].p, m->rhs.p, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
     scale_kernel<<<grid, 256, 0, st>>>(n, m->dinv.p, m->v[1].p, m->z[0].p);
+    if (m->use_coarse) coarse_apply_add(m->coarse.view(), m->n_node, m->v[1].p, m->z[0].p, st, sm);
     dot_fp64(m->z[0].p, m->v[1].p, n, m->partials.p, m->counter.p, sc + S_DOT2, st, sm);
     double g0sq = 0.0;
     MPHY_CUDA(cudaMemcpyAsync(&g0sq, sc + S_DOT2, sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -373,6 +382,10 @@ int minres(mphy_mixed* m, int32_t* its_out, double* relres) {
             dot_fp64(m->az.p, m->z[iz].p, n, m->partials.p, m->counter.p, sc + S_DOT1, st, sm);
             minres_v_kernel<<<grid, 256, 0, st>>>(n, m->az.p, m->v[iv].p, m->v[iv_old].p, m->dinv.p, sc,
                                                   m->v[iv_new].p, m->z[iz_new].p);
+            if (m->use_coarse) {
+                coarse_apply_add(m->coarse.view(), m->n_node, m->v[iv_new].p, m->z[iz_new].p, st, sm);
+                m->launches += 3;
+            }
             dot_fp64(m->z[iz_new].p, m->v[iv_new].p, n, m->partials.p, m->counter.p, sc + S_DOT2, st, sm);
             minres_scalar_kernel<<<1, 1, 0, st>>>(sc, m->opts.rtol);
             minres_w_kernel<<<grid, 256, 0, st>>>(n, m->z[iz].p, m->w[iw].p, m->w[iw_old].p, sc, m->w[iw_new].p,
@@ -420,6 +433,7 @@ void mphy_mixed_opts_default(mphy_mixed_opts* o) {
     o->tangent = MPHY_TANGENT_REFERENCE;
     o->max_it = 20000;
     o->rtol = 1e-10;
+    o->coarse_aggregates = 0;
 }
 
 int mphy_mixed_create(mphy_ctx* c, const mphy_mesh* mesh, const mphy_pattern* pat, const mphy_mixed_opts* o,
@@ -523,6 +537,10 @@ int mphy_mixed_create(mphy_ctx* c, const mphy_mesh* mesh, const mphy_pattern* pa
             m->counter.alloc(1);
             MPHY_CUDA(cudaMemsetAsync(m->counter.p, 0, sizeof(uint32_t), st));
             m->bad.alloc(1);
+            if (m->opts.coarse_aggregates > 0) {
+                m->coarse.init(c, mesh, pat, m->opts.coarse_aggregates);
+                m->use_coarse = true;
+            }
             MPHY_CUDA(cudaStreamSynchronize(st));
         } catch (...) {
             delete m;

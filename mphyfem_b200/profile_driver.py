@@ -7,6 +7,7 @@
     python -m mphyfem_b200.profile_driver --op newton --precision mixed --coarse 64 --reps 1
     python -m mphyfem_b200.profile_driver --op batch --instances 48 --reps 2
     python -m mphyfem_b200.profile_driver --op assemble --model 2 --reps 3
+    python -m mphyfem_b200.profile_driver --op mixed --nx 48 --ny 24 --nz 24 --reps 1
 
 Each run builds the hex8 cantilever of the given size (or, for ``batch``, the first blocks of
 the 512-block batched set), assembles it once at u = 0 and then repeats the chosen operation:
@@ -14,6 +15,9 @@ SpMV with the assembled matrix, the fused assembly, one Newton iteration (assemb
 update), or the batched persistent solve of all instances. ``--model`` gives every element one
 hyperelastic model (1 Mooney-Rivlin, 2 Gent, 3 Arruda-Boyce: the dense-tangent element kernel).
 The mean device time per repetition (CUDA events on the library's stream) goes to stderr.
+``mixed`` builds the tet10 Kuhn mesh of the given size as a mixed u-p problem (linear vertex
+pressure, kappa/mu = 1e4) and runs one load step of its Newton driver, printing per iteration
+the assembly and MINRES times and iterations.
 """
 from __future__ import annotations
 
@@ -25,7 +29,7 @@ import numpy as np
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--op", choices=["spmv", "assemble", "newton", "batch"], default="spmv")
+    ap.add_argument("--op", choices=["spmv", "assemble", "newton", "batch", "mixed"], default="spmv")
     ap.add_argument("--nx", type=int, default=128)
     ap.add_argument("--ny", type=int, default=32)
     ap.add_argument("--nz", type=int, default=32)
@@ -57,6 +61,18 @@ def main(argv=None):
         torch.cuda.synchronize()
         print(f"batch of {args.instances}: n_node={u.n_node} its mean {its.mean():.0f} max {its.max()} "
               f"ms {ms:.2f}", file=sys.stderr)
+        return
+    if args.op == "mixed":
+        q = meshgen.tet10_kuhn(args.nx, args.ny, args.nz, lx=4.0, traction=(0.0, 0.0, -0.02), kappa=1.0e4)
+        q.dt, q.t_final, q.max_steps, q.newton_rtol = 0.2, 0.2, 1, 1e-8
+        m = api.MixedSolidGpu(q, ctx, tangent=_lib.TANGENT_CONSISTENT, rtol=args.rtol, max_it=200000,
+                              coarse_aggregates=args.coarse)
+        for _ in range(args.reps):
+            res = m.solveWithNewtonRaphson(max_newton=10)
+            for row in res.hist:
+                print(f"iter {int(row[1])}: |R| {row[2]:.3e} minres_its {int(row[3])} "
+                      f"assembly_ms {row[5]:.2f} solve_ms {row[6]:.1f}", file=sys.stderr)
+        print(f"{q.name}: n_dof={q.n_dof} n_pres={m.n_pres} n_elem={q.n_elem} coupling_entries={m.nnz_coupling}")
         return
     p = meshgen.hex8_cantilever(args.nx, args.ny, args.nz)
     if args.model:

@@ -167,3 +167,20 @@ def test_nearly_incompressible(env, oracle, consistent):
     consistent(True)
     u, pres, _ = MixedProblem(p).newton(max_newton=15)
     assert np.linalg.norm(res.disp - u) <= 1e-7 * np.linalg.norm(u)
+
+
+def test_two_level_preconditioner(env, oracle, consistent):
+    # the rigid-body coarse space on the displacement block: same Newton result, fewer iterations
+    torch, api, _lib, ctx = env
+    from oracle.mixed_ref import MixedProblem
+    p = _problem((NH,), kappa=200.0)
+    runs = {}
+    for agg in (0, 8):
+        m = api.MixedSolidGpu(p, ctx, tangent=1, rtol=1e-12, coarse_aggregates=agg)
+        runs[agg] = m.solveWithNewtonRaphson(max_newton=15)
+        assert runs[agg].status == 0
+    consistent(True)
+    u, _, hist = MixedProblem(p).newton(max_newton=15)
+    assert np.array_equal(runs[8].hist[:, :2], hist[:, :2])
+    assert np.linalg.norm(runs[8].disp - u) <= 1e-8 * np.linalg.norm(u)
+    assert runs[8].hist[:, 3].sum() < runs[0].hist[:, 3].sum()
