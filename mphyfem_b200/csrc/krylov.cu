@@ -17,6 +17,9 @@
 #include <algorithm>
 #include <cmath>
 
+#include <mutex>
+#include <unordered_map>
+
 #include "krylov.cuh"
 
 namespace mphy {
@@ -27,6 +30,31 @@ unsigned stride_grid(int64_t n, int threads, int sm_count, int per_sm) {
     const int64_t want = (n + threads - 1) / threads;
     const int64_t cap = (int64_t)sm_count * per_sm;
     return (unsigned)(want < 1 ? 1 : (want > cap ? cap : want));
+}
+
+// Grid of a grid-stride kernel sized to what the SMs hold at once (the kernel's occupancy), so
+// that no second partial wave of CTAs runs at low occupancy after the first: a kernel with 40
+// registers per thread holds 6 CTAs of 256 per SM, and 8 CTAs per SM would leave a quarter of
+// the grid for a tail.
+namespace {
+std::mutex g_occ_mu;
+std::unordered_map<const void*, int> g_occ;
+}  // namespace
+
+unsigned resident_grid(const void* kernel, int64_t n, int threads, int sm_count) {
+    int per_sm = 0;
+    {
+        std::lock_guard<std::mutex> lk(g_occ_mu);
+        auto it = g_occ.find(kernel);
+        if (it != g_occ.end()) {
+            per_sm = it->second;
+        } else {
+            MPHY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0));
+            if (per_sm < 1) per_sm = 1;
+            g_occ.emplace(kernel, per_sm);
+        }
+    }
+    return stride_grid(n, threads, sm_count, per_sm);
 }
 
 namespace {
@@ -602,8 +630,8 @@ __global__ void gather_free_kernel(const double* __restrict__ v, const int32_t* 
 // ---------------------------------------------------------------- host wrappers
 template <typename VT, typename XT>
 void spmv(const SellView& A, const VT* val, const XT* x, XT* y, cudaStream_t s, int sm) {
-    spmv_kernel<VT, XT, false><<<stride_grid((int64_t)A.n_slices * 32, kThreads, sm), kThreads, 0, s>>>(
-        A, val, x, y, nullptr, nullptr);
+    const unsigned g = resident_grid((const void*)spmv_kernel<VT, XT, false>, (int64_t)A.n_slices * 32, kThreads, sm);
+    spmv_kernel<VT, XT, false><<<g, kThreads, 0, s>>>(A, val, x, y, nullptr, nullptr);
     MPHY_CUDA(cudaGetLastError());
 }
 template void spmv<double, double>(const SellView&, const double*, const double*, double*, cudaStream_t, int);
@@ -613,7 +641,7 @@ template void spmv<float, double>(const SellView&, const float*, const double*, 
 template <typename VT>
 void residual_fp64(const SellView& A, const VT* val, const double* x, const double* b, double* r, double* partials,
                    uint32_t* counter, double* out_dev, cudaStream_t s, int sm) {
-    residual_kernel<VT><<<stride_grid((int64_t)A.n_slices * 32, kThreads, sm), kThreads, 0, s>>>(
+    residual_kernel<VT><<<resident_grid((const void*)residual_kernel<VT>, (int64_t)A.n_slices * 32, kThreads, sm), kThreads, 0, s>>>(
         A, val, x, b, r, partials, counter, out_dev);
     MPHY_CUDA(cudaGetLastError());
 }
@@ -658,7 +686,7 @@ void export_fix_diagonal(const double* diag64, const int64_t* rowptr, const int3
 
 void dot_fp64(const double* a, const double* b, int64_t n, double* partials, uint32_t* counter, double* out_dev,
               cudaStream_t s, int sm) {
-    dot_kernel<<<stride_grid(n, kThreads, sm), kThreads, 0, s>>>(a, b, n, partials, counter, out_dev);
+    dot_kernel<<<resident_grid((const void*)dot_kernel, n, kThreads, sm), kThreads, 0, s>>>(a, b, n, partials, counter, out_dev);
     MPHY_CUDA(cudaGetLastError());
 }
 
@@ -677,7 +705,7 @@ void add_scaled_free(const uint8_t* fixed, const double* f, double scale, double
 }
 
 void axpy_inplace(double* y, const double* x, double a, int64_t n, cudaStream_t s, int sm) {
-    axpy_kernel<double><<<stride_grid(n, kThreads, sm), kThreads, 0, s>>>(y, x, a, n);
+    axpy_kernel<double><<<resident_grid((const void*)axpy_kernel<double>, n, kThreads, sm), kThreads, 0, s>>>(y, x, a, n);
     MPHY_CUDA(cudaGetLastError());
 }
 
@@ -723,8 +751,8 @@ Pcg<VT, XT>::~Pcg() {
 
 template <typename VT, typename XT>
 void Pcg<VT, XT>::record_iterations(const VT* val, XT* x, cudaStream_t s, int n_iter) {
-    const unsigned gs = stride_grid((int64_t)A_.n_slices * 32, kThreads, sm_);
-    const unsigned gv = stride_grid(n_, kThreads, sm_);
+    const unsigned gs = resident_grid((const void*)spmv_kernel<VT, XT, true>, (int64_t)A_.n_slices * 32, kThreads, sm_);
+    const unsigned gv = resident_grid((const void*)pcg_update_kernel<XT, true>, n_, kThreads, sm_);
     for (int it = 0; it < n_iter; ++it) {
         spmv_kernel<VT, XT, true><<<gs, kThreads, 0, s>>>(A_, val, p_.p, q_.p, partials_.p, st_.p);
         if (kind_ == PcKind::Jacobi) {
@@ -736,12 +764,13 @@ void Pcg<VT, XT>::record_iterations(const VT* val, XT* x, cudaStream_t s, int n_
             coarse_restrict_kernel<XT><<<std::min(coarse_.n_agg, sm_ * 8), kThreads, 0, s>>>(coarse_, r_.p, st_.p);
             coarse_gemv_kernel<<<stride_grid((int64_t)coarse_.kp * 32, kThreads, sm_), kThreads, 0, s>>>(coarse_,
                                                                                                           st_.p);
-            coarse_final_kernel<XT, false><<<stride_grid(A_.n_node, kThreads, sm_), kThreads, 0, s>>>(
+            coarse_final_kernel<XT, false><<<resident_grid((const void*)coarse_final_kernel<XT, false>, A_.n_node, kThreads, sm_), kThreads, 0, s>>>(
                 A_.n_node, coarse_, r_.p, z_.p, p_.p, dinv_.p, partials_.p, partials2_.p, st_.p, 0, 0, 0, 0, norm_type);
         } else {
             pcg_update_kernel<XT, false><<<gv, kThreads, 0, s>>>(n_, x, r_.p, z_.p, p_.p, q_.p, nullptr, nullptr,
                                                                   nullptr, st_.p);
-            const unsigned gg = stride_grid((int64_t)factor_.G.n_slices * 32, kThreads, sm_);
+            const unsigned gg = resident_grid((const void*)factor_apply_kernel<XT, false>,
+                                              (int64_t)factor_.G.n_slices * 32, kThreads, sm_);
             spmv_kernel<FactorT, XT, false><<<gg, kThreads, 0, s>>>(factor_.G, factor_.gval, r_.p, t_.p, nullptr, st_.p);
             if (kind_ == PcKind::FactorCoarse) {
                 coarse_restrict_kernel<XT><<<std::min(coarse_.n_agg, sm_ * 8), kThreads, 0, s>>>(coarse_, r_.p, st_.p);
@@ -772,7 +801,7 @@ int Pcg<VT, XT>::solve(const VT* val, const XT* b, XT* x, double rtol, double ab
                                                             st_.p, rtol, abstol, dtol, maxit, norm_type);
         coarse_restrict_kernel<XT><<<std::min(coarse_.n_agg, sm_ * 8), kThreads, 0, s>>>(coarse_, r_.p, nullptr);
         coarse_gemv_kernel<<<stride_grid((int64_t)coarse_.kp * 32, kThreads, sm_), kThreads, 0, s>>>(coarse_, nullptr);
-        coarse_final_kernel<XT, true><<<stride_grid(A_.n_node, kThreads, sm_), kThreads, 0, s>>>(
+        coarse_final_kernel<XT, true><<<resident_grid((const void*)coarse_final_kernel<XT, true>, A_.n_node, kThreads, sm_), kThreads, 0, s>>>(
             A_.n_node, coarse_, r_.p, z_.p, p_.p, dinv_.p, partials_.p, partials2_.p, st_.p, rtol, abstol, dtol,
             maxit, norm_type);
         launches += 5;

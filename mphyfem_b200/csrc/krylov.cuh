@@ -56,6 +56,8 @@ struct FactorView {
 
 // Grid of a grid-stride kernel over n items with the given block size.
 unsigned stride_grid(int64_t n, int threads, int sm_count, int per_sm = 8);
+// The same, capped at the CTAs the SMs hold at once for `kernel` (occupancy query, cached).
+unsigned resident_grid(const void* kernel, int64_t n, int threads, int sm_count);
 
 // y = A x.
 template <typename VT, typename XT>

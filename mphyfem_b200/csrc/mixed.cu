@@ -273,7 +273,7 @@ void apply(mphy_mixed* m, const double* x, double* y, cudaStream_t st) {
     const int sm = m->ctx->sm_count;
     spmv<double, double>(m->A, m->val.p, x, y, st, sm);
     const int64_t total = (int64_t)m->n_node + m->n_pres;
-    coupling_apply_kernel<<<stride_grid(total, 256, sm), 256, 0, st>>>(
+    coupling_apply_kernel<<<resident_grid((const void*)coupling_apply_kernel, total, 256, sm), 256, 0, st>>>(
         m->n_node, m->n_pres, m->b_ptr.p, m->b_col.p, m->b_val.p, m->bt_ptr.p, m->bt_col.p, m->bt_val.p, m->c_ptr.p,
         m->c_col.p, m->c_val.p, x, y);
     MPHY_CUDA(cudaGetLastError());
@@ -359,7 +359,7 @@ int minres(mphy_mixed* m, int32_t* its_out, double* relres) {
     cudaStream_t st = m->ctx->stream;
     const int sm = m->ctx->sm_count;
     const int64_t n = 3 * (int64_t)m->n_node + m->n_pres;
-    const unsigned grid = stride_grid(n, 256, sm);
+    const unsigned grid = resident_grid((const void*)minres_w_kernel, n, 256, sm);
     double* sc = m->sc.p;
     MPHY_CUDA(cudaMemsetAsync(m->x.p, 0, n * sizeof(double), st));
     for (int k = 0; k < 3; ++k) MPHY_CUDA(cudaMemsetAsync(m->w[k].p, 0, n * sizeof(double), st));
