@@ -179,9 +179,14 @@ __device__ __forceinline__ void store_tile(const double (*S)[TP], double* M, int
     for (int t = threadIdx.x; t < T * T; t += blockDim.x) M[(int64_t)(ti * T + t / T) * kp + tj * T + t % T] = S[t / T][t % T];
 }
 
-// factor the diagonal tile (j, j) in place (lower triangle; upper zeroed)
-__global__ void __launch_bounds__(256) potrf_tile(double* E, int kp, int j, int32_t* err) {
-    __shared__ double S[T][TP];
+// Factor the diagonal tile (j, j) in place (lower triangle; upper zeroed), and write its inverse
+// W_jj = L_jj^{-1} to W: the panel below becomes a tile product with W_jj (gemm_panel_tiles) and
+// the triangular inverse reuses W_jj. The inverse runs four threads per column: for row r, the
+// four lanes split sum_{c <= t < r} L_rt X_tc and combine it by shuffles.
+__global__ void __launch_bounds__(256) potrf_inv_tile(double* E, double* W, int kp, int j, int32_t* err) {
+    extern __shared__ double sm[];
+    double (*S)[TP] = reinterpret_cast<double (*)[TP]>(sm);
+    double (*X)[TP] = reinterpret_cast<double (*)[TP]>(sm + T * TP);
     load_tile(S, E, kp, j, j);
     __syncthreads();
     for (int c = 0; c < T; ++c) {
@@ -206,27 +211,18 @@ __global__ void __launch_bounds__(256) potrf_tile(double* E, int kp, int j, int3
         if (t % T > t / T) S[t / T][t % T] = 0.0;
     __syncthreads();
     store_tile(S, E, kp, j, j);
-}
-
-// tiles below the diagonal: L_ij = A_ij L_jj^{-T}
-__global__ void __launch_bounds__(256) trsm_tiles(double* E, int kp, int j) {
-    extern __shared__ double sm[];
-    double (*L)[TP] = reinterpret_cast<double (*)[TP]>(sm);
-    double (*X)[TP] = reinterpret_cast<double (*)[TP]>(sm + T * TP);
-    const int i = j + 1 + blockIdx.x;
-    load_tile(L, E, kp, j, j);
-    load_tile(X, E, kp, i, j);
-    __syncthreads();
-    if (threadIdx.x < T) {
-        const int r = threadIdx.x;
-        for (int c = 0; c < T; ++c) {
-            double s = X[r][c];
-            for (int t = 0; t < c; ++t) s -= X[r][t] * L[c][t];
-            X[r][c] = s / L[c][c];
-        }
+    const int col = threadIdx.x >> 2, sub = threadIdx.x & 3;  // blockDim.x == 4 T
+    for (int r = 0; r < T; ++r) {
+        double acc = 0.0;
+        if (r > col)
+            for (int t = col + sub; t < r; t += 4) acc += S[r][t] * X[t][col];
+        acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+        acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+        if (sub == 0) X[r][col] = r < col ? 0.0 : ((r == col ? 1.0 : 0.0) - acc) / S[r][r];
+        __syncwarp();
     }
     __syncthreads();
-    store_tile(X, E, kp, i, j);
+    store_tile(X, W, kp, j, j);
 }
 
 // C (tile ci, cj of M) += alpha * sum_t A[r][t] * B[c][t]  with A, B 64x64 tiles in shared memory
@@ -264,23 +260,20 @@ __global__ void __launch_bounds__(256) syrk_tiles(double* E, int kp, int j) {
         for (int r = 0; r < 4; ++r) E[(int64_t)(i * T + ty + 16 * q) * kp + k * T + tx + 16 * r] -= acc[q][r];
 }
 
-// W_ii = L_ii^{-1}
-__global__ void __launch_bounds__(256) trtri_tile(const double* E, double* W, int kp, int i) {
+// tiles below the diagonal as tile products: L_ij = A_ij L_jj^{-T} = A_ij W_jj^T
+__global__ void __launch_bounds__(256) gemm_panel_tiles(double* E, const double* W, int kp, int j) {
     extern __shared__ double sm[];
-    double (*L)[TP] = reinterpret_cast<double (*)[TP]>(sm);
-    double (*X)[TP] = reinterpret_cast<double (*)[TP]>(sm + T * TP);
-    load_tile(L, E, kp, i, i);
+    double (*A)[TP] = reinterpret_cast<double (*)[TP]>(sm);
+    double (*B)[TP] = reinterpret_cast<double (*)[TP]>(sm + T * TP);
+    const int i = j + 1 + blockIdx.x;
+    load_tile(A, E, kp, i, j);
+    load_tile(B, W, kp, j, j);
     __syncthreads();
-    if (threadIdx.x < T) {
-        const int c = threadIdx.x;  // column c of the inverse: L x = e_c
-        for (int r = 0; r < T; ++r) {
-            double s = r == c ? 1.0 : 0.0;
-            for (int t = c; t < r; ++t) s -= L[r][t] * X[t][c];
-            X[r][c] = r < c ? 0.0 : s / L[r][r];
-        }
-    }
-    __syncthreads();
-    store_tile(X, W, kp, i, i);
+    double acc[4][4] = {{0}};
+    tile_abt(A, B, acc);  // sum_t A_ij[r][t] W_jj[c][t]
+    const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;
+    for (int q = 0; q < 4; ++q)
+        for (int r = 0; r < 4; ++r) E[(int64_t)(i * T + ty + 16 * q) * kp + j * T + tx + 16 * r] = acc[q][r];
 }
 
 // Right-looking W = L^{-1}: the strictly lower tiles of W first accumulate
@@ -343,6 +336,11 @@ __global__ void __launch_bounds__(256) inverse_tiles(const double* W, double* ei
 }  // namespace
 
 void CoarseSpace::init(mphy_ctx* ctx, const mphy_mesh* mesh, const mphy_pattern* pat, int target) {
+    if (fact_graph_) {  // a new layout: the recorded factorisation refers to the old buffers
+        MPHY_CUDA(cudaGraphExecDestroy(fact_graph_));
+        fact_graph_ = nullptr;
+    }
+    boxd_ = 0.0;
     ctx_ = ctx;
     mesh_ = mesh;
     pat_ = pat;
@@ -409,8 +407,9 @@ void CoarseSpace::setup(const SellView& A, const VT* aval, const double* disp, c
     launches = 0;
     centroid_kernel<<<std::min(n_agg_, sm * 8), 256, 0, s>>>(n_agg_, agg_ptr_.p, agg_nodes_.p, mesh_->coords.p, disp,
                                                              cent_.p);
-    double boxd = 0.0;  // box diagonal of the reference grid scales the rotation modes to O(1)
-    {
+    if (!(boxd_ > 0.0)) {
+        // box diagonal of the reference grid: scales the rotation modes to O(1) (the reference
+        // coordinates do not change, so it is computed once)
         const std::vector<double>& X = mesh_->coords_host;
         double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
         for (size_t n = 0; n < X.size() / 3; ++n)
@@ -418,45 +417,81 @@ void CoarseSpace::setup(const SellView& A, const VT* aval, const double* disp, c
                 lo[d] = std::min(lo[d], X[3 * n + d]);
                 hi[d] = std::max(hi[d], X[3 * n + d]);
             }
-        for (int d = 0; d < 3; ++d) boxd += std::pow((hi[d] - lo[d]) / ng_[d], 2);
-        boxd = std::sqrt(std::max(boxd, 1e-300));
+        double b = 0.0;
+        for (int d = 0; d < 3; ++d) b += std::pow((hi[d] - lo[d]) / ng_[d], 2);
+        boxd_ = std::sqrt(std::max(b, 1e-300));
     }
     offsets_kernel<<<stride_grid(mesh_->n_node, 256, sm), 256, 0, s>>>(mesh_->n_node, agg_.p, mesh_->coords.p, disp,
-                                                                      cent_.p, 1.0 / boxd, d_.p);
+                                                                      cent_.p, 1.0 / boxd_, d_.p);
     MPHY_CUDA(cudaMemsetAsync(E_.p, 0, E_.bytes(), s));
     MPHY_CUDA(cudaMemsetAsync(W_.p, 0, W_.bytes(), s));
     MPHY_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(int32_t), s));
     CoarseView cv = view();
     coarse_matrix_kernel<VT><<<std::min(n_agg_, sm * 8), 256, 0, s>>>(A, aval, cv, ng_[0], ng_[1], ng_[2], E_.p,
                                                                        err_.p);
-    drop_null_modes<<<1, 1024, 0, s>>>(E_.p, kp_, 6 * n_agg_);
     MPHY_CUDA(cudaGetLastError());
-    launches += 4;
+    launches += 3;
     const int nb = kp_ / T;
     const size_t sm2 = 2 * (size_t)T * TP * sizeof(double);
     static bool attr = false;
     if (!attr) {
         MPHY_CUDA(cudaFuncSetAttribute(syrk_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
-        MPHY_CUDA(cudaFuncSetAttribute(trsm_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
-        MPHY_CUDA(cudaFuncSetAttribute(trtri_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
+        MPHY_CUDA(cudaFuncSetAttribute(potrf_inv_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
+        MPHY_CUDA(cudaFuncSetAttribute(gemm_panel_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
         MPHY_CUDA(cudaFuncSetAttribute(trtri_finalize, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
         MPHY_CUDA(cudaFuncSetAttribute(trtri_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
         MPHY_CUDA(cudaFuncSetAttribute(inverse_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
         attr = true;
     }
+    // The dense part (null modes, blocked Cholesky with tile inverses, triangular inverse,
+    // E^{-1} = W^T W) is the same launch sequence on the same buffers every time: it is captured
+    // once into a CUDA graph and replayed, so the short dependent launches run back to back.
+    if (fact_graph_) {
+        MPHY_CUDA(cudaGraphLaunch(fact_graph_, s));
+        launches += fact_launches_;
+    } else {
+        const int64_t l0 = launches;
+        cudaGraph_t g = nullptr;
+        MPHY_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        try {
+            record_factorisation(s, nb, sm2);
+        } catch (...) {
+            cudaStreamEndCapture(s, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
+        MPHY_CUDA(cudaStreamEndCapture(s, &g));
+        const cudaError_t e = cudaGraphInstantiate(&fact_graph_, g, 0);
+        cudaGraphDestroy(g);
+        MPHY_CUDA(e);
+        fact_launches_ = launches - l0;
+        MPHY_CUDA(cudaGraphLaunch(fact_graph_, s));
+    }
+    MPHY_CUDA(cudaGetLastError());
+    MPHY_CUDA(cudaEventRecord(ctx_->ev1, s));
+    int32_t h = 0;
+    MPHY_CUDA(cudaMemcpyAsync(&h, err_.p, sizeof(h), cudaMemcpyDeviceToHost, s));
+    MPHY_CUDA(cudaStreamSynchronize(s));
+    cudaEventElapsedTime(&last_setup_ms, ctx_->ev0, ctx_->ev1);
+    MPHY_REQUIRE(h != 1, MPHY_ERR_UNSUPPORTED, "coarse space: an element spans more than two aggregates");
+    MPHY_REQUIRE(h != 2, MPHY_ERR_INDEFINITE, "coarse space: Z^T A Z is not positive definite");
+}
+
+void CoarseSpace::record_factorisation(cudaStream_t s, int nb, size_t sm2) {
+    drop_null_modes<<<1, 1024, 0, s>>>(E_.p, kp_, 6 * n_agg_);
+    launches += 1;
     for (int j = 0; j < nb; ++j) {
-        potrf_tile<<<1, 256, 0, s>>>(E_.p, kp_, j, err_.p);
+        potrf_inv_tile<<<1, 256, sm2, s>>>(E_.p, W_.p, kp_, j, err_.p);
         const int m = nb - j - 1;
         if (m > 0) {
-            trsm_tiles<<<m, 256, sm2, s>>>(E_.p, kp_, j);
+            gemm_panel_tiles<<<m, 256, sm2, s>>>(E_.p, W_.p, kp_, j);
             syrk_tiles<<<m * (m + 1) / 2, 256, sm2, s>>>(E_.p, kp_, j);
             launches += 2;
         }
         launches += 1;
     }
+    // W = L^{-1}: the diagonal tiles W_kk are already there (potrf_inv_tile)
     for (int k = 0; k < nb; ++k) {
-        trtri_tile<<<1, 256, sm2, s>>>(E_.p, W_.p, kp_, k);
-        launches += 1;
         if (k > 0) {
             trtri_finalize<<<k, 256, sm2, s>>>(W_.p, kp_, k);
             launches += 1;
@@ -469,13 +504,10 @@ void CoarseSpace::setup(const SellView& A, const VT* aval, const double* disp, c
     inverse_tiles<<<nb * nb, 256, sm2, s>>>(W_.p, einv_.p, kp_, nb);
     launches += 1;
     MPHY_CUDA(cudaGetLastError());
-    MPHY_CUDA(cudaEventRecord(ctx_->ev1, s));
-    int32_t h = 0;
-    MPHY_CUDA(cudaMemcpyAsync(&h, err_.p, sizeof(h), cudaMemcpyDeviceToHost, s));
-    MPHY_CUDA(cudaStreamSynchronize(s));
-    cudaEventElapsedTime(&last_setup_ms, ctx_->ev0, ctx_->ev1);
-    MPHY_REQUIRE(h != 1, MPHY_ERR_UNSUPPORTED, "coarse space: an element spans more than two aggregates");
-    MPHY_REQUIRE(h != 2, MPHY_ERR_INDEFINITE, "coarse space: Z^T A Z is not positive definite");
+}
+
+CoarseSpace::~CoarseSpace() {
+    if (fact_graph_) cudaGraphExecDestroy(fact_graph_);
 }
 
 template void CoarseSpace::setup<double>(const SellView&, const double*, const double*, cudaStream_t);

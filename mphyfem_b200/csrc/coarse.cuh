@@ -28,7 +28,13 @@ class CoarseSpace {
     int64_t launches = 0;
     float last_setup_ms = 0.f;
 
+    ~CoarseSpace();
+
   private:
+    void record_factorisation(cudaStream_t s, int nb, size_t sm2);
+    cudaGraphExec_t fact_graph_ = nullptr;
+    int64_t fact_launches_ = 0;
+    double boxd_ = 0.0;
     mphy_ctx* ctx_ = nullptr;
     const mphy_mesh* mesh_ = nullptr;
     const mphy_pattern* pat_ = nullptr;
