@@ -463,15 +463,32 @@ __global__ void __launch_bounds__(kThreads) coarse_restrict_kernel(CoarseView cv
     }
 }
 
-// c = E^{-1} w: one warp per row of the FP64 inverse
+// c = E^{-1} w: one warp per row of the FP64 inverse. Each lane reads 16-byte pairs, four
+// independent loads per step (kp is a multiple of 64, rows start 512-byte aligned), so enough
+// bytes are in flight to stream E^{-1} at HBM rate.
 __global__ void __launch_bounds__(kThreads) coarse_gemv_kernel(CoarseView cv, const PcgState* st) {
     if (st && st->done) return;
     const int lane = threadIdx.x & 31;
     for (int64_t row = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; row < cv.kp;
          row += ((int64_t)gridDim.x * blockDim.x) >> 5) {
-        const double* e = cv.einv + row * cv.kp;
-        double acc = 0.0;
-        for (int col = lane; col < cv.kp; col += 32) acc += e[col] * cv.w[col];
+        const double2* e = reinterpret_cast<const double2*>(cv.einv + row * cv.kp);
+        const double2* wv = reinterpret_cast<const double2*>(cv.w);
+        const int np = cv.kp >> 1;  // double2 per row
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+        int c = lane;
+        for (; c + 96 < np; c += 128) {
+            const double2 e0 = e[c], e1 = e[c + 32], e2 = e[c + 64], e3 = e[c + 96];
+            const double2 w0 = wv[c], w1 = wv[c + 32], w2 = wv[c + 64], w3 = wv[c + 96];
+            a0 += e0.x * w0.x + e0.y * w0.y;
+            a1 += e1.x * w1.x + e1.y * w1.y;
+            a2 += e2.x * w2.x + e2.y * w2.y;
+            a3 += e3.x * w3.x + e3.y * w3.y;
+        }
+        for (; c < np; c += 32) {
+            const double2 e0 = e[c], w0 = wv[c];
+            a0 += e0.x * w0.x + e0.y * w0.y;
+        }
+        double acc = (a0 + a1) + (a2 + a3);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
         if (lane == 0) cv.c[row] = acc;
