@@ -212,7 +212,8 @@ def _method_name(args):
               "mixed_tc": "mixed FP32/FP64 (tensor-core split-BF16 tangent)"}[args.precision],
              {"jacobi": "Jacobi", "fsai": "FSAI", "learned": "learned FSAI"}[args.pc]]
     if args.coarse > 0:
-        parts.append(f"+ rigid-body coarse space ({args.coarse} aggregates)")
+        kind = "linear-mode" if args.coarse_modes == 12 else "rigid-body"
+        parts.append(f"+ {kind} coarse space ({args.coarse} aggregates x {args.coarse_modes} modes)")
     return " ".join(parts) + "-PCG"
 
 
@@ -226,6 +227,7 @@ def _make_solver(api, _lib, mesh, pat, args, precision, pc, coarse):
                         pc_type={"jacobi": _lib.PC_JACOBI, "fsai": _lib.PC_FSAI,
                                  "learned": _lib.PC_FSAI_LEARNED}[pc],
                         inner_rtol=args.inner_rtol, max_outer=args.max_outer, coarse_aggregates=coarse,
+                        coarse_modes=args.coarse_modes,
                         norm_type=args.norm)
     if pc == "learned":
         from mphyfem_b200 import learned
@@ -469,6 +471,8 @@ def main():
                     help="Krylov stopping norm: 1 = true residual ||b - Ax|| <= rtol ||b|| (every method compared "
                          "at the same accuracy), 0 = PETSc's preconditioned-residual default")
     ap.add_argument("--coarse", type=int, default=512, help="aggregates of the two-level coarse correction (0: off)")
+    ap.add_argument("--coarse-modes", dest="coarse_modes", type=int, default=6, choices=[6, 12],
+                    help="modes per aggregate: 6 rigid-body, 12 linear displacement")
     ap.add_argument("--no-plain", dest="no_plain", action="store_true",
                     help="skip the same-run measurement of the plain FP64 Jacobi-PCG method")
     ap.add_argument("--max-it", dest="max_it", type=int, default=20000)

@@ -97,6 +97,11 @@ typedef struct mphy_solver_opts {
                                 * preconditioner (Jacobi: D^{-1}, FSAI: G^T G) */
     int32_t norm_type;     /* KSP norm of the convergence test: 0 = preconditioned ||z|| (PETSc's
                             * CG default), 1 = unpreconditioned ||r|| (true residual vs ||b||) */
+    int32_t coarse_modes;  /* modes per aggregate of the coarse correction: 6 (0 = default:
+                            * translations and rotations about the aggregate's centroid) or 12
+                            * (linear displacement u = a + B (x - x_c): translations, stretches,
+                            * shears and rotations; a richer space of the same size at half the
+                            * aggregates) */
 } mphy_solver_opts;
 
 typedef struct mphy_newton_opts {
@@ -356,7 +361,8 @@ typedef struct mphy_mixed_opts {
     int32_t max_it;             /* MINRES iterations per solve */
     double rtol;                /* MINRES relative tolerance */
     int32_t coarse_aggregates;  /* > 0: the displacement block of the preconditioner adds the
-                                 * rigid-body coarse space over about this many aggregates */
+                                 * coarse space over about this many aggregates */
+    int32_t coarse_modes;       /* 6 (0 = default) or 12, as in mphy_solver_opts */
 } mphy_mixed_opts;
 void mphy_mixed_opts_default(mphy_mixed_opts* opts); /* reference tangent, 20000, 1e-10, 0 */
 /* mesh: tet10 (npe = 10); pattern: mphy_pattern_build of the same mesh. opts may be NULL. */

@@ -390,7 +390,7 @@ class MixedSolidGpu:
     the GPU: two-field assembly, MINRES solve and Newton load stepping (mphy_mixed_*)."""
 
     def __init__(self, prob, ctx: Context | None = None, tangent: int = L.TANGENT_REFERENCE, rtol: float = 1e-10,
-                 max_it: int = 20000, coarse_aggregates: int = 0):
+                 max_it: int = 20000, coarse_aggregates: int = 0, coarse_modes: int = 0):
         self.prob = prob
         self.ctx = ctx or Context(0)
         self.lib = self.ctx.lib
@@ -398,7 +398,8 @@ class MixedSolidGpu:
         self.pattern = Pattern(self.mesh)
         o = L.MixedOpts()
         self.lib.mphy_mixed_opts_default(C.byref(o))
-        o.tangent, o.rtol, o.max_it, o.coarse_aggregates = tangent, rtol, max_it, coarse_aggregates
+        o.tangent, o.rtol, o.max_it, o.coarse_aggregates, o.coarse_modes = (tangent, rtol, max_it, coarse_aggregates,
+                                                                             coarse_modes)
         h = C.c_void_p()
         L.check(self.lib.mphy_mixed_create(self.ctx.h, self.mesh.h, self.pattern.h, C.byref(o), C.byref(h)))
         self.h = h

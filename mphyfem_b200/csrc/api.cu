@@ -676,7 +676,7 @@ int mphy_solver_create(mphy_ctx* c, const mphy_mesh* m, const mphy_pattern* P, c
             }
             if (o.coarse_aggregates > 0) {
                 s->use_coarse = true;
-                s->coarse.init(c, m, P, o.coarse_aggregates);
+                s->coarse.init(c, m, P, o.coarse_aggregates, o.coarse_modes > 0 ? o.coarse_modes : 6);
                 const CoarseView cv = s->coarse.view();
                 if (o.precision == MPHY_PREC_MIXED || o.precision == MPHY_PREC_MIXED_TC) s->ir.inner().set_coarse(cv);
                 else if (o.precision == MPHY_PREC_MIXED_F32VEC) s->ir32.inner().set_coarse(cv);

@@ -148,6 +148,100 @@ __global__ void __launch_bounds__(256) coarse_matrix_kernel(SellView A, const VT
     }
 }
 
+// E = Z^T A Z for the twelve linear-displacement modes u = a + B d of every aggregate (columns
+// a_0..a_2, then B_ck at 3 + 3c + k). With Z_n's rows e_r (x) (1, d_n), the product needs no Z
+// matrix: T[r][j] = sum_m (A_nm Z_m)[r][j] is accumulated per neighbour-aggregate run, and
+// E[i][j] += (Z_n^T T)[i][j] = T[i][j] (i < 3) or d_n,k T[c][j] (i = 3 + 3c + k). Rows and
+// columns of prescribed DOFs drop out (their Z rows are zero).
+template <typename VT>
+__global__ void __launch_bounds__(256) coarse_matrix_linear_kernel(SellView A, const VT* __restrict__ aval,
+                                                                   CoarseView cv, int ngx, int ngy, int ngz,
+                                                                   double* __restrict__ E, int32_t* err) {
+    __shared__ double Eloc[27][144];
+    for (int a = blockIdx.x; a < cv.n_agg; a += gridDim.x) {
+        for (int i = threadIdx.x; i < 27 * 144; i += blockDim.x) (&Eloc[0][0])[i] = 0.0;
+        __syncthreads();
+        const int ax = a % ngx, ay = (a / ngx) % ngy, az = a / (ngx * ngy);
+        for (int64_t i = cv.agg_ptr[a] + threadIdx.x; i < cv.agg_ptr[a + 1]; i += blockDim.x) {
+            const int64_t n = cv.agg_nodes[i];
+            const double dn[3] = {cv.d[3 * n], cv.d[3 * n + 1], cv.d[3 * n + 2]};
+            const bool fn[3] = {cv.fixed[3 * n] != 0, cv.fixed[3 * n + 1] != 0, cv.fixed[3 * n + 2] != 0};
+            const int64_t s = n >> 5;
+            const int lane = (int)(n & 31);
+            const int64_t base = A.slice_base[s];
+            const int w = A.slice_width[s];
+            double T[3][12];
+            for (int r = 0; r < 3; ++r)
+                for (int j = 0; j < 12; ++j) T[r][j] = 0.0;
+            int cur = -1;
+            auto flush = [&](int slot) {
+                for (int r = 0; r < 3; ++r) {
+                    if (fn[r]) continue;
+                    for (int j = 0; j < 12; ++j) {
+                        const double t = T[r][j];
+                        if (t == 0.0) continue;
+                        atomicAdd(&Eloc[slot][12 * r + j], t);
+                        for (int k = 0; k < 3; ++k)
+                            if (dn[k] != 0.0) atomicAdd(&Eloc[slot][12 * (3 + 3 * r + k) + j], dn[k] * t);
+                    }
+                }
+                for (int r = 0; r < 3; ++r)
+                    for (int j = 0; j < 12; ++j) T[r][j] = 0.0;
+            };
+            for (int k = 0; k <= w; ++k) {
+                double blk[9];
+                int64_t m;
+                if (k < w) {
+                    m = A.col[base + 32 * (int64_t)k + lane];
+                    const VT* v = aval + 9 * (base + 32 * (int64_t)k) + lane;
+                    bool any = false;
+                    for (int q = 0; q < 9; ++q) {
+                        blk[q] = (double)v[32 * q];
+                        any |= blk[q] != 0.0;
+                    }
+                    if (!any) continue;
+                } else {
+                    if (!A.diag64) break;  // the FP32 storage keeps the diagonal blocks apart
+                    m = n;
+                    for (int q = 0; q < 9; ++q) blk[q] = A.diag64[9 * n + q];
+                }
+                for (int q = 0; q < 9; ++q)
+                    if (cv.fixed[3 * m + q % 3]) blk[q] = 0.0;  // prescribed columns: zero Z rows of m
+                const int b = cv.agg[m];
+                const int dx = b % ngx - ax, dy = (b / ngx) % ngy - ay, dz = b / (ngx * ngy) - az;
+                if (dx < -1 || dx > 1 || dy < -1 || dy > 1 || dz < -1 || dz > 1) {
+                    atomicExch(err, 1);
+                    continue;
+                }
+                const int slot = (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1);
+                if (slot != cur) {
+                    if (cur >= 0) flush(cur);
+                    cur = slot;
+                }
+                const double dm[3] = {cv.d[3 * m], cv.d[3 * m + 1], cv.d[3 * m + 2]};
+                for (int r = 0; r < 3; ++r)
+                    for (int c = 0; c < 3; ++c) {
+                        const double av = blk[3 * r + c];
+                        T[r][c] += av;
+                        T[r][3 + 3 * c] += av * dm[0];
+                        T[r][4 + 3 * c] += av * dm[1];
+                        T[r][5 + 3 * c] += av * dm[2];
+                    }
+            }
+            if (cur >= 0) flush(cur);
+        }
+        __syncthreads();
+        for (int t = threadIdx.x; t < 27 * 144; t += blockDim.x) {
+            const int slot = t / 144, q = t % 144;
+            const int bx = ax + slot % 3 - 1, by = ay + (slot / 3) % 3 - 1, bz = az + slot / 9 - 1;
+            if (bx < 0 || bx >= ngx || by < 0 || by >= ngy || bz < 0 || bz >= ngz) continue;
+            const int b = bx + ngx * (by + ngy * bz);
+            E[(int64_t)(12 * a + q / 12) * cv.kp + 12 * b + q % 12] = Eloc[slot][q];
+        }
+        __syncthreads();
+    }
+}
+
 // modes that vanish on the free DOFs (an aggregate of prescribed nodes) and the padding become
 // identity rows: their correction is zero
 __global__ void drop_null_modes(double* __restrict__ E, int kp, int k) {
@@ -335,7 +429,10 @@ __global__ void __launch_bounds__(256) inverse_tiles(const double* W, double* ei
 
 }  // namespace
 
-void CoarseSpace::init(mphy_ctx* ctx, const mphy_mesh* mesh, const mphy_pattern* pat, int target) {
+void CoarseSpace::init(mphy_ctx* ctx, const mphy_mesh* mesh, const mphy_pattern* pat, int target, int modes) {
+    MPHY_REQUIRE(modes == 6 || modes == 12, MPHY_ERR_INVALID_ARG,
+                 "coarse space: 6 (rigid-body) or 12 (linear) modes per aggregate");
+    nm_ = modes;
     if (fact_graph_) {  // a new layout: the recorded factorisation refers to the old buffers
         MPHY_CUDA(cudaGraphExecDestroy(fact_graph_));
         fact_graph_ = nullptr;
@@ -366,7 +463,7 @@ void CoarseSpace::init(mphy_ctx* ctx, const mphy_mesh* mesh, const mphy_pattern*
         ng_[d] = std::max(g, 1);
     }
     n_agg_ = ng_[0] * ng_[1] * ng_[2];
-    kp_ = ((6 * n_agg_ + T - 1) / T) * T;
+    kp_ = ((nm_ * n_agg_ + T - 1) / T) * T;
     MPHY_REQUIRE(kp_ <= 16384, MPHY_ERR_UNSUPPORTED, "coarse space larger than 16384");
     std::vector<int32_t> agg(nn), cnt(n_agg_, 0);
     for (int32_t n = 0; n < nn; ++n) {
@@ -427,8 +524,12 @@ void CoarseSpace::setup(const SellView& A, const VT* aval, const double* disp, c
     MPHY_CUDA(cudaMemsetAsync(W_.p, 0, W_.bytes(), s));
     MPHY_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(int32_t), s));
     CoarseView cv = view();
-    coarse_matrix_kernel<VT><<<std::min(n_agg_, sm * 8), 256, 0, s>>>(A, aval, cv, ng_[0], ng_[1], ng_[2], E_.p,
-                                                                       err_.p);
+    if (nm_ == 12)
+        coarse_matrix_linear_kernel<VT><<<std::min(n_agg_, sm * 8), 256, 0, s>>>(A, aval, cv, ng_[0], ng_[1], ng_[2],
+                                                                                  E_.p, err_.p);
+    else
+        coarse_matrix_kernel<VT><<<std::min(n_agg_, sm * 8), 256, 0, s>>>(A, aval, cv, ng_[0], ng_[1], ng_[2], E_.p,
+                                                                           err_.p);
     MPHY_CUDA(cudaGetLastError());
     launches += 3;
     const int nb = kp_ / T;
@@ -478,7 +579,7 @@ void CoarseSpace::setup(const SellView& A, const VT* aval, const double* disp, c
 }
 
 void CoarseSpace::record_factorisation(cudaStream_t s, int nb, size_t sm2) {
-    drop_null_modes<<<1, 1024, 0, s>>>(E_.p, kp_, 6 * n_agg_);
+    drop_null_modes<<<1, 1024, 0, s>>>(E_.p, kp_, nm_ * n_agg_);
     launches += 1;
     for (int j = 0; j < nb; ++j) {
         potrf_inv_tile<<<1, 256, sm2, s>>>(E_.p, W_.p, kp_, j, err_.p);
@@ -516,7 +617,8 @@ template void CoarseSpace::setup<float>(const SellView&, const float*, const dou
 CoarseView CoarseSpace::view() const {
     CoarseView v;
     v.n_agg = n_agg_;
-    v.k = 6 * n_agg_;
+    v.nm = nm_;
+    v.k = nm_ * n_agg_;
     v.kp = kp_;
     v.agg = agg_.p;
     v.agg_ptr = agg_ptr_.p;

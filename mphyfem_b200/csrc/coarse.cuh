@@ -16,14 +16,17 @@ class CoarseSpace {
   public:
     // Aggregates: a grid of boxes over the bounding box of the reference coordinates with about
     // target_aggregates boxes, as close to cubes as the box allows.
-    void init(mphy_ctx* ctx, const mphy_mesh* mesh, const mphy_pattern* pat, int target_aggregates);
+    // modes: 6 (rigid-body: translations and rotations about the box centroid) or 12 (linear
+    // displacement u = a + B d: translations, stretches, shears and rotations)
+    void init(mphy_ctx* ctx, const mphy_mesh* mesh, const mphy_pattern* pat, int target_aggregates, int modes = 6);
     // Modes from the current coordinates X + disp (disp may be null), E = Z^T A Z, its Cholesky
     // factor and inverse, all FP64.
     template <typename VT>
     void setup(const SellView& A, const VT* aval, const double* disp, cudaStream_t s);
     CoarseView view() const;
     int n_agg() const { return n_agg_; }
-    int coarse_size() const { return 6 * n_agg_; }
+    int coarse_size() const { return nm_ * n_agg_; }
+    int modes() const { return nm_; }
     const int* grid() const { return ng_; }
     int64_t launches = 0;
     float last_setup_ms = 0.f;
@@ -35,6 +38,7 @@ class CoarseSpace {
     cudaGraphExec_t fact_graph_ = nullptr;
     int64_t fact_launches_ = 0;
     double boxd_ = 0.0;
+    int nm_ = 6;
     mphy_ctx* ctx_ = nullptr;
     const mphy_mesh* mesh_ = nullptr;
     const mphy_pattern* pat_ = nullptr;

@@ -1,4 +1,4 @@
-// coarse_view.cuh -- device view of the rigid-body coarse space (see coarse.cuh).
+// coarse_view.cuh -- device view of the geometric coarse space (see coarse.cuh).
 #pragma once
 #include <stdint.h>
 
@@ -6,7 +6,8 @@ namespace mphy {
 
 struct CoarseView {
     int32_t n_agg;           // aggregates (boxes)
-    int32_t k;               // coarse size 6 n_agg (padded to kp in storage)
+    int32_t nm;              // modes per aggregate: 6 (rigid body) or 12 (linear displacement)
+    int32_t k;               // coarse size nm n_agg (padded to kp in storage)
     int32_t kp;              // padded size (multiple of 64)
     const int32_t* agg;      // [n_node] aggregate of every node
     const int64_t* agg_ptr;  // [n_agg+1] nodes of every aggregate (in agg_nodes)
@@ -20,5 +21,24 @@ struct CoarseView {
     double* w;               // [kp] restriction Z^T r
     double* c;               // [kp] coarse correction E^{-1} w
 };
+
+#ifdef __CUDACC__
+// The coarse field at node n, (Z c)_n, with d the node's scaled offset from its aggregate's
+// centroid. Rigid-body modes: c = (translation t, rotations w) and u = t + w x d with the
+// mode order of the restriction; linear modes: c = (a, B row-major) and u = a + B d.
+__device__ __forceinline__ void coarse_node_value(const CoarseView& cv, int64_t n, double zc[3]) {
+    const double dx = cv.d[3 * n], dy = cv.d[3 * n + 1], dz = cv.d[3 * n + 2];
+    if (cv.nm == 12) {
+        const double* c = cv.c + 12 * (int64_t)cv.agg[n];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) zc[a] = c[a] + c[3 + 3 * a] * dx + c[4 + 3 * a] * dy + c[5 + 3 * a] * dz;
+    } else {
+        const double* c = cv.c + 6 * (int64_t)cv.agg[n];
+        zc[0] = c[0] - dy * c[3] + dz * c[5];
+        zc[1] = c[1] + dx * c[3] - dz * c[4];
+        zc[2] = c[2] + dy * c[4] - dx * c[5];
+    }
+}
+#endif
 
 }  // namespace mphy

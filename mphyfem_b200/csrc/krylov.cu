@@ -265,11 +265,11 @@ __global__ void __launch_bounds__(kThreads) factor_apply_kernel(SellView A, Coar
         }
         if (row < A.n_node) {
             if (cv.n_agg > 0) {  // two-level: + Z c
-                const double* c = cv.c + 6 * (int64_t)cv.agg[row];
-                const double dx = cv.d[3 * row], dy = cv.d[3 * row + 1], dz = cv.d[3 * row + 2];
-                if (!cv.fixed[3 * row]) y0 += (Acc)(c[0] - dy * c[3] + dz * c[5]);
-                if (!cv.fixed[3 * row + 1]) y1 += (Acc)(c[1] + dx * c[3] - dz * c[4]);
-                if (!cv.fixed[3 * row + 2]) y2 += (Acc)(c[2] + dy * c[4] - dx * c[5]);
+                double zc[3];
+                coarse_node_value(cv, row, zc);
+                if (!cv.fixed[3 * row]) y0 += (Acc)zc[0];
+                if (!cv.fixed[3 * row + 1]) y1 += (Acc)zc[1];
+                if (!cv.fixed[3 * row + 2]) y2 += (Acc)zc[2];
             }
             const XT zz[3] = {(XT)y0, (XT)y1, (XT)y2};
 #pragma unroll
@@ -441,8 +441,9 @@ __global__ void __launch_bounds__(kThreads) coarse_restrict_kernel(CoarseView cv
                                                                    const PcgState* st) {
     __shared__ double sh[32];
     if (st && st->done) return;
+    const bool lin = cv.nm == 12;
     for (int a = blockIdx.x; a < cv.n_agg; a += gridDim.x) {
-        double w[6] = {0, 0, 0, 0, 0, 0};
+        double w[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
         for (int64_t i = cv.agg_ptr[a] + threadIdx.x; i < cv.agg_ptr[a + 1]; i += blockDim.x) {
             const int64_t n = cv.agg_nodes[i];
             const double rx = cv.fixed[3 * n] ? 0.0 : (double)r[3 * n];
@@ -452,13 +453,22 @@ __global__ void __launch_bounds__(kThreads) coarse_restrict_kernel(CoarseView cv
             w[0] += rx;
             w[1] += ry;
             w[2] += rz;
-            w[3] += -dy * rx + dx * ry;
-            w[4] += -dz * ry + dy * rz;
-            w[5] += dz * rx - dx * rz;
+            if (lin) {  // Z^T r for u = a + B d: w(a) = r, w(B_ck) = r_c d_k
+                const double rr[3] = {rx, ry, rz}, dd[3] = {dx, dy, dz};
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) w[3 + 3 * c + k] += rr[c] * dd[k];
+            } else {
+                w[3] += -dy * rx + dx * ry;
+                w[4] += -dz * ry + dy * rz;
+                w[5] += dz * rx - dx * rz;
+            }
         }
-        for (int j = 0; j < 6; ++j) {
+        const int nm = lin ? 12 : 6;
+        for (int j = 0; j < nm; ++j) {
             const double t = block_sum(w[j], sh);
-            if (threadIdx.x == 0) cv.w[6 * a + j] = t;
+            if (threadIdx.x == 0) cv.w[nm * a + j] = t;
         }
     }
 }
@@ -509,9 +519,8 @@ __global__ void __launch_bounds__(kThreads) coarse_final_kernel(int32_t n_node, 
     const bool unprec = INIT ? norm_type == 1 : st->norm_type == 1;
     double a1 = 0.0, a2 = 0.0;
     for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < n_node; n += (int64_t)gridDim.x * blockDim.x) {
-        const double* c = cv.c + 6 * (int64_t)cv.agg[n];
-        const double dx = cv.d[3 * n], dy = cv.d[3 * n + 1], dz = cv.d[3 * n + 2];
-        const double zc[3] = {c[0] - dy * c[3] + dz * c[5], c[1] + dx * c[3] - dz * c[4], c[2] + dy * c[4] - dx * c[5]};
+        double zc[3];
+        coarse_node_value(cv, n, zc);
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             const int64_t i = 3 * n + a;
@@ -671,9 +680,8 @@ namespace {
 // z_u += Z c on the free displacement DOFs (the prolongation of the coarse correction)
 __global__ void __launch_bounds__(kThreads) coarse_prolong_add_kernel(int32_t n_node, CoarseView cv, double* z) {
     for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < n_node; n += (int64_t)gridDim.x * blockDim.x) {
-        const double* c = cv.c + 6 * (int64_t)cv.agg[n];
-        const double dx = cv.d[3 * n], dy = cv.d[3 * n + 1], dz = cv.d[3 * n + 2];
-        const double zc[3] = {c[0] - dy * c[3] + dz * c[5], c[1] + dx * c[3] - dz * c[4], c[2] + dy * c[4] - dx * c[5]};
+        double zc[3];
+        coarse_node_value(cv, n, zc);
 #pragma unroll
         for (int a = 0; a < 3; ++a)
             if (!cv.fixed[3 * n + a]) z[3 * n + a] += zc[a];

@@ -434,6 +434,7 @@ void mphy_mixed_opts_default(mphy_mixed_opts* o) {
     o->max_it = 20000;
     o->rtol = 1e-10;
     o->coarse_aggregates = 0;
+    o->coarse_modes = 0;
 }
 
 int mphy_mixed_create(mphy_ctx* c, const mphy_mesh* mesh, const mphy_pattern* pat, const mphy_mixed_opts* o,
@@ -538,7 +539,8 @@ int mphy_mixed_create(mphy_ctx* c, const mphy_mesh* mesh, const mphy_pattern* pa
             MPHY_CUDA(cudaMemsetAsync(m->counter.p, 0, sizeof(uint32_t), st));
             m->bad.alloc(1);
             if (m->opts.coarse_aggregates > 0) {
-                m->coarse.init(c, mesh, pat, m->opts.coarse_aggregates);
+                m->coarse.init(c, mesh, pat, m->opts.coarse_aggregates,
+                               m->opts.coarse_modes > 0 ? m->opts.coarse_modes : 6);
                 m->use_coarse = true;
             }
             MPHY_CUDA(cudaStreamSynchronize(st));

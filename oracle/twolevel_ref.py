@@ -1,7 +1,7 @@
 """Numpy restatement of the two-level additive preconditioner
     M^{-1} = D^{-1} + Z (Z^T A Z)^{-1} Z^T
-with Z the six rigid-body modes of every box of a regular grid of boxes over the reference
-coordinates (zero on prescribed DOFs). Test infrastructure only: the checker for
+with Z the six rigid-body modes (or the twelve linear-displacement modes) of every box of a
+regular grid of boxes over the reference coordinates (zero on prescribed DOFs). Test infrastructure only: the checker for
 mphyfem_b200/csrc/coarse.cu and the coarse path of csrc/krylov.cu. The reference has no such
 preconditioner (its PC comes from PETSc options, src/mySolvers/SolverPetsc.cpp:117-140).
 """
@@ -20,7 +20,11 @@ def aggregates(coords, grid):
     return c[:, 0] + g[0] * (c[:, 1] + g[1] * c[:, 2]), L / g
 
 
-def prolongation(coords, fixed, grid):
+def prolongation(coords, fixed, grid, modes=6):
+    """Z: 6 rigid-body modes per box (translations, rotations about the centroid), or 12 linear
+    modes u = a + B d (a at columns 0..2, B_ck at 3 + 3c + k), d = (x - centroid) / box diagonal."""
+    if modes == 12:
+        return _prolongation_linear(coords, fixed, grid)
     agg, box = aggregates(coords, grid)
     n_agg = int(np.prod(grid))
     boxd = np.sqrt((box ** 2).sum())
@@ -43,9 +47,33 @@ def prolongation(coords, fixed, grid):
     return sp.diags((np.asarray(fixed) == 0).astype(float)) @ Z
 
 
-def preconditioner(A, coords, fixed, grid):
+def _prolongation_linear(coords, fixed, grid):
+    agg, box = aggregates(coords, grid)
+    n_agg = int(np.prod(grid))
+    boxd = np.sqrt((box ** 2).sum())
+    cent = np.zeros((n_agg, 3))
+    np.add.at(cent, agg, coords)
+    cnt = np.bincount(agg, minlength=n_agg)
+    cent /= np.maximum(cnt, 1)[:, None]
+    d = (coords - cent[agg]) / boxd
+    n = coords.shape[0]
+    rows, cols, vals = [], [], []
+    for comp in range(3):
+        rows.append(3 * np.arange(n) + comp)
+        cols.append(12 * agg + comp)
+        vals.append(np.ones(n))
+        for k in range(3):
+            rows.append(3 * np.arange(n) + comp)
+            cols.append(12 * agg + 3 + 3 * comp + k)
+            vals.append(d[:, k])
+    Z = sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
+                      shape=(3 * n, 12 * n_agg))
+    return sp.diags((np.asarray(fixed) == 0).astype(float)) @ Z
+
+
+def preconditioner(A, coords, fixed, grid, modes=6):
     """Returns a function r -> M^{-1} r (A: the node-major operator with identity prescribed rows)."""
-    Z = prolongation(coords, fixed, grid)
+    Z = prolongation(coords, fixed, grid, modes)
     E = (Z.T @ A @ Z).toarray()
     dg = np.diag(E)
     keep = dg > 1e-13 * dg.max()

@@ -1,4 +1,4 @@
-"""Two-level rigid-body coarse correction against its numpy restatement and the FP64 oracle.
+"""Two-level coarse correction (rigid-body or linear modes) against its numpy restatement and the FP64 oracle.
 
 Same aggregate grid on both sides: iteration counts agree within 3 % (summation order only);
 solutions agree with the oracle's FP64 CG to 1e-9 (FP64 path) at rtol 1e-12, and the coarse
@@ -31,13 +31,14 @@ def _solve(api, _lib, ctx, p, torch, **opts):
     return sol, pat, rc, its, sol.solution().cpu().numpy()
 
 
+@pytest.mark.parametrize("modes", [6, 12])
 @pytest.mark.parametrize("mk", [meshgen.cantilever_small,
                                 lambda: meshgen.two_phase_inclusions(32, 8, 8, seed=23, r_range=(0.1, 0.25))])
-def test_coarse_matches_restatement_and_oracle(env, oracle, mk):
+def test_coarse_matches_restatement_and_oracle(env, oracle, mk, modes):
     from oracle import fsai_ref, twolevel_ref
     torch, api, _lib, ctx = env
     p = mk()
-    sol, pat, rc, its, x = _solve(api, _lib, ctx, p, torch, rtol=1e-12, coarse_aggregates=24)
+    sol, pat, rc, its, x = _solve(api, _lib, ctx, p, torch, rtol=1e-12, coarse_aggregates=24, coarse_modes=modes)
     assert rc == 0
     info = sol.coarse_info()
     _, _, _, itj, _ = _solve(api, _lib, ctx, p, torch, rtol=1e-12)
@@ -49,7 +50,8 @@ def test_coarse_matches_restatement_and_oracle(env, oracle, mk):
     assert np.linalg.norm(x[free] - xo) <= 1e-9 * np.linalg.norm(xo)
     _, _, rp, col = op.pattern()
     A = fsai_ref.full_operator(p.n_node, p.fixed, rp, col, val)
-    Minv = twolevel_ref.preconditioner(A, p.coords, p.fixed, info["grid"])
+    assert info["coarse_size"] == modes * int(np.prod(info["grid"]))
+    Minv = twolevel_ref.preconditioner(A, p.coords, p.fixed, info["grid"], modes)
     _, its_ref = twolevel_ref.pcg(A, 0.2 * p.fnodal * (p.fixed == 0), Minv, rtol=1e-12)
     assert abs(its - its_ref) <= max(2, 0.03 * its_ref), (its, its_ref)
 
@@ -65,3 +67,17 @@ def test_coarse_mixed_and_newton(env):
     g = np.load(__import__("os").path.join(__import__("os").path.dirname(__file__), "golden", "cantilever_32x8x8.npz"))
     assert res.status == 0
     assert np.abs(res.disp - g["newton_consistent_u"]).max() <= 1e-8 * np.abs(g["newton_consistent_u"]).max()
+
+
+def test_linear_modes_need_fewer_iterations(env):
+    # the linear-displacement space contains the rigid-body one: at equal aggregates it can only
+    # help, and at equal coarse size (half the aggregates) it still beats it on the cantilever
+    torch, api, _lib, ctx = env
+    p = meshgen.hex8_cantilever(64, 16, 16)
+    its = {}
+    for agg, modes in ((64, 6), (64, 12), (32, 12)):
+        _, _, rc, it, _ = _solve(api, _lib, ctx, p, torch, rtol=1e-10, coarse_aggregates=agg, coarse_modes=modes,
+                                 norm_type=1)
+        assert rc == 0
+        its[(agg, modes)] = it
+    assert its[(64, 12)] < its[(64, 6)], its
