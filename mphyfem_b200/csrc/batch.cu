@@ -710,11 +710,10 @@ BatchView batch_view(mphy_batch* b, const uint8_t* active, bool totals, int maxi
 template <typename VT, bool COARSE>
 void launch_pcg(mphy_batch* b, const VT* val, const BatchView& v, cudaStream_t st, int cluster, int threads) {
     const size_t dyn = COARSE ? sizeof(CoarseSmem) : 0;
-    static bool smem_set = false;
-    if (COARSE && !smem_set) {
+    static std::atomic<uint64_t> smem_set{0};
+    if (COARSE && first_use_on_device(smem_set)) {
         MPHY_CUDA(cudaFuncSetAttribute(batch_pcg_kernel<VT, COARSE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)dyn));
-        smem_set = true;
     }
     cudaLaunchConfig_t cfg{};
     cudaLaunchAttribute attr[1];

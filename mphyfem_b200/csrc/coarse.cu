@@ -534,15 +534,14 @@ void CoarseSpace::setup(const SellView& A, const VT* aval, const double* disp, c
     launches += 3;
     const int nb = kp_ / T;
     const size_t sm2 = 2 * (size_t)T * TP * sizeof(double);
-    static bool attr = false;
-    if (!attr) {
+    static std::atomic<uint64_t> attr{0};
+    if (first_use_on_device(attr)) {
         MPHY_CUDA(cudaFuncSetAttribute(syrk_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
         MPHY_CUDA(cudaFuncSetAttribute(potrf_inv_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
         MPHY_CUDA(cudaFuncSetAttribute(gemm_panel_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
         MPHY_CUDA(cudaFuncSetAttribute(trtri_finalize, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
         MPHY_CUDA(cudaFuncSetAttribute(trtri_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
         MPHY_CUDA(cudaFuncSetAttribute(inverse_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
-        attr = true;
     }
     // The dense part (null modes, blocked Cholesky with tile inverses, triangular inverse,
     // E^{-1} = W^T W) is the same launch sequence on the same buffers every time: it is captured

@@ -1,6 +1,7 @@
 // common.cuh -- shared internals of libmphy.so: status plumbing, device buffers, handle structs.
 #pragma once
 
+#include <atomic>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -77,6 +78,17 @@ inline unsigned ceil_div(size_t a, size_t b) { return (unsigned)((a + b - 1) / b
 // ---------------------------------------------------------------------------------------------
 // Handle structs (opaque in the C ABI)
 // ---------------------------------------------------------------------------------------------
+namespace mphy {
+// True the first time it is called for the current device with this mask: kernel attributes
+// (cudaFuncSetAttribute) are per device, so a process that drives several GPUs sets them on each.
+inline bool first_use_on_device(std::atomic<uint64_t>& mask) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return true;
+    const uint64_t bit = 1ull << dev;
+    return (mask.fetch_or(bit) & bit) == 0;
+}
+}  // namespace mphy
+
 struct mphy_ctx {
     int device = 0;
     int sm_count = 148;

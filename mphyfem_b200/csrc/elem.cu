@@ -325,11 +325,10 @@ __global__ void __launch_bounds__(kEpb * NPE) elem_fp64_kernel(ElemArgs a) {
 template <int NPE, int MODE>
 void launch_fp64(const ElemArgs& a, cudaStream_t s) {
     const size_t smem = kEpb * sizeof(ElemSmem<NPE, ElemTraits<NPE>::NGP>);
-    static bool configured = false;
-    if (!configured) {
+    static std::atomic<uint64_t> configured{0};
+    if (first_use_on_device(configured)) {
         MPHY_CUDA(cudaFuncSetAttribute(elem_fp64_kernel<NPE, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem));
-        configured = true;
     }
     const unsigned grid = ceil_div((size_t)a.n_elem, kEpb);
     if (grid == 0) return;

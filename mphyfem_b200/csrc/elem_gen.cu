@@ -230,11 +230,10 @@ template <int NPE, int MODE>
 void launch_gen(const ElemArgs& a, cudaStream_t s) {
     constexpr int TPE = NPE * ((NPE + kGenCh - 1) / kGenCh);
     const size_t smem = kGenEpb * sizeof(GenSmem<NPE>);
-    static bool configured = false;
-    if (!configured) {
+    static std::atomic<uint64_t> configured{0};
+    if (first_use_on_device(configured)) {
         MPHY_CUDA(cudaFuncSetAttribute(elem_gen_kernel<NPE, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem));
-        configured = true;
     }
     const unsigned grid = ceil_div((size_t)a.n_elem, kGenEpb);
     if (grid == 0) return;
@@ -467,10 +466,9 @@ __global__ void __launch_bounds__(kGenEpb * 30) elem_mixed_kernel(MixedElemArgs 
 template <int MODE>
 void launch_mixed(const MixedElemArgs& a, cudaStream_t s) {
     const size_t smem = kGenEpb * sizeof(MixedSmem);
-    static bool configured = false;
-    if (!configured) {
+    static std::atomic<uint64_t> configured{0};
+    if (first_use_on_device(configured)) {
         MPHY_CUDA(cudaFuncSetAttribute(elem_mixed_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        configured = true;
     }
     const unsigned grid = ceil_div((size_t)a.base.n_elem, kGenEpb);
     if (grid == 0) return;

@@ -328,11 +328,10 @@ __global__ void __launch_bounds__(kTcThreads, 2) elem_tc_kernel(ElemArgs a) {
 template <int NPE, int MODE>
 void launch_tc(const ElemArgs& a, cudaStream_t s) {
     const size_t smem = kTcEpb * sizeof(TcSmem<NPE, TcTraits<NPE>::NGP>);
-    static bool configured = false;
-    if (!configured) {
+    static std::atomic<uint64_t> configured{0};
+    if (first_use_on_device(configured)) {
         MPHY_CUDA(cudaFuncSetAttribute(elem_tc_kernel<NPE, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem));
-        configured = true;
     }
     const unsigned grid = (unsigned)((a.n_elem + kTcEpb - 1) / kTcEpb);
     if (grid == 0) return;

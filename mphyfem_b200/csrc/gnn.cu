@@ -760,10 +760,9 @@ double Gnn::run(const GnnGraph& g, const mphy_pattern* Pt, const Fsai& F, const 
     // forward
     lin_fwd<kGnnNodeIn, H, true><<<gn, 256, 0, s>>>(nn, g.xnode.p, W + GnnLayout::w_in, W + GnnLayout::b_in, h_.p);
     const size_t upd_smem = (2 * H * (H + 1) + H + kWarpsPerCta * 2 * H) * sizeof(float);
-    static bool attr = false;
-    if (!attr) {
+    static std::atomic<uint64_t> attr{0};
+    if (first_use_on_device(attr)) {
         MPHY_CUDA(cudaFuncSetAttribute(update_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)upd_smem));
-        attr = true;
     }
     for (int l = 0; l < kGnnLayers; ++l) {
         const int o = GnnLayout::layer(l);
