@@ -491,9 +491,12 @@ void CoarseSpace::init(mphy_ctx* ctx, const mphy_mesh* mesh, const mphy_pattern*
     einv_.alloc((size_t)kp_ * kp_);
     w_.alloc(kp_);
     c_.alloc(kp_);
+    wpart_.alloc((size_t)n_agg_ * kMaxRestrictParts * nm_);
+    wcount_.alloc(n_agg_);
     err_.alloc(1);
     MPHY_CUDA(cudaMemsetAsync(w_.p, 0, w_.bytes(), s));
     MPHY_CUDA(cudaMemsetAsync(c_.p, 0, c_.bytes(), s));
+    MPHY_CUDA(cudaMemsetAsync(wcount_.p, 0, wcount_.bytes(), s));
     MPHY_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -626,6 +629,8 @@ CoarseView CoarseSpace::view() const {
     v.fixed = mesh_->fixed.p;
     v.einv = einv_.p;
     v.w = w_.p;
+    v.wpart = wpart_.p;
+    v.wcount = wcount_.p;
     v.c = c_.p;
     return v;
 }

@@ -49,6 +49,8 @@ class CoarseSpace {
     DevBuf<double> d_, cent_, E_, W_, w_, c_;
     DevBuf<double> einv_;
     DevBuf<uint8_t> drop_;
+    DevBuf<double> wpart_;
+    DevBuf<uint32_t> wcount_;
 };
 
 }  // namespace mphy

@@ -4,6 +4,9 @@
 
 namespace mphy {
 
+// Most CTAs that share one aggregate's restriction sum (w = Z^T r).
+constexpr int kMaxRestrictParts = 16;
+
 struct CoarseView {
     int32_t n_agg;           // aggregates (boxes)
     int32_t nm;              // modes per aggregate: 6 (rigid body) or 12 (linear displacement)
@@ -19,6 +22,8 @@ struct CoarseView {
     // on an indefinite preconditioner stalls
     const double* einv;
     double* w;               // [kp] restriction Z^T r
+    double* wpart;           // [n_agg][kMaxRestrictParts][nm] partial restriction sums
+    uint32_t* wcount;        // [n_agg] parts summed so far (zero between launches)
     double* c;               // [kp] coarse correction E^{-1} w
 };
 

@@ -69,6 +69,13 @@ __device__ __forceinline__ double mval(double x) { return x; }
 __device__ __forceinline__ float mval(float x) { return x; }
 __device__ __forceinline__ float mval(__nv_bfloat16 x) { return __bfloat162float(x); }
 
+// Matrix values and column indices are read once per product: evict-first loads, so that the
+// streamed matrix does not push the Krylov vectors (gathered and re-read through L2) out.
+template <typename T>
+__device__ __forceinline__ T ld_once(const T* p) {
+    return __ldcs(p);
+}
+
 // Deterministic block sum (fixed butterfly per warp, fixed order across warps); valid in all
 // threads of warp 0.
 __device__ __forceinline__ double block_sum(double v, double* sh) {
@@ -183,20 +190,20 @@ __global__ void __launch_bounds__(kThreads) spmv_kernel(SellView A, const VT* __
         const VT* vp = val + 9 * base + lane;
 #pragma unroll 2
         for (int k = 0; k < w; ++k) {
-            const int64_t c = cp[32 * k];
+            const int64_t c = ld_once(cp + 32 * k);
             const Acc x0 = (Acc)x[3 * c], x1 = (Acc)x[3 * c + 1], x2 = (Acc)x[3 * c + 2];
             const VT* v = vp + 288 * (int64_t)k;
-            y0 += (Acc)mval(v[0]) * x0 + (Acc)mval(v[32]) * x1 + (Acc)mval(v[64]) * x2;
-            y1 += (Acc)mval(v[96]) * x0 + (Acc)mval(v[128]) * x1 + (Acc)mval(v[160]) * x2;
-            y2 += (Acc)mval(v[192]) * x0 + (Acc)mval(v[224]) * x1 + (Acc)mval(v[256]) * x2;
+            y0 += (Acc)mval(ld_once(v)) * x0 + (Acc)mval(ld_once(v + 32)) * x1 + (Acc)mval(ld_once(v + 64)) * x2;
+            y1 += (Acc)mval(ld_once(v + 96)) * x0 + (Acc)mval(ld_once(v + 128)) * x1 + (Acc)mval(ld_once(v + 160)) * x2;
+            y2 += (Acc)mval(ld_once(v + 192)) * x0 + (Acc)mval(ld_once(v + 224)) * x1 + (Acc)mval(ld_once(v + 256)) * x2;
         }
         if (row < A.n_node) {
             if (A.diag64) {
                 const double* D = A.diag64 + 9 * row;
                 const double x0 = (double)x[3 * row], x1 = (double)x[3 * row + 1], x2 = (double)x[3 * row + 2];
-                y0 = (Acc)((double)y0 + D[0] * x0 + D[1] * x1 + D[2] * x2);
-                y1 = (Acc)((double)y1 + D[3] * x0 + D[4] * x1 + D[5] * x2);
-                y2 = (Acc)((double)y2 + D[6] * x0 + D[7] * x1 + D[8] * x2);
+                y0 = (Acc)((double)y0 + ld_once(D) * x0 + ld_once(D + 1) * x1 + ld_once(D + 2) * x2);
+                y1 = (Acc)((double)y1 + ld_once(D + 3) * x0 + ld_once(D + 4) * x1 + ld_once(D + 5) * x2);
+                y2 = (Acc)((double)y2 + ld_once(D + 6) * x0 + ld_once(D + 7) * x1 + ld_once(D + 8) * x2);
             }
             if (A.fixed) {
                 if (A.fixed[3 * row]) y0 = (Acc)x[3 * row];
@@ -396,7 +403,7 @@ __global__ void __launch_bounds__(kThreads) pcg_direction_kernel(int64_t n, XT* 
     if (st->done) return;
     const XT beta = (XT)st->beta;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        p[i] = z[i] + beta * p[i];
+        p[i] = ld_once(z + i) + beta * p[i];
 }
 
 // r = b, x = 0; JAC: z = D^-1 b, p = z, the fused (r, z), (z, z) and the initial state
@@ -435,47 +442,140 @@ __global__ void __launch_bounds__(kThreads) pcg_init_kernel(int64_t n, const XT*
 }
 
 // ---------------------------------------------------------------- two-level (coarse) apply
-// w = Z^T r per aggregate (one CTA per aggregate, fixed-order reduction)
-template <typename XT>
-__global__ void __launch_bounds__(kThreads) coarse_restrict_kernel(CoarseView cv, const XT* __restrict__ r,
-                                                                   const PcgState* st) {
-    __shared__ double sh[32];
+// Z^T r of one node added to w (fixed DOFs carry no residual). Rigid-body modes: translations
+// and the rotations about z, x, y; linear modes: translations and r_c d_k (u = a + B d).
+__device__ __forceinline__ void restrict_node(bool lin, const double rr[3], const double dd[3], double w[12]) {
+    w[0] += rr[0];
+    w[1] += rr[1];
+    w[2] += rr[2];
+    if (lin) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) w[3 + 3 * c + k] += rr[c] * dd[k];
+    } else {
+        w[3] += -dd[1] * rr[0] + dd[0] * rr[1];
+        w[4] += -dd[2] * rr[1] + dd[1] * rr[2];
+        w[5] += dd[2] * rr[0] - dd[0] * rr[2];
+    }
+}
+
+// w = Z^T r per aggregate. Work item (a, part) sums a contiguous part of aggregate a's node
+// list, two nodes per thread and step with every load issued before the arithmetic; the CTA
+// that finishes an aggregate's last part adds the parts' sums in part order, so w does not
+// depend on which CTA ran which part. A persistent grid walks the items. UPDATE first applies
+// this CG iteration's update: x += alpha p over a contiguous DOF slice per CTA, and
+// r -= alpha q on the item's nodes, the restriction reading the new r from registers.
+template <typename XT, bool UPDATE>
+__global__ void __launch_bounds__(kThreads, 3) coarse_restrict_kernel(CoarseView cv, int parts, int64_t n_dof,
+                                                                   XT* __restrict__ x, XT* __restrict__ r,
+                                                                   const XT* __restrict__ p,
+                                                                   const XT* __restrict__ q, const PcgState* st) {
+    __shared__ double sh[kThreads / 32][12];
+    __shared__ bool last;
     if (st && st->done) return;
+    XT alpha = 0;
+    if (UPDATE) {
+        alpha = (XT)st->alpha;
+        const int64_t per = (n_dof + gridDim.x - 1) / gridDim.x;
+        const int64_t lo = (int64_t)blockIdx.x * per;
+        const int64_t hi = lo + per < n_dof ? lo + per : n_dof;
+#pragma unroll 4
+        for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) __stcs(x + i, ld_once(x + i) + alpha * p[i]);
+    }
     const bool lin = cv.nm == 12;
-    for (int a = blockIdx.x; a < cv.n_agg; a += gridDim.x) {
+    const int nm = lin ? 12 : 6;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int items = cv.n_agg * parts;
+    for (int item = blockIdx.x; item < items; item += gridDim.x) {
+        const int a = item / parts, part = item - a * parts;
+        const int64_t b0 = cv.agg_ptr[a], len = cv.agg_ptr[a + 1] - b0;
+        const int64_t lo = b0 + len * part / parts, hi = b0 + len * (part + 1) / parts;
         double w[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-        for (int64_t i = cv.agg_ptr[a] + threadIdx.x; i < cv.agg_ptr[a + 1]; i += blockDim.x) {
-            const int64_t n = cv.agg_nodes[i];
-            const double rx = cv.fixed[3 * n] ? 0.0 : (double)r[3 * n];
-            const double ry = cv.fixed[3 * n + 1] ? 0.0 : (double)r[3 * n + 1];
-            const double rz = cv.fixed[3 * n + 2] ? 0.0 : (double)r[3 * n + 2];
-            const double dx = cv.d[3 * n], dy = cv.d[3 * n + 1], dz = cv.d[3 * n + 2];
-            w[0] += rx;
-            w[1] += ry;
-            w[2] += rz;
-            if (lin) {  // Z^T r for u = a + B d: w(a) = r, w(B_ck) = r_c d_k
-                const double rr[3] = {rx, ry, rz}, dd[3] = {dx, dy, dz};
+        for (int64_t i = lo + threadIdx.x; i < hi; i += 2 * (int64_t)blockDim.x) {
+            const bool two = i + blockDim.x < hi;
+            int64_t nd[2];
+            nd[0] = cv.agg_nodes[i];
+            nd[1] = two ? cv.agg_nodes[i + blockDim.x] : nd[0];
+            XT rv[2][3], qv[2][3];
+            double dv[2][3];
+            uint8_t fx[2][3];
 #pragma unroll
-                for (int c = 0; c < 3; ++c)
+            for (int k = 0; k < 2; ++k)
 #pragma unroll
-                    for (int k = 0; k < 3; ++k) w[3 + 3 * c + k] += rr[c] * dd[k];
-            } else {
-                w[3] += -dy * rx + dx * ry;
-                w[4] += -dz * ry + dy * rz;
-                w[5] += dz * rx - dx * rz;
+                for (int c = 0; c < 3; ++c) {
+                    rv[k][c] = r[3 * nd[k] + c];
+                    if (UPDATE) qv[k][c] = ld_once(q + 3 * nd[k] + c);
+                    dv[k][c] = cv.d[3 * nd[k] + c];
+                    fx[k][c] = cv.fixed[3 * nd[k] + c];
+                }
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                if (k == 1 && !two) break;
+                double rr[3];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    XT rn = rv[k][c];
+                    if (UPDATE) {
+                        rn = rv[k][c] - alpha * qv[k][c];
+                        r[3 * nd[k] + c] = rn;
+                    }
+                    rr[c] = fx[k][c] ? 0.0 : (double)rn;
+                }
+                restrict_node(lin, rr, dv[k], w);
             }
         }
-        const int nm = lin ? 12 : 6;
-        for (int j = 0; j < nm; ++j) {
-            const double t = block_sum(w[j], sh);
-            if (threadIdx.x == 0) cv.w[nm * a + j] = t;
+        // item sum: butterfly per warp, warps added in order
+        __syncthreads();  // sh and last of the previous item are no longer read
+#pragma unroll
+        for (int m = 0; m < 12; ++m) {
+            if (m < nm) {
+                double v = w[m];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                if (lane == 0) sh[warp][m] = v;
+            }
+        }
+        __syncthreads();
+        double t = 0.0;
+        if (threadIdx.x < nm)
+            for (int k = 0; k < kThreads / 32; ++k) t += sh[k][threadIdx.x];
+        if (parts == 1) {
+            if (threadIdx.x < nm) cv.w[nm * a + threadIdx.x] = t;
+            continue;
+        }
+        if (threadIdx.x < nm) cv.wpart[((int64_t)a * parts + part) * nm + threadIdx.x] = t;
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) last = atomicAdd(cv.wcount + a, 1u) == (uint32_t)parts - 1;
+        __syncthreads();
+        if (last) {
+            if (threadIdx.x < nm) {
+                double sum = 0.0;
+                for (int k = 0; k < parts; ++k)
+                    sum += __ldcg(cv.wpart + ((int64_t)a * parts + k) * nm + threadIdx.x);
+                cv.w[nm * a + threadIdx.x] = sum;
+            }
+            if (threadIdx.x == 0) cv.wcount[a] = 0;
         }
     }
 }
 
-// c = E^{-1} w: one warp per row of the FP64 inverse. Each lane reads 16-byte pairs, four
-// independent loads per step (kp is a multiple of 64, rows start 512-byte aligned), so enough
-// bytes are in flight to stream E^{-1} at HBM rate.
+// Persistent grid of the restriction with about two work items per resident CTA.
+template <typename XT, bool UPDATE>
+void launch_restrict(const CoarseView& cv, int64_t n_dof, XT* x, XT* r, const XT* p, const XT* q,
+                     const PcgState* st, cudaStream_t s, int sm) {
+    const unsigned grid = resident_grid((const void*)coarse_restrict_kernel<XT, UPDATE>, (int64_t)1 << 40, kThreads, sm);
+    int parts = (int)((2 * (int64_t)grid + cv.n_agg - 1) / cv.n_agg);
+    parts = std::max(1, std::min(parts, kMaxRestrictParts));
+    const unsigned g = (unsigned)std::min<int64_t>(grid, (int64_t)cv.n_agg * parts);
+    coarse_restrict_kernel<XT, UPDATE><<<g, kThreads, 0, s>>>(cv, parts, n_dof, x, r, p, q, st);
+}
+
+// c = E^{-1} w: one warp per row of the FP64 inverse. Each lane reads 16-byte pairs, eight
+// independent loads per step (kp is a multiple of 64, rows start 512-byte aligned), so a row
+// takes few dependent round trips and enough bytes are in flight to stream E^{-1} at HBM rate.
+// Pair j of a row goes to accumulator (j / 32) mod 4 in increasing j.
 __global__ void __launch_bounds__(kThreads) coarse_gemv_kernel(CoarseView cv, const PcgState* st) {
     if (st && st->done) return;
     const int lane = threadIdx.x & 31;
@@ -486,8 +586,25 @@ __global__ void __launch_bounds__(kThreads) coarse_gemv_kernel(CoarseView cv, co
         const int np = cv.kp >> 1;  // double2 per row
         double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
         int c = lane;
+        for (; c + 224 < np; c += 256) {
+            double2 ev[8], wv8[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                ev[k] = ld_once(e + c + 32 * k);
+                wv8[k] = wv[c + 32 * k];
+            }
+            a0 += ev[0].x * wv8[0].x + ev[0].y * wv8[0].y;
+            a1 += ev[1].x * wv8[1].x + ev[1].y * wv8[1].y;
+            a2 += ev[2].x * wv8[2].x + ev[2].y * wv8[2].y;
+            a3 += ev[3].x * wv8[3].x + ev[3].y * wv8[3].y;
+            a0 += ev[4].x * wv8[4].x + ev[4].y * wv8[4].y;
+            a1 += ev[5].x * wv8[5].x + ev[5].y * wv8[5].y;
+            a2 += ev[6].x * wv8[6].x + ev[6].y * wv8[6].y;
+            a3 += ev[7].x * wv8[7].x + ev[7].y * wv8[7].y;
+        }
         for (; c + 96 < np; c += 128) {
-            const double2 e0 = e[c], e1 = e[c + 32], e2 = e[c + 64], e3 = e[c + 96];
+            const double2 e0 = ld_once(e + c), e1 = ld_once(e + c + 32), e2 = ld_once(e + c + 64),
+                          e3 = ld_once(e + c + 96);
             const double2 w0 = wv[c], w1 = wv[c + 32], w2 = wv[c + 64], w3 = wv[c + 96];
             a0 += e0.x * w0.x + e0.y * w0.y;
             a1 += e1.x * w1.x + e1.y * w1.y;
@@ -495,7 +612,7 @@ __global__ void __launch_bounds__(kThreads) coarse_gemv_kernel(CoarseView cv, co
             a3 += e3.x * w3.x + e3.y * w3.y;
         }
         for (; c < np; c += 32) {
-            const double2 e0 = e[c], w0 = wv[c];
+            const double2 e0 = ld_once(e + c), w0 = wv[c];
             a0 += e0.x * w0.x + e0.y * w0.y;
         }
         double acc = (a0 + a1) + (a2 + a3);
@@ -518,18 +635,38 @@ __global__ void __launch_bounds__(kThreads) coarse_final_kernel(int32_t n_node, 
     if (!INIT && st->done) return;
     const bool unprec = INIT ? norm_type == 1 : st->norm_type == 1;
     double a1 = 0.0, a2 = 0.0;
-    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < n_node; n += (int64_t)gridDim.x * blockDim.x) {
-        double zc[3];
-        coarse_node_value(cv, n, zc);
+    // nodes n and n + stride per step (the order of a plain grid-stride loop), every load of
+    // both issued before the first store
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t n0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n0 < n_node; n0 += 2 * stride) {
+        const bool two = n0 + stride < n_node;
+        const int64_t nd[2] = {n0, two ? n0 + stride : n0};
+        double zc[2][3];
+        XT rv[2][3], dv[2][3];
+        uint8_t fx[2][3];
 #pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            const int64_t i = 3 * n + a;
-            const XT ri = r[i];
-            const XT zi = (XT)((double)dinv[i] * (double)ri + (cv.fixed[i] ? 0.0 : zc[a]));
-            z[i] = zi;
-            if (INIT) p[i] = zi;
-            a1 += (double)ri * (double)zi;
-            a2 += unprec ? (double)ri * (double)ri : (double)zi * (double)zi;
+        for (int k = 0; k < 2; ++k) {
+            coarse_node_value(cv, nd[k], zc[k]);
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                rv[k][a] = r[3 * nd[k] + a];
+                dv[k][a] = dinv[3 * nd[k] + a];
+                fx[k][a] = cv.fixed[3 * nd[k] + a];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            if (k == 1 && !two) break;
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                const int64_t i = 3 * nd[k] + a;
+                const XT ri = rv[k][a];
+                const XT zi = (XT)((double)dv[k][a] * (double)ri + (fx[k][a] ? 0.0 : zc[k][a]));
+                z[i] = zi;
+                if (INIT) p[i] = zi;
+                a1 += (double)ri * (double)zi;
+                a2 += unprec ? (double)ri * (double)ri : (double)zi * (double)zi;
+            }
         }
     }
     a1 = block_sum(a1, sh);
@@ -690,7 +827,8 @@ __global__ void __launch_bounds__(kThreads) coarse_prolong_add_kernel(int32_t n_
 }  // namespace
 
 void coarse_apply_add(const CoarseView& cv, int32_t n_node, const double* r, double* z, cudaStream_t s, int sm) {
-    coarse_restrict_kernel<double><<<std::min(cv.n_agg, sm * 8), kThreads, 0, s>>>(cv, r, nullptr);
+    launch_restrict<double, false>(cv, 3 * (int64_t)n_node, nullptr, const_cast<double*>(r), nullptr, nullptr, nullptr,
+                                   s, sm);
     coarse_gemv_kernel<<<stride_grid((int64_t)cv.kp * 32, kThreads, sm), kThreads, 0, s>>>(cv, nullptr);
     coarse_prolong_add_kernel<<<stride_grid(n_node, kThreads, sm), kThreads, 0, s>>>(n_node, cv, z);
     MPHY_CUDA(cudaGetLastError());
@@ -784,21 +922,21 @@ void Pcg<VT, XT>::record_iterations(const VT* val, XT* x, cudaStream_t s, int n_
             pcg_update_kernel<XT, true><<<gv, kThreads, 0, s>>>(n_, x, r_.p, z_.p, p_.p, q_.p, dinv_.p, partials_.p,
                                                                  partials2_.p, st_.p);
         } else if (kind_ == PcKind::JacobiCoarse) {
-            pcg_update_kernel<XT, false><<<gv, kThreads, 0, s>>>(n_, x, r_.p, z_.p, p_.p, q_.p, nullptr, nullptr,
-                                                                  nullptr, st_.p);
-            coarse_restrict_kernel<XT><<<std::min(coarse_.n_agg, sm_ * 8), kThreads, 0, s>>>(coarse_, r_.p, st_.p);
+            launch_restrict<XT, true>(coarse_, n_, x, r_.p, p_.p, q_.p, st_.p, s, sm_);
             coarse_gemv_kernel<<<stride_grid((int64_t)coarse_.kp * 32, kThreads, sm_), kThreads, 0, s>>>(coarse_,
                                                                                                           st_.p);
             coarse_final_kernel<XT, false><<<resident_grid((const void*)coarse_final_kernel<XT, false>, A_.n_node, kThreads, sm_), kThreads, 0, s>>>(
                 A_.n_node, coarse_, r_.p, z_.p, p_.p, dinv_.p, partials_.p, partials2_.p, st_.p, 0, 0, 0, 0, norm_type);
         } else {
-            pcg_update_kernel<XT, false><<<gv, kThreads, 0, s>>>(n_, x, r_.p, z_.p, p_.p, q_.p, nullptr, nullptr,
-                                                                  nullptr, st_.p);
+            if (kind_ == PcKind::FactorCoarse)
+                launch_restrict<XT, true>(coarse_, n_, x, r_.p, p_.p, q_.p, st_.p, s, sm_);
+            else
+                pcg_update_kernel<XT, false><<<gv, kThreads, 0, s>>>(n_, x, r_.p, z_.p, p_.p, q_.p, nullptr, nullptr,
+                                                                      nullptr, st_.p);
             const unsigned gg = resident_grid((const void*)factor_apply_kernel<XT, false>,
                                               (int64_t)factor_.G.n_slices * 32, kThreads, sm_);
             spmv_kernel<FactorT, XT, false><<<gg, kThreads, 0, s>>>(factor_.G, factor_.gval, r_.p, t_.p, nullptr, st_.p);
             if (kind_ == PcKind::FactorCoarse) {
-                coarse_restrict_kernel<XT><<<std::min(coarse_.n_agg, sm_ * 8), kThreads, 0, s>>>(coarse_, r_.p, st_.p);
                 coarse_gemv_kernel<<<stride_grid((int64_t)coarse_.kp * 32, kThreads, sm_), kThreads, 0, s>>>(coarse_,
                                                                                                               st_.p);
             }
@@ -824,7 +962,7 @@ int Pcg<VT, XT>::solve(const VT* val, const XT* b, XT* x, double rtol, double ab
         jacobi_kernel<VT, XT><<<stride_grid(A_.n_node, kThreads, sm_), kThreads, 0, s>>>(A_, val, dinv_.p);
         pcg_init_kernel<XT, false><<<gv, kThreads, 0, s>>>(n_, b, x, r_.p, z_.p, p_.p, nullptr, nullptr, nullptr,
                                                             st_.p, rtol, abstol, dtol, maxit, norm_type);
-        coarse_restrict_kernel<XT><<<std::min(coarse_.n_agg, sm_ * 8), kThreads, 0, s>>>(coarse_, r_.p, nullptr);
+        launch_restrict<XT, false>(coarse_, n_, nullptr, r_.p, nullptr, nullptr, nullptr, s, sm_);
         coarse_gemv_kernel<<<stride_grid((int64_t)coarse_.kp * 32, kThreads, sm_), kThreads, 0, s>>>(coarse_, nullptr);
         coarse_final_kernel<XT, true><<<resident_grid((const void*)coarse_final_kernel<XT, true>, A_.n_node, kThreads, sm_), kThreads, 0, s>>>(
             A_.n_node, coarse_, r_.p, z_.p, p_.p, dinv_.p, partials_.p, partials2_.p, st_.p, rtol, abstol, dtol,
@@ -836,7 +974,7 @@ int Pcg<VT, XT>::solve(const VT* val, const XT* b, XT* x, double rtol, double ab
         const unsigned gg = stride_grid((int64_t)factor_.G.n_slices * 32, kThreads, sm_);
         spmv_kernel<FactorT, XT, false><<<gg, kThreads, 0, s>>>(factor_.G, factor_.gval, r_.p, t_.p, nullptr, nullptr);
         if (kind_ == PcKind::FactorCoarse) {
-            coarse_restrict_kernel<XT><<<std::min(coarse_.n_agg, sm_ * 8), kThreads, 0, s>>>(coarse_, r_.p, nullptr);
+            launch_restrict<XT, false>(coarse_, n_, nullptr, r_.p, nullptr, nullptr, nullptr, s, sm_);
             coarse_gemv_kernel<<<stride_grid((int64_t)coarse_.kp * 32, kThreads, sm_), kThreads, 0, s>>>(coarse_,
                                                                                                           nullptr);
             launches += 2;
@@ -865,7 +1003,7 @@ int Pcg<VT, XT>::solve(const VT* val, const XT* b, XT* x, double rtol, double ab
         graph_stream_ = s;
         graph_kind_ = kind_;
     }
-    const int per_iter = kind_ == PcKind::Jacobi ? 3 : (kind_ == PcKind::Factor ? 5 : (kind_ == PcKind::FactorCoarse ? 7 : 6));
+    const int per_iter = kind_ == PcKind::Jacobi ? 3 : (kind_ == PcKind::Factor ? 5 : (kind_ == PcKind::FactorCoarse ? 6 : 5));
     PcgState h{};
     // every replay advances at most chunk_ iterations; the device stops at maxit
     const int64_t max_replays = (int64_t)(maxit > 0 ? maxit : 0) / chunk_ + 2;
