@@ -3,9 +3,10 @@
 //
 // Setup per operator:
 //   1. centroids of the current coordinates per aggregate and scaled offsets d_n = (x_n - c_a)/H;
-//   2. E = Z^T A Z: one CTA per aggregate walks its nodes' matrix rows and accumulates the 6x6
-//      blocks E[a][b] for its (at most 27) neighbour aggregates in shared memory -- every block
-//      of E is written by exactly one CTA, no atomics in global memory;
+//   2. E = Z^T A Z: the CTAs of an aggregate walk its nodes' matrix rows and accumulate the 6x6
+//      blocks E[a][b] for its neighbour aggregates (b <= a with rigid-body modes: the
+//      factorisation reads the lower triangle); the last of them stores the blocks -- every
+//      block of E is written once, no atomics in global memory;
 //   3. E = L L^T by a right-looking blocked Cholesky (64x64 tiles, FP64), W = L^{-1} by blocked
 //      forward substitution, E^{-1} = W^T W, kept in FP64 for the per-iteration GEMV (FP32
 //      rounding of the inverse of an ill-conditioned E can make it indefinite).
@@ -54,68 +55,100 @@ __global__ void offsets_kernel(int32_t n_node, const int32_t* __restrict__ agg, 
     }
 }
 
-// Z_n (3 x 6) of node n: translations, then rotations about z, x, y; zero rows on prescribed DOFs
-__device__ __forceinline__ void node_modes(const double* d, const uint8_t* fixed, int64_t n, double Z[3][6]) {
-    const double dx = d[3 * n], dy = d[3 * n + 1], dz = d[3 * n + 2];
-    const double m[3][6] = {{1, 0, 0, -dy, 0, dz}, {0, 1, 0, dx, -dz, 0}, {0, 0, 1, 0, dy, -dx}};
-    for (int i = 0; i < 3; ++i) {
-        const bool fx = fixed[3 * n + i] != 0;
-        for (int j = 0; j < 6; ++j) Z[i][j] = fx ? 0.0 : m[i][j];
-    }
-}
-
 // ---------------------------------------------------------------- E = Z^T A Z
+constexpr int kMatThreads = 128;
+constexpr int kMatParts = 8;         // most CTAs that share one aggregate
+constexpr int kMatItem = 21 + 13 * 36;  // one item's result: own block (lower), 13 lower neighbours
+
+// E = Z^T A Z for the rigid-body modes, lower triangle only: the blocked Cholesky reads tiles
+// (i, j) with i >= j and the lower half of the diagonal tiles, so for aggregate a only the
+// blocks E[a][b] with b < a (neighbour slots 0..12 of the 3x3x3 box stencil, z slowest) and the
+// lower half of E[a][a] are formed.
+//   Work item (a, part): a contiguous part of a's node list, one thread per node. For node n,
+// T = sum_m A_nm Z_m runs over the node's blocks in column order (neighbour aggregates change
+// rarely along a row) and Z_n^T T is added when the neighbour aggregate changes: to registers
+// for a's own block (fixed order, summed over the CTA by butterflies in warp order) and to the
+// item's shared slot buffer with shared atomics for the others. Column indices are read one
+// block ahead, so a block's loads do not wait for its own column index.
+//   Z_n = [I | R(d_n)] with R(d) = [[-dy, 0, dz], [dx, -dz, 0], [0, dy, -dx]] (translations,
+// then rotations about z, x, y) and zero rows on prescribed DOFs. The last CTA to finish an
+// aggregate's parts adds them in part order and stores the aggregate's blocks.
 template <typename VT>
-__global__ void __launch_bounds__(256) coarse_matrix_kernel(SellView A, const VT* __restrict__ aval, CoarseView cv,
-                                                            int ngx, int ngy, int ngz, double* __restrict__ E,
-                                                            int32_t* err) {
-    __shared__ double Eloc[27][36];
-    for (int a = blockIdx.x; a < cv.n_agg; a += gridDim.x) {
-        for (int i = threadIdx.x; i < 27 * 36; i += blockDim.x) (&Eloc[0][0])[i] = 0.0;
+__global__ void __launch_bounds__(kMatThreads, 3) coarse_matrix_kernel(SellView A, const VT* __restrict__ aval,
+                                                                    CoarseView cv, int ngx, int ngy, int ngz, int parts,
+                                                                    double* __restrict__ epart,
+                                                                    double* __restrict__ E, int32_t* err) {
+    __shared__ double Eloc[13][36];
+    __shared__ double red[kMatThreads / 32][21];
+    __shared__ bool last;
+    const int lane32 = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int items = cv.n_agg * parts;
+    for (int item = blockIdx.x; item < items; item += gridDim.x) {
+        const int a = item / parts, part = item - a * parts;
+        __syncthreads();  // the previous item's shared results are no longer read
+        for (int i = threadIdx.x; i < 13 * 36; i += blockDim.x) (&Eloc[0][0])[i] = 0.0;
         __syncthreads();
         const int ax = a % ngx, ay = (a / ngx) % ngy, az = a / (ngx * ngy);
-        for (int64_t i = cv.agg_ptr[a] + threadIdx.x; i < cv.agg_ptr[a + 1]; i += blockDim.x) {
+        const int64_t b0 = cv.agg_ptr[a], len = cv.agg_ptr[a + 1] - b0;
+        const int64_t lo = b0 + len * part / parts, hi = b0 + len * (part + 1) / parts;
+        double own[21];
+#pragma unroll
+        for (int v = 0; v < 21; ++v) own[v] = 0.0;
+        for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
             const int64_t n = cv.agg_nodes[i];
-            double Zn[3][6];
-            node_modes(cv.d, cv.fixed, n, Zn);
-            const int64_t s = n >> 5;
+            const double dnx = cv.d[3 * n], dny = cv.d[3 * n + 1], dnz = cv.d[3 * n + 2];
+            const double kn0 = cv.fixed[3 * n] ? 0.0 : 1.0, kn1 = cv.fixed[3 * n + 1] ? 0.0 : 1.0,
+                         kn2 = cv.fixed[3 * n + 2] ? 0.0 : 1.0;
+            const int64_t sl = n >> 5;
             const int lane = (int)(n & 31);
-            const int64_t base = A.slice_base[s];
-            const int w = A.slice_width[s];
-            // T = sum_m A_nm Z_m accumulated per neighbour aggregate (a node's neighbours are
-            // ascending, so they change aggregate rarely); E[a][slot] += Z_n^T T flushed once per
-            // aggregate run instead of once per block
-            double T[3][6] = {{0}};
+            const int64_t base = A.slice_base[sl];
+            const int w = A.slice_width[sl];
+            const int32_t* cp = A.col + base + lane;
+            const VT* vp = aval + 9 * base + lane;
+            double T[3][6];
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int j = 0; j < 6; ++j) T[r][j] = 0.0;
             int cur = -1;
+            // Z_n^T T of the current run into its destination, T cleared
             auto flush = [&](int slot) {
-                for (int i2 = 0; i2 < 6; ++i2)
-                    for (int j = 0; j < 6; ++j) {
-                        const double v = Zn[0][i2] * T[0][j] + Zn[1][i2] * T[1][j] + Zn[2][i2] * T[2][j];
-                        if (v != 0.0) atomicAdd(&Eloc[slot][6 * i2 + j], v);
+#pragma unroll
+                for (int j = 0; j < 6; ++j) {
+                    const double t0 = kn0 * T[0][j], t1 = kn1 * T[1][j], t2 = kn2 * T[2][j];
+                    const double c[6] = {t0, t1, t2, -dny * t0 + dnx * t1, -dnz * t1 + dny * t2, dnz * t0 - dnx * t2};
+                    if (slot == 13) {
+#pragma unroll
+                        for (int r = j; r < 6; ++r) own[r * (r + 1) / 2 + j] += c[r];
+                    } else {
+#pragma unroll
+                        for (int r = 0; r < 6; ++r)
+                            if (c[r] != 0.0) atomicAdd(&Eloc[slot][6 * r + j], c[r]);
                     }
+                }
+#pragma unroll
                 for (int r = 0; r < 3; ++r)
+#pragma unroll
                     for (int j = 0; j < 6; ++j) T[r][j] = 0.0;
             };
+            int64_t m_next = w > 0 ? (int64_t)cp[0] : n;
             for (int k = 0; k <= w; ++k) {
+                const int64_t m = m_next;
+                m_next = k + 1 < w ? (int64_t)cp[32 * (k + 1)] : n;  // the diagonal block comes last
                 double blk[9];
-                int64_t m;
                 if (k < w) {
-                    m = A.col[base + 32 * (int64_t)k + lane];
-                    const VT* v = aval + 9 * (base + 32 * (int64_t)k) + lane;
+                    const VT* v = vp + 288 * (int64_t)k;
                     bool any = false;
+#pragma unroll
                     for (int q = 0; q < 9; ++q) {
                         blk[q] = (double)v[32 * q];
                         any |= blk[q] != 0.0;
                     }
-                    if (!any) continue;
+                    if (!any) continue;  // SELL padding
                 } else {
-                    if (!A.diag64) break;  // the FP32 storage keeps the diagonal blocks apart
-                    m = n;
+                    if (!A.diag64) break;  // the FP64 storage keeps the diagonal blocks in the rows
+#pragma unroll
                     for (int q = 0; q < 9; ++q) blk[q] = A.diag64[9 * n + q];
-                }
-                if (A.fixed) {  // the FP32 storage is unmasked: prescribed DOFs act as identity rows
-                    for (int q = 0; q < 9; ++q)
-                        if (A.fixed[3 * n + q / 3] || A.fixed[3 * m + q % 3]) blk[q] = 0.0;
                 }
                 const int b = cv.agg[m];
                 const int dx = b % ngx - ax, dy = (b / ngx) % ngy - ay, dz = b / (ngx * ngy) - az;
@@ -124,27 +157,80 @@ __global__ void __launch_bounds__(256) coarse_matrix_kernel(SellView A, const VT
                     continue;
                 }
                 const int slot = (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1);
+                if (slot > 13) continue;  // upper triangle of E
                 if (slot != cur) {
                     if (cur >= 0) flush(cur);
                     cur = slot;
                 }
-                double Zm[3][6];
-                node_modes(cv.d, cv.fixed, m, Zm);
-                for (int r = 0; r < 3; ++r)
-                    for (int j = 0; j < 6; ++j)
-                        T[r][j] += blk[3 * r] * Zm[0][j] + blk[3 * r + 1] * Zm[1][j] + blk[3 * r + 2] * Zm[2][j];
+                const double dmx = cv.d[3 * m], dmy = cv.d[3 * m + 1], dmz = cv.d[3 * m + 2];
+                const double km0 = cv.fixed[3 * m] ? 0.0 : 1.0, km1 = cv.fixed[3 * m + 1] ? 0.0 : 1.0,
+                             km2 = cv.fixed[3 * m + 2] ? 0.0 : 1.0;
+#pragma unroll
+                for (int r = 0; r < 3; ++r) {
+                    const double c0 = km0 * blk[3 * r], c1 = km1 * blk[3 * r + 1], c2 = km2 * blk[3 * r + 2];
+                    T[r][0] += c0;
+                    T[r][1] += c1;
+                    T[r][2] += c2;
+                    T[r][3] += -dmy * c0 + dmx * c1;
+                    T[r][4] += -dmz * c1 + dmy * c2;
+                    T[r][5] += dmz * c0 - dmx * c2;
+                }
             }
             if (cur >= 0) flush(cur);
         }
-        __syncthreads();
-        for (int t = threadIdx.x; t < 27 * 36; t += blockDim.x) {
-            const int slot = t / 36, q = t % 36;
-            const int bx = ax + slot % 3 - 1, by = ay + (slot / 3) % 3 - 1, bz = az + slot / 9 - 1;
-            if (bx < 0 || bx >= ngx || by < 0 || by >= ngy || bz < 0 || bz >= ngz) continue;
-            const int b = bx + ngx * (by + ngy * bz);
-            E[(int64_t)(6 * a + q / 6) * cv.kp + 6 * b + q % 6] = Eloc[slot][q];
+#pragma unroll
+        for (int v = 0; v < 21; ++v) {
+            double x = own[v];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+            if (lane32 == 0) red[warp][v] = x;
         }
         __syncthreads();
+        // the item's value t of kMatItem: own block (lower, row-major) or a neighbour slot entry
+        auto item_value = [&](int t) {
+            if (t < 21) {
+                double x = 0.0;
+                for (int q = 0; q < kMatThreads / 32; ++q) x += red[q][t];
+                return x;
+            }
+            return (&Eloc[0][0])[t - 21];
+        };
+        // where value t goes in E (-1: the neighbour box is outside the grid)
+        auto e_index = [&](int t) -> int64_t {
+            if (t < 21) {
+                int r = 0;
+                while ((r + 1) * (r + 2) / 2 <= t) ++r;
+                const int j = t - r * (r + 1) / 2;
+                return (int64_t)(6 * a + r) * cv.kp + 6 * a + j;
+            }
+            const int slot = (t - 21) / 36, q = (t - 21) % 36;
+            const int bx = ax + slot % 3 - 1, by = ay + (slot / 3) % 3 - 1, bz = az + slot / 9 - 1;
+            if (bx < 0 || bx >= ngx || by < 0 || by >= ngy || bz < 0 || bz >= ngz) return -1;
+            const int b = bx + ngx * (by + ngy * bz);
+            return (int64_t)(6 * a + q / 6) * cv.kp + 6 * b + q % 6;
+        };
+        if (parts == 1) {
+            for (int t = threadIdx.x; t < kMatItem; t += blockDim.x) {
+                const int64_t e = e_index(t);
+                if (e >= 0) E[e] = item_value(t);
+            }
+            continue;
+        }
+        for (int t = threadIdx.x; t < kMatItem; t += blockDim.x)
+            epart[((int64_t)a * parts + part) * kMatItem + t] = item_value(t);
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) last = atomicAdd(cv.wcount + a, 1u) == (uint32_t)parts - 1;
+        __syncthreads();
+        if (!last) continue;
+        for (int t = threadIdx.x; t < kMatItem; t += blockDim.x) {
+            const int64_t e = e_index(t);
+            if (e < 0) continue;
+            double x = 0.0;
+            for (int q = 0; q < parts; ++q) x += __ldcg(epart + ((int64_t)a * parts + q) * kMatItem + t);
+            E[e] = x;
+        }
+        if (threadIdx.x == 0) cv.wcount[a] = 0;
     }
 }
 
@@ -493,6 +579,7 @@ void CoarseSpace::init(mphy_ctx* ctx, const mphy_mesh* mesh, const mphy_pattern*
     c_.alloc(kp_);
     wpart_.alloc((size_t)n_agg_ * kMaxRestrictParts * nm_);
     wcount_.alloc(n_agg_);
+    if (nm_ == 6) epart_.alloc((size_t)n_agg_ * kMatParts * kMatItem);
     err_.alloc(1);
     MPHY_CUDA(cudaMemsetAsync(w_.p, 0, w_.bytes(), s));
     MPHY_CUDA(cudaMemsetAsync(c_.p, 0, c_.bytes(), s));
@@ -530,9 +617,14 @@ void CoarseSpace::setup(const SellView& A, const VT* aval, const double* disp, c
     if (nm_ == 12)
         coarse_matrix_linear_kernel<VT><<<std::min(n_agg_, sm * 8), 256, 0, s>>>(A, aval, cv, ng_[0], ng_[1], ng_[2],
                                                                                   E_.p, err_.p);
-    else
-        coarse_matrix_kernel<VT><<<std::min(n_agg_, sm * 8), 256, 0, s>>>(A, aval, cv, ng_[0], ng_[1], ng_[2], E_.p,
-                                                                           err_.p);
+    else {
+        // persistent grid, about two work items per resident CTA
+        const unsigned grid = resident_grid((const void*)coarse_matrix_kernel<VT>, (int64_t)1 << 40, kMatThreads, sm);
+        const int parts = std::max(1, std::min(kMatParts, (int)((2 * (int64_t)grid + n_agg_ - 1) / n_agg_)));
+        const unsigned g = (unsigned)std::min<int64_t>(grid, (int64_t)n_agg_ * parts);
+        coarse_matrix_kernel<VT><<<g, kMatThreads, 0, s>>>(A, aval, cv, ng_[0], ng_[1], ng_[2], parts, epart_.p, E_.p,
+                                                           err_.p);
+    }
     MPHY_CUDA(cudaGetLastError());
     launches += 3;
     const int nb = kp_ / T;

@@ -51,6 +51,7 @@ class CoarseSpace {
     DevBuf<uint8_t> drop_;
     DevBuf<double> wpart_;
     DevBuf<uint32_t> wcount_;
+    DevBuf<double> epart_;  // per-part results of the E = Z^T A Z kernel
 };
 
 }  // namespace mphy

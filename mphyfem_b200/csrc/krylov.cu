@@ -463,26 +463,13 @@ __device__ __forceinline__ void restrict_node(bool lin, const double rr[3], cons
 // w = Z^T r per aggregate. Work item (a, part) sums a contiguous part of aggregate a's node
 // list, two nodes per thread and step with every load issued before the arithmetic; the CTA
 // that finishes an aggregate's last part adds the parts' sums in part order, so w does not
-// depend on which CTA ran which part. A persistent grid walks the items. UPDATE first applies
-// this CG iteration's update: x += alpha p over a contiguous DOF slice per CTA, and
-// r -= alpha q on the item's nodes, the restriction reading the new r from registers.
-template <typename XT, bool UPDATE>
-__global__ void __launch_bounds__(kThreads, 3) coarse_restrict_kernel(CoarseView cv, int parts, int64_t n_dof,
-                                                                   XT* __restrict__ x, XT* __restrict__ r,
-                                                                   const XT* __restrict__ p,
-                                                                   const XT* __restrict__ q, const PcgState* st) {
+// depend on which CTA ran which part. A persistent grid walks the items.
+template <typename XT>
+__global__ void __launch_bounds__(kThreads, 3) coarse_restrict_kernel(CoarseView cv, int parts,
+                                                                      const XT* __restrict__ r, const PcgState* st) {
     __shared__ double sh[kThreads / 32][12];
     __shared__ bool last;
     if (st && st->done) return;
-    XT alpha = 0;
-    if (UPDATE) {
-        alpha = (XT)st->alpha;
-        const int64_t per = (n_dof + gridDim.x - 1) / gridDim.x;
-        const int64_t lo = (int64_t)blockIdx.x * per;
-        const int64_t hi = lo + per < n_dof ? lo + per : n_dof;
-#pragma unroll 4
-        for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) __stcs(x + i, ld_once(x + i) + alpha * p[i]);
-    }
     const bool lin = cv.nm == 12;
     const int nm = lin ? 12 : 6;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -497,7 +484,7 @@ __global__ void __launch_bounds__(kThreads, 3) coarse_restrict_kernel(CoarseView
             int64_t nd[2];
             nd[0] = cv.agg_nodes[i];
             nd[1] = two ? cv.agg_nodes[i + blockDim.x] : nd[0];
-            XT rv[2][3], qv[2][3];
+            XT rv[2][3];
             double dv[2][3];
             uint8_t fx[2][3];
 #pragma unroll
@@ -505,7 +492,6 @@ __global__ void __launch_bounds__(kThreads, 3) coarse_restrict_kernel(CoarseView
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
                     rv[k][c] = r[3 * nd[k] + c];
-                    if (UPDATE) qv[k][c] = ld_once(q + 3 * nd[k] + c);
                     dv[k][c] = cv.d[3 * nd[k] + c];
                     fx[k][c] = cv.fixed[3 * nd[k] + c];
                 }
@@ -514,14 +500,7 @@ __global__ void __launch_bounds__(kThreads, 3) coarse_restrict_kernel(CoarseView
                 if (k == 1 && !two) break;
                 double rr[3];
 #pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    XT rn = rv[k][c];
-                    if (UPDATE) {
-                        rn = rv[k][c] - alpha * qv[k][c];
-                        r[3 * nd[k] + c] = rn;
-                    }
-                    rr[c] = fx[k][c] ? 0.0 : (double)rn;
-                }
+                for (int c = 0; c < 3; ++c) rr[c] = fx[k][c] ? 0.0 : (double)rv[k][c];
                 restrict_node(lin, rr, dv[k], w);
             }
         }
@@ -562,14 +541,13 @@ __global__ void __launch_bounds__(kThreads, 3) coarse_restrict_kernel(CoarseView
 }
 
 // Persistent grid of the restriction with about two work items per resident CTA.
-template <typename XT, bool UPDATE>
-void launch_restrict(const CoarseView& cv, int64_t n_dof, XT* x, XT* r, const XT* p, const XT* q,
-                     const PcgState* st, cudaStream_t s, int sm) {
-    const unsigned grid = resident_grid((const void*)coarse_restrict_kernel<XT, UPDATE>, (int64_t)1 << 40, kThreads, sm);
+template <typename XT>
+void launch_restrict(const CoarseView& cv, const XT* r, const PcgState* st, cudaStream_t s, int sm) {
+    const unsigned grid = resident_grid((const void*)coarse_restrict_kernel<XT>, (int64_t)1 << 40, kThreads, sm);
     int parts = (int)((2 * (int64_t)grid + cv.n_agg - 1) / cv.n_agg);
     parts = std::max(1, std::min(parts, kMaxRestrictParts));
     const unsigned g = (unsigned)std::min<int64_t>(grid, (int64_t)cv.n_agg * parts);
-    coarse_restrict_kernel<XT, UPDATE><<<g, kThreads, 0, s>>>(cv, parts, n_dof, x, r, p, q, st);
+    coarse_restrict_kernel<XT><<<g, kThreads, 0, s>>>(cv, parts, r, st);
 }
 
 // c = E^{-1} w: one warp per row of the FP64 inverse. Each lane reads 16-byte pairs, eight
@@ -827,8 +805,7 @@ __global__ void __launch_bounds__(kThreads) coarse_prolong_add_kernel(int32_t n_
 }  // namespace
 
 void coarse_apply_add(const CoarseView& cv, int32_t n_node, const double* r, double* z, cudaStream_t s, int sm) {
-    launch_restrict<double, false>(cv, 3 * (int64_t)n_node, nullptr, const_cast<double*>(r), nullptr, nullptr, nullptr,
-                                   s, sm);
+    launch_restrict<double>(cv, r, nullptr, s, sm);
     coarse_gemv_kernel<<<stride_grid((int64_t)cv.kp * 32, kThreads, sm), kThreads, 0, s>>>(cv, nullptr);
     coarse_prolong_add_kernel<<<stride_grid(n_node, kThreads, sm), kThreads, 0, s>>>(n_node, cv, z);
     MPHY_CUDA(cudaGetLastError());
@@ -922,21 +899,21 @@ void Pcg<VT, XT>::record_iterations(const VT* val, XT* x, cudaStream_t s, int n_
             pcg_update_kernel<XT, true><<<gv, kThreads, 0, s>>>(n_, x, r_.p, z_.p, p_.p, q_.p, dinv_.p, partials_.p,
                                                                  partials2_.p, st_.p);
         } else if (kind_ == PcKind::JacobiCoarse) {
-            launch_restrict<XT, true>(coarse_, n_, x, r_.p, p_.p, q_.p, st_.p, s, sm_);
+            pcg_update_kernel<XT, false><<<gv, kThreads, 0, s>>>(n_, x, r_.p, z_.p, p_.p, q_.p, nullptr, nullptr,
+                                                                  nullptr, st_.p);
+            launch_restrict<XT>(coarse_, r_.p, st_.p, s, sm_);
             coarse_gemv_kernel<<<stride_grid((int64_t)coarse_.kp * 32, kThreads, sm_), kThreads, 0, s>>>(coarse_,
                                                                                                           st_.p);
             coarse_final_kernel<XT, false><<<resident_grid((const void*)coarse_final_kernel<XT, false>, A_.n_node, kThreads, sm_), kThreads, 0, s>>>(
                 A_.n_node, coarse_, r_.p, z_.p, p_.p, dinv_.p, partials_.p, partials2_.p, st_.p, 0, 0, 0, 0, norm_type);
         } else {
-            if (kind_ == PcKind::FactorCoarse)
-                launch_restrict<XT, true>(coarse_, n_, x, r_.p, p_.p, q_.p, st_.p, s, sm_);
-            else
-                pcg_update_kernel<XT, false><<<gv, kThreads, 0, s>>>(n_, x, r_.p, z_.p, p_.p, q_.p, nullptr, nullptr,
-                                                                      nullptr, st_.p);
+            pcg_update_kernel<XT, false><<<gv, kThreads, 0, s>>>(n_, x, r_.p, z_.p, p_.p, q_.p, nullptr, nullptr,
+                                                                  nullptr, st_.p);
             const unsigned gg = resident_grid((const void*)factor_apply_kernel<XT, false>,
                                               (int64_t)factor_.G.n_slices * 32, kThreads, sm_);
             spmv_kernel<FactorT, XT, false><<<gg, kThreads, 0, s>>>(factor_.G, factor_.gval, r_.p, t_.p, nullptr, st_.p);
             if (kind_ == PcKind::FactorCoarse) {
+                launch_restrict<XT>(coarse_, r_.p, st_.p, s, sm_);
                 coarse_gemv_kernel<<<stride_grid((int64_t)coarse_.kp * 32, kThreads, sm_), kThreads, 0, s>>>(coarse_,
                                                                                                               st_.p);
             }
@@ -962,7 +939,7 @@ int Pcg<VT, XT>::solve(const VT* val, const XT* b, XT* x, double rtol, double ab
         jacobi_kernel<VT, XT><<<stride_grid(A_.n_node, kThreads, sm_), kThreads, 0, s>>>(A_, val, dinv_.p);
         pcg_init_kernel<XT, false><<<gv, kThreads, 0, s>>>(n_, b, x, r_.p, z_.p, p_.p, nullptr, nullptr, nullptr,
                                                             st_.p, rtol, abstol, dtol, maxit, norm_type);
-        launch_restrict<XT, false>(coarse_, n_, nullptr, r_.p, nullptr, nullptr, nullptr, s, sm_);
+        launch_restrict<XT>(coarse_, r_.p, nullptr, s, sm_);
         coarse_gemv_kernel<<<stride_grid((int64_t)coarse_.kp * 32, kThreads, sm_), kThreads, 0, s>>>(coarse_, nullptr);
         coarse_final_kernel<XT, true><<<resident_grid((const void*)coarse_final_kernel<XT, true>, A_.n_node, kThreads, sm_), kThreads, 0, s>>>(
             A_.n_node, coarse_, r_.p, z_.p, p_.p, dinv_.p, partials_.p, partials2_.p, st_.p, rtol, abstol, dtol,
@@ -974,7 +951,7 @@ int Pcg<VT, XT>::solve(const VT* val, const XT* b, XT* x, double rtol, double ab
         const unsigned gg = stride_grid((int64_t)factor_.G.n_slices * 32, kThreads, sm_);
         spmv_kernel<FactorT, XT, false><<<gg, kThreads, 0, s>>>(factor_.G, factor_.gval, r_.p, t_.p, nullptr, nullptr);
         if (kind_ == PcKind::FactorCoarse) {
-            launch_restrict<XT, false>(coarse_, n_, nullptr, r_.p, nullptr, nullptr, nullptr, s, sm_);
+            launch_restrict<XT>(coarse_, r_.p, nullptr, s, sm_);
             coarse_gemv_kernel<<<stride_grid((int64_t)coarse_.kp * 32, kThreads, sm_), kThreads, 0, s>>>(coarse_,
                                                                                                           nullptr);
             launches += 2;
@@ -1003,7 +980,7 @@ int Pcg<VT, XT>::solve(const VT* val, const XT* b, XT* x, double rtol, double ab
         graph_stream_ = s;
         graph_kind_ = kind_;
     }
-    const int per_iter = kind_ == PcKind::Jacobi ? 3 : (kind_ == PcKind::Factor ? 5 : (kind_ == PcKind::FactorCoarse ? 6 : 5));
+    const int per_iter = kind_ == PcKind::Jacobi ? 3 : (kind_ == PcKind::Factor ? 5 : (kind_ == PcKind::FactorCoarse ? 7 : 6));
     PcgState h{};
     // every replay advances at most chunk_ iterations; the device stops at maxit
     const int64_t max_replays = (int64_t)(maxit > 0 ? maxit : 0) / chunk_ + 2;
