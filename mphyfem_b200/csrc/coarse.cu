@@ -361,48 +361,105 @@ __device__ __forceinline__ void store_tile(const double (*S)[TP], double* M, int
 
 // Factor the diagonal tile (j, j) in place (lower triangle; upper zeroed), and write its inverse
 // W_jj = L_jj^{-1} to W: the panel below becomes a tile product with W_jj (gemm_panel_tiles) and
-// the triangular inverse reuses W_jj. The inverse runs four threads per column: for row r, the
-// four lanes split sum_{c <= t < r} L_rt X_tc and combine it by shuffles.
+// the triangular inverse reuses W_jj. The tile lives in registers: thread (ty, tx) of 16 x 16
+// holds rows ty + 16a and columns tx + 16b (a, b < 4). Cholesky step c: the holders of column c
+// put it in shared memory, every thread forms L(:, c) = column / sqrt(pivot) for its rows and
+// columns and applies the rank-1 update to its 16 entries. Inverse, row r of X = L^{-1}:
+// X(r, :) = (e_r - acc(r, :)) / L(r, r), written by the holders of row r with column r of L,
+// then acc(i, :) += L(i, r) X(r, :) for i > r. The shared vectors are double-buffered, so each
+// step needs one barrier.
 __global__ void __launch_bounds__(256) potrf_inv_tile(double* E, double* W, int kp, int j, int32_t* err) {
-    extern __shared__ double sm[];
-    double (*S)[TP] = reinterpret_cast<double (*)[TP]>(sm);
-    double (*X)[TP] = reinterpret_cast<double (*)[TP]>(sm + T * TP);
-    load_tile(S, E, kp, j, j);
-    __syncthreads();
+    __shared__ double colv[2][T];
+    __shared__ double rowv[2][T];
+    __shared__ double diag[T];
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;  // blockDim.x == 256
+    double S[4][4];
+    const double* Et = E + (int64_t)(j * T) * kp + j * T;
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) S[a][b] = Et[(int64_t)(ty + 16 * a) * kp + tx + 16 * b];
     for (int c = 0; c < T; ++c) {
-        double p = S[c][c];
+        const int buf = c & 1, bc = c >> 4;
+        if (tx == (c & 15)) {
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b)
+                    if (b == bc) colv[buf][ty + 16 * a] = S[a][b];
+        }
+        __syncthreads();
+        double p = colv[buf][c];
         if (!(p > 0.0)) {
             if (threadIdx.x == 0) atomicExch(err, 2);
             p = 1e-300;
         }
-        const double l = sqrt(p);
-        __syncthreads();
-        if (threadIdx.x == 0) S[c][c] = l;
-        for (int i = c + 1 + threadIdx.x; i < T; i += blockDim.x) S[i][c] /= l;
-        __syncthreads();
-        const int rem = T - c - 1;
-        for (int t = threadIdx.x; t < rem * rem; t += blockDim.x) {
-            const int i = c + 1 + t / rem, q = c + 1 + t % rem;
-            if (q <= i) S[i][q] -= S[i][c] * S[q][c];
+        const double l = sqrt(p), il = 1.0 / l;
+        if (threadIdx.x == 0) diag[c] = l;
+        double li[4], lj[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) li[a] = ty + 16 * a > c ? colv[buf][ty + 16 * a] * il : 0.0;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) lj[b] = tx + 16 * b > c ? colv[buf][tx + 16 * b] * il : 0.0;
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                S[a][b] -= li[a] * lj[b];
+                if (tx + 16 * b == c) S[a][b] = ty + 16 * a == c ? l : li[a];
+            }
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+            if (tx + 16 * b > ty + 16 * a) S[a][b] = 0.0;
+    double* Eo = E + (int64_t)(j * T) * kp + j * T;
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) Eo[(int64_t)(ty + 16 * a) * kp + tx + 16 * b] = S[a][b];
+    __syncthreads();  // diag complete
+    double X[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) X[a][b] = 0.0;
+    for (int r = 0; r < T; ++r) {
+        const int buf = r & 1, br = r >> 4;
+        const double idg = 1.0 / diag[r];
+        if (ty == (r & 15)) {
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+                if (a == br)
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) {
+                        const int jc = tx + 16 * b;
+                        const double x = jc <= r ? ((jc == r ? 1.0 : 0.0) - X[a][b]) * idg : 0.0;
+                        X[a][b] = x;
+                        rowv[buf][jc] = x;
+                    }
+        }
+        if (tx == (r & 15)) {
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b)
+                    if (b == br) colv[buf][ty + 16 * a] = S[a][b];
         }
         __syncthreads();
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const double lir = ty + 16 * a > r ? colv[buf][ty + 16 * a] : 0.0;
+#pragma unroll
+            for (int b = 0; b < 4; ++b) X[a][b] += lir * rowv[buf][tx + 16 * b];
+        }
     }
-    for (int t = threadIdx.x; t < T * T; t += blockDim.x)
-        if (t % T > t / T) S[t / T][t % T] = 0.0;
-    __syncthreads();
-    store_tile(S, E, kp, j, j);
-    const int col = threadIdx.x >> 2, sub = threadIdx.x & 3;  // blockDim.x == 4 T
-    for (int r = 0; r < T; ++r) {
-        double acc = 0.0;
-        if (r > col)
-            for (int t = col + sub; t < r; t += 4) acc += S[r][t] * X[t][col];
-        acc += __shfl_xor_sync(0xffffffffu, acc, 1);
-        acc += __shfl_xor_sync(0xffffffffu, acc, 2);
-        if (sub == 0) X[r][col] = r < col ? 0.0 : ((r == col ? 1.0 : 0.0) - acc) / S[r][r];
-        __syncwarp();
-    }
-    __syncthreads();
-    store_tile(X, W, kp, j, j);
+    double* Wo = W + (int64_t)(j * T) * kp + j * T;
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) Wo[(int64_t)(ty + 16 * a) * kp + tx + 16 * b] = X[a][b];
 }
 
 // C (tile ci, cj of M) += alpha * sum_t A[r][t] * B[c][t]  with A, B 64x64 tiles in shared memory
@@ -632,7 +689,6 @@ void CoarseSpace::setup(const SellView& A, const VT* aval, const double* disp, c
     static std::atomic<uint64_t> attr{0};
     if (first_use_on_device(attr)) {
         MPHY_CUDA(cudaFuncSetAttribute(syrk_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
-        MPHY_CUDA(cudaFuncSetAttribute(potrf_inv_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
         MPHY_CUDA(cudaFuncSetAttribute(gemm_panel_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
         MPHY_CUDA(cudaFuncSetAttribute(trtri_finalize, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
         MPHY_CUDA(cudaFuncSetAttribute(trtri_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
@@ -676,7 +732,7 @@ void CoarseSpace::record_factorisation(cudaStream_t s, int nb, size_t sm2) {
     drop_null_modes<<<1, 1024, 0, s>>>(E_.p, kp_, nm_ * n_agg_);
     launches += 1;
     for (int j = 0; j < nb; ++j) {
-        potrf_inv_tile<<<1, 256, sm2, s>>>(E_.p, W_.p, kp_, j, err_.p);
+        potrf_inv_tile<<<1, 256, 0, s>>>(E_.p, W_.p, kp_, j, err_.p);
         const int m = nb - j - 1;
         if (m > 0) {
             gemm_panel_tiles<<<m, 256, sm2, s>>>(E_.p, W_.p, kp_, j);

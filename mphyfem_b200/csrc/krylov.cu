@@ -373,8 +373,10 @@ __global__ void __launch_bounds__(kThreads) pcg_update_kernel(int64_t n, XT* __r
     const bool unprec = st->norm_type == 1;
     double a1 = 0.0, a2 = 0.0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        x[i] += alpha * p[i];
-        const XT ri = r[i] - alpha * q[i];
+        // x is next read in the next iteration's update and q is dead after this read: both
+        // leave L2 first
+        __stcs(x + i, ld_once(x + i) + alpha * p[i]);
+        const XT ri = r[i] - alpha * ld_once(q + i);
         r[i] = ri;
         if (JAC) {
             const XT zi = dinv[i] * ri;
