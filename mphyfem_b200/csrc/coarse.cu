@@ -55,6 +55,24 @@ __global__ void offsets_kernel(int32_t n_node, const int32_t* __restrict__ agg, 
     }
 }
 
+// d and the prescribed-DOF mask in the order of the aggregates' node lists, so that the
+// per-iteration restriction reads them coalesced and without waiting for the node index
+__global__ void permute_offsets_kernel(int32_t n_node, const int32_t* __restrict__ nodes, const double* __restrict__ d,
+                                       double* __restrict__ dperm) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n_node; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t n = nodes[i];
+        for (int k = 0; k < 3; ++k) dperm[3 * i + k] = d[3 * n + k];
+    }
+}
+
+__global__ void permute_mask_kernel(int32_t n_node, const int32_t* __restrict__ nodes,
+                                    const uint8_t* __restrict__ fixed, uint8_t* __restrict__ fperm) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n_node; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t n = nodes[i];
+        for (int k = 0; k < 3; ++k) fperm[3 * i + k] = fixed[3 * n + k];
+    }
+}
+
 // ---------------------------------------------------------------- E = Z^T A Z
 constexpr int kMatThreads = 128;
 constexpr int kMatParts = 8;         // most CTAs that share one aggregate
@@ -628,6 +646,10 @@ void CoarseSpace::init(mphy_ctx* ctx, const mphy_mesh* mesh, const mphy_pattern*
     agg_nodes_.alloc(nn);
     agg_nodes_.upload(nodes.data(), nn, s);
     d_.alloc(3 * (size_t)nn);
+    dperm_.alloc(3 * (size_t)nn);
+    fperm_.alloc(3 * (size_t)nn);
+    permute_mask_kernel<<<stride_grid(nn, 256, ctx->sm_count), 256, 0, s>>>(nn, agg_nodes_.p, mesh->fixed.p, fperm_.p);
+    MPHY_CUDA(cudaGetLastError());
     cent_.alloc(3 * (size_t)n_agg_);
     E_.alloc((size_t)kp_ * kp_);
     W_.alloc((size_t)kp_ * kp_);
@@ -667,6 +689,8 @@ void CoarseSpace::setup(const SellView& A, const VT* aval, const double* disp, c
     }
     offsets_kernel<<<stride_grid(mesh_->n_node, 256, sm), 256, 0, s>>>(mesh_->n_node, agg_.p, mesh_->coords.p, disp,
                                                                       cent_.p, 1.0 / boxd_, d_.p);
+    permute_offsets_kernel<<<stride_grid(mesh_->n_node, 256, sm), 256, 0, s>>>(mesh_->n_node, agg_nodes_.p, d_.p,
+                                                                              dperm_.p);
     MPHY_CUDA(cudaMemsetAsync(E_.p, 0, E_.bytes(), s));
     MPHY_CUDA(cudaMemsetAsync(W_.p, 0, W_.bytes(), s));
     MPHY_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(int32_t), s));
@@ -775,6 +799,8 @@ CoarseView CoarseSpace::view() const {
     v.agg_nodes = agg_nodes_.p;
     v.d = d_.p;
     v.fixed = mesh_->fixed.p;
+    v.dperm = dperm_.p;
+    v.fperm = fperm_.p;
     v.einv = einv_.p;
     v.w = w_.p;
     v.wpart = wpart_.p;

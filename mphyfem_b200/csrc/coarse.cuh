@@ -52,6 +52,8 @@ class CoarseSpace {
     DevBuf<double> wpart_;
     DevBuf<uint32_t> wcount_;
     DevBuf<double> epart_;  // per-part results of the E = Z^T A Z kernel
+    DevBuf<double> dperm_;  // d in agg_nodes order
+    DevBuf<uint8_t> fperm_; // fixed in agg_nodes order
 };
 
 }  // namespace mphy

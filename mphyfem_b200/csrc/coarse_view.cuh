@@ -17,6 +17,8 @@ struct CoarseView {
     const int32_t* agg_nodes;
     const double* d;         // [n_node][3] (x_n - c_agg) / H_agg at setup
     const uint8_t* fixed;    // [3 n_node]
+    const double* dperm;     // [n_node][3] d in the order of agg_nodes (the restriction's loads)
+    const uint8_t* fperm;    // [3 n_node] fixed in the order of agg_nodes
     // [kp][kp] inverse of E (row-major), FP64: with a large stiffness contrast E is so
     // ill-conditioned that rounding its inverse to FP32 makes the coarse term indefinite, and CG
     // on an indefinite preconditioner stalls

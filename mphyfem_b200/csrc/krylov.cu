@@ -463,7 +463,8 @@ __device__ __forceinline__ void restrict_node(bool lin, const double rr[3], cons
 }
 
 // w = Z^T r per aggregate. Work item (a, part) sums a contiguous part of aggregate a's node
-// list, two nodes per thread and step with every load issued before the arithmetic; the CTA
+// list, two nodes per thread and step with every load issued before the arithmetic (offsets and
+// mask from copies in node-list order, coalesced; only r is gathered); the CTA
 // that finishes an aggregate's last part adds the parts' sums in part order, so w does not
 // depend on which CTA ran which part. A persistent grid walks the items.
 template <typename XT>
@@ -483,9 +484,10 @@ __global__ void __launch_bounds__(kThreads, 3) coarse_restrict_kernel(CoarseView
         double w[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
         for (int64_t i = lo + threadIdx.x; i < hi; i += 2 * (int64_t)blockDim.x) {
             const bool two = i + blockDim.x < hi;
+            const int64_t li[2] = {i, two ? i + blockDim.x : i};  // positions in the node list
             int64_t nd[2];
-            nd[0] = cv.agg_nodes[i];
-            nd[1] = two ? cv.agg_nodes[i + blockDim.x] : nd[0];
+            nd[0] = cv.agg_nodes[li[0]];
+            nd[1] = cv.agg_nodes[li[1]];
             XT rv[2][3];
             double dv[2][3];
             uint8_t fx[2][3];
@@ -493,9 +495,9 @@ __global__ void __launch_bounds__(kThreads, 3) coarse_restrict_kernel(CoarseView
             for (int k = 0; k < 2; ++k)
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
+                    dv[k][c] = cv.dperm[3 * li[k] + c];
+                    fx[k][c] = cv.fperm[3 * li[k] + c];
                     rv[k][c] = r[3 * nd[k] + c];
-                    dv[k][c] = cv.d[3 * nd[k] + c];
-                    fx[k][c] = cv.fixed[3 * nd[k] + c];
                 }
 #pragma unroll
             for (int k = 0; k < 2; ++k) {
