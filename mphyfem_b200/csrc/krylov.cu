@@ -76,6 +76,23 @@ __device__ __forceinline__ T ld_once(const T* p) {
     return __ldcs(p);
 }
 
+// two consecutive vector entries as one 8- or 16-byte access
+template <typename T>
+struct Pair;
+template <>
+struct Pair<double> {
+    using type = double2;
+};
+template <>
+struct Pair<float> {
+    using type = float2;
+};
+// every pointer aligned for the paired access (16 bytes covers both types)
+__device__ __forceinline__ bool aligned16(const void* a, const void* b, const void* c, const void* d) {
+    return ((reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(b) | reinterpret_cast<uintptr_t>(c) |
+             reinterpret_cast<uintptr_t>(d)) & 15) == 0;
+}
+
 // Deterministic block sum (fixed butterfly per warp, fixed order across warps); valid in all
 // threads of warp 0.
 __device__ __forceinline__ double block_sum(double v, double* sh) {
@@ -370,6 +387,30 @@ __global__ void __launch_bounds__(kThreads) pcg_update_kernel(int64_t n, XT* __r
     __shared__ double sh[32];
     if (st->done) return;
     const XT alpha = (XT)st->alpha;
+    if (!JAC && aligned16(x, r, p, q)) {
+        // no reduction: 16-byte pairs, the same arithmetic per element
+        using V = typename Pair<XT>::type;
+        const int64_t n2 = n >> 1;
+        V* x2 = reinterpret_cast<V*>(x);
+        V* r2 = reinterpret_cast<V*>(r);
+        const V* p2 = reinterpret_cast<const V*>(p);
+        const V* q2 = reinterpret_cast<const V*>(q);
+        for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n2; i += (int64_t)gridDim.x * blockDim.x) {
+            V xv = ld_once(x2 + i), rv = r2[i];
+            const V pv = p2[i], qv = ld_once(q2 + i);
+            xv.x = xv.x + alpha * pv.x;
+            xv.y = xv.y + alpha * pv.y;
+            rv.x = rv.x - alpha * qv.x;
+            rv.y = rv.y - alpha * qv.y;
+            __stcs(x2 + i, xv);
+            r2[i] = rv;
+        }
+        if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+            x[n - 1] = x[n - 1] + alpha * p[n - 1];
+            r[n - 1] = r[n - 1] - alpha * q[n - 1];
+        }
+        return;
+    }
     const bool unprec = st->norm_type == 1;
     double a1 = 0.0, a2 = 0.0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -404,6 +445,22 @@ __global__ void __launch_bounds__(kThreads) pcg_direction_kernel(int64_t n, XT* 
                                                                  const PcgState* st) {
     if (st->done) return;
     const XT beta = (XT)st->beta;
+    if (aligned16(p, z, p, z)) {
+        // 16-byte pairs, the same arithmetic per element
+        using V = typename Pair<XT>::type;
+        const int64_t n2 = n >> 1;
+        V* p2 = reinterpret_cast<V*>(p);
+        const V* z2 = reinterpret_cast<const V*>(z);
+        for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n2; i += (int64_t)gridDim.x * blockDim.x) {
+            const V zv = ld_once(z2 + i);
+            V pv = p2[i];
+            pv.x = zv.x + beta * pv.x;
+            pv.y = zv.y + beta * pv.y;
+            p2[i] = pv;
+        }
+        if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) p[n - 1] = z[n - 1] + beta * p[n - 1];
+        return;
+    }
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         p[i] = ld_once(z + i) + beta * p[i];
 }
