@@ -33,18 +33,22 @@ struct CoarseView {
 // The coarse field at node n, (Z c)_n, with d the node's scaled offset from its aggregate's
 // centroid. Rigid-body modes: c = (translation t, rotations w) and u = t + w x d with the
 // mode order of the restriction; linear modes: c = (a, B row-major) and u = a + B d.
-__device__ __forceinline__ void coarse_node_value(const CoarseView& cv, int64_t n, double zc[3]) {
-    const double dx = cv.d[3 * n], dy = cv.d[3 * n + 1], dz = cv.d[3 * n + 2];
+// The same with the node's aggregate and offsets already loaded.
+__device__ __forceinline__ void coarse_node_value(const CoarseView& cv, int32_t agg, double dx, double dy, double dz,
+                                                  double zc[3]) {
     if (cv.nm == 12) {
-        const double* c = cv.c + 12 * (int64_t)cv.agg[n];
+        const double* c = cv.c + 12 * (int64_t)agg;
 #pragma unroll
         for (int a = 0; a < 3; ++a) zc[a] = c[a] + c[3 + 3 * a] * dx + c[4 + 3 * a] * dy + c[5 + 3 * a] * dz;
     } else {
-        const double* c = cv.c + 6 * (int64_t)cv.agg[n];
+        const double* c = cv.c + 6 * (int64_t)agg;
         zc[0] = c[0] - dy * c[3] + dz * c[5];
         zc[1] = c[1] + dx * c[3] - dz * c[4];
         zc[2] = c[2] + dy * c[4] - dx * c[5];
     }
+}
+__device__ __forceinline__ void coarse_node_value(const CoarseView& cv, int64_t n, double zc[3]) {
+    coarse_node_value(cv, cv.agg[n], cv.d[3 * n], cv.d[3 * n + 1], cv.d[3 * n + 2], zc);
 }
 #endif
 

@@ -674,39 +674,82 @@ __global__ void __launch_bounds__(kThreads) coarse_final_kernel(int32_t n_node, 
     if (!INIT && st->done) return;
     const bool unprec = INIT ? norm_type == 1 : st->norm_type == 1;
     double a1 = 0.0, a2 = 0.0;
-    // nodes n and n + stride per step (the order of a plain grid-stride loop), every load of
-    // both issued before the first store
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t n0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n0 < n_node; n0 += 2 * stride) {
-        const bool two = n0 + stride < n_node;
-        const int64_t nd[2] = {n0, two ? n0 + stride : n0};
-        double zc[2][3];
-        XT rv[2][3], dv[2][3];
-        uint8_t fx[2][3];
+    // a thread takes the adjacent nodes 2t and 2t + 1: their six DOFs of r, D^-1, z (and p) and
+    // their six offsets are three paired accesses each; every load comes before the first store
+    using V = typename Pair<XT>::type;
+    const bool paired = aligned16(r, z, dinv, INIT ? (const void*)p : (const void*)z) && aligned16(cv.d, cv.d, cv.d, cv.d);
+    const int64_t npair = ((int64_t)n_node + 1) >> 1;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < npair; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t n0 = 2 * t;
+        const int cnt = n0 + 1 < n_node ? 2 : 1;
+        XT rv[6], dv[6];
+        double od[6];
+        uint8_t fx[6];
+        int32_t ag[2];
+        if (cnt == 2 && paired) {
+            const V* r2 = reinterpret_cast<const V*>(r + 3 * n0);
+            const V* v2 = reinterpret_cast<const V*>(dinv + 3 * n0);
+            const double2* o2 = reinterpret_cast<const double2*>(cv.d + 3 * n0);
 #pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            coarse_node_value(cv, nd[k], zc[k]);
+            for (int q = 0; q < 3; ++q) {
+                const V a = r2[q], b = v2[q];
+                const double2 o = o2[q];
+                rv[2 * q] = a.x;
+                rv[2 * q + 1] = a.y;
+                dv[2 * q] = b.x;
+                dv[2 * q + 1] = b.y;
+                od[2 * q] = o.x;
+                od[2 * q + 1] = o.y;
+            }
+        } else {
 #pragma unroll
-            for (int a = 0; a < 3; ++a) {
-                rv[k][a] = r[3 * nd[k] + a];
-                dv[k][a] = dinv[3 * nd[k] + a];
-                fx[k][a] = cv.fixed[3 * nd[k] + a];
+            for (int e = 0; e < 6; ++e) {
+                const bool in = e < 3 * cnt;
+                rv[e] = in ? r[3 * n0 + e] : XT(0);
+                dv[e] = in ? dinv[3 * n0 + e] : XT(0);
+                od[e] = in ? cv.d[3 * n0 + e] : 0.0;
             }
         }
 #pragma unroll
+        for (int e = 0; e < 6; ++e) fx[e] = e < 3 * cnt ? cv.fixed[3 * n0 + e] : (uint8_t)1;
+        ag[0] = cv.agg[n0];
+        ag[1] = cnt == 2 ? cv.agg[n0 + 1] : ag[0];
+        XT zv[6];
+#pragma unroll
         for (int k = 0; k < 2; ++k) {
-            if (k == 1 && !two) break;
+            double zc[3];
+            coarse_node_value(cv, ag[k], od[3 * k], od[3 * k + 1], od[3 * k + 2], zc);
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
-                const int64_t i = 3 * nd[k] + a;
-                const XT ri = rv[k][a];
-                const XT zi = (XT)((double)dv[k][a] * (double)ri + (fx[k][a] ? 0.0 : zc[k][a]));
-                z[i] = zi;
-                if (INIT) p[i] = zi;
-                a1 += (double)ri * (double)zi;
-                a2 += unprec ? (double)ri * (double)ri : (double)zi * (double)zi;
+                const int e = 3 * k + a;
+                zv[e] = (XT)((double)dv[e] * (double)rv[e] + (fx[e] ? 0.0 : zc[a]));
             }
         }
+        if (cnt == 2 && paired) {
+            V* z2 = reinterpret_cast<V*>(z + 3 * n0);
+            V* p2 = reinterpret_cast<V*>(p + 3 * n0);
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                V v;
+                v.x = zv[2 * q];
+                v.y = zv[2 * q + 1];
+                z2[q] = v;
+                if (INIT) p2[q] = v;
+            }
+        } else {
+#pragma unroll
+            for (int e = 0; e < 6; ++e)
+                if (e < 3 * cnt) {
+                    z[3 * n0 + e] = zv[e];
+                    if (INIT) p[3 * n0 + e] = zv[e];
+                }
+        }
+#pragma unroll
+        for (int e = 0; e < 6; ++e)
+            if (e < 3 * cnt) {
+                a1 += (double)rv[e] * (double)zv[e];
+                a2 += unprec ? (double)rv[e] * (double)rv[e] : (double)zv[e] * (double)zv[e];
+            }
     }
     a1 = block_sum(a1, sh);
     if (threadIdx.x == 0) part_rz[blockIdx.x] = a1;
