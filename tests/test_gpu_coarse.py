@@ -81,3 +81,27 @@ def test_linear_modes_need_fewer_iterations(env):
         assert rc == 0
         its[(agg, modes)] = it
     assert its[(64, 12)] < its[(64, 6)], its
+
+
+def test_many_aggregates_one_item_each(env, oracle):
+    """About 1,400 aggregates, more than two per resident CTA of the E = Z^T A Z kernel and of the
+    restriction. Both then take one work item per aggregate, with no cross-CTA part sums. The
+    checks are the same as above: the FP64 oracle's solution, and the iteration count of the
+    numpy restatement on the same aggregate grid."""
+    from oracle import fsai_ref, twolevel_ref
+    torch, api, _lib, ctx = env
+    p = meshgen.hex8_cantilever(40, 20, 20)
+    sol, pat, rc, its, x = _solve(api, _lib, ctx, p, torch, rtol=1e-12, coarse_aggregates=1500)
+    assert rc == 0
+    info = sol.coarse_info()
+    assert int(np.prod(info["grid"])) >= 1184, info  # 2 x (4 CTAs per SM x 148 SMs)
+    op = oracle.OracleProblem(p)
+    val, _, _, _ = op.assemble(np.zeros(p.n_dof))
+    free = np.flatnonzero(p.fixed == 0)
+    xo, _, _, _ = op.cg(val, 0.2 * p.fnodal[free], rtol=1e-13)
+    assert np.linalg.norm(x[free] - xo) <= 1e-9 * np.linalg.norm(xo)
+    _, _, rp, col = op.pattern()
+    A = fsai_ref.full_operator(p.n_node, p.fixed, rp, col, val)
+    Minv = twolevel_ref.preconditioner(A, p.coords, p.fixed, info["grid"])
+    _, its_ref = twolevel_ref.pcg(A, 0.2 * p.fnodal * (p.fixed == 0), Minv, rtol=1e-12)
+    assert abs(its - its_ref) <= max(2, 0.03 * its_ref), (its, its_ref)
