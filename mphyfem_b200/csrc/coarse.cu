@@ -5,8 +5,9 @@
 //   1. centroids of the current coordinates per aggregate and scaled offsets d_n = (x_n - c_a)/H;
 //   2. E = Z^T A Z: the CTAs of an aggregate walk its nodes' matrix rows and accumulate the 6x6
 //      blocks E[a][b] for its neighbour aggregates (b <= a with rigid-body modes: the
-//      factorisation reads the lower triangle); the last of them stores the blocks -- every
-//      block of E is written once, no atomics in global memory;
+//      factorisation reads the lower triangle); the last of them, found by a per-aggregate
+//      ticket, stores the blocks -- every block of E is written once, never added to in global
+//      memory;
 //   3. E = L L^T by a right-looking blocked Cholesky (64x64 tiles, FP64), W = L^{-1} by blocked
 //      forward substitution, E^{-1} = W^T W, kept in FP64 for the per-iteration GEMV (FP32
 //      rounding of the inverse of an ill-conditioned E can make it indefinite).
