@@ -194,15 +194,17 @@ int mphy_elem_eval_tc(mphy_ctx* ctx, const mphy_mesh* mesh, const double* disp_d
                       double* Ke_dev, double* Re_dev, int64_t* first_bad);
 
 /* Allocation-free variant of mphy_elem_eval for callers that cannot let the library call
- * cudaMalloc (their mesh already lives in device memory under their own allocator, or they run
- * under a no-allocation policy). No counterpart in the reference: it is the same element
+ * cudaMalloc (their mesh already lives in device memory under their own arena allocator, or they
+ * run under a no-allocation policy). No counterpart in the reference: it is the same element
  * evaluation taking the caller's device arrays directly -- coords_dev [n_node][3], conn_dev
  * [n_elem][npe], mat_id_dev [n_elem], mats_dev [n_mat][3] = {mu, Kinv, Utype}, disp_dev
- * [3*n_node] -- and writing Ke_dev / Re_dev as mphy_elem_eval does. Its scratch is a fixed
- * ~32 KB device array inside libmphy.so (held by every GPU that loads it until exit), so n_mat is
- * limited to 1024 (larger values return MPHY_ERR_INVALID_ARG). The first call on a device looks
- * up that array's device address; make that first call before any stream capture. Calls share
- * the scratch: calls that overlap on the GPU race and must be serialised by the caller. */
+ * [3*n_node] -- and writing Ke_dev / Re_dev as mphy_elem_eval does. Ids out of range and rows
+ * with Kinv <= 0 return MPHY_ERR_INVALID_ARG. Its scratch is a fixed ~32 KB device array inside
+ * libmphy.so (held by every GPU that loads it until exit), so n_mat is limited to 1024 (larger
+ * values return MPHY_ERR_INVALID_ARG). The first call on a device looks up that array's device
+ * address; make that first call before any stream capture. Every call blocks the calling host
+ * thread until its result is ready (it synchronises the context's stream). Calls share the
+ * scratch: calls that overlap on the GPU race and must be serialised by the caller. */
 int mphy_elem_eval_noalloc(mphy_ctx* ctx, int32_t n_node, const double* coords_dev, int32_t n_elem,
                            int32_t npe, const int32_t* conn_dev, const int32_t* mat_id_dev,
                            int32_t n_mat, const double* mats_dev, const double* disp_dev,

@@ -2,17 +2,21 @@
 //
 // Some callers cannot let a library call cudaMalloc: a finite-element code that already holds
 // its mesh in device memory under its own arena allocator (every byte of the device is
-// reserved up front), a host application under a no-allocation policy in its time-stepping
-// loop, or code that wants the call recorded into its own CUDA graph where a cudaMalloc would
-// break the capture. mphy_elem_eval needs a mesh handle (which copies the mesh) and a small
-// per-call scratch buffer for the first-bad-element flag; mphy_elem_eval_noalloc takes the
-// caller's device arrays directly and keeps its scratch -- the flag, a validation flag and the
-// material table widened to the kernel's 4-double rows -- in one file-scope __device__ array.
+// reserved up front, so an allocation behind its back can fail or fragment the arena), or a
+// host application under a no-allocation policy in its time-stepping loop. mphy_elem_eval needs
+// a mesh handle (which copies the mesh) and a small per-call scratch buffer for the
+// first-bad-element flag; mphy_elem_eval_noalloc takes the caller's device arrays directly and
+// keeps its scratch -- the flag, a validation flag and the material table widened to the
+// kernel's 4-double rows -- in one file-scope __device__ array.
 //
 // That array (kNoAllocMaxMaterials materials, about 32 KB) is part of the library image: every
 // GPU that loads libmphy.so holds it until the process exits. All calls share it and it keeps
 // the last call's contents, so each call resets the flags it relies on; calls that overlap on
 // the GPU (other streams, other host threads) race on it and must be serialised by the caller.
+// The first call on a device looks up the array's device address (cudaGetSymbolAddress). Every
+// call runs on the context's stream and blocks the calling host thread until its result is
+// ready: it synchronises that stream twice, once after the input checks and once to read the
+// first-bad-element flag.
 #include <climits>
 #include <mutex>
 
@@ -53,13 +57,17 @@ NoAllocScratch* scratch_for_device(int device) {
     return g_scratch_ptr[device];
 }
 
-// Range checks the kernel itself does not make: connectivity within [0, n_node), material ids
-// within [0, n_mat).
+// Checks the kernel itself does not make, the same ones mphy_mesh_create makes on the host:
+// connectivity within [0, n_node), material ids within [0, n_mat), every material row's Kinv
+// (column 1 of the [n_mat][3] table) positive.
 __global__ void validate_ids(int64_t n_conn, const int32_t* __restrict__ conn, int32_t n_node, int32_t n_elem,
-                             const int32_t* __restrict__ mat_id, int32_t n_mat, int32_t* invalid) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n_conn; i += (int64_t)gridDim.x * blockDim.x) {
-        if (conn[i] < 0 || conn[i] >= n_node) *invalid = 1;
+                             const int32_t* __restrict__ mat_id, int32_t n_mat, const double* __restrict__ mats,
+                             int32_t* invalid) {
+    const int64_t n = n_conn > n_mat ? n_conn : n_mat;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        if (i < n_conn && (conn[i] < 0 || conn[i] >= n_node)) *invalid = 1;
         if (i < n_elem && (mat_id[i] < 0 || mat_id[i] >= n_mat)) *invalid = 1;
+        if (i < n_mat && !(mats[3 * i + 1] > 0.0)) *invalid = 1;
     }
 }
 
@@ -87,16 +95,20 @@ extern "C" int mphy_elem_eval_noalloc(mphy_ctx* c, int32_t n_node, const double*
         MPHY_CUDA(cudaMemsetAsync(&ptr->invalid, 0, sizeof(int32_t), s));
         MPHY_CUDA(cudaMemcpy2DAsync(ptr->mats, 4 * sizeof(double), mats_dev, 3 * sizeof(double), 3 * sizeof(double),
                                     n_mat, cudaMemcpyDeviceToDevice, s));
-        if (n_elem > 0) {
+        {
             const int64_t n_conn = (int64_t)n_elem * npe;
-            unsigned grid = ceil_div(n_conn, 256);
+            unsigned grid = ceil_div(n_conn > n_mat ? n_conn : (int64_t)n_mat, 256);
             if (grid > (unsigned)c->sm_count * 8) grid = c->sm_count * 8;
-            validate_ids<<<grid, 256, 0, s>>>(n_conn, conn_dev, n_node, n_elem, mat_id_dev, n_mat, &ptr->invalid);
+            validate_ids<<<grid, 256, 0, s>>>(n_conn, conn_dev, n_node, n_elem, mat_id_dev, n_mat, mats_dev,
+                                              &ptr->invalid);
             MPHY_CUDA(cudaGetLastError());
             int32_t invalid = 0;
             MPHY_CUDA(cudaMemcpyAsync(&invalid, &ptr->invalid, sizeof(invalid), cudaMemcpyDeviceToHost, s));
             MPHY_CUDA(cudaStreamSynchronize(s));
-            MPHY_REQUIRE(invalid == 0, MPHY_ERR_INVALID_ARG, "connectivity or material id out of range");
+            MPHY_REQUIRE(invalid == 0, MPHY_ERR_INVALID_ARG,
+                         "connectivity or material id out of range, or a material row with Kinv <= 0");
+        }
+        if (n_elem > 0) {
             ElemArgs a{};
             a.n_elem = n_elem;
             a.coords = coords_dev;

@@ -28,20 +28,25 @@ def setup():
 
 
 def _call_noalloc(torch, api, _lib, ctx, p, mats, disp, tangent=0):
-    dev = lambda a, dt: torch.tensor(np.ascontiguousarray(a), dtype=dt, device="cuda")  # noqa: E731
+    def dev(a, dt):
+        # at least one entry, so that an empty element list still passes valid (non-null) pointers
+        a = np.ascontiguousarray(a).ravel()
+        t = torch.zeros(max(a.size, 1), dtype=dt, device="cuda")
+        t[:a.size] = torch.as_tensor(a, dtype=dt)
+        return t
     coords = dev(p.coords, torch.float64)
     conn = dev(p.conn, torch.int32)
     mat_id = dev(p.mat_id, torch.int32)
     m = dev(mats, torch.float64)
     u = dev(disp, torch.float64)
     ns = 3 * p.npe
-    Ke = torch.full((p.n_elem, ns, ns), float("nan"), dtype=torch.float64, device="cuda")
-    Re = torch.full((p.n_elem, ns), float("nan"), dtype=torch.float64, device="cuda")
+    Ke = torch.full((max(p.n_elem, 1), ns, ns), float("nan"), dtype=torch.float64, device="cuda")
+    Re = torch.full((max(p.n_elem, 1), ns), float("nan"), dtype=torch.float64, device="cuda")
     bad = C.c_int64(123)
     ptr = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
     rc = ctx.lib.mphy_elem_eval_noalloc(ctx.h, p.n_node, ptr(coords), p.n_elem, p.npe, ptr(conn), ptr(mat_id),
-                                        m.shape[0], ptr(m), ptr(u), tangent, ptr(Ke), ptr(Re), C.byref(bad))
-    return rc, Ke.cpu().numpy(), Re.cpu().numpy(), bad.value
+                                        len(mats), ptr(m), ptr(u), tangent, ptr(Ke), ptr(Re), C.byref(bad))
+    return rc, Ke[:p.n_elem].cpu().numpy(), Re[:p.n_elem].cpu().numpy(), bad.value
 
 
 def _reference(torch, api, p, disp, tangent=0):
@@ -98,4 +103,35 @@ def test_noalloc_flags_reset_between_calls_and_limits(setup):
     q.mat_id = q.mat_id.copy()
     q.mat_id[5] = 1
     rc, _, _, _ = _call_noalloc(torch, api, _lib, ctx, q, q.mats, np.zeros(q.n_dof))
+    assert rc == _lib.ERR_INVALID_ARG
+
+
+def test_noalloc_largest_table_empty_mesh_and_bad_material(setup):
+    torch, api, _lib = setup
+    ctx = api.Context(0)
+    p = meshgen.hex8_cantilever(4, 2, 2)
+    rng = np.random.default_rng(11)
+    u = 0.01 * rng.standard_normal(p.n_dof) * (p.fixed == 0)
+    # the largest table the fixed scratch holds: 1024 rows, every element on the last one
+    mats = np.tile(meshgen.nh_material(1.0, 10.0), (1024, 1))
+    mats[1023] = meshgen.nh_material(0.7, 25.0, utype=4)
+    q = meshgen.hex8_cantilever(4, 2, 2)
+    q.mats = mats[1023:1024].copy()
+    q.mat_id = np.zeros(q.n_elem, dtype=np.int32)
+    p.mat_id = np.full(p.n_elem, 1023, dtype=np.int32)
+    rc, Ke, Re, bad = _call_noalloc(torch, api, _lib, ctx, p, mats, u)
+    assert rc == _lib.OK and bad == -1
+    Kr, Rr, br = _reference(torch, api, q, u)
+    assert br == -1 and _close(Ke, Kr) and _close(Re, Rr)
+    # an empty element list launches no element kernel and reports no bad element
+    e = meshgen.hex8_cantilever(4, 2, 2)
+    e.conn = e.conn[:0]
+    e.mat_id = e.mat_id[:0]
+    rc, Ke, Re, bad = _call_noalloc(torch, api, _lib, ctx, e, e.mats, np.zeros(e.n_dof))
+    assert rc == _lib.OK and bad == -1 and Ke.size == 0
+    # a material row with Kinv = 0 is refused, as mphy_mesh_create refuses it
+    z = meshgen.hex8_cantilever(4, 2, 2)
+    zm = np.stack([meshgen.nh_material(1.0, 10.0), meshgen.nh_material(1.0, 10.0)])
+    zm[1, 1] = 0.0
+    rc, _, _, _ = _call_noalloc(torch, api, _lib, ctx, z, zm, np.zeros(z.n_dof))
     assert rc == _lib.ERR_INVALID_ARG
