@@ -126,82 +126,120 @@ def _read_traffic(kind: str):
 
 
 # ------------------------------------------------------------------------------------- CPU side
-def cpu_newton_estimate(prob, gpu_its: int, rtol: float):
-    """Time the oracle (CPU restatement of the reference path) on bounded samples and scale to
-    the full workload: assembly per element on a 64x16x16 block, one CG iteration per nonzero on a
-    96x24x24 block, at the GPU's Krylov iteration count. About 10-20 s of CPU work."""
-    from mphyfem_b200 import meshgen
-    from oracle import binding
-    binding.build()
-    nthreads = os.cpu_count() or 1
-    a = meshgen.hex8_cantilever(64, 16, 16)
-    oa = binding.OracleProblem(a)
-    u0 = np.zeros(a.n_dof)
-    oa.assemble(u0, nthreads=nthreads)
-    t0 = time.perf_counter()
-    reps = 3
-    for _ in range(reps):
-        oa.assemble(u0, nthreads=nthreads, want_reac=False)
-    t_elem = (time.perf_counter() - t0) / reps / a.n_elem
-    b = meshgen.hex8_cantilever(96, 24, 24)
-    ob = binding.OracleProblem(b)
-    val, rhs, _, _ = ob.assemble(np.zeros(b.n_dof), nthreads=nthreads, want_reac=False)
-    rhs = rhs + b.dt * b.fnodal[np.flatnonzero(b.fixed == 0)]
-    cg_its = 60
-    t0 = time.perf_counter()
-    ob.cg(val, rhs, rtol=1e-30, maxit=cg_its, nthreads=nthreads)
-    t_cg_nnz = (time.perf_counter() - t0) / cg_its / ob.nnz
-    # nnz of the full workload from its node-block structure (3 free DOFs per free node)
-    nnz_full = _structured_nnz(prob)
-    t_asm = t_elem * prob.n_elem
-    t_iter = t_cg_nnz * nnz_full
-    t_newton = t_asm + gpu_its * t_iter
+def _threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+class CpuReference:
+    """The oracle (the FP64 C++ restatement of the reference's path: element loop, Neo-Hookean,
+    AIJ assembly, PETSc-KSPCG Jacobi-PCG) on the workload's own mesh and matrix, on this host's
+    cores. Building it takes the reference's prepareMatrixPattern on the CPU (timed once)."""
+
+    def __init__(self, prob):
+        from oracle import binding
+        binding.build()
+        self.prob = prob
+        self.nt = _threads()
+        t0 = time.perf_counter()
+        self.op = binding.OracleProblem(prob)
+        self.pattern_s = time.perf_counter() - t0
+        self.u0 = np.zeros(prob.n_dof)
+        self.val, rhs, _, _ = self.op.assemble(self.u0, nthreads=self.nt, want_reac=False)
+        self.b = rhs + prob.dt * prob.fnodal[np.flatnonzero(prob.fixed == 0)]
+
+    def assembly_s(self, nthreads):
+        t0 = time.perf_counter()
+        self.op.assemble(self.u0, nthreads=nthreads, want_reac=False)
+        return time.perf_counter() - t0
+
+    def cg_iter_s(self, nthreads, its):
+        """Seconds per Jacobi-PCG iteration on the workload's matrix (its iterations, no stop)."""
+        t0 = time.perf_counter()
+        _, done, _, _ = self.op.cg(self.val, self.b, rtol=1e-30, maxit=its, nthreads=nthreads)
+        return (time.perf_counter() - t0) / max(done, 1)
+
+    def cg_full(self, rtol, maxit):
+        """Jacobi-PCG from x = 0 to ||b - A x|| <= rtol ||b|| on all cores: (its, seconds)."""
+        t0 = time.perf_counter()
+        _, its, _, st = self.op.cg(self.val, self.b, rtol=rtol, maxit=maxit, nthreads=self.nt, norm_type=1)
+        return its, time.perf_counter() - t0, st
+
+
+def cpu_baseline_sample(prob, krylov_its: int, its_source: str):
+    """The CPU baseline beside the GPU numbers: one Newton iteration of the workload (assembly +
+    Jacobi-PCG + update) on the oracle, timed on the workload's own data. Measured: one full
+    assembly single-threaded (the reference's element loop has no OpenMP) and on all cores, and
+    Jacobi-PCG iterations on the assembled matrix, 5 single-threaded and 20 on all cores. The
+    iteration count to the tolerance (krylov_its, from its_source) multiplies the measured
+    per-iteration time; that product is the extrapolated part. About 30-40 s of CPU work."""
+    ref = CpuReference(prob)
+    a1 = ref.assembly_s(1)
+    an = ref.assembly_s(ref.nt)
+    c1 = ref.cg_iter_s(1, 5)
+    cn = ref.cg_iter_s(ref.nt, 20)
+    t1 = a1 + krylov_its * c1
+    tn = an + krylov_its * cn
     return {
-        "value": 1.0 / t_newton, "unit": "Newton iter/s", "cores": nthreads, "kind": "port",
-        "sample": (f"oracle (FP64 C++ restatement, OpenMP {nthreads} threads): assembly timed on "
-                   f"{a.n_elem} elements ({t_elem * 1e6:.2f} us/elem), CG timed for {cg_its} iterations on "
-                   f"{ob.nnz} nonzeros; scaled to {prob.n_elem} elements / {nnz_full} nonzeros at the GPU's "
-                   f"{gpu_its} Krylov iterations (extrapolated)"),
-        "assembly_s": t_asm, "cg_iter_s": t_iter,
+        "value": 1.0 / tn, "unit": "Newton iter/s", "cores": ref.nt, "kind": "port",
+        "sample": (f"oracle (FP64 C++ restatement of the reference path) on this workload's mesh and matrix "
+                   f"({prob.n_elem} elements, {ref.op.nnz} nonzeros): one full assembly and 20 Jacobi-PCG "
+                   f"iterations timed on {ref.nt} threads, x {krylov_its} Krylov iterations ({its_source})"),
+        "measured": {"threads": ref.nt, "assembly_s": an, "cg_iter_s": cn, "assembly_s_1thread": a1,
+                     "cg_iter_s_1thread": c1, "pattern_build_s": ref.pattern_s},
+        "single_thread": {"value": 1.0 / t1, "unit": "Newton iter/s", "cores": 1},
+        "krylov_its": krylov_its, "krylov_its_source": its_source,
     }
 
 
-def _structured_nnz(prob):
-    nx, ny, nz = prob.meta["nx"], prob.meta["ny"], prob.meta["nz"]
-
-    def nb(n):  # neighbours of each grid index along one axis, summed over the axis
-        return np.array([min(i + 1, n) - max(i - 1, 0) + 1 for i in range(n + 1)])
-    bx, by, bz = nb(nx), nb(ny), nb(nz)
-    # free rows: nodes with i > 0; free columns: neighbours with i > 0
-    bx_free_rows = bx[1:].copy()
-    bx_free_rows[0] -= 1  # node i=1 loses its i=0 neighbour
-    blocks = int(bx_free_rows.sum()) * int(by.sum()) * int(bz.sum())
-    return 9 * blocks
-
-
 def run_reference(args):
+    """The reference arm: the reference's own method (AIJ assembly + PETSc-style Jacobi-PCG, FP64)
+    through the oracle on the host cores, on the same workload. Setup builds the pattern and the
+    matrix and runs one complete Jacobi-PCG solve to the workload's tolerance (its iteration count
+    and time are measured, not supplied). Each step is a bounded sample: one full assembly and
+    10 Jacobi-PCG iterations on all cores; the step's time is that assembly plus the measured
+    per-iteration time times the measured iteration count."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     prob = _workload(args.workload)
-    its = args.ref_its
-    samples = []
-    est = None
-    for _ in range(max(1, args.warmup)):
-        est = cpu_newton_estimate(prob, its, args.rtol)
-    for _ in range(max(1, args.steps)):
-        est = cpu_newton_estimate(prob, its, args.rtol)
-        samples.append(1.0 / est["value"])
-    t = statistics.median(samples)
+    t_setup = time.perf_counter()
+    ref = CpuReference(prob)
+    its, full_s, st = ref.cg_full(args.rtol, args.max_it)
+    setup_s = time.perf_counter() - t_setup
+    steps, walls, asm, cgi = [], [], [], []
+    for k in range(max(3, args.warmup) + args.steps):
+        w0 = time.perf_counter()
+        a = ref.assembly_s(ref.nt)
+        c = ref.cg_iter_s(ref.nt, 10)
+        if k >= max(3, args.warmup):
+            steps.append(a + its * c)
+            asm.append(a)
+            cgi.append(c)
+            walls.append(time.perf_counter() - w0)
+    t = statistics.median(steps)
     line = {
         "impl": "reference", "metric": METRIC, "value": 1.0 / t, "unit": "Newton iter/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": _config(prob, args.rtol),
-        "cpu_baseline": {k: est[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "method": "FP64 AIJ assembly + Jacobi-PCG (PETSc KSPCG + PCJACOBI semantics), the reference's method",
+        "cpu_baseline": {
+            "value": 1.0 / t, "unit": "Newton iter/s", "cores": ref.nt, "kind": "port",
+            "sample": (f"oracle on the workload's own matrix ({ref.op.nnz} nonzeros): per step one full assembly "
+                       f"and 10 Jacobi-PCG iterations on {ref.nt} threads; Krylov count {its} measured by one "
+                       f"complete solve to the true relative residual {args.rtol:g} at setup ({full_s:.1f} s)")},
+        "measured": {"threads": ref.nt, "krylov_its": its, "krylov_status": int(st), "cg_full_s": full_s,
+                     "assembly_s": statistics.median(asm), "cg_iter_s": statistics.median(cgi),
+                     "pattern_build_s": ref.pattern_s, "setup_s": setup_s,
+                     "sample_wall_s_per_step": statistics.median(walls)},
         "e2e": {"value": 1.0 / t, "unit": "Newton iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "note": "the reference (PETSc/Eigen/Boost/MPI/VTK build) cannot be built on this image; "
-                "its path is timed through the FP64 CPU restatement",
+        "note": "the reference (PETSc/Eigen/Boost/MPI/VTK build) cannot be built on this image; its path is timed "
+                "through the FP64 CPU restatement. ms_per_step is the full Newton iteration, from the measured "
+                "assembly and per-iteration times and the measured iteration count; each step's own wall-clock "
+                "is sample_wall_s_per_step",
     }
     print(json.dumps(line), flush=True)
 
@@ -249,6 +287,76 @@ def _time_steps(torch, stream, step, steps, warmup):
     ev1.record(stream)
     torch.cuda.synchronize()
     return ev0.elapsed_time(ev1), stats
+
+
+def _time_leg(torch, api, _lib, mesh, pat, args, prob, disp, fext, dev, method, steps):
+    """One more method on the bench step (u = 0, lambda = dt, one Newton iteration): one untimed
+    iteration (graphs, preconditioner buffers), then `steps` timed with events on its stream."""
+    precision, pc, coarse = method
+    s = _make_solver(api, _lib, mesh, pat, args, precision, pc, coarse)
+    st = torch.cuda.ExternalStream(s.stream, device=dev)
+
+    def step():
+        disp.zero_()
+        return s.newton_iteration(disp, fext, prob.dt)
+
+    t, stats = _time_steps(torch, st, step, steps, 1)
+    out = {"method": _method_name(argparse.Namespace(**dict(vars(args), precision=precision, pc=pc, coarse=coarse))),
+           "ms_per_newton_iter": t / len(stats),
+           "krylov_its": int(statistics.median([q.krylov_its for q in stats])),
+           "krylov_status": sorted({_lib.status_string(int(q.status)) for q in stats}),
+           "true_relres": s.true_residual(),
+           "solve_ms": statistics.median([q.t_solve_ms for q in stats]),
+           "assembly_ms": statistics.median([q.t_assembly_ms for q in stats])}
+    if pc != "jacobi":
+        pcl = s.pc_last()
+        out["preconditioner"] = {"setup_ms": pcl["setup_ms"], "fallback": pcl["fallback"],
+                                 "first_relres": pcl["first_relres"]}
+    if coarse > 0:
+        out["coarse_setup_ms"] = s.coarse_info()["setup_ms"]
+    s.close()
+    return out
+
+
+def _parity_first_step(api, _lib, mesh, pat, args, prob, legs, newton_rtol=1e-8):
+    """Accuracy at the workload's size: the first load step (lambda = dt from u = 0) converged to
+    ||R|| < newton_rtol ||R_first|| with the consistent tangent (the reference's tangent need not
+    converge quadratically, or at all, at this load), by the plain FP64 GPU method (FP64 element
+    kernel, FP64 matrix, FP64 Jacobi-PCG: the FP64 solution) and by each method of `legs`.
+    Reports every method's Newton history and max|u - u64| / max|u64|."""
+    def run(method):
+        precision, pc, coarse = method
+        a = argparse.Namespace(**dict(vars(args), precision=precision, pc=pc, coarse=coarse))
+        s = api.SolverGpu(mesh, pat, rtol=args.rtol, max_it=args.max_it,
+                          precision={"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED,
+                                     "mixed32": _lib.PREC_MIXED_F32VEC, "mixed_tc": _lib.PREC_MIXED_TC}[precision],
+                          pc_type={"jacobi": _lib.PC_JACOBI, "fsai": _lib.PC_FSAI,
+                                   "learned": _lib.PC_FSAI_LEARNED}[pc],
+                          inner_rtol=args.inner_rtol, max_outer=args.max_outer, coarse_aggregates=coarse,
+                          coarse_modes=args.coarse_modes, norm_type=args.norm, tangent=_lib.TANGENT_CONSISTENT)
+        if pc == "learned":
+            _GNN[0].attach(s)
+        t0 = time.perf_counter()
+        r = api.newton_run(s, prob, max_newton=10, tol_rel=newton_rtol, t_final=prob.dt, max_steps=1)
+        wall = time.perf_counter() - t0
+        s.close()
+        hist = [{"iter": int(h[1]), "rhs_norm": float(h[2]), "krylov_its": int(h[3]),
+                 "krylov_status": _lib.status_string(int(h[4]))} for h in r.hist]
+        conv = len(r.hist) > 0 and r.hist[-1, 2] < newton_rtol * r.hist[0, 2]
+        return r.disp, {"method": _method_name(a), "newton": hist, "converged": bool(conv),
+                        "newton_status": _lib.status_string(int(r.status)), "wall_s": wall}
+
+    u64, ref = run(("fp64", "jacobi", 0))
+    out = {"case": f"first load step (lambda={prob.dt:g}) from u=0 to ||R|| < {newton_rtol:g} ||R_first||, "
+                   f"consistent tangent, Krylov to true relative residual {args.rtol:g}",
+           "fp64": ref}
+    scale = float(np.abs(u64).max())
+    for name, m in legs.items():
+        u, rec = run(m)
+        rec["disp_err_vs_fp64"] = float(np.abs(u - u64).max() / scale)
+        out[name] = rec
+    out["max_abs_u_fp64"] = scale
+    return out
 
 
 def run_ours(args):
@@ -337,24 +445,29 @@ def run_ours(args):
         e2e_total += e0.elapsed_time(e1)
     e2e_ms = ranks.max_over_ranks(e2e_total / e2e_steps, dev)
 
-    # the plain GPU method (FP64 Jacobi-PCG, the drop-in for the reference's KSPCG + PCJACOBI),
-    # same workload and step, measured in the same run
-    plain = None
-    if world == 1 and not args.no_plain and (args.precision, args.pc, args.coarse) != ("fp64", "jacobi", 0):
+    # the other methods on the same workload and step, measured in the same run (1 GPU): the
+    # plain GPU method (FP64 Jacobi-PCG, the drop-in for the reference's KSPCG + PCJACOBI) and the
+    # learned factorised preconditioner with the same coarse space
+    plain = learned_leg = parity = None
+    headline = (args.precision, args.pc, args.coarse)
+    if world == 1:
         sol.close()
-        psol = _make_solver(api, _lib, mesh, pat, args, "fp64", "jacobi", 0)
-        pstream = torch.cuda.ExternalStream(psol.stream, device=dev)
-
-        def pstep():
-            disp.zero_()
-            return psol.newton_iteration(disp, fext, prob.dt)
-
-        pms, pst = _time_steps(torch, pstream, pstep, max(1, min(args.steps, 2)), 1)
-        plain = {"method": "FP64 Jacobi-PCG (plain)", "ms_per_newton_iter": pms / len(pst),
-                 "krylov_its": int(statistics.median([q.krylov_its for q in pst])),
-                 "true_relres": psol.true_residual(),
-                 "speedup_of_this_method": (pms / len(pst)) / (ms / args.steps)}
-        psol.close()
+        if not args.no_plain and headline != ("fp64", "jacobi", 0):
+            plain = _time_leg(torch, api, _lib, mesh, pat, args, prob, disp, fext, dev, ("fp64", "jacobi", 0),
+                              max(1, min(args.steps, 2)))
+            plain["speedup_of_this_method"] = plain["ms_per_newton_iter"] / (ms / args.steps)
+        if not args.no_learned and headline[1] != "learned":
+            lh = (args.precision, "learned", args.coarse)
+            learned_leg = _time_leg(torch, api, _lib, mesh, pat, args, prob, disp, fext, dev, lh,
+                                    max(1, min(args.steps, 3)))
+            learned_leg["ms_vs_headline"] = learned_leg["ms_per_newton_iter"] / (ms / args.steps)
+        if not args.no_parity:
+            legs = {"headline": headline}
+            if learned_leg is not None:
+                legs["learned"] = (args.precision, "learned", args.coarse)
+            parity = _parity_first_step(api, _lib, mesh, pat, args, prob, legs)
+            if learned_leg is not None:
+                learned_leg["disp_err_vs_fp64"] = parity["learned"]["disp_err_vs_fp64"]
 
     if rank != 0:
         if world > 1:
@@ -362,14 +475,19 @@ def run_ours(args):
         return
     cpu = None
     if world == 1 and not args.no_cpu:
-        cpu = cpu_newton_estimate(prob, args.ref_its, args.rtol)
+        if plain is not None:
+            k_its, k_src = plain["krylov_its"], "the Jacobi-PCG count of the plain FP64 GPU leg measured in this run"
+        else:
+            k_its, k_src = int(statistics.median(its)), "this run's Krylov count"
+        cpu = cpu_baseline_sample(prob, k_its, k_src)
     line = {
         "metric": METRIC, "value": world * args.steps / (ms * 1e-3), "unit": "Newton iter/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
         "data": "synthetic",
-        "config": dict(_config(prob, args.rtol), method=_method_name(args),
-                       parallelism=f"replicas{world}" if world > 1 else "single"),
+        "config": _config(prob, args.rtol),
+        "method": _method_name(args),
+        "parallelism": f"replicas{world}" if world > 1 else "single",
         "krylov_its": int(statistics.median(its)),
         "krylov_status": [_lib.status_string(k) for k in kstatus],
         "true_relres": relres,
@@ -380,6 +498,8 @@ def run_ours(args):
                      "algorithmic_bytes": asm_bytes, "achieved_gbs": asm_bytes / (asm_ms * 1e-3) / 1e9,
                      "frac": asm_bytes / (asm_ms * 1e-3) / 1e9 / peak},
         "plain_gpu": plain,
+        "learned_gpu": learned_leg,
+        "parity": parity,
         "e2e": {"value": world * 1e3 / e2e_ms, "unit": "Newton iter/s", "h2d_bytes_per_step": 2 * prob.n_dof * 8,
                 "d2h_bytes_per_step": prob.n_dof * 8},
         "roofline": {"kernel": f"spmv_kernel (SELL-32 3x3, {'FP64' if vbytes == 8 else 'FP32'} values, FP64 vectors)",
@@ -387,7 +507,8 @@ def run_ours(args):
                      "frac": achieved / peak,
                      "traffic": _read_traffic("spmv_fp64" if vbytes == 8 else "spmv_mixed"),
                      "algorithmic_bytes": spmv_bytes, "launch_ms": spmv_ms},
-        "cpu_baseline": None if cpu is None else {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "cpu_baseline": None if cpu is None else {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample",
+                                                                      "measured", "single_thread", "krylov_its")},
         "clocks": clk.summary(),
         "gpu_launches": launches,
     }
@@ -410,19 +531,13 @@ def run_batched(args):
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=900))
     dev = f"cuda:{local}"
     allp = meshgen.batched_blocks(512, seed=11)
-    mine = ranks.shard_by_cost([q.n_elem for q in allp], world)[rank]
-    probs = [allp[i] for i in mine]
-    for q in probs:
+    for q in allp:
         q.newton_rtol = 1e-8
     ctx = api.Context(local)
     prec = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED}.get(args.precision, _lib.PREC_MIXED)
-    b = api.BatchGpu(probs, ctx, precision=prec, rtol=1e-10, norm_type=1, max_it=args.max_it,
-                     tangent=_lib.TANGENT_CONSISTENT)
-    b.set_coarse(8 if args.coarse > 0 else 0)
-    u = b.union
-    b.solver.calcStiffnessAndResidual(torch.zeros(u.n_dof, dtype=torch.float64, device=dev))
-    b.solver.addExternalForces(torch.tensor(u.fnodal, device=dev), 0.2)
-    b.autotune(maxit=0)
+    mine, b = ranks.batched_share(allp, rank, world, ctx, coarse_slabs=8 if args.coarse > 0 else 0, precision=prec,
+                                  rtol=1e-10, norm_type=1, max_it=args.max_it, tangent=_lib.TANGENT_CONSISTENT)
+    probs = [allp[i] for i in mine]
     for _ in range(args.warmup):
         b.newton_run(max_newton=15)
     torch.cuda.synchronize()
@@ -480,10 +595,11 @@ def main():
     ap.add_argument("--no-plain", dest="no_plain", action="store_true",
                     help="skip the same-run measurement of the plain FP64 Jacobi-PCG method")
     ap.add_argument("--max-it", dest="max_it", type=int, default=20000)
-    ap.add_argument("--ref-its", dest="ref_its", type=int, default=2434,
-                    help="Krylov iterations per Newton iteration for --impl reference: the Jacobi-PCG count "
-                         "this workload needs to a 1e-8 true relative residual (same algorithm on both arms)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-learned", dest="no_learned", action="store_true",
+                    help="skip the same-run measurement of the learned factorised preconditioner")
+    ap.add_argument("--no-parity", dest="no_parity", action="store_true",
+                    help="skip the first-load-step accuracy check against the FP64 GPU solution")
     args = ap.parse_args()
     if args.impl == "reference" and args.workload == "batched":
         if int(os.environ.get("RANK", "0")) == 0:

@@ -240,8 +240,18 @@ int mphy_solver_assemble(mphy_solver* s, const double* disp_dev, int64_t* first_
  * NULL; then n must equal n_elem). Adds to the current matrix; leaves ASSEMBLY_OK. */
 int mphy_solver_assemble_batch(mphy_solver* s, int32_t n, const int32_t* elem_ids_dev,
                                const double* Ke_dev, const double* Re_dev);
+/* The same with host arrays, for a caller that forms element matrices on the CPU one by one
+ * (SolverPetsc::assembleMatrixAndVector(row, col, Klocal, Flocal), SolverPetsc.h:72-74, called
+ * once per element by femSolidmechanics2.cpp:1097): elem_ids_host [n] (NULL: 0..n-1, n = n_elem),
+ * Ke_host [n][3npe][3npe] row-major, Re_host [n][3npe]. Copied to the device in chunks;
+ * ids outside [0, n_elem) return MPHY_ERR_INVALID_ARG. */
+int mphy_solver_assemble_batch_host(mphy_solver* s, int32_t n, const int32_t* elem_ids_host,
+                                    const double* Ke_host, const double* Re_host);
 /* rhs += scale * Fext[assyForSoln] (femSolidmechanics2.cpp:785-789); fext_dev: [3*n_node]. */
 int mphy_solver_add_nodal_forces(mphy_solver* s, const double* fext_dev, double scale);
+/* The same with a host array, the reference's VecSetValue(rhsVec, ii, Fext[assyForSoln[ii]],
+ * ADD_VALUES) loop (femSolidmechanics2.cpp:785-789) with Fext in host memory. */
+int mphy_solver_add_nodal_forces_host(mphy_solver* s, const double* fext_host, double scale);
 /* VecNorm(rhsVec, NORM_2) in FP64 (femSolidmechanics2.cpp:798-801). */
 int mphy_solver_rhs_norm(mphy_solver* s, double* norm_host);
 /* factoriseAndSolve (SolverPetsc.cpp:250-330): KSPSolve from x = 0. Returns MPHY_ERR_STATE unless
@@ -306,6 +316,8 @@ int mphy_solver_true_residual(mphy_solver* s, double* relres);
 /* Solution increment scattered to node-major layout (femSolidmechanics2.cpp:1183-1186):
  * dx_dev[assyForSoln[i]] = soln[i], prescribed DOFs 0. */
 int mphy_solver_get_solution(mphy_solver* s, double* dx_dev);
+/* The same into host memory (solnVec read back by factoriseSolveAndUpdate). */
+int mphy_solver_get_solution_host(mphy_solver* s, double* dx_host);
 /* disp_dev += solution (the update `SolnData.disp += SolnData.dispIncr`). */
 int mphy_solver_update_disp(mphy_solver* s, double* disp_dev);
 /* Copies for checks: CSR values in mphy_pattern_export_csr order [nnz], rhs over free DOFs

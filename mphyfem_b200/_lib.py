@@ -112,7 +112,9 @@ SIGNATURES = {
     "mphy_solver_zero": (C.c_int, [_vp]),
     "mphy_solver_assemble": (C.c_int, [_vp, _vp, _i64]),
     "mphy_solver_assemble_batch": (C.c_int, [_vp, C.c_int32, _vp, _vp, _vp]),
+    "mphy_solver_assemble_batch_host": (C.c_int, [_vp, C.c_int32, _i32, _d, _d]),
     "mphy_solver_add_nodal_forces": (C.c_int, [_vp, _vp, C.c_double]),
+    "mphy_solver_add_nodal_forces_host": (C.c_int, [_vp, _d, C.c_double]),
     "mphy_solver_rhs_norm": (C.c_int, [_vp, _d]),
     "mphy_solver_solve": (C.c_int, [_vp, _i32, _d]),
     "mphy_solver_spmv": (C.c_int, [_vp, _vp, _vp]),
@@ -134,6 +136,7 @@ SIGNATURES = {
     "mphy_solver_pc_last": (C.c_int, [_vp, _i32, C.POINTER(C.c_float), _i32, _i32, _d]),
     "mphy_solver_coarse_info": (C.c_int, [_vp, _i32, _i32, C.POINTER(C.c_float)]),
     "mphy_solver_get_solution": (C.c_int, [_vp, _vp]),
+    "mphy_solver_get_solution_host": (C.c_int, [_vp, _d]),
     "mphy_solver_update_disp": (C.c_int, [_vp, _vp]),
     "mphy_solver_export": (C.c_int, [_vp, _d, _d, _d]),
     "mphy_newton_iteration": (C.c_int, [_vp, _vp, _vp, C.c_double, C.c_double, C.POINTER(IterStats)]),

@@ -329,6 +329,27 @@ class NewtonResult:
     status: int
 
 
+def newton_run(solver: "SolverGpu", prob, max_newton: int = 10, tol_rel: float | None = None, tol_abs: float = 0.0,
+               disp: np.ndarray | None = None, max_hist: int = 4096, t_final: float | None = None,
+               max_steps: int | None = None) -> NewtonResult:
+    """solveWithNewtonRaphson (femSolidmechanics2.cpp:730-851) on an existing solver: load steps of
+    prob.dt up to t_final (default prob.t_final, at most max_steps), each iterated until
+    ||R|| < max(tol_abs, tol_rel ||R_first||), with the reference's cuts."""
+    p = prob
+    o = L.NewtonOpts(p.dt, p.t_final if t_final is None else t_final, p.max_steps if max_steps is None else max_steps,
+                     max_newton, p.newton_rtol if tol_rel is None else tol_rel, tol_abs)
+    u = np.zeros(p.n_dof) if disp is None else np.array(disp, np.float64)
+    f = _np(p.fnodal, np.float64)
+    hist = (L.IterStats * max_hist)()
+    n = C.c_int32(0)
+    rc = solver.lib.mphy_newton_run(solver.h, f.ctypes.data_as(L._d), C.byref(o), u.ctypes.data_as(L._d),
+                                    hist, max_hist, C.byref(n))
+    L.check(rc, allow=(L.ERR_TIME_STEP,))
+    rows = np.array([[h.step, h.iter, h.rhs_norm, h.krylov_its, h.status, h.t_assembly_ms, h.t_solve_ms]
+                     for h in hist[:n.value]], dtype=np.float64).reshape(-1, 7)
+    return NewtonResult(disp=u, hist=rows, status=rc)
+
+
 class FemSolidmechanicsGpu:
     """femSolidmechanics on the GPU: setSolver (pattern + solver) and solveWithNewtonRaphson."""
 
@@ -357,19 +378,7 @@ class FemSolidmechanicsGpu:
 
     def solveWithNewtonRaphson(self, max_newton: int = 10, tol_rel: float | None = None, tol_abs: float = 0.0,  # noqa: N802
                                disp: np.ndarray | None = None, max_hist: int = 4096) -> NewtonResult:
-        p = self.prob
-        o = L.NewtonOpts(p.dt, p.t_final, p.max_steps, max_newton, p.newton_rtol if tol_rel is None else tol_rel,
-                         tol_abs)
-        u = np.zeros(p.n_dof) if disp is None else np.array(disp, np.float64)
-        f = _np(p.fnodal, np.float64)
-        hist = (L.IterStats * max_hist)()
-        n = C.c_int32(0)
-        rc = self.ctx.lib.mphy_newton_run(self.solver.h, f.ctypes.data_as(L._d), C.byref(o), u.ctypes.data_as(L._d),
-                                          hist, max_hist, C.byref(n))
-        L.check(rc, allow=(L.ERR_TIME_STEP,))
-        rows = np.array([[h.step, h.iter, h.rhs_norm, h.krylov_its, h.status, h.t_assembly_ms, h.t_solve_ms]
-                         for h in hist[:n.value]], dtype=np.float64).reshape(-1, 7)
-        return NewtonResult(disp=u, hist=rows, status=rc)
+        return newton_run(self.solver, self.prob, max_newton, tol_rel, tol_abs, disp, max_hist)
 
     def solveWithArclength(self, max_newton: int = 10, tol_rel: float = 0.0, tol_abs: float | None = None,  # noqa: N802
                            disp: np.ndarray | None = None, max_hist: int = 4096) -> "ArclengthResult":

@@ -757,6 +757,57 @@ int mphy_solver_assemble_batch(mphy_solver* s, int32_t n, const int32_t* ids, co
     });
 }
 
+int mphy_solver_assemble_batch_host(mphy_solver* s, int32_t n, const int32_t* ids, const double* Ke,
+                                    const double* Re) {
+    return guarded([&] {
+        MPHY_REQUIRE(s && Ke && Re && n >= 0, MPHY_ERR_INVALID_ARG, "invalid argument");
+        MPHY_REQUIRE(ids || n == s->mesh->n_elem, MPHY_ERR_INVALID_ARG, "without ids, n must equal n_elem");
+        if (ids)
+            for (int32_t k = 0; k < n; ++k)
+                MPHY_REQUIRE(ids[k] >= 0 && ids[k] < s->mesh->n_elem, MPHY_ERR_INVALID_ARG, "element id out of range");
+        const int ns = 3 * s->mesh->npe;
+        constexpr int32_t kChunk = 16384;  // elements staged per copy (75 MB of hex8 matrices)
+        const int32_t m0 = n < kChunk ? n : kChunk;
+        DevBuf<double> kd((size_t)m0 * ns * ns), rd((size_t)m0 * ns);
+        DevBuf<int32_t> idd(m0);
+        std::vector<int32_t> iota;
+        cudaStream_t st = s->ctx->stream;
+        for (int32_t off = 0; off < n; off += kChunk) {
+            const int32_t m = n - off < kChunk ? n - off : kChunk;
+            kd.upload(Ke + (size_t)off * ns * ns, (size_t)m * ns * ns, st);
+            rd.upload(Re + (size_t)off * ns, (size_t)m * ns, st);
+            if (ids) {
+                idd.upload(ids + off, m, st);
+            } else {
+                iota.resize(m);
+                for (int32_t k = 0; k < m; ++k) iota[k] = off + k;
+                idd.upload(iota.data(), m, st);
+            }
+            launch_scatter_batch(s->mesh->npe, m, idd.p, s->mesh, s->pat, kd.p, rd.p, s->val.p,
+                                 s->mixed ? s->valf.p : nullptr, s->rhs.p, s->reac.p, st, s->ctx->sm_count);
+            // the staging buffers are reused by the next chunk
+            MPHY_CUDA(cudaStreamSynchronize(st));
+        }
+        if (s->mixed) diag_from_offdiag(s->A, s->valf.p, s->diag64.p, st, s->ctx->sm_count);
+        MPHY_CUDA(cudaStreamSynchronize(st));
+        s->state = MPHY_ASSEMBLY_OK;
+        return (int)MPHY_OK;
+    });
+}
+
+int mphy_solver_add_nodal_forces_host(mphy_solver* s, const double* fext, double scale) {
+    return guarded([&] {
+        MPHY_REQUIRE(s && fext, MPHY_ERR_INVALID_ARG, "null argument");
+        const size_t nd = 3 * (size_t)s->mesh->n_node;
+        if (s->fext_tmp.n != nd) s->fext_tmp.alloc(nd);
+        s->fext_tmp.upload(fext, nd, s->ctx->stream);
+        add_scaled_free(s->mesh->fixed.p, s->fext_tmp.p, scale, s->rhs.p, (int64_t)nd, s->ctx->stream,
+                        s->ctx->sm_count);
+        MPHY_CUDA(cudaStreamSynchronize(s->ctx->stream));
+        return (int)MPHY_OK;
+    });
+}
+
 int mphy_solver_add_nodal_forces(mphy_solver* s, const double* fext, double scale) {
     return guarded([&] {
         MPHY_REQUIRE(s && fext, MPHY_ERR_INVALID_ARG, "null argument");
@@ -883,6 +934,15 @@ int mphy_solver_get_solution(mphy_solver* s, double* dx) {
     return guarded([&] {
         MPHY_REQUIRE(s && dx, MPHY_ERR_INVALID_ARG, "null argument");
         MPHY_CUDA(cudaMemcpyAsync(dx, s->x.p, s->x.bytes(), cudaMemcpyDeviceToDevice, s->ctx->stream));
+        MPHY_CUDA(cudaStreamSynchronize(s->ctx->stream));
+        return (int)MPHY_OK;
+    });
+}
+
+int mphy_solver_get_solution_host(mphy_solver* s, double* dx) {
+    return guarded([&] {
+        MPHY_REQUIRE(s && dx, MPHY_ERR_INVALID_ARG, "null argument");
+        s->x.download(dx, s->x.n, s->ctx->stream);
         MPHY_CUDA(cudaStreamSynchronize(s->ctx->stream));
         return (int)MPHY_OK;
     });

@@ -43,3 +43,24 @@ def shard_by_cost(costs, world: int):
         parts[k].append(i)
         load[k] += costs[i]
     return [sorted(p) for p in parts]
+
+
+def batched_share(problems, rank: int, world: int, ctx, schedule=None, coarse_slabs: int = 0, **solver_opts):
+    """This rank's share of independent instances (LPT by element count) as one batched solver.
+    Ranks exchange nothing on the data path: each solves its own instances; the caller gathers
+    results or times. schedule: (cluster, threads), or None to autotune on the share's
+    tangent at u = 0, lambda = 0.2. Returns (instance ids of this rank, BatchGpu)."""
+    from . import api
+    mine = shard_by_cost([q.n_elem for q in problems], world)[rank]
+    b = api.BatchGpu([problems[i] for i in mine], ctx, **solver_opts)
+    b.set_coarse(coarse_slabs)
+    if schedule is not None:
+        b.set_schedule(*schedule)
+    else:
+        import numpy as np
+        import torch
+        u = b.union
+        b.solver.calcStiffnessAndResidual(torch.zeros(u.n_dof, dtype=torch.float64, device=f"cuda:{ctx.device}"))
+        b.solver.addExternalForces(torch.tensor(np.asarray(u.fnodal), device=f"cuda:{ctx.device}"), 0.2)
+        b.autotune(maxit=0)
+    return mine, b
