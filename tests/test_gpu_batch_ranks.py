@@ -1,7 +1,7 @@
 """The batched form's multi-rank data path on one GPU: two gloo ranks (processes) share cuda:0,
 each solves its LPT share of a 24-instance batch with ranks.batched_share (the path bench.py
 --workload batched runs under torchrun), and the union of their per-instance Newton solutions
-equals one rank solving all 24. The ranks' kernels never wait on each other: every instance is
+equals one rank solving all 24 (to 1e-9). The ranks' kernels never wait on each other: every instance is
 solved by its own rank's persistent launch, and the ranks exchange results on the host only."""
 import multiprocessing as mp
 import socket
@@ -11,7 +11,10 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-SCHEDULE = (2, 256)  # fixed, so that every instance runs the same arithmetic in every batch
+SCHEDULE = (2, 256)  # fixed, so that every instance runs the same solver schedule in every batch
+# The mixed-precision assembly adds FP32 element blocks with atomics, whose order (and so the last
+# bits of the stored operator) changes from run to run: the same instance agrees to about 1e-12.
+TOL = 1e-9
 
 
 def _free_port():
@@ -93,4 +96,4 @@ def test_two_ranks_on_one_gpu_equal_one_rank():
     assert st == ref_st and all(v == 0 for v in st.values())
     for i in range(24):
         scale = max(np.abs(ref_sols[i]).max(), 1e-300)
-        assert np.abs(sols[i] - ref_sols[i]).max() <= 1e-12 * scale, i
+        assert np.abs(sols[i] - ref_sols[i]).max() <= TOL * scale, i
