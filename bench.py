@@ -342,8 +342,14 @@ def _parity_first_step(api, _lib, mesh, pat, args, prob, legs, newton_rtol=1e-8)
         s.close()
         hist = [{"iter": int(h[1]), "rhs_norm": float(h[2]), "krylov_its": int(h[3]),
                  "krylov_status": _lib.status_string(int(h[4]))} for h in r.hist]
-        conv = len(r.hist) > 0 and r.hist[-1, 2] < newton_rtol * r.hist[0, 2]
-        return r.disp, {"method": _method_name(a), "newton": hist, "converged": bool(conv),
+        # a try that does not converge is cut (MyTime::cut: dt halved, the step retried from the
+        # last converged state): every try starts at iteration 1
+        tries = np.flatnonzero(r.hist[:, 1] == 1) if len(r.hist) else np.array([0])
+        cuts = max(0, len(tries) - 1)
+        last = r.hist[tries[-1]:] if len(r.hist) else r.hist
+        conv = cuts == 0 and len(last) > 0 and last[-1, 2] < newton_rtol * last[0, 2]
+        return r.disp, {"method": _method_name(a), "newton": hist, "converged": bool(conv), "cuts": cuts,
+                        "lambda_reached": prob.dt / 2 ** cuts,
                         "newton_status": _lib.status_string(int(r.status)), "wall_s": wall}
 
     u64, ref = run(("fp64", "jacobi", 0))

@@ -74,11 +74,17 @@ void solver_assemble(mphy_solver* s, const double* disp, uint8_t* bad_elem) {
     a.valf = s->mixed ? s->valf.p : nullptr;
     a.rhs = s->rhs.p;
     a.reac = s->reac.p;
+    const bool f32_tangent = s->mixed && !s->mesh->general && s->opts.precision != MPHY_PREC_MIXED_TC;
     if (s->mesh->general) launch_elem_gen(a, s->mesh->npe, 2, s->ctx->stream);
     else if (s->opts.precision == MPHY_PREC_MIXED_TC) launch_elem_tc(a, s->mesh->npe, 2, s->ctx->stream);
-    else launch_elem_fp64(a, s->mesh->npe, 2, s->ctx->stream);
+    else if (f32_tangent) {
+        // FP32 tangent blocks; the element kernel also sums the element diagonal blocks that the
+        // preconditioners read (the operator forms its own diagonal from the stored rows)
+        a.diag_out = s->diag64.p;
+        launch_elem_f32(a, s->mesh->npe, s->ctx->stream);
+    } else launch_elem_fp64(a, s->mesh->npe, 2, s->ctx->stream);
     s->launches += 1;
-    if (s->mixed) {
+    if (s->mixed && !f32_tangent) {
         diag_from_offdiag(s->A, s->valf.p, s->diag64.p, s->ctx->stream, s->ctx->sm_count);
         s->launches += 1;
     }
@@ -965,8 +971,11 @@ int mphy_solver_export(mphy_solver* s, double* val_host, double* rhs_host, doubl
             pattern_csr_columns(s->pat, true);
             DevBuf<double> tmp(s->pat->nnz);
             if (s->mixed) {
+                // the operator's diagonal blocks: minus the sums of the stored rows
+                DevBuf<double> dex(9 * (size_t)s->mesh->n_node);
+                diag_from_offdiag(s->A, s->valf.p, dex.p, st, sm);
                 gather_values<float>(s->valf.p, s->pat->csr_src.p, tmp.p, s->pat->nnz, st, sm);
-                export_fix_diagonal(s->diag64.p, s->pat->csr_rowptr.p, s->pat->csr_col.p, s->pat->assy_for_soln.p,
+                export_fix_diagonal(dex.p, s->pat->csr_rowptr.p, s->pat->csr_col.p, s->pat->assy_for_soln.p,
                                     s->pat->n_free, tmp.p, st, sm);
             } else {
                 gather_values<double>(s->val.p, s->pat->csr_src.p, tmp.p, s->pat->nnz, st, sm);

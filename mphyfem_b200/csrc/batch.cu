@@ -222,6 +222,7 @@ __device__ void coarse_setup(cg::cluster_group& cl, CoarseSmem& cs, const SellVi
             for (int r = 0; r < 3; ++r)
                 for (int j = 0; j < 6; ++j) T[r][j] = 0.0;
         };
+        double S[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // FP32 storage: the row's sum, in storage order
         for (int k = 0; k <= w; ++k) {
             double blk[9];
             int64_t m;
@@ -231,13 +232,14 @@ __device__ void coarse_setup(cg::cluster_group& cl, CoarseSmem& cs, const SellVi
                 bool any = false;
                 for (int q = 0; q < 9; ++q) {
                     blk[q] = (double)p[32 * q];
+                    S[q] += blk[q];
                     any |= blk[q] != 0.0;
                 }
                 if (!any) continue;
             } else {
-                if (!A.diag64) break;  // the FP32 storage keeps the diagonal blocks apart
+                if (!A.diag64) break;  // the FP32 storage's diagonal block: minus the row's sum
                 m = n;
-                for (int q = 0; q < 9; ++q) blk[q] = A.diag64[9 * n + q];
+                for (int q = 0; q < 9; ++q) blk[q] = -S[q];
             }
             if (A.fixed)
                 for (int q = 0; q < 9; ++q)
@@ -310,21 +312,25 @@ __device__ __forceinline__ void row_apply(const SellView& A, const VT* __restric
     const int32_t* cp = A.col + base + lane;
     const VT* vp = val + 9 * base + lane;
     y0 = y1 = y2 = 0.0;
+    RowSum<VT> S;  // FP32 storage: the row's diagonal block, minus the sum of its stored blocks
 #pragma unroll 2
     for (int k = 0; k < w; ++k) {
         const int64_t c = cp[32 * k];
         const double x0 = __ldcg(p + 3 * c), x1 = __ldcg(p + 3 * c + 1), x2 = __ldcg(p + 3 * c + 2);
         const VT* v = vp + 288 * (int64_t)k;
-        y0 += (double)v[0] * x0 + (double)v[32] * x1 + (double)v[64] * x2;
-        y1 += (double)v[96] * x0 + (double)v[128] * x1 + (double)v[160] * x2;
-        y2 += (double)v[192] * x0 + (double)v[224] * x1 + (double)v[256] * x2;
+        double b[9];
+#pragma unroll
+        for (int q = 0; q < 9; ++q) b[q] = (double)v[32 * q];
+        S.add(b);
+        y0 += b[0] * x0 + b[1] * x1 + b[2] * x2;
+        y1 += b[3] * x0 + b[4] * x1 + b[5] * x2;
+        y2 += b[6] * x0 + b[7] * x1 + b[8] * x2;
     }
-    if (A.diag64) {
-        const double* D = A.diag64 + 9 * row;
+    if (S.on(A)) {
         const double x0 = __ldcg(p + 3 * row), x1 = __ldcg(p + 3 * row + 1), x2 = __ldcg(p + 3 * row + 2);
-        y0 += D[0] * x0 + D[1] * x1 + D[2] * x2;
-        y1 += D[3] * x0 + D[4] * x1 + D[5] * x2;
-        y2 += D[6] * x0 + D[7] * x1 + D[8] * x2;
+        y0 += S.d(0) * x0 + S.d(1) * x1 + S.d(2) * x2;
+        y1 += S.d(3) * x0 + S.d(4) * x1 + S.d(5) * x2;
+        y2 += S.d(6) * x0 + S.d(7) * x1 + S.d(8) * x2;
     }
     if (A.fixed) {
         if (A.fixed[3 * row]) y0 = __ldcg(p + 3 * row);

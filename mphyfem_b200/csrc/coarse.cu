@@ -151,6 +151,7 @@ __global__ void __launch_bounds__(kMatThreads, 3) coarse_matrix_kernel(SellView 
                     for (int j = 0; j < 6; ++j) T[r][j] = 0.0;
             };
             int64_t m_next = w > 0 ? (int64_t)cp[0] : n;
+            double S[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // FP32 storage: the row's sum, in storage order
             for (int k = 0; k <= w; ++k) {
                 const int64_t m = m_next;
                 m_next = k + 1 < w ? (int64_t)cp[32 * (k + 1)] : n;  // the diagonal block comes last
@@ -161,13 +162,16 @@ __global__ void __launch_bounds__(kMatThreads, 3) coarse_matrix_kernel(SellView 
 #pragma unroll
                     for (int q = 0; q < 9; ++q) {
                         blk[q] = (double)v[32 * q];
+                        S[q] += blk[q];
                         any |= blk[q] != 0.0;
                     }
                     if (!any) continue;  // SELL padding
                 } else {
-                    if (!A.diag64) break;  // the FP64 storage keeps the diagonal blocks in the rows
+                    // the FP64 storage keeps the diagonal blocks in the rows; the FP32 storage's
+                    // diagonal block is minus the sum of the row's stored blocks
+                    if (!A.diag64) break;
 #pragma unroll
-                    for (int q = 0; q < 9; ++q) blk[q] = A.diag64[9 * n + q];
+                    for (int q = 0; q < 9; ++q) blk[q] = -S[q];
                 }
                 const int b = cv.agg[m];
                 const int dx = b % ngx - ax, dy = (b / ngx) % ngy - ay, dz = b / (ngx * ngy) - az;
@@ -293,6 +297,7 @@ __global__ void __launch_bounds__(256) coarse_matrix_linear_kernel(SellView A, c
                 for (int r = 0; r < 3; ++r)
                     for (int j = 0; j < 12; ++j) T[r][j] = 0.0;
             };
+            double S[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // FP32 storage: the row's sum, in storage order
             for (int k = 0; k <= w; ++k) {
                 double blk[9];
                 int64_t m;
@@ -302,13 +307,14 @@ __global__ void __launch_bounds__(256) coarse_matrix_linear_kernel(SellView A, c
                     bool any = false;
                     for (int q = 0; q < 9; ++q) {
                         blk[q] = (double)v[32 * q];
+                        S[q] += blk[q];
                         any |= blk[q] != 0.0;
                     }
                     if (!any) continue;
                 } else {
-                    if (!A.diag64) break;  // the FP32 storage keeps the diagonal blocks apart
+                    if (!A.diag64) break;  // the FP32 storage's diagonal block: minus the row's sum
                     m = n;
-                    for (int q = 0; q < 9; ++q) blk[q] = A.diag64[9 * n + q];
+                    for (int q = 0; q < 9; ++q) blk[q] = -S[q];
                 }
                 for (int q = 0; q < 9; ++q)
                     if (cv.fixed[3 * m + q % 3]) blk[q] = 0.0;  // prescribed columns: zero Z rows of m

@@ -85,6 +85,7 @@ void upload_shape_tables() {
     MPHY_CUDA(cudaMemcpyToSymbol(c_tet10_w, w4, sizeof(w4)));
     upload_shape_tables_tc(h8, w8, t10, w4);
     upload_shape_tables_gen(h8, w8, t10, w4);
+    upload_shape_tables_f32(h8, w8, t10, w4);
 }
 
 __device__ __forceinline__ double det3(const double A[3][3]) {

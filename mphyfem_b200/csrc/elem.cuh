@@ -26,6 +26,8 @@ struct ElemArgs {
                    // only, without Dirichlet masking (null-space-preserving storage)
     double* rhs;   // [n_node*3], prescribed DOFs untouched
     double* reac;  // [n_node*3] or null
+    double* diag_out = nullptr;  // FP32 storage: [n_node][9] FP64 diagonal blocks accumulated per
+                                 // element (elem_f32.cu), for the preconditioners
 };
 
 void upload_shape_tables();
@@ -34,6 +36,11 @@ void launch_elem_fp64(const ElemArgs& a, int npe, int mode, cudaStream_t s);
 // Mixed-precision element kernel (elem_tc.cu): FP64 residual, tangent contraction on tensor
 // cores (split-BF16, FP32 accumulation), FP32 off-diagonal scatter (a.valf) or Ke export.
 void launch_elem_tc(const ElemArgs& a, int npe, int mode, cudaStream_t s);
+// Mixed-precision element kernel (elem_f32.cu): FP64 kinematics, stress and residual, FP32
+// tangent blocks formed once per symmetric pair, coalesced FP32 scatter into a.valf, element
+// diagonal blocks into a.diag_out. Assembly only (Neo-Hookean, hex8 / tet10).
+void launch_elem_f32(const ElemArgs& a, int npe, cudaStream_t s);
+void upload_shape_tables_f32(const double* h8, const double* w8, const double* t10, const double* w4);
 // Element kernel for any material model of the table a.matx (elem_gen.cu).
 void launch_elem_gen(const ElemArgs& a, int npe, int mode, cudaStream_t s);
 void upload_shape_tables_gen(const double* h8, const double* w8, const double* t10, const double* w4);

@@ -203,6 +203,9 @@ __global__ void __launch_bounds__(kThreads) spmv_kernel(SellView A, const VT* __
         const int64_t base = A.slice_base[s];
         const int w = A.slice_width[s];
         Acc y0 = 0, y1 = 0, y2 = 0;
+        // FP32 storage (off-diagonal blocks only): the row's diagonal block is minus the FP64 sum
+        // of its stored blocks, summed here in storage order while the row streams past
+        RowSum<VT> S;
         const int32_t* cp = A.col + base + lane;
         const VT* vp = val + 9 * base + lane;
 #pragma unroll 2
@@ -210,17 +213,20 @@ __global__ void __launch_bounds__(kThreads) spmv_kernel(SellView A, const VT* __
             const int64_t c = ld_once(cp + 32 * k);
             const Acc x0 = (Acc)x[3 * c], x1 = (Acc)x[3 * c + 1], x2 = (Acc)x[3 * c + 2];
             const VT* v = vp + 288 * (int64_t)k;
-            y0 += (Acc)mval(ld_once(v)) * x0 + (Acc)mval(ld_once(v + 32)) * x1 + (Acc)mval(ld_once(v + 64)) * x2;
-            y1 += (Acc)mval(ld_once(v + 96)) * x0 + (Acc)mval(ld_once(v + 128)) * x1 + (Acc)mval(ld_once(v + 160)) * x2;
-            y2 += (Acc)mval(ld_once(v + 192)) * x0 + (Acc)mval(ld_once(v + 224)) * x1 + (Acc)mval(ld_once(v + 256)) * x2;
+            Acc b[9];
+#pragma unroll
+            for (int q = 0; q < 9; ++q) b[q] = (Acc)mval(ld_once(v + 32 * q));
+            S.add(b);
+            y0 += b[0] * x0 + b[1] * x1 + b[2] * x2;
+            y1 += b[3] * x0 + b[4] * x1 + b[5] * x2;
+            y2 += b[6] * x0 + b[7] * x1 + b[8] * x2;
         }
         if (row < A.n_node) {
-            if (A.diag64) {
-                const double* D = A.diag64 + 9 * row;
+            if (S.on(A)) {
                 const double x0 = (double)x[3 * row], x1 = (double)x[3 * row + 1], x2 = (double)x[3 * row + 2];
-                y0 = (Acc)((double)y0 + ld_once(D) * x0 + ld_once(D + 1) * x1 + ld_once(D + 2) * x2);
-                y1 = (Acc)((double)y1 + ld_once(D + 3) * x0 + ld_once(D + 4) * x1 + ld_once(D + 5) * x2);
-                y2 = (Acc)((double)y2 + ld_once(D + 6) * x0 + ld_once(D + 7) * x1 + ld_once(D + 8) * x2);
+                y0 = (Acc)((double)y0 + S.d(0) * x0 + S.d(1) * x1 + S.d(2) * x2);
+                y1 = (Acc)((double)y1 + S.d(3) * x0 + S.d(4) * x1 + S.d(5) * x2);
+                y2 = (Acc)((double)y2 + S.d(6) * x0 + S.d(7) * x1 + S.d(8) * x2);
             }
             if (A.fixed) {
                 if (A.fixed[3 * row]) y0 = (Acc)x[3 * row];
@@ -335,6 +341,7 @@ __global__ void __launch_bounds__(kThreads) residual_kernel(SellView A, const VT
         const int64_t base = A.slice_base[s];
         const int w = A.slice_width[s];
         double y0 = 0, y1 = 0, y2 = 0;
+        RowSum<VT> S;  // as in spmv_kernel
         const int32_t* cp = A.col + base + lane;
         const VT* vp = val + 9 * base + lane;
 #pragma unroll 2
@@ -342,17 +349,20 @@ __global__ void __launch_bounds__(kThreads) residual_kernel(SellView A, const VT
             const int64_t c = cp[32 * k];
             const double x0 = x[3 * c], x1 = x[3 * c + 1], x2 = x[3 * c + 2];
             const VT* v = vp + 288 * (int64_t)k;
-            y0 += (double)v[0] * x0 + (double)v[32] * x1 + (double)v[64] * x2;
-            y1 += (double)v[96] * x0 + (double)v[128] * x1 + (double)v[160] * x2;
-            y2 += (double)v[192] * x0 + (double)v[224] * x1 + (double)v[256] * x2;
+            double b[9];
+#pragma unroll
+            for (int q = 0; q < 9; ++q) b[q] = (double)v[32 * q];
+            S.add(b);
+            y0 += b[0] * x0 + b[1] * x1 + b[2] * x2;
+            y1 += b[3] * x0 + b[4] * x1 + b[5] * x2;
+            y2 += b[6] * x0 + b[7] * x1 + b[8] * x2;
         }
         if (row < A.n_node) {
-            if (A.diag64) {
-                const double* D = A.diag64 + 9 * row;
+            if (S.on(A)) {
                 const double x0 = x[3 * row], x1 = x[3 * row + 1], x2 = x[3 * row + 2];
-                y0 += D[0] * x0 + D[1] * x1 + D[2] * x2;
-                y1 += D[3] * x0 + D[4] * x1 + D[5] * x2;
-                y2 += D[6] * x0 + D[7] * x1 + D[8] * x2;
+                y0 += S.d(0) * x0 + S.d(1) * x1 + S.d(2) * x2;
+                y1 += S.d(3) * x0 + S.d(4) * x1 + S.d(5) * x2;
+                y2 += S.d(6) * x0 + S.d(7) * x1 + S.d(8) * x2;
             }
             if (A.fixed) {
                 if (A.fixed[3 * row]) y0 = x[3 * row];
@@ -829,6 +839,57 @@ __global__ void dot_kernel(const double* __restrict__ a, const double* __restric
     }
 }
 
+// Minimal-residual step of a refinement sweep: with q = r_old - r_new (= A d), the dot products
+// q.r_old and q.q into out[0], out[1]; deterministic (fixed-order partial sums, last CTA adds).
+__global__ void mr_dots_kernel(int64_t n, const double* __restrict__ rold, const double* __restrict__ rnew,
+                               double* __restrict__ part1, double* __restrict__ part2, uint32_t* counter,
+                               double* out) {
+    __shared__ double sh[32];
+    double a1 = 0.0, a2 = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double ro = rold[i], q = ro - rnew[i];
+        a1 += q * ro;
+        a2 += q * q;
+    }
+    a1 = block_sum(a1, sh);
+    if (threadIdx.x == 0) part1[blockIdx.x] = a1;
+    a2 = block_sum(a2, sh);
+    if (threadIdx.x == 0) part2[blockIdx.x] = a2;
+    if (!arrive_last(counter)) return;
+    const double t1 = reduce_partials(part1, gridDim.x, sh);
+    const double t2 = reduce_partials(part2, gridDim.x, sh);
+    if (threadIdx.x == 0) {
+        *counter = 0;
+        out[0] = t1;
+        out[1] = t2;
+    }
+}
+
+// x += (alpha - 1) d and r = r_old + alpha (r_new - r_old) (the residual of x_old + alpha d) in
+// place of r_new, with ||r||^2 into *out.
+template <typename XT>
+__global__ void mr_combine_kernel(int64_t n, double alpha, double* __restrict__ x, const XT* __restrict__ d,
+                                  const double* __restrict__ rold, double* __restrict__ r,
+                                  double* __restrict__ partials, uint32_t* counter, double* out) {
+    __shared__ double sh[32];
+    double acc = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        x[i] += (alpha - 1.0) * (double)d[i];
+        const double ro = rold[i];
+        const double ri = ro + alpha * (r[i] - ro);
+        r[i] = ri;
+        acc += ri * ri;
+    }
+    acc = block_sum(acc, sh);
+    if (threadIdx.x == 0) partials[blockIdx.x] = acc;
+    if (!arrive_last(counter)) return;
+    const double t = reduce_partials(partials, gridDim.x, sh);
+    if (threadIdx.x == 0) {
+        *counter = 0;
+        *out = t;
+    }
+}
+
 template <typename VT>
 __global__ void prescribed_diag_kernel(SellView A, const uint8_t* __restrict__ fixed, VT* __restrict__ val) {
     for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < A.n_node; n += (int64_t)gridDim.x * blockDim.x) {
@@ -1125,10 +1186,12 @@ void IterativeRefinement<XT>::init(const SellView& A, int sm_count, int chunk) {
     n_ = 3 * (int64_t)A.n_node;
     inner_.init(A, sm_count, chunk);
     r64_.alloc(n_);
+    rold_.alloc(n_);
     rin_.alloc(n_);
     d_.alloc(n_);
     partials_.alloc((size_t)sm_count * 8 + 8);
-    scalars_.alloc(2);
+    partials2_.alloc((size_t)sm_count * 8 + 8);
+    scalars_.alloc(3);
     counter_.alloc(1);
     MPHY_CUDA(cudaMemset(counter_.p, 0, sizeof(uint32_t)));
 }
@@ -1148,6 +1211,7 @@ int IterativeRefinement<XT>::solve(const float* val, const double* b, double* x,
     launches += 1;
     const double bnorm = std::sqrt(bb);
     int total = 0, k = 0, status = MPHY_OK, inner_status = MPHY_OK;
+    bool broke_down = false;
     double rel = bnorm > 0.0 ? 1.0 : 0.0;
     while (rel > rtol && k < max_outer && total < maxit) {
         to_inner(r64_.p, rin_.p, n_, gv, s);
@@ -1161,22 +1225,42 @@ int IterativeRefinement<XT>::solve(const float* val, const double* b, double* x,
         inner_status = st;
         launches += inner_.launches + 1;
         total += it;
-        axpy_kernel<XT><<<gv, kThreads, 0, s>>>(x, d_.p, 1.0, n_);
-        residual_fp64<float>(A_, val, x, b, r64_.p, partials_.p, counter_.p, scalars_.p, s, sm_);
-        launches += 2;
-        double rr = 0.0;
-        MPHY_CUDA(cudaMemcpyAsync(&rr, scalars_.p, sizeof(double), cudaMemcpyDeviceToHost, s));
-        MPHY_CUDA(cudaStreamSynchronize(s));
-        rel = std::sqrt(rr) / bnorm;
         ++k;
-        if (st == MPHY_ERR_INDEFINITE || st == MPHY_ERR_DIVERGED) {
+        if (st == MPHY_ERR_DIVERGED) {  // NaN in the inner solve: the correction is unusable
             status = st;
             break;
         }
+        // x += d, then the FP64 residual r_new = b - A x; with q = A d = r_old - r_new the sweep
+        // keeps the multiple alpha = (q.r_old)/(q.q) of d that minimises ||b - A (x_old + alpha d)||
+        // (alpha = 1 for an accurate correction). A correction cut short by a CG breakdown on the
+        // FP32 operator (p.Ap <= 0: the stored operator can be indefinite along directions of
+        // near-zero stiffness) then cannot raise the residual, and the next sweep restarts CG.
+        MPHY_CUDA(cudaMemcpyAsync(rold_.p, r64_.p, n_ * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        axpy_kernel<XT><<<gv, kThreads, 0, s>>>(x, d_.p, 1.0, n_);
+        residual_fp64<float>(A_, val, x, b, r64_.p, partials_.p, counter_.p, scalars_.p, s, sm_);
+        mr_dots_kernel<<<gv, kThreads, 0, s>>>(n_, rold_.p, r64_.p, partials_.p, partials2_.p, counter_.p,
+                                               scalars_.p + 1);
+        launches += 3;
+        double h3[3] = {0.0, 0.0, 0.0};  // ||r_new||^2, q.r_old, q.q
+        MPHY_CUDA(cudaMemcpyAsync(h3, scalars_.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, s));
+        MPHY_CUDA(cudaStreamSynchronize(s));
+        double rr = h3[0];
+        const double alpha = h3[2] > 0.0 ? h3[1] / h3[2] : 1.0;
+        if (alpha == alpha && std::fabs(alpha - 1.0) > 1e-12) {
+            mr_combine_kernel<XT><<<gv, kThreads, 0, s>>>(n_, alpha, x, d_.p, rold_.p, r64_.p, partials_.p,
+                                                          counter_.p, scalars_.p);
+            launches += 1;
+            MPHY_CUDA(cudaMemcpyAsync(&rr, scalars_.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+            MPHY_CUDA(cudaStreamSynchronize(s));
+        }
+        rel = std::sqrt(rr) / bnorm;
+        if (st == MPHY_ERR_INDEFINITE) broke_down = true;
     }
     // one sweep: the inner solve's KSP status decides (its stopping rule is PETSc's); more sweeps:
-    // the FP64 true residual does
-    if (status == MPHY_OK) status = max_outer <= 1 ? inner_status : (rel > rtol ? MPHY_ERR_NOT_CONVERGED : MPHY_OK);
+    // the FP64 true residual does (an unconverged solve that met a breakdown reports it)
+    if (status == MPHY_OK)
+        status = max_outer <= 1 ? inner_status
+                                : (rel > rtol ? (broke_down ? MPHY_ERR_INDEFINITE : MPHY_ERR_NOT_CONVERGED) : MPHY_OK);
     if (its) *its = total;
     if (sweeps) *sweeps = k;
     if (relres) *relres = rel;

@@ -1,6 +1,7 @@
 // krylov.cuh -- K4/K5: SELL-32 3x3 SpMV, preconditioned CG with PETSc KSPCG semantics (FP64, or
 // FP32 vectors with FP64 reductions), FP64 iterative refinement, and the vector operations.
 #pragma once
+#include <type_traits>
 #include <cuda_bf16.h>
 
 #include "common.cuh"
@@ -132,7 +133,7 @@ class IterativeRefinement {
     int sm_ = 148;
     int64_t n_ = 0;
     Pcg<float, XT> inner_;
-    DevBuf<double> r64_, partials_, scalars_;
+    DevBuf<double> r64_, rold_, partials_, partials2_, scalars_;
     DevBuf<XT> rin_, d_;
     DevBuf<uint32_t> counter_;
 };
@@ -157,5 +158,34 @@ void axpy_inplace(double* y, const double* x, double a, int64_t n, cudaStream_t 
 template <typename VT>
 void gather_values(const VT* val, const int64_t* src, double* out, int64_t n, cudaStream_t s, int sm);
 void gather_free(const double* v, const int32_t* assy, double* out, int64_t n_free, cudaStream_t s, int sm);
+
+// The FP32 storage keeps no diagonal blocks: the operator's diagonal block of a row is minus the
+// FP64 sum of the row's stored FP32 blocks, in storage order (k = 0 .. width-1), which makes the
+// stored operator map rigid translations exactly to zero. Every kernel that applies the operator
+// forms that sum while it streams the row (RowSum), with each value widened once. The FP64
+// storage has its diagonal blocks in the rows (RowSum<double> does nothing).
+template <typename VT>
+constexpr bool kOffDiagStorage = std::is_same<VT, float>::value;
+
+template <typename VT>
+struct RowSum {
+    template <typename T>
+    __device__ __forceinline__ void add(const T*) {}
+    template <typename V>
+    __device__ __forceinline__ bool on(const V&) const { return false; }
+    __device__ __forceinline__ double d(int) const { return 0.0; }
+};
+template <>
+struct RowSum<float> {
+    double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    template <typename T>
+    __device__ __forceinline__ void add(const T* b) {
+#pragma unroll
+        for (int q = 0; q < 9; ++q) acc[q] += (double)b[q];
+    }
+    template <typename V>
+    __device__ __forceinline__ bool on(const V& A) const { return A.diag64 != nullptr; }
+    __device__ __forceinline__ double d(int q) const { return -acc[q]; }
+};
 
 }  // namespace mphy

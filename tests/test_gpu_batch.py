@@ -3,7 +3,9 @@ union; each instance must get what it gets when solved alone (same Jacobi-PCG, s
 rules), for every schedule the autotuner may pick.
 
 Tolerances: linear solves to rtol 1e-10 (true-residual norm), solutions within 1e-7 of the
-single-instance GPU solve and iteration counts within 2 (reduction order differs); Newton runs
+single-instance GPU solve (1e-5 with the FP32 operator, which is assembled with FP32 atomic adds
+and so differs in its last bits between two assemblies) and iteration counts within 2 (reduction
+order differs); Newton runs
 (to 1e-8) against the FP64 oracle within 1e-8 relative displacement, same Newton solves and cuts."""
 import numpy as np
 import pytest
@@ -68,8 +70,13 @@ def test_batch_solve_matches_single_instances(env, precision):
         x = b.solver.solution().cpu().numpy()
         for i in range(len(probs)):
             xi = x[b.instance_slice(i)]
-            assert abs(int(its[i]) - ref_its[i]) <= 2, (cl, th, i, its[i], ref_its[i])
-            assert np.linalg.norm(xi - ref_x[i]) <= 1e-7 * np.linalg.norm(ref_x[i]), (cl, th, i)
+            its_tol = 2 if precision == 0 else max(2, 0.06 * ref_its[i])  # FP32 operators differ in last bits
+            assert abs(int(its[i]) - ref_its[i]) <= its_tol, (cl, th, i, its[i], ref_its[i])
+            # FP32 storage: the union and the instance are assembled separately and FP32 atomic
+            # adds round in arrival order, so the two stored operators differ in their last bits
+            # and the solutions by about cond(A) * 1e-7
+            tol = 1e-7 if precision == 0 else 1e-5
+            assert np.linalg.norm(xi - ref_x[i]) <= tol * np.linalg.norm(ref_x[i]), (cl, th, i)
 
 
 def _oracle_refs(probs):

@@ -72,7 +72,10 @@ def test_fsai_pcg_matches_oracle_with_fewer_iterations(env, oracle, prec):
     xo, _, _, _ = op.cg(val, 0.2 * p.fnodal[free], rtol=1e-13)
     tol = 1e-9 if prec == "PREC_FP64" else 1e-2  # FP32-stored operator: cond(A) * 6e-8
     assert np.linalg.norm(xs["PC_FSAI"][free] - xo) <= tol * np.linalg.norm(xo)
-    assert np.linalg.norm(xs["PC_FSAI"] - xs["PC_JACOBI"]) <= 1e-8 * np.linalg.norm(xs["PC_JACOBI"])
+    # two assemblies of the FP32 operator differ in their last bits (FP32 atomic adds round in
+    # arrival order): the two solutions then differ by about cond(A) * 1e-7
+    tol2 = 1e-8 if prec == "PREC_FP64" else 1e-5
+    assert np.linalg.norm(xs["PC_FSAI"] - xs["PC_JACOBI"]) <= tol2 * np.linalg.norm(xs["PC_JACOBI"])
     # on the cantilever the slowest modes are global bending modes that no local preconditioner
     # reaches: FSAI saves only a few percent of the iterations here (it wins on high contrast)
     assert its["PC_FSAI"] < its["PC_JACOBI"], its

@@ -110,3 +110,32 @@ def test_mixed_newton_reaches_fp64_solution(env):
         assert r[-1] < 1e-10 * r[0]
     u_ref = g["newton_consistent_u"]
     assert np.abs(res.disp - u_ref).max() <= 1e-6 * np.abs(u_ref).max()
+
+
+@pytest.mark.parametrize("case", ["hex8_two_phase", "tet10_kuhn"])
+@pytest.mark.parametrize("tangent", [0, 1], ids=["reference", "consistent"])
+def test_fp32_tangent_kernel_matches_oracle(env, oracle, case, tangent):
+    """The mixed-precision element kernel (FP64 kinematics, stress and residual; FP32 tangent
+    blocks, each symmetric pair formed once) against the FP64 oracle: off-diagonal entries within
+    1e-5 of the largest entry (FP32 arithmetic and storage), the operator's diagonal blocks (minus
+    the stored rows' sums) likewise, residual and reactions within 1e-12 (FP64)."""
+    from tests.golden.make_golden import probe_displacement
+    torch, api, _lib, ctx = env
+    if case == "hex8_two_phase":
+        p = meshgen.two_phase_inclusions(16, 4, 4, seed=3, r_range=(0.15, 0.3))
+    else:
+        p = meshgen.tet10_kuhn(6, 3, 3)
+    u = probe_displacement(p, amp=0.005)
+    mesh = api.Mesh(ctx, p)
+    sol = api.SolverGpu(mesh, api.Pattern(mesh), precision=_lib.PREC_MIXED, tangent=tangent)
+    sol.calcStiffnessAndResidual(torch.tensor(u, device="cuda"))
+    val, rhs, reac = sol.export()
+    oracle.set_consistent_tangent(bool(tangent))
+    try:
+        oval, orhs, oreac, bad = oracle.OracleProblem(p).assemble(u)
+    finally:
+        oracle.set_consistent_tangent(False)
+    assert bad == -1
+    assert np.abs(val - oval).max() <= 1e-5 * np.abs(oval).max()
+    assert np.abs(rhs - orhs).max() <= 1e-12 * np.abs(orhs).max()
+    assert np.abs(reac - oreac).max() <= 1e-12 * np.abs(oreac).max()

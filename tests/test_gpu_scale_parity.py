@@ -61,6 +61,7 @@ def test_headline_method_matches_fp64_at_mid_size(env, case):
     rmx = _first_step(api, _lib, ctx, p, newton_rtol, precision=_lib.PREC_MIXED, coarse_aggregates=coarse, **common)
     for r in (r64, rmx):
         assert r.status == 0
+        assert np.count_nonzero(r.hist[:, 1] == 1) == 1, r.hist[:, :5]  # converged without a cut
         assert r.hist[-1, 2] < newton_rtol * r.hist[0, 2], r.hist[:, :4]
     assert r64.hist[0, 2] == pytest.approx(rmx.hist[0, 2], rel=1e-12)  # the same load, the same R_0
     scale = np.abs(r64.disp).max()
