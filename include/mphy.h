@@ -320,6 +320,21 @@ int mphy_solver_get_solution(mphy_solver* s, double* dx_dev);
 int mphy_solver_get_solution_host(mphy_solver* s, double* dx_host);
 /* disp_dev += solution (the update `SolnData.disp += SolnData.dispIncr`). */
 int mphy_solver_update_disp(mphy_solver* s, double* disp_dev);
+/* ---- constant-pressure mixed element: Elem_Solid_3D_Mixed0 (Elem_Solid_3D_Mixed0.cpp), hex8 or
+ * tet10 displacement with one pressure per element, condensed in every element
+ * (calcStiffnessAndResidual, :93-101), the element pressures updated after every solve
+ * (solveForPressure, :112-200, called by factoriseSolveAndUpdate, femSolidmechanics2.cpp:1204-1212)
+ * and, in mphy_newton_run, saved with each converged step and restored by a cut. The materials
+ * take their mixed branch (the pressure replaces U'(J)); Utype -1 is refused (Kpp = 0).
+ * enable = 1 turns it on for every later assembly with zero pressures and zero last-step
+ * displacement; 0 turns it off. Not available with arc-length. */
+int mphy_solver_set_mixed_p0(mphy_solver* s, int32_t enable);
+/* Element pressures [n_elem], host: set_host (may be NULL) is copied in first, then get_host (may
+ * be NULL) receives them. */
+int mphy_solver_p0_pressure(mphy_solver* s, const double* set_host, double* get_host);
+/* SolutionDataSolid::saveSolution for callers that drive mphy_newton_iteration themselves: disp_dev
+ * becomes the last converged step (its J is the mixed element's Jn), with the element pressures. */
+int mphy_solver_save_step(mphy_solver* s, const double* disp_dev);
 /* Copies for checks: CSR values in mphy_pattern_export_csr order [nnz], rhs over free DOFs
  * [n_free], reactions [3*n_node]. Any pointer may be NULL. FP64 regardless of precision. */
 int mphy_solver_export(mphy_solver* s, double* val_host, double* rhs_host, double* reac_host);

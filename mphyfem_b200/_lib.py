@@ -139,6 +139,9 @@ SIGNATURES = {
     "mphy_solver_get_solution_host": (C.c_int, [_vp, _d]),
     "mphy_solver_update_disp": (C.c_int, [_vp, _vp]),
     "mphy_solver_export": (C.c_int, [_vp, _d, _d, _d]),
+    "mphy_solver_set_mixed_p0": (C.c_int, [_vp, C.c_int32]),
+    "mphy_solver_p0_pressure": (C.c_int, [_vp, _d, _d]),
+    "mphy_solver_save_step": (C.c_int, [_vp, _vp]),
     "mphy_newton_iteration": (C.c_int, [_vp, _vp, _vp, C.c_double, C.c_double, C.POINTER(IterStats)]),
     "mphy_newton_iteration_host": (C.c_int, [_vp, _d, _d, C.c_double, C.c_double, C.POINTER(IterStats)]),
     "mphy_newton_run": (C.c_int, [_vp, _d, C.POINTER(NewtonOpts), _d, C.POINTER(IterStats), C.c_int32, _i32]),

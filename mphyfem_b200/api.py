@@ -256,6 +256,22 @@ class SolverGpu:
         L.check(self.lib.mphy_solver_export(self.h, p(val), p(rhs), p(reac)))
         return val, rhs, reac
 
+    def set_mixed_p0(self, enable: bool = True):
+        """Elem_Solid_3D_Mixed0: one condensed pressure per element (zero to start)."""
+        L.check(self.lib.mphy_solver_set_mixed_p0(self.h, int(enable)))
+
+    def p0_pressure(self, set_to=None) -> np.ndarray:
+        """Element pressures of the constant-pressure element; set_to [n_elem] replaces them first."""
+        out = np.zeros(self.mesh.prob.n_elem)
+        src = None if set_to is None else _np(set_to, np.float64)
+        L.check(self.lib.mphy_solver_p0_pressure(self.h, None if src is None else src.ctypes.data_as(L._d),
+                                                 out.ctypes.data_as(L._d)))
+        return out
+
+    def save_step(self, disp_dev):
+        """The converged state of a load step (disp and the element pressures)."""
+        L.check(self.lib.mphy_solver_save_step(self.h, _ptr(disp_dev)))
+
     def newton_iteration(self, disp_dev, fext_dev, lam: float, tol_abs: float = 0.0) -> L.IterStats:
         st = L.IterStats()
         L.check(self.lib.mphy_newton_iteration(self.h, _ptr(disp_dev), _ptr(fext_dev) if fext_dev is not None else None,
@@ -353,7 +369,7 @@ def newton_run(solver: "SolverGpu", prob, max_newton: int = 10, tol_rel: float |
 class FemSolidmechanicsGpu:
     """femSolidmechanics on the GPU: setSolver (pattern + solver) and solveWithNewtonRaphson."""
 
-    def __init__(self, prob, ctx: Context | None = None, **solver_opts):
+    def __init__(self, prob, ctx: Context | None = None, mixed_p0: bool = False, **solver_opts):
         self.prob = prob
         self.ctx = ctx or Context(0)
         self.mesh = Mesh(self.ctx, prob)
@@ -361,6 +377,8 @@ class FemSolidmechanicsGpu:
         opts = dict(rtol=prob.cg_rtol)
         opts.update(solver_opts)
         self.solver = SolverGpu(self.mesh, self.pattern, **opts)
+        if mixed_p0 or prob.meta.get("element") == "ELEM_SOLID_3D_MIXED0":
+            self.solver.set_mixed_p0(True)
 
     @classmethod
     def from_reference_inputs(cls, config_path, ctx: Context | None = None, **solver_opts):

@@ -20,6 +20,7 @@
 #include "krylov.cuh"
 #include "pattern.cuh"
 #include "solver.cuh"
+#include "mixed.cuh"
 
 namespace mphy {
 
@@ -74,8 +75,17 @@ void solver_assemble(mphy_solver* s, const double* disp, uint8_t* bad_elem) {
     a.valf = s->mixed ? s->valf.p : nullptr;
     a.rhs = s->rhs.p;
     a.reac = s->reac.p;
-    const bool f32_tangent = s->mixed && !s->mesh->general && s->opts.precision != MPHY_PREC_MIXED_TC;
-    if (s->mesh->general) launch_elem_gen(a, s->mesh->npe, 2, s->ctx->stream);
+    const bool f32_tangent = s->mixed && !s->p0 && !s->mesh->general && s->opts.precision != MPHY_PREC_MIXED_TC;
+    if (s->p0) {
+        MixedElemArgs ma{};
+        ma.base = a;
+        ma.disp_prev = s->disp_prev.p;
+        ma.pe = s->pe.p;
+        ma.kup_e = s->kup_e.p;
+        ma.kpp_e = s->kpp_e.p;
+        ma.fp_e = s->fp_e.p;
+        launch_elem_mixed0(ma, s->mesh->npe, 2, s->ctx->stream);
+    } else if (s->mesh->general) launch_elem_gen(a, s->mesh->npe, 2, s->ctx->stream);
     else if (s->opts.precision == MPHY_PREC_MIXED_TC) launch_elem_tc(a, s->mesh->npe, 2, s->ctx->stream);
     else if (f32_tangent) {
         // FP32 tangent blocks; the element kernel also sums the element diagonal blocks that the
@@ -89,6 +99,17 @@ void solver_assemble(mphy_solver* s, const double* disp, uint8_t* bad_elem) {
         s->launches += 1;
     }
     s->state = MPHY_ASSEMBLY_OK;
+}
+
+void solver_update(mphy_solver* s, double* disp) {
+    mphy_ctx* c = s->ctx;
+    axpy_inplace(disp, s->x.p, 1.0, 3 * (int64_t)s->mesh->n_node, c->stream, c->sm_count);
+    s->launches += 1;
+    if (s->p0) {
+        launch_pressure_update_p0(s->mesh->n_elem, s->mesh->npe, s->mesh->conn.p, s->x.p, s->kup_e.p, s->kpp_e.p,
+                                  s->fp_e.p, s->pe.p, c->stream, c->sm_count);
+        s->launches += 1;
+    }
 }
 
 // ||rhs|| and the first bad element, one synchronisation
@@ -294,8 +315,7 @@ int newton_iteration(mphy_solver* s, double* disp, const double* fext, double la
         int32_t its = 0;
         double fn = 0.0;
         st.status = solver_solve(s, &its, &fn);
-        axpy_inplace(disp, s->x.p, 1.0, 3 * (int64_t)s->mesh->n_node, c->stream, c->sm_count);
-        s->launches += 1;
+        solver_update(s, disp);
         MPHY_CUDA(cudaEventRecord(c->ev1, c->stream));
         MPHY_CUDA(cudaEventSynchronize(c->ev1));
         st.t_solve_ms = elapsed_ms(c);
@@ -957,7 +977,60 @@ int mphy_solver_get_solution_host(mphy_solver* s, double* dx) {
 int mphy_solver_update_disp(mphy_solver* s, double* disp) {
     return guarded([&] {
         MPHY_REQUIRE(s && disp, MPHY_ERR_INVALID_ARG, "null argument");
-        axpy_inplace(disp, s->x.p, 1.0, 3 * (int64_t)s->mesh->n_node, s->ctx->stream, s->ctx->sm_count);
+        solver_update(s, disp);
+        return (int)MPHY_OK;
+    });
+}
+
+int mphy_solver_set_mixed_p0(mphy_solver* s, int32_t enable) {
+    return guarded([&] {
+        MPHY_REQUIRE(s, MPHY_ERR_INVALID_ARG, "null solver");
+        if (!enable) {
+            s->p0 = false;
+            return (int)MPHY_OK;
+        }
+        const mphy_mesh* m = s->mesh;
+        for (int32_t k = 0; k < m->n_mat; ++k)
+            MPHY_REQUIRE((int)m->matx_host[kMatRow * (size_t)k + 6] != -1, MPHY_ERR_UNSUPPORTED,
+                         "constant-pressure element: Utype -1 (incompressible) has Kpp = 0");
+        MPHY_CUDA(cudaSetDevice(s->device));
+        cudaStream_t st = s->ctx->stream;
+        const size_t nd = 3 * (size_t)m->n_node, ne = (size_t)m->n_elem;
+        s->pe.alloc(ne);
+        s->pe_prev.alloc(ne);
+        s->kup_e.alloc(ne * 3 * (size_t)m->npe);
+        s->kpp_e.alloc(ne);
+        s->fp_e.alloc(ne);
+        if (s->disp_prev.n != nd) s->disp_prev.alloc(nd);
+        for (DevBuf<double>* b : {&s->pe, &s->pe_prev, &s->disp_prev})
+            MPHY_CUDA(cudaMemsetAsync(b->p, 0, b->bytes(), st));
+        MPHY_CUDA(cudaStreamSynchronize(st));
+        s->p0 = true;
+        s->state = std::min(s->state, (int)MPHY_INIT_OK);
+        return (int)MPHY_OK;
+    });
+}
+
+int mphy_solver_p0_pressure(mphy_solver* s, const double* set_host, double* get_host) {
+    return guarded([&] {
+        MPHY_REQUIRE(s && s->p0, MPHY_ERR_STATE, "the constant-pressure element is not enabled");
+        cudaStream_t st = s->ctx->stream;
+        if (set_host) s->pe.upload(set_host, s->pe.n, st);
+        if (get_host) s->pe.download(get_host, s->pe.n, st);
+        MPHY_CUDA(cudaStreamSynchronize(st));
+        return (int)MPHY_OK;
+    });
+}
+
+int mphy_solver_save_step(mphy_solver* s, const double* disp) {
+    return guarded([&] {
+        MPHY_REQUIRE(s && disp, MPHY_ERR_INVALID_ARG, "null argument");
+        const size_t nd = 3 * (size_t)s->mesh->n_node;
+        cudaStream_t st = s->ctx->stream;
+        if (s->disp_prev.n != nd) s->disp_prev.alloc(nd);
+        MPHY_CUDA(cudaMemcpyAsync(s->disp_prev.p, disp, nd * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        if (s->p0) s->pe_prev.copy_from(s->pe, st);
+        MPHY_CUDA(cudaStreamSynchronize(st));
         return (int)MPHY_OK;
     });
 }
@@ -1043,6 +1116,7 @@ int mphy_newton_run(mphy_solver* s, const double* fext_host, const mphy_newton_o
             t += dt;
             const double lambda = t;
             MPHY_CUDA(cudaMemcpyAsync(s->disp_prev.p, disp, nd * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            if (s->p0) s->pe_prev.copy_from(s->pe, st);
             bool converged = false;
             double norm = -1.0, norm_prev = -1.0, tol = o->tol_abs;
             for (int iter = 1; iter <= o->max_newton; ++iter) {
@@ -1068,7 +1142,7 @@ int mphy_newton_run(mphy_solver* s, const double* fext_host, const mphy_newton_o
                     int32_t its = 0;
                     double fn = 0.0;
                     is.status = solver_solve(s, &its, &fn);  // KSP divergence is only reported
-                    axpy_inplace(disp, s->x.p, 1.0, (int64_t)nd, st, s->ctx->sm_count);
+                    solver_update(s, disp);
                     MPHY_CUDA(cudaEventRecord(s->ctx->ev1, st));
                     MPHY_CUDA(cudaEventSynchronize(s->ctx->ev1));
                     is.t_solve_ms = elapsed_ms(s->ctx);
@@ -1092,6 +1166,7 @@ int mphy_newton_run(mphy_solver* s, const double* fext_host, const mphy_newton_o
                     break;
                 }
                 MPHY_CUDA(cudaMemcpyAsync(disp, s->disp_prev.p, nd * sizeof(double), cudaMemcpyDeviceToDevice, st));
+                if (s->p0) s->pe.copy_from(s->pe_prev, st);
             }
         }
         s->disp_tmp.download(disp_host, nd, st);
@@ -1109,6 +1184,7 @@ int mphy_arclength_run(mphy_solver* s, const double* fext_host, const mphy_newto
         MPHY_REQUIRE(s && fext_host && o && disp_host, MPHY_ERR_INVALID_ARG, "null argument");
         MPHY_REQUIRE(o->dt > 0.0 && o->max_newton >= 2, MPHY_ERR_INVALID_ARG,
                      "arc-length needs dt > 0 and max_newton >= 2 (iterations 1..max_newton-1)");
+        MPHY_REQUIRE(!s->p0, MPHY_ERR_UNSUPPORTED, "arc-length with the constant-pressure element");
         const size_t nd = 3 * (size_t)s->mesh->n_node;
         const int64_t n = (int64_t)nd;
         cudaStream_t st = s->ctx->stream;

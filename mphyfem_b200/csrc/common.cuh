@@ -69,6 +69,9 @@ struct DevBuf {
     void download(T* host, size_t count, cudaStream_t s) const {
         if (count) MPHY_CUDA(cudaMemcpyAsync(host, p, count * sizeof(T), cudaMemcpyDeviceToHost, s));
     }
+    void copy_from(const DevBuf& o, cudaStream_t s) {
+        if (n) MPHY_CUDA(cudaMemcpyAsync(p, o.p, (n < o.n ? n : o.n) * sizeof(T), cudaMemcpyDeviceToDevice, s));
+    }
 };
 
 inline unsigned ceil_div(size_t a, size_t b) { return (unsigned)((a + b - 1) / b); }

@@ -476,6 +476,248 @@ void launch_mixed(const MixedElemArgs& a, cudaStream_t s) {
     MPHY_CUDA(cudaGetLastError());
 }
 
+// ---------------------------------------------------------------- constant-pressure u-p element
+// Elem_Solid_3D_Mixed0: ElementBase::calcStiffnessAndResidualMixed3D with one pressure function
+// (nlbfP = 1, Np = 1, p = the element's pressure; ElementBase2.cpp:385-389) on the hex8 or tet10
+// displacement element, then the condensation of Elem_Solid_3D_Mixed0::calcStiffnessAndResidual
+// (Elem_Solid_3D_Mixed0.cpp:93-101):
+//   K = Kuu - Kup Kpu / Kpp,   F = FU - Kup FP / Kpp,
+// with Kup(3I+a) = sum dvol h_aI = Kpu(3I+a), Kpp = -sum dvol0 thetahat and
+// FP = -sum dvol0 (J - Jhat - thetahat p). Kup, Kpp and FP are kept per element for the pressure
+// update after the solve (Elem_Solid_3D_Mixed0::solveForPressure, :112-200).
+template <int NPE>
+struct P0Smem {
+    static constexpr int NGP = GenTraits<NPE>::NGP;
+    double x0[NPE][3];
+    double u[NPE][3];
+    double up[NPE][3];
+    double h[NGP][NPE][3];
+    double C[NGP][81];   // dvol * C
+    double sig[NGP][9];  // dvol * sigma
+    double dvol[NGP], dvol0[NGP], th[NGP], resip[NGP];
+    double kup[NPE][3];
+    double kpp, fp;
+    double pad[2];
+};
+
+template <int NPE, int MODE>
+__global__ void __launch_bounds__(kGenEpb * NPE * ((NPE + kGenCh - 1) / kGenCh)) elem_mixed0_kernel(MixedElemArgs ma) {
+    const ElemArgs& a = ma.base;
+    using T = GenTraits<NPE>;
+    constexpr int NGP = T::NGP, NCH = (NPE + kGenCh - 1) / kGenCh, TPE = NPE * NCH, NS = 3 * NPE;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    auto* S = reinterpret_cast<P0Smem<NPE>*>(smem_raw);
+    const int el = threadIdx.x / TPE, loc = threadIdx.x % TPE;
+    const int I = loc % NPE, ch = loc / NPE;
+    const int64_t e = (int64_t)blockIdx.x * kGenEpb + el;
+    const bool live = e < a.n_elem;
+    P0Smem<NPE>& s = S[el];
+
+    int32_t node = 0;
+    if (live) {
+        node = a.conn[e * NPE + I];
+        if (ch == 0) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                s.x0[I][d] = a.coords[3 * (int64_t)node + d];
+                s.u[I][d] = a.disp[3 * (int64_t)node + d];
+                s.up[I][d] = ma.disp_prev[3 * (int64_t)node + d];
+            }
+        }
+    }
+    __syncthreads();
+
+    if (live && loc < NGP) {
+        const int gp = loc;
+        const double* dN = T::dN(gp);
+        double G[3][3] = {{0}}, Gc[3][3] = {{0}};
+#pragma unroll
+        for (int n = 0; n < NPE; ++n)
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                const double d = dN[r * NPE + n];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    G[r][c] += s.x0[n][c] * d;
+                    Gc[r][c] += (s.x0[n][c] + s.u[n][c]) * d;
+                }
+            }
+        double Gi[3][3], Gci[3][3];
+        const double jac0 = det3g(G);
+        inv3g(G, jac0, Gi);
+        const double jac = det3g(Gc);
+        inv3g(Gc, jac, Gci);
+        const double dvol = T::w(gp) * jac, dvol0 = T::w(gp) * jac0;
+        double F[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}}, Fn[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+#pragma unroll
+        for (int n = 0; n < NPE; ++n) {
+            double g0[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+                g0[c] = dN[n] * Gi[c][0] + dN[NPE + n] * Gi[c][1] + dN[2 * NPE + n] * Gi[c][2];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int m = 0; m < 3; ++m) {
+                    F[i][m] += s.u[n][i] * g0[m];
+                    Fn[i][m] += s.up[n][i] * g0[m];
+                }
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+                s.h[gp][n][c] = dN[n] * Gci[c][0] + dN[NPE + n] * Gci[c][1] + dN[2 * NPE + n] * Gci[c][2];
+        }
+        const double J = det3g(F);
+        if (J < 0.0) {
+            atomicMin(a.bad, (unsigned long long)e);
+            if (a.bad_elem) a.bad_elem[e] = 1;
+        }
+        double row[kMatRow];
+#pragma unroll
+        for (int q = 0; q < kMatRow; ++q) row[q] = a.matx[kMatRow * (int64_t)a.mat_id[e] + q];
+        // compute_constants_volumetric_functions (utilitiesmaterialHyperelastic.cpp:144-173)
+        double Jhat = 1.0, th = 0.0;
+        const int utype = (int)row[6];
+        if (utype != -1) {
+            double d1, d2;
+            const double Jn = det3g(Fn);
+            vol_derivs(utype, 1.0 / row[5], Jn, d1, d2);
+            Jhat = Jn - d1 / d2;
+            th = 1.0 / d2;
+        }
+        const double pres = ma.pe[e];
+        double b[3][3], b2[3][3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) b[i][j] = F[i][0] * F[j][0] + F[i][1] * F[j][1] + F[i][2] * F[j][2];
+        square3(b, b2);
+        const MatScalars m = material_scalars(row, a.tangent, b, b2, J, true, pres);
+        material_fill(m, b, b2, dvol, s.sig[gp], s.C[gp]);
+        s.dvol[gp] = dvol;
+        s.dvol0[gp] = dvol0;
+        s.th[gp] = th;
+        s.resip[gp] = J - Jhat - th * pres;
+    }
+    __syncthreads();
+    // the coupling column, Kpp and FP of the element (fixed Gauss-point order)
+    if (live && ch == 0) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            double k = 0.0;
+#pragma unroll
+            for (int gp = 0; gp < NGP; ++gp) k += s.dvol[gp] * s.h[gp][I][c];
+            s.kup[I][c] = k;
+        }
+        if (I == 0) {
+            double kpp = 0.0, fp = 0.0;
+#pragma unroll
+            for (int gp = 0; gp < NGP; ++gp) {
+                kpp -= s.dvol0[gp] * s.th[gp];
+                fp -= s.dvol0[gp] * s.resip[gp];
+            }
+            s.kpp = kpp;
+            s.fp = fp;
+        }
+    }
+    __syncthreads();
+    if (!live) return;
+
+    bool freeI[3] = {true, true, true};
+    if (MODE & 2) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) freeI[c] = a.fixed[3 * (int64_t)node + c] == 0;
+    }
+    const double rkpp = 1.0 / s.kpp;
+    if (ch == 0) {
+        double R[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            double r = 0.0;
+#pragma unroll
+            for (int gp = 0; gp < NGP; ++gp)
+                r -= s.h[gp][I][0] * s.sig[gp][c] + s.h[gp][I][1] * s.sig[gp][3 + c] + s.h[gp][I][2] * s.sig[gp][6 + c];
+            R[c] = r - s.kup[I][c] * (s.fp * rkpp);
+            if (ma.kup_e) ma.kup_e[e * NS + 3 * I + c] = s.kup[I][c];
+        }
+        store_residual<NPE, MODE>(a, e, I, node, freeI, R);
+        if (I == 0) {
+            if (ma.kpp_e) ma.kpp_e[e] = s.kpp;
+            if (ma.fp_e) ma.fp_e[e] = s.fp;
+        }
+    }
+    // Kuu - Kup Kpu / Kpp: thread (I, ch), column nodes 4 ch .. 4 ch + 3
+    const int J0 = ch * kGenCh;
+    double acc[kGenCh][9];
+#pragma unroll
+    for (int j = 0; j < kGenCh; ++j)
+#pragma unroll
+        for (int v = 0; v < 9; ++v) acc[j][v] = 0.0;
+#pragma unroll 1
+    for (int gp = 0; gp < NGP; ++gp) {
+        const double h0 = s.h[gp][I][0], h1 = s.h[gp][I][1], h2 = s.h[gp][I][2];
+        const double* C = s.C[gp];
+        double Gc[3][9];
+#pragma unroll
+        for (int aa = 0; aa < 3; ++aa)
+#pragma unroll
+            for (int q = 0; q < 9; ++q) Gc[aa][q] = h0 * C[9 * aa + q] + h1 * C[9 * (3 + aa) + q] + h2 * C[9 * (6 + aa) + q];
+#pragma unroll
+        for (int j = 0; j < kGenCh; ++j) {
+            if (J0 + j < NPE) {
+                const double g0 = s.h[gp][J0 + j][0], g1 = s.h[gp][J0 + j][1], g2 = s.h[gp][J0 + j][2];
+#pragma unroll
+                for (int aa = 0; aa < 3; ++aa)
+#pragma unroll
+                    for (int bb = 0; bb < 3; ++bb)
+                        acc[j][3 * aa + bb] += Gc[aa][bb] * g0 + Gc[aa][3 + bb] * g1 + Gc[aa][6 + bb] * g2;
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < kGenCh; ++j) {
+        const int J = J0 + j;
+        if (J < NPE) {
+#pragma unroll
+            for (int aa = 0; aa < 3; ++aa)
+#pragma unroll
+                for (int bb = 0; bb < 3; ++bb) acc[j][3 * aa + bb] -= s.kup[I][aa] * s.kup[J][bb] * rkpp;
+            store_block<NPE, MODE>(a, e, I, J, node, freeI, acc[j]);
+        }
+    }
+}
+
+template <int NPE, int MODE>
+void launch_mixed0(const MixedElemArgs& a, cudaStream_t s) {
+    constexpr int TPE = NPE * ((NPE + kGenCh - 1) / kGenCh);
+    const size_t smem = kGenEpb * sizeof(P0Smem<NPE>);
+    static std::atomic<uint64_t> configured{0};
+    if (first_use_on_device(configured)) {
+        MPHY_CUDA(cudaFuncSetAttribute(elem_mixed0_kernel<NPE, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
+    }
+    const unsigned grid = ceil_div((size_t)a.base.n_elem, kGenEpb);
+    if (grid == 0) return;
+    elem_mixed0_kernel<NPE, MODE><<<grid, kGenEpb * TPE, smem, s>>>(a);
+    MPHY_CUDA(cudaGetLastError());
+}
+
+// p_e += (FP - Kpu du_e) / Kpp, one thread per element
+template <int NPE>
+__global__ void pressure_update_p0_kernel(int64_t n_elem, const int32_t* __restrict__ conn, const double* __restrict__ du,
+                                          const double* __restrict__ kup_e, const double* __restrict__ kpp_e,
+                                          const double* __restrict__ fp_e, double* __restrict__ pe) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n_elem; e += (int64_t)gridDim.x * blockDim.x) {
+        double v = 0.0;
+#pragma unroll
+        for (int I = 0; I < NPE; ++I) {
+            const int64_t n = conn[e * NPE + I];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) v += kup_e[e * 3 * NPE + 3 * I + c] * du[3 * n + c];
+        }
+        pe[e] += (fp_e[e] - v) / kpp_e[e];
+    }
+}
+
 // Batched material call: F [n][9] row-major -> sigma [n][9], C [n][81] (reference index order).
 __global__ void material_eval_kernel(int n, const double* __restrict__ Fm, const double* __restrict__ row_in,
                                      int tangent, double* __restrict__ stre, double* __restrict__ Cout) {
@@ -521,6 +763,28 @@ void launch_elem_mixed(const MixedElemArgs& a, int mode, cudaStream_t s) {
     if (mode == 1) launch_mixed<1>(a, s);
     else if (mode == 2) launch_mixed<2>(a, s);
     else launch_mixed<3>(a, s);
+}
+
+void launch_elem_mixed0(const MixedElemArgs& a, int npe, int mode, cudaStream_t s) {
+    if (npe == 8) {
+        if (mode == 1) launch_mixed0<8, 1>(a, s);
+        else if (mode == 2) launch_mixed0<8, 2>(a, s);
+        else launch_mixed0<8, 3>(a, s);
+    } else {
+        if (mode == 1) launch_mixed0<10, 1>(a, s);
+        else if (mode == 2) launch_mixed0<10, 2>(a, s);
+        else launch_mixed0<10, 3>(a, s);
+    }
+}
+
+void launch_pressure_update_p0(int64_t n_elem, int npe, const int32_t* conn, const double* du, const double* kup_e,
+                               const double* kpp_e, const double* fp_e, double* pe, cudaStream_t s, int sm) {
+    if (n_elem <= 0) return;
+    unsigned grid = ceil_div((size_t)n_elem, 256);
+    if (grid > (unsigned)sm * 8) grid = sm * 8;
+    if (npe == 8) pressure_update_p0_kernel<8><<<grid, 256, 0, s>>>(n_elem, conn, du, kup_e, kpp_e, fp_e, pe);
+    else pressure_update_p0_kernel<10><<<grid, 256, 0, s>>>(n_elem, conn, du, kup_e, kpp_e, fp_e, pe);
+    MPHY_CUDA(cudaGetLastError());
 }
 
 void launch_material_eval(int n, const double* F, const double* row_dev, int tangent, double* stre, double* C,

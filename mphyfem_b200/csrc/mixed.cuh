@@ -26,8 +26,21 @@ struct MixedElemArgs {
     double* btval = nullptr;
     double* cval = nullptr;
     double* rhs_p = nullptr;  // [n_pres]
+    // constant-pressure element (Elem_Solid_3D_Mixed0): element pressures in, and per element the
+    // coupling column Kup [n_elem][3 npe], Kpp [n_elem] and FP [n_elem] of the last evaluation out
+    const double* pe = nullptr;
+    double* kup_e = nullptr;
+    double* kpp_e = nullptr;
+    double* fp_e = nullptr;
 };
 
 void launch_elem_mixed(const MixedElemArgs& a, int mode, cudaStream_t s);
+// Elem_Solid_3D_Mixed0 (hex8 or tet10, one pressure per element), condensed: the displacement
+// element's outputs (Ke/Re export or the scatter of ElemArgs) plus kup_e, kpp_e, fp_e.
+void launch_elem_mixed0(const MixedElemArgs& a, int npe, int mode, cudaStream_t s);
+// Elem_Solid_3D_Mixed0::solveForPressure for every element: p_e += (FP - Kpu du_e) / Kpp, du the
+// node-major solution increment.
+void launch_pressure_update_p0(int64_t n_elem, int npe, const int32_t* conn, const double* du, const double* kup_e,
+                               const double* kpp_e, const double* fp_e, double* pe, cudaStream_t s, int sm);
 
 }  // namespace mphy

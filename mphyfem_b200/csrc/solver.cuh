@@ -70,6 +70,10 @@ struct mphy_solver {
     double t_pc_ms = 0.0;                 // last preconditioner setup time
     int32_t last_sweeps = 0;
     double* pinned = nullptr;  // [0] norm, [1] bad as bits
+    // constant-pressure mixed element (Elem_Solid_3D_Mixed0): element pressures (current and at
+    // the last converged step) and the coupling terms of the last assembly
+    bool p0 = false;
+    DevBuf<double> pe, pe_prev, kup_e, kpp_e, fp_e;
 };
 
 struct mphy_gnn {
@@ -84,4 +88,7 @@ namespace mphy {
 void solver_assemble(mphy_solver* s, const double* disp, uint8_t* bad_elem = nullptr);
 // ||rhs|| and the first bad element (-1 if none), one synchronisation.
 double solver_norm_and_bad(mphy_solver* s, int64_t* first_bad);
+// disp += solution, and for the constant-pressure element the element pressures' update
+// (factoriseSolveAndUpdate, femSolidmechanics2.cpp:1183-1212).
+void solver_update(mphy_solver* s, double* disp);
 }  // namespace mphy

@@ -202,8 +202,15 @@ def _kv(line):
 
 
 def _sub_blocks(body):
-    """label { key : value ... } entries inside a block body -> {label: {key: value}}."""
-    out, i = {}, 0
+    """label { key : value ... } entries inside a block body -> {label: {key: value}} (a label
+    given twice keeps its last entry; see _sub_block_list for blocks that repeat labels)."""
+    return dict(_sub_block_list(body))
+
+
+def _sub_block_list(body):
+    """label { key : value ... } entries inside a block body, in order, as (label, {key: value}):
+    the reference reads every entry, so one patch may carry several entries (one per DOF)."""
+    out, i = [], 0
     while i < len(body):
         ln = body[i]
         i += 1
@@ -220,7 +227,7 @@ def _sub_blocks(body):
                 kv[k] = v
             i += 1
         i += 1
-        out[label] = kv
+        out.append((label, kv))
     return out
 
 
@@ -290,14 +297,18 @@ def traction_forces(coords, faces, value):
     return F
 
 
-def read_config(config_path, mesh_path=None):
-    """A Problem from the reference's config (and the mesh it names, relative to the config's
-    directory, unless mesh_path is given). meta carries the Solver block's tolerance and
-    maximumIterations, the domains and the load-factor slope."""
-    import os
-    text = open(config_path).read()
+# element types of the reference's Element block (myIDmaps.h) that this build solves
+ELEMENT_TYPES = ("ELEM_SOLID_3D_DISP", "ELEM_SOLID_3D_MIXED0", "ELEM_SOLID_3D_MIXED1")
+
+
+def parse_config(text):
+    """The blocks of a reference config (femBase::readInput, femBase.cpp:121-364): a dict with
+    files, domains {label: (material, element)}, materials {id: {key: value}}, elements
+    {id: {key: value}}, bcs, tractions {patch: {key: value}}, tfs {id: TimeFunction}, nodal
+    (time function, [(node, dof, value)]) or None, and solver {timeStep, finalTime, maximumSteps,
+    maximumIterations, tolerance}. Ids are 0-based."""
     blocks = _blocks(text)
-    files, domains, materials, elements, bcs, tractions, tfs = {}, {}, {}, {}, {}, {}, {}
+    files, domains, materials, elements, bcs, tractions, tfs = {}, {}, {}, {}, [], {}, {}
     nodal = None
     solver = dict(timeStep=1.0, finalTime=1.0, maximumSteps=1, maximumIterations=10, tolerance=1e-10)
     for key, body in blocks:
@@ -320,7 +331,7 @@ def read_config(config_path, mesh_path=None):
             if any(float(x) != 0.0 for x in kv.get("value", "0").split()):
                 raise NotImplementedError("config: a nonzero body force is not supported by this build")
         elif key == "Boundary Conditions":
-            bcs = _sub_blocks(body)
+            bcs = _sub_block_list(body)
         elif key == "Tractions":
             tractions = _sub_blocks(body)
         elif key == "Nodal Forces":
@@ -350,6 +361,18 @@ def read_config(config_path, mesh_path=None):
             continue
         else:
             raise ValueError(f"config: key not found: {key!r} (femBase::readInput)")
+    return dict(files=files, domains=domains, materials=materials, elements=elements, bcs=bcs, tractions=tractions,
+                tfs=tfs, nodal=nodal, solver=solver)
+
+
+def read_config(config_path, mesh_path=None):
+    """A Problem from the reference's config (and the mesh it names, relative to the config's
+    directory, unless mesh_path is given). meta carries the Solver block's tolerance and
+    maximumIterations, the domains, and the element type of the domains' Element block."""
+    import os
+    cfg = parse_config(open(config_path).read())
+    files, domains, materials, elements = cfg["files"], cfg["domains"], cfg["materials"], cfg["elements"]
+    bcs, tractions, tfs, nodal, solver = cfg["bcs"], cfg["tractions"], cfg["tfs"], cfg["nodal"], cfg["solver"]
     mesh_path = mesh_path or os.path.join(os.path.dirname(os.path.abspath(config_path)), files["mesh"])
     m = read_gmsh22(mesh_path)
     if m["ndim"] != 3:
@@ -392,7 +415,7 @@ def read_config(config_path, mesh_path=None):
     n_node = len(coords)
     # prescribed DOFs
     fixed = np.zeros((n_node, 3), dtype=np.uint8)
-    for label, kv in bcs.items():
+    for label, kv in bcs:
         if label not in m["faces"]:
             raise ValueError(f"config: boundary condition on unknown patch {label!r}")
         nodes = sorted({v for fc in m["faces"][label] for v in fc})
@@ -428,11 +451,19 @@ def read_config(config_path, mesh_path=None):
         c = slope_of(nodal[0])
         for n, d, v in nodal[1]:
             F[n, d] += c * v
+    etypes = {elements.get(domains[label][1], {}).get("type", "ELEM_SOLID_3D_DISP") for label in m["domains"]}
+    if len(etypes) != 1:
+        raise NotImplementedError("config: every domain must use the same element type")
+    etype = etypes.pop()
+    if etype not in ELEMENT_TYPES:
+        raise NotImplementedError(f"config: element type {etype!r}: supported are {ELEMENT_TYPES}")
+    if etype == "ELEM_SOLID_3D_MIXED1" and npe != 10:
+        raise NotImplementedError("config: ELEM_SOLID_3D_MIXED1 is built for tet10 meshes")
     prob = Problem(name=os.path.basename(config_path), coords=coords, conn=conn, mat_id=mat_id,
                    mats=np.array(rows, dtype=np.float64), fixed=fixed.ravel(), fnodal=F.ravel(),
                    dt=dt, t_final=tfin, max_steps=solver["maximumSteps"],
                    meta={"tolerance": solver["tolerance"], "maximumIterations": solver["maximumIterations"],
-                         "domains": m["domains"], "patches": list(m["patches"])})
+                         "domains": m["domains"], "patches": list(m["patches"]), "element": etype})
     if any(models):
         prob.mat_model = np.array(models, dtype=np.int32)
         prob.mat_data = np.array(mdata, dtype=np.float64)

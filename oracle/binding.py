@@ -61,6 +61,13 @@ def lib():
         L.orc_mixed_constants.argtypes = [C.c_int, C.c_double, C.c_double, _d, _d]
         L.orc_elem_mixed.argtypes = [C.c_int, _d, _d, _d, _d, C.c_int, _d, C.c_double, C.c_int, _d, _d, _d, _d,
                                      _d, _d]
+        L.orc_elem_mixed0.argtypes = [C.c_int, _d, _d, _d, C.c_double, C.c_int, _d, C.c_double, C.c_int, _d, _d,
+                                      _d, _d, _d]
+        L.orc_problem_set_mixed_p0.argtypes = [C.c_void_p, C.c_int]
+        L.orc_problem_p0_pressure.argtypes = [C.c_void_p, _d, _d]
+        L.orc_problem_p0_pressure.restype = None
+        L.orc_problem_save_step.argtypes = [C.c_void_p, _d]
+        L.orc_problem_save_step.restype = None
         L.orc_problem_create.argtypes = [C.c_int, _d, C.c_int, C.c_int, _i32, _i32, C.c_int, _d, _u8]
         L.orc_problem_create.restype = C.c_void_p
         L.orc_problem_destroy.argtypes = [C.c_void_p]
@@ -167,6 +174,21 @@ def elem_mixed(X, u, u_prev, pn, model, data, Kinv, utype=3):
     return Kuu, Kup, Kpu, Kpp, FU, FP, bad
 
 
+def elem_mixed0(X, u, u_prev, pres, model, data, Kinv, utype=3):
+    """Constant-pressure u-p element (hex8 or tet10), condensed: K, F, kup (= Kpu), Kpp, FP, bad."""
+    X, u, up = (np.ascontiguousarray(a, dtype=np.float64) for a in (X, u, u_prev))
+    npe = X.shape[0]
+    d = _mat_data(data)
+    ns = 3 * npe
+    K, F, kup = np.zeros((ns, ns)), np.zeros(ns), np.zeros(ns)
+    kpp, fp = np.zeros(1), np.zeros(1)
+    bad = lib().orc_elem_mixed0(npe, _p(X, _d), _p(u, _d), _p(up, _d), float(pres), int(model), _p(d, _d), Kinv, utype,
+                                _p(K, _d), _p(F, _d), _p(kup, _d), _p(kpp, _d), _p(fp, _d))
+    if bad == 2:
+        raise ValueError("oracle: the constant-pressure element is hex8 or tet10")
+    return K, F, kup, float(kpp[0]), float(fp[0]), bad
+
+
 def gauss_rule(npe):
     xi, w = np.zeros((8, 3)), np.zeros(8)
     N, dN = np.zeros((8, npe)), np.zeros((8, 3, npe))
@@ -201,6 +223,21 @@ class OracleProblem:
         if getattr(self, "h", None) and _lib is not None:
             _lib.orc_problem_destroy(self.h)
             self.h = None
+
+    def set_mixed_p0(self, enable=True):
+        """Elem_Solid_3D_Mixed0 for every element (condensed element pressures, zero to start)."""
+        if lib().orc_problem_set_mixed_p0(self.h, int(enable)):
+            raise ValueError("oracle: Utype -1 has no constant-pressure element (Kpp = 0)")
+
+    def p0_pressure(self, set_to=None):
+        out = np.zeros(self.prob.n_elem)
+        src = None if set_to is None else np.ascontiguousarray(set_to, np.float64)
+        lib().orc_problem_p0_pressure(self.h, _p(src, _d), _p(out, _d))
+        return out
+
+    def save_step(self, disp):
+        d = np.ascontiguousarray(disp, np.float64)
+        lib().orc_problem_save_step(self.h, _p(d, _d))
 
     def pattern(self):
         ns = 3 * self.prob.npe

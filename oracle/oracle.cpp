@@ -179,6 +179,11 @@ struct orc_problem {
     // position of each (element row i, element col j) entry in the CSR value array, -1 if
     // either DOF is prescribed (what MatSetValue's row search resolves, SolverPetsc.cpp:370-374)
     std::vector<int64_t> slot;  // [n_elem][nsize*nsize]
+    // constant-pressure mixed element (Elem_Solid_3D_Mixed0): element pressures, their values at
+    // the last converged step, that step's displacement (Jn), and the coupling terms of the last
+    // element evaluation (for solveForPressure)
+    bool p0 = false;
+    mutable std::vector<double> pe, pe_prev, disp_prev, kup, kpp, fp;
 };
 
 extern "C" {
@@ -633,8 +638,28 @@ void elem_eval(const orc_problem* p, int64_t e, const double* disp, double* K, d
     gather_element(p, e, disp, X, u);
     const size_t id = (size_t)p->mat_id[e];
     const double* m = &p->mats[3 * id];
+    if (p->p0) {
+        double X2[3 * kMaxNpe], up[3 * kMaxNpe];
+        gather_element(p, e, p->disp_prev.data(), X2, up);
+        const int ns = 3 * p->npe;
+        *bad = orc_elem_mixed0(p->npe, X, u, up, p->pe[e], p->model[id], &p->data[ORC_MAT_NDATA * id], m[1],
+                               (int)m[2], K, R, &p->kup[e * ns], &p->kpp[e], &p->fp[e]);
+        return;
+    }
     *bad = orc_elem_stiffness_residual_mat(p->npe, X, u, p->model[id], &p->data[ORC_MAT_NDATA * id], m[1], (int)m[2],
                                            K, R);
+}
+
+// Elem_Solid_3D_Mixed0::solveForPressure (Elem_Solid_3D_Mixed0.cpp:112-200) for every element:
+// p += (FP - Kpu du_e) / Kpp with du the node-major solution increment.
+void p0_pressure_update(const orc_problem* p, const double* du) {
+    const int ns = 3 * p->npe;
+    for (int64_t e = 0; e < p->n_elem; ++e) {
+        double v = 0.0;
+        for (int I = 0; I < p->npe; ++I)
+            for (int c = 0; c < 3; ++c) v += p->kup[e * ns + 3 * I + c] * du[3 * (size_t)p->conn[e * p->npe + I] + c];
+        p->pe[e] += (p->fp[e] - v) / p->kpp[e];
+    }
 }
 
 }  // namespace
@@ -874,6 +899,7 @@ int orc_newton_run(const orc_problem* p, const double* fnodal, const orc_newton_
         t += dt;
         const double lambda = t;
         std::copy(disp, disp + nd, disp_prev.begin());
+        if (p->p0) orc_problem_save_step(p, disp);
         bool converged = false;
         double norm = -1.0, norm_prev = -1.0, tol = o->tol_abs;
         for (int iter = 1; iter <= o->max_newton; ++iter) {
@@ -897,6 +923,11 @@ int orc_newton_run(const orc_problem* p, const double* fnodal, const orc_newton_
                 orc_cg_jacobi(p, val.data(), rhs.data(), dx.data(), o->cg_rtol, 1.0e-50, o->cg_maxit,
                               o->nthreads, &its, &fn);
                 for (int i = 0; i < n; ++i) disp[P.assy_for_soln[i]] += dx[i];
+                if (p->p0) {
+                    std::vector<double> du(nd, 0.0);
+                    for (int i = 0; i < n; ++i) du[P.assy_for_soln[i]] = dx[i];
+                    p0_pressure_update(p, du.data());
+                }
             }
             if (rows < max_hist && hist) {
                 hist[4 * rows + 0] = steps_done;
@@ -914,6 +945,7 @@ int orc_newton_run(const orc_problem* p, const double* fnodal, const orc_newton_
             dt *= 0.5;
             if (dt < dt0 * 0.01) return -1;
             std::copy(disp_prev.begin(), disp_prev.end(), disp);
+            if (p->p0) p->pe = p->pe_prev;
         }
     }
     return rows;
@@ -937,11 +969,14 @@ void orc_mixed_constants(int Utype, double Jn, double K, double* Jhat, double* t
 // Elem_Solid_3D_Mixed1.cpp:55-75, STATIC scheme (af = 1, no inertia or body force). X, u, u_prev:
 // [10][3]; pn: the 4 vertex pressures. Kuu [30][30], Kup [30][4], Kpu [4][30], Kpp [4][4], FU [30],
 // FP [4], row-major. Returns 0, 1 when some Gauss point has det F < 0, 2 for npe != 10.
-int orc_elem_mixed(int npe, const double* X, const double* u, const double* u_prev, const double* pn, int model,
-                   const double* data, double Kinv, int Utype, double* Kuu, double* Kup, double* Kpu, double* Kpp,
-                   double* FU, double* FP) {
-    if (npe != 10) return 2;
-    constexpr int NP = 4, NS = 30;
+// ElementBase::calcStiffnessAndResidualMixed3D (ElementBase2.cpp:278-553) for NP pressure
+// functions: NP = 4, the tet10 vertex-linear pressure of Elem_Solid_3D_Mixed1 (pn: the vertex
+// pressures), or NP = 1, the constant pressure of Elem_Solid_3D_Mixed0 (Np = 1, pn[0] = the
+// element's pressure; :385-389), on the hex8 or tet10 displacement element.
+static int mixed_blocks(int npe, int NP, const double* X, const double* u, const double* u_prev, const double* pn,
+                        int model, const double* data, double Kinv, int Utype, double* Kuu, double* Kup, double* Kpu,
+                        double* Kpp, double* FU, double* FP) {
+    const int NS = 3 * npe;
     GaussRule rule;
     element_rule(npe, rule);
     std::fill(Kuu, Kuu + NS * NS, 0.0);
@@ -975,9 +1010,15 @@ int orc_elem_mixed(int npe, const double* X, const double* u, const double* u_pr
         const double J = det3(Fa);
         if (J < 0.0) bad = 1;
         const double dvol = rule.w[q] * spatial_gradients(npe, x, dN, g);
-        // LagrangeBasisFunsTetra(4): the barycentric coordinates, vertex order
+        // LagrangeBasisFunsTetra(4): the barycentric coordinates, vertex order; or Np = 1
         const double* xi = rule.xi[q];
-        const double Np[NP] = {1.0 - xi[0] - xi[1] - xi[2], xi[0], xi[1], xi[2]};
+        double Np[4] = {1.0, 0.0, 0.0, 0.0};
+        if (NP == 4) {
+            Np[0] = 1.0 - xi[0] - xi[1] - xi[2];
+            Np[1] = xi[0];
+            Np[2] = xi[1];
+            Np[3] = xi[2];
+        }
         double pres = 0.0;
         for (int i = 0; i < NP; ++i) pres += Np[i] * pn[i];
         double stre[9], C[81];
@@ -1010,6 +1051,55 @@ int orc_elem_mixed(int npe, const double* X, const double* u, const double* u_pr
         }
     }
     return bad;
+}
+
+int orc_elem_mixed(int npe, const double* X, const double* u, const double* u_prev, const double* pn, int model,
+                   const double* data, double Kinv, int Utype, double* Kuu, double* Kup, double* Kpu, double* Kpp,
+                   double* FU, double* FP) {
+    if (npe != 10) return 2;
+    return mixed_blocks(10, 4, X, u, u_prev, pn, model, data, Kinv, Utype, Kuu, Kup, Kpu, Kpp, FU, FP);
+}
+
+int orc_elem_mixed0(int npe, const double* X, const double* u, const double* u_prev, double pres, int model,
+                    const double* data, double Kinv, int Utype, double* K, double* F, double* kup, double* kpp,
+                    double* fp) {
+    if (npe != 8 && npe != 10) return 2;
+    const int ns = 3 * npe;
+    double Kpu[3 * kMaxNpe], Kpp = 0.0, FP = 0.0;
+    const int bad = mixed_blocks(npe, 1, X, u, u_prev, &pres, model, data, Kinv, Utype, K, kup, Kpu, &Kpp, F, &FP);
+    if (bad == 2) return 2;
+    // static condensation of the element pressure (Elem_Solid_3D_Mixed0.cpp:97-98)
+    for (int i = 0; i < ns; ++i) {
+        for (int j = 0; j < ns; ++j) K[i * ns + j] -= kup[i] * (Kpu[j] / Kpp);
+        F[i] -= kup[i] * (FP / Kpp);
+    }
+    *kpp = Kpp;
+    *fp = FP;
+    return bad;
+}
+
+int orc_problem_set_mixed_p0(orc_problem* p, int enable) {
+    for (size_t k = 0; k < p->mats.size() / 3; ++k)
+        if (enable && (int)p->mats[3 * k + 2] == -1) return 2;
+    p->p0 = enable != 0;
+    const size_t ne = (size_t)p->n_elem;
+    p->pe.assign(ne, 0.0);
+    p->pe_prev.assign(ne, 0.0);
+    p->kup.assign(ne * 3 * p->npe, 0.0);
+    p->kpp.assign(ne, 0.0);
+    p->fp.assign(ne, 0.0);
+    p->disp_prev.assign(3 * (size_t)p->n_node, 0.0);
+    return 0;
+}
+
+void orc_problem_p0_pressure(const orc_problem* p, const double* set, double* get) {
+    if (set) std::copy(set, set + p->n_elem, p->pe.begin());
+    if (get) std::copy(p->pe.begin(), p->pe.end(), get);
+}
+
+void orc_problem_save_step(const orc_problem* p, const double* disp) {
+    p->disp_prev.assign(disp, disp + 3 * (size_t)p->n_node);
+    p->pe_prev = p->pe;
 }
 
 // femSolidmechanics::solveWithArclength (femSolidmechanics2.cpp:855-1039) with

@@ -67,6 +67,16 @@ int orc_elem_mixed(int npe, const double* X, const double* u, const double* u_pr
                    const double* data, double Kinv, int Utype, double* Kuu, double* Kup, double* Kpu, double* Kpp,
                    double* FU, double* FP);
 
+/* Constant-pressure mixed element (Elem_Solid_3D_Mixed0, Elem_Solid_3D_Mixed0.cpp): hex8 or tet10
+ * displacement, one pressure per element (nlbfP = 1, Np = 1, pres = the element's pressure), the
+ * blocks of ElementBase::calcStiffnessAndResidualMixed3D condensed (:93-101):
+ * K = Kuu - Kup Kpu / Kpp, F = FU - Kup FP / Kpp. Outputs K [3npe][3npe], F [3npe] and the
+ * coupling column kup [3npe] (= Kpu), Kpp and FP for solveForPressure (:112-200).
+ * Returns 0, 1 when some Gauss point has det F < 0, 2 for an unsupported npe or model. */
+int orc_elem_mixed0(int npe, const double* X, const double* u, const double* u_prev, double pres, int model,
+                    const double* data, double Kinv, int Utype, double* K, double* F, double* kup, double* kpp,
+                    double* fp);
+
 /* ---- see orc_problem_create below: every element of a tet10 problem as a mixed u-p element.
  * disp, disp_prev: [3*n_node]; pres: [n_node] nodal pressures (vertex nodes used). Outputs per
  * element: Kuu [30][30], Kup [30][4] (Kpu = Kup^T), Kpp [4][4], FU [30], FP [4]. Returns the
@@ -119,6 +129,16 @@ void orc_problem_destroy(orc_problem* p);
  * mats[3k]. Returns 0, 1 when n_mat differs from the problem's, 2 for an unknown model. */
 int orc_problem_set_materials(orc_problem* p, int n_mat, const int32_t* model, const double* data);
 int orc_problem_nfree(const orc_problem* p);
+/* Elem_Solid_3D_Mixed0 for every element (enable = 1; 0 = the displacement element): assembly,
+ * elements and Newton use the condensed element; the Newton run updates the element pressures
+ * after every solve (femSolidmechanics2.cpp:1204-1212), saves them with each converged step and
+ * restores them on a cut. Pressures and the last-step displacement start at zero.
+ * Returns 2 when a material has Utype -1 (Kpp = 0). */
+int orc_problem_set_mixed_p0(orc_problem* p, int enable);
+/* element pressures [n_elem]: set (may be NULL) copied in first, then get (may be NULL) filled */
+void orc_problem_p0_pressure(const orc_problem* p, const double* set, double* get);
+/* the last converged step: disp (its J is the mixed element's Jn) and the element pressures */
+void orc_problem_save_step(const orc_problem* p, const double* disp);
 int64_t orc_problem_nnz(const orc_problem* p);
 /* assy_for_soln: [n_free]; for_assy_vec: [n_elem][3npe]; rowptr: [n_free+1]; col: [nnz] */
 void orc_problem_export_pattern(const orc_problem* p, int32_t* assy_for_soln,

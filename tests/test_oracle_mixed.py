@@ -118,3 +118,36 @@ def test_uniaxial_patch(oracle, consistent, model, data):
     assert np.allclose(pres[vert], 20.0 * (J - 1.0), rtol=1e-9)
     # quadratic convergence: every step ends within 5 iterations
     assert max(np.bincount(hist[:, 0].astype(int))[1:]) <= 5
+
+
+@pytest.mark.parametrize("npe", [8, 10])
+@pytest.mark.parametrize("model,data", [(0, [0.7]), (2, [0.7, 12.0])], ids=["nh", "gent"])
+def test_constant_pressure_element_condensation(oracle, consistent, npe, model, data):
+    """Elem_Solid_3D_Mixed0: FU and FP are linear in the element pressure, so the condensed residual
+    F = FU - Kup FP / Kpp is FU at the pressure p* = p + FP / Kpp that zeroes FP, for any p; at p*
+    the condensed tangent K = Kuu - Kup Kpu / Kpp is minus its derivative (finite differences)."""
+    rng = np.random.default_rng(3)
+    if npe == 10:
+        X, u, up, _ = _tet10(7)
+    else:
+        X = meshgen.hex8_cantilever(1, 1, 1, lx=1.0).coords[meshgen.hex8_cantilever(1, 1, 1, lx=1.0).conn[0]]
+        X = X + 0.02 * rng.standard_normal(X.shape)
+        u, up = 0.05 * rng.standard_normal((8, 3)), 0.03 * rng.standard_normal((8, 3))
+    ns = 3 * npe
+    K0, F0, kup, kpp, fp, bad = oracle.elem_mixed0(X, u, up, 0.1, model, data, 0.05, 3)
+    assert bad == 0 and kpp < 0
+    pstar = 0.1 + fp / kpp
+    K, F, _, _, fp2, _ = oracle.elem_mixed0(X, u, up, pstar, model, data, 0.05, 3)
+    assert abs(fp2) <= 1e-12 * max(abs(fp), 1e-300) + 1e-15
+    assert np.abs(F - F0).max() <= 1e-12 * np.abs(F0).max()  # the condensed residual does not depend on p
+    assert np.abs(K - K.T).max() <= 1e-12 * np.abs(K).max() or model != 0
+    h = 1e-6
+    KF = np.zeros((ns, ns))
+    for j in range(ns):
+        a, b = u.ravel().copy(), u.ravel().copy()
+        a[j] += h
+        b[j] -= h
+        r1 = oracle.elem_mixed0(X, a.reshape(npe, 3), up, pstar, model, data, 0.05, 3)
+        r2 = oracle.elem_mixed0(X, b.reshape(npe, 3), up, pstar, model, data, 0.05, 3)
+        KF[:, j] = -(r1[1] - r2[1]) / (2 * h)
+    assert np.abs(K - KF).max() <= 1e-7 * np.abs(K).max()

@@ -1,5 +1,7 @@
 """The reference's input formats (Gmsh 2.2 + config): round trips of the generated workloads,
 traction quadrature against closed forms, and the config reader's rules and limits."""
+import os
+
 import numpy as np
 import pytest
 
@@ -175,3 +177,74 @@ def test_gent_block(tmp_path):
     (tmp_path / "config").write_text(CONFIG.replace("Matl_NeoHookean", "Matl_Gent"))
     with pytest.raises(ValueError):
         rio.read_config(tmp_path / "config")                     # Gent needs mu and Im
+
+
+EXAMPLE4 = "/root/reference/doc/examples/SolidMechanics/Example4/example4.rst"
+
+
+def _example4_config():
+    """The config of the reference's 3D mixed example (block under compression, Taylor-Hood
+    ELEM_SOLID_3D_MIXED1): the literal block of its documentation page."""
+    if not os.path.exists(EXAMPLE4):
+        pytest.skip("the reference's documentation is not available here")
+    lines = open(EXAMPLE4).read().splitlines()
+    start = next(i for i, ln in enumerate(lines) if ln.rstrip().endswith("::")) + 1
+    body = []
+    for ln in lines[start:]:
+        if ln.strip() and not ln.startswith(" "):
+            break
+        body.append(ln[4:] if ln.startswith("    ") else ln.strip())
+    return "\n".join(body)
+
+
+def test_reference_example4_config_parses():
+    cfg = rio.parse_config(_example4_config())
+    assert cfg["files"]["mesh"] == "block3d-P2-nelem8"
+    assert cfg["elements"][0]["type"] == "ELEM_SOLID_3D_MIXED1"
+    mat = cfg["materials"][0]
+    assert mat["name"] == "Matl_NeoHookean"
+    ut, kinv = mat["data_volumetric"].split()
+    assert int(ut) == 3 and float(kinv) == pytest.approx(2.494128406043830e-06)
+    assert float(mat["data_deviatoric"]) == pytest.approx(80.19367957863858)
+    assert cfg["domains"]["block"] == (0, 0)
+    assert cfg["tractions"]["pressure"]["value"].split() == ["-320", "0.0", "0.0"]
+    s = cfg["solver"]
+    assert (s["timeStep"], s["finalTime"], s["maximumSteps"], s["maximumIterations"]) == (0.2, 1.0, 10, 20)
+    assert s["tolerance"] == pytest.approx(1e-7)
+    assert cfg["tfs"][0](0.4) == pytest.approx(0.4)
+
+
+def test_reference_example4_on_a_generated_block(tmp_path):
+    """The example's config on a tet10 unit block with its patches (the quarter of the top face
+    at x, y <= 1/2 loaded, the rest of the top held in x and y, symmetry planes): element type,
+    material, the specified (zero) DOFs -- the config gives `top` and `pressure` one entry per DOF,
+    and every entry counts -- and the load resultant 320 * 1/4 along z."""
+    text = _example4_config()
+    p = meshgen.tet10_kuhn(4, 4, 4, lx=1.0, jitter=0.0)
+    X = p.coords
+    on = lambda c, v: np.isclose(X[:, c], v)  # noqa: E731
+    quarter = lambda Y: np.isclose(Y[:, 2], 1.0) & (Y[:, 0] <= 0.5 + 1e-12) & (Y[:, 1] <= 0.5 + 1e-12)  # noqa: E731
+    pressure = rio.boundary_faces(p, quarter)
+    top_all = rio.boundary_faces(p, lambda Y: np.isclose(Y[:, 2], 1.0))
+    pk = {tuple(sorted(f)) for f in pressure}
+    patches = {"symX": rio.boundary_faces(p, lambda Y: np.isclose(Y[:, 0], 0.0)),
+               "symY": rio.boundary_faces(p, lambda Y: np.isclose(Y[:, 1], 0.0)),
+               "symZ": rio.boundary_faces(p, lambda Y: np.isclose(Y[:, 2], 0.0)),
+               "top": [f for f in top_all if tuple(sorted(f)) not in pk], "pressure": pressure}
+    rio.write_gmsh22(tmp_path / "block.msh", p, patches, domain_names=["block"])
+    (tmp_path / "example4.cfg").write_text(text)
+    q = rio.read_config(tmp_path / "example4.cfg", mesh_path=tmp_path / "block.msh")
+    assert q.meta["element"] == "ELEM_SOLID_3D_MIXED1"
+    assert q.mats[0] == pytest.approx([80.19367957863858, 2.494128406043830e-06, 3.0])
+    fx = q.fixed.reshape(-1, 3)
+    assert np.all(fx[on(0, 0.0), 0] == 1) and np.all(fx[on(1, 0.0), 1] == 1) and np.all(fx[on(2, 0.0), 2] == 1)
+    top = on(2, 1.0)
+    assert np.all(fx[top, 0] == 1) and np.all(fx[top, 1] == 1)
+    free_inside = ~(on(0, 0.0) | on(1, 0.0) | on(2, 0.0) | top)
+    assert np.all(fx[free_inside] == 0)
+    # the reference's face normal is dx/deta x dx/dxi (BasisFunctionsLagrange.cpp:1711), which points
+    # into the block for the outward-ordered faces boundary_faces writes: s0 = -320 then pulls
+    F = q.fnodal.reshape(-1, 3)
+    assert F[:, 2].sum() == pytest.approx(320.0 * 0.25, rel=1e-12)
+    assert np.abs(F[:, :2]).max() <= 1e-12 * 320
+    assert (q.dt, q.t_final, q.max_steps) == (0.2, 1.0, 10)
