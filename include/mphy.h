@@ -143,6 +143,17 @@ int mphy_mesh_create(mphy_ctx* ctx, int32_t n_node, const double* coords_host, i
                      mphy_mesh** out);
 int mphy_mesh_destroy(mphy_mesh* mesh);
 
+/* Nonzero prescribed displacements ("specified" boundary conditions, femSolidmechanics1.cpp:813-891):
+ * the DOFs flagged in `fixed` take t * ramp_host[i] + const_host[i] at time t of the load stepping
+ * (a boundary condition with the time function lam = t, and one without a time function, which the
+ * reference applies in full from the first step). Host arrays [3*n_node], either may be NULL (zero);
+ * entries of free DOFs are ignored; all-zero values return the mesh to clamped DOFs. mphy_newton_run
+ * lifts each step's increment dispApplied = value(t) - disp into the first iteration's right-hand
+ * side (ElementBase::applyDirichletBCs, ElementBase.cpp:567-594) and adds it to the displacement
+ * with that iteration's solution (femSolidmechanics2.cpp:1137-1145). Not available with the
+ * MPHY_PREC_MIXED_TC tangent, the two-field mixed element, arc-length or the batched form. */
+int mphy_mesh_set_prescribed(mphy_mesh* mesh, const double* ramp_host, const double* const_host);
+
 /* ---- hyperelastic models (the compressible branch of utilitiesmaterialHyperelastic.cpp) and
  * their deviatoric parameters, as the reference's material blocks give them:
  *   MPHY_MAT_NEOHOOKEAN   Matl_NeoHookean    data_deviatoric : mu          (:186-295)

@@ -92,6 +92,7 @@ SIGNATURES = {
     "mphy_mesh_create": (C.c_int, [_vp, C.c_int32, _d, C.c_int32, C.c_int32, _i32, _i32, C.c_int32, _d, _u8,
                                    C.POINTER(_vp)]),
     "mphy_mesh_destroy": (C.c_int, [_vp]),
+    "mphy_mesh_set_prescribed": (C.c_int, [_vp, _d, _d]),
     "mphy_material_nh_eval": (C.c_int, [_vp, C.c_int32, _vp, C.c_double, C.c_double, C.c_int32, C.c_int32, _vp, _vp]),
     "mphy_mesh_set_materials": (C.c_int, [_vp, C.c_int32, _i32, _d]),
     "mphy_material_eval": (C.c_int, [_vp, C.c_int32, _vp, C.c_int32, _d, C.c_double, C.c_int32, C.c_int32, _vp,

@@ -78,6 +78,15 @@ class Mesh:
         self.h = h
         if getattr(prob, "mat_model", None) is not None:
             self.set_materials(prob.mat_model, prob.mat_data)
+        if getattr(prob, "presc_ramp", None) is not None or getattr(prob, "presc_const", None) is not None:
+            self.set_prescribed(prob.presc_ramp, prob.presc_const)
+
+    def set_prescribed(self, ramp=None, const=None):
+        """Nonzero prescribed displacements: t * ramp + const on the prescribed DOFs at time t."""
+        r = None if ramp is None else _np(ramp, np.float64)
+        c = None if const is None else _np(const, np.float64)
+        L.check(self.lib.mphy_mesh_set_prescribed(self.h, None if r is None else r.ctypes.data_as(L._d),
+                                                  None if c is None else c.ctypes.data_as(L._d)))
 
     def set_materials(self, model, data):
         """Per-material hyperelastic model (MAT_*) and parameters [n_mat, MAT_NDATA]

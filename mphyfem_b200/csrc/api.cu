@@ -66,10 +66,11 @@ ElemArgs elem_args(const mphy_mesh* m, const double* disp, int tangent, unsigned
     return a;
 }
 
-void solver_assemble(mphy_solver* s, const double* disp, uint8_t* bad_elem) {
+void solver_assemble(mphy_solver* s, const double* disp, uint8_t* bad_elem, const double* lift) {
     solver_zero(s);
     ElemArgs a = elem_args(s->mesh, disp, s->opts.tangent, s->bad.p);
     a.bad_elem = bad_elem;
+    a.lift = lift;
     a.e2v = s->pat->e2v.p;
     a.val = s->val.p;
     a.valf = s->mixed ? s->valf.p : nullptr;
@@ -499,6 +500,38 @@ int mphy_mesh_destroy(mphy_mesh* m) {
     cudaDeviceSynchronize();
     delete m;
     return MPHY_OK;
+}
+
+int mphy_mesh_set_prescribed(mphy_mesh* m, const double* ramp, const double* cst) {
+    return guarded([&] {
+        MPHY_REQUIRE(m, MPHY_ERR_INVALID_ARG, "null mesh");
+        const size_t nd = 3 * (size_t)m->n_node;
+        bool any = false;
+        std::vector<double> r(nd, 0.0), c(nd, 0.0);
+        for (size_t i = 0; i < nd; ++i) {
+            if (!m->fixed_host[i]) continue;
+            r[i] = ramp ? ramp[i] : 0.0;
+            c[i] = cst ? cst[i] : 0.0;
+            MPHY_REQUIRE(std::isfinite(r[i]) && std::isfinite(c[i]), MPHY_ERR_INVALID_ARG,
+                         "prescribed displacement is not finite");
+            any |= r[i] != 0.0 || c[i] != 0.0;
+        }
+        MPHY_CUDA(cudaSetDevice(m->device));
+        if (!any) {
+            m->presc_ramp.release();
+            m->presc_const.release();
+            m->has_presc = false;
+            return (int)MPHY_OK;
+        }
+        m->presc_ramp.alloc(nd);
+        m->presc_const.alloc(nd);
+        cudaStream_t st = m->ctx->stream;
+        m->presc_ramp.upload(r.data(), nd, st);
+        m->presc_const.upload(c.data(), nd, st);
+        MPHY_CUDA(cudaStreamSynchronize(st));
+        m->has_presc = true;
+        return (int)MPHY_OK;
+    });
 }
 
 int mphy_mesh_set_materials(mphy_mesh* m, int32_t n_mat, const int32_t* model, const double* data) {
@@ -1108,6 +1141,10 @@ int mphy_newton_run(mphy_solver* s, const double* fext_host, const mphy_newton_o
         double* disp = s->disp_tmp.p;
         s->disp_tmp.upload(disp_host, nd, st);
         s->fext_tmp.upload(fext_host, nd, st);
+        const bool presc = s->mesh->has_presc;
+        MPHY_REQUIRE(!presc || s->opts.precision != MPHY_PREC_MIXED_TC, MPHY_ERR_UNSUPPORTED,
+                     "prescribed displacements with the tensor-core tangent");
+        if (presc && s->lift.n != nd) s->lift.alloc(nd);
         double t = 0.0, dt = o->dt;
         const double dt0 = o->dt;
         int steps_done = 1, rows = 0, rc = MPHY_OK;
@@ -1117,12 +1154,17 @@ int mphy_newton_run(mphy_solver* s, const double* fext_host, const mphy_newton_o
             const double lambda = t;
             MPHY_CUDA(cudaMemcpyAsync(s->disp_prev.p, disp, nd * sizeof(double), cudaMemcpyDeviceToDevice, st));
             if (s->p0) s->pe_prev.copy_from(s->pe, st);
+            // setBoundaryConditions (femSolidmechanics1.cpp:813-891): dispApplied = value(t) - disp on
+            // the prescribed DOFs, lifted in the first iteration and added with its solution
+            if (presc)
+                prescribed_increment(s->mesh->fixed.p, s->mesh->presc_ramp.p, s->mesh->presc_const.p, t, disp,
+                                     s->lift.p, (int64_t)nd, st, s->ctx->sm_count);
             bool converged = false;
             double norm = -1.0, norm_prev = -1.0, tol = o->tol_abs;
             for (int iter = 1; iter <= o->max_newton; ++iter) {
                 mphy_iter_stats is{};
                 MPHY_CUDA(cudaEventRecord(s->ctx->ev0, st));
-                solver_assemble(s, disp);
+                solver_assemble(s, disp, nullptr, presc && iter == 1 ? s->lift.p : nullptr);
                 add_scaled_free(s->mesh->fixed.p, s->fext_tmp.p, lambda, s->rhs.p, (int64_t)nd, st, s->ctx->sm_count);
                 MPHY_CUDA(cudaEventRecord(s->ctx->ev1, st));
                 int64_t bad = -1;
@@ -1143,6 +1185,8 @@ int mphy_newton_run(mphy_solver* s, const double* fext_host, const mphy_newton_o
                     double fn = 0.0;
                     is.status = solver_solve(s, &its, &fn);  // KSP divergence is only reported
                     solver_update(s, disp);
+                    // dispIncr[prescribed] += dispApplied in the first iteration (femSolidmechanics2.cpp:1137-1145)
+                    if (presc && iter == 1) axpy_inplace(disp, s->lift.p, 1.0, (int64_t)nd, st, s->ctx->sm_count);
                     MPHY_CUDA(cudaEventRecord(s->ctx->ev1, st));
                     MPHY_CUDA(cudaEventSynchronize(s->ctx->ev1));
                     is.t_solve_ms = elapsed_ms(s->ctx);
@@ -1185,6 +1229,7 @@ int mphy_arclength_run(mphy_solver* s, const double* fext_host, const mphy_newto
         MPHY_REQUIRE(o->dt > 0.0 && o->max_newton >= 2, MPHY_ERR_INVALID_ARG,
                      "arc-length needs dt > 0 and max_newton >= 2 (iterations 1..max_newton-1)");
         MPHY_REQUIRE(!s->p0, MPHY_ERR_UNSUPPORTED, "arc-length with the constant-pressure element");
+        MPHY_REQUIRE(!s->mesh->has_presc, MPHY_ERR_UNSUPPORTED, "arc-length with nonzero prescribed displacements");
         const size_t nd = 3 * (size_t)s->mesh->n_node;
         const int64_t n = (int64_t)nd;
         cudaStream_t st = s->ctx->stream;

@@ -780,6 +780,8 @@ int mphy_batch_create(mphy_solver* s, int32_t n_inst, const int32_t* node_ptr, m
     return guarded([&] {
         MPHY_REQUIRE(s && node_ptr && out, MPHY_ERR_INVALID_ARG, "null argument");
         MPHY_REQUIRE(n_inst > 0, MPHY_ERR_INVALID_ARG, "no instances");
+        MPHY_REQUIRE(!s->mesh->has_presc && !s->p0, MPHY_ERR_UNSUPPORTED,
+                     "the batched form takes clamped displacement elements");
         MPHY_REQUIRE(s->opts.pc_type == MPHY_PC_JACOBI && s->opts.coarse_aggregates <= 0 &&
                          s->opts.precision != MPHY_PREC_MIXED_F32VEC,
                      MPHY_ERR_UNSUPPORTED, "batched solves use Jacobi-PCG with FP64 vectors");

@@ -113,6 +113,10 @@ struct mphy_mesh {
     bool general = false;          // some material is not Neo-Hookean: dense-tangent element kernel
     mphy::DevBuf<uint8_t> fixed;   // [n_node*3]
     std::vector<uint8_t> fixed_host;
+    // prescribed displacement of every prescribed DOF at time t: t * presc_ramp + presc_const
+    // (both [n_node*3]; allocated only once nonzero values are set)
+    mphy::DevBuf<double> presc_ramp, presc_const;
+    bool has_presc = false;
     std::vector<double> coords_host;  // reference coordinates (aggregation of the coarse space)
 };
 

@@ -273,6 +273,7 @@ __global__ void __launch_bounds__(kEpb * NPE) elem_fp64_kernel(ElemArgs a) {
         store_residual<NPE, MODE>(a, e, I, node, freeI, R);
     }
     constexpr int CH = 4;
+    double rl[3] = {0.0, 0.0, 0.0};
 #pragma unroll 1
     for (int J0 = 0; J0 < NPE; J0 += CH) {
         double acc[CH][9];
@@ -318,9 +319,11 @@ __global__ void __launch_bounds__(kEpb * NPE) elem_fp64_kernel(ElemArgs a) {
         for (int j = 0; j < CH; ++j) {
             const int J = J0 + j;
             if (J >= NPE) break;
+            lift_block<NPE, MODE>(a, e, J, acc[j], rl);
             store_block<NPE, MODE>(a, e, I, J, node, freeI, acc[j]);
         }
     }
+    store_lift<NPE, MODE>(a, node, freeI, rl);
 }
 
 template <int NPE, int MODE>

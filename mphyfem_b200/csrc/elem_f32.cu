@@ -351,6 +351,33 @@ __global__ void __launch_bounds__(kE * NPE, NPE == 8 ? 2 : 1) elem_f32_kernel(El
 #pragma unroll
         for (int v = 0; v < 9; ++v) atomicAdd(&a.diag_out[9 * (int64_t)node + v], D[v]);
     }
+    // the lift of prescribed increments (applyDirichletBCs): free rows get -sum_J K_IJ lift_J, with
+    // K_II = D_I, i.e. -sum_{J != I} K_IJ (lift_J - lift_I)
+    if (live && a.lift) {
+        const double lI[3] = {a.lift[3 * (int64_t)node], a.lift[3 * (int64_t)node + 1], a.lift[3 * (int64_t)node + 2]};
+        double rl[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int J = 0; J < NPE; ++J) {
+            if (J == I) continue;
+            const int64_t nJ = a.conn[elem * NPE + J];
+            const double dl[3] = {a.lift[3 * nJ] - lI[0], a.lift[3 * nJ + 1] - lI[1], a.lift[3 * nJ + 2] - lI[2]};
+            int d = J - I;
+            if (d < 0) d += NPE;
+            const bool own = 2 * d < NPE || (2 * d == NPE && I < J);
+            const int q = 2 * d < NPE ? d - 1 : (2 * d == NPE ? MAXP - 1 : NPE - d - 1);
+#pragma unroll
+            for (int aa = 0; aa < 3; ++aa)
+#pragma unroll
+                for (int bb = 0; bb < 3; ++bb)
+                    rl[aa] += (double)(own ? s.a.blk[I][q][3 * aa + bb][e] : s.a.blk[J][q][3 * bb + aa][e]) * dl[bb];
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            if ((fixed3 >> c) & 1u) continue;
+            atomicAdd(&a.rhs[3 * (int64_t)node + c], -rl[c]);
+            if (a.reac) atomicAdd(&a.reac[3 * (int64_t)node + c], -rl[c]);
+        }
+    }
 }
 
 template <int NPE>

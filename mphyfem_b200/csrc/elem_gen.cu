@@ -219,11 +219,16 @@ __global__ void __launch_bounds__(kGenEpb * NPE * ((NPE + kGenCh - 1) / kGenCh))
             }
         }
     }
+    double rl[3] = {0.0, 0.0, 0.0};
 #pragma unroll
     for (int j = 0; j < kGenCh; ++j) {
         const int J = J0 + j;
-        if (J < NPE) store_block<NPE, MODE>(a, e, I, J, node, freeI, acc[j]);
+        if (J < NPE) {
+            lift_block<NPE, MODE>(a, e, J, acc[j], rl);
+            store_block<NPE, MODE>(a, e, I, J, node, freeI, acc[j]);
+        }
     }
+    store_lift<NPE, MODE>(a, node, freeI, rl);
 }
 
 template <int NPE, int MODE>
@@ -673,6 +678,7 @@ __global__ void __launch_bounds__(kGenEpb * NPE * ((NPE + kGenCh - 1) / kGenCh))
             }
         }
     }
+    double rl[3] = {0.0, 0.0, 0.0};
 #pragma unroll
     for (int j = 0; j < kGenCh; ++j) {
         const int J = J0 + j;
@@ -681,9 +687,11 @@ __global__ void __launch_bounds__(kGenEpb * NPE * ((NPE + kGenCh - 1) / kGenCh))
             for (int aa = 0; aa < 3; ++aa)
 #pragma unroll
                 for (int bb = 0; bb < 3; ++bb) acc[j][3 * aa + bb] -= s.kup[I][aa] * s.kup[J][bb] * rkpp;
+            lift_block<NPE, MODE>(a, e, J, acc[j], rl);
             store_block<NPE, MODE>(a, e, I, J, node, freeI, acc[j]);
         }
     }
+    store_lift<NPE, MODE>(a, node, freeI, rl);
 }
 
 template <int NPE, int MODE>

@@ -58,4 +58,30 @@ __device__ __forceinline__ void store_block(const ElemArgs& a, int64_t e, int I,
     }
 }
 
+// Lift of prescribed displacement increments, ElementBase::applyDirichletBCs
+// (ElementBase.cpp:567-594), applied in the first Newton iteration of a step
+// (femSolidmechanics2.cpp:1080-1095): the free rows of element e get -sum_J K_IJ lift_J. Block
+// (I, J) adds K_IJ lift_J to the row node's accumulator rl (K as formed, before any masking).
+template <int NPE, int MODE>
+__device__ __forceinline__ void lift_block(const ElemArgs& a, int64_t e, int J, const double acc[9], double rl[3]) {
+    if (!(MODE & 2) || !a.lift) return;
+    const int64_t nJ = a.conn[e * NPE + J];
+    const double l0 = a.lift[3 * nJ], l1 = a.lift[3 * nJ + 1], l2 = a.lift[3 * nJ + 2];
+#pragma unroll
+    for (int aa = 0; aa < 3; ++aa) rl[aa] += acc[3 * aa] * l0 + acc[3 * aa + 1] * l1 + acc[3 * aa + 2] * l2;
+}
+
+// The accumulated lift of row node I into the right-hand side and the reactions (free DOFs: the
+// reference's reaction sum takes the element vector after the lift).
+template <int NPE, int MODE>
+__device__ __forceinline__ void store_lift(const ElemArgs& a, int32_t node, const bool freeI[3], const double rl[3]) {
+    if (!(MODE & 2) || !a.lift) return;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        if (!freeI[c] || rl[c] == 0.0) continue;
+        atomicAdd(&a.rhs[3 * (int64_t)node + c], -rl[c]);
+        if (a.reac) atomicAdd(&a.reac[3 * (int64_t)node + c], -rl[c]);
+    }
+}
+
 }  // namespace mphy

@@ -1003,6 +1003,19 @@ void set_prescribed_diagonal(const SellView& A, const uint8_t* fixed, VT* val, c
 template void set_prescribed_diagonal<double>(const SellView&, const uint8_t*, double*, cudaStream_t, int);
 template void set_prescribed_diagonal<float>(const SellView&, const uint8_t*, float*, cudaStream_t, int);
 
+__global__ void prescribed_increment_kernel(const uint8_t* __restrict__ fixed, const double* __restrict__ ramp,
+                                            const double* __restrict__ cst, double t, const double* __restrict__ disp,
+                                            double* __restrict__ lift, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        lift[i] = fixed[i] ? t * ramp[i] + cst[i] - disp[i] : 0.0;
+}
+
+void prescribed_increment(const uint8_t* fixed, const double* ramp, const double* cst, double t, const double* disp,
+                          double* lift, int64_t n, cudaStream_t s, int sm) {
+    prescribed_increment_kernel<<<stride_grid(n, kThreads, sm), kThreads, 0, s>>>(fixed, ramp, cst, t, disp, lift, n);
+    MPHY_CUDA(cudaGetLastError());
+}
+
 void add_scaled_free(const uint8_t* fixed, const double* f, double scale, double* rhs, int64_t n, cudaStream_t s,
                      int sm) {
     add_scaled_free_kernel<<<stride_grid(n, kThreads, sm), kThreads, 0, s>>>(fixed, f, scale, rhs, n);

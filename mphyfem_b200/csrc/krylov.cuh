@@ -154,6 +154,9 @@ template <typename VT>
 void set_prescribed_diagonal(const SellView& A, const uint8_t* fixed, VT* val, cudaStream_t s, int sm);
 void add_scaled_free(const uint8_t* fixed, const double* f, double scale, double* rhs, int64_t n, cudaStream_t s,
                      int sm);
+// dispApplied of a load step: lift = t ramp + cst - disp on prescribed DOFs, zero on free ones
+void prescribed_increment(const uint8_t* fixed, const double* ramp, const double* cst, double t, const double* disp,
+                          double* lift, int64_t n, cudaStream_t s, int sm);
 void axpy_inplace(double* y, const double* x, double a, int64_t n, cudaStream_t s, int sm);
 template <typename VT>
 void gather_values(const VT* val, const int64_t* src, double* out, int64_t n, cudaStream_t s, int sm);

@@ -441,6 +441,8 @@ int mphy_mixed_create(mphy_ctx* c, const mphy_mesh* mesh, const mphy_pattern* pa
                       mphy_mixed** out) {
     return guarded([&] {
         MPHY_REQUIRE(c && mesh && pat && out, MPHY_ERR_INVALID_ARG, "null argument");
+        MPHY_REQUIRE(!mesh->has_presc, MPHY_ERR_UNSUPPORTED,
+                     "mixed u-p elements with nonzero prescribed displacements");
         MPHY_REQUIRE(mesh->npe == 10, MPHY_ERR_UNSUPPORTED,
                      "mixed u-p elements: tet10 displacement with linear vertex pressure (npe = 10)");
         MPHY_REQUIRE(pat->mesh == mesh, MPHY_ERR_INVALID_ARG, "the pattern belongs to another mesh");

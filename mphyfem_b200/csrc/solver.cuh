@@ -74,6 +74,7 @@ struct mphy_solver {
     // the last converged step) and the coupling terms of the last assembly
     bool p0 = false;
     DevBuf<double> pe, pe_prev, kup_e, kpp_e, fp_e;
+    DevBuf<double> lift;  // [3 n_node] prescribed increments of the current load step
 };
 
 struct mphy_gnn {
@@ -85,7 +86,7 @@ struct mphy_gnn {
 namespace mphy {
 // Zero K and R, element kernel with scatter into the SELL values (femSolidmechanics2.cpp:1047-1120).
 // bad_elem: optional per-element det F < 0 flags (zeroed by the caller).
-void solver_assemble(mphy_solver* s, const double* disp, uint8_t* bad_elem = nullptr);
+void solver_assemble(mphy_solver* s, const double* disp, uint8_t* bad_elem = nullptr, const double* lift = nullptr);
 // ||rhs|| and the first bad element (-1 if none), one synchronisation.
 double solver_norm_and_bad(mphy_solver* s, int64_t* first_bad);
 // disp += solution, and for the constant-pressure element the element pressures' update

@@ -57,6 +57,9 @@ class Problem:
     meta: dict = field(default_factory=dict)
     mat_model: np.ndarray | None = None  # [n_mat] int32 hyperelastic model per material (None: Neo-Hookean)
     mat_data: np.ndarray | None = None  # [n_mat, 4] float64 model parameters (mu; c1 c2; mu Im; mu N)
+    # prescribed displacement of every prescribed DOF at time t: t * presc_ramp + presc_const
+    presc_ramp: np.ndarray | None = None  # [n_node*3] float64
+    presc_const: np.ndarray | None = None  # [n_node*3] float64
 
     @property
     def n_node(self) -> int:

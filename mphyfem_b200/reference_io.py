@@ -413,20 +413,6 @@ def read_config(config_path, mesh_path=None):
     mat_id = np.array([row_of[tag_mat[tag]] for _, tag, _ in vol], dtype=np.int32)
     coords = m["nodes"]
     n_node = len(coords)
-    # prescribed DOFs
-    fixed = np.zeros((n_node, 3), dtype=np.uint8)
-    for label, kv in bcs:
-        if label not in m["faces"]:
-            raise ValueError(f"config: boundary condition on unknown patch {label!r}")
-        nodes = sorted({v for fc in m["faces"][label] for v in fc})
-        if kv.get("type") == "fixed":
-            fixed[nodes, :] = 1
-        elif kv.get("type") == "specified":
-            if float(kv.get("value", "0")) != 0.0:
-                raise NotImplementedError("config: nonzero prescribed displacements are not supported by this build")
-            fixed[nodes, DOF_NAMES[kv["dof"].strip().lower()]] = 1
-        else:
-            raise ValueError(f"config: patch type {kv.get('type')!r} (femSolidmechanics::setBoundaryConditions)")
     # loads at unit time, with lam(t) = slope t checked on the steps
     dt, tfin = solver["timeStep"], solver["finalTime"]
     ts = [dt * k for k in range(1, int(round(tfin / dt)) + 1)] or [dt]
@@ -441,6 +427,29 @@ def read_config(config_path, mesh_path=None):
                 raise NotImplementedError("config: the load factor must be proportional to time (lam = c t)")
         return c
 
+    # prescribed DOFs and their values
+    fixed = np.zeros((n_node, 3), dtype=np.uint8)
+    presc_ramp, presc_const = np.zeros((n_node, 3)), np.zeros((n_node, 3))
+    for label, kv in bcs:
+        if label not in m["faces"]:
+            raise ValueError(f"config: boundary condition on unknown patch {label!r}")
+        nodes = sorted({v for fc in m["faces"][label] for v in fc})
+        if kv.get("type") == "fixed":
+            fixed[nodes, :] = 1
+        elif kv.get("type") == "specified":
+            # value(t) = value * lam(t) with the entry's time function, or value from the first
+            # step without one (femSolidmechanics1.cpp:840-868); constants only (no expressions)
+            dof = DOF_NAMES[kv["dof"].strip().lower()]
+            fixed[nodes, dof] = 1
+            value = float(kv.get("value", "0"))
+            if value != 0.0:
+                tfn = int(kv.get("timefunction", "0")) - 1
+                if tfn >= 0:
+                    presc_ramp[nodes, dof] = slope_of(tfn) * value
+                else:
+                    presc_const[nodes, dof] = value
+        else:
+            raise ValueError(f"config: patch type {kv.get('type')!r} (femSolidmechanics::setBoundaryConditions)")
     F = np.zeros((n_node, 3))
     for label, kv in tractions.items():
         if kv.get("type") != "traction":
@@ -464,6 +473,8 @@ def read_config(config_path, mesh_path=None):
                    dt=dt, t_final=tfin, max_steps=solver["maximumSteps"],
                    meta={"tolerance": solver["tolerance"], "maximumIterations": solver["maximumIterations"],
                          "domains": m["domains"], "patches": list(m["patches"]), "element": etype})
+    if presc_ramp.any() or presc_const.any():
+        prob.presc_ramp, prob.presc_const = presc_ramp.ravel(), presc_const.ravel()
     if any(models):
         prob.mat_model = np.array(models, dtype=np.int32)
         prob.mat_data = np.array(mdata, dtype=np.float64)

@@ -64,6 +64,7 @@ def lib():
         L.orc_elem_mixed0.argtypes = [C.c_int, _d, _d, _d, C.c_double, C.c_int, _d, C.c_double, C.c_int, _d, _d,
                                       _d, _d, _d]
         L.orc_problem_set_mixed_p0.argtypes = [C.c_void_p, C.c_int]
+        L.orc_problem_set_prescribed.argtypes = [C.c_void_p, _d, _d]
         L.orc_problem_p0_pressure.argtypes = [C.c_void_p, _d, _d]
         L.orc_problem_p0_pressure.restype = None
         L.orc_problem_save_step.argtypes = [C.c_void_p, _d]
@@ -218,6 +219,12 @@ class OracleProblem:
                 raise ValueError("oracle: invalid material models")
         self.n_free = lib().orc_problem_nfree(self.h)
         self.nnz = lib().orc_problem_nnz(self.h)
+        ramp, cst = getattr(prob, "presc_ramp", None), getattr(prob, "presc_const", None)
+        if ramp is not None or cst is not None:
+            r = None if ramp is None else np.ascontiguousarray(ramp, np.float64)
+            c = None if cst is None else np.ascontiguousarray(cst, np.float64)
+            self._keep += [r, c]
+            lib().orc_problem_set_prescribed(self.h, _p(r, _d), _p(c, _d))
 
     def __del__(self):
         if getattr(self, "h", None) and _lib is not None:

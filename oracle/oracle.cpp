@@ -184,6 +184,8 @@ struct orc_problem {
     // element evaluation (for solveForPressure)
     bool p0 = false;
     mutable std::vector<double> pe, pe_prev, disp_prev, kup, kpp, fp;
+    // prescribed displacements t * presc_ramp + presc_const (empty: all prescribed values zero)
+    std::vector<double> presc_ramp, presc_const;
 };
 
 extern "C" {
@@ -744,8 +746,11 @@ int64_t orc_problem_elements_mixed(const orc_problem* p, const double* disp, con
     return first_bad == p->n_elem ? -1 : first_bad;
 }
 
-int64_t orc_problem_assemble(const orc_problem* p, const double* disp, double* val, double* rhs,
-                             double* reac, int nthreads) {
+// femSolidmechanics::calcStiffnessAndResidual (femSolidmechanics2.cpp:1047-1120); lift (may be
+// null): the prescribed increments dispApplied, lifted by ElementBase::applyDirichletBCs
+// (ElementBase.cpp:567-594) into the free rows of every element before its scatter.
+static int64_t assemble_impl(const orc_problem* p, const double* disp, double* val, double* rhs, double* reac,
+                             int nthreads, const double* lift) {
     const CsrPattern& P = p->pat;
     const int ns = 3 * p->npe;
     if (val) std::fill(val, val + P.rowptr.back(), 0.0);
@@ -763,6 +768,14 @@ int64_t orc_problem_assemble(const orc_problem* p, const double* disp, double* v
             elem_eval(p, e, disp, K.data(), R.data(), &bad);
             if (bad && e < first_bad) first_bad = e;
             const int32_t* fa = &P.for_assy[e * ns];
+            if (lift) {
+                for (int ii = 0; ii < ns; ++ii) {
+                    if (fa[ii] != -1) continue;  // a prescribed DOF: its increment lifts the free rows
+                    const double fact = lift[3 * (size_t)p->conn[e * p->npe + ii / 3] + ii % 3];
+                    for (int jj = 0; jj < ns; ++jj)
+                        if (fa[jj] != -1) R[jj] -= K[jj * ns + ii] * fact;
+                }
+            }
             const int64_t* sl = &p->slot[e * ns * ns];
             for (int i = 0; i < ns; ++i) {
                 if (fa[i] == -1) continue;
@@ -802,6 +815,29 @@ int64_t orc_problem_assemble(const orc_problem* p, const double* disp, double* v
         }
     }
     return first_bad == p->n_elem ? -1 : first_bad;
+}
+
+int64_t orc_problem_assemble(const orc_problem* p, const double* disp, double* val, double* rhs, double* reac,
+                             int nthreads) {
+    return assemble_impl(p, disp, val, rhs, reac, nthreads, nullptr);
+}
+
+int orc_problem_set_prescribed(orc_problem* p, const double* ramp, const double* cst) {
+    const size_t nd = 3 * (size_t)p->n_node;
+    p->presc_ramp.assign(nd, 0.0);
+    p->presc_const.assign(nd, 0.0);
+    bool any = false;
+    for (size_t i = 0; i < nd; ++i) {
+        if (!p->fixed[i]) continue;
+        p->presc_ramp[i] = ramp ? ramp[i] : 0.0;
+        p->presc_const[i] = cst ? cst[i] : 0.0;
+        any |= p->presc_ramp[i] != 0.0 || p->presc_const[i] != 0.0;
+    }
+    if (!any) {
+        p->presc_ramp.clear();
+        p->presc_const.clear();
+    }
+    return 0;
 }
 
 // KSPCG (Hestenes-Stiefel) with PCJACOBI, restated from PETSc's documented algorithm as the
@@ -900,10 +936,19 @@ int orc_newton_run(const orc_problem* p, const double* fnodal, const orc_newton_
         const double lambda = t;
         std::copy(disp, disp + nd, disp_prev.begin());
         if (p->p0) orc_problem_save_step(p, disp);
+        // setBoundaryConditions (femSolidmechanics1.cpp:813-891): dispApplied = value(t) - disp
+        const bool presc = !p->presc_ramp.empty();
+        std::vector<double> lift;
+        if (presc) {
+            lift.assign(nd, 0.0);
+            for (size_t i = 0; i < nd; ++i)
+                if (p->fixed[i]) lift[i] = t * p->presc_ramp[i] + p->presc_const[i] - disp[i];
+        }
         bool converged = false;
         double norm = -1.0, norm_prev = -1.0, tol = o->tol_abs;
         for (int iter = 1; iter <= o->max_newton; ++iter) {
-            const int64_t bad = orc_problem_assemble(p, disp, val.data(), rhs.data(), nullptr, o->nthreads);
+            const int64_t bad = assemble_impl(p, disp, val.data(), rhs.data(), nullptr, o->nthreads,
+                                              presc && iter == 1 ? lift.data() : nullptr);
             if (bad >= 0) break;  // "Negative Jacobian encountered": the iteration loop ends
             for (int i = 0; i < n; ++i) rhs[i] += lambda * fnodal[P.assy_for_soln[i]];
             norm_prev = norm;
@@ -923,6 +968,9 @@ int orc_newton_run(const orc_problem* p, const double* fnodal, const orc_newton_
                 orc_cg_jacobi(p, val.data(), rhs.data(), dx.data(), o->cg_rtol, 1.0e-50, o->cg_maxit,
                               o->nthreads, &its, &fn);
                 for (int i = 0; i < n; ++i) disp[P.assy_for_soln[i]] += dx[i];
+                // dispIncr[prescribed] += dispApplied in the first iteration (femSolidmechanics2.cpp:1137-1145)
+                if (presc && iter == 1)
+                    for (size_t i = 0; i < nd; ++i) disp[i] += lift[i];
                 if (p->p0) {
                     std::vector<double> du(nd, 0.0);
                     for (int i = 0; i < n; ++i) du[P.assy_for_soln[i]] = dx[i];

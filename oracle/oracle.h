@@ -129,6 +129,11 @@ void orc_problem_destroy(orc_problem* p);
  * mats[3k]. Returns 0, 1 when n_mat differs from the problem's, 2 for an unknown model. */
 int orc_problem_set_materials(orc_problem* p, int n_mat, const int32_t* model, const double* data);
 int orc_problem_nfree(const orc_problem* p);
+/* Nonzero prescribed displacements: the DOFs flagged in `fixed` take t * ramp[i] + cst[i] at time t
+ * (either array may be NULL: zero). The Newton run lifts each step's increment (value(t) - disp)
+ * into the free rows of the first iteration (ElementBase::applyDirichletBCs, ElementBase.cpp:567-594)
+ * and adds it to the displacement with that iteration's solution (femSolidmechanics2.cpp:1137-1145). */
+int orc_problem_set_prescribed(orc_problem* p, const double* ramp, const double* cst);
 /* Elem_Solid_3D_Mixed0 for every element (enable = 1; 0 = the displacement element): assembly,
  * elements and Newton use the condensed element; the Newton run updates the element pressures
  * after every solve (femSolidmechanics2.cpp:1204-1212), saves them with each converged step and

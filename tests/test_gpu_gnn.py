@@ -93,6 +93,36 @@ def test_learned_beats_jacobi(env, trained, precision, rtol):
         assert np.linalg.norm(xs["learned"] - xs["jacobi"]) <= 1e-7 * np.linalg.norm(xs["jacobi"])
 
 
+@pytest.mark.parametrize("coarse", [0, 16], ids=["local", "with_coarse"])
+def test_learned_against_the_fsai_baselines(env, trained, coarse):
+    """What the trained network gains, on the held-out layout, against the preconditioners it sits
+    between: block-Jacobi FSAI (the network with zero weights, its starting point) and exact FSAI
+    (the minimiser of the Kaporin functional it is trained on), alone and with the rigid-body
+    coarse space. Every solve reaches the same FP64 true residual."""
+    torch, api, _lib, learned, ctx = env
+    gnn, _ = trained
+    zero = learned.Gnn(ctx, np.zeros(learned.param_count(), np.float32))
+    q = meshgen.two_phase_inclusions(24, 6, 6, seed=999, r_range=(1.5 / 6, 3.0 / 6 * 0.9))
+    its = {}
+    for name, pc, net in (("jacobi", _lib.PC_JACOBI, None), ("block_jacobi_fsai", _lib.PC_FSAI_LEARNED, zero),
+                          ("learned", _lib.PC_FSAI_LEARNED, gnn), ("exact_fsai", _lib.PC_FSAI, None)):
+        mesh = api.Mesh(ctx, q)
+        sol = api.SolverGpu(mesh, api.Pattern(mesh), pc_type=pc, precision=0, rtol=1e-10, norm_type=1,
+                            coarse_aggregates=coarse)
+        if net is not None:
+            net.attach(sol)
+        sol.calcStiffnessAndResidual(torch.zeros(q.n_dof, dtype=torch.float64, device="cuda"))
+        sol.addExternalForces(torch.tensor(q.fnodal, device="cuda"), 0.2)
+        rc, its[name], _ = sol.factoriseAndSolve()
+        assert rc == 0
+        if net is not None:
+            assert not sol.pc_last()["fallback"], name
+        assert sol.true_residual() <= 100 * 1e-10
+    assert its["learned"] < its["block_jacobi_fsai"], its
+    assert its["exact_fsai"] < its["block_jacobi_fsai"], its
+    assert its["block_jacobi_fsai"] <= its["jacobi"], its
+
+
 def test_untrained_network_is_block_jacobi(env):
     """Zero weights: the prediction is block-Jacobi FSAI, the exact block FSAI on the diagonal
     pattern (G_nn = L^T, L L^T = A_nn^-1), so G A G^T has identity diagonal blocks."""

@@ -139,8 +139,12 @@ def test_config_reader_rules(tmp_path):
     with pytest.raises(NotImplementedError):
         rio.read_config(tmp_path / "config")                     # constant load: not lam = c t
     (tmp_path / "config").write_text(CONFIG.replace("value  :  0.0", "value  :  0.1"))
-    with pytest.raises(NotImplementedError):
-        rio.read_config(tmp_path / "config")                     # nonzero prescribed value
+    q = rio.read_config(tmp_path / "config")                     # a nonzero value without a time
+    assert np.all(q.presc_const.reshape(-1, 3)[clamped, 0] == 0.1)  # function: applied from the start
+    assert not q.presc_ramp.any()
+    (tmp_path / "config").write_text(CONFIG.replace("value  :  0.0", "value  :  0.1\n    timefunction : 1"))
+    q = rio.read_config(tmp_path / "config")                     # with lam = 2 t: ramped
+    assert np.all(q.presc_ramp.reshape(-1, 3)[clamped, 0] == 0.2) and not q.presc_const.any()
     (tmp_path / "config").write_text(CONFIG.replace("Matl_NeoHookean", "Matl_LinearElastic"))
     with pytest.raises(NotImplementedError):
         rio.read_config(tmp_path / "config")
