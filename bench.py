@@ -318,12 +318,14 @@ def _time_leg(torch, api, _lib, mesh, pat, args, prob, disp, fext, dev, method, 
     return out
 
 
-def _parity_first_step(api, _lib, mesh, pat, args, prob, legs, newton_rtol=1e-8):
+def _parity_first_step(api, _lib, mesh, pat, args, prob, legs, newton_rtol=1e-8, max_newton=15):
     """Accuracy at the workload's size: the first load step (lambda = dt from u = 0) converged to
     ||R|| < newton_rtol ||R_first|| with the consistent tangent (the reference's tangent need not
     converge quadratically, or at all, at this load), by the plain FP64 GPU method (FP64 element
     kernel, FP64 matrix, FP64 Jacobi-PCG: the FP64 solution) and by each method of `legs`.
-    Reports every method's Newton history and max|u - u64| / max|u64|."""
+    Reports every method's Newton history and max|u - u64| / max|u64|. max_newton leaves room
+    for the FP32 tangent's slower final Newton iterations (its Jacobian is accurate to about
+    1e-7), which the histories show."""
     def run(method):
         precision, pc, coarse = method
         a = argparse.Namespace(**dict(vars(args), precision=precision, pc=pc, coarse=coarse))
@@ -337,7 +339,7 @@ def _parity_first_step(api, _lib, mesh, pat, args, prob, legs, newton_rtol=1e-8)
         if pc == "learned":
             _GNN[0].attach(s)
         t0 = time.perf_counter()
-        r = api.newton_run(s, prob, max_newton=10, tol_rel=newton_rtol, t_final=prob.dt, max_steps=1)
+        r = api.newton_run(s, prob, max_newton=max_newton, tol_rel=newton_rtol, t_final=prob.dt, max_steps=1)
         wall = time.perf_counter() - t0
         s.close()
         hist = [{"iter": int(h[1]), "rhs_norm": float(h[2]), "krylov_its": int(h[3]),
@@ -354,7 +356,8 @@ def _parity_first_step(api, _lib, mesh, pat, args, prob, legs, newton_rtol=1e-8)
 
     u64, ref = run(("fp64", "jacobi", 0))
     out = {"case": f"first load step (lambda={prob.dt:g}) from u=0 to ||R|| < {newton_rtol:g} ||R_first||, "
-                   f"consistent tangent, Krylov to true relative residual {args.rtol:g}",
+                   f"consistent tangent, Krylov to true relative residual {args.rtol:g}, at most {max_newton} "
+                   f"Newton iterations",
            "fp64": ref}
     scale = float(np.abs(u64).max())
     for name, m in legs.items():

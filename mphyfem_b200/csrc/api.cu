@@ -92,6 +92,7 @@ void solver_assemble(mphy_solver* s, const double* disp, uint8_t* bad_elem, cons
         // FP32 tangent blocks; the element kernel also sums the element diagonal blocks that the
         // preconditioners read (the operator forms its own diagonal from the stored rows)
         a.diag_out = s->diag64.p;
+        a.diag_full = s->opts.pc_type != MPHY_PC_JACOBI;  // FSAI and the network read whole blocks
         launch_elem_f32(a, s->mesh->npe, s->ctx->stream);
     } else launch_elem_fp64(a, s->mesh->npe, 2, s->ctx->stream);
     s->launches += 1;

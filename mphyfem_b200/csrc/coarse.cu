@@ -386,105 +386,61 @@ __device__ __forceinline__ void store_tile(const double (*S)[TP], double* M, int
 
 // Factor the diagonal tile (j, j) in place (lower triangle; upper zeroed), and write its inverse
 // W_jj = L_jj^{-1} to W: the panel below becomes a tile product with W_jj (gemm_panel_tiles) and
-// the triangular inverse reuses W_jj. The tile lives in registers: thread (ty, tx) of 16 x 16
-// holds rows ty + 16a and columns tx + 16b (a, b < 4). Cholesky step c: the holders of column c
-// put it in shared memory, every thread forms L(:, c) = column / sqrt(pivot) for its rows and
-// columns and applies the rank-1 update to its 16 entries. Inverse, row r of X = L^{-1}:
-// X(r, :) = (e_r - acc(r, :)) / L(r, r), written by the holders of row r with column r of L,
-// then acc(i, :) += L(i, r) X(r, :) for i > r. The shared vectors are double-buffered, so each
-// step needs one barrier.
-__global__ void __launch_bounds__(256) potrf_inv_tile(double* E, double* W, int kp, int j, int32_t* err) {
+// the triangular inverse reuses W_jj. Two warps; thread t holds row t of the tile in registers.
+// Cholesky step c: every row t >= c publishes its entry of column c, then each thread forms
+// L(t, c) = A(t, c) / sqrt(A(c, c)) and applies the rank-1 update to its row (columns c < k <= t);
+// the published column is double-buffered, so each step needs one barrier. Inverse: L goes to
+// shared memory once; thread t solves L x = e_t by forward substitution (column t of L^{-1}) with
+// no further barriers.
+__global__ void __launch_bounds__(T) potrf_inv_tile(double* E, double* W, int kp, int j, int32_t* err) {
     __shared__ double colv[2][T];
-    __shared__ double rowv[2][T];
-    __shared__ double diag[T];
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;  // blockDim.x == 256
-    double S[4][4];
+    __shared__ double Ls[T][TP];
+    const int t = threadIdx.x;  // blockDim.x == T
     const double* Et = E + (int64_t)(j * T) * kp + j * T;
+    double a[T];
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+    for (int k = 0; k < T; ++k) a[k] = Et[(int64_t)t * kp + k];
 #pragma unroll
-        for (int b = 0; b < 4; ++b) S[a][b] = Et[(int64_t)(ty + 16 * a) * kp + tx + 16 * b];
     for (int c = 0; c < T; ++c) {
-        const int buf = c & 1, bc = c >> 4;
-        if (tx == (c & 15)) {
-#pragma unroll
-            for (int a = 0; a < 4; ++a)
-#pragma unroll
-                for (int b = 0; b < 4; ++b)
-                    if (b == bc) colv[buf][ty + 16 * a] = S[a][b];
-        }
+        const int buf = c & 1;
+        if (t >= c) colv[buf][t] = a[c];
         __syncthreads();
         double p = colv[buf][c];
         if (!(p > 0.0)) {
-            if (threadIdx.x == 0) atomicExch(err, 2);
+            if (t == 0) atomicExch(err, 2);
             p = 1e-300;
         }
         const double l = sqrt(p), il = 1.0 / l;
-        if (threadIdx.x == 0) diag[c] = l;
-        double li[4], lj[4];
+        if (t > c) {
+            const double ltc = a[c] * il;
 #pragma unroll
-        for (int a = 0; a < 4; ++a) li[a] = ty + 16 * a > c ? colv[buf][ty + 16 * a] * il : 0.0;
-#pragma unroll
-        for (int b = 0; b < 4; ++b) lj[b] = tx + 16 * b > c ? colv[buf][tx + 16 * b] * il : 0.0;
-#pragma unroll
-        for (int a = 0; a < 4; ++a)
-#pragma unroll
-            for (int b = 0; b < 4; ++b) {
-                S[a][b] -= li[a] * lj[b];
-                if (tx + 16 * b == c) S[a][b] = ty + 16 * a == c ? l : li[a];
-            }
+            for (int k = c + 1; k < T; ++k)
+                if (k <= t) a[k] -= ltc * (colv[buf][k] * il);
+            a[c] = ltc;
+        } else if (t == c) {
+            a[c] = l;
+        }
     }
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b)
-            if (tx + 16 * b > ty + 16 * a) S[a][b] = 0.0;
     double* Eo = E + (int64_t)(j * T) * kp + j * T;
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+    for (int k = 0; k < T; ++k) {
+        const double v = k <= t ? a[k] : 0.0;
+        Ls[t][k] = v;
+        Eo[(int64_t)t * kp + k] = v;
+    }
+    __syncthreads();
+    // column t of X = L^{-1}: x_i = 0 (i < t), x_t = 1 / L_tt, x_i = -sum_{t <= m < i} L_im x_m / L_ii
+    double x[T];
 #pragma unroll
-        for (int b = 0; b < 4; ++b) Eo[(int64_t)(ty + 16 * a) * kp + tx + 16 * b] = S[a][b];
-    __syncthreads();  // diag complete
-    double X[4][4];
+    for (int i = 0; i < T; ++i) {
+        double acc = i == t ? 1.0 : 0.0;
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b) X[a][b] = 0.0;
-    for (int r = 0; r < T; ++r) {
-        const int buf = r & 1, br = r >> 4;
-        const double idg = 1.0 / diag[r];
-        if (ty == (r & 15)) {
-#pragma unroll
-            for (int a = 0; a < 4; ++a)
-                if (a == br)
-#pragma unroll
-                    for (int b = 0; b < 4; ++b) {
-                        const int jc = tx + 16 * b;
-                        const double x = jc <= r ? ((jc == r ? 1.0 : 0.0) - X[a][b]) * idg : 0.0;
-                        X[a][b] = x;
-                        rowv[buf][jc] = x;
-                    }
-        }
-        if (tx == (r & 15)) {
-#pragma unroll
-            for (int a = 0; a < 4; ++a)
-#pragma unroll
-                for (int b = 0; b < 4; ++b)
-                    if (b == br) colv[buf][ty + 16 * a] = S[a][b];
-        }
-        __syncthreads();
-#pragma unroll
-        for (int a = 0; a < 4; ++a) {
-            const double lir = ty + 16 * a > r ? colv[buf][ty + 16 * a] : 0.0;
-#pragma unroll
-            for (int b = 0; b < 4; ++b) X[a][b] += lir * rowv[buf][tx + 16 * b];
-        }
+        for (int m = 0; m < i; ++m) acc -= Ls[i][m] * x[m];
+        x[i] = i >= t ? acc / Ls[i][i] : 0.0;
     }
     double* Wo = W + (int64_t)(j * T) * kp + j * T;
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b) Wo[(int64_t)(ty + 16 * a) * kp + tx + 16 * b] = X[a][b];
+    for (int i = 0; i < T; ++i) Wo[(int64_t)i * kp + t] = x[i];
 }
 
 // C (tile ci, cj of M) += alpha * sum_t A[r][t] * B[c][t]  with A, B 64x64 tiles in shared memory
@@ -763,7 +719,7 @@ void CoarseSpace::record_factorisation(cudaStream_t s, int nb, size_t sm2) {
     drop_null_modes<<<1, 1024, 0, s>>>(E_.p, kp_, nm_ * n_agg_);
     launches += 1;
     for (int j = 0; j < nb; ++j) {
-        potrf_inv_tile<<<1, 256, 0, s>>>(E_.p, W_.p, kp_, j, err_.p);
+        potrf_inv_tile<<<1, T, 0, s>>>(E_.p, W_.p, kp_, j, err_.p);
         const int m = nb - j - 1;
         if (m > 0) {
             gemm_panel_tiles<<<m, 256, sm2, s>>>(E_.p, W_.p, kp_, j);

@@ -28,6 +28,7 @@ struct ElemArgs {
     double* reac;  // [n_node*3] or null
     double* diag_out = nullptr;  // FP32 storage: [n_node][9] FP64 diagonal blocks accumulated per
                                  // element (elem_f32.cu), for the preconditioners
+    int diag_full = 1;           // 0: only the blocks' diagonal entries (all that Jacobi reads)
     const double* lift = nullptr;  // [n_node*3] increments of prescribed displacements (zero on
                                    // free DOFs): free rows get -K lift (applyDirichletBCs)
 };

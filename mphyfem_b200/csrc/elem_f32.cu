@@ -20,10 +20,11 @@
 //            d = 1 .. npe/2, the d = npe/2 pairs owned by the smaller node). K is symmetric
 //            (K_JI = K_IJ^T), so every pair is formed once and scattered twice.
 //   phase 4  thread (element, node I): the element's diagonal block D_I = -sum_{J != I} K_IJ in
-//            FP64, added to the solver's FP64 diagonal blocks. Those serve the preconditioners
-//            (Jacobi, FSAI, the network's features); the operator itself recomputes each row's
-//            diagonal from its stored blocks, so the stored FP32 operator still maps rigid
-//            translations exactly to zero.
+//            FP64, added to the solver's FP64 diagonal blocks (only their diagonal entries when
+//            Jacobi is the local preconditioner). Those serve the preconditioners (Jacobi, FSAI,
+//            the network's features); the operator itself recomputes each row's diagonal from its
+//            stored blocks, so the stored FP32 operator still maps rigid translations exactly to
+//            zero.
 #include <cuda_pipeline.h>
 
 #include "common.cuh"
@@ -349,7 +350,8 @@ __global__ void __launch_bounds__(kE * NPE, NPE == 8 ? 2 : 1) elem_f32_kernel(El
             }
         }
 #pragma unroll
-        for (int v = 0; v < 9; ++v) atomicAdd(&a.diag_out[9 * (int64_t)node + v], D[v]);
+        for (int v = 0; v < 9; ++v)
+            if (a.diag_full || v % 4 == 0) atomicAdd(&a.diag_out[9 * (int64_t)node + v], D[v]);
     }
     // the lift of prescribed increments (applyDirichletBCs): free rows get -sum_J K_IJ lift_J, with
     // K_II = D_I, i.e. -sum_{J != I} K_IJ (lift_J - lift_I)

@@ -3,8 +3,9 @@ pressure per element, condensed) on the GPU against the oracle's restatement.
 
 Tolerances: the condensed system assembled at a probe state (displacement, last-step displacement,
 element pressures) within 1e-12 of the largest entry (FP64), and a near-incompressible Newton run
-(kappa/mu = 1e3, consistent tangent, two load steps) with the oracle's residual history (1e-6
-relative above round-off), displacements and element pressures within 1e-8.
+(kappa/mu = 1e3, consistent tangent, two load steps, Newton to 1e-8: the FP64 residual floor lies
+near 1e-10 of the first residual) with the oracle's residual history (1e-6 relative above
+round-off), displacements and element pressures within 1e-8.
 """
 import numpy as np
 import pytest
@@ -69,14 +70,15 @@ def test_newton_matches_oracle(env, oracle, kind):
     p = _mesh(kind)
     p.max_steps, p.t_final = 2, 2 * p.dt
     fem = api.FemSolidmechanicsGpu(p, ctx, mixed_p0=True, tangent=1, rtol=1e-12, max_it=50000)
-    res = fem.solveWithNewtonRaphson(max_newton=15, tol_rel=1e-10)
+    # Newton to 1e-8: kappa/mu = 1e3 puts the FP64 residual floor near 1e-10 of ||R_0||
+    res = fem.solveWithNewtonRaphson(max_newton=15, tol_rel=1e-8)
     assert res.status == 0
     pe = fem.solver.p0_pressure()
     oracle.set_consistent_tangent(True)
     try:
         op = oracle.OracleProblem(p)
         op.set_mixed_p0(True)
-        uo, ho = op.newton(tol_rel=1e-10, cg_rtol=1e-12, cg_maxit=50000, max_newton=15, nthreads=4)
+        uo, ho = op.newton(tol_rel=1e-8, cg_rtol=1e-12, cg_maxit=50000, max_newton=15, nthreads=4)
         peo = op.p0_pressure()
     finally:
         oracle.set_consistent_tangent(False)
