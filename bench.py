@@ -430,12 +430,21 @@ def run_ours(args):
     torch.cuda.synchronize()
     spmv_ms = e0.elapsed_time(e1) / nrep
     vbytes = mi["value_bytes"] // (9 * mi["stored_blocks"])  # 8 (FP64) or 4 (FP32) per value
-    spmv_bytes = mi["true_blocks"] * (9 * vbytes + 4) + 2 * prob.n_dof * 8
-    if vbytes == 4:  # FP64 diagonal blocks and the prescribed-DOF mask of the FP32 storage
-        spmv_bytes += prob.n_node * (72 + 3)
+    if vbytes == 8:
+        spmv_bytes = mi["true_blocks"] * (9 * 8 + 4) + 2 * prob.n_dof * 8
+    else:
+        # the FP32 storage holds the off-diagonal blocks only (each row's diagonal block is formed
+        # from them in the kernel), plus the prescribed-DOF mask
+        spmv_bytes = (mi["true_blocks"] - prob.n_node) * (9 * 4 + 4) + 2 * prob.n_dof * 8 + prob.n_node * 3
     peak, peak_kind = _peaks()
     achieved = spmv_bytes / (spmv_ms * 1e-3) / 1e9
-    asm_bytes = pat.nnz * (8 if vbytes == 8 else 4) + prob.n_free * 8 + prob.n_node * 48 + prob.n_elem * 36
+    # assembly: each matrix value written once (FP32: off-diagonal blocks plus the FP64 Jacobi
+    # diagonal), the residual, coordinates and displacements read, the connectivity read
+    if vbytes == 8:
+        mat_bytes = pat.nnz * 8
+    else:
+        mat_bytes = (pat.nnz - 9 * prob.n_node) * 4 + prob.n_dof * 8
+    asm_bytes = mat_bytes + prob.n_free * 8 + prob.n_node * 48 + prob.n_elem * 36
 
     # end to end through the C ABI with host buffers (H2D of u and f_ext, D2H of u every step)
     disp_h = torch.zeros(prob.n_dof, dtype=torch.float64).pin_memory().numpy()

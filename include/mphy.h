@@ -102,6 +102,11 @@ typedef struct mphy_solver_opts {
                             * (linear displacement u = a + B (x - x_c): translations, stretches,
                             * shears and rotations; a richer space of the same size at half the
                             * aggregates) */
+    int32_t coarse_lag;    /* > 0: the coarse operator (Z^T A Z)^{-1} formed by a solve is kept for
+                            * up to this many further solves instead of being rebuilt from each
+                            * new matrix; mphy_newton_run rebuilds it at the first iteration of
+                            * every load step. The preconditioner lags, the convergence test does
+                            * not. 0 (default): rebuilt for every new matrix, as PCSetUp is. */
 } mphy_solver_opts;
 
 typedef struct mphy_newton_opts {
@@ -319,7 +324,8 @@ int mphy_solver_attach_gnn(mphy_solver* s, mphy_gnn* g);
 int mphy_solver_pc_last(const mphy_solver* s, int32_t* fallback, float* setup_ms, int32_t* first_status,
                         int32_t* first_its, double* first_relres);
 /* Coarse space of the two-level correction: aggregate grid (boxes along x, y, z of the reference
- * bounding box) and coarse size (6 modes per box). *setup_ms: time of the last E setup.
+ * bounding box) and coarse size (6 modes per box). *setup_ms: time of the E setup done by the
+ * last solve (0 when it kept an earlier operator under coarse_lag).
  * No counterpart in the reference. */
 int mphy_solver_coarse_info(const mphy_solver* s, int32_t* grid3, int32_t* coarse_size, float* setup_ms);
 /* ||b - A x|| / ||b|| in FP64 for the last solve (A as stored: FP64, or the FP32 storage). */

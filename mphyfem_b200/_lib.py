@@ -44,7 +44,7 @@ class SolverOpts(C.Structure):
         ("precision", C.c_int32), ("pc_type", C.c_int32), ("tangent", C.c_int32), ("max_it", C.c_int32),
         ("rtol", C.c_double), ("abstol", C.c_double), ("dtol", C.c_double), ("inner_rtol", C.c_double),
         ("max_outer", C.c_int32), ("chunk", C.c_int32), ("coarse_aggregates", C.c_int32), ("norm_type", C.c_int32),
-        ("coarse_modes", C.c_int32),
+        ("coarse_modes", C.c_int32), ("coarse_lag", C.c_int32),
     ]
 
 

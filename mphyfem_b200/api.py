@@ -350,7 +350,9 @@ def calc_stiffness_and_residual(mesh: Mesh, disp_dev, tangent: int = L.TANGENT_R
 @dataclass
 class NewtonResult:
     disp: np.ndarray
-    hist: np.ndarray  # rows (step, iter, ||R||, krylov its, krylov status, t_assembly_ms, t_solve_ms)
+    # rows (step, iter, ||R||, krylov its, krylov status, t_assembly_ms, t_solve_ms), and for the
+    # displacement solver (newton_run) an eighth column: the library kernels the iteration launched
+    hist: np.ndarray
     status: int
 
 
@@ -370,8 +372,8 @@ def newton_run(solver: "SolverGpu", prob, max_newton: int = 10, tol_rel: float |
     rc = solver.lib.mphy_newton_run(solver.h, f.ctypes.data_as(L._d), C.byref(o), u.ctypes.data_as(L._d),
                                     hist, max_hist, C.byref(n))
     L.check(rc, allow=(L.ERR_TIME_STEP,))
-    rows = np.array([[h.step, h.iter, h.rhs_norm, h.krylov_its, h.status, h.t_assembly_ms, h.t_solve_ms]
-                     for h in hist[:n.value]], dtype=np.float64).reshape(-1, 7)
+    rows = np.array([[h.step, h.iter, h.rhs_norm, h.krylov_its, h.status, h.t_assembly_ms, h.t_solve_ms,
+                      h.kernel_launches] for h in hist[:n.value]], dtype=np.float64).reshape(-1, 8)
     return NewtonResult(disp=u, hist=rows, status=rc)
 
 

@@ -197,10 +197,18 @@ int solver_solve_once(mphy_solver* s, int32_t* its, double* fnorm) {
         s->t_pc_ms = ms;
     }
     if (setup && s->use_coarse) {
-        // the coarse operator follows the assembled matrix
-        if (s->mixed) s->coarse.setup<float>(s->A, s->valf.p, nullptr, s->ctx->stream);
-        else s->coarse.setup<double>(s->A, s->val.p, nullptr, s->ctx->stream);
-        s->launches += s->coarse.launches;
+        // the coarse operator follows the assembled matrix, unless a lag is asked for and the
+        // kept one is young enough
+        if (s->coarse_ready && s->opts.coarse_lag > 0 && s->coarse_age < s->opts.coarse_lag) {
+            ++s->coarse_age;
+            s->coarse.last_setup_ms = 0.f;  // this solve formed nothing
+        } else {
+            if (s->mixed) s->coarse.setup<float>(s->A, s->valf.p, nullptr, s->ctx->stream);
+            else s->coarse.setup<double>(s->A, s->val.p, nullptr, s->ctx->stream);
+            s->launches += s->coarse.launches;
+            s->coarse_ready = true;
+            s->coarse_age = 0;
+        }
     }
     if (s->mixed) {
         // FP32 inner PCG inside an FP64 refinement loop; *fnorm is ||b - A x|| / ||b|| in FP64
@@ -696,6 +704,7 @@ int mphy_solver_create(mphy_ctx* c, const mphy_mesh* m, const mphy_pattern* P, c
                      MPHY_ERR_INVALID_ARG, "unknown precision");
         MPHY_REQUIRE(o.pc_type == MPHY_PC_JACOBI || o.pc_type == MPHY_PC_FSAI || o.pc_type == MPHY_PC_FSAI_LEARNED,
                      MPHY_ERR_INVALID_ARG, "unknown preconditioner");
+        MPHY_REQUIRE(o.coarse_lag >= 0, MPHY_ERR_INVALID_ARG, "coarse_lag must be >= 0");
         MPHY_CUDA(cudaSetDevice(c->device));
         auto* s = new mphy_solver;
         try {
@@ -1162,8 +1171,10 @@ int mphy_newton_run(mphy_solver* s, const double* fext_host, const mphy_newton_o
                                      s->lift.p, (int64_t)nd, st, s->ctx->sm_count);
             bool converged = false;
             double norm = -1.0, norm_prev = -1.0, tol = o->tol_abs;
+            s->coarse_ready = false;  // a lagged coarse operator never outlives its load step
             for (int iter = 1; iter <= o->max_newton; ++iter) {
                 mphy_iter_stats is{};
+                const int64_t l0 = s->launches;
                 MPHY_CUDA(cudaEventRecord(s->ctx->ev0, st));
                 solver_assemble(s, disp, nullptr, presc && iter == 1 ? s->lift.p : nullptr);
                 add_scaled_free(s->mesh->fixed.p, s->fext_tmp.p, lambda, s->rhs.p, (int64_t)nd, st, s->ctx->sm_count);
@@ -1196,6 +1207,7 @@ int mphy_newton_run(mphy_solver* s, const double* fext_host, const mphy_newton_o
                 is.step = steps_done;
                 is.iter = iter;
                 is.rhs_norm = norm;
+                is.kernel_launches = s->launches - l0;
                 if (hist && rows < max_hist) hist[rows++] = is;
                 if (stop) break;
             }
@@ -1271,6 +1283,7 @@ int mphy_arclength_run(mphy_solver* s, const double* fext_host, const mphy_newto
             axpy_inplace(s->du_full.p, s->disp_prev.p, -1.0, n, st, sm);
             double dlam = lam - lam_prev;
             double norm = -1.0, tol = o->tol_abs;
+            s->coarse_ready = false;  // a lagged coarse operator never outlives its load step
             for (int iter = 1; iter < o->max_newton; ++iter) {
                 mphy_iter_stats is{};
                 const int64_t l0 = s->launches;

@@ -356,13 +356,22 @@ __global__ void __launch_bounds__(256) coarse_matrix_linear_kernel(SellView A, c
 // modes that vanish on the free DOFs (an aggregate of prescribed nodes) and the padding become
 // identity rows: their correction is zero
 __global__ void drop_null_modes(double* __restrict__ E, int kp, int k) {
-    __shared__ double mx;
-    if (threadIdx.x == 0) {
-        double m = 0.0;
-        for (int j = 0; j < k; ++j) m = fmax(m, fabs(E[(int64_t)j * kp + j]));
-        mx = m;
+    __shared__ double red[32];
+    // largest diagonal entry: per-thread maxima, then per warp and across warps
+    double m = 0.0;
+    for (int j = threadIdx.x; j < k; j += blockDim.x) m = fmax(m, fabs(E[(int64_t)j * kp + j]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        m = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (threadIdx.x == 0) red[0] = m;
     }
     __syncthreads();
+    const double mx = red[0];
     for (int j = threadIdx.x; j < kp; j += blockDim.x) {
         const bool drop = j >= k || !(E[(int64_t)j * kp + j] > 1e-13 * mx);
         if (!drop) continue;
@@ -380,67 +389,148 @@ __global__ void drop_null_modes(double* __restrict__ E, int kp, int k) {
 __device__ __forceinline__ void load_tile(double (*S)[TP], const double* M, int kp, int ti, int tj) {
     for (int t = threadIdx.x; t < T * T; t += blockDim.x) S[t / T][t % T] = M[(int64_t)(ti * T + t / T) * kp + tj * T + t % T];
 }
-__device__ __forceinline__ void store_tile(const double (*S)[TP], double* M, int kp, int ti, int tj) {
-    for (int t = threadIdx.x; t < T * T; t += blockDim.x) M[(int64_t)(ti * T + t / T) * kp + tj * T + t % T] = S[t / T][t % T];
-}
 
 // Factor the diagonal tile (j, j) in place (lower triangle; upper zeroed), and write its inverse
 // W_jj = L_jj^{-1} to W: the panel below becomes a tile product with W_jj (gemm_panel_tiles) and
-// the triangular inverse reuses W_jj. Two warps; thread t holds row t of the tile in registers.
-// Cholesky step c: every row t >= c publishes its entry of column c, then each thread forms
-// L(t, c) = A(t, c) / sqrt(A(c, c)) and applies the rank-1 update to its row (columns c < k <= t);
-// the published column is double-buffered, so each step needs one barrier. Inverse: L goes to
-// shared memory once; thread t solves L x = e_t by forward substitution (column t of L^{-1}) with
-// no further barriers.
-__global__ void __launch_bounds__(T) potrf_inv_tile(double* E, double* W, int kp, int j, int32_t* err) {
-    __shared__ double colv[2][T];
-    __shared__ double Ls[T][TP];
-    const int t = threadIdx.x;  // blockDim.x == T
+// the triangular inverse reuses W_jj. The tile's lower triangle is cut into 4x4 patches, one per
+// thread (136 patches), held in registers for the whole kernel with every patch index known at
+// compile time; a step exchanges only one column (or row) through shared memory, double-buffered,
+// so each step costs one barrier.
+//   Cholesky, step c: the owners of column c publish it (unscaled; final after step c - 1);
+//   every thread computes rd[c] = 1 / sqrt(A(c,c)), subtracts A(i,c) A(k,c) rd[c]^2 from its
+//   entries (i, k) with c < k <= i, and the owners scale their column c by rd[c], giving L.
+//   Inverse, step i: X = L^{-1} by right-looking forward substitution on B (initially I): the
+//   owners of column i of L and of row i of B publish them; every entry (m, l) with
+//   l <= i < m subtracts L(m,i) B(i,l) rd[i]. Row m of B is final after step m - 1 and
+//   X(m, l) = B(m, l) rd[m].
+constexpr int kPotrfPatches = (T / 4) * (T / 4 + 1) / 2;  // 136
+constexpr int kPotrfThreads = 160;                          // five warps, the last 24 threads idle
+
+__global__ void __launch_bounds__(kPotrfThreads) potrf_inv_tile(double* E, double* W, int kp, int j, int32_t* err) {
+    __shared__ double colv[2][T];  // Cholesky: column c; inverse: column i of L
+    __shared__ double rowv[2][T];  // inverse: row i of B
+    __shared__ double rd[T];
+    const int tid = threadIdx.x;
+    const bool owner = tid < kPotrfPatches;
+    // patch (P, Q), Q <= P, from the row-major triangular index
+    int P = (int)((sqrtf(8.0f * (float)tid + 1.0f) - 1.0f) * 0.5f);
+    while (P * (P + 1) / 2 > tid) --P;  // the float root, made exact
+    while ((P + 1) * (P + 2) / 2 <= tid) ++P;
+    const int Q = owner ? tid - P * (P + 1) / 2 : -1;
+    if (!owner) P = -1;
+    const int r0 = 4 * P, c0 = 4 * Q;
+    double A[4][4], B[4][4];
     const double* Et = E + (int64_t)(j * T) * kp + j * T;
-    double a[T];
+    if (owner) {
 #pragma unroll
-    for (int k = 0; k < T; ++k) a[k] = Et[(int64_t)t * kp + k];
+        for (int a = 0; a < 4; ++a) {
+            const double2* row = reinterpret_cast<const double2*>(Et + (int64_t)(r0 + a) * kp + c0);
+            const double2 v0 = row[0], v1 = row[1];
+            A[a][0] = v0.x;
+            A[a][1] = v0.y;
+            A[a][2] = v1.x;
+            A[a][3] = v1.y;
 #pragma unroll
-    for (int c = 0; c < T; ++c) {
-        const int buf = c & 1;
-        if (t >= c) colv[buf][t] = a[c];
-        __syncthreads();
-        double p = colv[buf][c];
-        if (!(p > 0.0)) {
-            if (t == 0) atomicExch(err, 2);
-            p = 1e-300;
-        }
-        const double l = sqrt(p), il = 1.0 / l;
-        if (t > c) {
-            const double ltc = a[c] * il;
-#pragma unroll
-            for (int k = c + 1; k < T; ++k)
-                if (k <= t) a[k] -= ltc * (colv[buf][k] * il);
-            a[c] = ltc;
-        } else if (t == c) {
-            a[c] = l;
+            for (int b = 0; b < 4; ++b) B[a][b] = r0 + a == c0 + b ? 1.0 : 0.0;
         }
     }
+    // ---- Cholesky: column c = 4 cq + kk, kk known at compile time
+    for (int cq = 0; cq < T / 4; ++cq) {
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) {
+            const int c = 4 * cq + kk, buf = c & 1;
+            if (Q == cq) {
+#pragma unroll
+                for (int a = 0; a < 4; ++a)
+                    if (r0 + a >= c) colv[buf][r0 + a] = A[a][kk];
+            }
+            __syncthreads();
+            double p = colv[buf][c];
+            if (!(p > 0.0)) {
+                if (tid == 0) atomicExch(err, 2);
+                p = 1e-300;
+            }
+            const double il = rsqrt(p);
+            const double f = il * il;
+            if (tid == 0) rd[c] = il;
+            if (owner && P >= cq) {
+                double ci[4], cf[4];
+#pragma unroll
+                for (int a = 0; a < 4; ++a) ci[a] = colv[buf][r0 + a];
+#pragma unroll
+                for (int b = 0; b < 4; ++b) cf[b] = colv[buf][c0 + b] * f;
+#pragma unroll
+                for (int a = 0; a < 4; ++a)
+#pragma unroll
+                    for (int b = 0; b < 4; ++b)
+                        if (c0 + b > c && c0 + b <= r0 + a) A[a][b] = fma(-ci[a], cf[b], A[a][b]);
+                if (Q == cq) {
+#pragma unroll
+                    for (int a = 0; a < 4; ++a)
+                        if (r0 + a >= c) A[a][kk] *= il;
+                }
+            }
+        }
+    }
+    // ---- inverse: step i = 4 iq + aa
+    for (int iq = 0; iq < T / 4; ++iq) {
+#pragma unroll
+        for (int aa = 0; aa < 4; ++aa) {
+            const int i = 4 * iq + aa, buf = i & 1;
+            if (i == T - 1) break;  // nothing below the last row
+            if (Q == iq) {
+#pragma unroll
+                for (int a = 0; a < 4; ++a)
+                    if (r0 + a > i) colv[buf][r0 + a] = A[a][aa];
+            }
+            if (P == iq) {
+#pragma unroll
+                for (int b = 0; b < 4; ++b)
+                    if (c0 + b <= i) rowv[buf][c0 + b] = B[aa][b];
+            }
+            __syncthreads();
+            if (owner && P >= iq) {
+                const double ri = rd[i];
+                double lm[4], bl[4];
+#pragma unroll
+                for (int a = 0; a < 4; ++a) lm[a] = colv[buf][r0 + a] * ri;
+#pragma unroll
+                for (int b = 0; b < 4; ++b) bl[b] = rowv[buf][c0 + b];
+#pragma unroll
+                for (int a = 0; a < 4; ++a)
+#pragma unroll
+                    for (int b = 0; b < 4; ++b)
+                        if (r0 + a > i && c0 + b <= i) B[a][b] = fma(-lm[a], bl[b], B[a][b]);
+            }
+        }
+    }
+    __syncthreads();  // rd complete
+    if (!owner) return;
     double* Eo = E + (int64_t)(j * T) * kp + j * T;
-#pragma unroll
-    for (int k = 0; k < T; ++k) {
-        const double v = k <= t ? a[k] : 0.0;
-        Ls[t][k] = v;
-        Eo[(int64_t)t * kp + k] = v;
-    }
-    __syncthreads();
-    // column t of X = L^{-1}: x_i = 0 (i < t), x_t = 1 / L_tt, x_i = -sum_{t <= m < i} L_im x_m / L_ii
-    double x[T];
-#pragma unroll
-    for (int i = 0; i < T; ++i) {
-        double acc = i == t ? 1.0 : 0.0;
-#pragma unroll
-        for (int m = 0; m < i; ++m) acc -= Ls[i][m] * x[m];
-        x[i] = i >= t ? acc / Ls[i][i] : 0.0;
-    }
     double* Wo = W + (int64_t)(j * T) * kp + j * T;
 #pragma unroll
-    for (int i = 0; i < T; ++i) Wo[(int64_t)i * kp + t] = x[i];
+    for (int a = 0; a < 4; ++a) {
+        const double rm = rd[r0 + a];
+        double l[4], x[4];
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const bool lower = c0 + b <= r0 + a;
+            l[b] = lower ? A[a][b] : 0.0;
+            x[b] = lower ? B[a][b] * rm : 0.0;
+        }
+        double2* er = reinterpret_cast<double2*>(Eo + (int64_t)(r0 + a) * kp + c0);
+        double2* wr = reinterpret_cast<double2*>(Wo + (int64_t)(r0 + a) * kp + c0);
+        er[0] = make_double2(l[0], l[1]);
+        er[1] = make_double2(l[2], l[3]);
+        wr[0] = make_double2(x[0], x[1]);
+        wr[1] = make_double2(x[2], x[3]);
+        if (P != Q) {
+            // the mirrored upper patch (Q, P) is zero in both
+            double2* eu = reinterpret_cast<double2*>(Eo + (int64_t)(c0 + a) * kp + r0);
+            double2* wu = reinterpret_cast<double2*>(Wo + (int64_t)(c0 + a) * kp + r0);
+            eu[0] = eu[1] = wu[0] = wu[1] = make_double2(0.0, 0.0);
+        }
+    }
 }
 
 // C (tile ci, cj of M) += alpha * sum_t A[r][t] * B[c][t]  with A, B 64x64 tiles in shared memory
@@ -457,17 +547,26 @@ __device__ __forceinline__ void tile_abt(const double (*A)[TP], const double (*B
     }
 }
 
-// trailing update A_ik -= L_ij L_kj^T for j < k <= i
-__global__ void __launch_bounds__(256) syrk_tiles(double* E, int kp, int j) {
+// trailing update A_ik -= L_ij L_kj^T of step j. col_only: the tile column k = j + 1 (one CTA
+// per tile i > j), which the next diagonal factorisation and panel need first; otherwise the
+// rest, j + 2 <= k <= i (one CTA per tile of that triangle).
+__global__ void __launch_bounds__(256) syrk_tiles(double* E, int kp, int j, int col_only) {
     extern __shared__ double sm[];
     double (*Li)[TP] = reinterpret_cast<double (*)[TP]>(sm);
     double (*Lk)[TP] = reinterpret_cast<double (*)[TP]>(sm + T * TP);
-    const int idx = blockIdx.x;
-    const int ii = (int)((sqrt(8.0 * idx + 1.0) - 1.0) / 2.0);
-    int a = ii, b = idx - ii * (ii + 1) / 2;
-    if (b > a) { ++a; b = idx - a * (a + 1) / 2; }  // guard the float square root
-    if (b < 0) { --a; b = idx - a * (a + 1) / 2; }
-    const int i = j + 1 + a, k = j + 1 + b;
+    int i, k;
+    if (col_only) {
+        i = j + 1 + (int)blockIdx.x;
+        k = j + 1;
+    } else {
+        const int idx = blockIdx.x;
+        const int ii = (int)((sqrt(8.0 * idx + 1.0) - 1.0) / 2.0);
+        int a = ii, b = idx - ii * (ii + 1) / 2;
+        if (b > a) { ++a; b = idx - a * (a + 1) / 2; }  // guard the float square root
+        if (b < 0) { --a; b = idx - a * (a + 1) / 2; }
+        i = j + 2 + a;
+        k = j + 2 + b;
+    }
     load_tile(Li, E, kp, i, j);
     load_tile(Lk, E, kp, k, j);
     __syncthreads();
@@ -529,12 +628,18 @@ __global__ void __launch_bounds__(256) trtri_update(const double* E, double* W, 
         for (int r = 0; r < 4; ++r) W[(int64_t)(i * T + ty + 16 * q) * kp + j * T + tx + 16 * r] += acc[q][r];
 }
 
-// E^{-1} = W^T W (tile (i, j) = sum_{k >= max(i,j)} W_ki^T W_kj), stored FP64
+// E^{-1} = W^T W, its lower tiles only (symmetric): tile (i, j), j <= i, is
+// sum_{k >= i} W_ki^T W_kj, stored FP64 at tile index i (i + 1) / 2 + j. A diagonal tile comes out
+// bitwise symmetric (entry (r, c) and (c, r) sum the same products in the same order).
 __global__ void __launch_bounds__(256) inverse_tiles(const double* W, double* einv, int kp, int nb) {
     extern __shared__ double sm[];
     double (*A)[TP] = reinterpret_cast<double (*)[TP]>(sm);
     double (*B)[TP] = reinterpret_cast<double (*)[TP]>(sm + T * TP);
-    const int i = blockIdx.x / nb, j = blockIdx.x % nb;
+    const int t = blockIdx.x;
+    int i = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+    while (i * (i + 1) / 2 > t) --i;  // the float root, made exact
+    while ((i + 1) * (i + 2) / 2 <= t) ++i;
+    const int j = t - i * (i + 1) / 2;
     const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;
     double acc[4][4] = {{0}};
     for (int k = max(i, j); k < nb; ++k) {
@@ -547,8 +652,9 @@ __global__ void __launch_bounds__(256) inverse_tiles(const double* W, double* ei
         tile_abt(A, B, acc);
         __syncthreads();
     }
+    double* o = einv + (int64_t)t * T * T;
     for (int q = 0; q < 4; ++q)
-        for (int r = 0; r < 4; ++r) einv[(int64_t)(i * T + ty + 16 * q) * kp + j * T + tx + 16 * r] = acc[q][r];
+        for (int r = 0; r < 4; ++r) o[(ty + 16 * q) * T + tx + 16 * r] = acc[q][r];
 }
 
 }  // namespace
@@ -616,7 +722,12 @@ void CoarseSpace::init(mphy_ctx* ctx, const mphy_mesh* mesh, const mphy_pattern*
     cent_.alloc(3 * (size_t)n_agg_);
     E_.alloc((size_t)kp_ * kp_);
     W_.alloc((size_t)kp_ * kp_);
-    einv_.alloc((size_t)kp_ * kp_);
+    const int nb = kp_ / T;
+    const size_t tiles = (size_t)nb * (nb + 1) / 2;
+    einv_.alloc(tiles * T * T);
+    gpart_.alloc(tiles * 2 * T);
+    gcount_.alloc(nb + 1);
+    wcrow_.alloc(nb);
     w_.alloc(kp_);
     c_.alloc(kp_);
     wpart_.alloc((size_t)n_agg_ * kMaxRestrictParts * nm_);
@@ -626,6 +737,7 @@ void CoarseSpace::init(mphy_ctx* ctx, const mphy_mesh* mesh, const mphy_pattern*
     MPHY_CUDA(cudaMemsetAsync(w_.p, 0, w_.bytes(), s));
     MPHY_CUDA(cudaMemsetAsync(c_.p, 0, c_.bytes(), s));
     MPHY_CUDA(cudaMemsetAsync(wcount_.p, 0, wcount_.bytes(), s));
+    MPHY_CUDA(cudaMemsetAsync(gcount_.p, 0, gcount_.bytes(), s));
     MPHY_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -715,37 +827,70 @@ void CoarseSpace::setup(const SellView& A, const VT* aval, const double* disp, c
     MPHY_REQUIRE(h != 2, MPHY_ERR_INDEFINITE, "coarse space: Z^T A Z is not positive definite");
 }
 
+// Three streams inside the capture. Main: the diagonal factorisation and the panel of step j,
+// then the update of tile column j + 1 (after the previous step's remaining update), so the next
+// diagonal tile is ready as early as possible. Side 1: the rest of step j's trailing update.
+// Side 2: the triangular inverse, step j as soon as column j of L and W_jj are final. Every
+// tile is written by one stream at a time, in step order.
 void CoarseSpace::record_factorisation(cudaStream_t s, int nb, size_t sm2) {
+    if (!side_[0]) {
+        for (auto& q : side_) MPHY_CUDA(cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking));
+        for (auto& e : ev_) MPHY_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    cudaStream_t s_rest = side_[0], s_tri = side_[1];
+    cudaEvent_t ev_col = ev_[0], ev_rest = ev_[1], ev_tri = ev_[2];
     drop_null_modes<<<1, 1024, 0, s>>>(E_.p, kp_, nm_ * n_agg_);
     launches += 1;
+    MPHY_CUDA(cudaEventRecord(ev_col, s));
+    MPHY_CUDA(cudaStreamWaitEvent(s_rest, ev_col, 0));
+    MPHY_CUDA(cudaStreamWaitEvent(s_tri, ev_col, 0));
+    bool rest_pending = false;
     for (int j = 0; j < nb; ++j) {
-        potrf_inv_tile<<<1, T, 0, s>>>(E_.p, W_.p, kp_, j, err_.p);
         const int m = nb - j - 1;
+        potrf_inv_tile<<<1, kPotrfThreads, 0, s>>>(E_.p, W_.p, kp_, j, err_.p);
+        launches += 1;
         if (m > 0) {
             gemm_panel_tiles<<<m, 256, sm2, s>>>(E_.p, W_.p, kp_, j);
-            syrk_tiles<<<m * (m + 1) / 2, 256, sm2, s>>>(E_.p, kp_, j);
-            launches += 2;
-        }
-        launches += 1;
-    }
-    // W = L^{-1}: the diagonal tiles W_kk are already there (potrf_inv_tile)
-    for (int k = 0; k < nb; ++k) {
-        if (k > 0) {
-            trtri_finalize<<<k, 256, sm2, s>>>(W_.p, kp_, k);
             launches += 1;
         }
-        if (k < nb - 1) {
-            trtri_update<<<(nb - k - 1) * (k + 1), 256, sm2, s>>>(E_.p, W_.p, kp_, k, nb);
+        MPHY_CUDA(cudaEventRecord(ev_col, s));  // column j of L and W_jj are final
+        MPHY_CUDA(cudaStreamWaitEvent(s_tri, ev_col, 0));
+        if (j > 0) {
+            trtri_finalize<<<j, 256, sm2, s_tri>>>(W_.p, kp_, j);
             launches += 1;
         }
+        if (m > 0) {
+            trtri_update<<<m * (j + 1), 256, sm2, s_tri>>>(E_.p, W_.p, kp_, j, nb);
+            launches += 1;
+            if (m > 1) {
+                MPHY_CUDA(cudaStreamWaitEvent(s_rest, ev_col, 0));
+                syrk_tiles<<<(m - 1) * m / 2, 256, sm2, s_rest>>>(E_.p, kp_, j, 0);
+                launches += 1;
+            }
+            // step j - 1's remaining update also covered tile column j + 1
+            if (rest_pending) MPHY_CUDA(cudaStreamWaitEvent(s, ev_rest, 0));
+            syrk_tiles<<<m, 256, sm2, s>>>(E_.p, kp_, j, 1);
+            launches += 1;
+            rest_pending = m > 1;
+            if (rest_pending) MPHY_CUDA(cudaEventRecord(ev_rest, s_rest));
+        }
     }
-    inverse_tiles<<<nb * nb, 256, sm2, s>>>(W_.p, einv_.p, kp_, nb);
+    // join both side streams before E^{-1} = W^T W
+    MPHY_CUDA(cudaEventRecord(ev_rest, s_rest));
+    MPHY_CUDA(cudaStreamWaitEvent(s, ev_rest, 0));
+    MPHY_CUDA(cudaEventRecord(ev_tri, s_tri));
+    MPHY_CUDA(cudaStreamWaitEvent(s, ev_tri, 0));
+    inverse_tiles<<<nb * (nb + 1) / 2, 256, sm2, s>>>(W_.p, einv_.p, kp_, nb);
     launches += 1;
     MPHY_CUDA(cudaGetLastError());
 }
 
 CoarseSpace::~CoarseSpace() {
     if (fact_graph_) cudaGraphExecDestroy(fact_graph_);
+    for (auto& e : ev_)
+        if (e) cudaEventDestroy(e);
+    for (auto& q : side_)
+        if (q) cudaStreamDestroy(q);
 }
 
 template void CoarseSpace::setup<double>(const SellView&, const double*, const double*, cudaStream_t);
@@ -765,6 +910,10 @@ CoarseView CoarseSpace::view() const {
     v.dperm = dperm_.p;
     v.fperm = fperm_.p;
     v.einv = einv_.p;
+    v.nb = kp_ / T;
+    v.gpart = gpart_.p;
+    v.gcount = gcount_.p;
+    v.wcrow = wcrow_.p;
     v.w = w_.p;
     v.wpart = wpart_.p;
     v.wcount = wcount_.p;

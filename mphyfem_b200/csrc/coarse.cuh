@@ -36,6 +36,8 @@ class CoarseSpace {
   private:
     void record_factorisation(cudaStream_t s, int nb, size_t sm2);
     cudaGraphExec_t fact_graph_ = nullptr;
+    cudaStream_t side_[2] = {nullptr, nullptr};  // captured side streams of the factorisation
+    cudaEvent_t ev_[3] = {nullptr, nullptr, nullptr};
     int64_t fact_launches_ = 0;
     double boxd_ = 0.0;
     int nm_ = 6;
@@ -47,7 +49,9 @@ class CoarseSpace {
     DevBuf<int32_t> agg_, agg_nodes_, err_;
     DevBuf<int64_t> agg_ptr_;
     DevBuf<double> d_, cent_, E_, W_, w_, c_;
-    DevBuf<double> einv_;
+    DevBuf<double> einv_;     // lower tiles of E^{-1}
+    DevBuf<double> gpart_, wcrow_;
+    DevBuf<uint32_t> gcount_;
     DevBuf<uint8_t> drop_;
     DevBuf<double> wpart_;
     DevBuf<uint32_t> wcount_;

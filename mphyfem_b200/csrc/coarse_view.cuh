@@ -19,7 +19,9 @@ struct CoarseView {
     const uint8_t* fixed;    // [3 n_node]
     const double* dperm;     // [n_node][3] d in the order of agg_nodes (the restriction's loads)
     const uint8_t* fperm;    // [3 n_node] fixed in the order of agg_nodes
-    // [kp][kp] inverse of E (row-major), FP64: with a large stiffness contrast E is so
+    int32_t nb;              // kp / 64 tiles per side
+    // inverse of E, FP64, symmetric: its lower 64x64 tiles (I, J), J <= I, at tile index
+    // I (I + 1) / 2 + J, each row-major. FP64: with a large stiffness contrast E is so
     // ill-conditioned that rounding its inverse to FP32 makes the coarse term indefinite, and CG
     // on an indefinite preconditioner stalls
     const double* einv;
@@ -27,6 +29,9 @@ struct CoarseView {
     double* wpart;           // [n_agg][kMaxRestrictParts][nm] partial restriction sums
     uint32_t* wcount;        // [n_agg] parts summed so far (zero between launches)
     double* c;               // [kp] coarse correction E^{-1} w
+    double* gpart;           // [tiles][2][64] the GEMV's per-tile products (E_IJ w_J, E_IJ^T w_I)
+    uint32_t* gcount;        // [nb + 1] GEMV tickets: tiles done per tile row, rows done (zero between launches)
+    double* wcrow;           // [nb] (w, c) per tile row
 };
 
 #ifdef __CUDACC__

@@ -450,6 +450,70 @@ __global__ void __launch_bounds__(kThreads) pcg_update_kernel(int64_t n, XT* __r
     }
 }
 
+// Two-level iteration with the ||r|| test: x += alpha p, r -= alpha q and the fused
+// (r, D^-1 r), (r, r), left in the state for the coarse GEMV (coarse_gemv_kernel<true>), which
+// adds (Z^T r, c) = (r, Z c) to complete (r, z); z = D^-1 r + Z c is then formed only inside the
+// direction update (coarse_final_dir_kernel).
+template <typename XT>
+__global__ void __launch_bounds__(kThreads) pcg_update_rdr_kernel(int64_t n, XT* __restrict__ x, XT* __restrict__ r,
+                                                                  const XT* __restrict__ p, const XT* __restrict__ q,
+                                                                  const XT* __restrict__ dinv,
+                                                                  double* __restrict__ part_a,
+                                                                  double* __restrict__ part_b, PcgState* st) {
+    __shared__ double sh[32];
+    if (st->done) return;
+    const XT alpha = (XT)st->alpha;
+    double a1 = 0.0, a2 = 0.0;
+    if (aligned16(x, r, p, q) && aligned16(dinv, dinv, dinv, dinv)) {
+        using V = typename Pair<XT>::type;
+        const int64_t n2 = n >> 1;
+        V* x2 = reinterpret_cast<V*>(x);
+        V* r2 = reinterpret_cast<V*>(r);
+        const V* p2 = reinterpret_cast<const V*>(p);
+        const V* q2 = reinterpret_cast<const V*>(q);
+        const V* d2 = reinterpret_cast<const V*>(dinv);
+        for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n2; i += (int64_t)gridDim.x * blockDim.x) {
+            V xv = ld_once(x2 + i), rv = r2[i];
+            const V pv = p2[i], qv = ld_once(q2 + i), dv = d2[i];
+            xv.x = xv.x + alpha * pv.x;
+            xv.y = xv.y + alpha * pv.y;
+            rv.x = rv.x - alpha * qv.x;
+            rv.y = rv.y - alpha * qv.y;
+            __stcs(x2 + i, xv);
+            r2[i] = rv;
+            a1 += (double)rv.x * ((double)dv.x * (double)rv.x) + (double)rv.y * ((double)dv.y * (double)rv.y);
+            a2 += (double)rv.x * (double)rv.x + (double)rv.y * (double)rv.y;
+        }
+        if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+            x[n - 1] = x[n - 1] + alpha * p[n - 1];
+            const XT ri = r[n - 1] - alpha * q[n - 1];
+            r[n - 1] = ri;
+            a1 += (double)ri * ((double)dinv[n - 1] * (double)ri);
+            a2 += (double)ri * (double)ri;
+        }
+    } else {
+        for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+            __stcs(x + i, ld_once(x + i) + alpha * p[i]);
+            const XT ri = r[i] - alpha * ld_once(q + i);
+            r[i] = ri;
+            a1 += (double)ri * ((double)dinv[i] * (double)ri);
+            a2 += (double)ri * (double)ri;
+        }
+    }
+    a1 = block_sum(a1, sh);
+    if (threadIdx.x == 0) part_a[blockIdx.x] = a1;
+    a2 = block_sum(a2, sh);
+    if (threadIdx.x == 0) part_b[blockIdx.x] = a2;
+    if (!arrive_last(&st->counter)) return;
+    const double rdr = reduce_partials(part_a, gridDim.x, sh);
+    const double rr = reduce_partials(part_b, gridDim.x, sh);
+    if (threadIdx.x == 0) {
+        st->counter = 0;
+        st->rdr = rdr;
+        st->rr = rr;
+    }
+}
+
 template <typename XT>
 __global__ void __launch_bounds__(kThreads) pcg_direction_kernel(int64_t n, XT* __restrict__ p, const XT* __restrict__ z,
                                                                  const PcgState* st) {
@@ -621,54 +685,152 @@ void launch_restrict(const CoarseView& cv, const XT* r, const PcgState* st, cuda
     coarse_restrict_kernel<XT><<<g, kThreads, 0, s>>>(cv, parts, r, st);
 }
 
-// c = E^{-1} w: one warp per row of the FP64 inverse. Each lane reads 16-byte pairs, eight
-// independent loads per step (kp is a multiple of 64, rows start 512-byte aligned), so a row
-// takes few dependent round trips and enough bytes are in flight to stream E^{-1} at HBM rate.
-// Pair j of a row goes to accumulator (j / 32) mod 4 in increasing j.
-__global__ void __launch_bounds__(kThreads) coarse_gemv_kernel(CoarseView cv, const PcgState* st) {
+// c = E^{-1} w with the symmetric FP64 inverse stored as its lower 64x64 tiles. One CTA per
+// stored tile (I, J) reads it once: a 16 x 16 thread grid, each thread a 4 x 4 patch (a half warp
+// streams one 512-byte tile row per load). It forms E_IJ w_J (rows of I) and, off the diagonal,
+// E_IJ^T w_I (rows of J): per-thread partials summed across the half warp, and across warps in
+// warp order. Both go to the tile's slots of gpart. Every tile row X is touched by nb tiles;
+// the CTA that completes X's ticket sums X's slots in tile order (J ascending) into c_X, so c
+// does not depend on which CTA ran which tile (four threads per entry take a quarter of the
+// slots each, added in order).
+// FIN (two-level iteration with the ||r|| test): the finisher of row X also stores (w_X, c_X);
+// the CTA that finishes the last row adds the rows in order and ends the iteration:
+// (r, z) = (r, D^-1 r) + (w, c), ||r||^2 from the update.
+__device__ __forceinline__ int64_t lower_tile(int i, int j) { return (int64_t)i * (i + 1) / 2 + j; }
+
+template <bool FIN>
+__global__ void __launch_bounds__(256) coarse_gemv_kernel(CoarseView cv, PcgState* st) {
+    __shared__ double wI[64], wJ[64];
+    __shared__ double colp[8][64];  // column partials per warp; the finisher's quarter sums
+    __shared__ double red[2];
+    __shared__ int finish[2];
+    __shared__ bool last_row;
     if (st && st->done) return;
-    const int lane = threadIdx.x & 31;
-    for (int64_t row = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; row < cv.kp;
-         row += ((int64_t)gridDim.x * blockDim.x) >> 5) {
-        const double2* e = reinterpret_cast<const double2*>(cv.einv + row * cv.kp);
-        const double2* wv = reinterpret_cast<const double2*>(cv.w);
-        const int np = cv.kp >> 1;  // double2 per row
-        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-        int c = lane;
-        for (; c + 224 < np; c += 256) {
-            double2 ev[8], wv8[8];
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                ev[k] = ld_once(e + c + 32 * k);
-                wv8[k] = wv[c + 32 * k];
-            }
-            a0 += ev[0].x * wv8[0].x + ev[0].y * wv8[0].y;
-            a1 += ev[1].x * wv8[1].x + ev[1].y * wv8[1].y;
-            a2 += ev[2].x * wv8[2].x + ev[2].y * wv8[2].y;
-            a3 += ev[3].x * wv8[3].x + ev[3].y * wv8[3].y;
-            a0 += ev[4].x * wv8[4].x + ev[4].y * wv8[4].y;
-            a1 += ev[5].x * wv8[5].x + ev[5].y * wv8[5].y;
-            a2 += ev[6].x * wv8[6].x + ev[6].y * wv8[6].y;
-            a3 += ev[7].x * wv8[7].x + ev[7].y * wv8[7].y;
-        }
-        for (; c + 96 < np; c += 128) {
-            const double2 e0 = ld_once(e + c), e1 = ld_once(e + c + 32), e2 = ld_once(e + c + 64),
-                          e3 = ld_once(e + c + 96);
-            const double2 w0 = wv[c], w1 = wv[c + 32], w2 = wv[c + 64], w3 = wv[c + 96];
-            a0 += e0.x * w0.x + e0.y * w0.y;
-            a1 += e1.x * w1.x + e1.y * w1.y;
-            a2 += e2.x * w2.x + e2.y * w2.y;
-            a3 += e3.x * w3.x + e3.y * w3.y;
-        }
-        for (; c < np; c += 32) {
-            const double2 e0 = ld_once(e + c), w0 = wv[c];
-            a0 += e0.x * w0.x + e0.y * w0.y;
-        }
-        double acc = (a0 + a1) + (a2 + a3);
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (lane == 0) cv.c[row] = acc;
+    const int t = blockIdx.x;
+    int I = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+    while (I * (I + 1) / 2 > t) --I;  // the float root, made exact
+    while ((I + 1) * (I + 2) / 2 <= t) ++I;
+    const int J = t - I * (I + 1) / 2;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid < 64) {
+        wI[tid] = cv.w[64 * I + tid];
+        wJ[tid] = cv.w[64 * J + tid];
     }
+    __syncthreads();
+    const int tx = lane & 15, ty = 2 * warp + (lane >> 4);
+    const double* E = cv.einv + (int64_t)t * 4096;
+    double rp[4], cp[4] = {0.0, 0.0, 0.0, 0.0};
+    double2 ev[4][2];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const double2* row = reinterpret_cast<const double2*>(E + 64 * (4 * ty + a) + 4 * tx);
+        ev[a][0] = ld_once(row);
+        ev[a][1] = ld_once(row + 1);
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const double e[4] = {ev[a][0].x, ev[a][0].y, ev[a][1].x, ev[a][1].y};
+        const double wi = wI[4 * ty + a];
+        rp[a] = 0.0;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            rp[a] += e[b] * wJ[4 * tx + b];
+            cp[b] += e[b] * wi;
+        }
+    }
+    // row sums over the 16 tx of a half warp
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int o = 8; o > 0; o >>= 1) rp[a] += __shfl_xor_sync(0xffffffffu, rp[a], o);
+    double* gp = cv.gpart + (int64_t)t * 128;
+    if (tx == 0)
+#pragma unroll
+        for (int a = 0; a < 4; ++a) gp[4 * ty + a] = rp[a];
+    if (I != J) {
+        // column sums: the two half warps, then the warps in order
+#pragma unroll
+        for (int b = 0; b < 4; ++b) cp[b] += __shfl_xor_sync(0xffffffffu, cp[b], 16);
+        if (lane < 16)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) colp[warp][4 * tx + b] = cp[b];
+        __syncthreads();
+        if (tid < 64) {
+            double x = 0.0;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) x += colp[q][tid];
+            gp[64 + tid] = x;
+        }
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) {
+        finish[0] = atomicAdd(cv.gcount + I, 1u) == (uint32_t)cv.nb - 1 ? I : -1;
+        finish[1] = I != J && atomicAdd(cv.gcount + J, 1u) == (uint32_t)cv.nb - 1 ? J : -1;
+    }
+    __syncthreads();
+    for (int f = 0; f < 2; ++f) {
+        const int X = finish[f];
+        if (X < 0) continue;
+        // four groups of 64 threads each sum a quarter of the row's nb slots in tile order;
+        // the quarters are then added in order
+        {
+            const int g = tid >> 6, i = tid & 63;
+            const int per = (cv.nb + 3) >> 2, k0 = g * per, k1 = min(cv.nb, k0 + per);
+            double x = 0.0;
+#pragma unroll 4
+            for (int K = k0; K < k1; ++K)
+                x += K <= X ? __ldcg(cv.gpart + lower_tile(X, K) * 128 + i)
+                            : __ldcg(cv.gpart + lower_tile(K, X) * 128 + 64 + i);
+            __syncthreads();  // colp is free (its last reads were before the ticket)
+            colp[g][i] = x;
+            __syncthreads();
+        }
+        double wc = 0.0;
+        if (tid < 64) {
+            const double x = (colp[0][tid] + colp[1][tid]) + (colp[2][tid] + colp[3][tid]);
+            const int i = 64 * X + tid;
+            cv.c[i] = x;
+            if (FIN && i < cv.k) wc = cv.w[i] * x;  // padding entries of w are zero and unused
+        }
+        if (FIN) {
+            // (w_X, c_X): butterflies in the two warps, then warp 0 + warp 1
+            if (tid < 64) {
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) wc += __shfl_xor_sync(0xffffffffu, wc, o);
+                if (lane == 0) red[warp] = wc;
+            }
+            __syncthreads();
+            if (tid == 0) cv.wcrow[X] = red[0] + red[1];
+        }
+        if (tid == 0) cv.gcount[X] = 0;  // every tile of row X has arrived
+        __syncthreads();
+    }
+    if (!FIN) return;
+    if (finish[0] < 0 && finish[1] < 0) return;
+    // rows done: the CTA that finishes the last one ends the iteration
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) {
+        const uint32_t nfin = (finish[0] >= 0) + (finish[1] >= 0);
+        last_row = atomicAdd(cv.gcount + cv.nb, nfin) + nfin == (uint32_t)cv.nb;
+    }
+    __syncthreads();
+    if (!last_row || warp != 0) return;
+    double wc = 0.0;
+    for (int X = lane; X < cv.nb; X += 32) wc += __ldcg(cv.wcrow + X);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) wc += __shfl_xor_sync(0xffffffffu, wc, o);
+    if (lane == 0) {
+        cv.gcount[cv.nb] = 0;
+        finish_iter(st, st->rdr + wc, st->rr);
+    }
+}
+
+// the coarse GEMV: one CTA per stored tile of E^{-1}
+template <bool FIN>
+void launch_gemv(const CoarseView& cv, PcgState* st, cudaStream_t s) {
+    coarse_gemv_kernel<FIN><<<(unsigned)((int64_t)cv.nb * (cv.nb + 1) / 2), 256, 0, s>>>(cv, st);
 }
 
 // z = D^{-1} r + Z c with the fused (r, z), (z, z); INIT also sets p = z and the initial state
@@ -772,6 +934,86 @@ __global__ void __launch_bounds__(kThreads) coarse_final_kernel(int32_t n_node, 
         st->counter = 0;
         if (INIT) finish_init(st, rz, zz, rtol, abstol, dtol, maxit, norm_type);
         else finish_iter(st, rz, zz);
+    }
+}
+
+// p = z + beta p with z = D^{-1} r + Z c formed in registers only (the two-level iteration with
+// the ||r|| test: (r, z) is already known from the update and the GEMV). Same node-pair layout and
+// the same arithmetic per entry as coarse_final_kernel followed by pcg_direction_kernel.
+template <typename XT>
+__global__ void __launch_bounds__(kThreads) coarse_final_dir_kernel(int32_t n_node, CoarseView cv,
+                                                                    const XT* __restrict__ r, XT* __restrict__ p,
+                                                                    const XT* __restrict__ dinv, const PcgState* st) {
+    if (st->done) return;
+    const XT beta = (XT)st->beta;
+    using V = typename Pair<XT>::type;
+    const bool paired = aligned16(r, p, dinv, cv.d);
+    const int64_t npair = ((int64_t)n_node + 1) >> 1;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < npair; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t n0 = 2 * t;
+        const int cnt = n0 + 1 < n_node ? 2 : 1;
+        XT rv[6], dv[6], pv[6];
+        double od[6];
+        uint8_t fx[6];
+        int32_t ag[2];
+        if (cnt == 2 && paired) {
+            const V* r2 = reinterpret_cast<const V*>(r + 3 * n0);
+            const V* v2 = reinterpret_cast<const V*>(dinv + 3 * n0);
+            const V* p2 = reinterpret_cast<const V*>(p + 3 * n0);
+            const double2* o2 = reinterpret_cast<const double2*>(cv.d + 3 * n0);
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                const V a = r2[q], b = v2[q], c = p2[q];
+                const double2 o = o2[q];
+                rv[2 * q] = a.x;
+                rv[2 * q + 1] = a.y;
+                dv[2 * q] = b.x;
+                dv[2 * q + 1] = b.y;
+                pv[2 * q] = c.x;
+                pv[2 * q + 1] = c.y;
+                od[2 * q] = o.x;
+                od[2 * q + 1] = o.y;
+            }
+        } else {
+#pragma unroll
+            for (int e = 0; e < 6; ++e) {
+                const bool in = e < 3 * cnt;
+                rv[e] = in ? r[3 * n0 + e] : XT(0);
+                dv[e] = in ? dinv[3 * n0 + e] : XT(0);
+                pv[e] = in ? p[3 * n0 + e] : XT(0);
+                od[e] = in ? cv.d[3 * n0 + e] : 0.0;
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < 6; ++e) fx[e] = e < 3 * cnt ? cv.fixed[3 * n0 + e] : (uint8_t)1;
+        ag[0] = cv.agg[n0];
+        ag[1] = cnt == 2 ? cv.agg[n0 + 1] : ag[0];
+        XT nv[6];
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            double zc[3];
+            coarse_node_value(cv, ag[k], od[3 * k], od[3 * k + 1], od[3 * k + 2], zc);
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                const int e = 3 * k + a;
+                const XT z = (XT)((double)dv[e] * (double)rv[e] + (fx[e] ? 0.0 : zc[a]));
+                nv[e] = z + beta * pv[e];
+            }
+        }
+        if (cnt == 2 && paired) {
+            V* p2 = reinterpret_cast<V*>(p + 3 * n0);
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                V v;
+                v.x = nv[2 * q];
+                v.y = nv[2 * q + 1];
+                p2[q] = v;
+            }
+        } else {
+#pragma unroll
+            for (int e = 0; e < 6; ++e)
+                if (e < 3 * cnt) p[3 * n0 + e] = nv[e];
+        }
     }
 }
 
@@ -971,7 +1213,7 @@ __global__ void __launch_bounds__(kThreads) coarse_prolong_add_kernel(int32_t n_
 
 void coarse_apply_add(const CoarseView& cv, int32_t n_node, const double* r, double* z, cudaStream_t s, int sm) {
     launch_restrict<double>(cv, r, nullptr, s, sm);
-    coarse_gemv_kernel<<<stride_grid((int64_t)cv.kp * 32, kThreads, sm), kThreads, 0, s>>>(cv, nullptr);
+    launch_gemv<false>(cv, nullptr, s);
     coarse_prolong_add_kernel<<<stride_grid(n_node, kThreads, sm), kThreads, 0, s>>>(n_node, cv, z);
     MPHY_CUDA(cudaGetLastError());
 }
@@ -1076,12 +1318,21 @@ void Pcg<VT, XT>::record_iterations(const VT* val, XT* x, cudaStream_t s, int n_
         if (kind_ == PcKind::Jacobi) {
             pcg_update_kernel<XT, true><<<gv, kThreads, 0, s>>>(n_, x, r_.p, z_.p, p_.p, q_.p, dinv_.p, partials_.p,
                                                                  partials2_.p, st_.p);
+        } else if (kind_ == PcKind::JacobiCoarse && norm_type == 1) {
+            // (r, z) from (r, D^-1 r) and (Z^T r, c): z is formed only inside the direction update
+            const unsigned gu = resident_grid((const void*)pcg_update_rdr_kernel<XT>, n_, kThreads, sm_);
+            pcg_update_rdr_kernel<XT><<<gu, kThreads, 0, s>>>(n_, x, r_.p, p_.p, q_.p, dinv_.p, partials_.p,
+                                                               partials2_.p, st_.p);
+            launch_restrict<XT>(coarse_, r_.p, st_.p, s, sm_);
+            launch_gemv<true>(coarse_, st_.p, s);
+            coarse_final_dir_kernel<XT><<<resident_grid((const void*)coarse_final_dir_kernel<XT>, A_.n_node, kThreads, sm_),
+                                          kThreads, 0, s>>>(A_.n_node, coarse_, r_.p, p_.p, dinv_.p, st_.p);
+            continue;
         } else if (kind_ == PcKind::JacobiCoarse) {
             pcg_update_kernel<XT, false><<<gv, kThreads, 0, s>>>(n_, x, r_.p, z_.p, p_.p, q_.p, nullptr, nullptr,
                                                                   nullptr, st_.p);
             launch_restrict<XT>(coarse_, r_.p, st_.p, s, sm_);
-            coarse_gemv_kernel<<<stride_grid((int64_t)coarse_.kp * 32, kThreads, sm_), kThreads, 0, s>>>(coarse_,
-                                                                                                          st_.p);
+            launch_gemv<false>(coarse_, st_.p, s);
             coarse_final_kernel<XT, false><<<resident_grid((const void*)coarse_final_kernel<XT, false>, A_.n_node, kThreads, sm_), kThreads, 0, s>>>(
                 A_.n_node, coarse_, r_.p, z_.p, p_.p, dinv_.p, partials_.p, partials2_.p, st_.p, 0, 0, 0, 0, norm_type);
         } else {
@@ -1092,8 +1343,7 @@ void Pcg<VT, XT>::record_iterations(const VT* val, XT* x, cudaStream_t s, int n_
             spmv_kernel<FactorT, XT, false><<<gg, kThreads, 0, s>>>(factor_.G, factor_.gval, r_.p, t_.p, nullptr, st_.p);
             if (kind_ == PcKind::FactorCoarse) {
                 launch_restrict<XT>(coarse_, r_.p, st_.p, s, sm_);
-                coarse_gemv_kernel<<<stride_grid((int64_t)coarse_.kp * 32, kThreads, sm_), kThreads, 0, s>>>(coarse_,
-                                                                                                              st_.p);
+                launch_gemv<false>(coarse_, st_.p, s);
             }
             factor_apply_kernel<XT, false><<<gg, kThreads, 0, s>>>(factor_.GT, kind_ == PcKind::FactorCoarse ? coarse_ : CoarseView{},
                                                                     factor_.gtval, t_.p, z_.p, r_.p, p_.p,
@@ -1118,7 +1368,7 @@ int Pcg<VT, XT>::solve(const VT* val, const XT* b, XT* x, double rtol, double ab
         pcg_init_kernel<XT, false><<<gv, kThreads, 0, s>>>(n_, b, x, r_.p, z_.p, p_.p, nullptr, nullptr, nullptr,
                                                             st_.p, rtol, abstol, dtol, maxit, norm_type);
         launch_restrict<XT>(coarse_, r_.p, nullptr, s, sm_);
-        coarse_gemv_kernel<<<stride_grid((int64_t)coarse_.kp * 32, kThreads, sm_), kThreads, 0, s>>>(coarse_, nullptr);
+        launch_gemv<false>(coarse_, nullptr, s);
         coarse_final_kernel<XT, true><<<resident_grid((const void*)coarse_final_kernel<XT, true>, A_.n_node, kThreads, sm_), kThreads, 0, s>>>(
             A_.n_node, coarse_, r_.p, z_.p, p_.p, dinv_.p, partials_.p, partials2_.p, st_.p, rtol, abstol, dtol,
             maxit, norm_type);
@@ -1130,8 +1380,7 @@ int Pcg<VT, XT>::solve(const VT* val, const XT* b, XT* x, double rtol, double ab
         spmv_kernel<FactorT, XT, false><<<gg, kThreads, 0, s>>>(factor_.G, factor_.gval, r_.p, t_.p, nullptr, nullptr);
         if (kind_ == PcKind::FactorCoarse) {
             launch_restrict<XT>(coarse_, r_.p, nullptr, s, sm_);
-            coarse_gemv_kernel<<<stride_grid((int64_t)coarse_.kp * 32, kThreads, sm_), kThreads, 0, s>>>(coarse_,
-                                                                                                          nullptr);
+            launch_gemv<false>(coarse_, nullptr, s);
             launches += 2;
         }
         factor_apply_kernel<XT, true><<<gg, kThreads, 0, s>>>(factor_.GT, kind_ == PcKind::FactorCoarse ? coarse_ : CoarseView{},
@@ -1142,7 +1391,7 @@ int Pcg<VT, XT>::solve(const VT* val, const XT* b, XT* x, double rtol, double ab
     }
     MPHY_CUDA(cudaGetLastError());
     if (!graph_ || graph_val_ != (const void*)val || graph_x_ != (void*)x || graph_stream_ != s ||
-        graph_kind_ != kind_) {
+        graph_kind_ != kind_ || graph_norm_ != norm_type) {
         if (graph_) {
             cudaGraphExecDestroy(graph_);
             graph_ = nullptr;
@@ -1157,8 +1406,12 @@ int Pcg<VT, XT>::solve(const VT* val, const XT* b, XT* x, double rtol, double ab
         graph_x_ = x;
         graph_stream_ = s;
         graph_kind_ = kind_;
+        graph_norm_ = norm_type;
     }
-    const int per_iter = kind_ == PcKind::Jacobi ? 3 : (kind_ == PcKind::Factor ? 5 : (kind_ == PcKind::FactorCoarse ? 7 : 6));
+    const int per_iter = kind_ == PcKind::Jacobi ? 3
+                         : kind_ == PcKind::Factor ? 5
+                         : kind_ == PcKind::FactorCoarse ? 7
+                         : norm_type == 1 ? 5 : 6;
     PcgState h{};
     // every replay advances at most chunk_ iterations; the device stops at maxit
     const int64_t max_replays = (int64_t)(maxit > 0 ? maxit : 0) / chunk_ + 2;

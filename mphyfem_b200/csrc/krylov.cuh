@@ -27,6 +27,10 @@ struct PcgState {
     int32_t maxit;
     uint32_t counter;  // last-CTA detection, reset by the last CTA
     int32_t norm_type; // 0: ||z|| (KSP_NORM_PRECONDITIONED), 1: ||r|| (KSP_NORM_UNPRECONDITIONED)
+    // two-level iteration with ||r||: (r, D^-1 r) and (r, r) from the update, completed by the
+    // coarse GEMV with (Z^T r, c), c = E^-1 Z^T r, into (r, z) (z itself is not formed)
+    double rdr;
+    double rr;
 };
 
 struct SellView {
@@ -110,6 +114,7 @@ class Pcg {
     void* graph_x_ = nullptr;
     cudaStream_t graph_stream_ = nullptr;
     PcKind graph_kind_ = PcKind::Jacobi;
+    int graph_norm_ = -1;
 };
 
 using PcgFp64 = Pcg<double, double>;

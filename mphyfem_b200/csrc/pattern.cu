@@ -417,6 +417,7 @@ void build_pattern(mphy_ctx* ctx, const mphy_mesh* mesh, mphy_pattern* P) {
     pad_missing_rows<<<1, 256, 0, s>>>(nn, P->n_slices, P->slice_base.p, P->slice_width.p, P->sell_col.p);
     check_err(err, s);
 
+
     // element block offsets
     P->e2v.alloc((size_t)ne * npe * npe);
     element_block_offsets<<<grid_for((int64_t)ne * npe * npe, 256, sm), 256, 0, s>>>(

@@ -60,6 +60,8 @@ struct mphy_solver {
     IterativeRefinement<float> ir32;      // MIXED_F32VEC
     Fsai fsai;                            // MPHY_PC_FSAI*
     CoarseSpace coarse;                   // coarse_aggregates > 0
+    bool coarse_ready = false;            // coarse holds an operator formed by an earlier solve
+    int coarse_age = 0;                   // solves since it was formed (coarse_lag)
     mphy_gnn* gnn = nullptr;              // MPHY_PC_FSAI_LEARNED: network run before every solve
     int32_t last_fallback = 0;            // the last solve fell back to Jacobi
     int32_t first_status = 0, first_its = 0;  // the learned attempt of the last solve

@@ -83,21 +83,22 @@ def preconditioner(A, coords, fixed, grid, modes=6):
     return lambda r: r / d + Zk @ sla.cho_solve(cf, Zk.T @ r)
 
 
-def pcg(A, b, Minv, rtol=1e-8, maxit=100000):
-    """KSPCG semantics (preconditioned norm, x0 = 0)."""
+def pcg(A, b, Minv, rtol=1e-8, maxit=100000, norm_type=0):
+    """KSPCG semantics, x0 = 0; the test on ||z|| (norm_type 0, KSP_NORM_PRECONDITIONED) or on
+    ||r|| (norm_type 1, KSP_NORM_UNPRECONDITIONED)."""
     x = np.zeros_like(b)
     r = b.copy()
     z = Minv(r)
     p = z.copy()
     rz = r @ z
-    dp0 = np.linalg.norm(z)
+    dp0 = np.linalg.norm(r if norm_type == 1 else z)
     for i in range(maxit):
         q = A @ p
         a = rz / (p @ q)
         x += a * p
         r -= a * q
         z = Minv(r)
-        if np.linalg.norm(z) <= rtol * dp0:
+        if np.linalg.norm(r if norm_type == 1 else z) <= rtol * dp0:
             return x, i + 1
         rzn = r @ z
         p = z + (rzn / rz) * p

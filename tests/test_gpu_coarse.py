@@ -56,6 +56,42 @@ def test_coarse_matches_restatement_and_oracle(env, oracle, mk, modes):
     assert abs(its - its_ref) <= max(2, 0.03 * its_ref), (its, its_ref)
 
 
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_coarse_with_residual_norm_matches_restatement(env, oracle, prec):
+    """The ||r|| test (the iteration completes (r, z) from (r, D^-1 r) and (Z^T r, E^-1 Z^T r) and
+    forms z only inside the direction update). FP64: iteration count within 3 % of the numpy
+    restatement with the same test, solution to 1e-9 of the FP64 oracle's. Mixed: the solve is of
+    the FP32-stored operator (on this two-phase mesh its solution differs from the FP64 one by
+    the FP32 rounding times the condition number), so it is held to its own FP64 true residual
+    (rtol 1e-10, up to four refinement sweeps) and to the FP64 solve's iteration count (5 %)."""
+    from oracle import fsai_ref, twolevel_ref
+    torch, api, _lib, ctx = env
+    p = meshgen.two_phase_inclusions(32, 8, 8, seed=23, r_range=(0.1, 0.25))
+    precision = _lib.PREC_FP64 if prec == "fp64" else _lib.PREC_MIXED
+    if prec == "mixed":
+        sol, pat, rc, its, x = _solve(api, _lib, ctx, p, torch, rtol=1e-10, coarse_aggregates=24, norm_type=1,
+                                      precision=precision, max_outer=4)
+        assert rc == 0
+        assert sol.true_residual() <= 1e-10
+        _, _, rc64, its64, _ = _solve(api, _lib, ctx, p, torch, rtol=1e-10, coarse_aggregates=24, norm_type=1)
+        assert rc64 == 0 and abs(its - its64) <= max(3, 0.05 * its64), (its, its64)
+        return
+    sol, pat, rc, its, x = _solve(api, _lib, ctx, p, torch, rtol=1e-12, coarse_aggregates=24, norm_type=1)
+    assert rc == 0
+    info = sol.coarse_info()
+    op = oracle.OracleProblem(p)
+    val, _, _, _ = op.assemble(np.zeros(p.n_dof))
+    free = np.flatnonzero(p.fixed == 0)
+    xo, _, _, _ = op.cg(val, 0.2 * p.fnodal[free], rtol=1e-13)
+    assert np.linalg.norm(x[free] - xo) <= 1e-9 * np.linalg.norm(xo)
+    if prec == "fp64":
+        _, _, rp, col = op.pattern()
+        A = fsai_ref.full_operator(p.n_node, p.fixed, rp, col, val)
+        Minv = twolevel_ref.preconditioner(A, p.coords, p.fixed, info["grid"], 6)
+        _, its_ref = twolevel_ref.pcg(A, 0.2 * p.fnodal * (p.fixed == 0), Minv, rtol=1e-12, norm_type=1)
+        assert abs(its - its_ref) <= max(2, 0.03 * its_ref), (its, its_ref)
+
+
 def test_coarse_mixed_and_newton(env):
     torch, api, _lib, ctx = env
     p = meshgen.cantilever_small()
@@ -67,6 +103,45 @@ def test_coarse_mixed_and_newton(env):
     g = np.load(__import__("os").path.join(__import__("os").path.dirname(__file__), "golden", "cantilever_32x8x8.npz"))
     assert res.status == 0
     assert np.abs(res.disp - g["newton_consistent_u"]).max() <= 1e-8 * np.abs(g["newton_consistent_u"]).max()
+
+
+def test_coarse_lag_keeps_the_operator(env, oracle):
+    """coarse_lag = 2: a solve forms the coarse operator and the next two solves keep it (setup
+    time 0), whatever their matrices; each solve still meets its own tolerance, so the solutions
+    agree with the FP64 oracle's on each solve's own matrix. In Newton, the first iteration of
+    every load step forms it afresh, and the converged displacements equal the golden ones."""
+    from tests.golden.make_golden import probe_displacement
+    torch, api, _lib, ctx = env
+    p = meshgen.cantilever_small()
+    mesh = api.Mesh(ctx, p)
+    # the consistent tangent at displacements small enough that it stays positive definite (the
+    # oracle's CG converges on each), as CG needs
+    sol = api.SolverGpu(mesh, api.Pattern(mesh), rtol=1e-12, coarse_aggregates=24, coarse_lag=2, norm_type=1,
+                        tangent=_lib.TANGENT_CONSISTENT)
+    op = oracle.OracleProblem(p)
+    free = np.flatnonzero(p.fixed == 0)
+    formed = []
+    oracle.set_consistent_tangent(True)
+    try:
+        for k in range(4):
+            u = 0.1 * probe_displacement(p, seed=5 + k, amp=0.005)  # small enough for an SPD tangent
+            sol.calcStiffnessAndResidual(torch.tensor(u, device="cuda"))
+            sol.addExternalForces(torch.tensor(p.fnodal, device="cuda"), 0.2)
+            rc, its, _ = sol.factoriseAndSolve()
+            assert rc == 0
+            formed.append(sol.coarse_info()["setup_ms"] > 0.0)
+            val, rhs, _, _ = op.assemble(u)
+            xo, _, _, _ = op.cg(val, rhs + 0.2 * p.fnodal[free], rtol=1e-13)
+            x = sol.solution().cpu().numpy()
+            assert np.linalg.norm(x[free] - xo) <= 1e-9 * np.linalg.norm(xo)
+    finally:
+        oracle.set_consistent_tangent(False)
+    assert formed == [True, False, False, True], formed
+    g = np.load(__import__("os").path.join(__import__("os").path.dirname(__file__), "golden", "cantilever_32x8x8.npz"))
+    fem = api.FemSolidmechanicsGpu(p, ctx, tangent=1, rtol=1e-10, coarse_aggregates=24, coarse_lag=3, norm_type=1)
+    r = fem.solveWithNewtonRaphson(max_newton=15)
+    assert r.status == 0
+    assert np.abs(r.disp - g["newton_consistent_u"]).max() <= 1e-8 * np.abs(g["newton_consistent_u"]).max()
 
 
 def test_linear_modes_need_fewer_iterations(env):
