@@ -318,6 +318,48 @@ def _time_leg(torch, api, _lib, mesh, pat, args, prob, disp, fext, dev, method, 
     return out
 
 
+def _other_workloads(torch, api, _lib, args, dev):
+    """The two other GPU workloads of the north star, measured in the default run so that their
+    figures come from the same run as the headline (each after the headline's buffers are freed):
+      - tet10: the 10-node-tet Kuhn cantilever 96(x) x 48 x 48 (1.33 M elements, 5.45 M DOFs),
+        near-incompressible (kappa = 100), the headline's method, one Newton iteration from u = 0
+        (one untimed, two timed);
+      - batched: 512 independent hex8 blocks (batched_blocks(512, seed=11), 2.09 M elements,
+        7.79 M DOFs), FP64, consistent tangent, persistent cluster PCG with 8 rigid-body slabs per
+        instance on the (2 CTAs, 512 threads) schedule, every instance's 5 load steps with Newton
+        to 1e-8 and PCG to true residual 1e-10: one whole job, timed by the library's events."""
+    from mphyfem_b200 import meshgen, ranks
+    out = {}
+    q = meshgen.tet10_kuhn(96, 48, 48)
+    mesh = api.Mesh(api.Context(0), q)
+    pat = api.Pattern(mesh)
+    disp = torch.zeros(q.n_dof, dtype=torch.float64, device=dev)
+    fext = torch.tensor(q.fnodal, device=dev)
+    leg = _time_leg(torch, api, _lib, mesh, pat, args, q, disp, fext, dev, (args.precision, args.pc, args.coarse), 2)
+    leg.update({"workload": f"{q.name}: {q.n_elem} tet10 elements, {q.n_dof} DOFs, one Newton iteration from u = 0 at "
+                            f"lambda = {q.dt:g}, PCG to true relative residual {args.rtol:g}",
+                "melems_per_s_assembly": q.n_elem / (leg["assembly_ms"] * 1e-3) / 1e6})
+    out["tet10_gpu"] = leg
+    del mesh, pat, disp, fext
+    allp = meshgen.batched_blocks(512, seed=11)
+    for b in allp:
+        b.newton_rtol = 1e-8
+    ctx = api.Context(0)
+    _, bat = ranks.batched_share(allp, 0, 1, ctx, schedule=(2, 512), coarse_slabs=8, precision=_lib.PREC_FP64,
+                                 rtol=1e-10, norm_type=1, max_it=args.max_it, tangent=_lib.TANGENT_CONSISTENT)
+    o = bat.newton_run(max_newton=15)
+    out["batched_gpu"] = {
+        "workload": "batched_blocks(512, seed=11): 512 hex8 blocks, nx, ny ~ U{4..16}, nz ~ U{16..64}, 5 load steps "
+                    "each, Newton to 1e-8, PCG to true relative residual 1e-10, FP64, 8 rigid-body slabs",
+        "n_elem": sum(b.n_elem for b in allp), "n_dof": sum(b.n_dof for b in allp),
+        "ms_per_job": o["stats"]["t_ms"], "instances_per_s": len(allp) / (o["stats"]["t_ms"] * 1e-3),
+        "graph_replays": o["stats"]["graph_replays"], "kernel_launches": o["stats"]["kernel_launches"],
+        "krylov_its_mean": float(o["krylov_its"].mean()), "cuts": int(o["cuts"].sum()),
+        "instances_ok": int((o["status"] == 0).sum()), "schedule": list(bat.schedule())}
+    bat.close()
+    return out
+
+
 def _parity_first_step(api, _lib, mesh, pat, args, prob, legs, newton_rtol=1e-8, max_newton=15):
     """Accuracy at the workload's size: the first load step (lambda = dt from u = 0) converged to
     ||R|| < newton_rtol ||R_first|| with the consistent tangent (the reference's tangent need not
@@ -415,17 +457,18 @@ def run_ours(args):
     coarse = sol.coarse_info() if args.coarse > 0 else None
     pc_info = sol.pc_last() if args.pc != "jacobi" else None
 
-    # dominant kernel: the SpMV of the Krylov loop, timed standalone with events on its stream
+    # dominant kernel: the SpMV of the Krylov loop (the same kernel: y = A p with the fused p.Ap),
+    # timed back to back with events on its stream; each call also zeroes its 96-byte state
     mi = sol.matrix_info()
     x = torch.randn(prob.n_dof, dtype=torch.float64, device=dev)
     y = torch.empty_like(x)
     for _ in range(3):
-        sol.spmv(x, y)
+        sol.spmv_dot(x, y, want_dot=False)
     nrep = 20
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(nrep):
-        sol.spmv(x, y)
+        sol.spmv_dot(x, y, want_dot=False)
     e1.record(stream)
     torch.cuda.synchronize()
     spmv_ms = e0.elapsed_time(e1) / nrep
@@ -466,7 +509,7 @@ def run_ours(args):
     # the other methods on the same workload and step, measured in the same run (1 GPU): the
     # plain GPU method (FP64 Jacobi-PCG, the drop-in for the reference's KSPCG + PCJACOBI) and the
     # learned factorised preconditioner with the same coarse space
-    plain = learned_leg = parity = None
+    plain = learned_leg = parity = others = None
     headline = (args.precision, args.pc, args.coarse)
     if world == 1:
         sol.close()
@@ -486,6 +529,8 @@ def run_ours(args):
             parity = _parity_first_step(api, _lib, mesh, pat, args, prob, legs)
             if learned_leg is not None:
                 learned_leg["disp_err_vs_fp64"] = parity["learned"]["disp_err_vs_fp64"]
+        if not args.no_others and args.workload == "large":
+            others = _other_workloads(torch, api, _lib, args, dev)
 
     if rank != 0:
         if world > 1:
@@ -517,10 +562,12 @@ def run_ours(args):
                      "frac": asm_bytes / (asm_ms * 1e-3) / 1e9 / peak},
         "plain_gpu": plain,
         "learned_gpu": learned_leg,
+        "other_workloads": others,
         "parity": parity,
         "e2e": {"value": world * 1e3 / e2e_ms, "unit": "Newton iter/s", "h2d_bytes_per_step": 2 * prob.n_dof * 8,
                 "d2h_bytes_per_step": prob.n_dof * 8},
-        "roofline": {"kernel": f"spmv_kernel (SELL-32 3x3, {'FP64' if vbytes == 8 else 'FP32'} values, FP64 vectors)",
+        "roofline": {"kernel": f"spmv_kernel with p.Ap, as in the CG iteration (SELL-32 3x3, "
+                               f"{'FP64' if vbytes == 8 else 'FP32 off-diagonal'} values, FP64 vectors)",
                      "bound": "hbm", "achieved": achieved, "peak": peak, "peak_source": peak_kind, "unit": "GB/s",
                      "frac": achieved / peak,
                      "traffic": _read_traffic("spmv_fp64" if vbytes == 8 else "spmv_mixed"),
@@ -618,6 +665,8 @@ def main():
                     help="skip the same-run measurement of the learned factorised preconditioner")
     ap.add_argument("--no-parity", dest="no_parity", action="store_true",
                     help="skip the first-load-step accuracy check against the FP64 GPU solution")
+    ap.add_argument("--no-others", dest="no_others", action="store_true",
+                    help="skip the tet10 and batched workloads measured after the headline")
     args = ap.parse_args()
     if args.impl == "reference" and args.workload == "batched":
         if int(os.environ.get("RANK", "0")) == 0:

@@ -275,6 +275,9 @@ int mphy_solver_rhs_norm(mphy_solver* s, double* norm_host);
 int mphy_solver_solve(mphy_solver* s, int32_t* its, double* final_norm);
 /* y = A x with the assembled matrix (MatMult), x_dev / y_dev: [3*n_node] FP64. */
 int mphy_solver_spmv(mphy_solver* s, const double* x_dev, double* y_dev);
+/* y = A x and (x, y) in one pass (MatMult followed by VecDot): the SpMV kernel that the CG
+ * iteration runs. *xy_host (may be NULL: no copy and no host wait) receives (x, y). */
+int mphy_solver_spmv_dot(mphy_solver* s, const double* x_dev, double* y_dev, double* xy_host);
 /* Sizes of the assembled operator: stored 3x3 blocks (with padding), true blocks, value bytes. */
 int mphy_solver_matrix_info(const mphy_solver* s, int64_t* stored_blocks, int64_t* true_blocks,
                             int64_t* value_bytes);

@@ -119,6 +119,7 @@ SIGNATURES = {
     "mphy_solver_rhs_norm": (C.c_int, [_vp, _d]),
     "mphy_solver_solve": (C.c_int, [_vp, _i32, _d]),
     "mphy_solver_spmv": (C.c_int, [_vp, _vp, _vp]),
+    "mphy_solver_spmv_dot": (C.c_int, [_vp, _vp, _vp, _d]),
     "mphy_solver_matrix_info": (C.c_int, [_vp, _i64, _i64, _i64]),
     "mphy_solver_pc_pattern": (C.c_int, [_vp, _i64, _i64, _i32]),
     "mphy_solver_pc_get_blocks": (C.c_int, [_vp, _vp]),

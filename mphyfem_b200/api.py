@@ -197,6 +197,13 @@ class SolverGpu:
         """y = A x with the assembled operator (MatMult); ordered on the library stream."""
         L.check(self.lib.mphy_solver_spmv(self.h, _ptr(x_dev), _ptr(y_dev)))
 
+    def spmv_dot(self, x_dev, y_dev, want_dot: bool = True):
+        """y = A x and (x, y) in one pass, the CG iteration's SpMV kernel; returns (x, y) (or None
+        without a host wait when want_dot is False)."""
+        v = C.c_double()
+        L.check(self.lib.mphy_solver_spmv_dot(self.h, _ptr(x_dev), _ptr(y_dev), C.byref(v) if want_dot else None))
+        return v.value if want_dot else None
+
     def matrix_info(self):
         a, b, c = C.c_int64(), C.c_int64(), C.c_int64()
         L.check(self.lib.mphy_solver_matrix_info(self.h, C.byref(a), C.byref(b), C.byref(c)))

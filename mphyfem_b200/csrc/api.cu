@@ -913,6 +913,28 @@ int mphy_solver_spmv(mphy_solver* s, const double* x, double* y) {
     });
 }
 
+int mphy_solver_spmv_dot(mphy_solver* s, const double* x, double* y, double* xy_host) {
+    return guarded([&] {
+        MPHY_REQUIRE(s && x && y, MPHY_ERR_INVALID_ARG, "null argument");
+        if (!s->dot_st.p) {
+            s->dot_st.alloc(1);
+            s->dot_part.alloc((size_t)s->ctx->sm_count * 8 + 8);
+        }
+        cudaStream_t st = s->ctx->stream;
+        if (s->mixed)
+            spmv_dot<float, double>(s->A, s->valf.p, x, y, s->dot_part.p, s->dot_st.p, st, s->ctx->sm_count);
+        else spmv_dot<double, double>(s->A, s->val.p, x, y, s->dot_part.p, s->dot_st.p, st, s->ctx->sm_count);
+        s->launches += 1;
+        if (xy_host) {
+            PcgState h{};
+            MPHY_CUDA(cudaMemcpyAsync(&h, s->dot_st.p, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
+            MPHY_CUDA(cudaStreamSynchronize(st));
+            *xy_host = h.pq;
+        }
+        return (int)MPHY_OK;
+    });
+}
+
 int mphy_solver_matrix_info(const mphy_solver* s, int64_t* stored, int64_t* true_blocks, int64_t* value_bytes) {
     if (!s) return MPHY_ERR_INVALID_ARG;
     if (stored) *stored = s->pat->sell_blocks;

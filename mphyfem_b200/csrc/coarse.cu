@@ -454,16 +454,18 @@ __global__ void __launch_bounds__(kPotrfThreads) potrf_inv_tile(double* E, doubl
             const double f = il * il;
             if (tid == 0) rd[c] = il;
             if (owner && P >= cq) {
+                // rows <= c and columns <= c take a zero factor, so the 16 updates need no
+                // predicates (the strictly upper entries of a diagonal patch change too; they are
+                // never read and never written out)
                 double ci[4], cf[4];
 #pragma unroll
-                for (int a = 0; a < 4; ++a) ci[a] = colv[buf][r0 + a];
+                for (int a = 0; a < 4; ++a) ci[a] = r0 + a > c ? colv[buf][r0 + a] : 0.0;
 #pragma unroll
-                for (int b = 0; b < 4; ++b) cf[b] = colv[buf][c0 + b] * f;
+                for (int b = 0; b < 4; ++b) cf[b] = c0 + b > c ? colv[buf][c0 + b] * f : 0.0;
 #pragma unroll
                 for (int a = 0; a < 4; ++a)
 #pragma unroll
-                    for (int b = 0; b < 4; ++b)
-                        if (c0 + b > c && c0 + b <= r0 + a) A[a][b] = fma(-ci[a], cf[b], A[a][b]);
+                    for (int b = 0; b < 4; ++b) A[a][b] = fma(-ci[a], cf[b], A[a][b]);
                 if (Q == cq) {
 #pragma unroll
                     for (int a = 0; a < 4; ++a)
@@ -490,17 +492,17 @@ __global__ void __launch_bounds__(kPotrfThreads) potrf_inv_tile(double* E, doubl
             }
             __syncthreads();
             if (owner && P >= iq) {
+                // zero factors for rows <= i and columns > i, as above
                 const double ri = rd[i];
                 double lm[4], bl[4];
 #pragma unroll
-                for (int a = 0; a < 4; ++a) lm[a] = colv[buf][r0 + a] * ri;
+                for (int a = 0; a < 4; ++a) lm[a] = r0 + a > i ? colv[buf][r0 + a] * ri : 0.0;
 #pragma unroll
-                for (int b = 0; b < 4; ++b) bl[b] = rowv[buf][c0 + b];
+                for (int b = 0; b < 4; ++b) bl[b] = c0 + b <= i ? rowv[buf][c0 + b] : 0.0;
 #pragma unroll
                 for (int a = 0; a < 4; ++a)
 #pragma unroll
-                    for (int b = 0; b < 4; ++b)
-                        if (r0 + a > i && c0 + b <= i) B[a][b] = fma(-lm[a], bl[b], B[a][b]);
+                    for (int b = 0; b < 4; ++b) B[a][b] = fma(-lm[a], bl[b], B[a][b]);
             }
         }
     }

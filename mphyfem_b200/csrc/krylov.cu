@@ -1186,6 +1186,19 @@ template void spmv<double, double>(const SellView&, const double*, const double*
 template void spmv<float, float>(const SellView&, const float*, const float*, float*, cudaStream_t, int);
 template void spmv<float, double>(const SellView&, const float*, const double*, double*, cudaStream_t, int);
 
+template <typename VT, typename XT>
+void spmv_dot(const SellView& A, const VT* val, const XT* x, XT* y, double* partials, PcgState* st, cudaStream_t s,
+              int sm) {
+    MPHY_CUDA(cudaMemsetAsync(st, 0, sizeof(PcgState), s));
+    const unsigned g = resident_grid((const void*)spmv_kernel<VT, XT, true>, (int64_t)A.n_slices * 32, kThreads, sm);
+    spmv_kernel<VT, XT, true><<<g, kThreads, 0, s>>>(A, val, x, y, partials, st);
+    MPHY_CUDA(cudaGetLastError());
+}
+template void spmv_dot<double, double>(const SellView&, const double*, const double*, double*, double*, PcgState*,
+                                       cudaStream_t, int);
+template void spmv_dot<float, double>(const SellView&, const float*, const double*, double*, double*, PcgState*,
+                                      cudaStream_t, int);
+
 template <typename VT>
 void residual_fp64(const SellView& A, const VT* val, const double* x, const double* b, double* r, double* partials,
                    uint32_t* counter, double* out_dev, cudaStream_t s, int sm) {

@@ -67,6 +67,11 @@ unsigned resident_grid(const void* kernel, int64_t n, int threads, int sm_count)
 // y = A x.
 template <typename VT, typename XT>
 void spmv(const SellView& A, const VT* val, const XT* x, XT* y, cudaStream_t s, int sm);
+// y = A x and st->pq = (x, y) in one pass: the SpMV kernel of the CG iteration, on a scratch
+// state (zeroed first) and a partials buffer of at least 8 entries per SM
+template <typename VT, typename XT>
+void spmv_dot(const SellView& A, const VT* val, const XT* x, XT* y, double* partials, PcgState* st, cudaStream_t s,
+              int sm);
 
 // r = b - A x in FP64 (A in VT), and ||r||^2 into *out_dev; partials [sm*8+8], counter zeroed.
 template <typename VT>

@@ -55,6 +55,8 @@ struct mphy_solver {
     DevBuf<double> disp_prev2, du_full, x_first, arc_dots;  // arc-length continuation
     DevBuf<double> ref_r, ref_d;          // FP64 refinement sweeps (max_outer > 1), true residual
     DevBuf<float> pred_blocks;            // network-predicted G blocks (learned FSAI)
+    DevBuf<PcgState> dot_st;              // mphy_solver_spmv_dot scratch
+    DevBuf<double> dot_part;
     PcgFp64 pcg;
     IterativeRefinement<double> ir;       // MIXED
     IterativeRefinement<float> ir32;      // MIXED_F32VEC

@@ -109,3 +109,28 @@ def test_spmv_natural_and_permuted_numbering(api, ctx, torch, prec):
     tol = 1e-12 if prec == "fp64" else 1e-6
     assert np.abs(yq[free] - y_nat[free]).max() <= tol * np.abs(y_nat[free]).max()
     sol.close()
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_spmv_dot_is_the_spmv_with_its_dot(api, ctx, torch, prec):
+    """mphy_solver_spmv_dot (the CG iteration's SpMV kernel with the fused (x, Ax)) gives the same
+    y as mphy_solver_spmv, bit for bit, and (x, y) to 1e-11 of torch's FP64 dot (both are FP64
+    sums of ~10^5 terms in different orders)."""
+    from mphyfem_b200 import _lib
+    from tests.golden.make_golden import probe_displacement
+    precision = _lib.PREC_FP64 if prec == "fp64" else _lib.PREC_MIXED
+    p = meshgen.hex8_cantilever(48, 12, 12)
+    mesh = api.Mesh(ctx, p)
+    sol = api.SolverGpu(mesh, api.Pattern(mesh), precision=precision)
+    sol.calcStiffnessAndResidual(torch.tensor(probe_displacement(p, amp=0.001), device="cuda"))
+    x = torch.tensor(np.random.default_rng(3).standard_normal(p.n_dof), device="cuda")
+    x[torch.tensor(p.fixed == 1, device="cuda")] = 0.0
+    y1 = torch.empty_like(x)
+    y2 = torch.empty_like(x)
+    sol.spmv(x, y1)
+    xy = sol.spmv_dot(x, y2)
+    torch.cuda.synchronize()
+    assert torch.equal(y1, y2)
+    ref = float(torch.dot(x, y2))
+    assert abs(xy - ref) <= 1e-11 * abs(ref)
+    sol.close()
