@@ -47,19 +47,23 @@ __global__ void centroid_kernel(int32_t n_agg, const int64_t* __restrict__ agg_p
     }
 }
 
+// d_n = (x_n - c_a) / H, stored in FP32: the offsets only choose the coarse basis Z, and every
+// kernel (E = Z^T A Z, restriction, prolongation) reads the same rounded values, so Z stays one
+// basis while the per-iteration kernels read half the bytes
 __global__ void offsets_kernel(int32_t n_node, const int32_t* __restrict__ agg, const double* __restrict__ X,
                                const double* __restrict__ u, const double* __restrict__ cent, double inv_h,
-                               double* __restrict__ d) {
+                               float* __restrict__ d) {
     for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < n_node; n += (int64_t)gridDim.x * blockDim.x) {
         const int a = agg[n];
-        for (int k = 0; k < 3; ++k) d[3 * n + k] = (X[3 * n + k] + (u ? u[3 * n + k] : 0.0) - cent[3 * a + k]) * inv_h;
+        for (int k = 0; k < 3; ++k)
+            d[3 * n + k] = (float)((X[3 * n + k] + (u ? u[3 * n + k] : 0.0) - cent[3 * a + k]) * inv_h);
     }
 }
 
 // d and the prescribed-DOF mask in the order of the aggregates' node lists, so that the
 // per-iteration restriction reads them coalesced and without waiting for the node index
-__global__ void permute_offsets_kernel(int32_t n_node, const int32_t* __restrict__ nodes, const double* __restrict__ d,
-                                       double* __restrict__ dperm) {
+__global__ void permute_offsets_kernel(int32_t n_node, const int32_t* __restrict__ nodes, const float* __restrict__ d,
+                                       float* __restrict__ dperm) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n_node; i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t n = nodes[i];
         for (int k = 0; k < 3; ++k) dperm[3 * i + k] = d[3 * n + k];

@@ -48,7 +48,8 @@ class CoarseSpace {
     int n_agg_ = 0, kp_ = 0;
     DevBuf<int32_t> agg_, agg_nodes_, err_;
     DevBuf<int64_t> agg_ptr_;
-    DevBuf<double> d_, cent_, E_, W_, w_, c_;
+    DevBuf<float> d_;       // FP32 offsets (x_n - c_a) / H
+    DevBuf<double> cent_, E_, W_, w_, c_;
     DevBuf<double> einv_;     // lower tiles of E^{-1}
     DevBuf<double> gpart_, wcrow_;
     DevBuf<uint32_t> gcount_;
@@ -56,7 +57,7 @@ class CoarseSpace {
     DevBuf<double> wpart_;
     DevBuf<uint32_t> wcount_;
     DevBuf<double> epart_;  // per-part results of the E = Z^T A Z kernel
-    DevBuf<double> dperm_;  // d in agg_nodes order
+    DevBuf<float> dperm_;   // d in agg_nodes order
     DevBuf<uint8_t> fperm_; // fixed in agg_nodes order
 };
 

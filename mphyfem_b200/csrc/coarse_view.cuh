@@ -15,9 +15,9 @@ struct CoarseView {
     const int32_t* agg;      // [n_node] aggregate of every node
     const int64_t* agg_ptr;  // [n_agg+1] nodes of every aggregate (in agg_nodes)
     const int32_t* agg_nodes;
-    const double* d;         // [n_node][3] (x_n - c_agg) / H_agg at setup
+    const float* d;          // [n_node][3] (x_n - c_agg) / H_agg at setup, FP32 (one rounded basis)
     const uint8_t* fixed;    // [3 n_node]
-    const double* dperm;     // [n_node][3] d in the order of agg_nodes (the restriction's loads)
+    const float* dperm;      // [n_node][3] d in the order of agg_nodes (the restriction's loads)
     const uint8_t* fperm;    // [3 n_node] fixed in the order of agg_nodes
     int32_t nb;              // kp / 64 tiles per side
     // inverse of E, FP64, symmetric: its lower 64x64 tiles (I, J), J <= I, at tile index

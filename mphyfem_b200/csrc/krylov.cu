@@ -457,24 +457,25 @@ __global__ void __launch_bounds__(kThreads) pcg_update_kernel(int64_t n, XT* __r
 template <typename XT>
 __global__ void __launch_bounds__(kThreads) pcg_update_rdr_kernel(int64_t n, XT* __restrict__ x, XT* __restrict__ r,
                                                                   const XT* __restrict__ p, const XT* __restrict__ q,
-                                                                  const XT* __restrict__ dinv,
+                                                                  const float* __restrict__ dinv,
                                                                   double* __restrict__ part_a,
                                                                   double* __restrict__ part_b, PcgState* st) {
     __shared__ double sh[32];
     if (st->done) return;
     const XT alpha = (XT)st->alpha;
     double a1 = 0.0, a2 = 0.0;
-    if (aligned16(x, r, p, q) && aligned16(dinv, dinv, dinv, dinv)) {
+    if (aligned16(x, r, p, q) && (reinterpret_cast<uintptr_t>(dinv) & 7) == 0) {
         using V = typename Pair<XT>::type;
         const int64_t n2 = n >> 1;
         V* x2 = reinterpret_cast<V*>(x);
         V* r2 = reinterpret_cast<V*>(r);
         const V* p2 = reinterpret_cast<const V*>(p);
         const V* q2 = reinterpret_cast<const V*>(q);
-        const V* d2 = reinterpret_cast<const V*>(dinv);
+        const float2* d2 = reinterpret_cast<const float2*>(dinv);
         for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n2; i += (int64_t)gridDim.x * blockDim.x) {
             V xv = ld_once(x2 + i), rv = r2[i];
-            const V pv = p2[i], qv = ld_once(q2 + i), dv = d2[i];
+            const V pv = p2[i], qv = ld_once(q2 + i);
+            const float2 dv = d2[i];
             xv.x = xv.x + alpha * pv.x;
             xv.y = xv.y + alpha * pv.y;
             rv.x = rv.x - alpha * qv.x;
@@ -837,7 +838,7 @@ void launch_gemv(const CoarseView& cv, PcgState* st, cudaStream_t s) {
 template <typename XT, bool INIT>
 __global__ void __launch_bounds__(kThreads) coarse_final_kernel(int32_t n_node, CoarseView cv, const XT* __restrict__ r,
                                                                 XT* __restrict__ z, XT* __restrict__ p,
-                                                                const XT* __restrict__ dinv,
+                                                                const float* __restrict__ dinv,
                                                                 double* __restrict__ part_rz,
                                                                 double* __restrict__ part_zz, PcgState* st,
                                                                 double rtol, double abstol, double dtol, int maxit,
@@ -849,23 +850,25 @@ __global__ void __launch_bounds__(kThreads) coarse_final_kernel(int32_t n_node, 
     // a thread takes the adjacent nodes 2t and 2t + 1: their six DOFs of r, D^-1, z (and p) and
     // their six offsets are three paired accesses each; every load comes before the first store
     using V = typename Pair<XT>::type;
-    const bool paired = aligned16(r, z, dinv, INIT ? (const void*)p : (const void*)z) && aligned16(cv.d, cv.d, cv.d, cv.d);
+    const bool paired = aligned16(r, z, INIT ? (const void*)p : (const void*)z, z);
     const int64_t npair = ((int64_t)n_node + 1) >> 1;
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < npair; t += (int64_t)gridDim.x * blockDim.x) {
         const int64_t n0 = 2 * t;
         const int cnt = n0 + 1 < n_node ? 2 : 1;
-        XT rv[6], dv[6];
+        XT rv[6];
+        float dv[6];
         double od[6];
         uint8_t fx[6];
         int32_t ag[2];
         if (cnt == 2 && paired) {
             const V* r2 = reinterpret_cast<const V*>(r + 3 * n0);
-            const V* v2 = reinterpret_cast<const V*>(dinv + 3 * n0);
-            const double2* o2 = reinterpret_cast<const double2*>(cv.d + 3 * n0);
+            const float2* v2 = reinterpret_cast<const float2*>(dinv + 3 * n0);
+            const float2* o2 = reinterpret_cast<const float2*>(cv.d + 3 * n0);
 #pragma unroll
             for (int q = 0; q < 3; ++q) {
-                const V a = r2[q], b = v2[q];
-                const double2 o = o2[q];
+                const V a = r2[q];
+                const float2 b = v2[q];
+                const float2 o = o2[q];
                 rv[2 * q] = a.x;
                 rv[2 * q + 1] = a.y;
                 dv[2 * q] = b.x;
@@ -878,8 +881,8 @@ __global__ void __launch_bounds__(kThreads) coarse_final_kernel(int32_t n_node, 
             for (int e = 0; e < 6; ++e) {
                 const bool in = e < 3 * cnt;
                 rv[e] = in ? r[3 * n0 + e] : XT(0);
-                dv[e] = in ? dinv[3 * n0 + e] : XT(0);
-                od[e] = in ? cv.d[3 * n0 + e] : 0.0;
+                dv[e] = in ? dinv[3 * n0 + e] : 0.0f;
+                od[e] = in ? (double)cv.d[3 * n0 + e] : 0.0;
             }
         }
 #pragma unroll
@@ -943,28 +946,30 @@ __global__ void __launch_bounds__(kThreads) coarse_final_kernel(int32_t n_node, 
 template <typename XT>
 __global__ void __launch_bounds__(kThreads) coarse_final_dir_kernel(int32_t n_node, CoarseView cv,
                                                                     const XT* __restrict__ r, XT* __restrict__ p,
-                                                                    const XT* __restrict__ dinv, const PcgState* st) {
+                                                                    const float* __restrict__ dinv, const PcgState* st) {
     if (st->done) return;
     const XT beta = (XT)st->beta;
     using V = typename Pair<XT>::type;
-    const bool paired = aligned16(r, p, dinv, cv.d);
+    const bool paired = aligned16(r, p, r, p);
     const int64_t npair = ((int64_t)n_node + 1) >> 1;
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < npair; t += (int64_t)gridDim.x * blockDim.x) {
         const int64_t n0 = 2 * t;
         const int cnt = n0 + 1 < n_node ? 2 : 1;
-        XT rv[6], dv[6], pv[6];
+        XT rv[6], pv[6];
+        float dv[6];
         double od[6];
         uint8_t fx[6];
         int32_t ag[2];
         if (cnt == 2 && paired) {
             const V* r2 = reinterpret_cast<const V*>(r + 3 * n0);
-            const V* v2 = reinterpret_cast<const V*>(dinv + 3 * n0);
+            const float2* v2 = reinterpret_cast<const float2*>(dinv + 3 * n0);
             const V* p2 = reinterpret_cast<const V*>(p + 3 * n0);
-            const double2* o2 = reinterpret_cast<const double2*>(cv.d + 3 * n0);
+            const float2* o2 = reinterpret_cast<const float2*>(cv.d + 3 * n0);
 #pragma unroll
             for (int q = 0; q < 3; ++q) {
-                const V a = r2[q], b = v2[q], c = p2[q];
-                const double2 o = o2[q];
+                const V a = r2[q], c = p2[q];
+                const float2 b = v2[q];
+                const float2 o = o2[q];
                 rv[2 * q] = a.x;
                 rv[2 * q + 1] = a.y;
                 dv[2 * q] = b.x;
@@ -979,9 +984,9 @@ __global__ void __launch_bounds__(kThreads) coarse_final_dir_kernel(int32_t n_no
             for (int e = 0; e < 6; ++e) {
                 const bool in = e < 3 * cnt;
                 rv[e] = in ? r[3 * n0 + e] : XT(0);
-                dv[e] = in ? dinv[3 * n0 + e] : XT(0);
+                dv[e] = in ? dinv[3 * n0 + e] : 0.0f;
                 pv[e] = in ? p[3 * n0 + e] : XT(0);
-                od[e] = in ? cv.d[3 * n0 + e] : 0.0;
+                od[e] = in ? (double)cv.d[3 * n0 + e] : 0.0;
             }
         }
 #pragma unroll
@@ -1310,6 +1315,7 @@ void Pcg<VT, XT>::init(const SellView& A, int sm_count, int chunk) {
     q_.alloc(n_);
     t_.alloc(n_);
     dinv_.alloc(n_);
+    dinv32_.alloc(n_);
     const size_t np = (size_t)sm_ * 8 + 8;
     partials_.alloc(np);
     partials2_.alloc(np);
@@ -1334,12 +1340,12 @@ void Pcg<VT, XT>::record_iterations(const VT* val, XT* x, cudaStream_t s, int n_
         } else if (kind_ == PcKind::JacobiCoarse && norm_type == 1) {
             // (r, z) from (r, D^-1 r) and (Z^T r, c): z is formed only inside the direction update
             const unsigned gu = resident_grid((const void*)pcg_update_rdr_kernel<XT>, n_, kThreads, sm_);
-            pcg_update_rdr_kernel<XT><<<gu, kThreads, 0, s>>>(n_, x, r_.p, p_.p, q_.p, dinv_.p, partials_.p,
+            pcg_update_rdr_kernel<XT><<<gu, kThreads, 0, s>>>(n_, x, r_.p, p_.p, q_.p, dinv32_.p, partials_.p,
                                                                partials2_.p, st_.p);
             launch_restrict<XT>(coarse_, r_.p, st_.p, s, sm_);
             launch_gemv<true>(coarse_, st_.p, s);
             coarse_final_dir_kernel<XT><<<resident_grid((const void*)coarse_final_dir_kernel<XT>, A_.n_node, kThreads, sm_),
-                                          kThreads, 0, s>>>(A_.n_node, coarse_, r_.p, p_.p, dinv_.p, st_.p);
+                                          kThreads, 0, s>>>(A_.n_node, coarse_, r_.p, p_.p, dinv32_.p, st_.p);
             continue;
         } else if (kind_ == PcKind::JacobiCoarse) {
             pcg_update_kernel<XT, false><<<gv, kThreads, 0, s>>>(n_, x, r_.p, z_.p, p_.p, q_.p, nullptr, nullptr,
@@ -1347,7 +1353,7 @@ void Pcg<VT, XT>::record_iterations(const VT* val, XT* x, cudaStream_t s, int n_
             launch_restrict<XT>(coarse_, r_.p, st_.p, s, sm_);
             launch_gemv<false>(coarse_, st_.p, s);
             coarse_final_kernel<XT, false><<<resident_grid((const void*)coarse_final_kernel<XT, false>, A_.n_node, kThreads, sm_), kThreads, 0, s>>>(
-                A_.n_node, coarse_, r_.p, z_.p, p_.p, dinv_.p, partials_.p, partials2_.p, st_.p, 0, 0, 0, 0, norm_type);
+                A_.n_node, coarse_, r_.p, z_.p, p_.p, dinv32_.p, partials_.p, partials2_.p, st_.p, 0, 0, 0, 0, norm_type);
         } else {
             pcg_update_kernel<XT, false><<<gv, kThreads, 0, s>>>(n_, x, r_.p, z_.p, p_.p, q_.p, nullptr, nullptr,
                                                                   nullptr, st_.p);
@@ -1377,13 +1383,15 @@ int Pcg<VT, XT>::solve(const VT* val, const XT* b, XT* x, double rtol, double ab
                                                            partials2_.p, st_.p, rtol, abstol, dtol, maxit, norm_type);
         launches += 2;
     } else if (kind_ == PcKind::JacobiCoarse) {
-        jacobi_kernel<VT, XT><<<stride_grid(A_.n_node, kThreads, sm_), kThreads, 0, s>>>(A_, val, dinv_.p);
+        // the two-level kernels read D^-1 in FP32: a rounded Jacobi preconditioner, the same in
+        // every application
+        jacobi_kernel<VT, float><<<stride_grid(A_.n_node, kThreads, sm_), kThreads, 0, s>>>(A_, val, dinv32_.p);
         pcg_init_kernel<XT, false><<<gv, kThreads, 0, s>>>(n_, b, x, r_.p, z_.p, p_.p, nullptr, nullptr, nullptr,
                                                             st_.p, rtol, abstol, dtol, maxit, norm_type);
         launch_restrict<XT>(coarse_, r_.p, nullptr, s, sm_);
         launch_gemv<false>(coarse_, nullptr, s);
         coarse_final_kernel<XT, true><<<resident_grid((const void*)coarse_final_kernel<XT, true>, A_.n_node, kThreads, sm_), kThreads, 0, s>>>(
-            A_.n_node, coarse_, r_.p, z_.p, p_.p, dinv_.p, partials_.p, partials2_.p, st_.p, rtol, abstol, dtol,
+            A_.n_node, coarse_, r_.p, z_.p, p_.p, dinv32_.p, partials_.p, partials2_.p, st_.p, rtol, abstol, dtol,
             maxit, norm_type);
         launches += 5;
     } else {

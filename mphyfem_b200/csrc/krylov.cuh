@@ -112,6 +112,7 @@ class Pcg {
     int sm_ = 148, chunk_ = 32;
     int64_t n_ = 0;
     DevBuf<XT> r_, z_, p_, q_, t_, dinv_;
+    DevBuf<float> dinv32_;  // D^-1 of the two-level (Jacobi + coarse) iteration
     DevBuf<double> partials_, partials2_;
     DevBuf<PcgState> st_;
     cudaGraphExec_t graph_ = nullptr;
