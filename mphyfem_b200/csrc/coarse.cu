@@ -733,7 +733,7 @@ void CoarseSpace::init(mphy_ctx* ctx, const mphy_mesh* mesh, const mphy_pattern*
     einv_.alloc(tiles * T * T);
     gpart_.alloc(tiles * 2 * T);
     gcount_.alloc(nb + 1);
-    wcrow_.alloc(nb);
+    tilewc_.alloc(tiles);
     w_.alloc(kp_);
     c_.alloc(kp_);
     wpart_.alloc((size_t)n_agg_ * kMaxRestrictParts * nm_);
@@ -919,7 +919,7 @@ CoarseView CoarseSpace::view() const {
     v.nb = kp_ / T;
     v.gpart = gpart_.p;
     v.gcount = gcount_.p;
-    v.wcrow = wcrow_.p;
+    v.tilewc = tilewc_.p;
     v.w = w_.p;
     v.wpart = wpart_.p;
     v.wcount = wcount_.p;

@@ -51,7 +51,7 @@ class CoarseSpace {
     DevBuf<float> d_;       // FP32 offsets (x_n - c_a) / H
     DevBuf<double> cent_, E_, W_, w_, c_;
     DevBuf<double> einv_;     // lower tiles of E^{-1}
-    DevBuf<double> gpart_, wcrow_;
+    DevBuf<double> gpart_, tilewc_;
     DevBuf<uint32_t> gcount_;
     DevBuf<uint8_t> drop_;
     DevBuf<double> wpart_;

@@ -598,15 +598,18 @@ __device__ __forceinline__ void restrict_node(bool lin, const double rr[3], cons
 // list, two nodes per thread and step with every load issued before the arithmetic (offsets and
 // mask from copies in node-list order, coalesced; only r is gathered); the CTA
 // that finishes an aggregate's last part adds the parts' sums in part order, so w does not
-// depend on which CTA ran which part. A persistent grid walks the items.
-template <typename XT>
-__global__ void __launch_bounds__(kThreads, 3) coarse_restrict_kernel(CoarseView cv, int parts,
-                                                                      const XT* __restrict__ r, const PcgState* st) {
-    __shared__ double sh[kThreads / 32][12];
+// depend on which CTA ran which part. A persistent grid walks the items. NM (modes per
+// aggregate) is a template parameter, so the rigid-body form keeps six accumulators and fits
+// four CTAs per SM.
+template <typename XT, int NM>
+__global__ void __launch_bounds__(kThreads, NM == 6 ? 4 : 3) coarse_restrict_kernel(CoarseView cv, int parts,
+                                                                                   const XT* __restrict__ r,
+                                                                                   const PcgState* st) {
+    __shared__ double sh[kThreads / 32][NM];
     __shared__ bool last;
     if (st && st->done) return;
-    const bool lin = cv.nm == 12;
-    const int nm = lin ? 12 : 6;
+    constexpr bool lin = NM == 12;
+    constexpr int nm = NM;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int items = cv.n_agg * parts;
     for (int item = blockIdx.x; item < items; item += gridDim.x) {
@@ -677,13 +680,18 @@ __global__ void __launch_bounds__(kThreads, 3) coarse_restrict_kernel(CoarseView
 }
 
 // Persistent grid of the restriction with about two work items per resident CTA.
-template <typename XT>
-void launch_restrict(const CoarseView& cv, const XT* r, const PcgState* st, cudaStream_t s, int sm) {
-    const unsigned grid = resident_grid((const void*)coarse_restrict_kernel<XT>, (int64_t)1 << 40, kThreads, sm);
+template <typename XT, int NM>
+void launch_restrict_nm(const CoarseView& cv, const XT* r, const PcgState* st, cudaStream_t s, int sm) {
+    const unsigned grid = resident_grid((const void*)coarse_restrict_kernel<XT, NM>, (int64_t)1 << 40, kThreads, sm);
     int parts = (int)((2 * (int64_t)grid + cv.n_agg - 1) / cv.n_agg);
     parts = std::max(1, std::min(parts, kMaxRestrictParts));
     const unsigned g = (unsigned)std::min<int64_t>(grid, (int64_t)cv.n_agg * parts);
-    coarse_restrict_kernel<XT><<<g, kThreads, 0, s>>>(cv, parts, r, st);
+    coarse_restrict_kernel<XT, NM><<<g, kThreads, 0, s>>>(cv, parts, r, st);
+}
+template <typename XT>
+void launch_restrict(const CoarseView& cv, const XT* r, const PcgState* st, cudaStream_t s, int sm) {
+    if (cv.nm == 12) launch_restrict_nm<XT, 12>(cv, r, st, s, sm);
+    else launch_restrict_nm<XT, 6>(cv, r, st, s, sm);
 }
 
 // c = E^{-1} w with the symmetric FP64 inverse stored as its lower 64x64 tiles. One CTA per
@@ -694,18 +702,19 @@ void launch_restrict(const CoarseView& cv, const XT* r, const PcgState* st, cuda
 // the CTA that completes X's ticket sums X's slots in tile order (J ascending) into c_X, so c
 // does not depend on which CTA ran which tile (four threads per entry take a quarter of the
 // slots each, added in order).
-// FIN (two-level iteration with the ||r|| test): the finisher of row X also stores (w_X, c_X);
-// the CTA that finishes the last row adds the rows in order and ends the iteration:
-// (r, z) = (r, D^-1 r) + (w, c), ||r||^2 from the update.
+// FIN (two-level iteration with the ||r|| test): every tile also stores its share of
+// (w, c) = w^T E^{-1} w, w_I^T E_IJ w_J (twice that off the diagonal, for the mirrored tile); the
+// last tile CTA to arrive adds the shares in tile order and ends the iteration:
+// (r, z) = (r, D^-1 r) + (w, c), ||r||^2 from the update. This needs no wait for the rows.
 __device__ __forceinline__ int64_t lower_tile(int i, int j) { return (int64_t)i * (i + 1) / 2 + j; }
 
 template <bool FIN>
 __global__ void __launch_bounds__(256) coarse_gemv_kernel(CoarseView cv, PcgState* st) {
     __shared__ double wI[64], wJ[64];
     __shared__ double colp[8][64];  // column partials per warp; the finisher's quarter sums
-    __shared__ double red[2];
+    __shared__ double red[8];
     __shared__ int finish[2];
-    __shared__ bool last_row;
+    __shared__ bool last_tile;
     if (st && st->done) return;
     const int t = blockIdx.x;
     int I = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
@@ -748,6 +757,23 @@ __global__ void __launch_bounds__(256) coarse_gemv_kernel(CoarseView cv, PcgStat
     if (tx == 0)
 #pragma unroll
         for (int a = 0; a < 4; ++a) gp[4 * ty + a] = rp[a];
+    if (FIN) {
+        // this tile's share of w^T E^{-1} w: rows in order within the patch, the two half warps,
+        // then the warps in order
+        double sw = 0.0;
+        if (tx == 0)
+#pragma unroll
+            for (int a = 0; a < 4; ++a) sw += wI[4 * ty + a] * rp[a];
+        sw += __shfl_xor_sync(0xffffffffu, sw, 16);
+        if (lane == 0) red[warp] = sw;
+        __syncthreads();
+        if (tid == 0) {
+            double x = 0.0;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) x += red[q];
+            cv.tilewc[t] = I != J ? 2.0 * x : x;
+        }
+    }
     if (I != J) {
         // column sums: the two half warps, then the warps in order
 #pragma unroll
@@ -765,11 +791,27 @@ __global__ void __launch_bounds__(256) coarse_gemv_kernel(CoarseView cv, PcgStat
     }
     __threadfence();
     __syncthreads();
+    const uint32_t ntiles = (uint32_t)((int64_t)cv.nb * (cv.nb + 1) / 2);
     if (tid == 0) {
         finish[0] = atomicAdd(cv.gcount + I, 1u) == (uint32_t)cv.nb - 1 ? I : -1;
         finish[1] = I != J && atomicAdd(cv.gcount + J, 1u) == (uint32_t)cv.nb - 1 ? J : -1;
+        last_tile = FIN && atomicAdd(cv.gcount + cv.nb, 1u) == ntiles - 1;
     }
     __syncthreads();
+    if (FIN && last_tile) {
+        // every tile's share has arrived: a contiguous run of shares per thread, the threads in
+        // order (block_sum), then the end of the iteration
+        const uint32_t per = (ntiles + blockDim.x - 1) / blockDim.x;
+        const uint32_t k0 = tid * per, k1 = min(ntiles, k0 + per);
+        double x = 0.0;
+        for (uint32_t k = k0; k < k1; ++k) x += __ldcg(cv.tilewc + k);
+        x = block_sum(x, colp[0]);
+        if (tid == 0) {
+            cv.gcount[cv.nb] = 0;
+            finish_iter(st, st->rdr + x, st->rr);
+        }
+        __syncthreads();  // colp is reused by the row sums below
+    }
     for (int f = 0; f < 2; ++f) {
         const int X = finish[f];
         if (X < 0) continue;
@@ -787,44 +829,9 @@ __global__ void __launch_bounds__(256) coarse_gemv_kernel(CoarseView cv, PcgStat
             colp[g][i] = x;
             __syncthreads();
         }
-        double wc = 0.0;
-        if (tid < 64) {
-            const double x = (colp[0][tid] + colp[1][tid]) + (colp[2][tid] + colp[3][tid]);
-            const int i = 64 * X + tid;
-            cv.c[i] = x;
-            if (FIN && i < cv.k) wc = cv.w[i] * x;  // padding entries of w are zero and unused
-        }
-        if (FIN) {
-            // (w_X, c_X): butterflies in the two warps, then warp 0 + warp 1
-            if (tid < 64) {
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) wc += __shfl_xor_sync(0xffffffffu, wc, o);
-                if (lane == 0) red[warp] = wc;
-            }
-            __syncthreads();
-            if (tid == 0) cv.wcrow[X] = red[0] + red[1];
-        }
+        if (tid < 64) cv.c[64 * X + tid] = (colp[0][tid] + colp[1][tid]) + (colp[2][tid] + colp[3][tid]);
         if (tid == 0) cv.gcount[X] = 0;  // every tile of row X has arrived
         __syncthreads();
-    }
-    if (!FIN) return;
-    if (finish[0] < 0 && finish[1] < 0) return;
-    // rows done: the CTA that finishes the last one ends the iteration
-    __threadfence();
-    __syncthreads();
-    if (tid == 0) {
-        const uint32_t nfin = (finish[0] >= 0) + (finish[1] >= 0);
-        last_row = atomicAdd(cv.gcount + cv.nb, nfin) + nfin == (uint32_t)cv.nb;
-    }
-    __syncthreads();
-    if (!last_row || warp != 0) return;
-    double wc = 0.0;
-    for (int X = lane; X < cv.nb; X += 32) wc += __ldcg(cv.wcrow + X);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) wc += __shfl_xor_sync(0xffffffffu, wc, o);
-    if (lane == 0) {
-        cv.gcount[cv.nb] = 0;
-        finish_iter(st, st->rdr + wc, st->rr);
     }
 }
 
