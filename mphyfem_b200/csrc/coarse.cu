@@ -98,7 +98,8 @@ constexpr int kMatItem = 21 + 13 * 36;  // one item's result: own block (lower),
 // aggregate's parts adds them in part order and stores the aggregate's blocks.
 template <typename VT>
 __global__ void __launch_bounds__(kMatThreads, 3) coarse_matrix_kernel(SellView A, const VT* __restrict__ aval,
-                                                                    CoarseView cv, int ngx, int ngy, int ngz, int parts,
+                                                                    CoarseView cv, const int32_t* __restrict__ aggbox,
+                                                                    int ngx, int ngy, int ngz, int parts,
                                                                     double* __restrict__ epart,
                                                                     double* __restrict__ E, int32_t* err) {
     __shared__ double Eloc[13][36];
@@ -177,8 +178,8 @@ __global__ void __launch_bounds__(kMatThreads, 3) coarse_matrix_kernel(SellView 
 #pragma unroll
                     for (int q = 0; q < 9; ++q) blk[q] = -S[q];
                 }
-                const int b = cv.agg[m];
-                const int dx = b % ngx - ax, dy = (b / ngx) % ngy - ay, dz = b / (ngx * ngy) - az;
+                const int pb = aggbox[m];  // the neighbour's box, packed: no integer division
+                const int dx = (pb & 1023) - ax, dy = ((pb >> 10) & 1023) - ay, dz = (pb >> 20) - az;
                 if (dx < -1 || dx > 1 || dy < -1 || dy > 1 || dz < -1 || dz > 1) {
                     atomicExch(err, 1);
                     continue;
@@ -268,7 +269,8 @@ __global__ void __launch_bounds__(kMatThreads, 3) coarse_matrix_kernel(SellView 
 // columns of prescribed DOFs drop out (their Z rows are zero).
 template <typename VT>
 __global__ void __launch_bounds__(256) coarse_matrix_linear_kernel(SellView A, const VT* __restrict__ aval,
-                                                                   CoarseView cv, int ngx, int ngy, int ngz,
+                                                                   CoarseView cv, const int32_t* __restrict__ aggbox,
+                                                                   int ngx, int ngy, int ngz,
                                                                    double* __restrict__ E, int32_t* err) {
     __shared__ double Eloc[27][144];
     for (int a = blockIdx.x; a < cv.n_agg; a += gridDim.x) {
@@ -322,8 +324,8 @@ __global__ void __launch_bounds__(256) coarse_matrix_linear_kernel(SellView A, c
                 }
                 for (int q = 0; q < 9; ++q)
                     if (cv.fixed[3 * m + q % 3]) blk[q] = 0.0;  // prescribed columns: zero Z rows of m
-                const int b = cv.agg[m];
-                const int dx = b % ngx - ax, dy = (b / ngx) % ngy - ay, dz = b / (ngx * ngy) - az;
+                const int pb = aggbox[m];  // the neighbour's box, packed: no integer division
+                const int dx = (pb & 1023) - ax, dy = ((pb >> 10) & 1023) - ay, dz = (pb >> 20) - az;
                 if (dx < -1 || dx > 1 || dy < -1 || dy > 1 || dz < -1 || dz > 1) {
                     atomicExch(err, 1);
                     continue;
@@ -716,6 +718,19 @@ void CoarseSpace::init(mphy_ctx* ctx, const mphy_mesh* mesh, const mphy_pattern*
     cudaStream_t s = ctx->stream;
     agg_.alloc(nn);
     agg_.upload(agg.data(), nn, s);
+    // every node's aggregate box (bx, by, bz) packed in 10 bits each, for the E kernel
+    MPHY_REQUIRE(ng_[0] <= 1024 && ng_[1] <= 1024 && ng_[2] <= 1024, MPHY_ERR_UNSUPPORTED,
+                 "coarse space: more than 1024 aggregates along one axis");
+    {
+        std::vector<int32_t> box(nn);
+        for (int32_t n = 0; n < nn; ++n) {
+            const int a = agg[n];
+            box[n] = (a % ng_[0]) | (((a / ng_[0]) % ng_[1]) << 10) | ((a / (ng_[0] * ng_[1])) << 20);
+        }
+        aggbox_.alloc(nn);
+        aggbox_.upload(box.data(), nn, s);
+        MPHY_CUDA(cudaStreamSynchronize(s));  // box lives on the host stack until the copy ends
+    }
     agg_ptr_.alloc(n_agg_ + 1);
     agg_ptr_.upload(ptr.data(), n_agg_ + 1, s);
     agg_nodes_.alloc(nn);
@@ -777,14 +792,15 @@ void CoarseSpace::setup(const SellView& A, const VT* aval, const double* disp, c
     MPHY_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(int32_t), s));
     CoarseView cv = view();
     if (nm_ == 12)
-        coarse_matrix_linear_kernel<VT><<<std::min(n_agg_, sm * 8), 256, 0, s>>>(A, aval, cv, ng_[0], ng_[1], ng_[2],
-                                                                                  E_.p, err_.p);
+        coarse_matrix_linear_kernel<VT><<<std::min(n_agg_, sm * 8), 256, 0, s>>>(A, aval, cv, aggbox_.p, ng_[0],
+                                                                                  ng_[1], ng_[2], E_.p, err_.p);
     else {
         // persistent grid, about two work items per resident CTA
         const unsigned grid = resident_grid((const void*)coarse_matrix_kernel<VT>, (int64_t)1 << 40, kMatThreads, sm);
         const int parts = std::max(1, std::min(kMatParts, (int)((2 * (int64_t)grid + n_agg_ - 1) / n_agg_)));
         const unsigned g = (unsigned)std::min<int64_t>(grid, (int64_t)n_agg_ * parts);
-        coarse_matrix_kernel<VT><<<g, kMatThreads, 0, s>>>(A, aval, cv, ng_[0], ng_[1], ng_[2], parts, epart_.p, E_.p,
+        coarse_matrix_kernel<VT><<<g, kMatThreads, 0, s>>>(A, aval, cv, aggbox_.p, ng_[0], ng_[1], ng_[2], parts,
+                                                           epart_.p, E_.p,
                                                            err_.p);
     }
     MPHY_CUDA(cudaGetLastError());

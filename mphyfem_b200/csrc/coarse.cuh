@@ -47,6 +47,7 @@ class CoarseSpace {
     int ng_[3] = {1, 1, 1};
     int n_agg_ = 0, kp_ = 0;
     DevBuf<int32_t> agg_, agg_nodes_, err_;
+    DevBuf<int32_t> aggbox_;  // [n_node] aggregate box bx | by << 10 | bz << 20
     DevBuf<int64_t> agg_ptr_;
     DevBuf<float> d_;       // FP32 offsets (x_n - c_a) / H
     DevBuf<double> cent_, E_, W_, w_, c_;
