@@ -414,7 +414,9 @@ typedef struct mphy_mixed_opts {
     int32_t coarse_modes;       /* 6 (0 = default) or 12, as in mphy_solver_opts */
 } mphy_mixed_opts;
 void mphy_mixed_opts_default(mphy_mixed_opts* opts); /* reference tangent, 20000, 1e-10, 0 */
-/* mesh: tet10 (npe = 10); pattern: mphy_pattern_build of the same mesh. opts may be NULL. */
+/* Elem_Solid_3D_Mixed1 meshes: tet10 (npe = 10, linear pressure on the 4 vertices) or the P2-P1
+ * hex27 (npe = 27, trilinear pressure on the 8 corners; 3x3x3 rule); pattern: mphy_pattern_build
+ * of the same mesh. opts may be NULL. */
 int mphy_mixed_create(mphy_ctx* ctx, const mphy_mesh* mesh, const mphy_pattern* pattern,
                       const mphy_mixed_opts* opts, mphy_mixed** out);
 int mphy_mixed_destroy(mphy_mixed* m);
@@ -423,9 +425,10 @@ int mphy_mixed_info(mphy_mixed* m, int32_t* n_pres, int64_t* nnz_coupling, int64
 /* the global node of each pressure DOF (assyForSolnPres) [n_pres], host */
 int mphy_mixed_pressure_nodes(mphy_mixed* m, int32_t* nodes_host);
 /* calcStiffnessAndResidualMixed for every element. Device arrays: disp, disp_prev (the last
- * converged step, for Jn) [3 n_node], pres [n_node] nodal pressures (vertex nodes used);
- * outputs Kuu [n_elem][30][30], FU [n_elem][30], Kup [n_elem][30][4] (Kpu = Kup^T),
- * Kpp [n_elem][4][4], FP [n_elem][4]. MPHY_ERR_NEG_JACOBIAN as mphy_elem_eval. */
+ * converged step, for Jn) [3 n_node], pres [n_node] nodal pressures (pressure nodes used);
+ * with ns = 3 npe and NP pressure nodes per element (4 tet10, 8 hex27), outputs Kuu
+ * [n_elem][ns][ns], FU [n_elem][ns], Kup [n_elem][ns][NP] (Kpu = Kup^T), Kpp [n_elem][NP][NP],
+ * FP [n_elem][NP]. MPHY_ERR_NEG_JACOBIAN as mphy_elem_eval. */
 int mphy_mixed_elem_eval(mphy_mixed* m, const double* disp_dev, const double* disp_prev_dev,
                          const double* pres_dev, double* Kuu_dev, double* FU_dev, double* Kup_dev,
                          double* Kpp_dev, double* FP_dev, int64_t* first_bad);

@@ -431,8 +431,9 @@ class MixedNewtonResult:
 
 
 class MixedSolidGpu:
-    """A mixed u-p problem (tet10 displacement, linear vertex pressure; Elem_Solid_3D_Mixed1) on
-    the GPU: two-field assembly, MINRES solve and Newton load stepping (mphy_mixed_*)."""
+    """A mixed u-p problem (Elem_Solid_3D_Mixed1: tet10 displacement with linear vertex pressure,
+    or the P2-P1 hex27 with trilinear corner pressure) on the GPU: two-field assembly, MINRES
+    solve and Newton load stepping (mphy_mixed_*)."""
 
     def __init__(self, prob, ctx: Context | None = None, tangent: int = L.TANGENT_REFERENCE, rtol: float = 1e-10,
                  max_it: int = 20000, coarse_aggregates: int = 0, coarse_modes: int = 0):
@@ -463,8 +464,9 @@ class MixedSolidGpu:
         torch = _torch()
         ne = self.prob.n_elem
         dev = dict(dtype=torch.float64, device="cuda")
-        Kuu, FU = torch.empty((ne, 30, 30), **dev), torch.empty((ne, 30), **dev)
-        Kup, Kpp, FP = torch.empty((ne, 30, 4), **dev), torch.empty((ne, 4, 4), **dev), torch.empty((ne, 4), **dev)
+        ns, NP = 3 * self.prob.npe, {10: 4, 27: 8}[self.prob.npe]  # pressure nodes per element
+        Kuu, FU = torch.empty((ne, ns, ns), **dev), torch.empty((ne, ns), **dev)
+        Kup, Kpp, FP = torch.empty((ne, ns, NP), **dev), torch.empty((ne, NP, NP), **dev), torch.empty((ne, NP), **dev)
         bad = C.c_int64(-1)
         rc = self.lib.mphy_mixed_elem_eval(self.h, _ptr(disp), _ptr(disp_prev), _ptr(pres), _ptr(Kuu), _ptr(FU),
                                            _ptr(Kup), _ptr(Kpp), _ptr(FP), C.byref(bad))

@@ -344,6 +344,8 @@ int elem_eval(mphy_ctx* c, const mphy_mesh* m, const double* disp, int32_t tange
               int64_t* first_bad, bool tc) {
     return guarded([&] {
         MPHY_REQUIRE(c && m && disp && Ke && Re, MPHY_ERR_INVALID_ARG, "null argument");
+        MPHY_REQUIRE(m->npe == 8 || m->npe == 10, MPHY_ERR_UNSUPPORTED,
+                     "the displacement element is hex8 or tet10 (27-node hexes: mphy_mixed_elem_eval)");
         DevBuf<unsigned long long> bad(1);
         MPHY_CUDA(cudaMemsetAsync(bad.p, 0xff, sizeof(unsigned long long), c->stream));
         ElemArgs a = elem_args(m, disp, tangent, bad.p);
@@ -449,7 +451,8 @@ int mphy_mesh_create(mphy_ctx* c, int32_t n_node, const double* coords, int32_t 
                      const uint8_t* fixed, mphy_mesh** out) {
     return guarded([&] {
         MPHY_REQUIRE(c && out && coords && conn && mat_id && mats && fixed, MPHY_ERR_INVALID_ARG, "null argument");
-        MPHY_REQUIRE(npe == 8 || npe == 10, MPHY_ERR_UNSUPPORTED, "npe must be 8 (hex8) or 10 (tet10)");
+        MPHY_REQUIRE(npe == 8 || npe == 10 || npe == 27, MPHY_ERR_UNSUPPORTED,
+                     "npe must be 8 (hex8), 10 (tet10) or 27 (hex27, mixed u-p meshes only)");
         MPHY_REQUIRE(n_node > 0 && n_elem > 0 && n_mat > 0, MPHY_ERR_INVALID_ARG, "empty mesh");
         for (int32_t e = 0; e < n_elem; ++e)
             MPHY_REQUIRE(mat_id[e] >= 0 && mat_id[e] < n_mat, MPHY_ERR_INVALID_ARG, "material id out of range");
@@ -696,6 +699,8 @@ int mphy_solver_create(mphy_ctx* c, const mphy_mesh* m, const mphy_pattern* P, c
     return guarded([&] {
         MPHY_REQUIRE(c && m && P && out, MPHY_ERR_INVALID_ARG, "null argument");
         MPHY_REQUIRE(P->n_node == m->n_node && P->n_elem == m->n_elem, MPHY_ERR_INVALID_ARG, "pattern/mesh mismatch");
+        MPHY_REQUIRE(m->npe == 8 || m->npe == 10, MPHY_ERR_UNSUPPORTED,
+                     "the displacement element is hex8 or tet10; a 27-node hex mesh is for mphy_mixed_create");
         mphy_solver_opts o;
         mphy_solver_opts_default(&o);
         if (opts) o = *opts;

@@ -13,6 +13,8 @@
 // F, the spatial gradients h and dvol * {sigma, C} in shared memory. Phase 2: thread (I, ch) owns
 // row node I and the column nodes J of chunk ch (4 per chunk), so the 9 * 4 accumulators stay in
 // registers; chunk 0 also forms the residual of node I.
+#include <vector>
+
 #include "common.cuh"
 #include "elem.cuh"
 #include "elem_store.cuh"
@@ -246,24 +248,22 @@ void launch_gen(const ElemArgs& a, cudaStream_t s) {
     MPHY_CUDA(cudaGetLastError());
 }
 
-// ---------------------------------------------------------------- mixed u-p tet10 element
-// ElementBase::calcStiffnessAndResidualMixed3D (ElementBase2.cpp:278-553) for Elem_Solid_3D_Mixed1
-// with npElem = 10: quadratic displacement, linear pressure on the four vertex nodes (basis the
-// barycentric coordinates, LagrangeBasisFunsTetra(4)), the displacement element's 4-point rule.
+// ---------------------------------------------------------------- mixed u-p element (Mixed1)
+// ElementBase::calcStiffnessAndResidualMixed3D (ElementBase2.cpp:278-553) for Elem_Solid_3D_Mixed1:
+//   - tet10: quadratic displacement, linear pressure on the four vertex nodes (basis the
+//     barycentric coordinates, LagrangeBasisFunsTetra(4)), the 4-point rule;
+//   - hex27 (P2-P1): triquadratic displacement, trilinear pressure on the eight corner nodes
+//     (LagrangeBasisFunsHexa(8)), the 3x3x3 rule that getGaussPoints3D gives a 27-node hex.
 // Per Gauss point: F from u, Fn from the last converged step (Jn, then Jhat = Jn - U'(Jn)/U''(Jn),
 // thetahat = 1/U''(Jn)), p = sum Np_i p_i, the mixed material branch, and
 //   Kup(3I+a, j) = sum dvol h_aI Np_j = Kpu(j, 3I+a),   Kpp(i, j) = -sum dvol0 thetahat Np_i Np_j,
 //   FP(i) = -sum dvol0 Np_i (J - Jhat - thetahat p),    Kuu and FU as the displacement element.
-struct MixedSmem {
-    double x0[10][3];
-    double u[10][3];
-    double up[10][3];
-    double h[4][10][3];
-    double C[4][81];
-    double sig[4][9];
-    double dvol[4], dvol0[4], th[4], resip[4];
-    double pad[8];  // element stride 594 doubles
-};
+
+// hex27 tables in global memory (the 27 Gauss-point threads read different points at once, which
+// the constant cache would serialise): dN/dxi [gp][3][27], weights [gp], trilinear Np [gp][8]
+__device__ double g_hex27_dN[27 * 3 * 27];
+__device__ double g_hex27_w[27];
+__device__ double g_hex27_np[27 * 8];
 
 // tet 4-point rule (QuadratureUtil.cpp:690-712) points in barycentric form: Np(gp, i)
 __device__ __forceinline__ double tet4_np(int gp, int i) {
@@ -272,18 +272,53 @@ __device__ __forceinline__ double tet4_np(int gp, int i) {
     return gp == i ? b : a;
 }
 
-template <int MODE>
-__global__ void __launch_bounds__(kGenEpb * 30) elem_mixed_kernel(MixedElemArgs ma) {
+template <int NPE>
+struct MixedTraits;
+template <>
+struct MixedTraits<10> {
+    static constexpr int NGP = 4, NP = 4, EPB = kGenEpb;
+    static constexpr int PAD = 8;  // element stride 594 doubles
+    __device__ static const double* dN(int gp) { return GenTraits<10>::dN(gp); }
+    __device__ static double w(int gp) { return GenTraits<10>::w(gp); }
+    __device__ static double np(int gp, int i) { return tet4_np(gp, i); }
+};
+template <>
+struct MixedTraits<27> {
+    static constexpr int NGP = 27, NP = 8, EPB = 1;  // one element (189 threads, 39 KB) per CTA
+    static constexpr int PAD = 0;
+    __device__ static const double* dN(int gp) { return g_hex27_dN + gp * 3 * 27; }
+    __device__ static double w(int gp) { return g_hex27_w[gp]; }
+    __device__ static double np(int gp, int i) { return g_hex27_np[gp * 8 + i]; }
+};
+
+template <int NPE>
+struct MixedSmem {
+    static constexpr int NGP = MixedTraits<NPE>::NGP;
+    double x0[NPE][3];
+    double u[NPE][3];
+    double up[NPE][3];
+    double h[NGP][NPE][3];
+    double C[NGP][81];
+    double sig[NGP][9];
+    double dvol[NGP], dvol0[NGP], th[NGP], resip[NGP];
+    double pad[MixedTraits<NPE>::PAD > 0 ? MixedTraits<NPE>::PAD : 1];
+};
+
+template <int NPE>
+constexpr int mixed_tpe() { return NPE * ((NPE + kGenCh - 1) / kGenCh); }
+
+template <int NPE, int MODE>
+__global__ void __launch_bounds__(MixedTraits<NPE>::EPB * mixed_tpe<NPE>()) elem_mixed_kernel(MixedElemArgs ma) {
     const ElemArgs& a = ma.base;
-    using T = GenTraits<10>;
-    constexpr int NPE = 10, NGP = 4, TPE = 30, NS = 30;
+    using T = MixedTraits<NPE>;
+    constexpr int NGP = T::NGP, NP = T::NP, TPE = mixed_tpe<NPE>(), NS = 3 * NPE;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    auto* S = reinterpret_cast<MixedSmem*>(smem_raw);
+    auto* S = reinterpret_cast<MixedSmem<NPE>*>(smem_raw);
     const int el = threadIdx.x / TPE, loc = threadIdx.x % TPE;
     const int I = loc % NPE, ch = loc / NPE;
-    const int64_t e = (int64_t)blockIdx.x * kGenEpb + el;
+    const int64_t e = (int64_t)blockIdx.x * T::EPB + el;
     const bool live = e < a.n_elem;
-    MixedSmem& s = S[el];
+    MixedSmem<NPE>& s = S[el];
 
     int32_t node = 0;
     if (live) {
@@ -358,7 +393,7 @@ __global__ void __launch_bounds__(kGenEpb * 30) elem_mixed_kernel(MixedElemArgs 
         }
         double pres = 0.0;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) pres += tet4_np(gp, i) * ma.pres[a.conn[e * NPE + i]];
+        for (int i = 0; i < NP; ++i) pres += T::np(gp, i) * ma.pres[a.conn[e * NPE + i]];
         double b[3][3], b2[3][3];
 #pragma unroll
         for (int i = 0; i < 3; ++i)
@@ -382,7 +417,7 @@ __global__ void __launch_bounds__(kGenEpb * 30) elem_mixed_kernel(MixedElemArgs 
     }
     if (ch == 0) {
         double R[3] = {0, 0, 0};
-        double kup[3][4] = {{0}};
+        double kup[3][NP] = {{0}};
 #pragma unroll
         for (int gp = 0; gp < NGP; ++gp) {
 #pragma unroll
@@ -390,7 +425,7 @@ __global__ void __launch_bounds__(kGenEpb * 30) elem_mixed_kernel(MixedElemArgs 
                 R[c] -= s.h[gp][I][0] * s.sig[gp][c] + s.h[gp][I][1] * s.sig[gp][3 + c] +
                         s.h[gp][I][2] * s.sig[gp][6 + c];
 #pragma unroll
-                for (int j = 0; j < 4; ++j) kup[c][j] += s.dvol[gp] * s.h[gp][I][c] * tet4_np(gp, j);
+                for (int j = 0; j < NP; ++j) kup[c][j] += s.dvol[gp] * s.h[gp][I][c] * T::np(gp, j);
             }
         }
         store_residual<NPE, MODE>(a, e, I, node, freeI, R);
@@ -398,12 +433,12 @@ __global__ void __launch_bounds__(kGenEpb * 30) elem_mixed_kernel(MixedElemArgs 
 #pragma unroll
             for (int c = 0; c < 3; ++c)
 #pragma unroll
-                for (int j = 0; j < 4; ++j) ma.Kup[(e * NS + 3 * I + c) * 4 + j] = kup[c][j];
+                for (int j = 0; j < NP; ++j) ma.Kup[(e * NS + 3 * I + c) * NP + j] = kup[c][j];
         }
         if (MODE & 2) {
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const uint32_t ib = ma.e2b[(e * NPE + I) * 4 + j], it = ma.e2bt[(e * 4 + j) * NPE + I];
+            for (int j = 0; j < NP; ++j) {
+                const uint32_t ib = ma.e2b[(e * NPE + I) * NP + j], it = ma.e2bt[(e * NP + j) * NPE + I];
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
                     if (!freeI[c]) continue;
@@ -412,25 +447,25 @@ __global__ void __launch_bounds__(kGenEpb * 30) elem_mixed_kernel(MixedElemArgs 
                 }
             }
         }
-    } else if (ch == 1 && I < 4) {
-        // pressure row i = I (vertex node)
-        double fp = 0.0, kpp[4] = {0, 0, 0, 0};
+    } else if (ch == 1 && I < NP) {
+        // pressure row i = I (a vertex / corner node)
+        double fp = 0.0, kpp[NP] = {0};
 #pragma unroll
         for (int gp = 0; gp < NGP; ++gp) {
-            const double w = s.dvol0[gp] * tet4_np(gp, I);
+            const double w = s.dvol0[gp] * T::np(gp, I);
             fp -= w * s.resip[gp];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) kpp[j] -= w * s.th[gp] * tet4_np(gp, j);
+            for (int j = 0; j < NP; ++j) kpp[j] -= w * s.th[gp] * T::np(gp, j);
         }
         if (MODE & 1) {
-            ma.FP[e * 4 + I] = fp;
+            ma.FP[e * NP + I] = fp;
 #pragma unroll
-            for (int j = 0; j < 4; ++j) ma.Kpp[(e * 4 + I) * 4 + j] = kpp[j];
+            for (int j = 0; j < NP; ++j) ma.Kpp[(e * NP + I) * NP + j] = kpp[j];
         }
         if (MODE & 2) {
             atomicAdd(&ma.rhs_p[ma.pres_id[node]], fp);
 #pragma unroll
-            for (int j = 0; j < 4; ++j) atomicAdd(&ma.cval[ma.e2c[(e * 4 + I) * 4 + j]], kpp[j]);
+            for (int j = 0; j < NP; ++j) atomicAdd(&ma.cval[ma.e2c[(e * NP + I) * NP + j]], kpp[j]);
         }
     }
     // Kuu: thread (I, ch), column nodes 4 ch .. 4 ch + 3
@@ -468,16 +503,18 @@ __global__ void __launch_bounds__(kGenEpb * 30) elem_mixed_kernel(MixedElemArgs 
     }
 }
 
-template <int MODE>
+template <int NPE, int MODE>
 void launch_mixed(const MixedElemArgs& a, cudaStream_t s) {
-    const size_t smem = kGenEpb * sizeof(MixedSmem);
+    using T = MixedTraits<NPE>;
+    const size_t smem = T::EPB * sizeof(MixedSmem<NPE>);
     static std::atomic<uint64_t> configured{0};
     if (first_use_on_device(configured)) {
-        MPHY_CUDA(cudaFuncSetAttribute(elem_mixed_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        MPHY_CUDA(cudaFuncSetAttribute(elem_mixed_kernel<NPE, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
     }
-    const unsigned grid = ceil_div((size_t)a.base.n_elem, kGenEpb);
+    const unsigned grid = ceil_div((size_t)a.base.n_elem, T::EPB);
     if (grid == 0) return;
-    elem_mixed_kernel<MODE><<<grid, kGenEpb * 30, smem, s>>>(a);
+    elem_mixed_kernel<NPE, MODE><<<grid, T::EPB * mixed_tpe<NPE>(), smem, s>>>(a);
     MPHY_CUDA(cudaGetLastError());
 }
 
@@ -767,10 +804,61 @@ void launch_elem_gen(const ElemArgs& a, int npe, int mode, cudaStream_t s) {
     }
 }
 
-void launch_elem_mixed(const MixedElemArgs& a, int mode, cudaStream_t s) {
-    if (mode == 1) launch_mixed<1>(a, s);
-    else if (mode == 2) launch_mixed<2>(a, s);
-    else launch_mixed<3>(a, s);
+// The hex27 tables: the 27-node hex of BasisFunctionsLagrange.cpp:1300-1399 (1D quadratic
+// Lagrange triple ordered -1, +1, 0; node a at the 1D indices kHex27Ijk[a]) and the 3x3x3 rule of
+// QuadratureUtil.cpp:497-524 (point q at the 1D indices of node q, weights 5/9, 5/9, 8/9),
+// with the trilinear pressure basis of the 8 corners at the same points.
+void upload_hex27_tables() {
+    static const int kHex27Ijk[27][3] = {
+        {0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0}, {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1},
+        {2, 0, 0}, {0, 2, 0}, {0, 0, 2}, {1, 2, 0}, {1, 0, 2}, {2, 1, 0}, {1, 1, 2}, {0, 1, 2},
+        {2, 0, 1}, {0, 2, 1}, {1, 2, 1}, {2, 1, 1}, {2, 2, 0}, {2, 0, 2}, {0, 2, 2}, {1, 2, 2},
+        {2, 1, 2}, {2, 2, 1}, {2, 2, 2}};
+    const double g[3] = {-0.774596669241483, 0.774596669241483, 0.0};
+    const double wt[3] = {5.0 / 9.0, 5.0 / 9.0, 8.0 / 9.0};
+    std::vector<double> dN(27 * 3 * 27), w(27), np(27 * 8);
+    for (int q = 0; q < 27; ++q) {
+        double xi[3], n1[3][3], d1[3][3], l1[3][2];
+        for (int d = 0; d < 3; ++d) {
+            const double x = g[kHex27Ijk[q][d]], x2 = x * x;
+            xi[d] = x;
+            n1[d][0] = 0.5 * (x2 - x);
+            n1[d][1] = 0.5 * (x2 + x);
+            n1[d][2] = 1.0 - x2;
+            d1[d][0] = 0.5 * (2.0 * x - 1.0);
+            d1[d][1] = 0.5 * (2.0 * x + 1.0);
+            d1[d][2] = -2.0 * x;
+            l1[d][0] = 0.5 * (1.0 - x);
+            l1[d][1] = 0.5 * (1.0 + x);
+        }
+        w[q] = wt[kHex27Ijk[q][0]] * wt[kHex27Ijk[q][1]] * wt[kHex27Ijk[q][2]];
+        for (int a = 0; a < 27; ++a) {
+            const int i = kHex27Ijk[a][0], j = kHex27Ijk[a][1], k = kHex27Ijk[a][2];
+            dN[(q * 3 + 0) * 27 + a] = d1[0][i] * n1[1][j] * n1[2][k];
+            dN[(q * 3 + 1) * 27 + a] = n1[0][i] * d1[1][j] * n1[2][k];
+            dN[(q * 3 + 2) * 27 + a] = n1[0][i] * n1[1][j] * d1[2][k];
+        }
+        for (int a = 0; a < 8; ++a) {
+            const int i = kHex27Ijk[a][0], j = kHex27Ijk[a][1], k = kHex27Ijk[a][2];
+            np[q * 8 + a] = l1[0][i] * l1[1][j] * l1[2][k];
+        }
+        (void)xi;
+    }
+    MPHY_CUDA(cudaMemcpyToSymbol(g_hex27_dN, dN.data(), dN.size() * sizeof(double)));
+    MPHY_CUDA(cudaMemcpyToSymbol(g_hex27_w, w.data(), w.size() * sizeof(double)));
+    MPHY_CUDA(cudaMemcpyToSymbol(g_hex27_np, np.data(), np.size() * sizeof(double)));
+}
+
+void launch_elem_mixed(const MixedElemArgs& a, int npe, int mode, cudaStream_t s) {
+    if (npe == 27) {
+        if (mode == 1) launch_mixed<27, 1>(a, s);
+        else if (mode == 2) launch_mixed<27, 2>(a, s);
+        else launch_mixed<27, 3>(a, s);
+    } else {
+        if (mode == 1) launch_mixed<10, 1>(a, s);
+        else if (mode == 2) launch_mixed<10, 2>(a, s);
+        else launch_mixed<10, 3>(a, s);
+    }
 }
 
 void launch_elem_mixed0(const MixedElemArgs& a, int npe, int mode, cudaStream_t s) {

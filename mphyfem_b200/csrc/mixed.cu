@@ -43,6 +43,7 @@ struct mphy_mixed {
     int device = 0;
     mphy_mixed_opts opts{};
     int32_t n_node = 0, n_elem = 0, n_pres = 0;
+    int npe = 10, np_elem = 4;  // element nodes and pressure nodes per element (tet10: 4, hex27: 8)
     int64_t nb = 0, nc = 0;  // B (= B^T) and C entries
     int64_t launches = 0;
     SellView A{};
@@ -324,7 +325,7 @@ void assemble(mphy_mixed* m, const double* disp, const double* disp_prev, const 
     a.btval = m->bt_val.p;
     a.cval = m->c_val.p;
     a.rhs_p = m->rhs.p + 3 * (int64_t)m->n_node;
-    launch_elem_mixed(a, 2, st);
+    launch_elem_mixed(a, m->npe, 2, st);
     if (fext) add_scaled_free(m->mesh->fixed.p, fext, lambda, m->rhs.p, 3 * (int64_t)m->n_node, st, sm);
     precond_u_kernel<<<stride_grid(m->n_node, 256, sm), 256, 0, st>>>(m->n_node, m->A.dvoff, m->val.p, m->dinv.p);
     precond_p_kernel<<<stride_grid(m->n_pres, 256, sm), 256, 0, st>>>(m->n_node, m->n_pres, m->bt_ptr.p, m->bt_col.p,
@@ -443,8 +444,9 @@ int mphy_mixed_create(mphy_ctx* c, const mphy_mesh* mesh, const mphy_pattern* pa
         MPHY_REQUIRE(c && mesh && pat && out, MPHY_ERR_INVALID_ARG, "null argument");
         MPHY_REQUIRE(!mesh->has_presc, MPHY_ERR_UNSUPPORTED,
                      "mixed u-p elements with nonzero prescribed displacements");
-        MPHY_REQUIRE(mesh->npe == 10, MPHY_ERR_UNSUPPORTED,
-                     "mixed u-p elements: tet10 displacement with linear vertex pressure (npe = 10)");
+        MPHY_REQUIRE(mesh->npe == 10 || mesh->npe == 27, MPHY_ERR_UNSUPPORTED,
+                     "mixed u-p elements: tet10 with linear vertex pressure (npe = 10) or hex27 with trilinear "
+                     "corner pressure (npe = 27)");
         MPHY_REQUIRE(pat->mesh == mesh, MPHY_ERR_INVALID_ARG, "the pattern belongs to another mesh");
         MPHY_CUDA(cudaSetDevice(c->device));
         auto* m = new mphy_mixed;
@@ -458,11 +460,18 @@ int mphy_mixed_create(mphy_ctx* c, const mphy_mesh* mesh, const mphy_pattern* pa
             m->n_node = mesh->n_node;
             m->n_elem = mesh->n_elem;
             const int32_t nn = mesh->n_node, ne = mesh->n_elem;
-            const std::vector<int32_t> conn = download_i32(mesh->conn.p, (size_t)ne * 10);
-            // pressure DOFs: vertex nodes in ascending order
+            const int npe = mesh->npe, NP = npe == 27 ? 8 : 4;  // pressure nodes: the first NP of each element
+            m->npe = npe;
+            m->np_elem = NP;
+            if (npe == 27) {
+                static std::atomic<uint64_t> tables{0};
+                if (first_use_on_device(tables)) upload_hex27_tables();
+            }
+            const std::vector<int32_t> conn = download_i32(mesh->conn.p, (size_t)ne * npe);
+            // pressure DOFs: vertex (corner) nodes in ascending order
             std::vector<int32_t> pid(nn, -1);
             for (int32_t e = 0; e < ne; ++e)
-                for (int i = 0; i < 4; ++i) pid[conn[10 * (size_t)e + i]] = 0;
+                for (int i = 0; i < NP; ++i) pid[conn[npe * (size_t)e + i]] = 0;
             int32_t np = 0;
             m->pres_node_host.clear();
             for (int32_t n = 0; n < nn; ++n)
@@ -473,18 +482,18 @@ int mphy_mixed_create(mphy_ctx* c, const mphy_mesh* mesh, const mphy_pattern* pa
             m->n_pres = np;
             // B (node rows), B^T (pressure rows), C (pressure rows)
             std::vector<int64_t> kb, kbt, kc;
-            kb.reserve((size_t)ne * 40);
-            kbt.reserve((size_t)ne * 40);
-            kc.reserve((size_t)ne * 16);
+            kb.reserve((size_t)ne * npe * NP);
+            kbt.reserve((size_t)ne * npe * NP);
+            kc.reserve((size_t)ne * NP * NP);
             for (int32_t e = 0; e < ne; ++e) {
-                const int32_t* cn = &conn[10 * (size_t)e];
-                for (int j = 0; j < 4; ++j) {
+                const int32_t* cn = &conn[npe * (size_t)e];
+                for (int j = 0; j < NP; ++j) {
                     const int64_t pj = pid[cn[j]];
-                    for (int I = 0; I < 10; ++I) {
+                    for (int I = 0; I < npe; ++I) {
                         kb.push_back((int64_t)cn[I] * np + pj);
                         kbt.push_back(pj * nn + cn[I]);
                     }
-                    for (int i = 0; i < 4; ++i) kc.push_back((int64_t)pid[cn[i]] * np + pj);
+                    for (int i = 0; i < NP; ++i) kc.push_back((int64_t)pid[cn[i]] * np + pj);
                 }
             }
             std::vector<int64_t> bp, btp, cp;
@@ -494,16 +503,17 @@ int mphy_mixed_create(mphy_ctx* c, const mphy_mesh* mesh, const mphy_pattern* pa
             build_rows(kc, np, np, cp, cc);
             m->nb = (int64_t)bc.size();
             m->nc = (int64_t)cc.size();
-            std::vector<uint32_t> e2b((size_t)ne * 40), e2bt((size_t)ne * 40), e2c((size_t)ne * 16);
+            std::vector<uint32_t> e2b((size_t)ne * npe * NP), e2bt((size_t)ne * npe * NP), e2c((size_t)ne * NP * NP);
             for (int32_t e = 0; e < ne; ++e) {
-                const int32_t* cn = &conn[10 * (size_t)e];
-                for (int I = 0; I < 10; ++I)
-                    for (int j = 0; j < 4; ++j) {
-                        e2b[(10 * (size_t)e + I) * 4 + j] = find_entry(bp, bc, cn[I], pid[cn[j]]);
-                        e2bt[(4 * (size_t)e + j) * 10 + I] = find_entry(btp, btc, pid[cn[j]], cn[I]);
+                const int32_t* cn = &conn[npe * (size_t)e];
+                for (int I = 0; I < npe; ++I)
+                    for (int j = 0; j < NP; ++j) {
+                        e2b[(npe * (size_t)e + I) * NP + j] = find_entry(bp, bc, cn[I], pid[cn[j]]);
+                        e2bt[(NP * (size_t)e + j) * npe + I] = find_entry(btp, btc, pid[cn[j]], cn[I]);
                     }
-                for (int i = 0; i < 4; ++i)
-                    for (int j = 0; j < 4; ++j) e2c[(4 * (size_t)e + i) * 4 + j] = find_entry(cp, cc, pid[cn[i]], pid[cn[j]]);
+                for (int i = 0; i < NP; ++i)
+                    for (int j = 0; j < NP; ++j)
+                        e2c[(NP * (size_t)e + i) * NP + j] = find_entry(cp, cc, pid[cn[i]], pid[cn[j]]);
             }
             cudaStream_t st = c->stream;
             auto up32 = [&](DevBuf<int32_t>& d, const std::vector<int32_t>& h) { d.alloc(std::max<size_t>(1, h.size())); d.upload(h.data(), h.size(), st); };
@@ -594,7 +604,7 @@ int mphy_mixed_elem_eval(mphy_mixed* m, const double* disp, const double* disp_p
         a.Kup = Kup;
         a.Kpp = Kpp;
         a.FP = FP;
-        launch_elem_mixed(a, 1, st);
+        launch_elem_mixed(a, m->npe, 1, st);
         unsigned long long h = 0;
         MPHY_CUDA(cudaMemcpyAsync(&h, m->bad.p, sizeof(h), cudaMemcpyDeviceToHost, st));
         MPHY_CUDA(cudaStreamSynchronize(st));

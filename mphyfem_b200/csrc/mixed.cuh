@@ -19,9 +19,9 @@ struct MixedElemArgs {
     double* Kpp = nullptr;
     double* FP = nullptr;
     // assembly: entry indices of element pairs, values (3 per B / B^T entry, 1 per C entry)
-    const uint32_t* e2b = nullptr;   // [n_elem][10][4]
-    const uint32_t* e2bt = nullptr;  // [n_elem][4][10]
-    const uint32_t* e2c = nullptr;   // [n_elem][4][4]
+    const uint32_t* e2b = nullptr;   // [n_elem][npe][NP]  (NP pressure nodes: 4 tet10, 8 hex27)
+    const uint32_t* e2bt = nullptr;  // [n_elem][NP][npe]
+    const uint32_t* e2c = nullptr;   // [n_elem][NP][NP]
     double* bval = nullptr;
     double* btval = nullptr;
     double* cval = nullptr;
@@ -34,7 +34,11 @@ struct MixedElemArgs {
     double* fp_e = nullptr;
 };
 
-void launch_elem_mixed(const MixedElemArgs& a, int mode, cudaStream_t s);
+// Elem_Solid_3D_Mixed1 element kernel: npe 10 (tet10, 4 vertex pressures) or 27 (hex27, 8
+// corner pressures)
+void launch_elem_mixed(const MixedElemArgs& a, int npe, int mode, cudaStream_t s);
+// hex27 shape tables of the Mixed1 kernel (once per device before its first launch)
+void upload_hex27_tables();
 // Elem_Solid_3D_Mixed0 (hex8 or tet10, one pressure per element), condensed: the displacement
 // element's outputs (Ke/Re export or the scatter of ElemArgs) plus kup_e, kpp_e, fp_e.
 void launch_elem_mixed0(const MixedElemArgs& a, int npe, int mode, cudaStream_t s);

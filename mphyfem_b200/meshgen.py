@@ -202,6 +202,65 @@ def tet10_kuhn(nx: int, ny: int, nz: int, lx: float = 4.0, ly: float = 1.0, lz: 
     )
 
 
+# 27-node hex node order (BasisFunctionsLagrange.cpp:1300-1399): the 1D indices (i, j, k) of each
+# node, 0 at xi = -1, 1 at xi = +1, 2 at the midpoint (the 1D quadratic Lagrange order)
+HEX27_IJK = np.array([
+    [0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0], [0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1],
+    [2, 0, 0], [0, 2, 0], [0, 0, 2], [1, 2, 0], [1, 0, 2], [2, 1, 0], [1, 1, 2], [0, 1, 2],
+    [2, 0, 1], [0, 2, 1], [1, 2, 1], [2, 1, 1], [2, 2, 0], [2, 0, 2], [0, 2, 2], [1, 2, 2],
+    [2, 1, 2], [2, 2, 1], [2, 2, 2]], dtype=np.int64)
+
+
+def hex27_cantilever(nx: int, ny: int, nz: int, lx: float = 4.0, ly: float = 1.0, lz: float = 1.0,
+                     jitter: float = 0.0, seed: int = 7, traction=(0.0, 0.0, -0.02), mu: float = 1.0,
+                     kappa: float = 100.0, name: str | None = None) -> Problem:
+    """27-node hex block [0,lx]x[0,ly]x[0,lz] (the P2 displacement of Elem_Solid_3D_Mixed1's
+    P2-P1 hex; its 8 corner nodes carry the pressure), clamped at x = 0, uniform traction on
+    x = lx. Nodes sit on the (2nx+1)(2ny+1)(2nz+1) half-spacing grid, x fastest; interior grid
+    nodes may be jittered by U(-jitter*h/2, jitter*h/2) per coordinate (numpy PCG64(seed)), which
+    keeps every element's edges straight only when jitter = 0."""
+    mx, my, mz = 2 * nx + 1, 2 * ny + 1, 2 * nz + 1
+    gx, gy, gz = np.linspace(0.0, lx, mx), np.linspace(0.0, ly, my), np.linspace(0.0, lz, mz)
+    Z, Y, X = np.meshgrid(gz, gy, gx, indexing="ij")
+    coords = np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1)
+    if jitter > 0.0:
+        h = np.array([lx / nx, ly / ny, lz / nz]) * 0.5
+        rng = np.random.Generator(np.random.PCG64(seed))
+        jit = rng.uniform(-jitter, jitter, size=coords.shape) * h[None, :]
+        interior = ((coords[:, 0] > 1e-12) & (coords[:, 0] < lx - 1e-12) & (coords[:, 1] > 1e-12)
+                    & (coords[:, 1] < ly - 1e-12) & (coords[:, 2] > 1e-12) & (coords[:, 2] < lz - 1e-12))
+        coords = coords + jit * interior[:, None]
+    off = np.array([0, 2, 1])  # grid offset of 1D index 0 (xi = -1), 1 (xi = +1), 2 (midpoint)
+    ex, ey, ez = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    ex, ey, ez = ex.transpose(2, 1, 0).ravel(), ey.transpose(2, 1, 0).ravel(), ez.transpose(2, 1, 0).ravel()
+    gxi = 2 * ex[:, None] + off[HEX27_IJK[:, 0]][None, :]
+    gyi = 2 * ey[:, None] + off[HEX27_IJK[:, 1]][None, :]
+    gzi = 2 * ez[:, None] + off[HEX27_IJK[:, 2]][None, :]
+    conn = (gxi + mx * (gyi + my * gzi)).astype(np.int32)
+    n_node = coords.shape[0]
+    fixed = np.zeros((n_node, 3), dtype=np.uint8)
+    fixed[np.abs(coords[:, 0]) < 1e-12] = 1
+    # consistent nodal forces of a uniform traction on the 9-node faces of x = lx: the 1D
+    # quadratic weights (1/6, 2/3, 1/6) of each face edge, tensored
+    t = np.asarray(traction, dtype=np.float64)
+    fnodal = np.zeros((n_node, 3), dtype=np.float64)
+    w1 = np.array([1.0 / 6.0, 2.0 / 3.0, 1.0 / 6.0])
+    area = (ly / ny) * (lz / nz)
+    for fy in range(ny):
+        for fz in range(nz):
+            for a in range(3):
+                for b in range(3):
+                    nid = (mx - 1) + mx * ((2 * fy + a) + my * (2 * fz + b))
+                    fnodal[nid] += t * area * w1[a] * w1[b]
+    return Problem(
+        name=name or f"hex27_{nx}x{ny}x{nz}",
+        coords=coords, conn=conn, mat_id=np.zeros(conn.shape[0], np.int32),
+        mats=nh_material(mu, kappa)[None, :], fixed=fixed.ravel(), fnodal=fnodal.ravel(),
+        dt=0.1, max_steps=10, newton_rtol=1e-8, cg_rtol=1e-8,
+        meta={"nx": nx, "ny": ny, "nz": nz, "seed": seed, "traction": list(map(float, t)), "element": "hex27"},
+    )
+
+
 def tet10_near_incompressible() -> Problem:
     """Near-incompressible unstructured form: Kuhn tet10 on 96(x) x 48 x 48, kappa = 100."""
     return tet10_kuhn(96, 48, 48, name="tet10_kuhn_96x48x48")

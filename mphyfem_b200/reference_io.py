@@ -46,13 +46,13 @@ import numpy as np
 
 from .meshgen import Problem
 
-GMSH_VOLUME = {5: 8, 11: 10}          # hex8, tet10
+GMSH_VOLUME = {5: 8, 11: 10, 12: 27}  # hex8, tet10, hex27 (the 27-node hex order is Gmsh's)
 # material name -> (model code of mphy.h, config line holding its parameters, parameter count)
 MATERIALS = {"Matl_NeoHookean": (0, "data_deviatoric", 1), "Matl_MooneyRivlin": (1, "data_deviatoric", 2),
              "Matl_Gent": (2, "data_deviatoric", 2), "Matl_ArrudaBoyce": (3, "data", 2)}
 MATERIAL_NAME = {code: name for name, (code, _, _) in MATERIALS.items()}
-GMSH_FACE = {3: 4, 2: 3, 9: 6}        # quad4, tri3, tri6
-GMSH_TYPE_OF = {8: 5, 10: 11, 4: 3, 3: 2, 6: 9}
+GMSH_FACE = {3: 4, 2: 3, 9: 6, 10: 9}  # quad4, tri3, tri6, quad9
+GMSH_TYPE_OF = {8: 5, 10: 11, 27: 12, 4: 3, 3: 2, 6: 9, 9: 10}
 DOF_NAMES = {"x": 0, "y": 1, "z": 2, "ux": 0, "uy": 1, "uz": 2, "0": 0, "1": 1, "2": 2}
 
 
@@ -251,17 +251,39 @@ class TimeFunction:
 _G = 0.577350269189626
 
 
+_G3 = (-0.774596669241483, 0.774596669241483, 0.0)   # QuadratureUtil.cpp:29-33
+_W3 = (5.0 / 9.0, 5.0 / 9.0, 8.0 / 9.0)
+
+
 def _face_rule(npf):
     if npf == 4:
         return [(-_G, -_G, 1.0), (_G, -_G, 1.0), (_G, _G, 1.0), (-_G, _G, 1.0)]
+    if npf == 9:
+        # 3x3 rule on the quad9 face (its points in xi1-fastest order)
+        return [(_G3[i], _G3[j], _W3[i] * _W3[j]) for j in range(3) for i in range(3)]
     if npf == 3:
         return [(1.0 / 3.0, 1.0 / 3.0, 0.5)]
     if npf == 6:
         return [(1.0 / 6.0, 1.0 / 6.0, 0.5 / 3.0), (4.0 / 6.0, 1.0 / 6.0, 0.5 / 3.0), (1.0 / 6.0, 4.0 / 6.0, 0.5 / 3.0)]
-    raise ValueError(f"face with {npf} nodes: quad4, tri3 and tri6 faces are supported")
+    raise ValueError(f"face with {npf} nodes: quad4, quad9, tri3 and tri6 faces are supported")
+
+
+# quad9 face nodes (BasisFunctionsLagrange.cpp, LagrangeBasisFunsQuad case 9): the 1D quadratic
+# indices (u, v) of each node, 0 at -1, 1 at +1, 2 at the midpoint -- corners, mid-edges of
+# (0,1), (1,2), (2,3), (3,0), centre (Gmsh's quad9 order)
+_QUAD9 = ((0, 0), (1, 0), (1, 1), (0, 1), (2, 0), (1, 2), (2, 1), (0, 2), (2, 2))
 
 
 def _face_shape(npf, a, b):
+    if npf == 9:
+        def q(x):
+            return (0.5 * (x * x - x), 0.5 * (x * x + x), 1.0 - x * x), (x - 0.5, x + 0.5, -2.0 * x)
+        nu, dnu = q(a)
+        nv, dnv = q(b)
+        N = np.array([nv[j] * nu[i] for i, j in _QUAD9])
+        d1 = np.array([nv[j] * dnu[i] for i, j in _QUAD9])
+        d2 = np.array([dnv[j] * nu[i] for i, j in _QUAD9])
+        return N, d1, d2
     if npf == 4:
         nu, dnu = [0.5 * (1 - a), 0.5 * (1 + a)], [-0.5, 0.5]
         nv, dnv = [0.5 * (1 - b), 0.5 * (1 + b)], [-0.5, 0.5]
@@ -376,11 +398,12 @@ def read_config(config_path, mesh_path=None):
     mesh_path = mesh_path or os.path.join(os.path.dirname(os.path.abspath(config_path)), files["mesh"])
     m = read_gmsh22(mesh_path)
     if m["ndim"] != 3:
-        raise NotImplementedError("config: this build solves 3D meshes (hex8, tet10)")
+        raise NotImplementedError("config: this build solves 3D meshes (hex8, tet10, hex27)")
     vol = m["volume"]
     npe = {GMSH_VOLUME.get(t) for t, _, _ in vol}
     if None in npe or len(npe) != 1:
-        raise NotImplementedError("mesh: volume elements must all be hex8 (type 5) or all tet10 (type 11)")
+        raise NotImplementedError("mesh: volume elements must all be hex8 (type 5), all tet10 (type 11) or all "
+                                  "hex27 (type 12)")
     npe = npe.pop()
     # materials: one row per material the domains use, in domain-tag order of first use
     tag_mat = {}
@@ -466,8 +489,10 @@ def read_config(config_path, mesh_path=None):
     etype = etypes.pop()
     if etype not in ELEMENT_TYPES:
         raise NotImplementedError(f"config: element type {etype!r}: supported are {ELEMENT_TYPES}")
-    if etype == "ELEM_SOLID_3D_MIXED1" and npe != 10:
-        raise NotImplementedError("config: ELEM_SOLID_3D_MIXED1 is built for tet10 meshes")
+    if etype == "ELEM_SOLID_3D_MIXED1" and npe not in (10, 27):
+        raise NotImplementedError("config: ELEM_SOLID_3D_MIXED1 is built for tet10 and hex27 meshes")
+    if npe == 27 and etype != "ELEM_SOLID_3D_MIXED1":
+        raise NotImplementedError("config: 27-node hexes are built for ELEM_SOLID_3D_MIXED1 (P2-P1) only")
     prob = Problem(name=os.path.basename(config_path), coords=coords, conn=conn, mat_id=mat_id,
                    mats=np.array(rows, dtype=np.float64), fixed=fixed.ravel(), fnodal=F.ravel(),
                    dt=dt, t_final=tfin, max_steps=solver["maximumSteps"],
@@ -500,7 +525,9 @@ def write_config(path, mesh_name, prob: Problem, fixed_patches=(), domain_names=
         out += ["Material", "{", f"  id              : {m + 1}", f"  name            : {name}",
                 "  density         : 1.0", f"  {line:<15} : " + " ".join(repr(float(v)) for v in par),
                 f"  data_volumetric : {int(ut)} {float(kinv)!r}", "}", ""]
-    etype = "ELEM_SOLID_3D_DISP"
+    etype = prob.meta.get("element") or ("ELEM_SOLID_3D_MIXED1" if prob.npe == 27 else "ELEM_SOLID_3D_DISP")
+    if etype == "hex27":
+        etype = "ELEM_SOLID_3D_MIXED1"
     out += ["Element", "{", "  id   : 1", f"  type : {etype}", "}", ""]
     if fixed_patches:
         out += ["Boundary Conditions", "{"]
@@ -530,9 +557,14 @@ def write_config(path, mesh_name, prob: Problem, fixed_patches=(), domain_names=
 
 def boundary_faces(prob: Problem, predicate):
     """Faces of the volume elements whose nodes all satisfy predicate(coords) (hex8: quad4 faces
-    in the element's outward corner order; tet10: tri6 faces), each face once."""
+    in the element's outward corner order; hex27: quad9 faces, the same corners, then the
+    mid-edge nodes and the face centre; tet10: tri6 faces), each face once."""
     if prob.npe == 8:
         local = [[0, 3, 2, 1], [4, 5, 6, 7], [0, 1, 5, 4], [1, 2, 6, 5], [2, 3, 7, 6], [3, 0, 4, 7]]
+    elif prob.npe == 27:
+        local = [[0, 3, 2, 1, 9, 13, 11, 8, 20], [4, 5, 6, 7, 16, 18, 19, 17, 25],
+                 [0, 1, 5, 4, 8, 12, 16, 10, 21], [1, 2, 6, 5, 11, 14, 18, 12, 23],
+                 [2, 3, 7, 6, 13, 15, 19, 14, 24], [3, 0, 4, 7, 9, 10, 17, 15, 22]]
     else:
         # tet10 faces: vertices then the mid-side nodes of (0,1), (1,2), (2,0) of the face
         local = [[0, 2, 1, 6, 5, 4], [0, 1, 3, 4, 9, 7], [1, 2, 3, 5, 8, 9], [0, 3, 2, 7, 8, 6]]

@@ -162,16 +162,26 @@ def material_stress_tangent_mixed(model, data, F, Kinv, pres, utype=3):
     return s, Cm.reshape(9, 9)
 
 
+def mixed_pressure_nodes(npe: int) -> int:
+    """Pressure nodes of Elem_Solid_3D_Mixed1: the 4 vertices of a tet10, the 8 corners of a hex27."""
+    return {10: 4, 27: 8}[npe]
+
+
 def elem_mixed(X, u, u_prev, pn, model, data, Kinv, utype=3):
-    """Mixed u-p tet10 element (linear vertex pressure): Kuu, Kup, Kpu, Kpp, FU, FP, bad."""
+    """Mixed u-p element, Elem_Solid_3D_Mixed1: tet10 with linear vertex pressure, or hex27 with
+    trilinear corner pressure (P2-P1). Returns Kuu, Kup, Kpu, Kpp, FU, FP, bad."""
     X, u, up, pn = (np.ascontiguousarray(a, dtype=np.float64) for a in (X, u, u_prev, pn))
+    npe = X.shape[0]
+    if npe not in (10, 27):
+        raise ValueError("oracle: the mixed element is tet10 or hex27")
+    ns, NP = 3 * npe, mixed_pressure_nodes(npe)
     d = _mat_data(data)
-    Kuu, Kup, Kpu, Kpp = np.zeros((30, 30)), np.zeros((30, 4)), np.zeros((4, 30)), np.zeros((4, 4))
-    FU, FP = np.zeros(30), np.zeros(4)
-    bad = lib().orc_elem_mixed(X.shape[0], _p(X, _d), _p(u, _d), _p(up, _d), _p(pn, _d), int(model), _p(d, _d), Kinv,
+    Kuu, Kup, Kpu, Kpp = np.zeros((ns, ns)), np.zeros((ns, NP)), np.zeros((NP, ns)), np.zeros((NP, NP))
+    FU, FP = np.zeros(ns), np.zeros(NP)
+    bad = lib().orc_elem_mixed(npe, _p(X, _d), _p(u, _d), _p(up, _d), _p(pn, _d), int(model), _p(d, _d), Kinv,
                                utype, _p(Kuu, _d), _p(Kup, _d), _p(Kpu, _d), _p(Kpp, _d), _p(FU, _d), _p(FP, _d))
     if bad == 2:
-        raise ValueError("oracle: the mixed element is tet10 only")
+        raise ValueError("oracle: the mixed element is tet10 or hex27")
     return Kuu, Kup, Kpu, Kpp, FU, FP, bad
 
 
@@ -191,8 +201,8 @@ def elem_mixed0(X, u, u_prev, pres, model, data, Kinv, utype=3):
 
 
 def gauss_rule(npe):
-    xi, w = np.zeros((8, 3)), np.zeros(8)
-    N, dN = np.zeros((8, npe)), np.zeros((8, 3, npe))
+    xi, w = np.zeros((27, 3)), np.zeros(27)
+    N, dN = np.zeros((27, npe)), np.zeros((27, 3, npe))
     ngp = lib().orc_gauss_rule(npe, _p(xi, _d), _p(w, _d), _p(N, _d), _p(dN, _d))
     return xi[:ngp], w[:ngp], N[:ngp], dN[:ngp]
 

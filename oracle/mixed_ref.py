@@ -1,5 +1,6 @@
-"""Mixed u-p problems (tet10 displacement, linear vertex pressure): numpy/scipy restatement of the
-two-field assembly and of the Newton load stepping with pressure unknowns.
+"""Mixed u-p problems (Elem_Solid_3D_Mixed1: tet10 displacement with linear vertex pressure, or
+hex27 displacement with trilinear corner pressure): numpy/scipy restatement of the two-field
+assembly and of the Newton load stepping with pressure unknowns.
 
 TEST INFRASTRUCTURE ONLY: the checker for the GPU mixed path (tests/). The element matrices come
 from the C oracle (orc_problem_elements_mixed); this module restates:
@@ -29,7 +30,7 @@ from . import binding as B
 
 def pressure_dofs(prob):
     """(pressure nodes ascending, id_pres [n_node] with -1 off the pressure nodes)."""
-    pn = np.unique(np.asarray(prob.conn)[:, :4])
+    pn = np.unique(np.asarray(prob.conn)[:, :B.mixed_pressure_nodes(prob.npe)])
     idp = -np.ones(prob.n_node, np.int64)
     idp[pn] = np.arange(len(pn))
     return pn, idp
@@ -37,9 +38,10 @@ def pressure_dofs(prob):
 
 class MixedProblem:
     def __init__(self, prob):
-        if prob.npe != 10:
-            raise ValueError("mixed u-p problems are tet10 (linear vertex pressure)")
+        if prob.npe not in (10, 27):
+            raise ValueError("mixed u-p problems are tet10 or hex27")
         self.prob = prob
+        self.ns, self.NP = 3 * prob.npe, B.mixed_pressure_nodes(prob.npe)
         self.op = B.OracleProblem(prob)
         self.afs, self.fav, _, _ = self.op.pattern()
         self.nu = self.op.n_free
@@ -50,9 +52,9 @@ class MixedProblem:
         lib.orc_problem_elements_mixed.restype = C.c_int64
 
     def elements(self, disp, disp_prev, pres, nthreads=1):
-        ne = self.prob.n_elem
-        Kuu, Kup, Kpp = np.zeros((ne, 30, 30)), np.zeros((ne, 30, 4)), np.zeros((ne, 4, 4))
-        FU, FP = np.zeros((ne, 30)), np.zeros((ne, 4))
+        ne, ns, NP = self.prob.n_elem, self.ns, self.NP
+        Kuu, Kup, Kpp = np.zeros((ne, ns, ns)), np.zeros((ne, ns, NP)), np.zeros((ne, NP, NP))
+        FU, FP = np.zeros((ne, ns)), np.zeros((ne, NP))
         d, dp, p = (np.ascontiguousarray(a, np.float64) for a in (disp, disp_prev, pres))
         bad = B.lib().orc_problem_elements_mixed(self.op.h, B._p(d, B._d), B._p(dp, B._d), B._p(p, B._d),
                                                  B._p(Kuu, B._d), B._p(Kup, B._d), B._p(Kpp, B._d), B._p(FU, B._d),
@@ -62,9 +64,9 @@ class MixedProblem:
     def assemble(self, disp, disp_prev, pres, nthreads=1):
         """(A [nu+np, nu+np] CSR, rhs [nu+np], reactions [3 n_node], first bad element or -1)."""
         Kuu, Kup, Kpp, FU, FP, bad = self.elements(disp, disp_prev, pres, nthreads)
-        nu, n = self.nu, self.nu + self.np
+        nu, n, ns, NP = self.nu, self.nu + self.np, self.ns, self.NP
         fav = self.fav.astype(np.int64)
-        pdof = nu + self.idp[np.asarray(self.prob.conn)[:, :4]]  # [ne, 4]
+        pdof = nu + self.idp[np.asarray(self.prob.conn)[:, :NP]]  # [ne, NP]
         rows, cols, vals = [], [], []
 
         def add(r, c, v):
@@ -73,16 +75,16 @@ class MixedProblem:
             cols.append(c[m])
             vals.append(v[m])
 
-        add(np.repeat(fav, 30, axis=1).ravel(), np.tile(fav, (1, 30)).ravel(), Kuu.ravel())
-        add(np.repeat(fav, 4, axis=1).ravel(), np.tile(pdof, (1, 30)).ravel(), Kup.ravel())
-        add(np.tile(pdof, (1, 30)).ravel(), np.repeat(fav, 4, axis=1).ravel(), Kup.ravel())
-        add(np.repeat(pdof, 4, axis=1).ravel(), np.tile(pdof, (1, 4)).ravel(), Kpp.ravel())
+        add(np.repeat(fav, ns, axis=1).ravel(), np.tile(fav, (1, ns)).ravel(), Kuu.ravel())
+        add(np.repeat(fav, NP, axis=1).ravel(), np.tile(pdof, (1, ns)).ravel(), Kup.ravel())
+        add(np.tile(pdof, (1, ns)).ravel(), np.repeat(fav, NP, axis=1).ravel(), Kup.ravel())
+        add(np.repeat(pdof, NP, axis=1).ravel(), np.tile(pdof, (1, NP)).ravel(), Kpp.ravel())
         A = sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(n, n))
         rhs = np.zeros(n)
         m = fav >= 0
         np.add.at(rhs, fav[m], FU[m])
         np.add.at(rhs, pdof.ravel(), FP.ravel())
-        gdof = (3 * np.asarray(self.prob.conn, np.int64)[:, :, None] + np.arange(3)).reshape(-1, 30)
+        gdof = (3 * np.asarray(self.prob.conn, np.int64)[:, :, None] + np.arange(3)).reshape(-1, ns)
         reac = np.zeros(self.prob.n_dof)
         np.add.at(reac, gdof.ravel(), FU.ravel())
         return A, rhs, reac, bad

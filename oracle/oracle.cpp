@@ -18,8 +18,8 @@
 
 namespace {
 
-constexpr int kMaxNpe = 10;
-constexpr int kMaxGp = 8;
+constexpr int kMaxNpe = 27;
+constexpr int kMaxGp = 27;
 
 struct GaussRule {
     int ngp = 0;
@@ -93,14 +93,62 @@ void shape_tet10(const double* xi, double* N, double dN[3][kMaxNpe]) {
     }
 }
 
+// Triquadratic hex (BasisFunctionsLagrange.cpp:1202-1399): tensor product of the quadratic 1D
+// Lagrange triple of :45-61, ordered (xi = -1, xi = +1, xi = 0), with the 27-node order of
+// :1300-1399 -- corners as hex8, then the mid-edge nodes 8..19, the mid-face nodes 20..25 and
+// the centre 26. Entry a of kHex27 holds the 1D indices (i, j, k) of node a.
+constexpr int kHex27[27][3] = {
+    {0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0}, {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1},
+    {2, 0, 0}, {0, 2, 0}, {0, 0, 2}, {1, 2, 0}, {1, 0, 2}, {2, 1, 0}, {1, 1, 2}, {0, 1, 2},
+    {2, 0, 1}, {0, 2, 1}, {1, 2, 1}, {2, 1, 1}, {2, 2, 0}, {2, 0, 2}, {0, 2, 2}, {1, 2, 2},
+    {2, 1, 2}, {2, 2, 1}, {2, 2, 2}};
+
+void shape_hex27(const double* xi, double* N, double dN[3][kMaxNpe]) {
+    double n1[3][3], d1[3][3];
+    for (int d = 0; d < 3; ++d) {
+        const double x = xi[d], x2 = x * x;
+        n1[d][0] = 0.5 * (x2 - x);
+        n1[d][1] = 0.5 * (x2 + x);
+        n1[d][2] = 1.0 - x2;
+        d1[d][0] = 0.5 * (2.0 * x - 1.0);
+        d1[d][1] = 0.5 * (2.0 * x + 1.0);
+        d1[d][2] = -2.0 * x;
+    }
+    for (int a = 0; a < 27; ++a) {
+        const int i = kHex27[a][0], j = kHex27[a][1], k = kHex27[a][2];
+        N[a] = n1[0][i] * n1[1][j] * n1[2][k];
+        dN[0][a] = d1[0][i] * n1[1][j] * n1[2][k];
+        dN[1][a] = n1[0][i] * d1[1][j] * n1[2][k];
+        dN[2][a] = n1[0][i] * n1[1][j] * d1[2][k];
+    }
+}
+
+// Hex 3x3x3 rule of QuadratureUtil.cpp:497-524: the 3-point 1D rule of :29-33 (-0.7746.., +0.7746..,
+// 0; weights 5/9, 5/9, 8/9), point q at the 1D indices of hex27 node q (kHex27), weight
+// w_i w_j w_k in that product order.
+void rule_hex27(GaussRule& r) {
+    const double g[3] = {-0.774596669241483, 0.774596669241483, 0.0};
+    const double wt[3] = {5.0 / 9.0, 5.0 / 9.0, 8.0 / 9.0};
+    r.ngp = 27;
+    for (int q = 0; q < 27; ++q) {
+        for (int d = 0; d < 3; ++d) r.xi[q][d] = g[kHex27[q][d]];
+        r.w[q] = wt[kHex27[q][0]] * wt[kHex27[q][1]] * wt[kHex27[q][2]];
+    }
+}
+
+// The quadrature of each element, getGaussPoints3D (QuadratureUtil.cpp:268-317): 2x2x2 for
+// hex8, 4 points for tet10, 3x3x3 for the 27-node hex (which ElementBase::calcStiffnessAndResidualMixed3D
+// uses for Elem_Solid_3D_Mixed1, ElementBase2.cpp:320, whatever nGP prepareElemData set).
 bool element_rule(int npe, GaussRule& r) {
     if (npe == 8) { rule_hex8(r); return true; }
     if (npe == 10) { rule_tet4(r); return true; }
+    if (npe == 27) { rule_hex27(r); return true; }
     return false;
 }
 
 void shape(int npe, const double* xi, double* N, double dN[3][kMaxNpe]) {
     if (npe == 8) shape_hex8(xi, N, dN);
+    else if (npe == 27) shape_hex27(xi, N, dN);
     else shape_tet10(xi, N, dN);
 }
 
@@ -486,7 +534,7 @@ int orc_elem_stiffness_residual(int npe, const double* X, const double* u, doubl
 int orc_elem_stiffness_residual_mat(int npe, const double* X, const double* u, int model, const double* data,
                                     double Kinv, int Utype, double* K, double* R) {
     GaussRule rule;
-    if (!element_rule(npe, rule)) return 2;
+    if (npe == 27 || !element_rule(npe, rule)) return 2;  // displacement element: hex8 and tet10
     const int ns = 3 * npe;
     std::fill(K, K + ns * ns, 0.0);
     std::fill(R, R + ns, 0.0);
@@ -671,7 +719,8 @@ extern "C" {
 orc_problem* orc_problem_create(int n_node, const double* coords, int n_elem, int npe,
                                 const int32_t* conn, const int32_t* mat_id, int n_mat,
                                 const double* mats, const uint8_t* fixed) {
-    if (npe != 8 && npe != 10) return nullptr;
+    // 27-node hexes only for the mixed u-p element (orc_problem_elements_mixed)
+    if (npe != 8 && npe != 10 && npe != 27) return nullptr;
     orc_problem* p = new orc_problem;
     p->n_node = n_node;
     p->n_elem = n_elem;
@@ -712,6 +761,7 @@ void orc_problem_export_pattern(const orc_problem* p, int32_t* assy_for_soln, in
 
 int64_t orc_problem_elements(const orc_problem* p, const double* disp, double* Ke, double* Re,
                              int nthreads) {
+    if (p->npe == 27) return -2;  // displacement element: hex8 and tet10 only
     const int ns = 3 * p->npe;
     // the first bad element in ascending order, as the reference's serial loop meets it
     int64_t first_bad = p->n_elem;
@@ -725,22 +775,26 @@ int64_t orc_problem_elements(const orc_problem* p, const double* disp, double* K
     return first_bad == p->n_elem ? -1 : first_bad;
 }
 
+// Per element: Kuu [ns][ns], Kup [ns][NP], Kpp [NP][NP], FU [ns], FP [NP] with ns = 3 npe and
+// NP = 4 (tet10) or 8 (hex27).
 int64_t orc_problem_elements_mixed(const orc_problem* p, const double* disp, const double* disp_prev,
                                    const double* pres, double* Kuu, double* Kup, double* Kpp, double* FU, double* FP,
                                    int nthreads) {
-    if (p->npe != 10) return -2;
+    if (p->npe != 10 && p->npe != 27) return -2;
+    const int npe = p->npe, NP = npe == 10 ? 4 : 8, ns = 3 * npe;
     int64_t first_bad = p->n_elem;
     set_threads(nthreads);
 #pragma omp parallel for schedule(static) reduction(min : first_bad) if (nthreads > 1)
     for (int64_t e = 0; e < p->n_elem; ++e) {
-        double X[30], u[30], up[30], pn[4], Kpu[120];
+        double X[3 * kMaxNpe], u[3 * kMaxNpe], up[3 * kMaxNpe], pn[8], Kpu[8 * 3 * kMaxNpe];
         gather_element(p, e, disp, X, u);
         gather_element(p, e, disp_prev, X, up);
-        for (int i = 0; i < 4; ++i) pn[i] = pres[p->conn[e * 10 + i]];
+        for (int i = 0; i < NP; ++i) pn[i] = pres[p->conn[e * npe + i]];
         const size_t id = (size_t)p->mat_id[e];
         const double* m = &p->mats[3 * id];
-        const int bad = orc_elem_mixed(10, X, u, up, pn, p->model[id], &p->data[ORC_MAT_NDATA * id], m[1], (int)m[2],
-                                       Kuu + e * 900, Kup + e * 120, Kpu, Kpp + e * 16, FU + e * 30, FP + e * 4);
+        const int bad = orc_elem_mixed(npe, X, u, up, pn, p->model[id], &p->data[ORC_MAT_NDATA * id], m[1], (int)m[2],
+                                       Kuu + e * ns * ns, Kup + e * ns * NP, Kpu, Kpp + e * NP * NP, FU + e * ns,
+                                       FP + e * NP);
         if (bad && e < first_bad) first_bad = e;
     }
     return first_bad == p->n_elem ? -1 : first_bad;
@@ -751,6 +805,7 @@ int64_t orc_problem_elements_mixed(const orc_problem* p, const double* disp, con
 // (ElementBase.cpp:567-594) into the free rows of every element before its scatter.
 static int64_t assemble_impl(const orc_problem* p, const double* disp, double* val, double* rhs, double* reac,
                              int nthreads, const double* lift) {
+    if (p->npe == 27) return -2;  // the displacement element's 27-point hex27 rule is not restated
     const CsrPattern& P = p->pat;
     const int ns = 3 * p->npe;
     if (val) std::fill(val, val + P.rowptr.back(), 0.0);
@@ -1058,14 +1113,18 @@ static int mixed_blocks(int npe, int NP, const double* X, const double* u, const
         const double J = det3(Fa);
         if (J < 0.0) bad = 1;
         const double dvol = rule.w[q] * spatial_gradients(npe, x, dN, g);
-        // LagrangeBasisFunsTetra(4): the barycentric coordinates, vertex order; or Np = 1
+        // pressure basis: LagrangeBasisFunsTetra(4) (the barycentric coordinates, vertex order),
+        // LagrangeBasisFunsHexa(8) (trilinear, the hex27's corner nodes), or Np = 1
         const double* xi = rule.xi[q];
-        double Np[4] = {1.0, 0.0, 0.0, 0.0};
+        double Np[8] = {1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         if (NP == 4) {
             Np[0] = 1.0 - xi[0] - xi[1] - xi[2];
             Np[1] = xi[0];
             Np[2] = xi[1];
             Np[3] = xi[2];
+        } else if (NP == 8) {
+            double dNp[3][kMaxNpe];
+            shape_hex8(xi, Np, dNp);
         }
         double pres = 0.0;
         for (int i = 0; i < NP; ++i) pres += Np[i] * pn[i];
@@ -1101,11 +1160,14 @@ static int mixed_blocks(int npe, int NP, const double* X, const double* u, const
     return bad;
 }
 
+// Elem_Solid_3D_Mixed1 (Elem_Solid_3D_Mixed1.cpp:34-76): tet10 with 4 vertex pressures, or the
+// 27-node hex with 8 corner pressures (P2-P1).
 int orc_elem_mixed(int npe, const double* X, const double* u, const double* u_prev, const double* pn, int model,
                    const double* data, double Kinv, int Utype, double* Kuu, double* Kup, double* Kpu, double* Kpp,
                    double* FU, double* FP) {
-    if (npe != 10) return 2;
-    return mixed_blocks(10, 4, X, u, u_prev, pn, model, data, Kinv, Utype, Kuu, Kup, Kpu, Kpp, FU, FP);
+    if (npe != 10 && npe != 27) return 2;
+    return mixed_blocks(npe, npe == 10 ? 4 : 8, X, u, u_prev, pn, model, data, Kinv, Utype, Kuu, Kup, Kpu, Kpp, FU,
+                        FP);
 }
 
 int orc_elem_mixed0(int npe, const double* X, const double* u, const double* u_prev, double pres, int model,

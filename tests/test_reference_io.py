@@ -252,3 +252,31 @@ def test_reference_example4_on_a_generated_block(tmp_path):
     assert F[:, 2].sum() == pytest.approx(320.0 * 0.25, rel=1e-12)
     assert np.abs(F[:, :2]).max() <= 1e-12 * 320
     assert (q.dt, q.t_final, q.max_steps) == (0.2, 1.0, 10)
+
+
+def test_hex27_round_trip_and_element_type(tmp_path):
+    """A 27-node hex mesh (Gmsh type 12, the same node order as the reference's hex27) with its
+    quad9 clamp faces: read back as the same problem, element type ELEM_SOLID_3D_MIXED1."""
+    p = meshgen.hex27_cantilever(3, 2, 2, jitter=0.1)
+    clamp = rio.boundary_faces(p, lambda X: np.isclose(X[:, 0], 0.0))
+    assert len(clamp) == 4 and all(len(fc) == 9 for fc in clamp)
+    q = _write(tmp_path, p, {"clamp": clamp})
+    assert q.npe == 27 and q.meta["element"] == "ELEM_SOLID_3D_MIXED1"
+    assert np.array_equal(q.coords, p.coords) and np.array_equal(q.conn, p.conn)
+    assert np.array_equal(q.fixed, p.fixed) and np.array_equal(q.fnodal, p.fnodal)
+
+
+def test_quad9_traction_matches_consistent_nodal_forces():
+    """The hex27 cantilever's load, t = (0, 0, -0.05) on x = 4, as a Tractions block on the quad9
+    faces ordered so that dx/dxi1 runs along z: the generator's consistent nodal forces (the 1D
+    quadratic weights 1/6, 2/3, 1/6, tensored), and the total force."""
+    p = meshgen.hex27_cantilever(4, 2, 2, traction=(0.0, 0.0, -0.05))
+    faces = [[fc[0], fc[3], fc[2], fc[1], fc[7], fc[6], fc[5], fc[4], fc[8]]
+             for fc in rio.boundary_faces(p, lambda X: np.isclose(X[:, 0], 4.0))]
+    hz = 1.0 / 2
+    F = rio.traction_forces(p.coords, faces, [0.0, -0.05 / (hz / 2.0), 0.0])
+    assert np.allclose(F.ravel(), p.fnodal, rtol=1e-13, atol=1e-16)
+    assert np.allclose(F.sum(axis=0), [0.0, 0.0, -0.05 * 1.0], rtol=1e-13)
+    # normal part: the face area (outward corner order: dv x du points into the body)
+    Fn = rio.traction_forces(p.coords, rio.boundary_faces(p, lambda X: np.isclose(X[:, 0], 4.0)), [0.3, 0.0, 0.0])
+    assert np.allclose(Fn.sum(axis=0), [-0.3, 0.0, 0.0], rtol=1e-13, atol=1e-15)
