@@ -3,11 +3,10 @@
 //
 // Setup per operator:
 //   1. centroids of the current coordinates per aggregate and scaled offsets d_n = (x_n - c_a)/H;
-//   2. E = Z^T A Z: the CTAs of an aggregate walk its nodes' matrix rows and accumulate the 6x6
-//      blocks E[a][b] for its neighbour aggregates (b <= a with rigid-body modes: the
-//      factorisation reads the lower triangle); the last of them, found by a per-aggregate
-//      ticket, stores the blocks -- every block of E is written once, never added to in global
-//      memory;
+//   2. E = Z^T A Z, lower triangle (the factorisation reads no other): one thread per matrix row
+//      sums the row's blocks per neighbour aggregate into per-node entries, then one CTA per
+//      (aggregate, neighbour) adds the entries in a fixed order -- no atomics, so E is bitwise
+//      the same on every run;
 //   3. E = L L^T by a right-looking blocked Cholesky (64x64 tiles, FP64), W = L^{-1} by blocked
 //      forward substitution, E^{-1} = W^T W, kept in FP64 for the per-iteration GEMV (FP32
 //      rounding of the inverse of an ill-conditioned E can make it indefinite).
@@ -79,288 +78,237 @@ __global__ void permute_mask_kernel(int32_t n_node, const int32_t* __restrict__ 
 }
 
 // ---------------------------------------------------------------- E = Z^T A Z
-constexpr int kMatThreads = 128;
-constexpr int kMatParts = 8;         // most CTAs that share one aggregate
-constexpr int kMatItem = 21 + 13 * 36;  // one item's result: own block (lower), 13 lower neighbours
+// E = Z^T A Z, lower triangle only (the blocked Cholesky reads tiles (i, j) with i >= j and the
+// lower half of the diagonal tiles): for aggregate a the blocks E[a][b] with b < a (neighbour
+// slots 0..12 of the 3x3x3 box stencil, z slowest) and the lower half of E[a][a] (slot 13).
+// Two kernels, no atomics, every sum in a fixed order, so E is bitwise the same on every run:
+//   1. one thread per matrix row n, in SELL order (coalesced like the SpMV): the row's blocks
+//      are summed per neighbour box, T_{n,b} = sum_{m in b} A_nm Z_m (3 x NM), and stored as the
+//      node's entries: T_{n,a} for its own box, then one per lower neighbour box its row reaches
+//      (slot order);
+//   2. one CTA per (aggregate, slot): E[a][b] = sum_n Z_n^T T_{n,b} over a fixed list of the
+//      aggregate's nodes (node-list order), each thread one output value over a contiguous part
+//      of the list, the parts added in order.
+// Rigid-body modes: Z_n = [I | R(d_n)] with R(d) = [[-dy, 0, dz], [dx, -dz, 0], [0, dy, -dx]]
+// (translations, then rotations about z, x, y). Linear modes: u = a + B d, columns a_0..a_2
+// then B_ck at 3 + 3c + k. Rows of prescribed DOFs are zero in Z.
+constexpr int kRowThreads = 128;
+constexpr int kSumThreads = 256;
+constexpr int kSlots = 14;  // 13 lower neighbour slots and the own box
 
-// E = Z^T A Z for the rigid-body modes, lower triangle only: the blocked Cholesky reads tiles
-// (i, j) with i >= j and the lower half of the diagonal tiles, so for aggregate a only the
-// blocks E[a][b] with b < a (neighbour slots 0..12 of the 3x3x3 box stencil, z slowest) and the
-// lower half of E[a][a] are formed.
-//   Work item (a, part): a contiguous part of a's node list, one thread per node. For node n,
-// T = sum_m A_nm Z_m runs over the node's blocks in column order (neighbour aggregates change
-// rarely along a row) and Z_n^T T is added when the neighbour aggregate changes: to registers
-// for a's own block (fixed order, summed over the CTA by butterflies in warp order) and to the
-// item's shared slot buffer with shared atomics for the others. Column indices are read one
-// block ahead, so a block's loads do not wait for its own column index.
-//   Z_n = [I | R(d_n)] with R(d) = [[-dy, 0, dz], [dx, -dz, 0], [0, dy, -dx]] (translations,
-// then rotations about z, x, y) and zero rows on prescribed DOFs. The last CTA to finish an
-// aggregate's parts adds them in part order and stores the aggregate's blocks.
-template <typename VT>
-__global__ void __launch_bounds__(kMatThreads, 3) coarse_matrix_kernel(SellView A, const VT* __restrict__ aval,
-                                                                    CoarseView cv, const int32_t* __restrict__ aggbox,
-                                                                    int ngx, int ngy, int ngz, int parts,
-                                                                    double* __restrict__ epart,
-                                                                    double* __restrict__ E, int32_t* err) {
-    __shared__ double Eloc[13][36];
-    __shared__ double red[kMatThreads / 32][21];
-    __shared__ bool last;
-    const int lane32 = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int items = cv.n_agg * parts;
-    for (int item = blockIdx.x; item < items; item += gridDim.x) {
-        const int a = item / parts, part = item - a * parts;
-        __syncthreads();  // the previous item's shared results are no longer read
-        for (int i = threadIdx.x; i < 13 * 36; i += blockDim.x) (&Eloc[0][0])[i] = 0.0;
-        __syncthreads();
-        const int ax = a % ngx, ay = (a / ngx) % ngy, az = a / (ngx * ngy);
-        const int64_t b0 = cv.agg_ptr[a], len = cv.agg_ptr[a + 1] - b0;
-        const int64_t lo = b0 + len * part / parts, hi = b0 + len * (part + 1) / parts;
-        double own[21];
-#pragma unroll
-        for (int v = 0; v < 21; ++v) own[v] = 0.0;
-        for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-            const int64_t n = cv.agg_nodes[i];
-            const double dnx = cv.d[3 * n], dny = cv.d[3 * n + 1], dnz = cv.d[3 * n + 2];
-            const double kn0 = cv.fixed[3 * n] ? 0.0 : 1.0, kn1 = cv.fixed[3 * n + 1] ? 0.0 : 1.0,
-                         kn2 = cv.fixed[3 * n + 2] ? 0.0 : 1.0;
-            const int64_t sl = n >> 5;
-            const int lane = (int)(n & 31);
-            const int64_t base = A.slice_base[sl];
-            const int w = A.slice_width[sl];
-            const int32_t* cp = A.col + base + lane;
-            const VT* vp = aval + 9 * base + lane;
-            double T[3][6];
-#pragma unroll
-            for (int r = 0; r < 3; ++r)
-#pragma unroll
-                for (int j = 0; j < 6; ++j) T[r][j] = 0.0;
-            int cur = -1;
-            // Z_n^T T of the current run into its destination, T cleared
-            auto flush = [&](int slot) {
-#pragma unroll
-                for (int j = 0; j < 6; ++j) {
-                    const double t0 = kn0 * T[0][j], t1 = kn1 * T[1][j], t2 = kn2 * T[2][j];
-                    const double c[6] = {t0, t1, t2, -dny * t0 + dnx * t1, -dnz * t1 + dny * t2, dnz * t0 - dnx * t2};
-                    if (slot == 13) {
-#pragma unroll
-                        for (int r = j; r < 6; ++r) own[r * (r + 1) / 2 + j] += c[r];
-                    } else {
-#pragma unroll
-                        for (int r = 0; r < 6; ++r)
-                            if (c[r] != 0.0) atomicAdd(&Eloc[slot][6 * r + j], c[r]);
-                    }
-                }
-#pragma unroll
-                for (int r = 0; r < 3; ++r)
-#pragma unroll
-                    for (int j = 0; j < 6; ++j) T[r][j] = 0.0;
-            };
-            int64_t m_next = w > 0 ? (int64_t)cp[0] : n;
-            double S[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // FP32 storage: the row's sum, in storage order
-            for (int k = 0; k <= w; ++k) {
-                const int64_t m = m_next;
-                m_next = k + 1 < w ? (int64_t)cp[32 * (k + 1)] : n;  // the diagonal block comes last
-                double blk[9];
-                if (k < w) {
-                    const VT* v = vp + 288 * (int64_t)k;
-                    bool any = false;
-#pragma unroll
-                    for (int q = 0; q < 9; ++q) {
-                        blk[q] = (double)v[32 * q];
-                        S[q] += blk[q];
-                        any |= blk[q] != 0.0;
-                    }
-                    if (!any) continue;  // SELL padding
-                } else {
-                    // the FP64 storage keeps the diagonal blocks in the rows; the FP32 storage's
-                    // diagonal block is minus the sum of the row's stored blocks
-                    if (!A.diag64) break;
-#pragma unroll
-                    for (int q = 0; q < 9; ++q) blk[q] = -S[q];
-                }
-                const int pb = aggbox[m];  // the neighbour's box, packed: no integer division
-                const int dx = (pb & 1023) - ax, dy = ((pb >> 10) & 1023) - ay, dz = (pb >> 20) - az;
-                if (dx < -1 || dx > 1 || dy < -1 || dy > 1 || dz < -1 || dz > 1) {
-                    atomicExch(err, 1);
-                    continue;
-                }
-                const int slot = (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1);
-                if (slot > 13) continue;  // upper triangle of E
-                if (slot != cur) {
-                    if (cur >= 0) flush(cur);
-                    cur = slot;
-                }
-                const double dmx = cv.d[3 * m], dmy = cv.d[3 * m + 1], dmz = cv.d[3 * m + 2];
-                const double km0 = cv.fixed[3 * m] ? 0.0 : 1.0, km1 = cv.fixed[3 * m + 1] ? 0.0 : 1.0,
-                             km2 = cv.fixed[3 * m + 2] ? 0.0 : 1.0;
-#pragma unroll
-                for (int r = 0; r < 3; ++r) {
-                    const double c0 = km0 * blk[3 * r], c1 = km1 * blk[3 * r + 1], c2 = km2 * blk[3 * r + 2];
-                    T[r][0] += c0;
-                    T[r][1] += c1;
-                    T[r][2] += c2;
-                    T[r][3] += -dmy * c0 + dmx * c1;
-                    T[r][4] += -dmz * c1 + dmy * c2;
-                    T[r][5] += dmz * c0 - dmx * c2;
-                }
-            }
-            if (cur >= 0) flush(cur);
+__device__ __forceinline__ int box_slot(int pb, int ax, int ay, int az) {
+    const int dx = (pb & 1023) - ax, dy = ((pb >> 10) & 1023) - ay, dz = (pb >> 20) - az;
+    if (dx < -1 || dx > 1 || dy < -1 || dy > 1 || dz < -1 || dz > 1) return -1;
+    return (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1);
+}
+
+// The lower neighbour slots every row reaches (the pattern and the boxes only: computed once per
+// layout). err = 1: a row reaches a box that is not a neighbour of its own.
+__global__ void row_slots_kernel(SellView A, const int32_t* __restrict__ aggbox, uint16_t* __restrict__ lmask,
+                                 int32_t* __restrict__ err) {
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < A.n_node;
+         n += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t sl = n >> 5;
+        const int lane = (int)(n & 31);
+        const int64_t base = A.slice_base[sl];
+        const int w = A.slice_width[sl];
+        const int pn = aggbox[n];
+        const int ax = pn & 1023, ay = (pn >> 10) & 1023, az = pn >> 20;
+        uint32_t mask = 0;
+        for (int k = 0; k < w; ++k) {
+            const int slot = box_slot(aggbox[A.col[base + 32 * (int64_t)k + lane]], ax, ay, az);
+            if (slot < 0)
+                atomicExch(err, 1);
+            else if (slot < 13)
+                mask |= 1u << slot;
         }
-#pragma unroll
-        for (int v = 0; v < 21; ++v) {
-            double x = own[v];
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-            if (lane32 == 0) red[warp][v] = x;
-        }
-        __syncthreads();
-        // the item's value t of kMatItem: own block (lower, row-major) or a neighbour slot entry
-        auto item_value = [&](int t) {
-            if (t < 21) {
-                double x = 0.0;
-                for (int q = 0; q < kMatThreads / 32; ++q) x += red[q][t];
-                return x;
-            }
-            return (&Eloc[0][0])[t - 21];
-        };
-        // where value t goes in E (-1: the neighbour box is outside the grid)
-        auto e_index = [&](int t) -> int64_t {
-            if (t < 21) {
-                int r = 0;
-                while ((r + 1) * (r + 2) / 2 <= t) ++r;
-                const int j = t - r * (r + 1) / 2;
-                return (int64_t)(6 * a + r) * cv.kp + 6 * a + j;
-            }
-            const int slot = (t - 21) / 36, q = (t - 21) % 36;
-            const int bx = ax + slot % 3 - 1, by = ay + (slot / 3) % 3 - 1, bz = az + slot / 9 - 1;
-            if (bx < 0 || bx >= ngx || by < 0 || by >= ngy || bz < 0 || bz >= ngz) return -1;
-            const int b = bx + ngx * (by + ngy * bz);
-            return (int64_t)(6 * a + q / 6) * cv.kp + 6 * b + q % 6;
-        };
-        if (parts == 1) {
-            for (int t = threadIdx.x; t < kMatItem; t += blockDim.x) {
-                const int64_t e = e_index(t);
-                if (e >= 0) E[e] = item_value(t);
-            }
-            continue;
-        }
-        for (int t = threadIdx.x; t < kMatItem; t += blockDim.x)
-            epart[((int64_t)a * parts + part) * kMatItem + t] = item_value(t);
-        __threadfence();
-        __syncthreads();
-        if (threadIdx.x == 0) last = atomicAdd(cv.wcount + a, 1u) == (uint32_t)parts - 1;
-        __syncthreads();
-        if (!last) continue;
-        for (int t = threadIdx.x; t < kMatItem; t += blockDim.x) {
-            const int64_t e = e_index(t);
-            if (e < 0) continue;
-            double x = 0.0;
-            for (int q = 0; q < parts; ++q) x += __ldcg(epart + ((int64_t)a * parts + q) * kMatItem + t);
-            E[e] = x;
-        }
-        if (threadIdx.x == 0) cv.wcount[a] = 0;
+        lmask[n] = (uint16_t)mask;
     }
 }
 
-// E = Z^T A Z for the twelve linear-displacement modes u = a + B d of every aggregate (columns
-// a_0..a_2, then B_ck at 3 + 3c + k). With Z_n's rows e_r (x) (1, d_n), the product needs no Z
-// matrix: T[r][j] = sum_m (A_nm Z_m)[r][j] is accumulated per neighbour-aggregate run, and
-// E[i][j] += (Z_n^T T)[i][j] = T[i][j] (i < 3) or d_n,k T[c][j] (i = 3 + 3c + k). Rows and
-// columns of prescribed DOFs drop out (their Z rows are zero).
-template <typename VT>
-__global__ void __launch_bounds__(256) coarse_matrix_linear_kernel(SellView A, const VT* __restrict__ aval,
-                                                                   CoarseView cv, const int32_t* __restrict__ aggbox,
-                                                                   int ngx, int ngy, int ngz,
-                                                                   double* __restrict__ E, int32_t* err) {
-    __shared__ double Eloc[27][144];
-    for (int a = blockIdx.x; a < cv.n_agg; a += gridDim.x) {
-        for (int i = threadIdx.x; i < 27 * 144; i += blockDim.x) (&Eloc[0][0])[i] = 0.0;
-        __syncthreads();
-        const int ax = a % ngx, ay = (a / ngx) % ngy, az = a / (ngx * ngy);
-        for (int64_t i = cv.agg_ptr[a] + threadIdx.x; i < cv.agg_ptr[a + 1]; i += blockDim.x) {
-            const int64_t n = cv.agg_nodes[i];
-            const double dn[3] = {cv.d[3 * n], cv.d[3 * n + 1], cv.d[3 * n + 2]};
-            const bool fn[3] = {cv.fixed[3 * n] != 0, cv.fixed[3 * n + 1] != 0, cv.fixed[3 * n + 2] != 0};
-            const int64_t s = n >> 5;
-            const int lane = (int)(n & 31);
-            const int64_t base = A.slice_base[s];
-            const int w = A.slice_width[s];
-            double T[3][12];
-            for (int r = 0; r < 3; ++r)
-                for (int j = 0; j < 12; ++j) T[r][j] = 0.0;
-            int cur = -1;
-            auto flush = [&](int slot) {
-                for (int r = 0; r < 3; ++r) {
-                    if (fn[r]) continue;
-                    for (int j = 0; j < 12; ++j) {
-                        const double t = T[r][j];
-                        if (t == 0.0) continue;
-                        atomicAdd(&Eloc[slot][12 * r + j], t);
-                        for (int k = 0; k < 3; ++k)
-                            if (dn[k] != 0.0) atomicAdd(&Eloc[slot][12 * (3 + 3 * r + k) + j], dn[k] * t);
-                    }
-                }
-                for (int r = 0; r < 3; ++r)
-                    for (int j = 0; j < 12; ++j) T[r][j] = 0.0;
-            };
-            double S[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // FP32 storage: the row's sum, in storage order
-            for (int k = 0; k <= w; ++k) {
-                double blk[9];
-                int64_t m;
-                if (k < w) {
-                    m = A.col[base + 32 * (int64_t)k + lane];
-                    const VT* v = aval + 9 * (base + 32 * (int64_t)k) + lane;
-                    bool any = false;
-                    for (int q = 0; q < 9; ++q) {
-                        blk[q] = (double)v[32 * q];
-                        S[q] += blk[q];
-                        any |= blk[q] != 0.0;
-                    }
-                    if (!any) continue;
-                } else {
-                    if (!A.diag64) break;  // the FP32 storage's diagonal block: minus the row's sum
-                    m = n;
-                    for (int q = 0; q < 9; ++q) blk[q] = -S[q];
-                }
-                for (int q = 0; q < 9; ++q)
-                    if (cv.fixed[3 * m + q % 3]) blk[q] = 0.0;  // prescribed columns: zero Z rows of m
-                const int pb = aggbox[m];  // the neighbour's box, packed: no integer division
-                const int dx = (pb & 1023) - ax, dy = ((pb >> 10) & 1023) - ay, dz = (pb >> 20) - az;
-                if (dx < -1 || dx > 1 || dy < -1 || dy > 1 || dz < -1 || dz > 1) {
-                    atomicExch(err, 1);
-                    continue;
-                }
-                const int slot = (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1);
-                if (slot != cur) {
-                    if (cur >= 0) flush(cur);
-                    cur = slot;
-                }
-                const double dm[3] = {cv.d[3 * m], cv.d[3 * m + 1], cv.d[3 * m + 2]};
-                for (int r = 0; r < 3; ++r)
-                    for (int c = 0; c < 3; ++c) {
-                        const double av = blk[3 * r + c];
-                        T[r][c] += av;
-                        T[r][3 + 3 * c] += av * dm[0];
-                        T[r][4 + 3 * c] += av * dm[1];
-                        T[r][5 + 3 * c] += av * dm[2];
-                    }
+// T += A_nm Z_m for one 3x3 block (column masks of m's prescribed DOFs applied)
+template <int NM>
+__device__ __forceinline__ void add_block_z(double (&T)[3][NM], const double blk[9], const float* __restrict__ d,
+                                            const uint8_t* __restrict__ fixed, int64_t m) {
+    const double dmx = d[3 * m], dmy = d[3 * m + 1], dmz = d[3 * m + 2];
+    const double km0 = fixed[3 * m] ? 0.0 : 1.0, km1 = fixed[3 * m + 1] ? 0.0 : 1.0, km2 = fixed[3 * m + 2] ? 0.0 : 1.0;
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        const double c0 = km0 * blk[3 * r], c1 = km1 * blk[3 * r + 1], c2 = km2 * blk[3 * r + 2];
+        T[r][0] += c0;
+        T[r][1] += c1;
+        T[r][2] += c2;
+        if constexpr (NM == 6) {
+            T[r][3] += -dmy * c0 + dmx * c1;
+            T[r][4] += -dmz * c1 + dmy * c2;
+            T[r][5] += dmz * c0 - dmx * c2;
+        } else {
+            const double dm[3] = {dmx, dmy, dmz};
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                T[r][3 + k] += c0 * dm[k];
+                T[r][6 + k] += c1 * dm[k];
+                T[r][9 + k] += c2 * dm[k];
             }
-            if (cur >= 0) flush(cur);
         }
-        __syncthreads();
-        for (int t = threadIdx.x; t < 27 * 144; t += blockDim.x) {
-            const int slot = t / 144, q = t % 144;
-            const int bx = ax + slot % 3 - 1, by = ay + (slot / 3) % 3 - 1, bz = az + slot / 9 - 1;
-            if (bx < 0 || bx >= ngx || by < 0 || by >= ngy || bz < 0 || bz >= ngz) continue;
-            const int b = bx + ngx * (by + ngy * bz);
-            E[(int64_t)(12 * a + q / 12) * cv.kp + 12 * b + q % 12] = Eloc[slot][q];
-        }
-        __syncthreads();
     }
 }
 
-// modes that vanish on the free DOFs (an aggregate of prescribed nodes) and the padding become
-// identity rows: their correction is zero
+// Kernel 1: row n's entries (3 x NM each, row-major) at tbuf[toff[n] ..]: own box first, then
+// the lower slots of lmask[n] in slot order. Rigid-body modes sum the own box and the first
+// lower slot in one walk of the row; every further slot (rows at box edges and corners) walks
+// the row again. The FP32 storage's diagonal block is minus the row's stored blocks, summed in
+// storage order as the SpMV forms it.
+template <typename VT, int NM>
+__global__ void __launch_bounds__(kRowThreads, 4) coarse_rows_kernel(SellView A, const VT* __restrict__ aval, CoarseView cv,
+                                                                  const int32_t* __restrict__ aggbox,
+                                                                  const uint16_t* __restrict__ lmask,
+                                                                  const int32_t* __restrict__ toff,
+                                                                  double* __restrict__ tbuf) {
+    constexpr bool kDual = NM == 6;
+    const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (n >= A.n_node) return;
+    const int64_t sl = n >> 5;
+    const int lane = (int)(n & 31);
+    const int64_t base = A.slice_base[sl];
+    const int w = A.slice_width[sl];
+    const int32_t* cp = A.col + base + lane;
+    const VT* vp = aval + 9 * base + lane;
+    const int pn = aggbox[n];
+    const int ax = pn & 1023, ay = (pn >> 10) & 1023, az = pn >> 20;
+    uint32_t todo = lmask[n];
+    double* out = tbuf + (int64_t)toff[n] * (3 * NM);
+    int want = 13, want2 = -1;
+    if (kDual && todo) {
+        want2 = __ffs(todo) - 1;
+        todo &= todo - 1;
+    }
+    for (bool first = true;; first = false) {
+        double T[3][NM], U[3][NM];  // U: the second slot of a rigid-body walk
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int j = 0; j < NM; ++j) {
+                T[r][j] = 0.0;
+                U[r][j] = 0.0;
+            }
+        double S[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int k = 0; k <= w; ++k) {
+            double blk[9];
+            int64_t m;
+            if (k < w) {
+                m = cp[32 * (int64_t)k];
+                const VT* v = vp + 288 * (int64_t)k;
+                bool any = false;
+#pragma unroll
+                for (int q = 0; q < 9; ++q) {
+                    blk[q] = (double)v[32 * q];
+                    S[q] += blk[q];
+                    any |= blk[q] != 0.0;
+                }
+                if (!any) continue;  // SELL padding, zero blocks
+            } else {
+                if (!first || !A.diag64) break;  // the diagonal block belongs to the own box
+                m = n;
+#pragma unroll
+                for (int q = 0; q < 9; ++q) blk[q] = -S[q];
+            }
+            const int slot = box_slot(aggbox[m], ax, ay, az);
+            if (slot == want) {
+                add_block_z<NM>(T, blk, cv.d, cv.fixed, m);
+            } else if constexpr (kDual) {
+                if (slot == want2) add_block_z<NM>(U, blk, cv.d, cv.fixed, m);
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int j = 0; j < NM; ++j) out[NM * r + j] = T[r][j];
+        out += 3 * NM;
+        if (want2 >= 0) {
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int j = 0; j < NM; ++j) out[NM * r + j] = U[r][j];
+            out += 3 * NM;
+        }
+        if (!todo) break;
+        want = __ffs(todo) - 1;
+        todo &= todo - 1;
+        want2 = -1;
+    }
+}
+
+// Kernel 2: one CTA per (aggregate a, slot s); list[lptr[a 14 + s] ..) holds the entries of the
+// nodes of a that reach slot s (node-list order) and their nodes. Thread (g, v) sums output value
+// v over part g of the list; the parts are added in order.
+template <int NM>
+__global__ void __launch_bounds__(kSumThreads) coarse_sum_kernel(CoarseView cv, int ngx, int ngy,
+                                                                 const int64_t* __restrict__ lptr,
+                                                                 const int32_t* __restrict__ lent,
+                                                                 const int32_t* __restrict__ lnode,
+                                                                 const double* __restrict__ tbuf,
+                                                                 double* __restrict__ E) {
+    __shared__ double part[kSumThreads];
+    const int a = blockIdx.x / kSlots, s = blockIdx.x % kSlots;
+    const int64_t b0 = lptr[blockIdx.x], len = lptr[blockIdx.x + 1] - b0;
+    if (len == 0) return;
+    const bool own = s == 13;
+    const int nval = own ? NM * (NM + 1) / 2 : NM * NM;
+    const int groups = kSumThreads / nval;
+    const int v = threadIdx.x % nval, g = threadIdx.x / nval;
+    int i, j;
+    if (own) {
+        i = 0;
+        while ((i + 1) * (i + 2) / 2 <= v) ++i;
+        j = v - i * (i + 1) / 2;
+    } else {
+        i = v / NM;
+        j = v % NM;
+    }
+    double acc = 0.0;
+    if (g < groups) {
+        // (Z_n^T T)[i][j] = c1 T[r1][j] + c2 T[r2][j]
+        int r1 = i, r2 = 0, dk1 = -1, dk2 = -1;
+        double s1 = 1.0, s2 = 0.0;
+        if (NM == 6) {
+            // i = 3: -dy T0 + dx T1; i = 4: -dz T1 + dy T2; i = 5: dz T0 - dx T2
+            if (i >= 3) {
+                r1 = i == 4 ? 1 : 0;
+                r2 = i == 3 ? 1 : 2;
+                dk1 = i == 3 ? 1 : 2;
+                dk2 = i == 4 ? 1 : 0;
+                s1 = i == 5 ? 1.0 : -1.0;
+                s2 = -s1;
+            }
+        } else if (i >= 3) {
+            r1 = (i - 3) / 3;
+            dk1 = (i - 3) % 3;
+        }
+        const int64_t lo = b0 + len * g / groups, hi = b0 + len * (g + 1) / groups;
+        for (int64_t q = lo; q < hi; ++q) {
+            const int64_t n = lnode[q];
+            const double* t = tbuf + (int64_t)lent[q] * (3 * NM);
+            double c1 = cv.fixed[3 * n + r1] ? 0.0 : s1;
+            if (dk1 >= 0) c1 *= (double)cv.d[3 * n + dk1];
+            double x = c1 * t[NM * r1 + j];
+            if (dk2 >= 0) {
+                const double c2 = cv.fixed[3 * n + r2] ? 0.0 : s2 * (double)cv.d[3 * n + dk2];
+                x += c2 * t[NM * r2 + j];
+            }
+            acc += x;
+        }
+    }
+    part[threadIdx.x] = acc;
+    __syncthreads();
+    if (threadIdx.x >= nval) return;
+    double x = 0.0;
+    for (int q = 0; q < groups; ++q) x += part[q * nval + v];
+    const int ax = a % ngx, ay = (a / ngx) % ngy, az = a / (ngx * ngy);
+    const int b = own ? a : (ax + s % 3 - 1) + ngx * ((ay + (s / 3) % 3 - 1) + ngy * (az + s / 9 - 1));
+    E[(int64_t)(NM * a + i) * cv.kp + NM * b + j] = x;
+}
+
 __global__ void drop_null_modes(double* __restrict__ E, int kp, int k) {
     __shared__ double red[32];
     // largest diagonal entry: per-thread maxima, then per warp and across warps
@@ -715,6 +663,7 @@ void CoarseSpace::init(mphy_ctx* ctx, const mphy_mesh* mesh, const mphy_pattern*
     std::vector<int32_t> nodes(nn);
     std::vector<int64_t> cur(ptr.begin(), ptr.end() - 1);
     for (int32_t n = 0; n < nn; ++n) nodes[cur[agg[n]]++] = n;
+    lists_ready_ = false;
     cudaStream_t s = ctx->stream;
     agg_.alloc(nn);
     agg_.upload(agg.data(), nn, s);
@@ -735,6 +684,8 @@ void CoarseSpace::init(mphy_ctx* ctx, const mphy_mesh* mesh, const mphy_pattern*
     agg_ptr_.upload(ptr.data(), n_agg_ + 1, s);
     agg_nodes_.alloc(nn);
     agg_nodes_.upload(nodes.data(), nn, s);
+    nodes_host_ = std::move(nodes);
+    ptr_host_ = ptr;
     d_.alloc(3 * (size_t)nn);
     dperm_.alloc(3 * (size_t)nn);
     fperm_.alloc(3 * (size_t)nn);
@@ -753,7 +704,6 @@ void CoarseSpace::init(mphy_ctx* ctx, const mphy_mesh* mesh, const mphy_pattern*
     c_.alloc(kp_);
     wpart_.alloc((size_t)n_agg_ * kMaxRestrictParts * nm_);
     wcount_.alloc(n_agg_);
-    if (nm_ == 6) epart_.alloc((size_t)n_agg_ * kMatParts * kMatItem);
     err_.alloc(1);
     MPHY_CUDA(cudaMemsetAsync(w_.p, 0, w_.bytes(), s));
     MPHY_CUDA(cudaMemsetAsync(c_.p, 0, c_.bytes(), s));
@@ -790,21 +740,20 @@ void CoarseSpace::setup(const SellView& A, const VT* aval, const double* disp, c
     MPHY_CUDA(cudaMemsetAsync(E_.p, 0, E_.bytes(), s));
     MPHY_CUDA(cudaMemsetAsync(W_.p, 0, W_.bytes(), s));
     MPHY_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(int32_t), s));
+    if (!lists_ready_) build_entry_lists(A, s);
     CoarseView cv = view();
-    if (nm_ == 12)
-        coarse_matrix_linear_kernel<VT><<<std::min(n_agg_, sm * 8), 256, 0, s>>>(A, aval, cv, aggbox_.p, ng_[0],
-                                                                                  ng_[1], ng_[2], E_.p, err_.p);
-    else {
-        // persistent grid, about two work items per resident CTA
-        const unsigned grid = resident_grid((const void*)coarse_matrix_kernel<VT>, (int64_t)1 << 40, kMatThreads, sm);
-        const int parts = std::max(1, std::min(kMatParts, (int)((2 * (int64_t)grid + n_agg_ - 1) / n_agg_)));
-        const unsigned g = (unsigned)std::min<int64_t>(grid, (int64_t)n_agg_ * parts);
-        coarse_matrix_kernel<VT><<<g, kMatThreads, 0, s>>>(A, aval, cv, aggbox_.p, ng_[0], ng_[1], ng_[2], parts,
-                                                           epart_.p, E_.p,
-                                                           err_.p);
+    const unsigned rows = (unsigned)((mesh_->n_node + kRowThreads - 1) / kRowThreads);
+    if (nm_ == 12) {
+        coarse_rows_kernel<VT, 12><<<rows, kRowThreads, 0, s>>>(A, aval, cv, aggbox_.p, lmask_.p, toff_.p, tbuf_.p);
+        coarse_sum_kernel<12><<<n_agg_ * kSlots, kSumThreads, 0, s>>>(cv, ng_[0], ng_[1], lptr_.p, lent_.p, lnode_.p,
+                                                                      tbuf_.p, E_.p);
+    } else {
+        coarse_rows_kernel<VT, 6><<<rows, kRowThreads, 0, s>>>(A, aval, cv, aggbox_.p, lmask_.p, toff_.p, tbuf_.p);
+        coarse_sum_kernel<6><<<n_agg_ * kSlots, kSumThreads, 0, s>>>(cv, ng_[0], ng_[1], lptr_.p, lent_.p, lnode_.p,
+                                                                     tbuf_.p, E_.p);
     }
     MPHY_CUDA(cudaGetLastError());
-    launches += 3;
+    launches += 4;
     const int nb = kp_ / T;
     const size_t sm2 = 2 * (size_t)T * TP * sizeof(double);
     static std::atomic<uint64_t> attr{0};
@@ -845,8 +794,62 @@ void CoarseSpace::setup(const SellView& A, const VT* aval, const double* disp, c
     MPHY_CUDA(cudaMemcpyAsync(&h, err_.p, sizeof(h), cudaMemcpyDeviceToHost, s));
     MPHY_CUDA(cudaStreamSynchronize(s));
     cudaEventElapsedTime(&last_setup_ms, ctx_->ev0, ctx_->ev1);
-    MPHY_REQUIRE(h != 1, MPHY_ERR_UNSUPPORTED, "coarse space: an element spans more than two aggregates");
     MPHY_REQUIRE(h != 2, MPHY_ERR_INDEFINITE, "coarse space: Z^T A Z is not positive definite");
+}
+
+// The lower slots of every row (device), then on the host the entry offsets and the
+// per-(aggregate, slot) lists in node-list order. Once per layout: the pattern and the boxes
+// decide them, not the values.
+void CoarseSpace::build_entry_lists(const SellView& A, cudaStream_t s) {
+    const int32_t nn = mesh_->n_node;
+    lmask_.alloc(nn);
+    MPHY_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(int32_t), s));
+    row_slots_kernel<<<stride_grid(nn, 256, ctx_->sm_count), 256, 0, s>>>(A, aggbox_.p, lmask_.p, err_.p);
+    MPHY_CUDA(cudaGetLastError());
+    std::vector<uint16_t> mask(nn);
+    int32_t h = 0;
+    MPHY_CUDA(cudaMemcpyAsync(mask.data(), lmask_.p, nn * sizeof(uint16_t), cudaMemcpyDeviceToHost, s));
+    MPHY_CUDA(cudaMemcpyAsync(&h, err_.p, sizeof(h), cudaMemcpyDeviceToHost, s));
+    MPHY_CUDA(cudaStreamSynchronize(s));
+    MPHY_REQUIRE(h == 0, MPHY_ERR_UNSUPPORTED, "coarse space: an element spans more than two aggregates");
+    std::vector<int32_t> toff(nn);
+    int64_t entries = 0;
+    for (int32_t n = 0; n < nn; ++n) {
+        toff[n] = (int32_t)entries;
+        entries += 1 + __builtin_popcount(mask[n]);
+        MPHY_REQUIRE(entries < INT32_MAX, MPHY_ERR_UNSUPPORTED, "coarse space: too many row entries");
+    }
+    std::vector<int64_t> lptr((size_t)n_agg_ * kSlots + 1, 0);
+    std::vector<int32_t> lent, lnode;
+    lent.reserve(entries);
+    lnode.reserve(entries);
+    for (int a = 0; a < n_agg_; ++a)
+        for (int sl = 0; sl < kSlots; ++sl) {
+            for (int64_t i = ptr_host_[a]; i < ptr_host_[a + 1]; ++i) {
+                const int32_t n = nodes_host_[i];
+                const uint32_t m = mask[n];
+                if (sl == 13) {
+                    lent.push_back(toff[n]);
+                } else if (m >> sl & 1u) {
+                    lent.push_back(toff[n] + 1 + __builtin_popcount(m & ((1u << sl) - 1u)));
+                } else {
+                    continue;
+                }
+                lnode.push_back(n);
+            }
+            lptr[(size_t)a * kSlots + sl + 1] = (int64_t)lent.size();
+        }
+    toff_.alloc(nn);
+    toff_.upload(toff.data(), nn, s);
+    lptr_.alloc(lptr.size());
+    lptr_.upload(lptr.data(), lptr.size(), s);
+    lent_.alloc(lent.size());
+    lent_.upload(lent.data(), lent.size(), s);
+    lnode_.alloc(lnode.size());
+    lnode_.upload(lnode.data(), lnode.size(), s);
+    tbuf_.alloc((size_t)entries * 3 * nm_);
+    MPHY_CUDA(cudaStreamSynchronize(s));  // the host vectors end here
+    lists_ready_ = true;
 }
 
 // Three streams inside the capture. Main: the diagonal factorisation and the panel of step j,

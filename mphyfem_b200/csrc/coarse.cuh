@@ -6,6 +6,8 @@
 // DOFs. M^{-1} is symmetric positive definite, so CG keeps its guarantees; the coarse term takes
 // care of the global, smooth modes (beam bending) that no local preconditioner reaches.
 #pragma once
+#include <vector>
+
 #include "common.cuh"
 #include "coarse_view.cuh"
 #include "krylov.cuh"
@@ -35,6 +37,7 @@ class CoarseSpace {
 
   private:
     void record_factorisation(cudaStream_t s, int nb, size_t sm2);
+    void build_entry_lists(const SellView& A, cudaStream_t s);
     cudaGraphExec_t fact_graph_ = nullptr;
     cudaStream_t side_[2] = {nullptr, nullptr};  // captured side streams of the factorisation
     cudaEvent_t ev_[3] = {nullptr, nullptr, nullptr};
@@ -57,7 +60,16 @@ class CoarseSpace {
     DevBuf<uint8_t> drop_;
     DevBuf<double> wpart_;
     DevBuf<uint32_t> wcount_;
-    DevBuf<double> epart_;  // per-part results of the E = Z^T A Z kernel
+    // E = Z^T A Z in two passes (built at the first setup of a layout): per node, the lower
+    // neighbour slots its row reaches and the offset of its entries (T_{n,b} = sum_{m in b} A_nm
+    // Z_m, own box first); per (aggregate, slot), the list of entries and nodes to add, in order
+    bool lists_ready_ = false;
+    std::vector<int32_t> nodes_host_;  // agg_nodes
+    std::vector<int64_t> ptr_host_;    // agg_ptr
+    DevBuf<uint16_t> lmask_;
+    DevBuf<int32_t> toff_, lent_, lnode_;
+    DevBuf<int64_t> lptr_;
+    DevBuf<double> tbuf_;
     DevBuf<float> dperm_;   // d in agg_nodes order
     DevBuf<uint8_t> fperm_; // fixed in agg_nodes order
 };

@@ -161,10 +161,10 @@ def test_linear_modes_need_fewer_iterations(env):
 
 
 def test_many_aggregates_one_item_each(env, oracle):
-    """About 1,400 aggregates, more than two per resident CTA of the E = Z^T A Z kernel and of the
-    restriction. Both then take one work item per aggregate, with no cross-CTA part sums. The
-    checks are the same as above: the FP64 oracle's solution, and the iteration count of the
-    numpy restatement on the same aggregate grid."""
+    """About 1,400 aggregates (19,600 (aggregate, slot) CTAs of the E = Z^T A Z sum kernel), more
+    than two per resident CTA of the restriction, which then takes one work item per aggregate,
+    with no cross-CTA part sums. The checks are the same as above: the FP64 oracle's solution,
+    and the iteration count of the numpy restatement on the same aggregate grid."""
     from oracle import fsai_ref, twolevel_ref
     torch, api, _lib, ctx = env
     p = meshgen.hex8_cantilever(40, 20, 20)
@@ -182,3 +182,27 @@ def test_many_aggregates_one_item_each(env, oracle):
     Minv = twolevel_ref.preconditioner(A, p.coords, p.fixed, info["grid"])
     _, its_ref = twolevel_ref.pcg(A, 0.2 * p.fnodal * (p.fixed == 0), Minv, rtol=1e-12)
     assert abs(its - its_ref) <= max(2, 0.03 * its_ref), (its, its_ref)
+
+
+@pytest.mark.parametrize("prec,modes", [("fp64", 6), ("mixed", 6), ("fp64", 12)])
+def test_coarse_operator_is_bitwise_reproducible(env, prec, modes):
+    """E = Z^T A Z is summed in a fixed order, with no atomics: per-row sums per neighbour box,
+    then a fixed list per (aggregate, neighbour). Two solves of one assembled system, each
+    forming E and its inverse afresh, give bitwise equal solutions and equal iteration counts."""
+    torch, api, _lib, ctx = env
+    p = meshgen.hex8_cantilever(48, 12, 12)
+    mesh = api.Mesh(ctx, p)
+    opts = dict(rtol=1e-10, coarse_aggregates=60, coarse_modes=modes, norm_type=1)
+    if prec == "mixed":
+        opts["precision"] = _lib.PREC_MIXED
+    sol = api.SolverGpu(mesh, api.Pattern(mesh), **opts)
+    sol.calcStiffnessAndResidual(torch.zeros(p.n_dof, dtype=torch.float64, device="cuda"))
+    sol.addExternalForces(torch.tensor(p.fnodal, device="cuda"), 0.2)
+    runs = []
+    for _ in range(2):
+        rc, its, _ = sol.factoriseAndSolve()
+        assert rc == 0
+        assert sol.coarse_info()["setup_ms"] > 0.0  # formed by this solve
+        runs.append((its, sol.solution().cpu().numpy().copy()))
+    assert runs[0][0] == runs[1][0], (runs[0][0], runs[1][0])
+    assert np.array_equal(runs[0][1], runs[1][1])
