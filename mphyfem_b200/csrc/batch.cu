@@ -97,6 +97,16 @@ struct BatchView {
     const double* slab_cent;  // [n_inst][kMaxSlabs][3] slab centroids (reference coordinates)
     const double* coords;     // [n_node][3] reference coordinates
     const uint8_t* fixed;     // [3 n_node] prescribed DOFs (zero rows of Z)
+    const uint8_t* slab;      // [n_node] slab of every node within its instance
+    // E = Z^T A Z without atomics: node n's row sums T_{n,s} (3 x 6 each, own slab first, then
+    // every other slab its row reaches, in slab order) at tbuf[18 toff[n] ..]; per (instance,
+    // slab pair sn * 8 + sm) the entries of its nodes in slab sn that reach slab sm, in node order
+    const uint8_t* omask;     // [n_node] other slabs the row reaches
+    const int32_t* toff;      // [n_node]
+    const int64_t* lptr;      // [n_inst * 64 + 1]
+    const int32_t* lent;      // entry of every list item
+    const int32_t* lnode;     // node of every list item
+    double* tbuf;             // [entries][18]
 };
 
 constexpr int kMaxSlabs = 8;
@@ -115,14 +125,6 @@ struct CoarseSmem {
     int drop[kMaxCoarse];
 };
 
-__device__ __forceinline__ int slab_of(const BatchView& v, int inst, int64_t n) {
-    const double* g = v.slab_geo + 4 * inst;
-    const int ax = (int)g[0];
-    const double t = (v.coords[3 * n + ax] - g[1]) / (g[2] - g[1]);
-    int s = (int)floor(t * v.ns);
-    return s < 0 ? 0 : (s >= v.ns ? v.ns - 1 : s);
-}
-
 // Z_n (3 x 6): translations and rotations about the slab centroid, zero rows on prescribed DOFs
 __device__ __forceinline__ void slab_modes(const BatchView& v, int inst, int64_t n, int s, double Z[3][6]) {
     const double* cen = v.slab_cent + 3 * ((int64_t)inst * kMaxSlabs + s);
@@ -133,6 +135,49 @@ __device__ __forceinline__ void slab_modes(const BatchView& v, int inst, int64_t
     for (int i = 0; i < 3; ++i) {
         const bool fx = v.fixed[3 * n + i] != 0;
         for (int j = 0; j < 6; ++j) Z[i][j] = fx ? 0.0 : m[i][j];
+    }
+}
+
+// Column i of Z_n: z[r] = Z_n[r][i]
+__device__ __forceinline__ void slab_mode_col(const BatchView& v, int inst, int64_t n, int s, int i, double z[3]) {
+    const double* cen = v.slab_cent + 3 * ((int64_t)inst * kMaxSlabs + s);
+    const double h = v.slab_geo[4 * inst + 3];
+    const double dx = (v.coords[3 * n] - cen[0]) / h, dy = (v.coords[3 * n + 1] - cen[1]) / h,
+                 dz = (v.coords[3 * n + 2] - cen[2]) / h;
+    // the columns of [[1, 0, 0, -dy, 0, dz], [0, 1, 0, dx, -dz, 0], [0, 0, 1, 0, dy, -dx]]
+    const double c0 = i == 0 ? 1.0 : i == 3 ? -dy : i == 5 ? dz : 0.0;
+    const double c1 = i == 1 ? 1.0 : i == 3 ? dx : i == 4 ? -dz : 0.0;
+    const double c2 = i == 2 ? 1.0 : i == 4 ? dy : i == 5 ? -dx : 0.0;
+    z[0] = v.fixed[3 * n] ? 0.0 : c0;
+    z[1] = v.fixed[3 * n + 1] ? 0.0 : c1;
+    z[2] = v.fixed[3 * n + 2] ? 0.0 : c2;
+}
+
+// first position in lnode[lo, hi) whose node is >= n (the lists are in node order)
+__device__ __forceinline__ int64_t list_lower_bound(const int32_t* __restrict__ lnode, int64_t lo, int64_t hi,
+                                                    int64_t n) {
+    while (lo < hi) {
+        const int64_t mid = lo + (hi - lo) / 2;
+        if (lnode[mid] < n) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// The slabs other than its own that every row reaches (the pattern decides them, not the values)
+__global__ void slab_mask_kernel(SellView A, const uint8_t* __restrict__ slab, uint8_t* __restrict__ omask) {
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < A.n_node;
+         n += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t sl = n >> 5;
+        const int lane = (int)(n & 31);
+        const int64_t base = A.slice_base[sl];
+        const int w = A.slice_width[sl], s = slab[n];
+        uint32_t mask = 0;
+        for (int k = 0; k < w; ++k) {
+            const int sm = slab[A.col[base + 32 * (int64_t)k + lane]];
+            if (sm != s) mask |= 1u << sm;
+        }
+        omask[n] = (uint8_t)mask;
     }
 }
 
@@ -150,21 +195,36 @@ __device__ __forceinline__ void cluster_sum_vec(cg::cluster_group& cl, CoarseSme
     __syncthreads();
 }
 
-// This CTA's rows' Z^T r (per-warp shared accumulators, then fixed warp order) and r.r into
-// vec[par]; then the cluster sum into w.
+// This CTA's rows' Z^T r and r.r into vec[par]; then the cluster sum into w. No atomics: per
+// step of 32 rows a warp sums each slab's six values with a fixed butterfly and lane 0 adds them
+// to the warp's own accumulators; the warps' accumulators are then added in warp order.
 __device__ __forceinline__ void coarse_restrict(cg::cluster_group& cl, CoarseSmem& cs, const BatchView& v, int inst,
                                                 int64_t a0, int64_t a1, double rr, double* sh, int& par) {
-    const int K = 6 * v.ns, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int K = 6 * v.ns, warp = threadIdx.x >> 5, nw = blockDim.x >> 5, lane = threadIdx.x & 31;
     for (int t = threadIdx.x; t < kMaxWarps * kMaxCoarse; t += blockDim.x) (&cs.wacc[0][0])[t] = 0.0;
     __syncthreads();
-    for (int64_t n = a0 + threadIdx.x; n < a1; n += blockDim.x) {
-        const int s = slab_of(v, inst, n);
-        double Z[3][6];
-        slab_modes(v, inst, n, s, Z);
-        const double r0 = v.r[3 * n], r1 = v.r[3 * n + 1], r2 = v.r[3 * n + 2];
-        for (int j = 0; j < 6; ++j) {
-            const double t = Z[0][j] * r0 + Z[1][j] * r1 + Z[2][j] * r2;
-            if (t != 0.0) atomicAdd(&cs.wacc[warp][6 * s + j], t);
+    for (int64_t base = a0; base < a1; base += blockDim.x) {  // the same trip count in every thread
+        const int64_t n = base + threadIdx.x;
+        const bool in = n < a1;
+        int s = 0;
+        double t[6] = {0, 0, 0, 0, 0, 0};
+        if (in) {
+            s = v.slab[n];
+            double Z[3][6];
+            slab_modes(v, inst, n, s, Z);
+            const double r0 = v.r[3 * n], r1 = v.r[3 * n + 1], r2 = v.r[3 * n + 2];
+#pragma unroll
+            for (int j = 0; j < 6; ++j) t[j] = Z[0][j] * r0 + Z[1][j] * r1 + Z[2][j] * r2;
+        }
+        for (uint32_t present = __reduce_or_sync(0xffffffffu, in ? 1u << s : 0u); present; present &= present - 1) {
+            const int sl = __ffs(present) - 1;
+#pragma unroll
+            for (int j = 0; j < 6; ++j) {
+                double x = in && s == sl ? t[j] : 0.0;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+                if (lane == 0) cs.wacc[warp][6 * sl + j] += x;
+            }
         }
     }
     rr = bsum(rr, sh);
@@ -196,66 +256,80 @@ __device__ __forceinline__ void coarse_solve(CoarseSmem& cs, int K) {
     __syncthreads();
 }
 
-// E = Z^T A Z of the instance (this CTA's rows, then the cluster sum), its inverse in place
+// E = Z^T A Z of the instance (this CTA's rows, then the cluster sum), its inverse in place.
+// No atomics, every sum in a fixed order: each row's sums per slab go to the row's entries, then
+// every value of this CTA's share of E is one thread's sum over its list in node order.
 template <typename VT>
 __device__ void coarse_setup(cg::cluster_group& cl, CoarseSmem& cs, const SellView& A, const VT* __restrict__ val,
                              const BatchView& v, int inst, int64_t a0, int64_t a1) {
     const int K = 6 * v.ns;
     for (int t = threadIdx.x; t < kMaxCoarse * kMaxCoarse; t += blockDim.x) cs.Epart[t] = 0.0;
-    __syncthreads();
     for (int64_t n = a0 + threadIdx.x; n < a1; n += blockDim.x) {
-        const int sn = slab_of(v, inst, n);
-        double Zn[3][6];
-        slab_modes(v, inst, n, sn, Zn);
+        const int sn = v.slab[n];
         const int64_t sl = n >> 5;
         const int lane = (int)(n & 31);
         const int64_t base = A.slice_base[sl];
         const int w = A.slice_width[sl];
-        double T[3][6] = {{0}};
-        int cur = -1;
-        auto flush = [&](int sm) {
-            for (int i = 0; i < 6; ++i)
-                for (int j = 0; j < 6; ++j) {
-                    const double e = Zn[0][i] * T[0][j] + Zn[1][i] * T[1][j] + Zn[2][i] * T[2][j];
-                    if (e != 0.0) atomicAdd(&cs.Epart[(6 * sn + i) * kMaxCoarse + 6 * sm + j], e);
+        double* out = v.tbuf + 18 * (int64_t)v.toff[n];
+        uint32_t todo = v.omask[n];
+        for (int want = sn;;) {
+            double T[3][6] = {{0}};
+            double S[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // FP32 storage: the row's sum, in storage order
+            for (int k = 0; k <= w; ++k) {
+                double blk[9];
+                int64_t m;
+                if (k < w) {
+                    m = A.col[base + 32 * (int64_t)k + lane];
+                    const VT* p = val + 9 * (base + 32 * (int64_t)k) + lane;
+                    bool any = false;
+                    for (int q = 0; q < 9; ++q) {
+                        blk[q] = (double)p[32 * q];
+                        S[q] += blk[q];
+                        any |= blk[q] != 0.0;
+                    }
+                    if (!any) continue;
+                } else {
+                    // the FP32 storage's diagonal block, minus the row's sum: the own slab's pass
+                    if (!A.diag64 || want != sn) break;
+                    m = n;
+                    for (int q = 0; q < 9; ++q) blk[q] = -S[q];
                 }
-            for (int r = 0; r < 3; ++r)
-                for (int j = 0; j < 6; ++j) T[r][j] = 0.0;
-        };
-        double S[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // FP32 storage: the row's sum, in storage order
-        for (int k = 0; k <= w; ++k) {
-            double blk[9];
-            int64_t m;
-            if (k < w) {
-                m = A.col[base + 32 * (int64_t)k + lane];
-                const VT* p = val + 9 * (base + 32 * (int64_t)k) + lane;
-                bool any = false;
-                for (int q = 0; q < 9; ++q) {
-                    blk[q] = (double)p[32 * q];
-                    S[q] += blk[q];
-                    any |= blk[q] != 0.0;
-                }
-                if (!any) continue;
-            } else {
-                if (!A.diag64) break;  // the FP32 storage's diagonal block: minus the row's sum
-                m = n;
-                for (int q = 0; q < 9; ++q) blk[q] = -S[q];
+                const int sm = v.slab[m];
+                if (sm != want) continue;
+                if (A.fixed)
+                    for (int q = 0; q < 9; ++q)
+                        if (A.fixed[3 * n + q / 3] || A.fixed[3 * m + q % 3]) blk[q] = 0.0;
+                double Zm[3][6];
+                slab_modes(v, inst, m, sm, Zm);
+                for (int r = 0; r < 3; ++r)
+                    for (int j = 0; j < 6; ++j)
+                        T[r][j] += blk[3 * r] * Zm[0][j] + blk[3 * r + 1] * Zm[1][j] + blk[3 * r + 2] * Zm[2][j];
             }
-            if (A.fixed)
-                for (int q = 0; q < 9; ++q)
-                    if (A.fixed[3 * n + q / 3] || A.fixed[3 * m + q % 3]) blk[q] = 0.0;
-            const int sm = slab_of(v, inst, m);
-            if (sm != cur) {
-                if (cur >= 0) flush(cur);
-                cur = sm;
-            }
-            double Zm[3][6];
-            slab_modes(v, inst, m, sm, Zm);
             for (int r = 0; r < 3; ++r)
-                for (int j = 0; j < 6; ++j)
-                    T[r][j] += blk[3 * r] * Zm[0][j] + blk[3 * r + 1] * Zm[1][j] + blk[3 * r + 2] * Zm[2][j];
+                for (int j = 0; j < 6; ++j) out[6 * r + j] = T[r][j];
+            out += 18;
+            if (!todo) break;
+            want = __ffs(todo) - 1;
+            todo &= todo - 1;
         }
-        if (cur >= 0) flush(cur);
+    }
+    __syncthreads();  // the entries and the zeroed share are visible to the whole CTA
+    const int64_t* lp = v.lptr + 64 * (int64_t)inst;
+    for (int t = threadIdx.x; t < 64 * 36; t += blockDim.x) {
+        const int key = t / 36, val_ = t % 36, sn = key >> 3, sm = key & 7;
+        if (sn >= v.ns || sm >= v.ns || lp[key] == lp[key + 1]) continue;
+        const int64_t lo = list_lower_bound(v.lnode, lp[key], lp[key + 1], a0);
+        const int64_t hi = list_lower_bound(v.lnode, lo, lp[key + 1], a1);
+        const int i = val_ / 6, j = val_ % 6;
+        double acc = 0.0;
+        for (int64_t q = lo; q < hi; ++q) {
+            const int64_t n = v.lnode[q];
+            const double* T = v.tbuf + 18 * (int64_t)v.lent[q];
+            double z[3];
+            slab_mode_col(v, inst, n, sn, i, z);
+            acc += z[0] * T[j] + z[1] * T[6 + j] + z[2] * T[12 + j];
+        }
+        cs.Epart[(6 * sn + i) * kMaxCoarse + 6 * sm + j] = acc;
     }
     cl.sync();
     const unsigned nb = cl.num_blocks();
@@ -402,7 +476,7 @@ __global__ void __launch_bounds__(512) batch_pcg_kernel(SellView A, const VT* __
             coarse_restrict(cl, cs, v, inst, a0, a1, rr0, sh, vpar);
             coarse_solve(cs, K);
             for (int64_t n = a0 + threadIdx.x; n < a1; n += blockDim.x) {
-                const int sl = slab_of(v, inst, n);
+                const int sl = v.slab[n];
                 double Z[3][6];
                 slab_modes(v, inst, n, sl, Z);
                 const double* cc = cs.c + 6 * sl;
@@ -478,7 +552,7 @@ __global__ void __launch_bounds__(512) batch_pcg_kernel(SellView A, const VT* __
                 coarse_restrict(cl, cs, v, inst, a0, a1, rr1, sh, vpar);
                 coarse_solve(cs, K);
                 for (int64_t n = a0 + threadIdx.x; n < a1; n += blockDim.x) {
-                    const int sl = slab_of(v, inst, n);
+                    const int sl = v.slab[n];
                     double Z[3][6];
                     slab_modes(v, inst, n, sl, Z);
                     const double* cc = cs.c + 6 * sl;
@@ -669,6 +743,10 @@ struct mphy_batch {
     int32_t cluster = 1, threads = 256;
     int32_t ns = 0;                          // slabs per instance of the two-level variant (0: off)
     DevBuf<double> slab_geo, slab_cent;
+    DevBuf<uint8_t> slab_node, omask;  // slab of every node; other slabs its row reaches
+    DevBuf<int32_t> toff, lent, lnode;
+    DevBuf<int64_t> lptr;
+    DevBuf<double> tbuf;
     cudaGraphExec_t graph = nullptr;
     int graph_cluster = 0, graph_threads = 0, graph_ns = 0;
     double graph_key[6] = {0, 0, 0, 0, 0, 0};
@@ -710,6 +788,13 @@ BatchView batch_view(mphy_batch* b, const uint8_t* active, bool totals, int maxi
     v.slab_cent = b->slab_cent.p;
     v.coords = s->mesh->coords.p;
     v.fixed = s->mesh->fixed.p;
+    v.slab = b->slab_node.p;
+    v.omask = b->omask.p;
+    v.toff = b->toff.p;
+    v.lptr = b->lptr.p;
+    v.lent = b->lent.p;
+    v.lnode = b->lnode.p;
+    v.tbuf = b->tbuf.p;
     return v;
 }
 
@@ -886,6 +971,10 @@ int mphy_batch_set_coarse(mphy_batch* b, int32_t slabs) {
         MPHY_REQUIRE(b, MPHY_ERR_INVALID_ARG, "null argument");
         MPHY_REQUIRE(slabs >= 0 && slabs <= kMaxSlabs, MPHY_ERR_INVALID_ARG,
                      "batched coarse space: 0 (off) to 8 slabs per instance");
+        if (b->graph) {  // the recorded Newton iteration refers to the coarse buffers replaced here
+            MPHY_CUDA(cudaGraphExecDestroy(b->graph));
+            b->graph = nullptr;
+        }
         if (slabs == 0) {
             b->ns = 0;
             return (int)MPHY_OK;
@@ -894,6 +983,7 @@ int mphy_batch_set_coarse(mphy_batch* b, int32_t slabs) {
         const std::vector<double>& X = m->coords_host;
         const size_t ni = (size_t)b->n_inst;
         std::vector<double> geo(4 * ni), cen(3 * ni * kMaxSlabs, 0.0);
+        std::vector<uint8_t> slab(m->n_node, 0);
         for (size_t i = 0; i < ni; ++i) {
             const int32_t n0 = b->node_ptr_host[i], n1 = b->node_ptr_host[i + 1];
             double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
@@ -917,6 +1007,7 @@ int mphy_batch_set_coarse(mphy_batch* b, int32_t slabs) {
             for (int32_t n = n0; n < n1; ++n) {
                 int sl = (int)std::floor((X[3 * (size_t)n + ax] - lo[ax]) / len * slabs);
                 sl = sl < 0 ? 0 : (sl >= slabs ? slabs - 1 : sl);
+                slab[n] = (uint8_t)sl;
                 cnt[sl] += 1.0;
                 for (int d = 0; d < 3; ++d) cen[3 * (i * kMaxSlabs + sl) + d] += X[3 * (size_t)n + d];
             }
@@ -930,6 +1021,61 @@ int mphy_batch_set_coarse(mphy_batch* b, int32_t slabs) {
         b->slab_geo.upload(geo.data(), geo.size(), st);
         b->slab_cent.alloc(cen.size());
         b->slab_cent.upload(cen.data(), cen.size(), st);
+        const int32_t nn = m->n_node;
+        b->slab_node.alloc(nn);
+        b->slab_node.upload(slab.data(), nn, st);
+        b->omask.alloc(nn);
+        slab_mask_kernel<<<stride_grid(nn, 256, b->s->ctx->sm_count), 256, 0, st>>>(b->s->A, b->slab_node.p,
+                                                                                   b->omask.p);
+        MPHY_CUDA(cudaGetLastError());
+        std::vector<uint8_t> om(nn);
+        MPHY_CUDA(cudaMemcpyAsync(om.data(), b->omask.p, nn, cudaMemcpyDeviceToHost, st));
+        MPHY_CUDA(cudaStreamSynchronize(st));
+        // entries: own slab first, then the other slabs in slab order; lists per (instance, slab
+        // pair) in node order
+        std::vector<int32_t> toff(nn);
+        int64_t entries = 0;
+        for (int32_t n = 0; n < nn; ++n) {
+            toff[n] = (int32_t)entries;
+            entries += 1 + __builtin_popcount(om[n]);
+            MPHY_REQUIRE(entries < INT32_MAX, MPHY_ERR_UNSUPPORTED, "batched coarse space: too many row entries");
+        }
+        std::vector<int64_t> lptr(64 * ni + 1, 0);
+        std::vector<int32_t> lent, lnode;
+        lent.reserve(entries);
+        lnode.reserve(entries);
+        std::vector<std::vector<int32_t>> be(64), bn(64);
+        for (size_t i = 0; i < ni; ++i) {
+            for (int k = 0; k < 64; ++k) {
+                be[k].clear();
+                bn[k].clear();
+            }
+            for (int32_t n = b->node_ptr_host[i]; n < b->node_ptr_host[i + 1]; ++n) {
+                const int sn = slab[n];
+                const uint32_t o = om[n];
+                be[8 * sn + sn].push_back(toff[n]);
+                bn[8 * sn + sn].push_back(n);
+                for (int sm = 0; sm < slabs; ++sm)
+                    if (o >> sm & 1u) {
+                        be[8 * sn + sm].push_back(toff[n] + 1 + __builtin_popcount(o & ((1u << sm) - 1u)));
+                        bn[8 * sn + sm].push_back(n);
+                    }
+            }
+            for (int k = 0; k < 64; ++k) {
+                lent.insert(lent.end(), be[k].begin(), be[k].end());
+                lnode.insert(lnode.end(), bn[k].begin(), bn[k].end());
+                lptr[64 * i + k + 1] = (int64_t)lent.size();
+            }
+        }
+        b->toff.alloc(nn);
+        b->toff.upload(toff.data(), nn, st);
+        b->lptr.alloc(lptr.size());
+        b->lptr.upload(lptr.data(), lptr.size(), st);
+        b->lent.alloc(lent.size());
+        b->lent.upload(lent.data(), lent.size(), st);
+        b->lnode.alloc(lnode.size());
+        b->lnode.upload(lnode.data(), lnode.size(), st);
+        b->tbuf.alloc((size_t)entries * 18);
         MPHY_CUDA(cudaStreamSynchronize(st));
         b->ns = slabs;
         return (int)MPHY_OK;
