@@ -47,6 +47,7 @@ import numpy as np
 from .meshgen import Problem
 
 GMSH_VOLUME = {5: 8, 11: 10, 12: 27}  # hex8, tet10, hex27 (the 27-node hex order is Gmsh's)
+GMSH_PRISM18 = 13
 # material name -> (model code of mphy.h, config line holding its parameters, parameter count)
 MATERIALS = {"Matl_NeoHookean": (0, "data_deviatoric", 1), "Matl_MooneyRivlin": (1, "data_deviatoric", 2),
              "Matl_Gent": (2, "data_deviatoric", 2), "Matl_ArrudaBoyce": (3, "data", 2)}
@@ -400,6 +401,13 @@ def read_config(config_path, mesh_path=None):
     if m["ndim"] != 3:
         raise NotImplementedError("config: this build solves 3D meshes (hex8, tet10, hex27)")
     vol = m["volume"]
+    if any(t == GMSH_PRISM18 for t, _, _ in vol):
+        # Elem_Solid_3D_Mixed1 declares the 18-node wedge (Elem_Solid_3D_Mixed1.cpp:48-53), but the
+        # reference cannot evaluate it: computeBasisFunctions3D has no branch for ELEM_SHAPE_WEDGE
+        # and throws (GeomDataLagrange.cpp:349-382), and LagrangeBasisFunsPrism defines the 6-node
+        # prism only (BasisFunctionsLagrange.cpp:1412-1490). The same refusal here.
+        raise NotImplementedError("mesh: 18-node prisms (Gmsh type 13) have no Lagrange basis in the reference "
+                                  "(computeBasisFunctions3D ... Invalid element type)")
     npe = {GMSH_VOLUME.get(t) for t, _, _ in vol}
     if None in npe or len(npe) != 1:
         raise NotImplementedError("mesh: volume elements must all be hex8 (type 5), all tet10 (type 11) or all "

@@ -280,3 +280,23 @@ def test_quad9_traction_matches_consistent_nodal_forces():
     # normal part: the face area (outward corner order: dv x du points into the body)
     Fn = rio.traction_forces(p.coords, rio.boundary_faces(p, lambda X: np.isclose(X[:, 0], 4.0)), [0.3, 0.0, 0.0])
     assert np.allclose(Fn.sum(axis=0), [-0.3, 0.0, 0.0], rtol=1e-13, atol=1e-15)
+
+
+def test_prism18_is_refused_like_the_reference(tmp_path):
+    """An 18-node prism mesh (Gmsh type 13) for ELEM_SOLID_3D_MIXED1: the reference declares the
+    element (Elem_Solid_3D_Mixed1.cpp:48-53) but throws when it evaluates it (no ELEM_SHAPE_WEDGE
+    branch in GeomDataLagrange.cpp:349-382, no 18-node case in LagrangeBasisFunsPrism), so the
+    reader refuses the mesh."""
+    p = meshgen.hex27_cantilever(2, 1, 1)
+    clamp = rio.boundary_faces(p, lambda X: np.isclose(X[:, 0], 0.0))
+    _write(tmp_path, p, {"clamp": clamp})
+    lines = (tmp_path / "m.msh").read_text().splitlines()
+    out = []
+    for ln in lines:
+        tok = ln.split()
+        if len(tok) == 5 + 27 and tok[1] == "12":
+            ln = " ".join([tok[0], "13"] + tok[2:5] + tok[5:23])
+        out.append(ln)
+    (tmp_path / "m.msh").write_text("\n".join(out) + "\n")
+    with pytest.raises(NotImplementedError, match="18-node prisms"):
+        rio.read_config(tmp_path / "config")
