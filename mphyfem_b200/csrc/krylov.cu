@@ -595,12 +595,13 @@ __device__ __forceinline__ void restrict_node(bool lin, const double rr[3], cons
 }
 
 // w = Z^T r per aggregate. Work item (a, part) sums a contiguous part of aggregate a's node
-// list, two nodes per thread and step with every load issued before the arithmetic (offsets and
-// mask from copies in node-list order, coalesced; only r is gathered); the CTA
+// list, kRestrictNodes nodes per thread and step with every load issued before the arithmetic
+// (offsets and mask from copies in node-list order, coalesced; only r is gathered); the CTA
 // that finishes an aggregate's last part adds the parts' sums in part order, so w does not
-// depend on which CTA ran which part. A persistent grid walks the items. NM (modes per
+// depend on which CTA ran which part. The CTAs walk the items in a grid-stride loop. NM (modes per
 // aggregate) is a template parameter, so the rigid-body form keeps six accumulators and fits
 // four CTAs per SM.
+constexpr int kRestrictNodes = 2;  // nodes per thread and step, all loads issued first
 template <typename XT, int NM>
 __global__ void __launch_bounds__(kThreads, NM == 6 ? 4 : 3) coarse_restrict_kernel(CoarseView cv, int parts,
                                                                                    const XT* __restrict__ r,
@@ -617,17 +618,18 @@ __global__ void __launch_bounds__(kThreads, NM == 6 ? 4 : 3) coarse_restrict_ker
         const int64_t b0 = cv.agg_ptr[a], len = cv.agg_ptr[a + 1] - b0;
         const int64_t lo = b0 + len * part / parts, hi = b0 + len * (part + 1) / parts;
         double w[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-        for (int64_t i = lo + threadIdx.x; i < hi; i += 2 * (int64_t)blockDim.x) {
-            const bool two = i + blockDim.x < hi;
-            const int64_t li[2] = {i, two ? i + blockDim.x : i};  // positions in the node list
-            int64_t nd[2];
-            nd[0] = cv.agg_nodes[li[0]];
-            nd[1] = cv.agg_nodes[li[1]];
-            XT rv[2][3];
-            double dv[2][3];
-            uint8_t fx[2][3];
+        for (int64_t i = lo + threadIdx.x; i < hi; i += kRestrictNodes * (int64_t)blockDim.x) {
+            int64_t li[kRestrictNodes], nd[kRestrictNodes];  // positions in the node list, nodes
 #pragma unroll
-            for (int k = 0; k < 2; ++k)
+            for (int k = 0; k < kRestrictNodes; ++k) {
+                li[k] = i + k * (int64_t)blockDim.x < hi ? i + k * (int64_t)blockDim.x : i;
+                nd[k] = cv.agg_nodes[li[k]];
+            }
+            XT rv[kRestrictNodes][3];
+            double dv[kRestrictNodes][3];
+            uint8_t fx[kRestrictNodes][3];
+#pragma unroll
+            for (int k = 0; k < kRestrictNodes; ++k)
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
                     dv[k][c] = cv.dperm[3 * li[k] + c];
@@ -635,8 +637,8 @@ __global__ void __launch_bounds__(kThreads, NM == 6 ? 4 : 3) coarse_restrict_ker
                     rv[k][c] = r[3 * nd[k] + c];
                 }
 #pragma unroll
-            for (int k = 0; k < 2; ++k) {
-                if (k == 1 && !two) break;
+            for (int k = 0; k < kRestrictNodes; ++k) {
+                if (i + k * (int64_t)blockDim.x >= hi) break;
                 double rr[3];
 #pragma unroll
                 for (int c = 0; c < 3; ++c) rr[c] = fx[k][c] ? 0.0 : (double)rv[k][c];
@@ -679,11 +681,13 @@ __global__ void __launch_bounds__(kThreads, NM == 6 ? 4 : 3) coarse_restrict_ker
     }
 }
 
-// Persistent grid of the restriction with about two work items per resident CTA.
+// Grid of the restriction: at most one work item per resident CTA (whole aggregates when there
+// are about as many aggregates as resident CTAs), so every CTA pays the item's reduction, fence
+// and ticket once.
 template <typename XT, int NM>
 void launch_restrict_nm(const CoarseView& cv, const XT* r, const PcgState* st, cudaStream_t s, int sm) {
     const unsigned grid = resident_grid((const void*)coarse_restrict_kernel<XT, NM>, (int64_t)1 << 40, kThreads, sm);
-    int parts = (int)((2 * (int64_t)grid + cv.n_agg - 1) / cv.n_agg);
+    int parts = (int)((int64_t)grid / cv.n_agg);
     parts = std::max(1, std::min(parts, kMaxRestrictParts));
     const unsigned g = (unsigned)std::min<int64_t>(grid, (int64_t)cv.n_agg * parts);
     coarse_restrict_kernel<XT, NM><<<g, kThreads, 0, s>>>(cv, parts, r, st);
@@ -722,21 +726,22 @@ __global__ void __launch_bounds__(256) coarse_gemv_kernel(CoarseView cv, PcgStat
     while ((I + 1) * (I + 2) / 2 <= t) ++I;
     const int J = t - I * (I + 1) / 2;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (tid < 64) {
-        wI[tid] = cv.w[64 * I + tid];
-        wJ[tid] = cv.w[64 * J + tid];
-    }
-    __syncthreads();
     const int tx = lane & 15, ty = 2 * warp + (lane >> 4);
     const double* E = cv.einv + (int64_t)t * 4096;
     double rp[4], cp[4] = {0.0, 0.0, 0.0, 0.0};
     double2 ev[4][2];
+    // the tile's loads first: they do not wait for w
 #pragma unroll
     for (int a = 0; a < 4; ++a) {
         const double2* row = reinterpret_cast<const double2*>(E + 64 * (4 * ty + a) + 4 * tx);
         ev[a][0] = ld_once(row);
         ev[a][1] = ld_once(row + 1);
     }
+    if (tid < 64) {
+        wI[tid] = cv.w[64 * I + tid];
+        wJ[tid] = cv.w[64 * J + tid];
+    }
+    __syncthreads();
 #pragma unroll
     for (int a = 0; a < 4; ++a) {
         const double e[4] = {ev[a][0].x, ev[a][0].y, ev[a][1].x, ev[a][1].y};
