@@ -9,8 +9,11 @@
 //      the same on every run;
 //   3. E = L L^T by a right-looking blocked Cholesky (64x64 tiles, FP64), W = L^{-1} by blocked
 //      forward substitution, E^{-1} = W^T W, kept in FP64 for the per-iteration GEMV (FP32
-//      rounding of the inverse of an ill-conditioned E can make it indefinite).
+//      rounding of the inverse of an ill-conditioned E can make it indefinite). The aggregates
+//      are numbered with the longest box axis slowest, so E is banded; L stays inside the band
+//      and the Cholesky and forward-substitution steps touch only the tiles inside it.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <vector>
 
@@ -568,11 +571,11 @@ __global__ void __launch_bounds__(256) trtri_finalize(double* W, int kp, int k) 
         for (int r = 0; r < 4; ++r) W[(int64_t)(k * T + ty + 16 * q) * kp + j * T + tx + 16 * r] = -acc[q][r];
 }
 
-__global__ void __launch_bounds__(256) trtri_update(const double* E, double* W, int kp, int k, int nb) {
+// rows: the tile rows i = k + 1 .. k + rows whose L_ik can be nonzero (E's band)
+__global__ void __launch_bounds__(256) trtri_update(const double* E, double* W, int kp, int k, int rows) {
     extern __shared__ double sm[];
     double (*A)[TP] = reinterpret_cast<double (*)[TP]>(sm);
     double (*B)[TP] = reinterpret_cast<double (*)[TP]>(sm + T * TP);
-    const int rows = nb - k - 1;
     const int i = k + 1 + (int)(blockIdx.x % rows), j = (int)(blockIdx.x / rows);
     const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;
     load_tile(A, E, kp, i, k);  // L_ik
@@ -650,12 +653,23 @@ void CoarseSpace::init(mphy_ctx* ctx, const mphy_mesh* mesh, const mphy_pattern*
     }
     n_agg_ = ng_[0] * ng_[1] * ng_[2];
     kp_ = ((nm_ * n_agg_ + T - 1) / T) * T;
+    // numbering: the axis with the most boxes varies slowest, so that E = Z^T A Z has the
+    // narrowest band (neighbour boxes are at most 1 + n0 + n0 n1 apart in index). E's Cholesky
+    // factor fills only inside that band, and the factorisation skips the tiles outside it.
+    std::array<int, 3> ord = {0, 1, 2};
+    std::stable_sort(ord.begin(), ord.end(), [&](int p, int q) { return ng_[p] < ng_[q]; });
+    for (int k = 0; k < 3; ++k) ngl_[k] = ng_[ord[k]];
+    {
+        const int64_t reach = 1 + ngl_[0] + (int64_t)ngl_[0] * ngl_[1];
+        const int64_t rows = reach * nm_ + nm_ - 1;  // largest row - column distance inside the band
+        band_tiles_ = (int)std::min<int64_t>(kp_ / T - 1, (rows + T - 1) / T);
+    }
     MPHY_REQUIRE(kp_ <= 16384, MPHY_ERR_UNSUPPORTED, "coarse space larger than 16384");
     std::vector<int32_t> agg(nn), cnt(n_agg_, 0);
     for (int32_t n = 0; n < nn; ++n) {
         int c[3];
         for (int d = 0; d < 3; ++d) c[d] = std::min(ng_[d] - 1, (int)((X[3 * n + d] - lo[d]) / L[d] * ng_[d]));
-        agg[n] = c[0] + ng_[0] * (c[1] + ng_[1] * c[2]);
+        agg[n] = c[ord[0]] + ngl_[0] * (c[ord[1]] + ngl_[1] * c[ord[2]]);
         ++cnt[agg[n]];
     }
     std::vector<int64_t> ptr(n_agg_ + 1, 0);
@@ -674,7 +688,7 @@ void CoarseSpace::init(mphy_ctx* ctx, const mphy_mesh* mesh, const mphy_pattern*
         std::vector<int32_t> box(nn);
         for (int32_t n = 0; n < nn; ++n) {
             const int a = agg[n];
-            box[n] = (a % ng_[0]) | (((a / ng_[0]) % ng_[1]) << 10) | ((a / (ng_[0] * ng_[1])) << 20);
+            box[n] = (a % ngl_[0]) | (((a / ngl_[0]) % ngl_[1]) << 10) | ((a / (ngl_[0] * ngl_[1])) << 20);
         }
         aggbox_.alloc(nn);
         aggbox_.upload(box.data(), nn, s);
@@ -745,11 +759,11 @@ void CoarseSpace::setup(const SellView& A, const VT* aval, const double* disp, c
     const unsigned rows = (unsigned)((mesh_->n_node + kRowThreads - 1) / kRowThreads);
     if (nm_ == 12) {
         coarse_rows_kernel<VT, 12><<<rows, kRowThreads, 0, s>>>(A, aval, cv, aggbox_.p, lmask_.p, toff_.p, tbuf_.p);
-        coarse_sum_kernel<12><<<n_agg_ * kSlots, kSumThreads, 0, s>>>(cv, ng_[0], ng_[1], lptr_.p, lent_.p, lnode_.p,
+        coarse_sum_kernel<12><<<n_agg_ * kSlots, kSumThreads, 0, s>>>(cv, ngl_[0], ngl_[1], lptr_.p, lent_.p, lnode_.p,
                                                                       tbuf_.p, E_.p);
     } else {
         coarse_rows_kernel<VT, 6><<<rows, kRowThreads, 0, s>>>(A, aval, cv, aggbox_.p, lmask_.p, toff_.p, tbuf_.p);
-        coarse_sum_kernel<6><<<n_agg_ * kSlots, kSumThreads, 0, s>>>(cv, ng_[0], ng_[1], lptr_.p, lent_.p, lnode_.p,
+        coarse_sum_kernel<6><<<n_agg_ * kSlots, kSumThreads, 0, s>>>(cv, ngl_[0], ngl_[1], lptr_.p, lent_.p, lnode_.p,
                                                                      tbuf_.p, E_.p);
     }
     MPHY_CUDA(cudaGetLastError());
@@ -871,7 +885,7 @@ void CoarseSpace::record_factorisation(cudaStream_t s, int nb, size_t sm2) {
     MPHY_CUDA(cudaStreamWaitEvent(s_tri, ev_col, 0));
     bool rest_pending = false;
     for (int j = 0; j < nb; ++j) {
-        const int m = nb - j - 1;
+        const int m = std::min(nb - j - 1, band_tiles_);  // tiles below (j, j) inside E's band
         potrf_inv_tile<<<1, kPotrfThreads, 0, s>>>(E_.p, W_.p, kp_, j, err_.p);
         launches += 1;
         if (m > 0) {
@@ -885,7 +899,7 @@ void CoarseSpace::record_factorisation(cudaStream_t s, int nb, size_t sm2) {
             launches += 1;
         }
         if (m > 0) {
-            trtri_update<<<m * (j + 1), 256, sm2, s_tri>>>(E_.p, W_.p, kp_, j, nb);
+            trtri_update<<<m * (j + 1), 256, sm2, s_tri>>>(E_.p, W_.p, kp_, j, m);
             launches += 1;
             if (m > 1) {
                 MPHY_CUDA(cudaStreamWaitEvent(s_rest, ev_col, 0));

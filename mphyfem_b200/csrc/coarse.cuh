@@ -47,7 +47,9 @@ class CoarseSpace {
     mphy_ctx* ctx_ = nullptr;
     const mphy_mesh* mesh_ = nullptr;
     const mphy_pattern* pat_ = nullptr;
-    int ng_[3] = {1, 1, 1};
+    int ng_[3] = {1, 1, 1};   // boxes along x, y, z
+    int ngl_[3] = {1, 1, 1};  // boxes along the numbering's axes, fastest first (fewest boxes first)
+    int band_tiles_ = 0;      // tiles of E's Cholesky factor below the diagonal tile that can be nonzero
     int n_agg_ = 0, kp_ = 0;
     DevBuf<int32_t> agg_, agg_nodes_, err_;
     DevBuf<int32_t> aggbox_;  // [n_node] aggregate box bx | by << 10 | bz << 20
