@@ -242,9 +242,71 @@ __global__ void __launch_bounds__(kRowThreads, 4) coarse_rows_kernel(SellView A,
     }
 }
 
-// Kernel 2: one CTA per (aggregate a, slot s); list[lptr[a 14 + s] ..) holds the entries of the
-// nodes of a that reach slot s (node-list order) and their nodes. Thread (g, v) sums output value
-// v over part g of the list; the parts are added in order.
+// Kernel 2, rigid-body modes: one CTA per (aggregate a, slot s); list[lptr[a 14 + s] ..) holds
+// the entries of the nodes of a that reach slot s (node-list order) and their nodes. Each thread
+// takes every kSumRigidThreads-th list item and adds its whole block Z_n^T T_{n,b} (36 values)
+// in registers; the block is then summed over the CTA (butterfly per warp, warps in order).
+constexpr int kSumRigidThreads = 128;
+__global__ void __launch_bounds__(kSumRigidThreads) coarse_sum_rigid_kernel(CoarseView cv, int ngx, int ngy,
+                                                                            const int64_t* __restrict__ lptr,
+                                                                            const int32_t* __restrict__ lent,
+                                                                            const int32_t* __restrict__ lnode,
+                                                                            const double* __restrict__ tbuf,
+                                                                            double* __restrict__ E) {
+    __shared__ double red[kSumRigidThreads / 32][36];
+    const int a = blockIdx.x / kSlots, s = blockIdx.x % kSlots;
+    const int64_t b0 = lptr[blockIdx.x], b1 = lptr[blockIdx.x + 1];
+    if (b0 == b1) return;
+    double acc[36];
+#pragma unroll
+    for (int v = 0; v < 36; ++v) acc[v] = 0.0;
+    for (int64_t q = b0 + threadIdx.x; q < b1; q += kSumRigidThreads) {
+        const int64_t n = lnode[q];
+        const double2* t2 = reinterpret_cast<const double2*>(tbuf + 18 * (int64_t)lent[q]);
+        double T[18];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            const double2 v = t2[k];
+            T[2 * k] = v.x;
+            T[2 * k + 1] = v.y;
+        }
+        const double dx = cv.d[3 * n], dy = cv.d[3 * n + 1], dz = cv.d[3 * n + 2];
+        const double k0 = cv.fixed[3 * n] ? 0.0 : 1.0, k1 = cv.fixed[3 * n + 1] ? 0.0 : 1.0,
+                     k2 = cv.fixed[3 * n + 2] ? 0.0 : 1.0;
+#pragma unroll
+        for (int j = 0; j < 6; ++j) {
+            const double t0 = k0 * T[j], t1 = k1 * T[6 + j], t2v = k2 * T[12 + j];
+            acc[j] += t0;
+            acc[6 + j] += t1;
+            acc[12 + j] += t2v;
+            acc[18 + j] += -dy * t0 + dx * t1;
+            acc[24 + j] += -dz * t1 + dy * t2v;
+            acc[30 + j] += dz * t0 - dx * t2v;
+        }
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int v = 0; v < 36; ++v) {
+        double x = acc[v];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) red[warp][v] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x >= 36) return;
+    const int i = threadIdx.x / 6, j = threadIdx.x % 6;
+    const bool own = s == 13;
+    if (own && j > i) return;  // E's lower triangle
+    double x = 0.0;
+#pragma unroll
+    for (int w = 0; w < kSumRigidThreads / 32; ++w) x += red[w][threadIdx.x];
+    const int ax = a % ngx, ay = (a / ngx) % ngy, az = a / (ngx * ngy);
+    const int b = own ? a : (ax + s % 3 - 1) + ngx * ((ay + (s / 3) % 3 - 1) + ngy * (az + s / 9 - 1));
+    E[(int64_t)(6 * a + i) * cv.kp + 6 * b + j] = x;
+}
+
+// Kernel 2, linear modes (144 values per block, too many for registers): thread (g, v) sums
+// output value v over part g of the list; the parts are added in order.
 template <int NM>
 __global__ void __launch_bounds__(kSumThreads) coarse_sum_kernel(CoarseView cv, int ngx, int ngy,
                                                                  const int64_t* __restrict__ lptr,
@@ -763,8 +825,8 @@ void CoarseSpace::setup(const SellView& A, const VT* aval, const double* disp, c
                                                                       tbuf_.p, E_.p);
     } else {
         coarse_rows_kernel<VT, 6><<<rows, kRowThreads, 0, s>>>(A, aval, cv, aggbox_.p, lmask_.p, toff_.p, tbuf_.p);
-        coarse_sum_kernel<6><<<n_agg_ * kSlots, kSumThreads, 0, s>>>(cv, ngl_[0], ngl_[1], lptr_.p, lent_.p, lnode_.p,
-                                                                     tbuf_.p, E_.p);
+        coarse_sum_rigid_kernel<<<n_agg_ * kSlots, kSumRigidThreads, 0, s>>>(cv, ngl_[0], ngl_[1], lptr_.p, lent_.p,
+                                                                             lnode_.p, tbuf_.p, E_.p);
     }
     MPHY_CUDA(cudaGetLastError());
     launches += 4;
