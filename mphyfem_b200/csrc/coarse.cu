@@ -418,17 +418,14 @@ __device__ __forceinline__ void load_tile(double (*S)[TP], const double* M, int 
 //   Cholesky, step c: the owners of column c publish it (unscaled; final after step c - 1);
 //   every thread computes rd[c] = 1 / sqrt(A(c,c)), subtracts A(i,c) A(k,c) rd[c]^2 from its
 //   entries (i, k) with c < k <= i, and the owners scale their column c by rd[c], giving L.
-//   Inverse, step i: X = L^{-1} by right-looking forward substitution on B (initially I): the
-//   owners of column i of L and of row i of B publish them; every entry (m, l) with
-//   l <= i < m subtracts L(m,i) B(i,l) rd[i]. Row m of B is final after step m - 1 and
-//   X(m, l) = B(m, l) rd[m].
+//   Inverse: L and the patches' inverses go to shared memory (dynamic, two padded tiles), and
+//   X = L^{-1} is formed by recursive doubling (four levels, below).
 constexpr int kPotrfPatches = (T / 4) * (T / 4 + 1) / 2;  // 136
 constexpr int kPotrfThreads = 160;                          // five warps, the last 24 threads idle
 
 __global__ void __launch_bounds__(kPotrfThreads) potrf_inv_tile(double* E, double* W, int kp, int j, int32_t* err) {
-    __shared__ double colv[2][T];  // Cholesky: column c; inverse: column i of L
-    __shared__ double rowv[2][T];  // inverse: row i of B
-    __shared__ double rd[T];
+    __shared__ double colv[2][T];  // Cholesky: column c
+    __shared__ double rd[T];       // 1 / L(c, c)
     const int tid = threadIdx.x;
     const bool owner = tid < kPotrfPatches;
     // patch (P, Q), Q <= P, from the row-major triangular index
@@ -438,7 +435,7 @@ __global__ void __launch_bounds__(kPotrfThreads) potrf_inv_tile(double* E, doubl
     const int Q = owner ? tid - P * (P + 1) / 2 : -1;
     if (!owner) P = -1;
     const int r0 = 4 * P, c0 = 4 * Q;
-    double A[4][4], B[4][4];
+    double A[4][4];
     const double* Et = E + (int64_t)(j * T) * kp + j * T;
     if (owner) {
 #pragma unroll
@@ -449,8 +446,6 @@ __global__ void __launch_bounds__(kPotrfThreads) potrf_inv_tile(double* E, doubl
             A[a][1] = v0.y;
             A[a][2] = v1.x;
             A[a][3] = v1.y;
-#pragma unroll
-            for (int b = 0; b < 4; ++b) B[a][b] = r0 + a == c0 + b ? 1.0 : 0.0;
         }
     }
     // ---- Cholesky: column c = 4 cq + kk, kk known at compile time
@@ -493,51 +488,111 @@ __global__ void __launch_bounds__(kPotrfThreads) potrf_inv_tile(double* E, doubl
             }
         }
     }
-    // ---- inverse: step i = 4 iq + aa
-    for (int iq = 0; iq < T / 4; ++iq) {
+    // ---- inverse X = L^{-1} by recursive doubling over the 4x4 patches: the diagonal patches
+    // first (forward substitution in registers, 1 / L(i,i) = rd[i]), then for half sizes of
+    // 1, 2, 4, 8 patches every pair of diagonal blocks [A 0; C B] gets its lower block
+    // X_BA = -X_B (L_BA X_A). Patch (P, Q), P > Q, belongs to the level of the highest bit in
+    // which P and Q differ, so each owner works at one level; four barriers per level.
+    extern __shared__ double dsm[];
+    double (*Ls)[TP] = reinterpret_cast<double (*)[TP]>(dsm);
+    double (*Xs)[TP] = reinterpret_cast<double (*)[TP]>(dsm + T * TP);
+    __syncthreads();  // rd complete
+    if (owner) {
+        double x[4][4];
 #pragma unroll
-        for (int aa = 0; aa < 4; ++aa) {
-            const int i = 4 * iq + aa, buf = i & 1;
-            if (i == T - 1) break;  // nothing below the last row
-            if (Q == iq) {
+        for (int a = 0; a < 4; ++a)
 #pragma unroll
-                for (int a = 0; a < 4; ++a)
-                    if (r0 + a > i) colv[buf][r0 + a] = A[a][aa];
-            }
-            if (P == iq) {
+            for (int b = 0; b < 4; ++b) x[a][b] = 0.0;
+        if (P == Q) {
 #pragma unroll
-                for (int b = 0; b < 4; ++b)
-                    if (c0 + b <= i) rowv[buf][c0 + b] = B[aa][b];
-            }
-            __syncthreads();
-            if (owner && P >= iq) {
-                // zero factors for rows <= i and columns > i, as above
-                const double ri = rd[i];
-                double lm[4], bl[4];
+            for (int a = 0; a < 4; ++a) {
+                const double di = rd[r0 + a];
+                x[a][a] = di;
 #pragma unroll
-                for (int a = 0; a < 4; ++a) lm[a] = r0 + a > i ? colv[buf][r0 + a] * ri : 0.0;
+                for (int b = 0; b < a; ++b) {
+                    double t = 0.0;
 #pragma unroll
-                for (int b = 0; b < 4; ++b) bl[b] = c0 + b <= i ? rowv[buf][c0 + b] : 0.0;
-#pragma unroll
-                for (int a = 0; a < 4; ++a)
-#pragma unroll
-                    for (int b = 0; b < 4; ++b) B[a][b] = fma(-lm[a], bl[b], B[a][b]);
+                    for (int k = b; k < a; ++k) t = fma(A[a][k], x[k][b], t);
+                    x[a][b] = -di * t;
+                }
             }
         }
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                Ls[r0 + a][c0 + b] = c0 + b <= r0 + a ? A[a][b] : 0.0;
+                Xs[r0 + a][c0 + b] = x[a][b];
+            }
     }
-    __syncthreads();  // rd complete
+    const int lvl = owner && P != Q ? 31 - __clz(P ^ Q) : -1;
+    for (int lv = 0; lv < 4; ++lv) {
+        const bool act = lvl == lv;
+        const int mid = 4 * (((P >> (lv + 1)) << (lv + 1)) + (1 << lv));  // first row of block B
+        double t[4][4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) t[a][b] = 0.0;
+        __syncthreads();  // the previous level's X (and the patches above) are in Xs
+        if (act) {
+            // T = L_BA X_A over the rows of block A from this patch's column on (X_A is lower)
+            for (int k = c0; k < mid; ++k) {
+                double l[4], xa[4];
+#pragma unroll
+                for (int a = 0; a < 4; ++a) l[a] = Ls[r0 + a][k];
+#pragma unroll
+                for (int b = 0; b < 4; ++b) xa[b] = Xs[k][c0 + b];
+#pragma unroll
+                for (int a = 0; a < 4; ++a)
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) t[a][b] = fma(l[a], xa[b], t[a][b]);
+            }
+        }
+        __syncthreads();
+        if (act)
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) Xs[r0 + a][c0 + b] = t[a][b];  // T in X_BA's place
+        __syncthreads();
+        if (act) {
+            // X_BA = -X_B T over the rows of block B up to this patch's last row (X_B is lower)
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) t[a][b] = 0.0;
+            for (int k = mid; k < r0 + 4; ++k) {
+                double xb[4], tt[4];
+#pragma unroll
+                for (int a = 0; a < 4; ++a) xb[a] = Xs[r0 + a][k];
+#pragma unroll
+                for (int b = 0; b < 4; ++b) tt[b] = Xs[k][c0 + b];
+#pragma unroll
+                for (int a = 0; a < 4; ++a)
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) t[a][b] = fma(-xb[a], tt[b], t[a][b]);
+            }
+        }
+        __syncthreads();
+        if (act)
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) Xs[r0 + a][c0 + b] = t[a][b];
+    }
+    __syncthreads();
     if (!owner) return;
     double* Eo = E + (int64_t)(j * T) * kp + j * T;
     double* Wo = W + (int64_t)(j * T) * kp + j * T;
 #pragma unroll
     for (int a = 0; a < 4; ++a) {
-        const double rm = rd[r0 + a];
         double l[4], x[4];
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
             const bool lower = c0 + b <= r0 + a;
             l[b] = lower ? A[a][b] : 0.0;
-            x[b] = lower ? B[a][b] * rm : 0.0;
+            x[b] = lower ? Xs[r0 + a][c0 + b] : 0.0;
         }
         double2* er = reinterpret_cast<double2*>(Eo + (int64_t)(r0 + a) * kp + c0);
         double2* wr = reinterpret_cast<double2*>(Wo + (int64_t)(r0 + a) * kp + c0);
@@ -839,6 +894,7 @@ void CoarseSpace::setup(const SellView& A, const VT* aval, const double* disp, c
         MPHY_CUDA(cudaFuncSetAttribute(trtri_finalize, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
         MPHY_CUDA(cudaFuncSetAttribute(trtri_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
         MPHY_CUDA(cudaFuncSetAttribute(inverse_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
+        MPHY_CUDA(cudaFuncSetAttribute(potrf_inv_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
     }
     // The dense part (null modes, blocked Cholesky with tile inverses, triangular inverse,
     // E^{-1} = W^T W) is the same launch sequence on the same buffers every time: it is captured
@@ -948,7 +1004,7 @@ void CoarseSpace::record_factorisation(cudaStream_t s, int nb, size_t sm2) {
     bool rest_pending = false;
     for (int j = 0; j < nb; ++j) {
         const int m = std::min(nb - j - 1, band_tiles_);  // tiles below (j, j) inside E's band
-        potrf_inv_tile<<<1, kPotrfThreads, 0, s>>>(E_.p, W_.p, kp_, j, err_.p);
+        potrf_inv_tile<<<1, kPotrfThreads, sm2, s>>>(E_.p, W_.p, kp_, j, err_.p);
         launches += 1;
         if (m > 0) {
             gemm_panel_tiles<<<m, 256, sm2, s>>>(E_.p, W_.p, kp_, j);
