@@ -413,19 +413,17 @@ __device__ __forceinline__ void load_tile(double (*S)[TP], const double* M, int 
 // W_jj = L_jj^{-1} to W: the panel below becomes a tile product with W_jj (gemm_panel_tiles) and
 // the triangular inverse reuses W_jj. The tile's lower triangle is cut into 4x4 patches, one per
 // thread (136 patches), held in registers for the whole kernel with every patch index known at
-// compile time; a step exchanges only one column (or row) through shared memory, double-buffered,
-// so each step costs one barrier.
-//   Cholesky, step c: the owners of column c publish it (unscaled; final after step c - 1);
-//   every thread computes rd[c] = 1 / sqrt(A(c,c)), subtracts A(i,c) A(k,c) rd[c]^2 from its
-//   entries (i, k) with c < k <= i, and the owners scale their column c by rd[c], giving L.
+// compile time.
+//   Cholesky: right-looking over the 16 patch columns (blocked by 4), two barriers per step.
 //   Inverse: L and the patches' inverses go to shared memory (dynamic, two padded tiles), and
 //   X = L^{-1} is formed by recursive doubling (four levels, below).
 constexpr int kPotrfPatches = (T / 4) * (T / 4 + 1) / 2;  // 136
 constexpr int kPotrfThreads = 160;                          // five warps, the last 24 threads idle
 
 __global__ void __launch_bounds__(kPotrfThreads) potrf_inv_tile(double* E, double* W, int kp, int j, int32_t* err) {
-    __shared__ double colv[2][T];  // Cholesky: column c
-    __shared__ double rd[T];       // 1 / L(c, c)
+    __shared__ double pinv[4][4];      // inverse of the current step's diagonal patch
+    __shared__ double panel[2][T][4];  // the current step's L_Pc, double-buffered
+    __shared__ double rd[T];           // 1 / L(c, c)
     const int tid = threadIdx.x;
     const bool owner = tid < kPotrfPatches;
     // patch (P, Q), Q <= P, from the row-major triangular index
@@ -448,44 +446,82 @@ __global__ void __launch_bounds__(kPotrfThreads) potrf_inv_tile(double* E, doubl
             A[a][3] = v1.y;
         }
     }
-    // ---- Cholesky: column c = 4 cq + kk, kk known at compile time
+    // ---- Cholesky, right-looking in steps of one patch column cq (16 steps, two barriers each):
+    // the owner of the diagonal patch factors it in registers and publishes its inverse; the
+    // owners of the patches below form L_Pc = A_Pc L_cc^{-T} and publish them; every patch
+    // (P, Q) with P >= Q > cq subtracts L_Pc L_Qc^T
     for (int cq = 0; cq < T / 4; ++cq) {
+        const int buf = cq & 1;
+        if (P == cq && Q == cq) {
 #pragma unroll
-        for (int kk = 0; kk < 4; ++kk) {
-            const int c = 4 * cq + kk, buf = c & 1;
-            if (Q == cq) {
-#pragma unroll
-                for (int a = 0; a < 4; ++a)
-                    if (r0 + a >= c) colv[buf][r0 + a] = A[a][kk];
-            }
-            __syncthreads();
-            double p = colv[buf][c];
-            if (!(p > 0.0)) {
-                if (tid == 0) atomicExch(err, 2);
-                p = 1e-300;
-            }
-            const double il = rsqrt(p);
-            const double f = il * il;
-            if (tid == 0) rd[c] = il;
-            if (owner && P >= cq) {
-                // rows <= c and columns <= c take a zero factor, so the 16 updates need no
-                // predicates (the strictly upper entries of a diagonal patch change too; they are
-                // never read and never written out)
-                double ci[4], cf[4];
-#pragma unroll
-                for (int a = 0; a < 4; ++a) ci[a] = r0 + a > c ? colv[buf][r0 + a] : 0.0;
-#pragma unroll
-                for (int b = 0; b < 4; ++b) cf[b] = c0 + b > c ? colv[buf][c0 + b] * f : 0.0;
+            for (int kk = 0; kk < 4; ++kk) {
+                double p = A[kk][kk];
+                if (!(p > 0.0)) {
+                    atomicExch(err, 2);
+                    p = 1e-300;
+                }
+                const double il = rsqrt(p);
+                rd[4 * cq + kk] = il;
 #pragma unroll
                 for (int a = 0; a < 4; ++a)
+                    if (a >= kk) A[a][kk] *= il;
 #pragma unroll
-                    for (int b = 0; b < 4; ++b) A[a][b] = fma(-ci[a], cf[b], A[a][b]);
-                if (Q == cq) {
+                for (int bb = 0; bb < 4; ++bb)
 #pragma unroll
                     for (int a = 0; a < 4; ++a)
-                        if (r0 + a >= c) A[a][kk] *= il;
+                        if (bb > kk && a >= bb) A[a][bb] = fma(-A[a][kk], A[bb][kk], A[a][bb]);
+            }
+            // the patch's inverse (forward substitution, 1 / L(i,i) = rd)
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                const double di = rd[4 * cq + a];
+#pragma unroll
+                for (int bb = 0; bb < 4; ++bb) {
+                    double t = 0.0;
+#pragma unroll
+                    for (int k = 0; k < 4; ++k)
+                        if (k >= bb && k < a) t = fma(A[a][k], pinv[k][bb], t);
+                    pinv[a][bb] = bb < a ? -di * t : (bb == a ? di : 0.0);
                 }
             }
+        }
+        __syncthreads();
+        if (owner && Q == cq && P > cq) {
+            double l[4][4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int bb = 0; bb < 4; ++bb) {
+                    double t = 0.0;
+#pragma unroll
+                    for (int k = 0; k < 4; ++k)
+                        if (k <= bb) t = fma(A[a][k], pinv[bb][k], t);  // (L_cc^{-T})[k][bb]
+                    l[a][bb] = t;
+                }
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int bb = 0; bb < 4; ++bb) {
+                    A[a][bb] = l[a][bb];
+                    panel[buf][r0 + a][bb] = l[a][bb];
+                }
+        }
+        __syncthreads();
+        if (owner && Q > cq) {
+            double lp[4][4], lq[4][4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    lp[a][k] = panel[buf][r0 + a][k];
+                    lq[a][k] = panel[buf][c0 + a][k];
+                }
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int bb = 0; bb < 4; ++bb)
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) A[a][bb] = fma(-lp[a][k], lq[bb][k], A[a][bb]);
         }
     }
     // ---- inverse X = L^{-1} by recursive doubling over the 4x4 patches: the diagonal patches
