@@ -865,7 +865,6 @@ void CoarseSpace::init(mphy_ctx* ctx, const mphy_mesh* mesh, const mphy_pattern*
     const size_t tiles = (size_t)nb * (nb + 1) / 2;
     einv_.alloc(tiles * T * T);
     gpart_.alloc(tiles * 2 * T);
-    gcount_.alloc(nb + 1);
     tilewc_.alloc(tiles);
     w_.alloc(kp_);
     c_.alloc(kp_);
@@ -875,7 +874,6 @@ void CoarseSpace::init(mphy_ctx* ctx, const mphy_mesh* mesh, const mphy_pattern*
     MPHY_CUDA(cudaMemsetAsync(w_.p, 0, w_.bytes(), s));
     MPHY_CUDA(cudaMemsetAsync(c_.p, 0, c_.bytes(), s));
     MPHY_CUDA(cudaMemsetAsync(wcount_.p, 0, wcount_.bytes(), s));
-    MPHY_CUDA(cudaMemsetAsync(gcount_.p, 0, gcount_.bytes(), s));
     MPHY_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -1105,7 +1103,6 @@ CoarseView CoarseSpace::view() const {
     v.einv = einv_.p;
     v.nb = kp_ / T;
     v.gpart = gpart_.p;
-    v.gcount = gcount_.p;
     v.tilewc = tilewc_.p;
     v.w = w_.p;
     v.wpart = wpart_.p;

@@ -58,7 +58,6 @@ class CoarseSpace {
     DevBuf<double> cent_, E_, W_, w_, c_;
     DevBuf<double> einv_;     // lower tiles of E^{-1}
     DevBuf<double> gpart_, tilewc_;
-    DevBuf<uint32_t> gcount_;
     DevBuf<uint8_t> drop_;
     DevBuf<double> wpart_;
     DevBuf<uint32_t> wcount_;

@@ -30,7 +30,6 @@ struct CoarseView {
     uint32_t* wcount;        // [n_agg] parts summed so far (zero between launches)
     double* c;               // [kp] coarse correction E^{-1} w
     double* gpart;           // [tiles][2][64] the GEMV's per-tile products (E_IJ w_J, E_IJ^T w_I)
-    uint32_t* gcount;        // [nb + 1] GEMV tickets: tiles done per tile row, tiles done (zero between launches)
     double* tilewc;          // [tiles] each tile's share of w^T E^{-1} w
 };
 

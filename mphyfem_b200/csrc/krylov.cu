@@ -703,13 +703,12 @@ void launch_restrict(const CoarseView& cv, const XT* r, const PcgState* st, cuda
 // streams one 512-byte tile row per load). It forms E_IJ w_J (rows of I) and, off the diagonal,
 // E_IJ^T w_I (rows of J): per-thread partials summed across the half warp, and across warps in
 // warp order. Both go to the tile's slots of gpart. Every tile row X is touched by nb tiles;
-// the CTA that completes X's ticket sums X's slots in tile order (J ascending) into c_X, so c
-// does not depend on which CTA ran which tile (four threads per entry take a quarter of the
-// slots each, added in order).
+// the second kernel (coarse_gemv_finish_kernel) sums X's slots in tile order (J ascending) into
+// c_X, so c does not depend on which CTA ran which tile.
 // FIN (two-level iteration with the ||r|| test): every tile also stores its share of
-// (w, c) = w^T E^{-1} w, w_I^T E_IJ w_J (twice that off the diagonal, for the mirrored tile); the
-// last tile CTA to arrive adds the shares in tile order and ends the iteration:
-// (r, z) = (r, D^-1 r) + (w, c), ||r||^2 from the update. This needs no wait for the rows.
+// (w, c) = w^T E^{-1} w, w_I^T E_IJ w_J (twice that off the diagonal, for the mirrored tile),
+// which the second kernel adds in tile order to end the iteration. The kernel boundary replaces
+// the fences and tickets a single kernel would need.
 __device__ __forceinline__ int64_t lower_tile(int i, int j) { return (int64_t)i * (i + 1) / 2 + j; }
 
 template <bool FIN>
@@ -717,8 +716,6 @@ __global__ void __launch_bounds__(256) coarse_gemv_kernel(CoarseView cv, PcgStat
     __shared__ double wI[64], wJ[64];
     __shared__ double colp[8][64];  // column partials per warp; the finisher's quarter sums
     __shared__ double red[8];
-    __shared__ int finish[2];
-    __shared__ bool last_tile;
     if (st && st->done) return;
     const int t = blockIdx.x;
     int I = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
@@ -794,56 +791,46 @@ __global__ void __launch_bounds__(256) coarse_gemv_kernel(CoarseView cv, PcgStat
             gp[64 + tid] = x;
         }
     }
-    __threadfence();
-    __syncthreads();
-    const uint32_t ntiles = (uint32_t)((int64_t)cv.nb * (cv.nb + 1) / 2);
-    if (tid == 0) {
-        finish[0] = atomicAdd(cv.gcount + I, 1u) == (uint32_t)cv.nb - 1 ? I : -1;
-        finish[1] = I != J && atomicAdd(cv.gcount + J, 1u) == (uint32_t)cv.nb - 1 ? J : -1;
-        last_tile = FIN && atomicAdd(cv.gcount + cv.nb, 1u) == ntiles - 1;
-    }
-    __syncthreads();
-    if (FIN && last_tile) {
-        // every tile's share has arrived: a contiguous run of shares per thread, the threads in
-        // order (block_sum), then the end of the iteration
+}
+
+// The GEMV's second kernel (the kernel boundary orders it after every tile): CTA X < nb sums
+// tile row X's slots in tile order into c_X (four groups of 64 threads each take a quarter of
+// the nb slots, added in order); FIN: CTA nb adds the tiles' shares of w^T E^{-1} w in tile
+// order and ends the iteration: (r, z) = (r, D^-1 r) + (w, c), ||r||^2 from the update.
+template <bool FIN>
+__global__ void __launch_bounds__(256) coarse_gemv_finish_kernel(CoarseView cv, PcgState* st) {
+    __shared__ double part[4][64];
+    __shared__ double sh[32];
+    if (st && st->done) return;
+    const int tid = threadIdx.x;
+    const int X = blockIdx.x;
+    if (X == cv.nb) {
+        const uint32_t ntiles = (uint32_t)((int64_t)cv.nb * (cv.nb + 1) / 2);
         const uint32_t per = (ntiles + blockDim.x - 1) / blockDim.x;
         const uint32_t k0 = tid * per, k1 = min(ntiles, k0 + per);
         double x = 0.0;
-        for (uint32_t k = k0; k < k1; ++k) x += __ldcg(cv.tilewc + k);
-        x = block_sum(x, colp[0]);
-        if (tid == 0) {
-            cv.gcount[cv.nb] = 0;
-            finish_iter(st, st->rdr + x, st->rr);
-        }
-        __syncthreads();  // colp is reused by the row sums below
+        for (uint32_t k = k0; k < k1; ++k) x += cv.tilewc[k];
+        x = block_sum(x, sh);
+        if (tid == 0) finish_iter(st, st->rdr + x, st->rr);
+        return;
     }
-    for (int f = 0; f < 2; ++f) {
-        const int X = finish[f];
-        if (X < 0) continue;
-        // four groups of 64 threads each sum a quarter of the row's nb slots in tile order;
-        // the quarters are then added in order
-        {
-            const int g = tid >> 6, i = tid & 63;
-            const int per = (cv.nb + 3) >> 2, k0 = g * per, k1 = min(cv.nb, k0 + per);
-            double x = 0.0;
+    const int g = tid >> 6, i = tid & 63;
+    const int per = (cv.nb + 3) >> 2, k0 = g * per, k1 = min(cv.nb, k0 + per);
+    double x = 0.0;
 #pragma unroll 4
-            for (int K = k0; K < k1; ++K)
-                x += K <= X ? __ldcg(cv.gpart + lower_tile(X, K) * 128 + i)
-                            : __ldcg(cv.gpart + lower_tile(K, X) * 128 + 64 + i);
-            __syncthreads();  // colp is free (its last reads were before the ticket)
-            colp[g][i] = x;
-            __syncthreads();
-        }
-        if (tid < 64) cv.c[64 * X + tid] = (colp[0][tid] + colp[1][tid]) + (colp[2][tid] + colp[3][tid]);
-        if (tid == 0) cv.gcount[X] = 0;  // every tile of row X has arrived
-        __syncthreads();
-    }
+    for (int K = k0; K < k1; ++K)
+        x += K <= X ? cv.gpart[lower_tile(X, K) * 128 + i] : cv.gpart[lower_tile(K, X) * 128 + 64 + i];
+    part[g][i] = x;
+    __syncthreads();
+    if (tid < 64) cv.c[64 * X + tid] = (part[0][tid] + part[1][tid]) + (part[2][tid] + part[3][tid]);
 }
 
-// the coarse GEMV: one CTA per stored tile of E^{-1}
+// the coarse GEMV: one CTA per stored tile of E^{-1}, then one per tile row (and FIN: one for
+// the end of the iteration)
 template <bool FIN>
 void launch_gemv(const CoarseView& cv, PcgState* st, cudaStream_t s) {
     coarse_gemv_kernel<FIN><<<(unsigned)((int64_t)cv.nb * (cv.nb + 1) / 2), 256, 0, s>>>(cv, st);
+    coarse_gemv_finish_kernel<FIN><<<(unsigned)(cv.nb + (FIN ? 1 : 0)), 256, 0, s>>>(cv, st);
 }
 
 // z = D^{-1} r + Z c with the fused (r, z), (z, z); INIT also sets p = z and the initial state
@@ -1405,7 +1392,7 @@ int Pcg<VT, XT>::solve(const VT* val, const XT* b, XT* x, double rtol, double ab
         coarse_final_kernel<XT, true><<<resident_grid((const void*)coarse_final_kernel<XT, true>, A_.n_node, kThreads, sm_), kThreads, 0, s>>>(
             A_.n_node, coarse_, r_.p, z_.p, p_.p, dinv32_.p, partials_.p, partials2_.p, st_.p, rtol, abstol, dtol,
             maxit, norm_type);
-        launches += 5;
+        launches += 6;
     } else {
         pcg_init_kernel<XT, false><<<gv, kThreads, 0, s>>>(n_, b, x, r_.p, z_.p, p_.p, nullptr, nullptr, nullptr,
                                                             st_.p, rtol, abstol, dtol, maxit, norm_type);
@@ -1414,7 +1401,7 @@ int Pcg<VT, XT>::solve(const VT* val, const XT* b, XT* x, double rtol, double ab
         if (kind_ == PcKind::FactorCoarse) {
             launch_restrict<XT>(coarse_, r_.p, nullptr, s, sm_);
             launch_gemv<false>(coarse_, nullptr, s);
-            launches += 2;
+            launches += 3;
         }
         factor_apply_kernel<XT, true><<<gg, kThreads, 0, s>>>(factor_.GT, kind_ == PcKind::FactorCoarse ? coarse_ : CoarseView{},
                                                                factor_.gtval, t_.p, z_.p, r_.p, p_.p,
@@ -1443,8 +1430,8 @@ int Pcg<VT, XT>::solve(const VT* val, const XT* b, XT* x, double rtol, double ab
     }
     const int per_iter = kind_ == PcKind::Jacobi ? 3
                          : kind_ == PcKind::Factor ? 5
-                         : kind_ == PcKind::FactorCoarse ? 7
-                         : norm_type == 1 ? 5 : 6;
+                         : kind_ == PcKind::FactorCoarse ? 8
+                         : norm_type == 1 ? 6 : 7;
     PcgState h{};
     // every replay advances at most chunk_ iterations; the device stops at maxit
     const int64_t max_replays = (int64_t)(maxit > 0 ? maxit : 0) / chunk_ + 2;
