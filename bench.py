@@ -53,11 +53,11 @@ def _workload(name: str):
 
 
 def _auto_coarse(n_node: int) -> int:
-    """Default size of the coarse space: about one aggregate per 2,100 nodes (20 x 5 x 5 boxes on
-    the 256 x 64 x 64 hex8 cantilever, 24 x 6 x 6 on the 96 x 48 x 48 tet10 block). Larger spaces
-    cut iterations but every CG iteration's GEMV reads the whole E^-1; measured sweeps on both
-    workloads put the optimum near this density."""
-    return max(8, int(round(n_node / 2100)))
+    """Default size of the coarse space: about one aggregate per 1,300 nodes (24 x 6 x 6 boxes on
+    the 256 x 64 x 64 hex8 cantilever, 28 x 7 x 7 on the 96 x 48 x 48 tet10 block). Larger spaces
+    cut iterations but every CG iteration's GEMV reads the whole E^-1 and the dense setup grows
+    with its tile count; measured sweeps on both workloads put the optimum near this density."""
+    return max(8, int(round(n_node / 1300)))
 
 
 def _config(prob, rtol):
@@ -667,8 +667,8 @@ def main():
                     help="Krylov stopping norm: 1 = true residual ||b - Ax|| <= rtol ||b|| (every method compared "
                          "at the same accuracy), 0 = PETSc's preconditioned-residual default")
     ap.add_argument("--coarse", type=int, default=-1,
-                    help="aggregates of the two-level coarse correction (0: off; -1: about one per 2,100 nodes, "
-                         "which gives the 20 x 5 x 5 grid at the headline size)")
+                    help="aggregates of the two-level coarse correction (0: off; -1: about one per 1,300 nodes, "
+                         "which gives the 24 x 6 x 6 grid at the headline size)")
     ap.add_argument("--coarse-modes", dest="coarse_modes", type=int, default=6, choices=[6, 12],
                     help="modes per aggregate: 6 rigid-body, 12 linear displacement")
     ap.add_argument("--no-plain", dest="no_plain", action="store_true",
