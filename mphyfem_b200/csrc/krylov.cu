@@ -794,12 +794,14 @@ __global__ void __launch_bounds__(256) coarse_gemv_kernel(CoarseView cv, PcgStat
 }
 
 // The GEMV's second kernel (the kernel boundary orders it after every tile): CTA X < nb sums
-// tile row X's slots in tile order into c_X (four groups of 64 threads each take a quarter of
-// the nb slots, added in order); FIN: CTA nb adds the tiles' shares of w^T E^{-1} w in tile
-// order and ends the iteration: (r, z) = (r, D^-1 r) + (w, c), ||r||^2 from the update.
+// tile row X's slots in tile order into c_X (kFinishGroups groups of 64 threads each take a
+// contiguous share of the nb slots, added in order, so each thread waits for only a few loads);
+// FIN: CTA nb adds the tiles' shares of w^T E^{-1} w in tile order and ends the iteration:
+// (r, z) = (r, D^-1 r) + (w, c), ||r||^2 from the update.
+constexpr int kFinishGroups = 16;
 template <bool FIN>
-__global__ void __launch_bounds__(256) coarse_gemv_finish_kernel(CoarseView cv, PcgState* st) {
-    __shared__ double part[4][64];
+__global__ void __launch_bounds__(64 * kFinishGroups) coarse_gemv_finish_kernel(CoarseView cv, PcgState* st) {
+    __shared__ double part[kFinishGroups][64];
     __shared__ double sh[32];
     if (st && st->done) return;
     const int tid = threadIdx.x;
@@ -815,14 +817,19 @@ __global__ void __launch_bounds__(256) coarse_gemv_finish_kernel(CoarseView cv, 
         return;
     }
     const int g = tid >> 6, i = tid & 63;
-    const int per = (cv.nb + 3) >> 2, k0 = g * per, k1 = min(cv.nb, k0 + per);
+    const int per = (cv.nb + kFinishGroups - 1) / kFinishGroups, k0 = g * per, k1 = min(cv.nb, k0 + per);
     double x = 0.0;
 #pragma unroll 4
     for (int K = k0; K < k1; ++K)
         x += K <= X ? cv.gpart[lower_tile(X, K) * 128 + i] : cv.gpart[lower_tile(K, X) * 128 + 64 + i];
     part[g][i] = x;
     __syncthreads();
-    if (tid < 64) cv.c[64 * X + tid] = (part[0][tid] + part[1][tid]) + (part[2][tid] + part[3][tid]);
+    if (tid < 64) {
+        double c = 0.0;
+#pragma unroll
+        for (int q = 0; q < kFinishGroups; ++q) c += part[q][tid];
+        cv.c[64 * X + tid] = c;
+    }
 }
 
 // the coarse GEMV: one CTA per stored tile of E^{-1}, then one per tile row (and FIN: one for
@@ -830,7 +837,7 @@ __global__ void __launch_bounds__(256) coarse_gemv_finish_kernel(CoarseView cv, 
 template <bool FIN>
 void launch_gemv(const CoarseView& cv, PcgState* st, cudaStream_t s) {
     coarse_gemv_kernel<FIN><<<(unsigned)((int64_t)cv.nb * (cv.nb + 1) / 2), 256, 0, s>>>(cv, st);
-    coarse_gemv_finish_kernel<FIN><<<(unsigned)(cv.nb + (FIN ? 1 : 0)), 256, 0, s>>>(cv, st);
+    coarse_gemv_finish_kernel<FIN><<<(unsigned)(cv.nb + (FIN ? 1 : 0)), 64 * kFinishGroups, 0, s>>>(cv, st);
 }
 
 // z = D^{-1} r + Z c with the fused (r, z), (z, z); INIT also sets p = z and the initial state
