@@ -601,12 +601,13 @@ __device__ __forceinline__ void restrict_node(bool lin, const double rr[3], cons
 // depend on which CTA ran which part. The CTAs walk the items in a grid-stride loop. NM (modes per
 // aggregate) is a template parameter, so the rigid-body form keeps six accumulators and fits
 // four CTAs per SM.
-constexpr int kRestrictNodes = 2;  // nodes per thread and step, all loads issued first
+constexpr int kRestrictNodes = 2;     // nodes per thread and step, all loads issued first
+constexpr int kRestrictThreads = 128;  // small CTAs: about one aggregate each at the default coarse size
 template <typename XT, int NM>
-__global__ void __launch_bounds__(kThreads, NM == 6 ? 4 : 3) coarse_restrict_kernel(CoarseView cv, int parts,
+__global__ void __launch_bounds__(kRestrictThreads, NM == 6 ? 8 : 6) coarse_restrict_kernel(CoarseView cv, int parts,
                                                                                    const XT* __restrict__ r,
                                                                                    const PcgState* st) {
-    __shared__ double sh[kThreads / 32][NM];
+    __shared__ double sh[kRestrictThreads / 32][NM];
     __shared__ bool last;
     if (st && st->done) return;
     constexpr bool lin = NM == 12;
@@ -659,7 +660,7 @@ __global__ void __launch_bounds__(kThreads, NM == 6 ? 4 : 3) coarse_restrict_ker
         __syncthreads();
         double t = 0.0;
         if (threadIdx.x < nm)
-            for (int k = 0; k < kThreads / 32; ++k) t += sh[k][threadIdx.x];
+            for (int k = 0; k < kRestrictThreads / 32; ++k) t += sh[k][threadIdx.x];
         if (parts == 1) {
             if (threadIdx.x < nm) cv.w[nm * a + threadIdx.x] = t;
             continue;
@@ -686,11 +687,11 @@ __global__ void __launch_bounds__(kThreads, NM == 6 ? 4 : 3) coarse_restrict_ker
 // and ticket once.
 template <typename XT, int NM>
 void launch_restrict_nm(const CoarseView& cv, const XT* r, const PcgState* st, cudaStream_t s, int sm) {
-    const unsigned grid = resident_grid((const void*)coarse_restrict_kernel<XT, NM>, (int64_t)1 << 40, kThreads, sm);
+    const unsigned grid = resident_grid((const void*)coarse_restrict_kernel<XT, NM>, (int64_t)1 << 40, kRestrictThreads, sm);
     int parts = (int)((int64_t)grid / cv.n_agg);
     parts = std::max(1, std::min(parts, kMaxRestrictParts));
     const unsigned g = (unsigned)std::min<int64_t>(grid, (int64_t)cv.n_agg * parts);
-    coarse_restrict_kernel<XT, NM><<<g, kThreads, 0, s>>>(cv, parts, r, st);
+    coarse_restrict_kernel<XT, NM><<<g, kRestrictThreads, 0, s>>>(cv, parts, r, st);
 }
 template <typename XT>
 void launch_restrict(const CoarseView& cv, const XT* r, const PcgState* st, cudaStream_t s, int sm) {
