@@ -8,10 +8,11 @@
 //      (aggregate, neighbour) adds the entries in a fixed order -- no atomics, so E is bitwise
 //      the same on every run;
 //   3. E = L L^T by a right-looking blocked Cholesky (64x64 tiles, FP64), W = L^{-1} by blocked
-//      forward substitution, E^{-1} = W^T W, kept in FP64 for the per-iteration GEMV (FP32
-//      rounding of the inverse of an ill-conditioned E can make it indefinite). The aggregates
-//      are numbered with the longest box axis slowest, so E is banded; L stays inside the band
-//      and the Cholesky and forward-substitution steps touch only the tiles inside it.
+//      forward substitution, then W rounded to FP32 for the per-iteration E^{-1} w = W~^T (W~ w)
+//      (W~^T W~ is symmetric positive definite whatever the rounding, where an FP32 copy of E^{-1}
+//      itself can be indefinite when E is ill-conditioned). The aggregates are numbered with the
+//      longest box axis slowest, so E is banded; L stays inside the band and the Cholesky and
+//      forward-substitution steps touch only the tiles inside it.
 #include <algorithm>
 #include <array>
 #include <cmath>
@@ -740,33 +741,17 @@ __global__ void __launch_bounds__(256) trtri_update(const double* E, double* W, 
         for (int r = 0; r < 4; ++r) W[(int64_t)(i * T + ty + 16 * q) * kp + j * T + tx + 16 * r] += acc[q][r];
 }
 
-// E^{-1} = W^T W, its lower tiles only (symmetric): tile (i, j), j <= i, is
-// sum_{k >= i} W_ki^T W_kj, stored FP64 at tile index i (i + 1) / 2 + j. A diagonal tile comes out
-// bitwise symmetric (entry (r, c) and (c, r) sum the same products in the same order).
-__global__ void __launch_bounds__(256) inverse_tiles(const double* W, double* einv, int kp, int nb) {
-    extern __shared__ double sm[];
-    double (*A)[TP] = reinterpret_cast<double (*)[TP]>(sm);
-    double (*B)[TP] = reinterpret_cast<double (*)[TP]>(sm + T * TP);
+// The lower tiles of W = L^{-1} rounded to FP32, packed (tile (i, j), j <= i, row-major at
+// tile index i (i + 1) / 2 + j) for the per-iteration W~^T (W~ w)
+__global__ void __launch_bounds__(256) pack_w32_tiles(const double* __restrict__ W, float* __restrict__ w32, int kp) {
     const int t = blockIdx.x;
     int i = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
     while (i * (i + 1) / 2 > t) --i;  // the float root, made exact
     while ((i + 1) * (i + 2) / 2 <= t) ++i;
     const int j = t - i * (i + 1) / 2;
-    const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;
-    double acc[4][4] = {{0}};
-    for (int k = max(i, j); k < nb; ++k) {
-        // A = W_ki^T, B = W_kj^T: tile_abt gives sum_t W_ki[t][r] W_kj[t][c]
-        for (int t = threadIdx.x; t < T * T; t += blockDim.x) {
-            A[t % T][t / T] = W[(int64_t)(k * T + t / T) * kp + i * T + t % T];
-            B[t % T][t / T] = W[(int64_t)(k * T + t / T) * kp + j * T + t % T];
-        }
-        __syncthreads();
-        tile_abt(A, B, acc);
-        __syncthreads();
-    }
-    double* o = einv + (int64_t)t * T * T;
-    for (int q = 0; q < 4; ++q)
-        for (int r = 0; r < 4; ++r) o[(ty + 16 * q) * T + tx + 16 * r] = acc[q][r];
+    float* o = w32 + (int64_t)t * T * T;
+    for (int q = threadIdx.x; q < T * T; q += blockDim.x)
+        o[q] = (float)W[(int64_t)(i * T + q / T) * kp + j * T + q % T];
 }
 
 }  // namespace
@@ -863,9 +848,10 @@ void CoarseSpace::init(mphy_ctx* ctx, const mphy_mesh* mesh, const mphy_pattern*
     W_.alloc((size_t)kp_ * kp_);
     const int nb = kp_ / T;
     const size_t tiles = (size_t)nb * (nb + 1) / 2;
-    einv_.alloc(tiles * T * T);
+    w32_.alloc(tiles * T * T);
+    y_.alloc(kp_);
     gpart_.alloc(tiles * 2 * T);
-    tilewc_.alloc(tiles);
+    rowyy_.alloc(nb);
     w_.alloc(kp_);
     c_.alloc(kp_);
     wpart_.alloc((size_t)n_agg_ * kMaxRestrictParts * nm_);
@@ -927,11 +913,10 @@ void CoarseSpace::setup(const SellView& A, const VT* aval, const double* disp, c
         MPHY_CUDA(cudaFuncSetAttribute(gemm_panel_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
         MPHY_CUDA(cudaFuncSetAttribute(trtri_finalize, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
         MPHY_CUDA(cudaFuncSetAttribute(trtri_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
-        MPHY_CUDA(cudaFuncSetAttribute(inverse_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
         MPHY_CUDA(cudaFuncSetAttribute(potrf_inv_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
     }
     // The dense part (null modes, blocked Cholesky with tile inverses, triangular inverse,
-    // E^{-1} = W^T W) is the same launch sequence on the same buffers every time: it is captured
+    // W in FP32) is the same launch sequence on the same buffers every time: it is captured
     // once into a CUDA graph and replayed, so the short dependent launches run back to back.
     if (fact_graph_) {
         MPHY_CUDA(cudaGraphLaunch(fact_graph_, s));
@@ -1066,12 +1051,12 @@ void CoarseSpace::record_factorisation(cudaStream_t s, int nb, size_t sm2) {
             if (rest_pending) MPHY_CUDA(cudaEventRecord(ev_rest, s_rest));
         }
     }
-    // join both side streams before E^{-1} = W^T W
+    // join both side streams before W is rounded to FP32
     MPHY_CUDA(cudaEventRecord(ev_rest, s_rest));
     MPHY_CUDA(cudaStreamWaitEvent(s, ev_rest, 0));
     MPHY_CUDA(cudaEventRecord(ev_tri, s_tri));
     MPHY_CUDA(cudaStreamWaitEvent(s, ev_tri, 0));
-    inverse_tiles<<<nb * (nb + 1) / 2, 256, sm2, s>>>(W_.p, einv_.p, kp_, nb);
+    pack_w32_tiles<<<nb * (nb + 1) / 2, 256, 0, s>>>(W_.p, w32_.p, kp_);
     launches += 1;
     MPHY_CUDA(cudaGetLastError());
 }
@@ -1100,10 +1085,11 @@ CoarseView CoarseSpace::view() const {
     v.fixed = mesh_->fixed.p;
     v.dperm = dperm_.p;
     v.fperm = fperm_.p;
-    v.einv = einv_.p;
+    v.w32 = w32_.p;
+    v.y = y_.p;
     v.nb = kp_ / T;
     v.gpart = gpart_.p;
-    v.tilewc = tilewc_.p;
+    v.rowyy = rowyy_.p;
     v.w = w_.p;
     v.wpart = wpart_.p;
     v.wcount = wcount_.p;

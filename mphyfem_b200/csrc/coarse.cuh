@@ -56,8 +56,8 @@ class CoarseSpace {
     DevBuf<int64_t> agg_ptr_;
     DevBuf<float> d_;       // FP32 offsets (x_n - c_a) / H
     DevBuf<double> cent_, E_, W_, w_, c_;
-    DevBuf<double> einv_;     // lower tiles of E^{-1}
-    DevBuf<double> gpart_, tilewc_;
+    DevBuf<float> w32_;       // lower tiles of W = L^{-1}, FP32
+    DevBuf<double> y_, gpart_, rowyy_;
     DevBuf<uint8_t> drop_;
     DevBuf<double> wpart_;
     DevBuf<uint32_t> wcount_;

@@ -20,17 +20,20 @@ struct CoarseView {
     const float* dperm;      // [n_node][3] d in the order of agg_nodes (the restriction's loads)
     const uint8_t* fperm;    // [3 n_node] fixed in the order of agg_nodes
     int32_t nb;              // kp / 64 tiles per side
-    // inverse of E, FP64, symmetric: its lower 64x64 tiles (I, J), J <= I, at tile index
-    // I (I + 1) / 2 + J, each row-major. FP64: with a large stiffness contrast E is so
-    // ill-conditioned that rounding its inverse to FP32 makes the coarse term indefinite, and CG
-    // on an indefinite preconditioner stalls
-    const double* einv;
+    // E^{-1} = W^T W with W = L^{-1} (E = L L^T), applied as W~^T (W~ w) with W~ the FP32
+    // rounding of W: its lower 64x64 tiles (I, J), J <= I, at tile index I (I + 1) / 2 + J,
+    // each row-major. W~^T W~ is symmetric positive definite whatever the rounding (W~ stays
+    // nonsingular), so the coarse term keeps CG's guarantees even when E is ill-conditioned;
+    // the rounding only perturbs it by about 2^-24 times the condition number of W, the square
+    // root of E's
+    const float* w32;
     double* w;               // [kp] restriction Z^T r
     double* wpart;           // [n_agg][kMaxRestrictParts][nm] partial restriction sums
     uint32_t* wcount;        // [n_agg] parts summed so far (zero between launches)
     double* c;               // [kp] coarse correction E^{-1} w
-    double* gpart;           // [tiles][2][64] the GEMV's per-tile products (E_IJ w_J, E_IJ^T w_I)
-    double* tilewc;          // [tiles] each tile's share of w^T E^{-1} w
+    double* y;               // [kp] W~ w
+    double* gpart;           // [tiles][2][64] the per-tile products W_IJ w_J and W_IJ^T y_I
+    double* rowyy;           // [nb] each tile row's share of y^T y = w^T E^{-1} w
 };
 
 #ifdef __CUDACC__

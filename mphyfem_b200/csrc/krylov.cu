@@ -699,24 +699,22 @@ void launch_restrict(const CoarseView& cv, const XT* r, const PcgState* st, cuda
     else launch_restrict_nm<XT, 6>(cv, r, st, s, sm);
 }
 
-// c = E^{-1} w with the symmetric FP64 inverse stored as its lower 64x64 tiles. One CTA per
-// stored tile (I, J) reads it once: a 16 x 16 thread grid, each thread a 4 x 4 patch (a half warp
-// streams one 512-byte tile row per load). It forms E_IJ w_J (rows of I) and, off the diagonal,
-// E_IJ^T w_I (rows of J): per-thread partials summed across the half warp, and across warps in
-// warp order. Both go to the tile's slots of gpart. Every tile row X is touched by nb tiles;
-// the second kernel (coarse_gemv_finish_kernel) sums X's slots in tile order (J ascending) into
-// c_X, so c does not depend on which CTA ran which tile.
-// FIN (two-level iteration with the ||r|| test): every tile also stores its share of
-// (w, c) = w^T E^{-1} w, w_I^T E_IJ w_J (twice that off the diagonal, for the mirrored tile),
-// which the second kernel adds in tile order to end the iteration. The kernel boundary replaces
-// the fences and tickets a single kernel would need.
+// c = E^{-1} w = W~^T (W~ w), W~ the FP32 lower tiles of W = L^{-1} (coarse_view.cuh), in two
+// passes of two kernels each. A tile kernel has one CTA per stored tile (I, J), J <= I, reading
+// it once (a 16 x 16 thread grid, each thread a 4 x 4 patch: one 16-byte load per patch row);
+// it writes its 64 partial sums to the tile's slot of gpart: pass 1 W_IJ w_J (rows of I, summed
+// across the half warp), pass 2 W_IJ^T y_I (rows of J, summed across the warps in warp order).
+// A row kernel then adds each tile row's slots in tile order, so y and c do not depend on which
+// CTA ran which tile: pass 1 y_X = sum_{J <= X}, with the row's share of y^T y; pass 2
+// c_X = sum_{I >= X}. FIN (two-level iteration with the ||r|| test): the second row kernel has
+// one more CTA, which adds the rows' shares of y^T y = w^T E^{-1} w in row order and ends the
+// iteration: (r, z) = (r, D^-1 r) + (w, c). The kernel boundaries replace fences and tickets.
 __device__ __forceinline__ int64_t lower_tile(int i, int j) { return (int64_t)i * (i + 1) / 2 + j; }
 
-template <bool FIN>
-__global__ void __launch_bounds__(256) coarse_gemv_kernel(CoarseView cv, PcgState* st) {
-    __shared__ double wI[64], wJ[64];
-    __shared__ double colp[8][64];  // column partials per warp; the finisher's quarter sums
-    __shared__ double red[8];
+template <int PASS>
+__global__ void __launch_bounds__(256) coarse_wtile_kernel(CoarseView cv, const PcgState* st) {
+    __shared__ double v[64];
+    __shared__ double colp[8][64];
     if (st && st->done) return;
     const int t = blockIdx.x;
     int I = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
@@ -725,59 +723,36 @@ __global__ void __launch_bounds__(256) coarse_gemv_kernel(CoarseView cv, PcgStat
     const int J = t - I * (I + 1) / 2;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int tx = lane & 15, ty = 2 * warp + (lane >> 4);
-    const double* E = cv.einv + (int64_t)t * 4096;
-    double rp[4], cp[4] = {0.0, 0.0, 0.0, 0.0};
-    double2 ev[4][2];
-    // the tile's loads first: they do not wait for w
+    const float* W = cv.w32 + (int64_t)t * 4096;
+    float4 ev[4];
+    // the tile's loads first: they do not wait for the vector
 #pragma unroll
-    for (int a = 0; a < 4; ++a) {
-        const double2* row = reinterpret_cast<const double2*>(E + 64 * (4 * ty + a) + 4 * tx);
-        ev[a][0] = ld_once(row);
-        ev[a][1] = ld_once(row + 1);
-    }
-    if (tid < 64) {
-        wI[tid] = cv.w[64 * I + tid];
-        wJ[tid] = cv.w[64 * J + tid];
-    }
+    for (int a = 0; a < 4; ++a) ev[a] = ld_once(reinterpret_cast<const float4*>(W + 64 * (4 * ty + a) + 4 * tx));
+    if (tid < 64) v[tid] = PASS == 0 ? cv.w[64 * J + tid] : cv.y[64 * I + tid];
     __syncthreads();
-#pragma unroll
-    for (int a = 0; a < 4; ++a) {
-        const double e[4] = {ev[a][0].x, ev[a][0].y, ev[a][1].x, ev[a][1].y};
-        const double wi = wI[4 * ty + a];
-        rp[a] = 0.0;
-#pragma unroll
-        for (int b = 0; b < 4; ++b) {
-            rp[a] += e[b] * wJ[4 * tx + b];
-            cp[b] += e[b] * wi;
-        }
-    }
-    // row sums over the 16 tx of a half warp
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int o = 8; o > 0; o >>= 1) rp[a] += __shfl_xor_sync(0xffffffffu, rp[a], o);
     double* gp = cv.gpart + (int64_t)t * 128;
-    if (tx == 0)
+    if (PASS == 0) {
+        double rp[4];
 #pragma unroll
-        for (int a = 0; a < 4; ++a) gp[4 * ty + a] = rp[a];
-    if (FIN) {
-        // this tile's share of w^T E^{-1} w: rows in order within the patch, the two half warps,
-        // then the warps in order
-        double sw = 0.0;
+        for (int a = 0; a < 4; ++a) {
+            rp[a] = (double)ev[a].x * v[4 * tx] + (double)ev[a].y * v[4 * tx + 1] + (double)ev[a].z * v[4 * tx + 2] +
+                    (double)ev[a].w * v[4 * tx + 3];
+#pragma unroll
+            for (int o = 8; o > 0; o >>= 1) rp[a] += __shfl_xor_sync(0xffffffffu, rp[a], o);
+        }
         if (tx == 0)
 #pragma unroll
-            for (int a = 0; a < 4; ++a) sw += wI[4 * ty + a] * rp[a];
-        sw += __shfl_xor_sync(0xffffffffu, sw, 16);
-        if (lane == 0) red[warp] = sw;
-        __syncthreads();
-        if (tid == 0) {
-            double x = 0.0;
+            for (int a = 0; a < 4; ++a) gp[4 * ty + a] = rp[a];
+    } else {
+        double cp[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-            for (int q = 0; q < 8; ++q) x += red[q];
-            cv.tilewc[t] = I != J ? 2.0 * x : x;
+        for (int a = 0; a < 4; ++a) {
+            const double va = v[4 * ty + a];
+            cp[0] += (double)ev[a].x * va;
+            cp[1] += (double)ev[a].y * va;
+            cp[2] += (double)ev[a].z * va;
+            cp[3] += (double)ev[a].w * va;
         }
-    }
-    if (I != J) {
         // column sums: the two half warps, then the warps in order
 #pragma unroll
         for (int b = 0; b < 4; ++b) cp[b] += __shfl_xor_sync(0xffffffffu, cp[b], 16);
@@ -794,51 +769,65 @@ __global__ void __launch_bounds__(256) coarse_gemv_kernel(CoarseView cv, PcgStat
     }
 }
 
-// The GEMV's second kernel (the kernel boundary orders it after every tile): CTA X < nb sums
-// tile row X's slots in tile order into c_X (kFinishGroups groups of 64 threads each take a
-// contiguous share of the nb slots, added in order, so each thread waits for only a few loads);
-// FIN: CTA nb adds the tiles' shares of w^T E^{-1} w in tile order and ends the iteration:
-// (r, z) = (r, D^-1 r) + (w, c), ||r||^2 from the update.
+// Row kernel of a pass: CTA X < nb adds tile row X's slots in tile order (kFinishGroups groups
+// of 64 threads each take a contiguous share, added in order, so each thread waits for only a
+// few loads). Pass 1: y_X = sum_{J <= X} slot(X, J), and FIN: y_X . y_X into rowyy[X]. Pass 2:
+// c_X = sum_{I >= X} slot(I, X), and FIN: CTA nb adds rowyy in row order and ends the iteration.
 constexpr int kFinishGroups = 16;
-template <bool FIN>
-__global__ void __launch_bounds__(64 * kFinishGroups) coarse_gemv_finish_kernel(CoarseView cv, PcgState* st) {
+template <int PASS, bool FIN>
+__global__ void __launch_bounds__(64 * kFinishGroups) coarse_wrow_kernel(CoarseView cv, PcgState* st) {
     __shared__ double part[kFinishGroups][64];
     __shared__ double sh[32];
     if (st && st->done) return;
     const int tid = threadIdx.x;
     const int X = blockIdx.x;
-    if (X == cv.nb) {
-        const uint32_t ntiles = (uint32_t)((int64_t)cv.nb * (cv.nb + 1) / 2);
-        const uint32_t per = (ntiles + blockDim.x - 1) / blockDim.x;
-        const uint32_t k0 = tid * per, k1 = min(ntiles, k0 + per);
-        double x = 0.0;
-        for (uint32_t k = k0; k < k1; ++k) x += cv.tilewc[k];
+    if (PASS == 1 && FIN && X == cv.nb) {
+        double x = tid < cv.nb ? cv.rowyy[tid] : 0.0;  // nb <= 1024: one row each, in row order
         x = block_sum(x, sh);
         if (tid == 0) finish_iter(st, st->rdr + x, st->rr);
         return;
     }
     const int g = tid >> 6, i = tid & 63;
-    const int per = (cv.nb + kFinishGroups - 1) / kFinishGroups, k0 = g * per, k1 = min(cv.nb, k0 + per);
+    const int k_lo = PASS == 0 ? 0 : X, k_hi = PASS == 0 ? X + 1 : cv.nb;  // tiles (X, K) / (K, X)
+    const int per = (k_hi - k_lo + kFinishGroups - 1) / kFinishGroups;
+    const int k0 = k_lo + g * per, k1 = min(k_hi, k0 + per);
     double x = 0.0;
 #pragma unroll 4
     for (int K = k0; K < k1; ++K)
-        x += K <= X ? cv.gpart[lower_tile(X, K) * 128 + i] : cv.gpart[lower_tile(K, X) * 128 + 64 + i];
+        x += PASS == 0 ? cv.gpart[lower_tile(X, K) * 128 + i] : cv.gpart[lower_tile(K, X) * 128 + 64 + i];
     part[g][i] = x;
     __syncthreads();
     if (tid < 64) {
         double c = 0.0;
 #pragma unroll
         for (int q = 0; q < kFinishGroups; ++q) c += part[q][tid];
-        cv.c[64 * X + tid] = c;
+        if (PASS == 0) {
+            cv.y[64 * X + tid] = c;
+            if (FIN) {
+                double yy = c * c;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) yy += __shfl_xor_sync(0xffffffffu, yy, o);
+                if ((tid & 31) == 0) sh[tid >> 5] = yy;
+            }
+        } else {
+            cv.c[64 * X + tid] = c;
+        }
+    }
+    if (PASS == 0 && FIN) {
+        __syncthreads();
+        if (tid == 0) cv.rowyy[X] = sh[0] + sh[1];
     }
 }
 
-// the coarse GEMV: one CTA per stored tile of E^{-1}, then one per tile row (and FIN: one for
-// the end of the iteration)
+// the coarse GEMV c = W~^T (W~ w): per pass, one CTA per stored tile, then one per tile row (FIN:
+// and one for the end of the iteration)
 template <bool FIN>
 void launch_gemv(const CoarseView& cv, PcgState* st, cudaStream_t s) {
-    coarse_gemv_kernel<FIN><<<(unsigned)((int64_t)cv.nb * (cv.nb + 1) / 2), 256, 0, s>>>(cv, st);
-    coarse_gemv_finish_kernel<FIN><<<(unsigned)(cv.nb + (FIN ? 1 : 0)), 64 * kFinishGroups, 0, s>>>(cv, st);
+    const unsigned tiles = (unsigned)((int64_t)cv.nb * (cv.nb + 1) / 2);
+    coarse_wtile_kernel<0><<<tiles, 256, 0, s>>>(cv, st);
+    coarse_wrow_kernel<0, FIN><<<(unsigned)cv.nb, 64 * kFinishGroups, 0, s>>>(cv, st);
+    coarse_wtile_kernel<1><<<tiles, 256, 0, s>>>(cv, st);
+    coarse_wrow_kernel<1, FIN><<<(unsigned)(cv.nb + (FIN ? 1 : 0)), 64 * kFinishGroups, 0, s>>>(cv, st);
 }
 
 // z = D^{-1} r + Z c with the fused (r, z), (z, z); INIT also sets p = z and the initial state
@@ -1400,7 +1389,7 @@ int Pcg<VT, XT>::solve(const VT* val, const XT* b, XT* x, double rtol, double ab
         coarse_final_kernel<XT, true><<<resident_grid((const void*)coarse_final_kernel<XT, true>, A_.n_node, kThreads, sm_), kThreads, 0, s>>>(
             A_.n_node, coarse_, r_.p, z_.p, p_.p, dinv32_.p, partials_.p, partials2_.p, st_.p, rtol, abstol, dtol,
             maxit, norm_type);
-        launches += 6;
+        launches += 8;
     } else {
         pcg_init_kernel<XT, false><<<gv, kThreads, 0, s>>>(n_, b, x, r_.p, z_.p, p_.p, nullptr, nullptr, nullptr,
                                                             st_.p, rtol, abstol, dtol, maxit, norm_type);
@@ -1409,7 +1398,7 @@ int Pcg<VT, XT>::solve(const VT* val, const XT* b, XT* x, double rtol, double ab
         if (kind_ == PcKind::FactorCoarse) {
             launch_restrict<XT>(coarse_, r_.p, nullptr, s, sm_);
             launch_gemv<false>(coarse_, nullptr, s);
-            launches += 3;
+            launches += 5;
         }
         factor_apply_kernel<XT, true><<<gg, kThreads, 0, s>>>(factor_.GT, kind_ == PcKind::FactorCoarse ? coarse_ : CoarseView{},
                                                                factor_.gtval, t_.p, z_.p, r_.p, p_.p,
@@ -1438,8 +1427,8 @@ int Pcg<VT, XT>::solve(const VT* val, const XT* b, XT* x, double rtol, double ab
     }
     const int per_iter = kind_ == PcKind::Jacobi ? 3
                          : kind_ == PcKind::Factor ? 5
-                         : kind_ == PcKind::FactorCoarse ? 8
-                         : norm_type == 1 ? 6 : 7;
+                         : kind_ == PcKind::FactorCoarse ? 10
+                         : norm_type == 1 ? 8 : 9;
     PcgState h{};
     // every replay advances at most chunk_ iterations; the device stops at maxit
     const int64_t max_replays = (int64_t)(maxit > 0 ? maxit : 0) / chunk_ + 2;

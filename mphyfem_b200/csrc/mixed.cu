@@ -369,7 +369,7 @@ int minres(mphy_mixed* m, int32_t* its_out, double* relres) {
     scale_kernel<<<grid, 256, 0, st>>>(n, m->dinv.p, m->v[1].p, m->z[0].p);
     if (m->use_coarse) {
         coarse_apply_add(m->coarse.view(), m->n_node, m->v[1].p, m->z[0].p, st, sm);
-        m->launches += 4;
+        m->launches += 6;
     }
     dot_fp64(m->z[0].p, m->v[1].p, n, m->partials.p, m->counter.p, sc + S_DOT2, st, sm);
     double g0sq = 0.0;
@@ -388,7 +388,7 @@ int minres(mphy_mixed* m, int32_t* its_out, double* relres) {
                                                   m->v[iv_new].p, m->z[iz_new].p);
             if (m->use_coarse) {
                 coarse_apply_add(m->coarse.view(), m->n_node, m->v[iv_new].p, m->z[iz_new].p, st, sm);
-                m->launches += 4;
+                m->launches += 6;
             }
             dot_fp64(m->z[iz_new].p, m->v[iv_new].p, n, m->partials.p, m->counter.p, sc + S_DOT2, st, sm);
             minres_scalar_kernel<<<1, 1, 0, st>>>(sc, m->opts.rtol);
