@@ -94,7 +94,9 @@ typedef struct mphy_solver_opts {
     int32_t coarse_aggregates; /* > 0: add the two-level rigid-body coarse correction
                                 * M^{-1} = D^{-1} + Z (Z^T A Z)^{-1} Z^T over about this many
                                 * geometric aggregates (6 modes each) to the local
-                                * preconditioner (Jacobi: D^{-1}, FSAI: G^T G); about one
+                                * preconditioner (Jacobi: D^{-1}, FSAI: G^T G); the coarse
+                                * inverse is applied as W^T W with W the inverse Cholesky
+                                * factor rounded to FP32 (still SPD); about one
                                 * aggregate per 1,300 nodes was the measured optimum on the
                                 * 1.1 M-node hex8 and 1.8 M-node tet10 cantilevers */
     int32_t norm_type;     /* KSP norm of the convergence test: 0 = preconditioned ||z|| (PETSc's
